@@ -1,0 +1,738 @@
+// pms_oracle.cpp -- CPU restatement of pmsim 0.3.0's implicit solid hot path.
+//
+// TEST INFRASTRUCTURE ONLY.  This file is the parity oracle: the tests, the smoke check
+// and the CPU-baseline leg of bench.py load it as the checker (or as the timed CPU
+// restatement).  The product path (pmsim_b200, libpms_b200.so) never links or calls it.
+//
+// What it restates (reference file:line, paths inside the pmsim project):
+//   * VonMises::update_stress / stiffness        src/material/von_mises.rs:124-226
+//   * LinearElastic::update_stress / stiffness   src/material/linear_elastic.rs:49-71
+//   * LocalState (elastic, int_vars=[z,lambda], stress)  src/material/local_state.rs:9-44
+//   * calculate_strain (2D plane strain, 3D)     src/base/calculate_strain.rs:18-60
+//   * ElementSolid::calc_f_int / calc_jacobian / update_secondary_values
+//                                                src/fem/element_solid.rs:124-224
+//   * assemble_vector / assemble_matrix (COO with duplicates, symmetry check)
+//                                                src/base/assembly.rs:38-139
+//   * Elements loops over cells                  src/fem/elements.rs:132-205
+// Third-party arithmetic the reference delegates to un-vendored crates (gemlab,
+// russell_tensor; path dependencies with no lockfile, so their versions are unpinned)
+// is restated from the textbook mathematics:
+//   * Lagrange / serendipity shape functions of Tri3/Tri6/Qua4/Qua8/Qua9/Tet4/Tet10/
+//     Hex8/Hex20 (Zienkiewicz & Taylor, The Finite Element Method, Vol. 1, ch. 6),
+//   * tensor-product Gauss-Legendre rules on [-1,1]^d and the standard interior rules of
+//     the reference triangle/tetrahedron (Strang & Fix; Hammer-Stroud),
+//   * Mandel (Kelvin) notation for symmetric second/fourth order tensors,
+//     sigma = [xx, yy, zz, sqrt2*xy, sqrt2*yz, sqrt2*xz] (de Souza Neto, Peric & Owen,
+//     Computational Methods for Plasticity, 2008).
+// Node ordering (corners, then mid-edges 0-1,1-2,2-3,3-0 for Qua8; bottom, top, vertical
+// mid-edges for Hex20) is the one pinned by the reference's mesh files
+// (data/results/artificial/*.msh, src/base/sample_meshes.rs:541-625).
+// Parity pins: the inline KATs of src/material/von_mises.rs:324-480 and the SPO/HYPLAS
+// golden runs (data/spo/*.json) replayed by oracle/driver.py (tests/test_oracle_*.py).
+
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <vector>
+#include <algorithm>
+#include <numeric>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+namespace {
+
+enum Kind { TRI3 = 0, TRI6 = 1, QUA4 = 2, QUA8 = 3, QUA9 = 4, TET4 = 5, TET10 = 6, HEX8 = 7, HEX20 = 8 };
+
+const double SQRT2 = 1.4142135623730951;
+const double SQRT_2_BY_3 = 0.816496580927726;   // sqrt(2/3)
+const double F_TOL = 1e-6;                       // src/material/von_mises.rs:23
+
+int kind_nnode(int k) {
+    static const int n[] = {3, 6, 4, 8, 9, 4, 10, 8, 20};
+    return (k >= 0 && k <= 8) ? n[k] : -1;
+}
+int kind_ndim(int k) { return (k <= QUA9) ? 2 : 3; }
+
+int default_ngauss(int k) {
+    static const int n[] = {3, 3, 4, 9, 9, 4, 4, 8, 27};
+    return (k >= 0 && k <= 8) ? n[k] : -1;
+}
+
+// ---------------------------------------------------------------- Gauss rules
+void legendre_1d(int n, double* x, double* w) {
+    if (n == 1) { x[0] = 0.0; w[0] = 2.0; }
+    else if (n == 2) { double a = 1.0 / std::sqrt(3.0); x[0] = -a; x[1] = a; w[0] = w[1] = 1.0; }
+    else { double a = std::sqrt(3.0 / 5.0); x[0] = -a; x[1] = 0.0; x[2] = a;
+           w[0] = 5.0 / 9.0; w[1] = 8.0 / 9.0; w[2] = 5.0 / 9.0; }
+}
+
+// Tensor-product rule, x varies fastest, then y, then z.
+int gauss_rule(int kind, int ngauss, double* ksi /*ngauss*3*/, double* w) {
+    int nd = kind_ndim(kind);
+    bool simplex = (kind == TRI3 || kind == TRI6 || kind == TET4 || kind == TET10);
+    if (!simplex) {
+        int n1 = 0;
+        if (nd == 2) { if (ngauss == 1) n1 = 1; else if (ngauss == 4) n1 = 2; else if (ngauss == 9) n1 = 3; }
+        else { if (ngauss == 1) n1 = 1; else if (ngauss == 8) n1 = 2; else if (ngauss == 27) n1 = 3; }
+        if (n1 == 0) return -1;
+        double x[3], ww[3];
+        legendre_1d(n1, x, ww);
+        int p = 0;
+        int nz = (nd == 3) ? n1 : 1;
+        for (int k = 0; k < nz; k++)
+            for (int j = 0; j < n1; j++)
+                for (int i = 0; i < n1; i++) {
+                    ksi[3 * p + 0] = x[i];
+                    ksi[3 * p + 1] = x[j];
+                    ksi[3 * p + 2] = (nd == 3) ? x[k] : 0.0;
+                    w[p] = ww[i] * ww[j] * ((nd == 3) ? ww[k] : 1.0);
+                    p++;
+                }
+        return p;
+    }
+    if (nd == 2) {
+        if (ngauss == 1) { ksi[0] = 1.0 / 3.0; ksi[1] = 1.0 / 3.0; ksi[2] = 0; w[0] = 0.5; return 1; }
+        if (ngauss == 3) {
+            const double a = 1.0 / 6.0, b = 2.0 / 3.0;
+            double pts[3][2] = {{a, a}, {b, a}, {a, b}};
+            for (int p = 0; p < 3; p++) { ksi[3*p] = pts[p][0]; ksi[3*p+1] = pts[p][1]; ksi[3*p+2] = 0; w[p] = 1.0 / 6.0; }
+            return 3;
+        }
+        return -1;
+    }
+    if (ngauss == 1) { ksi[0] = ksi[1] = ksi[2] = 0.25; w[0] = 1.0 / 6.0; return 1; }
+    if (ngauss == 4) {
+        const double a = (5.0 + 3.0 * std::sqrt(5.0)) / 20.0, b = (5.0 - std::sqrt(5.0)) / 20.0;
+        double pts[4][3] = {{b, b, b}, {a, b, b}, {b, a, b}, {b, b, a}};
+        for (int p = 0; p < 4; p++) { for (int d = 0; d < 3; d++) ksi[3*p+d] = pts[p][d]; w[p] = 1.0 / 24.0; }
+        return 4;
+    }
+    return -1;
+}
+
+// ---------------------------------------------------------------- shape functions
+// N[m], dN[m*nd + j] = dN_m/dksi_j
+void shape(int kind, const double* k, double* N, double* dN) {
+    const double r = k[0], s = k[1], t = k[2];
+    switch (kind) {
+    case TRI3:
+        N[0] = 1 - r - s; N[1] = r; N[2] = s;
+        dN[0] = -1; dN[1] = -1; dN[2] = 1; dN[3] = 0; dN[4] = 0; dN[5] = 1;
+        break;
+    case TRI6: {
+        double L0 = 1 - r - s, L1 = r, L2 = s;
+        N[0] = L0 * (2 * L0 - 1); N[1] = L1 * (2 * L1 - 1); N[2] = L2 * (2 * L2 - 1);
+        N[3] = 4 * L0 * L1; N[4] = 4 * L1 * L2; N[5] = 4 * L2 * L0;
+        // dL0 = (-1,-1), dL1 = (1,0), dL2 = (0,1)
+        double d0 = 4 * L0 - 1, d1 = 4 * L1 - 1, d2 = 4 * L2 - 1;
+        dN[0] = -d0; dN[1] = -d0;
+        dN[2] = d1;  dN[3] = 0;
+        dN[4] = 0;   dN[5] = d2;
+        dN[6] = 4 * (L0 - L1); dN[7] = -4 * L1;
+        dN[8] = 4 * L2;        dN[9] = 4 * L1;
+        dN[10] = -4 * L2;      dN[11] = 4 * (L0 - L2);
+        break;
+    }
+    case QUA4: {
+        static const double xi[4][2] = {{-1, -1}, {1, -1}, {1, 1}, {-1, 1}};
+        for (int m = 0; m < 4; m++) {
+            double a = xi[m][0], b = xi[m][1];
+            N[m] = (1 + a * r) * (1 + b * s) / 4.0;
+            dN[2 * m] = a * (1 + b * s) / 4.0;
+            dN[2 * m + 1] = b * (1 + a * r) / 4.0;
+        }
+        break;
+    }
+    case QUA8: {
+        static const double xi[8][2] = {{-1, -1}, {1, -1}, {1, 1}, {-1, 1}, {0, -1}, {1, 0}, {0, 1}, {-1, 0}};
+        for (int m = 0; m < 8; m++) {
+            double a = xi[m][0], b = xi[m][1];
+            if (m < 4) {
+                N[m] = (1 + a * r) * (1 + b * s) * (a * r + b * s - 1) / 4.0;
+                dN[2 * m] = a * (1 + b * s) * (2 * a * r + b * s) / 4.0;
+                dN[2 * m + 1] = b * (1 + a * r) * (a * r + 2 * b * s) / 4.0;
+            } else if (a == 0) {
+                N[m] = (1 - r * r) * (1 + b * s) / 2.0;
+                dN[2 * m] = -r * (1 + b * s);
+                dN[2 * m + 1] = b * (1 - r * r) / 2.0;
+            } else {
+                N[m] = (1 + a * r) * (1 - s * s) / 2.0;
+                dN[2 * m] = a * (1 - s * s) / 2.0;
+                dN[2 * m + 1] = -s * (1 + a * r);
+            }
+        }
+        break;
+    }
+    case QUA9: {
+        // 1D quadratic Lagrange at -1, 0, +1
+        auto l = [](int i, double x) { return i == 0 ? x * (x - 1) / 2.0 : (i == 1 ? 1 - x * x : x * (x + 1) / 2.0); };
+        auto dl = [](int i, double x) { return i == 0 ? x - 0.5 : (i == 1 ? -2 * x : x + 0.5); };
+        static const int ij[9][2] = {{0, 0}, {2, 0}, {2, 2}, {0, 2}, {1, 0}, {2, 1}, {1, 2}, {0, 1}, {1, 1}};
+        for (int m = 0; m < 9; m++) {
+            int i = ij[m][0], j = ij[m][1];
+            N[m] = l(i, r) * l(j, s);
+            dN[2 * m] = dl(i, r) * l(j, s);
+            dN[2 * m + 1] = l(i, r) * dl(j, s);
+        }
+        break;
+    }
+    case TET4:
+        N[0] = 1 - r - s - t; N[1] = r; N[2] = s; N[3] = t;
+        for (int j = 0; j < 3; j++) dN[j] = -1;
+        dN[3] = 1; dN[4] = 0; dN[5] = 0;
+        dN[6] = 0; dN[7] = 1; dN[8] = 0;
+        dN[9] = 0; dN[10] = 0; dN[11] = 1;
+        break;
+    case TET10: {
+        double L[4] = {1 - r - s - t, r, s, t};
+        static const double dL[4][3] = {{-1, -1, -1}, {1, 0, 0}, {0, 1, 0}, {0, 0, 1}};
+        static const int ed[6][2] = {{0, 1}, {1, 2}, {2, 0}, {0, 3}, {1, 3}, {2, 3}};
+        for (int m = 0; m < 4; m++) {
+            N[m] = L[m] * (2 * L[m] - 1);
+            for (int j = 0; j < 3; j++) dN[3 * m + j] = (4 * L[m] - 1) * dL[m][j];
+        }
+        for (int e = 0; e < 6; e++) {
+            int a = ed[e][0], b = ed[e][1], m = 4 + e;
+            N[m] = 4 * L[a] * L[b];
+            for (int j = 0; j < 3; j++) dN[3 * m + j] = 4 * (dL[a][j] * L[b] + L[a] * dL[b][j]);
+        }
+        break;
+    }
+    case HEX8: {
+        static const double xi[8][3] = {{-1, -1, -1}, {1, -1, -1}, {1, 1, -1}, {-1, 1, -1},
+                                        {-1, -1, 1},  {1, -1, 1},  {1, 1, 1},  {-1, 1, 1}};
+        for (int m = 0; m < 8; m++) {
+            double a = xi[m][0], b = xi[m][1], c = xi[m][2];
+            N[m] = (1 + a * r) * (1 + b * s) * (1 + c * t) / 8.0;
+            dN[3 * m] = a * (1 + b * s) * (1 + c * t) / 8.0;
+            dN[3 * m + 1] = b * (1 + a * r) * (1 + c * t) / 8.0;
+            dN[3 * m + 2] = c * (1 + a * r) * (1 + b * s) / 8.0;
+        }
+        break;
+    }
+    case HEX20: {
+        static const double xi[20][3] = {
+            {-1, -1, -1}, {1, -1, -1}, {1, 1, -1}, {-1, 1, -1}, {-1, -1, 1}, {1, -1, 1}, {1, 1, 1}, {-1, 1, 1},
+            {0, -1, -1},  {1, 0, -1},  {0, 1, -1}, {-1, 0, -1}, {0, -1, 1},  {1, 0, 1},  {0, 1, 1}, {-1, 0, 1},
+            {-1, -1, 0},  {1, -1, 0},  {1, 1, 0},  {-1, 1, 0}};
+        for (int m = 0; m < 20; m++) {
+            double a = xi[m][0], b = xi[m][1], c = xi[m][2];
+            if (m < 8) {
+                double ar = 1 + a * r, bs = 1 + b * s, ct = 1 + c * t, q = a * r + b * s + c * t - 2;
+                N[m] = ar * bs * ct * q / 8.0;
+                dN[3 * m] = a * bs * ct * (q + ar) / 8.0;
+                dN[3 * m + 1] = b * ar * ct * (q + bs) / 8.0;
+                dN[3 * m + 2] = c * ar * bs * (q + ct) / 8.0;
+            } else if (a == 0) {
+                double bs = 1 + b * s, ct = 1 + c * t;
+                N[m] = (1 - r * r) * bs * ct / 4.0;
+                dN[3 * m] = -2 * r * bs * ct / 4.0;
+                dN[3 * m + 1] = (1 - r * r) * b * ct / 4.0;
+                dN[3 * m + 2] = (1 - r * r) * bs * c / 4.0;
+            } else if (b == 0) {
+                double ar = 1 + a * r, ct = 1 + c * t;
+                N[m] = ar * (1 - s * s) * ct / 4.0;
+                dN[3 * m] = a * (1 - s * s) * ct / 4.0;
+                dN[3 * m + 1] = -2 * s * ar * ct / 4.0;
+                dN[3 * m + 2] = ar * (1 - s * s) * c / 4.0;
+            } else {
+                double ar = 1 + a * r, bs = 1 + b * s;
+                N[m] = ar * bs * (1 - t * t) / 4.0;
+                dN[3 * m] = a * bs * (1 - t * t) / 4.0;
+                dN[3 * m + 1] = ar * b * (1 - t * t) / 4.0;
+                dN[3 * m + 2] = -2 * t * ar * bs / 4.0;
+            }
+        }
+        break;
+    }
+    }
+}
+
+// ---------------------------------------------------------------- Mandel helpers
+// I = [1,1,1,0,0,0];  Psd = Id - I(x)I/3 (symmetric deviatoric projector)
+inline double Ivec(int i) { return i < 3 ? 1.0 : 0.0; }
+inline double Psd(int i, int j) {
+    if (i < 3 && j < 3) return (i == j) ? 2.0 / 3.0 : -1.0 / 3.0;
+    return (i == j) ? 1.0 : 0.0;
+}
+inline double sigma_m(const double* v) { return (v[0] + v[1] + v[2]) / 3.0; }
+inline double sigma_d(const double* v, int nc) {
+    double m = sigma_m(v), s2 = 0;
+    for (int i = 0; i < nc; i++) { double s = v[i] - (i < 3 ? m : 0.0); s2 += s * s; }
+    return std::sqrt(1.5 * s2);  // sqrt(3 J2), J2 = s:s/2
+}
+
+struct Params { double young, poisson, hh, z_ini; };
+
+void bulk_shear(const Params& p, double& kk, double& gg) {
+    kk = p.young / (3.0 * (1.0 - 2.0 * p.poisson));
+    gg = p.young / (2.0 * (1.0 + p.poisson));
+}
+
+// Hooke's modulus in Mandel form (plane strain uses the 4x4 top-left block)
+void elastic_modulus(const Params& p, int nc, double* dd) {
+    double c = p.young / ((1.0 + p.poisson) * (1.0 - 2.0 * p.poisson));
+    for (int i = 0; i < nc * nc; i++) dd[i] = 0;
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) dd[i * nc + j] = (i == j) ? c * (1.0 - p.poisson) : c * p.poisson;
+    for (int i = 3; i < nc; i++) dd[i * nc + i] = c * (1.0 - 2.0 * p.poisson);
+}
+
+// model: 0 = LinearElastic, 1 = VonMises.  ivs = [z, lambda]. returns 0 ok, else error code
+//   2: "von Mises plastic update must not lead to zero sigma_d (sigma_d < 1e-10)"
+//   3: "von Mises stiffness cannot be computed with zero deviatoric norm (norm_s < 1e-10)"
+int model_update_stress(int model, const Params& p, int nc, double* sig, double* ivs, uint8_t* elastic,
+                        const double* deps) {
+    double dd[36];
+    elastic_modulus(p, nc, dd);
+    if (model == 0) {  // src/material/linear_elastic.rs:61-71
+        double ds[6];
+        for (int i = 0; i < nc; i++) { ds[i] = 0; for (int j = 0; j < nc; j++) ds[i] += dd[i * nc + j] * deps[j]; }
+        for (int i = 0; i < nc; i++) sig[i] += ds[i];
+        return 0;
+    }
+    // src/material/von_mises.rs:170-226
+    *elastic = 1;
+    ivs[1] = 0.0;
+    double ds[6];
+    for (int i = 0; i < nc; i++) { ds[i] = 0; for (int j = 0; j < nc; j++) ds[i] += dd[i * nc + j] * deps[j]; }
+    for (int i = 0; i < nc; i++) sig[i] += ds[i];
+    double f_trial = sigma_d(sig, nc) - ivs[0];
+    if (f_trial / p.z_ini <= F_TOL) return 0;
+    double kk, gg;
+    bulk_shear(p, kk, gg);
+    double sm = sigma_m(sig), sd_trial = sigma_d(sig, nc);
+    double lambda = f_trial / (3.0 * gg + p.hh);
+    double beta = 1.0 - lambda * 3.0 * gg / sd_trial;
+    double s[6];
+    for (int i = 0; i < nc; i++) s[i] = sig[i] - (i < 3 ? sm : 0.0);
+    for (int i = 0; i < nc; i++) sig[i] = sm * Ivec(i) + beta * s[i];
+    if (sigma_d(sig, nc) < 1e-10) return 2;
+    ivs[0] += p.hh * lambda;
+    *elastic = 0;
+    ivs[1] = lambda;
+    return 0;
+}
+
+int model_stiffness(int model, const Params& p, int nc, const double* sig, const double* ivs, uint8_t elastic,
+                    double* dd) {
+    if (model == 0 || elastic) { elastic_modulus(p, nc, dd); return 0; }
+    // src/material/von_mises.rs:124-167
+    double kk, gg;
+    bulk_shear(p, kk, gg);
+    double lambda = ivs[1];
+    double sm = sigma_m(sig);
+    double s[6];
+    for (int i = 0; i < nc; i++) s[i] = sig[i] - (i < 3 ? sm : 0.0);
+    double sd = sigma_d(sig, nc);
+    double sd_trial = sd + lambda * 3.0 * gg;
+    double norm_s = sd * SQRT_2_BY_3;
+    if (norm_s < 1e-10) return 3;
+    double d = 3.0 * gg + p.hh;
+    double a = 2.0 * gg * (1.0 - lambda * 3.0 * gg / sd_trial);
+    double b = 6.0 * gg * gg * (lambda / sd_trial - 1.0 / d) / (norm_s * norm_s);
+    for (int i = 0; i < nc; i++)
+        for (int j = 0; j < nc; j++) dd[i * nc + j] = a * Psd(i, j) + b * s[i] * s[j] + kk * Ivec(i) * Ivec(j);
+    return 0;
+}
+
+// ---------------------------------------------------------------- element geometry
+struct IpGeo { double det; double G[20 * 3]; double N[20]; };
+
+// returns 0 ok, 4 = non-positive Jacobian determinant
+int ip_geometry(int kind, const double* X /*nnode*nd*/, const double* ksi, IpGeo& g) {
+    int nn = kind_nnode(kind), nd = kind_ndim(kind);
+    double dN[20 * 3];
+    shape(kind, ksi, g.N, dN);
+    double J[9] = {0};
+    for (int m = 0; m < nn; m++)
+        for (int i = 0; i < nd; i++)
+            for (int j = 0; j < nd; j++) J[i * nd + j] += X[m * nd + i] * dN[m * nd + j];
+    double Ji[9];
+    if (nd == 2) {
+        g.det = J[0] * J[3] - J[1] * J[2];
+        if (!(g.det > 0)) return 4;
+        Ji[0] = J[3] / g.det; Ji[1] = -J[1] / g.det; Ji[2] = -J[2] / g.det; Ji[3] = J[0] / g.det;
+    } else {
+        g.det = J[0] * (J[4] * J[8] - J[5] * J[7]) - J[1] * (J[3] * J[8] - J[5] * J[6]) + J[2] * (J[3] * J[7] - J[4] * J[6]);
+        if (!(g.det > 0)) return 4;
+        Ji[0] = (J[4] * J[8] - J[5] * J[7]) / g.det;
+        Ji[1] = (J[2] * J[7] - J[1] * J[8]) / g.det;
+        Ji[2] = (J[1] * J[5] - J[2] * J[4]) / g.det;
+        Ji[3] = (J[5] * J[6] - J[3] * J[8]) / g.det;
+        Ji[4] = (J[0] * J[8] - J[2] * J[6]) / g.det;
+        Ji[5] = (J[2] * J[3] - J[0] * J[5]) / g.det;
+        Ji[6] = (J[3] * J[7] - J[4] * J[6]) / g.det;
+        Ji[7] = (J[1] * J[6] - J[0] * J[7]) / g.det;
+        Ji[8] = (J[0] * J[4] - J[1] * J[3]) / g.det;
+    }
+    // G[m][i] = sum_j dN[m][j] * Jinv[j][i]
+    for (int m = 0; m < nn; m++)
+        for (int i = 0; i < nd; i++) {
+            double v = 0;
+            for (int j = 0; j < nd; j++) v += dN[m * nd + j] * Ji[j * nd + i];
+            g.G[m * nd + i] = v;
+        }
+    return 0;
+}
+
+// Mandel B matrix, nc x (nn*nd), row-major
+void b_matrix(int nn, int nd, const double* G, double* B) {
+    int nc = 2 * nd, ne = nn * nd;
+    for (int i = 0; i < nc * ne; i++) B[i] = 0;
+    for (int m = 0; m < nn; m++) {
+        if (nd == 2) {
+            double gx = G[2 * m], gy = G[2 * m + 1];
+            B[0 * ne + 2 * m] = gx;
+            B[1 * ne + 2 * m + 1] = gy;
+            B[3 * ne + 2 * m] = gy / SQRT2;
+            B[3 * ne + 2 * m + 1] = gx / SQRT2;
+        } else {
+            double gx = G[3 * m], gy = G[3 * m + 1], gz = G[3 * m + 2];
+            B[0 * ne + 3 * m] = gx;
+            B[1 * ne + 3 * m + 1] = gy;
+            B[2 * ne + 3 * m + 2] = gz;
+            B[3 * ne + 3 * m] = gy / SQRT2; B[3 * ne + 3 * m + 1] = gx / SQRT2;
+            B[4 * ne + 3 * m + 1] = gz / SQRT2; B[4 * ne + 3 * m + 2] = gy / SQRT2;
+            B[5 * ne + 3 * m] = gz / SQRT2; B[5 * ne + 3 * m + 2] = gx / SQRT2;
+        }
+    }
+}
+
+struct ElemCtx {
+    int kind, nn, nd, nc, ngauss;
+    double ksi[27 * 3], w[27];
+    double thickness;
+};
+
+bool make_ctx(int kind, int ngauss, double thickness, ElemCtx& c) {
+    c.kind = kind;
+    c.nn = kind_nnode(kind);
+    if (c.nn < 0) return false;
+    c.nd = kind_ndim(kind);
+    c.nc = 2 * c.nd;
+    if (ngauss <= 0) ngauss = default_ngauss(kind);
+    c.ngauss = gauss_rule(kind, ngauss, c.ksi, c.w);
+    c.thickness = thickness;
+    return c.ngauss > 0;
+}
+
+// f_int: vec_04_tb -- f[m*nd+i] = sum_p sum_j sigma_ij G[m][j] |J| w_p t
+int elem_f_int(const ElemCtx& c, const double* X, const double* sig /*ngauss*nc*/, double* f) {
+    int ne = c.nn * c.nd;
+    for (int i = 0; i < ne; i++) f[i] = 0;
+    IpGeo g;
+    for (int p = 0; p < c.ngauss; p++) {
+        int st = ip_geometry(c.kind, X, c.ksi + 3 * p, g);
+        if (st) return st;
+        double coef = g.det * c.w[p] * c.thickness;
+        const double* v = sig + p * c.nc;
+        double S[3][3];
+        S[0][0] = v[0]; S[1][1] = v[1]; S[2][2] = v[2];
+        S[0][1] = S[1][0] = v[3] / SQRT2;
+        if (c.nd == 3) { S[1][2] = S[2][1] = v[4] / SQRT2; S[0][2] = S[2][0] = v[5] / SQRT2; }
+        for (int m = 0; m < c.nn; m++)
+            for (int i = 0; i < c.nd; i++) {
+                double s = 0;
+                for (int j = 0; j < c.nd; j++) s += S[i][j] * g.G[m * c.nd + j];
+                f[m * c.nd + i] += coef * s;
+            }
+    }
+    return 0;
+}
+
+// K: mat_10_bdb -- K = sum_p B^T D B |J| w_p t  (dense, as the reference does it)
+int elem_jacobian(const ElemCtx& c, const double* X, int model, const Params& prm, const double* sig,
+                  const double* ivs, const uint8_t* elastic, double* K) {
+    int ne = c.nn * c.nd;
+    for (int i = 0; i < ne * ne; i++) K[i] = 0;
+    IpGeo g;
+    std::vector<double> B(c.nc * ne), DB(c.nc * ne);
+    double dd[36];
+    for (int p = 0; p < c.ngauss; p++) {
+        int st = ip_geometry(c.kind, X, c.ksi + 3 * p, g);
+        if (st) return st;
+        st = model_stiffness(model, prm, c.nc, sig + p * c.nc, ivs + 2 * p, elastic[p], dd);
+        if (st) return st;
+        double coef = g.det * c.w[p] * c.thickness;
+        b_matrix(c.nn, c.nd, g.G, B.data());
+        for (int k = 0; k < c.nc; k++)
+            for (int col = 0; col < ne; col++) {
+                double s = 0;
+                for (int l = 0; l < c.nc; l++) s += dd[k * c.nc + l] * B[l * ne + col];
+                DB[k * ne + col] = s;
+            }
+        // upper triangle, mirrored: D is symmetric, so K is symmetric by construction
+        for (int r = 0; r < ne; r++)
+            for (int col = r; col < ne; col++) {
+                double s = 0;
+                for (int k = 0; k < c.nc; k++) s += B[k * ne + r] * DB[k * ne + col];
+                K[r * ne + col] += coef * s;
+            }
+    }
+    for (int r = 0; r < ne; r++)
+        for (int col = 0; col < r; col++) K[r * ne + col] = K[col * ne + r];
+    return 0;
+}
+
+// calculate_strain + update_stress at every IP (src/fem/element_solid.rs:190-224)
+int elem_update(const ElemCtx& c, const double* X, int model, const Params& prm, const double* du /*nn*nd*/,
+                double* sig, double* ivs, uint8_t* elastic, int* bad_ip) {
+    IpGeo g;
+    for (int p = 0; p < c.ngauss; p++) {
+        int st = ip_geometry(c.kind, X, c.ksi + 3 * p, g);
+        if (st) { if (bad_ip) *bad_ip = p; return st; }
+        double eps[6] = {0, 0, 0, 0, 0, 0};
+        if (c.nd == 2) {
+            for (int m = 0; m < c.nn; m++) {
+                double ux = du[2 * m], uy = du[2 * m + 1], gx = g.G[2 * m], gy = g.G[2 * m + 1];
+                eps[0] += ux * gx;
+                eps[1] += uy * gy;
+                eps[3] += SQRT2 * ((ux * gy + uy * gx) / 2.0);
+            }
+        } else {
+            for (int m = 0; m < c.nn; m++) {
+                double ux = du[3 * m], uy = du[3 * m + 1], uz = du[3 * m + 2];
+                double gx = g.G[3 * m], gy = g.G[3 * m + 1], gz = g.G[3 * m + 2];
+                eps[0] += ux * gx;
+                eps[1] += uy * gy;
+                eps[2] += uz * gz;
+                eps[3] += SQRT2 * ((ux * gy + uy * gx) / 2.0);
+                eps[4] += SQRT2 * ((uy * gz + uz * gy) / 2.0);
+                eps[5] += SQRT2 * ((ux * gz + uz * gx) / 2.0);
+            }
+        }
+        st = model_update_stress(model, prm, c.nc, sig + p * c.nc, ivs + 2 * p, elastic + p, eps);
+        if (st) { if (bad_ip) *bad_ip = p; return st; }
+    }
+    return 0;
+}
+
+void gather_X(const ElemCtx& c, const double* coords, const int64_t* conn, int64_t e, double* X) {
+    for (int m = 0; m < c.nn; m++) {
+        int64_t pt = conn[e * c.nn + m];
+        for (int i = 0; i < c.nd; i++) X[m * c.nd + i] = coords[pt * c.nd + i];
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+int orc_default_ngauss(int kind) { return default_ngauss(kind); }
+int orc_kind_nnode(int kind) { return kind_nnode(kind); }
+
+int orc_gauss(int kind, int ngauss, double* ksi, double* w) {
+    if (ngauss <= 0) ngauss = default_ngauss(kind);
+    return gauss_rule(kind, ngauss, ksi, w);
+}
+
+int orc_shape(int kind, const double* ksi, double* N, double* dN) {
+    if (kind_nnode(kind) < 0) return -1;
+    shape(kind, ksi, N, dN);
+    return 0;
+}
+
+int orc_model_update_stress(int model, const double* prm, int ndim, double* sig, double* ivs, uint8_t* elastic,
+                            const double* deps) {
+    Params p{prm[0], prm[1], prm[2], prm[3]};
+    return model_update_stress(model, p, 2 * ndim, sig, ivs, elastic, deps);
+}
+
+int orc_model_stiffness(int model, const double* prm, int ndim, const double* sig, const double* ivs,
+                        uint8_t elastic, double* dd) {
+    Params p{prm[0], prm[1], prm[2], prm[3]};
+    return model_stiffness(model, p, 2 * ndim, sig, ivs, elastic, dd);
+}
+
+// Batched material call over n IPs, AoS state (sig n*nc, ivs n*2, elastic n); optional OpenMP.
+int orc_model_update_and_stiffness_batch(int model, const double* prm, int ndim, int64_t n, double* sig, double* ivs,
+                                         uint8_t* elastic, const double* deps, double* dd /*n*nc*nc or null*/,
+                                         int nthreads) {
+    Params p{prm[0], prm[1], prm[2], prm[3]};
+    int nc = 2 * ndim;
+    int err = 0;
+#ifdef _OPENMP
+    if (nthreads <= 0) nthreads = omp_get_max_threads();
+#pragma omp parallel for num_threads(nthreads) schedule(static) reduction(max : err)
+#endif
+    for (int64_t i = 0; i < n; i++) {
+        int st = model_update_stress(model, p, nc, sig + i * nc, ivs + 2 * i, elastic + i, deps + i * nc);
+        if (!st && dd) st = model_stiffness(model, p, nc, sig + i * nc, ivs + 2 * i, elastic[i], dd + i * nc * nc);
+        if (st > err) err = st;
+    }
+    (void)nthreads;
+    return err;
+}
+
+int orc_elem_f_int(int kind, int ngauss, double thickness, const double* X, const double* sig, double* f) {
+    ElemCtx c;
+    if (!make_ctx(kind, ngauss, thickness, c)) return -1;
+    return elem_f_int(c, X, sig, f);
+}
+
+int orc_elem_jacobian(int kind, int ngauss, double thickness, const double* X, int model, const double* prm,
+                      const double* sig, const double* ivs, const uint8_t* elastic, double* K) {
+    ElemCtx c;
+    if (!make_ctx(kind, ngauss, thickness, c)) return -1;
+    Params p{prm[0], prm[1], prm[2], prm[3]};
+    return elem_jacobian(c, X, model, p, sig, ivs, elastic, K);
+}
+
+// ---- mesh level (Elements loops, src/fem/elements.rs:132-205) ----
+// State arrays are per IP in cell-major order: ip_global = cell*ngauss + p.
+// DOF numbering: eq = ndim*point + d (solid-only mesh, src/base/all_dofs.rs:87-116).
+
+int orc_assemble_f_int(int kind, int ngauss, double thickness, int64_t npoint, const double* coords, int64_t ncell,
+                       const int64_t* conn, const double* sig, double* ff /*npoint*nd, zeroed here*/) {
+    ElemCtx c;
+    if (!make_ctx(kind, ngauss, thickness, c)) return -1;
+    int ne = c.nn * c.nd;
+    for (int64_t i = 0; i < npoint * c.nd; i++) ff[i] = 0;
+    double X[60], f[60];
+    for (int64_t e = 0; e < ncell; e++) {
+        gather_X(c, coords, conn, e, X);
+        int st = elem_f_int(c, X, sig + e * c.ngauss * c.nc, f);
+        if (st) return st;
+        for (int l = 0; l < ne; l++) {
+            int m = l / c.nd, i = l % c.nd;
+            ff[conn[e * c.nn + m] * c.nd + i] += f[l];
+        }
+    }
+    return 0;
+}
+
+// COO triplets with duplicates, element order, l-major / ll-minor (src/base/assembly.rs:120-135).
+// rows/cols/vals hold ncell*ne*ne entries. sym_tol < 0 disables the symmetry check.
+// nthreads > 1 runs elements in parallel (each writes its own slice, so the output is identical).
+int orc_assemble_kk_coo(int kind, int ngauss, double thickness, const double* coords, int64_t ncell,
+                        const int64_t* conn, int model, const double* prm, const double* sig, const double* ivs,
+                        const uint8_t* elastic, double sym_tol, int64_t* rows, int64_t* cols, double* vals,
+                        int nthreads, int64_t* bad_cell) {
+    ElemCtx c;
+    if (!make_ctx(kind, ngauss, thickness, c)) return -1;
+    Params p{prm[0], prm[1], prm[2], prm[3]};
+    int ne = c.nn * c.nd;
+    int err = 0;
+    int64_t bad = -1;
+#ifdef _OPENMP
+    if (nthreads <= 0) nthreads = omp_get_max_threads();
+#pragma omp parallel num_threads(nthreads)
+#endif
+    {
+        std::vector<double> K(ne * ne);
+        double X[60];
+#ifdef _OPENMP
+#pragma omp for schedule(dynamic, 64)
+#endif
+        for (int64_t e = 0; e < ncell; e++) {
+            gather_X(c, coords, conn, e, X);
+            int64_t ip0 = e * c.ngauss;
+            int st = elem_jacobian(c, X, model, p, sig + ip0 * c.nc, ivs + ip0 * 2, elastic + ip0, K.data());
+            if (!st && sym_tol >= 0) {
+                for (int l = 0; l < ne && !st; l++)
+                    for (int ll = l + 1; ll < ne; ll++)
+                        if (std::fabs(K[l * ne + ll] - K[ll * ne + l]) > sym_tol) { st = 5; break; }
+            }
+            if (st) {
+#ifdef _OPENMP
+#pragma omp critical
+#endif
+                { if (st > err) { err = st; bad = e; } }
+                continue;
+            }
+            int64_t o = e * (int64_t)ne * ne;
+            for (int l = 0; l < ne; l++) {
+                int64_t g = conn[e * c.nn + l / c.nd] * c.nd + l % c.nd;
+                for (int ll = 0; ll < ne; ll++) {
+                    int64_t gg = conn[e * c.nn + ll / c.nd] * c.nd + ll % c.nd;
+                    rows[o] = g; cols[o] = gg; vals[o] = K[l * ne + ll]; o++;
+                }
+            }
+        }
+    }
+    (void)nthreads;
+    if (bad_cell) *bad_cell = bad;
+    return err;
+}
+
+// COO (with duplicates) -> CSR, summing duplicates in insertion order.
+// Pass 1 (rowptr only): indptr must hold nrow+1; returns nnz.  Pass 2 fills indices/data.
+int64_t orc_coo_to_csr(int64_t nrow, int64_t ntrip, const int64_t* rows, const int64_t* cols, const double* vals,
+                       int64_t* indptr, int64_t* indices, double* data) {
+    std::vector<int64_t> cnt(nrow + 1, 0);
+    for (int64_t k = 0; k < ntrip; k++) cnt[rows[k] + 1]++;
+    for (int64_t r = 0; r < nrow; r++) cnt[r + 1] += cnt[r];
+    std::vector<int64_t> order(ntrip);
+    {
+        std::vector<int64_t> pos(cnt.begin(), cnt.end() - 1);
+        for (int64_t k = 0; k < ntrip; k++) order[pos[rows[k]]++] = k;
+    }
+    int64_t nnz = 0;
+    std::vector<int64_t> rowptr(nrow + 1, 0);
+    std::vector<int64_t> tmp;
+    for (int64_t r = 0; r < nrow; r++) {
+        int64_t a = cnt[r], b = cnt[r + 1];
+        tmp.assign(order.begin() + a, order.begin() + b);
+        std::stable_sort(tmp.begin(), tmp.end(), [&](int64_t x, int64_t y) { return cols[x] < cols[y]; });
+        int64_t prev = -1;
+        for (int64_t k : tmp) {
+            if (cols[k] != prev) {
+                if (indices) { indices[nnz] = cols[k]; data[nnz] = vals[k]; }
+                nnz++;
+                prev = cols[k];
+            } else if (indices) {
+                data[nnz - 1] += vals[k];
+            }
+        }
+        rowptr[r + 1] = nnz;
+    }
+    if (indptr) std::memcpy(indptr, rowptr.data(), (nrow + 1) * sizeof(int64_t));
+    return nnz;
+}
+
+// update_secondary_values over all cells; ddu is the global (step) displacement increment.
+int orc_update_secondary(int kind, int ngauss, double thickness, const double* coords, int64_t ncell,
+                         const int64_t* conn, int model, const double* prm, const double* ddu, double* sig,
+                         double* ivs, uint8_t* elastic, int nthreads, int64_t* bad_cell, int* bad_ip) {
+    ElemCtx c;
+    if (!make_ctx(kind, ngauss, thickness, c)) return -1;
+    Params p{prm[0], prm[1], prm[2], prm[3]};
+    int err = 0;
+    int64_t bc = -1;
+    int bi = -1;
+#ifdef _OPENMP
+    if (nthreads <= 0) nthreads = omp_get_max_threads();
+#pragma omp parallel for num_threads(nthreads) schedule(dynamic, 64)
+#endif
+    for (int64_t e = 0; e < ncell; e++) {
+        double X[60], du[60];
+        gather_X(c, coords, conn, e, X);
+        for (int m = 0; m < c.nn; m++)
+            for (int i = 0; i < c.nd; i++) du[m * c.nd + i] = ddu[conn[e * c.nn + m] * c.nd + i];
+        int64_t ip0 = e * c.ngauss;
+        int ip = -1;
+        int st = elem_update(c, X, model, p, du, sig + ip0 * c.nc, ivs + ip0 * 2, elastic + ip0, &ip);
+        if (st) {
+#ifdef _OPENMP
+#pragma omp critical
+#endif
+            { if (st > err) { err = st; bc = e; bi = ip; } }
+        }
+    }
+    (void)nthreads;
+    if (bad_cell) *bad_cell = bc;
+    if (bad_ip) *bad_ip = bi;
+    return err;
+}
+
+int orc_max_threads() {
+#ifdef _OPENMP
+    return omp_get_max_threads();
+#else
+    return 1;
+#endif
+}
+
+}  // extern "C"

@@ -1,0 +1,210 @@
+"""Pins the CPU oracle against the reference's own golden data (no GPU needed).
+
+* von Mises KATs: reference ``src/material/von_mises.rs:288-480``
+* LinearElastic == VonMises elastic path: ``tests/test_elastic_in_elastoplastic.rs``
+* SPO/HYPLAS FE runs with the reference's own tolerances: ``tests/test_von_mises_*.rs``,
+  ``tests/test_spo_754_footing.rs``, ``tests/test_spo_755_tensile.rs``
+* linear-elastic Qua4 run: ``tests/test_solid_smith_5d11_qua4_plane_strain_uy.rs``
+* pmsim's own FemState output for uniform fields: ``data/results/artificial/*``
+"""
+import numpy as np
+import pytest
+
+import oracle
+from oracle.driver import OracleSolver
+from pmsim_b200.mesh import Mesh, kind_from_name
+import problems
+
+YOUNG, POISSON, HH, Z_INI = 1500.0, 0.25, 800.0, 9.0
+SQRT_3 = np.sqrt(3.0)
+SQRT_3_BY_2 = np.sqrt(1.5)
+
+
+def params():
+    return oracle.Params(YOUNG, POISSON, HH, Z_INI)
+
+
+def bulk_shear(E, nu):
+    return E / (3 * (1 - 2 * nu)), E / (2 * (1 + nu))
+
+
+def octahedral(eps_v, eps_d, lode, ndim):
+    """Diagonal strain with volumetric invariant eps_v = tr, deviatoric invariant
+    eps_d = sqrt(2/3)|dev| and Lode parameter cos(3 theta) (octahedral distance eps_v/sqrt3,
+    radius eps_d*sqrt(3/2), as Tensor2::new_from_octahedral builds it in the reference KATs)."""
+    theta = np.arccos(np.clip(lode, -1, 1)) / 3.0
+    dev = eps_d * np.array([np.cos(theta), np.cos(theta - 2 * np.pi / 3), 0.0])
+    dev[2] = -dev[0] - dev[1]
+    out = np.zeros(2 * ndim)
+    out[:3] = dev + eps_v / 3.0
+    return out
+
+
+def invariants(sig):
+    m = sig[:3].sum() / 3.0
+    s = sig.copy()
+    s[:3] -= m
+    return m, np.sqrt(1.5 * np.dot(s, s))
+
+
+def new_state(ndim):
+    return np.zeros(2 * ndim), np.array([Z_INI, 0.0]), np.ones(1, np.uint8)
+
+
+def update_to_yield_surface(ndim, lode):
+    """von_mises.rs:288-313: elastic step from zero stress exactly onto the yield surface."""
+    kk, gg = bulk_shear(YOUNG, POISSON)
+    sig, ivs, el = new_state(ndim)
+    deps_v = 1.0 / kk  # d(sigma_m) = 1
+    deps_d = Z_INI / (3 * gg)  # d(sigma_d) = z_ini: exactly onto the yield surface
+    assert oracle.model_update_stress(1, params(), ndim, sig, ivs, el, octahedral(deps_v, deps_d, lode, ndim)) == 0
+    return sig, ivs, el
+
+
+@pytest.mark.parametrize("ndim", [2, 3])
+@pytest.mark.parametrize("lode", [-1.0, 0.0, 1.0])
+def test_update_stress_works_elastic(ndim, lode):
+    sig, ivs, el = update_to_yield_surface(ndim, lode)
+    m, d = invariants(sig)
+    assert abs(m - 1.0) <= 1e-14
+    assert abs(d - Z_INI) <= 1e-14
+    assert el[0] == 1
+    assert list(ivs) == [Z_INI, 0.0]
+
+
+@pytest.mark.parametrize("ndim", [2, 3])
+def test_update_stress_works_elastoplastic(ndim):
+    deps_v, deps_d = 0.001, 0.005
+    sig, ivs, el = update_to_yield_surface(ndim, 1.0)
+    m1, d1 = invariants(sig)
+    deps = octahedral(deps_v, deps_d, 1.0, ndim)
+    assert oracle.model_update_stress(1, params(), ndim, sig, ivs, el, deps) == 0
+    m2, d2 = invariants(sig)
+    kk, gg = bulk_shear(YOUNG, POISSON)
+    assert abs(m2 - (m1 + kk * deps_v)) <= 1e-15
+    assert abs(d2 - (d1 + 3 * gg * HH * deps_d / (3 * gg + HH))) <= 1e-14
+    assert el[0] == 0
+    assert abs(ivs[0] - (d1 + 3 * gg * HH * deps_d / (3 * gg + HH))) <= 1e-14
+    assert ivs[1] > 0
+
+
+def test_stiffness_works_elastoplastic_2d():
+    """von_mises.rs:418-480 (SPO D_ep values, Mandel shear x2)."""
+    sig, ivs, el = new_state(2)
+    E, nu, z = YOUNG, POISSON, Z_INI
+    dy = z * (1 - nu * nu) / (E * np.sqrt(1 - nu + nu * nu))
+    eps_x, eps_y = dy * nu / (1 - nu), -dy
+    deps = np.array([0.9999 * eps_x, 0.9999 * eps_y, 0.0, 0.0])
+    assert oracle.model_update_stress(1, params(), 2, sig, ivs, el, deps) == 0
+    dd = oracle.model_stiffness(1, params(), 2, sig, ivs, el[0])
+    mp = [0, 1, 3]
+    spo = np.array([[1800.0, 600.0, 0.0], [600.0, 1800.0, 0.0], [0.0, 0.0, 600.0]])
+    for i in range(3):
+        for j in range(3):
+            m = 2.0 if (i == 2 and j == 2) else 1.0
+            assert abs(dd[mp[i], mp[j]] - m * spo[i, j]) <= 1e-16
+    assert el[0] == 1 and list(ivs) == [z, 0.0]
+    deps = np.array([(2 - 0.9999) * eps_x, (2 - 0.9999) * eps_y, 0.0, 0.0])
+    assert oracle.model_update_stress(1, params(), 2, sig, ivs, el, deps) == 0
+    dd = oracle.model_stiffness(1, params(), 2, sig, ivs, el[0])
+    spo = np.array([[1.389940828402367e03, 9.248520710059172e02, -2.081794007857600e-15],
+                    [9.248520710059172e02, 1.262130177514793e03, 2.914511611000640e-15],
+                    [-2.081794007857600e-15, 2.914511611000640e-15, 3.923076923076923e02]])
+    for i in range(3):
+        for j in range(3):
+            m = 2.0 if (i == 2 and j == 2) else 1.0
+            assert abs(dd[mp[i], mp[j]] - m * spo[i, j]) <= 1e-12
+    assert el[0] == 0
+    assert ivs[0] == invariants(sig)[1]
+    assert abs(ivs[1] - 3.461538461538463e-03) <= 1e-15
+
+
+@pytest.mark.parametrize("ndim", [2, 3])
+def test_elastic_in_elastoplastic(ndim):
+    """VonMises inside the yield surface equals LinearElastic (tests/test_elastic_in_elastoplastic.rs)."""
+    rng = np.random.default_rng(7)
+    kk, gg = bulk_shear(YOUNG, POISSON)
+    for _ in range(50):
+        deps = rng.normal(0, 0.1 * Z_INI / (2 * gg), 2 * ndim)
+        a, ia, ea = new_state(ndim)
+        b, ib, eb = new_state(ndim)
+        assert oracle.model_update_stress(1, params(), ndim, a, ia, ea, deps) == 0
+        assert oracle.model_update_stress(0, params(), ndim, b, ib, eb, deps) == 0
+        assert ea[0] == 1
+        np.testing.assert_allclose(a, b, rtol=0, atol=1e-15)
+
+
+@pytest.mark.parametrize("name", list(problems.SPO_PROBLEMS))
+def test_oracle_vs_spo_golden(name):
+    pb = problems.SPO_PROBLEMS[name]()
+    m = pb["mesh"]
+    el = oracle.OracleElements(m, oracle.MODEL_VON_MISES, oracle.Params(*pb["params"]), ngauss=pb["ngauss"],
+                               sym_tol=pb["sym_tol"])
+    solver = OracleSolver(el, m.ndof, pb["essential"], lagrange_mult_method=True, n_max_iterations=20,
+                          t_fin=float(pb["nsteps"]))
+    worst = [0.0, 0.0]
+
+    def cb(step, t, u, el):
+        du, ds = problems.compare_step(pb["golden"], step, u, el.sig, pb["ngauss"])
+        worst[0] = max(worst[0], du)
+        worst[1] = max(worst[1], ds)
+
+    assert solver.solve(cb) == pb["nsteps"]
+    assert worst[0] <= pb["tol_u"], worst
+    assert worst[1] <= pb["tol_s"], worst
+
+
+def test_oracle_smith_5d11_linear_elastic():
+    pb = problems.smith_5d11()
+    m = pb["mesh"]
+    el = oracle.OracleElements(m, oracle.MODEL_LINEAR_ELASTIC, oracle.Params(*pb["params"]))
+    out = {}
+    solver = OracleSolver(el, m.ndof, pb["essential"], lagrange_mult_method=True, t_fin=1.0)
+    solver.solve(lambda step, t, u, el: out.setdefault("u", u))
+    np.testing.assert_allclose(out["u"], pb["golden"]["uu_correct"], rtol=0, atol=1e-13)
+
+
+@pytest.mark.parametrize("fixture", ["artificial_2d_qua8.npz", "artificial_2d_tri3.npz",
+                                     "artificial_3d_hex8.npz"])
+def test_oracle_vs_pmsim_artificial_states(fixture):
+    """pmsim's own FemState files: uniform stretch/shear fields, linear elastic E=1500, nu=0.25."""
+    g = problems.load(fixture)
+    m = Mesh(g["coords"].shape[1], g["coords"], g["cells"], kind_from_name(str(g["kind"])))
+    for k in range(3):
+        el = oracle.OracleElements(m, oracle.MODEL_LINEAR_ELASTIC, oracle.Params(1500.0, 0.25))
+        assert el.ngauss == g["stress"].shape[2]
+        el.initialize()
+        el.update_secondary_values(np.asarray(g["u"][k]))
+        np.testing.assert_allclose(el.sig.reshape(g["stress"][k].shape), g["stress"][k], rtol=0, atol=1e-13)
+
+
+def test_oracle_fd_jacobian():
+    """Analytic K equals a central finite difference of f_int (src/fem/elements.rs:352-386), von Mises."""
+    from pmsim_b200.mesh import structured_2d, QUA8
+    m = structured_2d(QUA8, 1, 1, 1.0, 1.0)
+    X = m.coords[m.cells[0]]
+    prm = oracle.Params(YOUNG, POISSON, HH, Z_INI)
+    rng = np.random.default_rng(3)
+    du = rng.normal(0, 2e-3, 16)
+    ng = 9
+
+    l2g = (2 * m.cells[0][:, None] + np.arange(2)[None, :]).ravel()
+
+    def fint(du):
+        el = oracle.OracleElements(m, 1, prm, ngauss=ng)
+        el.initialize()
+        dug = np.zeros(m.ndof)
+        dug[l2g] = du  # element-local -> global equation numbers
+        el.update_secondary_values(dug)
+        return oracle.elem_f_int(m.kind, ng, X, el.sig), el
+
+    f0, el = fint(du)
+    assert el.elastic.min() == 0  # some IPs plastic
+    K = oracle.elem_jacobian(m.kind, ng, X, 1, prm, el.sig, el.ivs, el.elastic)
+    h = 1e-7
+    Kfd = np.zeros_like(K)
+    for j in range(16):
+        e = np.zeros(16)
+        e[j] = h
+        Kfd[:, j] = (fint(du + e)[0] - fint(du - e)[0]) / (2 * h)
+    assert np.max(np.abs(K - Kfd)) / np.max(np.abs(K)) < 1e-6
