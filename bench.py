@@ -1,0 +1,401 @@
+"""Benchmark of the pmsim solid hot path on B200.
+
+Default workload (one GPU): the single large 3D problem -- a 64x64x32 block of Hex20 cells with
+27 Gauss points (131,072 cells, 3,538,944 IPs, 1,647,555 DOF, CSR nnz 279,514,377), von Mises
+E=2e5, nu=0.3, z0=250, H=1e3.  One step = one Newton iteration of the element hot path:
+stress update (radial return) at every IP from the step-start state, F_int = sum B^T sigma,
+consistent tangent K = sum B^T D_ep B, deterministic gather of K into CSR and of F_int into R.
+The displacement increment is a seeded synthetic footing indentation of the block's top
+(mid-load), so that plastic and elastic IPs mix.  Metric: IP stress-update+tangent per second.
+
+Also measured in the same run: the stand-alone von Mises batch kernel on 16,777,216 IPs
+(``k1_microbench``), the FP64 FMA peak of the GPU (``fp64_peak``), and the CPU restatement of
+the reference (oracle port, all host cores) on a bounded sample (``cpu_baseline``).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference] [--small]
+Multi-GPU (torchrun): every rank processes its own block (weak scaling, no data-path
+collective); the time is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+E, NU, Z0, HH = 2e5, 0.3, 250.0, 1e3
+PEAKS_FALLBACK = {"hbm_gbs": 6650.0}
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--small", action="store_true", help="16x16x8 Hex20 block (profiling captures)")
+    ap.add_argument("--no-k1", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--cpu-cells", type=int, default=0)
+    return ap.parse_args()
+
+
+def workload_dims(small):
+    return (16, 16, 8) if small else (64, 64, 32)
+
+
+def make_problem(small):
+    from pmsim_b200 import mesh as M
+    nx, ny, nz = workload_dims(small)
+    m = M.structured_3d(M.HEX20, nx, ny, nz, float(nx), float(ny), float(nz))
+    return m
+
+
+def synthetic_ddu(m, small, seed=20241203):
+    """Seeded mid-load increment of the footing indentation: the central quarter of the top face is
+    pushed down (prescribed uz), decaying with depth and across the footing edge, plus noise."""
+    nx, ny, nz = workload_dims(small)
+    x, y, z = m.coords[:, 0], m.coords[:, 1], m.coords[:, 2]
+    cx, cy = nx / 2.0, ny / 2.0
+    hx, hy = nx / 4.0, ny / 4.0
+    # smooth plateau under the footing: 1 inside |x-cx|<=hx, |y-cy|<=hy, tanh decay outside
+    fx = 0.5 * (np.tanh((hx - np.abs(x - cx)) / 2.0) + 1.0)
+    fy = 0.5 * (np.tanh((hy - np.abs(y - cy)) / 2.0) + 1.0)
+    depth = np.exp(-(nz - z) / (0.5 * nz))
+    delta = 0.005 * nz * 0.35  # 35% of the total indentation (0.5% of the height)
+    u = np.zeros_like(m.coords)
+    u[:, 2] = -delta * fx * fy * depth
+    u[:, 0] = 0.15 * delta * (x - cx) / nx * fy * depth
+    u[:, 1] = 0.15 * delta * (y - cy) / ny * fx * depth
+    rng = np.random.default_rng(seed)
+    u += rng.normal(0.0, 2e-4, size=u.shape)
+    return u.reshape(-1).copy()
+
+
+def flops_per_ip_hex20():
+    """Algorithmic FP64 FLOPs of the fused element kernel per Hex20 IP (FMA = 2).
+    J (20 nodes x 9 FMA) + J^-T dN (20 x 9) + strain (20 x 9) + B^T sigma (20 x 9) +
+    h = S g (20 x 9) + three scaled copies (20 x 9 MUL, counted 1) + 210 node pairs x 33 FMA."""
+    fma = 20 * 9 * 5 + 210 * 33
+    mul = 20 * 9
+    return 2 * fma + mul
+
+
+def algorithmic_bytes_step(m, ng, nnz):
+    """Bytes a fused implementation must move per Newton iteration: coordinates, connectivity,
+    dU (read once), IP state read (sigma, z: 56 B) and written (sigma, z, lambda: 64 B + flag),
+    R (8 ndof) and the CSR values written once (8 nnz)."""
+    nip = m.ncell * ng
+    return (m.npoint * 24 + m.ncell * m.nnode * 4 + m.ndof * 8 + nip * 56 + nip * 65 + m.ndof * 8 + nnz * 8)
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    def __init__(self, index):
+        self.f = tempfile.NamedTemporaryFile(prefix="clk", suffix=".csv", delete=False)
+        self.p = None
+        try:
+            self.p = subprocess.Popen(
+                ["nvidia-smi", "-i", str(index),
+                 "--query-gpu=clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+                 "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
+                 "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return None
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except Exception:
+            self.p.kill()
+        self.f.close()
+        rows = []
+        for line in open(self.f.name):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) >= 8:
+                rows.append(parts)
+        os.unlink(self.f.name)
+        if not rows:
+            return None
+        sm = [float(r[0]) for r in rows if r[0].replace(".", "").isdigit()]
+        mx = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if "Active" in r[4 + k] and "Not" not in r[4 + k]})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return d, "measured"
+    return PEAKS_FALLBACK, "fallback"
+
+
+def fp64_peak(torch, L, stream):
+    out = torch.empty(148 * 8 * 256, dtype=torch.float64, device="cuda")
+    iters = 20000
+    for _ in range(2):
+        L.pms_probe_fp64_fma(1000, 148 * 8, out.data_ptr(), stream.cuda_stream)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    L.pms_probe_fp64_fma(iters, 148 * 8, out.data_ptr(), stream.cuda_stream)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    flops = 148 * 8 * 256 * 8 * iters * 2
+    return flops / (ms * 1e-3) / 1e12
+
+
+def run_k1(torch, stream, steps, warmup):
+    """Stand-alone von Mises batch on 16,777,216 IPs (3D, SoA), sigma0 = 0, z0 = 250,
+    deps ~ N(0, (1.5 z0/(2G))^2), H ~ U[0, 2e3]; K1 reads 112 B and writes 233 B per IP."""
+    from pmsim_b200.material import VonMisesBatch
+    n = 16_777_216
+    gg = E / (2 * (1 + NU))
+    g = torch.Generator(device="cuda").manual_seed(1234)
+    deps = torch.randn((6, n), generator=g, device="cuda", dtype=torch.float64) * (1.5 * Z0 / (2 * gg))
+    hh = torch.rand(n, generator=g, device="cuda", dtype=torch.float64) * 2e3
+    sig = torch.zeros((6, n), device="cuda", dtype=torch.float64)
+    z = torch.full((n,), Z0, device="cuda", dtype=torch.float64)
+    lam = torch.zeros(n, device="cuda", dtype=torch.float64)
+    el = torch.zeros(n, device="cuda", dtype=torch.uint8)
+    dd = torch.empty((21, n), device="cuda", dtype=torch.float64)
+    vm = VonMisesBatch(E, NU, 0.0, Z0, ndim=3)
+    times = []
+    with torch.cuda.stream(stream):
+        for i in range(warmup + steps):
+            sig.zero_()
+            z.fill_(Z0)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            vm.update_and_stiffness(sig, z, lam, el, deps, hh=hh, dd=dd, stream=stream)
+            e1.record(stream)
+            if i >= warmup:
+                times.append((e0, e1))
+    torch.cuda.synchronize()
+    ms = statistics.mean(a.elapsed_time(b) for a, b in times)
+    yielded = float(1.0 - el.double().mean().item())
+    bytes_ip = 112 + 233
+    return {"ips": n, "ms": ms, "ip_per_s": n / (ms * 1e-3), "gbs": n * bytes_ip / (ms * 1e-3) / 1e9,
+            "bytes_per_ip": bytes_ip, "yield_fraction": yielded}
+
+
+def cpu_sample(m, ddu, ncell_sample, nthreads):
+    """The oracle (C++ restatement of pmsim's element/material path, structured like the reference:
+    per-cell dense B^T D B, COO triplets with duplicates, sort/sum to CSR) on the first
+    ncell_sample cells.  Returns seconds for update + F_int + K(COO) + CSR and the IP count."""
+    import oracle
+    from pmsim_b200 import mesh as M
+    sub = M.Mesh(3, m.coords, m.cells[:ncell_sample], m.kind)
+    el = oracle.OracleElements(sub, oracle.MODEL_VON_MISES, oracle.Params(E, NU, HH, Z0), sym_tol=-1.0,
+                               nthreads=nthreads)
+    el.initialize()
+    t0 = time.perf_counter()
+    el.update_secondary_values(ddu)
+    el.assemble_f_int()
+    rows, cols, vals = el.assemble_kk_coo()
+    oracle.coo_to_csr(m.ndof, rows, cols, vals)
+    dt = time.perf_counter() - t0
+    return dt, ncell_sample * el.ngauss
+
+
+def reference_arm(args, rank):
+    """--impl reference: the reference's CPU path (oracle port; the Rust reference cannot be built
+    here) on the host cores, same metric and workload, each step a bounded sample."""
+    if rank != 0:
+        return
+    import oracle
+    m = make_problem(args.small)
+    ddu = synthetic_ddu(m, args.small)
+    nthreads = oracle.lib().orc_max_threads()
+    ncs = args.cpu_cells or (512 if args.small else 4096)
+    cpu_sample(m, ddu, min(ncs, 256), nthreads)  # warm-up (page-in, thread pool)
+    tot, ips = 0.0, 0
+    for _ in range(args.steps):
+        dt, n = cpu_sample(m, ddu, ncs, nthreads)
+        tot += dt
+        ips += n
+    value = ips / tot
+    nx, ny, nz = workload_dims(args.small)
+    line = {
+        "impl": "reference", "metric": "IP stress-update+tangent/s FP64", "value": value, "unit": "IP/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"hex20 {nx}x{ny}x{nz} block, 27 IP, von Mises (one Newton iteration)",
+                   "parallelism": "host threads"},
+        "cpu_baseline": {"value": value, "unit": "IP/s", "cores": nthreads, "kind": "port",
+                         "sample": f"first {ncs} cells ({ncs * 27} IPs) per step: update + F_int + K COO + CSR"},
+        "e2e": {"value": value, "unit": "IP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        reference_arm(args, rank)
+        return
+    import torch
+    import torch.distributed as dist
+    if world > 1:
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    from pmsim_b200 import _lib
+    from pmsim_b200.elements import Elements, Material
+    L = _lib.load()
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.Stream(device=dev)
+
+    m = make_problem(args.small)
+    ddu_h = synthetic_ddu(m, args.small, seed=20241203 + rank)
+    el = Elements(m, Material.von_mises(E, NU, HH, Z0))
+    el.set_stream(stream)
+    ng, nnz, ndof = el.ngauss, el.nnz, el.ndof
+    d_ddu = torch.tensor(ddu_h, device=dev)
+    d_ff = torch.empty(ndof, device=dev, dtype=torch.float64)
+    d_csr = torch.empty(nnz, device=dev, dtype=torch.float64)
+    el.initialize_internal_values()
+    el.backup_secondary_values()
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    # warm-up
+    for _ in range(args.warmup):
+        el.update_and_assemble(d_ddu, d_ff, d_csr)
+    el.sync()
+    torch.cuda.synchronize(dev)
+    sig, ivs, elastic = el.get_state()
+    plastic = float(1.0 - elastic.mean())
+
+    # timed region: device-resident inputs (every buffer is far larger than the 126 MB L2)
+    L.pms_elements_set_timing(el.h, 1)
+    L.pms_elements_kernel_times(el.h, None, None)
+    clocks = Clocks(local)
+    launches0 = el.launch_count()
+    barrier()
+    torch.cuda.synchronize(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        el.update_and_assemble(d_ddu, d_ff, d_csr)
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    barrier()
+    clk = clocks.stop()
+    launches = el.launch_count() - launches0
+    ms = e0.elapsed_time(e1) / args.steps
+    kt = np.zeros(3)
+    kc = np.zeros(3, np.int64)
+    L.pms_elements_kernel_times(el.h, _lib.ptr(kt), _lib.ptr(kc))
+    L.pms_elements_set_timing(el.h, 0)
+    el.sync()
+    ms_max = ms
+    if world > 1:
+        t = torch.tensor([ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_max = float(t.item())
+    nip = m.ncell * ng
+    value = world * nip / (ms_max * 1e-3)
+
+    # e2e through the C ABI with host buffers (pinned): dU in, R and CSR values out, every step
+    e2e = None
+    if not args.no_e2e:
+        h_ddu = torch.tensor(ddu_h).pin_memory().numpy()
+        h_ff = torch.empty(ndof, dtype=torch.float64).pin_memory().numpy()
+        h_csr = torch.empty(nnz, dtype=torch.float64).pin_memory().numpy()
+        el.update_and_assemble(h_ddu, h_ff, h_csr)
+        barrier()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            el.update_and_assemble(h_ddu, h_ff, h_csr)
+        t_e2e = (time.perf_counter() - t0) / args.steps
+        if world > 1:
+            t = torch.tensor([t_e2e], device=dev, dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            t_e2e = float(t.item())
+        e2e = {"value": world * nip / t_e2e, "unit": "IP/s", "h2d_bytes_per_step": ndof * 8,
+               "d2h_bytes_per_step": (ndof + nnz) * 8, "ms_per_step": t_e2e * 1e3}
+        del h_csr
+
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+
+    peaks, peaks_kind = measured_peaks()
+    fp64 = fp64_peak(torch, L, stream)
+    k1 = None
+    if not args.no_k1 and not args.small:
+        del d_csr
+        torch.cuda.empty_cache()
+        k1 = run_k1(torch, stream, max(3, args.steps), args.warmup)
+        k1["roofline"] = {"bound": "hbm", "achieved": k1["gbs"], "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                          "frac": k1["gbs"] / peaks["hbm_gbs"], "peak_source": peaks_kind}
+
+    ms_elem = kt[0] / max(kc[0], 1)
+    fl_ip = flops_per_ip_hex20()
+    achieved_tf = nip * fl_ip / (ms_elem * 1e-3) / 1e12
+    alg_bytes = algorithmic_bytes_step(m, ng, nnz)
+    step_gbs = alg_bytes / (ms * 1e-3) / 1e9
+    cpu = None
+    if not args.no_cpu:
+        import oracle
+        nthreads = oracle.lib().orc_max_threads()
+        ncs = args.cpu_cells or (512 if args.small else 4096)
+        cpu_sample(m, ddu_h, 256, nthreads)
+        dt, n = cpu_sample(m, ddu_h, ncs, nthreads)
+        dt1, n1 = cpu_sample(m, ddu_h, max(ncs // 8, 64), 1)
+        cpu = {"value": n / dt, "unit": "IP/s", "cores": nthreads, "kind": "port",
+               "sample": f"first {ncs} cells ({n} IPs): update + F_int + K COO + CSR sum, all threads",
+               "single_thread_ip_per_s": n1 / dt1}
+    nx, ny, nz = workload_dims(args.small)
+    line = {
+        "metric": "IP stress-update+tangent/s FP64",
+        "value": value, "unit": "IP/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms_max, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"hex20 {nx}x{ny}x{nz} block, 27 IP, von Mises E=2e5 nu=0.3 z0=250 H=1e3: "
+                               f"one fused Newton iteration (update + F_int + K + CSR)",
+                   "ncell": m.ncell, "nip": nip, "ndof": ndof, "nnz": nnz,
+                   "plastic_fraction": plastic, "l2": "inputs larger than L2 (no flush)",
+                   "parallelism": f"replica per GPU x{world}"},
+        "roofline": {"bound": "fp64", "achieved": achieved_tf, "peak": fp64, "unit": "TFLOP/s",
+                     "frac": achieved_tf / fp64, "traffic": None,
+                     "kernel": "element_kernel<3,20> (fused update + B^T sigma + B^T D B)",
+                     "flop_per_ip": fl_ip, "peak_source": "FP64 FMA probe measured in this run"},
+        "roofline_hbm": {"bound": "hbm", "achieved": step_gbs, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                         "frac": step_gbs / peaks["hbm_gbs"], "algorithmic_bytes_per_step": alg_bytes,
+                         "peak_source": peaks_kind},
+        "kernels_ms_per_step": {"element": ms_elem, "f_gather": kt[1] / max(kc[1], 1),
+                                "kk_gather": kt[2] / max(kc[2], 1)},
+        "gpu_launches": int(launches),
+        "e2e": e2e, "cpu_baseline": cpu, "k1_microbench": k1, "fp64_peak_tflops": fp64, "clocks": clk,
+    }
+    print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

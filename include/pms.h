@@ -1,0 +1,191 @@
+/* pms.h -- C ABI of libpms_b200.so, the B200 (sm_100a) implementation of pmsim's implicit
+ * solid hot path: von Mises radial return + consistent tangent at every integration point
+ * (IP), per-element residual B^T.sigma and tangent B^T.D.B, and a deterministic scatter of
+ * the element blocks into a global CSR matrix.  All arithmetic is FP64.
+ *
+ * Each entry point replaces one call of the reference (pmsim 0.3.0, paths inside that project):
+ *   ElementTrait           src/fem/element_trait.rs:6-38     -> pms_elements_* (batched over cells)
+ *   Elements loops         src/fem/elements.rs:132-205       -> pms_elements_* (one launch per call)
+ *   StressStrainTrait      src/material/model_stress_strain.rs:8-43 -> pms_vm_*_batch
+ *   assemble_vector/matrix src/base/assembly.rs:38-139       -> CSR/R gathers inside pms_elements_assemble_*
+ * Errors: the reference returns Result<_, &'static str>; here every call returns an int status
+ * (PMS_OK = 0) and pms_elements_last_error() returns the reference's message text.
+ * No torch or CUDA types cross this boundary: pointers are plain, streams are void*.
+ */
+#ifndef PMS_B200_H
+#define PMS_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---------------------------------------------------------------------- */
+enum pms_status_code {
+    PMS_OK = 0,
+    PMS_ERR_INVALID = 1,      /* invalid argument (message in pms_elements_last_error) */
+    PMS_ERR_CUDA = 2,         /* CUDA runtime error */
+    PMS_ERR_ZERO_SIGMA_D = 3, /* "von Mises plastic update must not lead to zero sigma_d (sigma_d < 1e-10)"
+                                 src/material/von_mises.rs:212-216 */
+    PMS_ERR_ZERO_NORM_S = 4,  /* "von Mises stiffness cannot be computed with zero deviatoric norm
+                                 (norm_s < 1e-10)"  src/material/von_mises.rs:147-150 */
+    PMS_ERR_JACOBIAN = 5,     /* non-positive Jacobian determinant at an IP (gemlab calc_gradient) */
+    PMS_ERR_NOMEM = 6,        /* device allocation failed */
+    PMS_ERR_UNSUPPORTED = 7   /* idealization/kind not implemented (plane stress, axisymmetric) */
+};
+
+/* ---- element kinds (gemlab GeoKind subset used by solids) ---------------------------------- */
+enum pms_kind {
+    PMS_TRI3 = 0, PMS_TRI6 = 1, PMS_QUA4 = 2, PMS_QUA8 = 3, PMS_QUA9 = 4,
+    PMS_TET4 = 5, PMS_TET10 = 6, PMS_HEX8 = 7, PMS_HEX20 = 8
+};
+
+/* ---- stress-strain models (src/base/parameters.rs:17-35) ---------------------------------- */
+enum pms_model { PMS_LINEAR_ELASTIC = 0, PMS_VON_MISES = 1 };
+
+/* where a caller's buffer lives */
+enum pms_mem { PMS_MEM_HOST = 0, PMS_MEM_DEVICE = 1 };
+
+/* StressStrain::VonMises { young, poisson, hh, z_ini } / LinearElastic { young, poisson } */
+typedef struct pms_material {
+    int32_t model;  /* enum pms_model */
+    double young;
+    double poisson;
+    double hh;      /* hardening H (von Mises) */
+    double z_ini;   /* initial yield-surface size (von Mises); must be > 1e-6 */
+} pms_material;
+
+/* Homogeneous mesh: ncell cells of one kind; coords[npoint*ndim]; cells[ncell*nnode] (point ids).
+ * Global DOF numbering: eq = ndim*point + d (src/base/all_dofs.rs:87-116).
+ * cell_material (nullable) selects materials[cell_material[c]] per cell (cell attribute). */
+typedef struct pms_mesh {
+    int32_t ndim;
+    int32_t kind;          /* enum pms_kind */
+    int64_t npoint;
+    int64_t ncell;
+    const double* coords;  /* host */
+    const int64_t* cells;  /* host */
+    const int32_t* cell_material; /* host, nullable */
+} pms_mesh;
+
+/* The Config fields the hot path reads (src/base/config.rs:19-229). */
+typedef struct pms_config {
+    int32_t ngauss;        /* 0 = default rule of the kind (ParamSolid::ngauss = None) */
+    int32_t plane_stress;  /* must be 0: von Mises rejects plane stress (von_mises.rs:60-62) */
+    int32_t axisymmetric;  /* must be 0 (not implemented) */
+    double thickness;      /* Idealization::thickness, default 1.0 */
+} pms_config;
+
+typedef struct pms_elements_info {
+    int32_t ndim, kind, nnode, ngauss, ncomp;  /* ncomp = Mandel components (4 in 2D, 6 in 3D) */
+    int64_t npoint, ncell, ndof, nip;          /* nip = ncell*ngauss */
+    int64_t nnz;                               /* CSR nonzeros of K (full, both triangles) */
+    int64_t nblock_upper;                      /* node-pair blocks with A <= B */
+    int64_t ncontrib;                          /* element blocks summed into them */
+    int64_t device_bytes;                      /* device memory held by the handle */
+} pms_elements_info;
+
+typedef struct pms_elements pms_elements; /* opaque; not thread-safe; one CUDA stream per handle */
+
+/* Elements::new + ElementSolid::new for all cells (src/fem/elements.rs:45-70,
+ * src/fem/element_solid.rs:47-92): uploads the mesh, builds the CSR pattern of K and the
+ * deterministic gather maps, allocates the device-resident IP state (SoA). */
+int pms_elements_create(const pms_mesh* mesh, const pms_material* materials, int32_t nmaterial,
+                        const pms_config* config, pms_elements** out);
+void pms_elements_destroy(pms_elements* h);
+int pms_elements_get_info(const pms_elements* h, pms_elements_info* out);
+/* stream: a cudaStream_t (or NULL for the handle's own stream) */
+int pms_elements_set_stream(pms_elements* h, void* stream);
+/* CSR pattern of K (sorted columns): indptr[ndof+1], indices[nnz] (host or device) */
+int pms_elements_csr_pattern(pms_elements* h, int64_t* indptr, int32_t* indices, int32_t mem);
+
+/* ElementTrait::initialize_internal_values (von_mises.rs:107-116): sigma = 0, z = z_ini,
+ * lambda = 0, elastic = true at every IP */
+int pms_elements_initialize(pms_elements* h);
+/* ElementTrait::reset_algorithmic_variables (von_mises.rs:119-121): lambda = 0 */
+int pms_elements_reset_algorithmic(pms_elements* h);
+/* ElementTrait::backup_secondary_values / restore_secondary_values
+ * (element_solid.rs:227-238; LocalState::mirror, local_state.rs:40-44) */
+int pms_elements_backup(pms_elements* h);
+int pms_elements_restore(pms_elements* h);
+
+/* ElementTrait::update_secondary_values (element_solid.rs:190-224): per IP,
+ * delta_eps = B.ddu, then update_stress in place on the current state (the Newton loop has
+ * just backed it up or restored it).  ddu[ndof] is the cumulative step increment. */
+int pms_elements_update_secondary(pms_elements* h, const double* ddu, int32_t mem);
+/* Elements::assemble_f_int (elements.rs:132-138; element_solid.rs:124-138; assembly.rs:38-46):
+ * ff_int[ndof] = sum_e sum_p B^T sigma |J| w t  (overwritten, not accumulated) */
+int pms_elements_assemble_f_int(pms_elements* h, double* ff_int, int32_t mem);
+/* Elements::assemble_kke (elements.rs:156-163; element_solid.rs:168-185; assembly.rs:70-139):
+ * csr_values[nnz] = sum_e sum_p B^T D_ep B |J| w t in the pattern of pms_elements_csr_pattern.
+ * Bit-reproducible: every entry sums its element contributions in ascending cell order. */
+int pms_elements_assemble_kk(pms_elements* h, double* csr_values, int32_t mem);
+/* Fused Newton-iteration call = restore + update_secondary(ddu) + assemble_f_int + assemble_kk
+ * on the updated state, in one pass over the cells (ff_int/csr_values nullable).  Every IP starts
+ * from the backed-up state (pms_elements_backup at iteration 0), as SolverImplicit::iterate does
+ * (src/fem/solver_implicit.rs:254-263); the backup itself is not modified. */
+int pms_elements_update_and_assemble(pms_elements* h, const double* ddu, double* ff_int, double* csr_values,
+                                     int32_t mem);
+/* Per-cell drop-ins for callers that loop over cells themselves (host output):
+ * ElementTrait::calc_f_int -> f[nnode*ndim]; ElementTrait::calc_jacobian -> kk[ne*ne] row-major */
+int pms_element_calc_f_int(pms_elements* h, int64_t cell, double* f);
+int pms_element_calc_jacobian(pms_elements* h, int64_t cell, double* kk);
+
+/* IP state in the reference's LocalState layout, cell-major (ip = cell*ngauss + p):
+ * sig[nip*ncomp] (Mandel), ivs[nip*2] = [z, lambda], elastic[nip]; host buffers */
+int pms_elements_get_state(pms_elements* h, double* sig, double* ivs, uint8_t* elastic);
+int pms_elements_set_state(pms_elements* h, const double* sig, const double* ivs, const uint8_t* elastic);
+
+/* Instrumentation: when on, every batched call records CUDA events around its kernels on the
+ * handle's stream; pms_elements_kernel_times waits for the stream and returns the summed device
+ * time (ms) and launch count of [0] element kernel, [1] F_int gather, [2] CSR gather since the
+ * previous query. */
+int pms_elements_set_timing(pms_elements* h, int32_t on);
+int pms_elements_kernel_times(pms_elements* h, double* ms, int64_t* counts);
+
+/* Host-only (no GPU needed): the CSR pattern pms_elements_create would build for this mesh.
+ * Call with indices = NULL to get nnz (indptr[ndof+1] may already be filled). */
+int pms_mesh_csr_pattern(const pms_mesh* mesh, int64_t* indptr, int32_t* indices, int64_t* nnz);
+
+/* Waits for the handle's stream and returns the first device-side error (PMS_OK if none). */
+int pms_elements_sync(pms_elements* h);
+const char* pms_elements_last_error(const pms_elements* h);
+/* cell and IP of the first failing integration point (-1 if none) */
+int pms_elements_error_location(const pms_elements* h, int64_t* cell, int32_t* ip);
+/* Number of kernels this handle has launched since creation (instrumentation). */
+int64_t pms_elements_launch_count(const pms_elements* h);
+
+/* ---- material batch (StressStrainTrait::update_stress + stiffness over n IPs) -------------
+ * Device buffers, structure-of-arrays with component stride n:
+ *   sig[ncomp*n] (in/out), z[n] (in/out), lambda[n] (out), elastic[n] (out), deps[ncomp*n] (in),
+ *   hh[n] (nullable: per-IP hardening, else mat->hh), dd[nd*n] (out, nullable): upper triangle of
+ *   the Mandel tangent, row-major (i <= j), nd = ncomp*(ncomp+1)/2 (21 in 3D, 10 in 2D).
+ * VonMises::update_stress (von_mises.rs:170-226) then VonMises::stiffness (von_mises.rs:124-167)
+ * on the updated state; LinearElastic (linear_elastic.rs:49-71) when mat->model == 0.
+ * status (device int[4], nullable): {code, ip_lo, ip_hi, 0} of the first failing IP. */
+int pms_vm_update_and_stiffness_batch(const pms_material* mat, int32_t ndim, int64_t n, double* sig, double* z,
+                                      double* lambda, uint8_t* elastic, const double* deps, const double* hh,
+                                      double* dd, int32_t* status, void* stream);
+/* VonMises::stiffness alone, from a given state (sig, lambda, elastic) */
+int pms_vm_stiffness_batch(const pms_material* mat, int32_t ndim, int64_t n, const double* sig,
+                           const double* lambda, const uint8_t* elastic, const double* hh, double* dd,
+                           int32_t* status, void* stream);
+/* Same as pms_vm_update_and_stiffness_batch on HOST buffers: copies in, runs, copies out
+ * (the library keeps a device staging area, grown on demand). */
+int pms_vm_update_and_stiffness_host(const pms_material* mat, int32_t ndim, int64_t n, double* sig, double* z,
+                                     double* lambda, uint8_t* elastic, const double* deps, const double* hh,
+                                     double* dd);
+
+/* Measures the FP64 FMA pipe: blocks x 256 threads, 8 independent FMA chains of `iters` each
+ * (16*iters FLOP per thread); out[blocks*256] receives the chain sums.  Used as the FP64 peak. */
+int pms_probe_fp64_fma(int64_t iters, int32_t blocks, double* out, void* stream);
+
+/* Library version string and the number of kernels launched by the material entry points. */
+const char* pms_version(void);
+int64_t pms_material_launch_count(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PMS_B200_H */

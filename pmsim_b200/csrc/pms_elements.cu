@@ -1,0 +1,1072 @@
+// pms_elements.cu -- fused per-element kernels (strain -> return map -> B^T sigma -> B^T D B)
+// and the deterministic CSR / residual gathers, behind the pms_elements_* C ABI.
+//
+// Reference calls replaced (pmsim 0.3.0):
+//   ElementSolid::update_secondary_values  src/fem/element_solid.rs:190-224 (+ calculate_strain,
+//                                          src/base/calculate_strain.rs:18-60)
+//   ElementSolid::calc_f_int               src/fem/element_solid.rs:124-138 (gemlab integ::vec_04_tb)
+//   ElementSolid::calc_jacobian            src/fem/element_solid.rs:168-185 (gemlab integ::mat_10_bdb)
+//   Elements::{assemble_f_int, assemble_kke, update_secondary_values, backup, restore, reset}
+//                                          src/fem/elements.rs:132-205
+//   assemble_vector / assemble_matrix      src/base/assembly.rs:38-139
+//
+// Work decomposition: one warp per cell.  Lane m < nnode owns node m (coordinates, dU, its
+// share of f_int); lane p < ngauss owns the state of integration point p (loaded coalesced at
+// the start, broadcast by shuffle when p is processed).  Per IP the warp reduces J and the
+// strain increment by shuffles, every lane runs the (identical) return map, and each lane
+// accumulates its share of the upper-triangular node-pair blocks of K_e in registers.
+//
+// Tangent algebra.  The von Mises / Hooke tangent is D = a Psd + b s(x)s + K I(x)I.  With the
+// node gradients g_m, h_m = S g_m (S the deviatoric stress tensor) and the Mandel B matrix,
+//   B_a^T B_b = 1/2 ((g_a.g_b) 1 + g_b (x) g_a),  B_a^T I = g_a,  B_a^T s = h_a,
+// so the 3x3 (2x2) block of node pair (a, b) is
+//   K_ab += w|J| [ a/2 (g_a.g_b) 1 + a/2 g_b(x)g_a + (K - a/3) g_a(x)g_b + b h_a(x)h_b ].
+// This is B^T D B exactly (same bilinear form), evaluated with 3 FMA per block entry instead of
+// forming D and D.B; results agree with the dense product to rounding.
+// FLOPs per IP and pair (3D): 3 (dot) + 9*3 (entries) + 3 (diagonal) = 33 FMA; per node: J^-T
+// dN (9), h = S g (9), three scaled copies (9).
+//
+// Assembly: element blocks go to a scratch buffer ke[cell][pair][nd*nd]; kk_gather_kernel owns
+// each node-pair block (A <= B) with one thread, sums its contributions in ascending cell order
+// and writes K_AB and K_BA.  No atomics: bit-identical on every run.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdint>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/pms.h"
+#include "pms_device.cuh"
+#include "pms_pattern.h"
+#include "pms_shapes.h"
+
+using namespace pms;
+
+namespace {
+
+constexpr unsigned FULL = 0xffffffffu;
+constexpr int WPB = 4;  // warps (cells) per block
+
+// Modes of the element kernel
+enum { UPD_NONE = 0, UPD_CURRENT = 1, UPD_BACKUP = 2 };
+
+struct ElemArgs {
+    int64_t ncell;     // cells in this launch
+    int64_t cell0;     // first cell of this launch
+    int64_t nip;       // total IPs of the mesh (SoA stride)
+    int ngauss;
+    double thickness;
+    const double* coords;   // npoint*nd
+    const int32_t* conn;    // ncell_total*nn
+    const int32_t* cmat;    // per-cell material (nullable)
+    const MatConst* mats;
+    const double* ddu;      // ndof
+    const double* tab;      // dN[ngauss][nn][nd], then w[ngauss]
+    // IP state, SoA with stride nip: sig[c*nip + ip]
+    const double* sig_src; const double* z_src; const double* lam_src; const uint8_t* el_src;
+    double* sig; double* z; double* lam; uint8_t* el;
+    double* fe;   // [cell][nn][nd]
+    double* ke;   // [cell][npair][nd*nd]
+    int32_t* status;  // {code, cell, ip, 0}
+};
+
+__device__ __forceinline__ void report(int32_t* status, int code, int64_t cell, int ip) {
+    if (code == OK) return;
+    if (atomicCAS(status, 0, code) == 0) {
+        status[1] = (int32_t)cell;
+        status[2] = ip;
+    }
+}
+
+// sum over the warp, result identical on every lane (tree to lane 0, then broadcast)
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(FULL, v, off);
+    return __shfl_sync(FULL, v, 0);
+}
+
+template <int ND>
+__device__ __forceinline__ double inv_jacobian(const double* J, double* Ji) {
+    if (ND == 2) {
+        double det = J[0] * J[3] - J[1] * J[2];
+        double id = 1.0 / det;
+        Ji[0] = J[3] * id;
+        Ji[1] = -J[1] * id;
+        Ji[2] = -J[2] * id;
+        Ji[3] = J[0] * id;
+        return det;
+    } else {
+        double c0 = J[4] * J[8] - J[5] * J[7];
+        double c1 = J[5] * J[6] - J[3] * J[8];
+        double c2 = J[3] * J[7] - J[4] * J[6];
+        double det = J[0] * c0 + J[1] * c1 + J[2] * c2;
+        double id = 1.0 / det;
+        Ji[0] = c0 * id;
+        Ji[1] = (J[2] * J[7] - J[1] * J[8]) * id;
+        Ji[2] = (J[1] * J[5] - J[2] * J[4]) * id;
+        Ji[3] = c1 * id;
+        Ji[4] = (J[0] * J[8] - J[2] * J[6]) * id;
+        Ji[5] = (J[2] * J[3] - J[0] * J[5]) * id;
+        Ji[6] = c2 * id;
+        Ji[7] = (J[1] * J[6] - J[0] * J[7]) * id;
+        Ji[8] = (J[0] * J[4] - J[1] * J[3]) * id;
+        return det;
+    }
+}
+
+template <int ND, int NN, int UPD, bool DOF, bool DOK>
+__global__ void __launch_bounds__(WPB * 32) element_kernel(ElemArgs A) {
+    constexpr int NC = 2 * ND;
+    constexpr int NPAIR = NN * (NN + 1) / 2;
+    constexpr int P = (NPAIR + 31) / 32;  // pair slots per lane
+    constexpr int NODE_STRIDE = 5 * ND;   // per node in smem: Ag, Cg, Hh (scaled), g, h
+    extern __shared__ double smem[];
+    const int ng = A.ngauss;
+    double* tab = smem;                                   // ng*NN*ND + ng
+    const int tab_len = ng * NN * ND + ng;
+    const int tab_pad = (tab_len + 1) & ~1;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    double* nbuf = smem + tab_pad + wid * 2 * NN * NODE_STRIDE;  // double buffer per warp
+
+    for (int i = threadIdx.x; i < tab_len; i += blockDim.x) tab[i] = A.tab[i];
+    __syncthreads();
+
+    const int64_t cl = (int64_t)blockIdx.x * WPB + wid;
+    if (cl >= A.ncell) return;  // whole warp exits together
+    const int64_t cell = A.cell0 + cl;
+    const MatConst mc = A.mats[A.cmat ? A.cmat[cell] : 0];
+
+    // node data (lane m < NN)
+    double X[ND], du[ND];
+#pragma unroll
+    for (int i = 0; i < ND; i++) { X[i] = 0.0; du[i] = 0.0; }
+    if (lane < NN) {
+        const int pt = A.conn[cell * NN + lane];
+#pragma unroll
+        for (int i = 0; i < ND; i++) {
+            X[i] = A.coords[(int64_t)pt * ND + i];
+            if (UPD != UPD_NONE) du[i] = A.ddu[(int64_t)pt * ND + i];
+        }
+    }
+    // IP state (lane p < ng)
+    const int64_t ip0 = cell * ng;
+    double st_sig[NC], st_z = 0.0, st_lam = 0.0;
+    int st_el = 1;
+#pragma unroll
+    for (int c = 0; c < NC; c++) st_sig[c] = 0.0;
+    if (lane < ng) {
+        const double* ssrc = (UPD == UPD_BACKUP) ? A.sig_src : A.sig;
+        const double* zsrc = (UPD == UPD_BACKUP) ? A.z_src : A.z;
+        const double* lsrc = (UPD == UPD_BACKUP) ? A.lam_src : A.lam;
+        const uint8_t* esrc = (UPD == UPD_BACKUP) ? A.el_src : A.el;
+#pragma unroll
+        for (int c = 0; c < NC; c++) st_sig[c] = ssrc[(int64_t)c * A.nip + ip0 + lane];
+        st_z = zsrc[ip0 + lane];
+        st_lam = lsrc[ip0 + lane];
+        st_el = esrc[ip0 + lane];
+    }
+
+    // pair slots of this lane: q = lane + 32*k
+    int pa[P], pb[P];
+#pragma unroll
+    for (int k = 0; k < P; k++) {
+        int q = lane + 32 * k;
+        int a = 0;
+        if (q < NPAIR) {
+            while (q >= (a + 1) * NN - (a + 1) * a / 2) a++;
+            pa[k] = a;
+            pb[k] = a + (q - (a * NN - a * (a - 1) / 2));
+        } else {
+            pa[k] = -1;
+            pb[k] = -1;
+        }
+    }
+    double acc[DOK ? P : 1][ND][ND];
+#pragma unroll
+    for (int k = 0; k < (DOK ? P : 1); k++)
+#pragma unroll
+        for (int i = 0; i < ND; i++)
+#pragma unroll
+            for (int j = 0; j < ND; j++) acc[k][i][j] = 0.0;
+    double f[ND];
+#pragma unroll
+    for (int i = 0; i < ND; i++) f[i] = 0.0;
+    int err = OK, err_ip = -1;
+
+    for (int p = 0; p < ng; p++) {
+        const double* dN = tab + (p * NN + (lane < NN ? lane : 0)) * ND;
+        const double wp = tab[ng * NN * ND + p];
+        // Jacobian J[i][j] = sum_m X_m[i] dN_m[j]
+        double J[ND * ND], Ji[ND * ND];
+#pragma unroll
+        for (int i = 0; i < ND; i++)
+#pragma unroll
+            for (int j = 0; j < ND; j++) J[i * ND + j] = warp_sum(lane < NN ? X[i] * dN[j] : 0.0);
+        const double det = inv_jacobian<ND>(J, Ji);
+        if (!(det > 0.0) && err == OK) { err = E_JACOBIAN; err_ip = p; }
+        // gradient g_m = J^-T dN_m
+        double g[ND];
+#pragma unroll
+        for (int i = 0; i < ND; i++) {
+            double v = 0.0;
+#pragma unroll
+            for (int j = 0; j < ND; j++) v += dN[j] * Ji[j * ND + i];
+            g[i] = (lane < NN) ? v : 0.0;
+        }
+        const double coef = det * wp * A.thickness;
+        // state of IP p
+        double sig[NC], z, lam;
+        int el;
+#pragma unroll
+        for (int c = 0; c < NC; c++) sig[c] = __shfl_sync(FULL, st_sig[c], p);
+        z = __shfl_sync(FULL, st_z, p);
+        lam = __shfl_sync(FULL, st_lam, p);
+        el = __shfl_sync(FULL, st_el, p);
+        if (UPD != UPD_NONE) {
+            // strain increment (Mandel) = sum_m sym(g_m (x) du_m)
+            double eps[NC];
+            eps[0] = warp_sum(du[0] * g[0]);
+            eps[1] = warp_sum(du[1] * g[1]);
+            if constexpr (ND == 2) {
+                eps[2] = 0.0;
+                eps[3] = warp_sum(SQRT2 * ((du[0] * g[1] + du[1] * g[0]) / 2.0));
+            } else {
+                eps[2] = warp_sum(du[ND - 1] * g[ND - 1]);
+                eps[3] = warp_sum(SQRT2 * ((du[0] * g[1] + du[1] * g[0]) / 2.0));
+                eps[4 % NC] = warp_sum(SQRT2 * ((du[1] * g[ND - 1] + du[ND - 1] * g[1]) / 2.0));
+                eps[5 % NC] = warp_sum(SQRT2 * ((du[0] * g[ND - 1] + du[ND - 1] * g[0]) / 2.0));
+            }
+            const double hh = mc.hh;
+            int st = ip_update<NC>(mc, hh, sig, z, lam, el, eps);
+            if (st != OK && err == OK) { err = st; err_ip = p; }
+            if (lane == p) {
+#pragma unroll
+                for (int c = 0; c < NC; c++) st_sig[c] = sig[c];
+                st_z = z;
+                st_lam = lam;
+                st_el = el;
+            }
+        }
+        if (DOF) {
+            // f_m[i] += coef * sum_j sigma_ij g_m[j]
+            double S[ND][ND];
+            S[0][0] = sig[0];
+            S[1][1] = sig[1];
+            S[0][1] = S[1][0] = sig[3] * INV_SQRT2;
+            if constexpr (ND == 3) {
+                S[ND - 1][ND - 1] = sig[2];
+                S[1][ND - 1] = S[ND - 1][1] = sig[4 % NC] * INV_SQRT2;
+                S[0][ND - 1] = S[ND - 1][0] = sig[5 % NC] * INV_SQRT2;
+            }
+#pragma unroll
+            for (int i = 0; i < ND; i++) {
+                double v = 0.0;
+#pragma unroll
+                for (int j = 0; j < ND; j++) v += S[i][j] * g[j];
+                f[i] += coef * v;
+            }
+        }
+        if (DOK) {
+            double a, b, s[NC];
+            int st = tangent_coefs<NC>(mc, mc.hh, sig, lam, el, a, b, s);
+            if (st != OK && err == OK) { err = st; err_ip = p; }
+            const double al = coef * 0.5 * a, ga = coef * (mc.kk - a / 3.0), be = coef * b;
+            double Sd[ND][ND];
+            Sd[0][0] = s[0];
+            Sd[1][1] = s[1];
+            Sd[0][1] = Sd[1][0] = s[3] * INV_SQRT2;
+            if constexpr (ND == 3) {
+                Sd[ND - 1][ND - 1] = s[2];
+                Sd[1][ND - 1] = Sd[ND - 1][1] = s[4 % NC] * INV_SQRT2;
+                Sd[0][ND - 1] = Sd[ND - 1][0] = s[5 % NC] * INV_SQRT2;
+            }
+            double* buf = nbuf + (p & 1) * NN * NODE_STRIDE;
+            if (lane < NN) {
+                double h[ND];
+#pragma unroll
+                for (int i = 0; i < ND; i++) {
+                    double v = 0.0;
+#pragma unroll
+                    for (int j = 0; j < ND; j++) v += Sd[i][j] * g[j];
+                    h[i] = v;
+                }
+                double* nb = buf + lane * NODE_STRIDE;
+#pragma unroll
+                for (int i = 0; i < ND; i++) {
+                    nb[i] = al * g[i];
+                    nb[ND + i] = ga * g[i];
+                    nb[2 * ND + i] = be * h[i];
+                    nb[3 * ND + i] = g[i];
+                    nb[4 * ND + i] = h[i];
+                }
+            }
+            __syncwarp();
+#pragma unroll
+            for (int k = 0; k < P; k++) {
+                if (pa[k] >= 0) {
+                    const double* ra = buf + pa[k] * NODE_STRIDE;
+                    const double* cb = buf + pb[k] * NODE_STRIDE;
+                    double Aa[ND], Ca[ND], Ha[ND], gb[ND], hb[ND];
+#pragma unroll
+                    for (int i = 0; i < ND; i++) {
+                        Aa[i] = ra[i];
+                        Ca[i] = ra[ND + i];
+                        Ha[i] = ra[2 * ND + i];
+                        gb[i] = cb[3 * ND + i];
+                        hb[i] = cb[4 * ND + i];
+                    }
+                    double dot = 0.0;
+#pragma unroll
+                    for (int i = 0; i < ND; i++) dot += Aa[i] * gb[i];
+#pragma unroll
+                    for (int i = 0; i < ND; i++)
+#pragma unroll
+                        for (int j = 0; j < ND; j++) {
+                            double v = acc[k][i][j];
+                            v = fma(Aa[j], gb[i], v);
+                            v = fma(Ca[i], gb[j], v);
+                            v = fma(Ha[i], hb[j], v);
+                            if (i == j) v += dot;
+                            acc[k][i][j] = v;
+                        }
+                }
+            }
+            // the other buffer is rewritten at p+1; p+2 reuses this one after a full pair pass,
+            // which every lane finishes before reaching the __syncwarp of p+1
+        }
+    }
+
+    if (lane == 0 && err != OK) report(A.status, err, cell, err_ip);
+    if (UPD != UPD_NONE && lane < ng) {
+#pragma unroll
+        for (int c = 0; c < NC; c++) A.sig[(int64_t)c * A.nip + ip0 + lane] = st_sig[c];
+        A.z[ip0 + lane] = st_z;
+        A.lam[ip0 + lane] = st_lam;
+        A.el[ip0 + lane] = (uint8_t)st_el;
+    }
+    if (DOF && lane < NN) {
+#pragma unroll
+        for (int i = 0; i < ND; i++) A.fe[(cell * NN + lane) * ND + i] = f[i];
+    }
+    if (DOK) {
+#pragma unroll
+        for (int k = 0; k < P; k++) {
+            if (pa[k] >= 0) {
+                const int q = lane + 32 * k;
+                double* dst = A.ke + (cell * NPAIR + q) * (ND * ND);
+#pragma unroll
+                for (int i = 0; i < ND; i++)
+#pragma unroll
+                    for (int j = 0; j < ND; j++) dst[i * ND + j] = acc[k][i][j];
+            }
+        }
+    }
+}
+
+// One thread per node-pair block (A <= B): fixed-order sum of the element blocks, written to
+// both (A, B) and (B, A) positions of the scalar CSR.
+template <int ND>
+__global__ void __launch_bounds__(256) kk_gather_kernel(int64_t nupper, const int32_t* __restrict__ u_row,
+                                                        const int32_t* __restrict__ u_col,
+                                                        const int32_t* __restrict__ u_kab,
+                                                        const int32_t* __restrict__ u_kba,
+                                                        const int64_t* __restrict__ u_cptr,
+                                                        const int32_t* __restrict__ u_contrib,
+                                                        const int64_t* __restrict__ bptr,
+                                                        const double* __restrict__ ke, double* __restrict__ csr) {
+    for (int64_t u = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; u < nupper;
+         u += (int64_t)gridDim.x * blockDim.x) {
+        double s[ND * ND];
+#pragma unroll
+        for (int i = 0; i < ND * ND; i++) s[i] = 0.0;
+        const int64_t c0 = u_cptr[u], c1 = u_cptr[u + 1];
+        for (int64_t c = c0; c < c1; c++) {
+            const uint32_t code = (uint32_t)u_contrib[c];
+            const double* blk = ke + (int64_t)(code & 0x7fffffffu) * (ND * ND);
+            if (code & 0x80000000u) {
+#pragma unroll
+                for (int i = 0; i < ND; i++)
+#pragma unroll
+                    for (int j = 0; j < ND; j++) s[i * ND + j] += blk[j * ND + i];
+            } else {
+#pragma unroll
+                for (int i = 0; i < ND * ND; i++) s[i] += blk[i];
+            }
+        }
+        const int32_t Ar = u_row[u], Bc = u_col[u];
+        const int64_t ba = bptr[Ar], nba = bptr[Ar + 1] - ba;
+        const int64_t posAB = (int64_t)ND * ND * ba + (int64_t)u_kab[u] * ND;
+#pragma unroll
+        for (int i = 0; i < ND; i++)
+#pragma unroll
+            for (int j = 0; j < ND; j++) csr[posAB + i * ND * nba + j] = s[i * ND + j];
+        if (Bc != Ar) {
+            const int64_t bb = bptr[Bc], nbb = bptr[Bc + 1] - bb;
+            const int64_t posBA = (int64_t)ND * ND * bb + (int64_t)u_kba[u] * ND;
+#pragma unroll
+            for (int i = 0; i < ND; i++)
+#pragma unroll
+                for (int j = 0; j < ND; j++) csr[posBA + j * ND * nbb + i] = s[i * ND + j];
+        }
+    }
+}
+
+// One thread per point: R[A*nd + i] = sum over its incidences (ascending cell) of f_e.
+template <int ND>
+__global__ void __launch_bounds__(256) f_gather_kernel(int64_t npoint, const int64_t* __restrict__ inc_ptr,
+                                                       const int32_t* __restrict__ inc,
+                                                       const double* __restrict__ fe, double* __restrict__ ff) {
+    for (int64_t A = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; A < npoint;
+         A += (int64_t)gridDim.x * blockDim.x) {
+        double s[ND];
+#pragma unroll
+        for (int i = 0; i < ND; i++) s[i] = 0.0;
+        for (int64_t k = inc_ptr[A]; k < inc_ptr[A + 1]; k++) {
+            const double* v = fe + (int64_t)inc[k] * ND;
+#pragma unroll
+            for (int i = 0; i < ND; i++) s[i] += v[i];
+        }
+#pragma unroll
+        for (int i = 0; i < ND; i++) ff[A * ND + i] = s[i];
+    }
+}
+
+__global__ void init_state_kernel(int64_t nip, int nc, const MatConst* mats, const int32_t* cmat, int ng,
+                                  double* sig, double* z, double* lam, uint8_t* el) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nip; i += (int64_t)gridDim.x * blockDim.x) {
+        for (int c = 0; c < nc; c++) sig[(int64_t)c * nip + i] = 0.0;
+        const MatConst m = mats[cmat ? cmat[i / ng] : 0];
+        z[i] = (m.model == 1) ? m.z_ini : 0.0;
+        lam[i] = 0.0;
+        el[i] = 1;
+    }
+}
+
+__global__ void zero_lambda_kernel(int64_t nip, double* lam) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nip; i += (int64_t)gridDim.x * blockDim.x)
+        lam[i] = 0.0;
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------------------- handle
+struct pms_elements {
+    int nd = 0, kind = 0, nn = 0, ng = 0, nc = 0, npair = 0;
+    int64_t npoint = 0, ncell = 0, ndof = 0, nip = 0, nnz = 0;
+    double thickness = 1.0;
+    std::vector<MatConst> mats;
+    Pattern pat;
+    std::vector<double> tab;  // dN table + weights
+    // device buffers
+    double* d_coords = nullptr;
+    int32_t* d_conn = nullptr;
+    int32_t* d_cmat = nullptr;
+    MatConst* d_mats = nullptr;
+    double* d_tab = nullptr;
+    double *d_sig = nullptr, *d_z = nullptr, *d_lam = nullptr;
+    uint8_t* d_el = nullptr;
+    double *d_sig_b = nullptr, *d_z_b = nullptr, *d_lam_b = nullptr;
+    uint8_t* d_el_b = nullptr;
+    double* d_fe = nullptr;
+    double* d_ke = nullptr;
+    int64_t* d_inc_ptr = nullptr;
+    int32_t* d_inc = nullptr;
+    int64_t* d_bptr = nullptr;
+    int32_t *d_urow = nullptr, *d_ucol = nullptr, *d_ukab = nullptr, *d_ukba = nullptr, *d_ucontrib = nullptr;
+    int64_t* d_ucptr = nullptr;
+    double *d_ddu = nullptr, *d_ff = nullptr, *d_csr = nullptr;  // staging for host-memory calls
+    int32_t* d_status = nullptr;
+    int64_t device_bytes = 0;
+    cudaStream_t stream = nullptr;
+    cudaStream_t own_stream = nullptr;
+    std::string last_error;
+    int64_t err_cell = -1;
+    int32_t err_ip = -1;
+    int64_t launches = 0;
+    int smem_bytes = 0;
+    std::vector<void*> allocs;
+    // optional CUDA-event timing of the three kernels of a batched call
+    bool timing = false;
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev_pool, ev_pending[3];
+
+    template <typename T>
+    bool alloc(T** p, size_t count) {
+        *p = nullptr;
+        if (count == 0) count = 1;
+        if (cudaMalloc((void**)p, count * sizeof(T)) != cudaSuccess) return false;
+        allocs.push_back((void*)*p);
+        device_bytes += (int64_t)(count * sizeof(T));
+        return true;
+    }
+    template <typename T>
+    bool upload(T** p, const T* src, size_t count) {
+        if (!alloc(p, count)) return false;
+        if (count && cudaMemcpy(*p, src, count * sizeof(T), cudaMemcpyHostToDevice) != cudaSuccess) return false;
+        return true;
+    }
+    std::pair<cudaEvent_t, cudaEvent_t> event_pair() {
+        if (!ev_pool.empty()) {
+            auto e = ev_pool.back();
+            ev_pool.pop_back();
+            return e;
+        }
+        std::pair<cudaEvent_t, cudaEvent_t> e;
+        cudaEventCreate(&e.first);
+        cudaEventCreate(&e.second);
+        return e;
+    }
+    ~pms_elements() {
+        if (own_stream) cudaStreamSynchronize(own_stream);
+        for (auto& v : ev_pending)
+            for (auto& e : v) ev_pool.push_back(e);
+        for (auto& e : ev_pool) {
+            cudaEventDestroy(e.first);
+            cudaEventDestroy(e.second);
+        }
+        for (void* p : allocs) cudaFree(p);
+        if (own_stream) cudaStreamDestroy(own_stream);
+    }
+};
+
+namespace {
+
+int fail(pms_elements* h, int code, const char* msg) {
+    if (h) h->last_error = msg;
+    return code;
+}
+
+int cuda_check(pms_elements* h) {
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return fail(h, PMS_ERR_CUDA, cudaGetErrorString(e));
+    return PMS_OK;
+}
+
+int grid_1d(int64_t n) {
+    int64_t b = (n + 255) / 256;
+    if (b > 148 * 16) b = 148 * 16;
+    return (int)std::max<int64_t>(b, 1);
+}
+
+template <int ND, int NN, int UPD, bool DOF, bool DOK>
+void launch_elem_t(pms_elements* h, const ElemArgs& a) {
+    auto kern = element_kernel<ND, NN, UPD, DOF, DOK>;
+    static thread_local bool configured = false;
+    if (!configured) {
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
+        configured = true;
+    }
+    int64_t blocks = (a.ncell + WPB - 1) / WPB;
+    kern<<<(unsigned)blocks, WPB * 32, h->smem_bytes, h->stream>>>(a);
+}
+
+template <int ND, int NN>
+void launch_elem_nn(pms_elements* h, const ElemArgs& a, int upd, bool dof, bool dok) {
+    if (upd == UPD_NONE) {
+        if (dof && dok) launch_elem_t<ND, NN, UPD_NONE, true, true>(h, a);
+        else if (dof) launch_elem_t<ND, NN, UPD_NONE, true, false>(h, a);
+        else launch_elem_t<ND, NN, UPD_NONE, false, true>(h, a);
+    } else if (upd == UPD_CURRENT) {
+        if (dof || dok) launch_elem_t<ND, NN, UPD_CURRENT, true, true>(h, a);
+        else launch_elem_t<ND, NN, UPD_CURRENT, false, false>(h, a);
+    } else {
+        if (dof || dok) launch_elem_t<ND, NN, UPD_BACKUP, true, true>(h, a);
+        else launch_elem_t<ND, NN, UPD_BACKUP, false, false>(h, a);
+    }
+}
+
+void launch_elem(pms_elements* h, const ElemArgs& a, int upd, bool dof, bool dok) {
+    switch (h->kind) {
+    case PMS_TRI3: launch_elem_nn<2, 3>(h, a, upd, dof, dok); break;
+    case PMS_TRI6: launch_elem_nn<2, 6>(h, a, upd, dof, dok); break;
+    case PMS_QUA4: launch_elem_nn<2, 4>(h, a, upd, dof, dok); break;
+    case PMS_QUA8: launch_elem_nn<2, 8>(h, a, upd, dof, dok); break;
+    case PMS_QUA9: launch_elem_nn<2, 9>(h, a, upd, dof, dok); break;
+    case PMS_TET4: launch_elem_nn<3, 4>(h, a, upd, dof, dok); break;
+    case PMS_TET10: launch_elem_nn<3, 10>(h, a, upd, dof, dok); break;
+    case PMS_HEX8: launch_elem_nn<3, 8>(h, a, upd, dof, dok); break;
+    case PMS_HEX20: launch_elem_nn<3, 20>(h, a, upd, dof, dok); break;
+    }
+    h->launches++;
+}
+
+ElemArgs make_args(pms_elements* h, const double* ddu) {
+    ElemArgs a;
+    a.ncell = h->ncell;
+    a.cell0 = 0;
+    a.nip = h->nip;
+    a.ngauss = h->ng;
+    a.thickness = h->thickness;
+    a.coords = h->d_coords;
+    a.conn = h->d_conn;
+    a.cmat = h->d_cmat;
+    a.mats = h->d_mats;
+    a.ddu = ddu;
+    a.tab = h->d_tab;
+    a.sig_src = h->d_sig_b;
+    a.z_src = h->d_z_b;
+    a.lam_src = h->d_lam_b;
+    a.el_src = h->d_el_b;
+    a.sig = h->d_sig;
+    a.z = h->d_z;
+    a.lam = h->d_lam;
+    a.el = h->d_el;
+    a.fe = h->d_fe;
+    a.ke = h->d_ke;
+    a.status = h->d_status;
+    return a;
+}
+
+void launch_kk_gather(pms_elements* h, double* csr) {
+    int64_t nu = h->pat.nupper();
+    if (h->nd == 2)
+        kk_gather_kernel<2><<<grid_1d(nu), 256, 0, h->stream>>>(nu, h->d_urow, h->d_ucol, h->d_ukab, h->d_ukba,
+                                                                 h->d_ucptr, h->d_ucontrib, h->d_bptr, h->d_ke, csr);
+    else
+        kk_gather_kernel<3><<<grid_1d(nu), 256, 0, h->stream>>>(nu, h->d_urow, h->d_ucol, h->d_ukab, h->d_ukba,
+                                                                 h->d_ucptr, h->d_ucontrib, h->d_bptr, h->d_ke, csr);
+    h->launches++;
+}
+
+void launch_f_gather(pms_elements* h, double* ff) {
+    if (h->nd == 2)
+        f_gather_kernel<2><<<grid_1d(h->npoint), 256, 0, h->stream>>>(h->npoint, h->d_inc_ptr, h->d_inc, h->d_fe, ff);
+    else
+        f_gather_kernel<3><<<grid_1d(h->npoint), 256, 0, h->stream>>>(h->npoint, h->d_inc_ptr, h->d_inc, h->d_fe, ff);
+    h->launches++;
+}
+
+}  // namespace
+
+extern "C" {
+
+int pms_elements_create(const pms_mesh* mesh, const pms_material* materials, int32_t nmaterial,
+                        const pms_config* config, pms_elements** out) {
+    if (!out) return PMS_ERR_INVALID;
+    *out = nullptr;
+    if (!mesh || !materials || nmaterial < 1 || !config || !mesh->coords || !mesh->cells) return PMS_ERR_INVALID;
+    int kind = mesh->kind;
+    if (kind < 0 || kind > 8 || kind_ndim(kind) != mesh->ndim) return PMS_ERR_INVALID;
+    if (config->plane_stress) return PMS_ERR_UNSUPPORTED;
+    if (config->axisymmetric) return PMS_ERR_UNSUPPORTED;
+    if (mesh->npoint < 1 || mesh->ncell < 1) return PMS_ERR_INVALID;
+    auto* h = new pms_elements();
+    h->kind = kind;
+    h->nd = mesh->ndim;
+    h->nc = 2 * h->nd;
+    h->nn = kind_nnode(kind);
+    h->npair = h->nn * (h->nn + 1) / 2;
+    h->npoint = mesh->npoint;
+    h->ncell = mesh->ncell;
+    h->ndof = h->npoint * h->nd;
+    h->thickness = config->thickness > 0 ? config->thickness : 1.0;
+    std::vector<double> ksi, w;
+    h->ng = integration_rule(kind, config->ngauss, ksi, w);
+    if (h->ng <= 0 || h->ng > 32) {
+        delete h;
+        return PMS_ERR_INVALID;
+    }
+    h->nip = h->ncell * h->ng;
+    for (int i = 0; i < nmaterial; i++) {
+        const pms_material& m = materials[i];
+        if (m.model != PMS_LINEAR_ELASTIC && m.model != PMS_VON_MISES) { delete h; return PMS_ERR_INVALID; }
+        if (m.model == PMS_VON_MISES && !(m.z_ini > F_TOL)) { delete h; return PMS_ERR_INVALID; }
+        h->mats.push_back(make_matconst(m.model, m.young, m.poisson, m.hh, m.z_ini));
+    }
+    if (mesh->cell_material) {
+        for (int64_t c = 0; c < h->ncell; c++)
+            if (mesh->cell_material[c] < 0 || mesh->cell_material[c] >= nmaterial) { delete h; return PMS_ERR_INVALID; }
+    }
+    // shape tables
+    h->tab.assign((size_t)h->ng * h->nn * h->nd + h->ng, 0.0);
+    {
+        double N[20], dN[60];
+        for (int p = 0; p < h->ng; p++) {
+            shape_eval(kind, &ksi[3 * p], N, dN);
+            for (int m = 0; m < h->nn; m++)
+                for (int j = 0; j < h->nd; j++) h->tab[(p * h->nn + m) * h->nd + j] = dN[m * h->nd + j];
+            h->tab[(size_t)h->ng * h->nn * h->nd + p] = w[p];
+        }
+    }
+    const char* msg = nullptr;
+    if (!build_pattern(h->nd, h->nn, h->npoint, h->ncell, mesh->cells, h->pat, &msg)) {
+        delete h;
+        return PMS_ERR_INVALID;
+    }
+    h->nnz = h->pat.nblock() * h->nd * h->nd;
+    // device uploads
+    std::vector<int32_t> conn32((size_t)h->ncell * h->nn);
+    for (size_t i = 0; i < conn32.size(); i++) conn32[i] = (int32_t)mesh->cells[i];
+    bool ok = h->upload(&h->d_coords, mesh->coords, (size_t)h->npoint * h->nd) &&
+              h->upload(&h->d_conn, conn32.data(), conn32.size()) &&
+              h->upload(&h->d_mats, h->mats.data(), h->mats.size()) &&
+              h->upload(&h->d_tab, h->tab.data(), h->tab.size());
+    if (ok && mesh->cell_material) ok = h->upload(&h->d_cmat, mesh->cell_material, (size_t)h->ncell);
+    ok = ok && h->alloc(&h->d_sig, (size_t)h->nip * h->nc) && h->alloc(&h->d_z, h->nip) &&
+         h->alloc(&h->d_lam, h->nip) && h->alloc(&h->d_el, h->nip) &&
+         h->alloc(&h->d_sig_b, (size_t)h->nip * h->nc) && h->alloc(&h->d_z_b, h->nip) &&
+         h->alloc(&h->d_lam_b, h->nip) && h->alloc(&h->d_el_b, h->nip) &&
+         h->alloc(&h->d_fe, (size_t)h->ncell * h->nn * h->nd) &&
+         h->alloc(&h->d_ke, (size_t)h->ncell * h->npair * h->nd * h->nd) &&
+         h->upload(&h->d_inc_ptr, h->pat.inc_ptr.data(), h->pat.inc_ptr.size()) &&
+         h->upload(&h->d_inc, h->pat.inc.data(), h->pat.inc.size()) &&
+         h->upload(&h->d_bptr, h->pat.bptr.data(), h->pat.bptr.size()) &&
+         h->upload(&h->d_urow, h->pat.u_row.data(), h->pat.u_row.size()) &&
+         h->upload(&h->d_ucol, h->pat.u_col.data(), h->pat.u_col.size()) &&
+         h->upload(&h->d_ukab, h->pat.u_kab.data(), h->pat.u_kab.size()) &&
+         h->upload(&h->d_ukba, h->pat.u_kba.data(), h->pat.u_kba.size()) &&
+         h->upload(&h->d_ucptr, h->pat.u_cptr.data(), h->pat.u_cptr.size()) &&
+         h->upload(&h->d_ucontrib, h->pat.u_contrib.data(), h->pat.u_contrib.size()) &&
+         h->alloc(&h->d_ddu, h->ndof) && h->alloc(&h->d_ff, h->ndof) && h->alloc(&h->d_status, 4);
+    if (!ok) {
+        delete h;
+        return PMS_ERR_NOMEM;
+    }
+    cudaMemset(h->d_status, 0, 16);
+    if (cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking) != cudaSuccess) {
+        delete h;
+        return PMS_ERR_CUDA;
+    }
+    h->stream = h->own_stream;
+    int tab_len = h->ng * h->nn * h->nd + h->ng;
+    h->smem_bytes = (((tab_len + 1) & ~1) + WPB * 2 * h->nn * 5 * h->nd) * (int)sizeof(double);
+    // the state starts as LocalState::new: zero stress, elastic, zero internal variables
+    init_state_kernel<<<grid_1d(h->nip), 256, 0, h->stream>>>(h->nip, h->nc, h->d_mats, h->d_cmat, h->ng, h->d_sig,
+                                                              h->d_z, h->d_lam, h->d_el);
+    if (cudaStreamSynchronize(h->stream) != cudaSuccess) {
+        delete h;
+        return PMS_ERR_CUDA;
+    }
+    *out = h;
+    return PMS_OK;
+}
+
+void pms_elements_destroy(pms_elements* h) { delete h; }
+
+int pms_elements_get_info(const pms_elements* h, pms_elements_info* o) {
+    if (!h || !o) return PMS_ERR_INVALID;
+    o->ndim = h->nd;
+    o->kind = h->kind;
+    o->nnode = h->nn;
+    o->ngauss = h->ng;
+    o->ncomp = h->nc;
+    o->npoint = h->npoint;
+    o->ncell = h->ncell;
+    o->ndof = h->ndof;
+    o->nip = h->nip;
+    o->nnz = h->nnz;
+    o->nblock_upper = h->pat.nupper();
+    o->ncontrib = (int64_t)h->pat.u_contrib.size();
+    o->device_bytes = h->device_bytes;
+    return PMS_OK;
+}
+
+int pms_elements_set_stream(pms_elements* h, void* stream) {
+    if (!h) return PMS_ERR_INVALID;
+    h->stream = stream ? (cudaStream_t)stream : h->own_stream;
+    return PMS_OK;
+}
+
+int pms_elements_csr_pattern(pms_elements* h, int64_t* indptr, int32_t* indices, int32_t mem) {
+    if (!h) return PMS_ERR_INVALID;
+    const int nd = h->nd;
+    std::vector<int64_t> ip;
+    std::vector<int32_t> ix;
+    int64_t* ipo = indptr;
+    int32_t* ixo = indices;
+    if (mem == PMS_MEM_DEVICE) {
+        ip.resize(h->ndof + 1);
+        ix.resize(indices ? h->nnz : 0);
+        ipo = ip.data();
+        ixo = indices ? ix.data() : nullptr;
+    }
+    const Pattern& p = h->pat;
+    for (int64_t A = 0; A < h->npoint; A++) {
+        int64_t b0 = p.bptr[A], nb = p.bptr[A + 1] - b0;
+        for (int i = 0; i < nd; i++) {
+            int64_t r = A * nd + i;
+            int64_t start = (int64_t)nd * nd * b0 + (int64_t)i * nd * nb;
+            if (ipo) ipo[r] = start;
+            if (ixo)
+                for (int64_t k = 0; k < nb; k++)
+                    for (int j = 0; j < nd; j++) ixo[start + k * nd + j] = p.bcol[b0 + k] * nd + j;
+        }
+    }
+    if (ipo) ipo[h->ndof] = h->nnz;
+    if (mem == PMS_MEM_DEVICE) {
+        if (indptr && cudaMemcpy(indptr, ip.data(), ip.size() * 8, cudaMemcpyHostToDevice) != cudaSuccess)
+            return fail(h, PMS_ERR_CUDA, "copy of indptr failed");
+        if (indices && cudaMemcpy(indices, ix.data(), ix.size() * 4, cudaMemcpyHostToDevice) != cudaSuccess)
+            return fail(h, PMS_ERR_CUDA, "copy of indices failed");
+    }
+    return PMS_OK;
+}
+
+int pms_elements_initialize(pms_elements* h) {
+    if (!h) return PMS_ERR_INVALID;
+    init_state_kernel<<<grid_1d(h->nip), 256, 0, h->stream>>>(h->nip, h->nc, h->d_mats, h->d_cmat, h->ng, h->d_sig,
+                                                              h->d_z, h->d_lam, h->d_el);
+    h->launches++;
+    return cuda_check(h);
+}
+
+int pms_elements_reset_algorithmic(pms_elements* h) {
+    if (!h) return PMS_ERR_INVALID;
+    zero_lambda_kernel<<<grid_1d(h->nip), 256, 0, h->stream>>>(h->nip, h->d_lam);
+    h->launches++;
+    return cuda_check(h);
+}
+
+static int copy_state(pms_elements* h, bool to_backup) {
+    size_t bs = (size_t)h->nip * h->nc * 8, bn = (size_t)h->nip * 8;
+    double *ss = h->d_sig, *zs = h->d_z, *ls = h->d_lam, *sd = h->d_sig_b, *zd = h->d_z_b, *ld = h->d_lam_b;
+    uint8_t *es = h->d_el, *ed = h->d_el_b;
+    if (!to_backup) {
+        std::swap(ss, sd);
+        std::swap(zs, zd);
+        std::swap(ls, ld);
+        std::swap(es, ed);
+    }
+    cudaMemcpyAsync(sd, ss, bs, cudaMemcpyDeviceToDevice, h->stream);
+    cudaMemcpyAsync(zd, zs, bn, cudaMemcpyDeviceToDevice, h->stream);
+    cudaMemcpyAsync(ld, ls, bn, cudaMemcpyDeviceToDevice, h->stream);
+    cudaMemcpyAsync(ed, es, (size_t)h->nip, cudaMemcpyDeviceToDevice, h->stream);
+    return cuda_check(h);
+}
+
+int pms_elements_backup(pms_elements* h) { return h ? copy_state(h, true) : PMS_ERR_INVALID; }
+int pms_elements_restore(pms_elements* h) { return h ? copy_state(h, false) : PMS_ERR_INVALID; }
+
+static int finish_host(pms_elements* h) {
+    int32_t st[4];
+    if (cudaMemcpyAsync(st, h->d_status, 16, cudaMemcpyDeviceToHost, h->stream) != cudaSuccess ||
+        cudaStreamSynchronize(h->stream) != cudaSuccess)
+        return fail(h, PMS_ERR_CUDA, cudaGetErrorString(cudaGetLastError()));
+    if (st[0] != 0) {
+        h->err_cell = st[1];
+        h->err_ip = st[2];
+        cudaMemsetAsync(h->d_status, 0, 16, h->stream);
+        switch (st[0]) {
+        case E_ZERO_SIGMA_D:
+            return fail(h, PMS_ERR_ZERO_SIGMA_D,
+                        "von Mises plastic update must not lead to zero sigma_d (sigma_d < 1e-10)");
+        case E_ZERO_NORM_S:
+            return fail(h, PMS_ERR_ZERO_NORM_S,
+                        "von Mises stiffness cannot be computed with zero deviatoric norm (norm_s < 1e-10)");
+        case E_JACOBIAN:
+            return fail(h, PMS_ERR_JACOBIAN, "the determinant of the Jacobian must be positive");
+        default:
+            return fail(h, PMS_ERR_INVALID, "device error");
+        }
+    }
+    return PMS_OK;
+}
+
+int pms_elements_sync(pms_elements* h) { return h ? finish_host(h) : PMS_ERR_INVALID; }
+
+// Common path of the four batched calls.
+static int run(pms_elements* h, const double* ddu, double* ff, double* csr, int mem, int upd, bool dof, bool dok) {
+    if (!h || (mem != PMS_MEM_HOST && mem != PMS_MEM_DEVICE)) return PMS_ERR_INVALID;
+    if (upd != UPD_NONE && !ddu) return fail(h, PMS_ERR_INVALID, "ddu is required");
+    const double* d_ddu = ddu;
+    double* d_ff = ff;
+    double* d_csr = csr;
+    if (mem == PMS_MEM_HOST) {
+        if (upd != UPD_NONE) {
+            cudaMemcpyAsync(h->d_ddu, ddu, (size_t)h->ndof * 8, cudaMemcpyHostToDevice, h->stream);
+            d_ddu = h->d_ddu;
+        }
+        d_ff = ff ? h->d_ff : nullptr;
+        if (csr) {
+            if (!h->d_csr && !h->alloc(&h->d_csr, (size_t)h->nnz)) return fail(h, PMS_ERR_NOMEM, "out of memory");
+            d_csr = h->d_csr;
+        }
+    }
+    dof = dof && d_ff;
+    dok = dok && d_csr;
+    ElemArgs a = make_args(h, d_ddu);
+    auto timed = [h](int k, auto&& fn) {
+        if (!h->timing) {
+            fn();
+            return;
+        }
+        auto e = h->event_pair();
+        cudaEventRecord(e.first, h->stream);
+        fn();
+        cudaEventRecord(e.second, h->stream);
+        h->ev_pending[k].push_back(e);
+    };
+    if (upd != UPD_NONE || dof || dok) timed(0, [&] { launch_elem(h, a, upd, dof, dok); });
+    if (dof) timed(1, [&] { launch_f_gather(h, d_ff); });
+    if (dok) timed(2, [&] { launch_kk_gather(h, d_csr); });
+    int rc = cuda_check(h);
+    if (rc) return rc;
+    if (mem == PMS_MEM_HOST) {
+        if (dof) cudaMemcpyAsync(ff, d_ff, (size_t)h->ndof * 8, cudaMemcpyDeviceToHost, h->stream);
+        if (dok) cudaMemcpyAsync(csr, d_csr, (size_t)h->nnz * 8, cudaMemcpyDeviceToHost, h->stream);
+        return finish_host(h);
+    }
+    return PMS_OK;
+}
+
+int pms_elements_update_secondary(pms_elements* h, const double* ddu, int32_t mem) {
+    return run(h, ddu, nullptr, nullptr, mem, UPD_CURRENT, false, false);
+}
+
+int pms_elements_assemble_f_int(pms_elements* h, double* ff_int, int32_t mem) {
+    if (!ff_int) return PMS_ERR_INVALID;
+    return run(h, nullptr, ff_int, nullptr, mem, UPD_NONE, true, false);
+}
+
+int pms_elements_assemble_kk(pms_elements* h, double* csr_values, int32_t mem) {
+    if (!csr_values) return PMS_ERR_INVALID;
+    return run(h, nullptr, nullptr, csr_values, mem, UPD_NONE, false, true);
+}
+
+int pms_elements_update_and_assemble(pms_elements* h, const double* ddu, double* ff_int, double* csr_values,
+                                     int32_t mem) {
+    return run(h, ddu, ff_int, csr_values, mem, UPD_BACKUP, ff_int != nullptr, csr_values != nullptr);
+}
+
+static int one_cell(pms_elements* h, int64_t cell, bool dof, bool dok) {
+    if (!h || cell < 0 || cell >= h->ncell) return PMS_ERR_INVALID;
+    ElemArgs a = make_args(h, nullptr);
+    a.ncell = 1;
+    a.cell0 = cell;
+    launch_elem(h, a, UPD_NONE, dof, dok);
+    int rc = cuda_check(h);
+    if (rc) return rc;
+    return finish_host(h);
+}
+
+int pms_element_calc_f_int(pms_elements* h, int64_t cell, double* f) {
+    if (!f) return PMS_ERR_INVALID;
+    int rc = one_cell(h, cell, true, false);
+    if (rc) return rc;
+    if (cudaMemcpy(f, h->d_fe + cell * h->nn * h->nd, (size_t)h->nn * h->nd * 8, cudaMemcpyDeviceToHost) !=
+        cudaSuccess)
+        return fail(h, PMS_ERR_CUDA, "copy failed");
+    return PMS_OK;
+}
+
+int pms_element_calc_jacobian(pms_elements* h, int64_t cell, double* kk) {
+    if (!kk) return PMS_ERR_INVALID;
+    int rc = one_cell(h, cell, false, true);
+    if (rc) return rc;
+    const int nd = h->nd, nn = h->nn, ne = nn * nd;
+    std::vector<double> blk((size_t)h->npair * nd * nd);
+    if (cudaMemcpy(blk.data(), h->d_ke + cell * h->npair * nd * nd, blk.size() * 8, cudaMemcpyDeviceToHost) !=
+        cudaSuccess)
+        return fail(h, PMS_ERR_CUDA, "copy failed");
+    for (int a = 0; a < nn; a++)
+        for (int b = a; b < nn; b++) {
+            const double* B = blk.data() + (size_t)pair_index(nn, a, b) * nd * nd;
+            for (int i = 0; i < nd; i++)
+                for (int j = 0; j < nd; j++) {
+                    kk[(a * nd + i) * ne + b * nd + j] = B[i * nd + j];
+                    kk[(b * nd + j) * ne + a * nd + i] = B[i * nd + j];
+                }
+        }
+    return PMS_OK;
+}
+
+int pms_elements_get_state(pms_elements* h, double* sig, double* ivs, uint8_t* elastic) {
+    if (!h) return PMS_ERR_INVALID;
+    if (cudaStreamSynchronize(h->stream) != cudaSuccess) return fail(h, PMS_ERR_CUDA, "sync failed");
+    const int64_t n = h->nip;
+    std::vector<double> s((size_t)n * h->nc), z(n), l(n);
+    std::vector<uint8_t> e(n);
+    cudaMemcpy(s.data(), h->d_sig, s.size() * 8, cudaMemcpyDeviceToHost);
+    cudaMemcpy(z.data(), h->d_z, n * 8, cudaMemcpyDeviceToHost);
+    cudaMemcpy(l.data(), h->d_lam, n * 8, cudaMemcpyDeviceToHost);
+    cudaMemcpy(e.data(), h->d_el, n, cudaMemcpyDeviceToHost);
+    for (int64_t i = 0; i < n; i++) {
+        if (sig)
+            for (int c = 0; c < h->nc; c++) sig[i * h->nc + c] = s[(size_t)c * n + i];
+        if (ivs) {
+            ivs[2 * i] = z[i];
+            ivs[2 * i + 1] = l[i];
+        }
+        if (elastic) elastic[i] = e[i];
+    }
+    return cuda_check(h);
+}
+
+int pms_elements_set_state(pms_elements* h, const double* sig, const double* ivs, const uint8_t* elastic) {
+    if (!h || !sig || !ivs || !elastic) return PMS_ERR_INVALID;
+    const int64_t n = h->nip;
+    std::vector<double> s((size_t)n * h->nc), z(n), l(n);
+    for (int64_t i = 0; i < n; i++) {
+        for (int c = 0; c < h->nc; c++) s[(size_t)c * n + i] = sig[i * h->nc + c];
+        z[i] = ivs[2 * i];
+        l[i] = ivs[2 * i + 1];
+    }
+    cudaStreamSynchronize(h->stream);
+    cudaMemcpy(h->d_sig, s.data(), s.size() * 8, cudaMemcpyHostToDevice);
+    cudaMemcpy(h->d_z, z.data(), n * 8, cudaMemcpyHostToDevice);
+    cudaMemcpy(h->d_lam, l.data(), n * 8, cudaMemcpyHostToDevice);
+    cudaMemcpy(h->d_el, elastic, n, cudaMemcpyHostToDevice);
+    return cuda_check(h);
+}
+
+const char* pms_elements_last_error(const pms_elements* h) { return h ? h->last_error.c_str() : "null handle"; }
+
+int pms_elements_error_location(const pms_elements* h, int64_t* cell, int32_t* ip) {
+    if (!h) return PMS_ERR_INVALID;
+    if (cell) *cell = h->err_cell;
+    if (ip) *ip = h->err_ip;
+    return PMS_OK;
+}
+
+int64_t pms_elements_launch_count(const pms_elements* h) { return h ? h->launches : 0; }
+
+int pms_elements_set_timing(pms_elements* h, int32_t on) {
+    if (!h) return PMS_ERR_INVALID;
+    h->timing = on != 0;
+    return PMS_OK;
+}
+
+int pms_elements_kernel_times(pms_elements* h, double* ms, int64_t* counts) {
+    if (!h) return PMS_ERR_INVALID;
+    if (cudaStreamSynchronize(h->stream) != cudaSuccess) return fail(h, PMS_ERR_CUDA, "sync failed");
+    for (int k = 0; k < 3; k++) {
+        double tot = 0.0;
+        for (auto& e : h->ev_pending[k]) {
+            float t = 0.f;
+            cudaEventElapsedTime(&t, e.first, e.second);
+            tot += t;
+            h->ev_pool.push_back(e);
+        }
+        if (ms) ms[k] = tot;
+        if (counts) counts[k] = (int64_t)h->ev_pending[k].size();
+        h->ev_pending[k].clear();
+    }
+    return cuda_check(h);
+}
+
+int pms_mesh_csr_pattern(const pms_mesh* mesh, int64_t* indptr, int32_t* indices, int64_t* nnz) {
+    if (!mesh || !mesh->cells || mesh->kind < 0 || mesh->kind > 8 || kind_ndim(mesh->kind) != mesh->ndim)
+        return PMS_ERR_INVALID;
+    Pattern p;
+    const char* msg = nullptr;
+    const int nd = mesh->ndim;
+    if (!build_pattern(nd, kind_nnode(mesh->kind), mesh->npoint, mesh->ncell, mesh->cells, p, &msg))
+        return PMS_ERR_INVALID;
+    const int64_t total = p.nblock() * nd * nd;
+    if (nnz) *nnz = total;
+    for (int64_t A = 0; A < mesh->npoint; A++) {
+        int64_t b0 = p.bptr[A], nb = p.bptr[A + 1] - b0;
+        for (int i = 0; i < nd; i++) {
+            int64_t start = (int64_t)nd * nd * b0 + (int64_t)i * nd * nb;
+            if (indptr) indptr[A * nd + i] = start;
+            if (indices)
+                for (int64_t k = 0; k < nb; k++)
+                    for (int j = 0; j < nd; j++) indices[start + k * nd + j] = p.bcol[b0 + k] * nd + j;
+        }
+    }
+    if (indptr) indptr[mesh->npoint * nd] = total;
+    return PMS_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,78 @@
+"""C-ABI checks that need no GPU: the library loads, exports every symbol include/pms.h declares,
+and the host-only CSR pattern equals the oracle's COO->CSR pattern."""
+import ctypes
+import os
+import re
+
+import numpy as np
+import pytest
+
+import oracle
+from pmsim_b200 import _lib
+from pmsim_b200 import mesh as M
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_functions():
+    names = set()
+    for fn in os.listdir(os.path.join(ROOT, "include")):
+        if fn.endswith(".h"):
+            txt = open(os.path.join(ROOT, "include", fn)).read()
+            txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
+            names |= set(re.findall(r"\b(pms_\w+)\s*\(", txt))
+    return names
+
+
+def test_library_exports_every_declared_symbol():
+    L = _lib.load()
+    names = declared_functions()
+    assert len(names) >= 25
+    missing = [n for n in sorted(names) if not hasattr(L, n)]
+    assert not missing, missing
+    assert set(_lib.SIGNATURES) == names
+
+
+def test_version_string():
+    assert b"sm_100a" in _lib.load().pms_version()
+
+
+@pytest.mark.parametrize("kind", [M.TRI3, M.TRI6, M.QUA4, M.QUA8, M.QUA9, M.TET4, M.HEX8, M.HEX20])
+def test_host_csr_pattern_matches_oracle(kind):
+    if M.KIND_NDIM[kind] == 2:
+        m = M.structured_2d(kind, 3, 2, 3.0, 2.0)
+    else:
+        m = M.structured_3d(kind, 2, 2, 1)
+    L = _lib.load()
+    cm = _lib.Mesh_(m.ndim, m.kind, m.npoint, m.ncell, _lib.ptr(m.coords), _lib.ptr(m.cells), None)
+    nnz = ctypes.c_int64()
+    indptr = np.zeros(m.ndof + 1, np.int64)
+    assert L.pms_mesh_csr_pattern(ctypes.byref(cm), _lib.ptr(indptr), None, ctypes.byref(nnz)) == 0
+    indices = np.zeros(nnz.value, np.int32)
+    assert L.pms_mesh_csr_pattern(ctypes.byref(cm), _lib.ptr(indptr), _lib.ptr(indices), ctypes.byref(nnz)) == 0
+    o = oracle.OracleElements(m, 0, oracle.Params(1.0, 0.3))
+    o.initialize()
+    ip, ix, _ = o.assemble_kk_csr()
+    assert np.array_equal(ip, indptr) and np.array_equal(ix, indices)
+
+
+def test_hex20_block_sizes_of_the_large_problem():
+    """64x64x32 Hex20: 549,185 points, 1,647,555 DOF, nnz 279,514,377 (host pattern, no GPU)."""
+    m = M.structured_3d(M.HEX20, 64, 64, 32, 64.0, 64.0, 32.0)
+    assert (m.npoint, m.ncell, m.ndof) == (549185, 131072, 1647555)
+    L = _lib.load()
+    cm = _lib.Mesh_(m.ndim, m.kind, m.npoint, m.ncell, _lib.ptr(m.coords), _lib.ptr(m.cells), None)
+    nnz = ctypes.c_int64()
+    assert L.pms_mesh_csr_pattern(ctypes.byref(cm), None, None, ctypes.byref(nnz)) == 0
+    assert nnz.value == 279514377
+
+
+def test_invalid_arguments_are_rejected_without_gpu():
+    L = _lib.load()
+    bad = _lib.Mesh_(2, 99, 4, 1, None, None, None)
+    assert L.pms_mesh_csr_pattern(ctypes.byref(bad), None, None, None) == 1
+    m = M.structured_2d(M.QUA4, 1, 1)
+    cells = m.cells.copy()
+    cells[0, 0] = 100  # point out of range
+    cm = _lib.Mesh_(2, M.QUA4, m.npoint, 1, _lib.ptr(m.coords), _lib.ptr(cells), None)
+    assert L.pms_mesh_csr_pattern(ctypes.byref(cm), None, None, None) == 1

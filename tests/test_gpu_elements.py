@@ -1,0 +1,160 @@
+"""K2 parity: fused element kernels + deterministic CSR gather vs the CPU oracle, every kind.
+
+Reference: ElementSolid::{update_secondary_values, calc_f_int, calc_jacobian}
+(src/fem/element_solid.rs:124-224), Elements loops (src/fem/elements.rs:132-205), COO assembly
+(src/base/assembly.rs:38-139).  Tolerance: relative (normwise) 1e-12; CSR bit-reproducible.
+"""
+import numpy as np
+import pytest
+
+import oracle
+from gpu_util import assert_close, perturbed_mesh, plastic_ddu
+from pmsim_b200 import mesh as M
+
+pytestmark = pytest.mark.gpu
+
+E, NU, H, Z0 = 2e5, 0.3, 1e3, 250.0
+KINDS = [M.TRI3, M.TRI6, M.QUA4, M.QUA8, M.QUA9, M.TET4, M.HEX8, M.HEX20]
+GRID = {2: (4, 3, 1), 3: (2, 2, 2)}
+
+
+def make(kind, model=1, ngauss=0, seed=0):
+    from pmsim_b200.elements import Elements, Material
+    m = perturbed_mesh(kind, seed=seed, n=GRID[M.KIND_NDIM[kind]])
+    mat = Material.von_mises(E, NU, H, Z0) if model == 1 else Material.linear_elastic(E, NU)
+    g = Elements(m, mat, ngauss=ngauss)
+    o = oracle.OracleElements(m, model, oracle.Params(E, NU, H, Z0), ngauss=ngauss, sym_tol=-1.0)
+    return m, g, o
+
+
+def oracle_csr_values(o, indptr, indices):
+    ip, ix, data = o.assemble_kk_csr()
+    assert np.array_equal(ip, indptr) and np.array_equal(ix, indices)
+    return data
+
+
+@pytest.mark.parametrize("kind", KINDS, ids=[M.KIND_NAMES[k] for k in KINDS])
+def test_fused_update_and_assemble_matches_oracle(kind):
+    m, g, o = make(kind)
+    indptr, indices = g.csr_pattern()
+    g.initialize_internal_values()
+    o.initialize()
+    # iteration 0 of a step: assemble from the initial (elastic) state
+    assert np.all(g.assemble_f_int() == 0.0)
+    k0 = g.assemble_kk()
+    assert_close(k0, oracle_csr_values(o, indptr, indices), what="K elastic")
+    # one Newton update from the backed-up state, then F_int and K on the updated state
+    ddu = plastic_ddu(m, seed=kind)
+    g.backup_secondary_values()
+    ff = np.zeros(g.ndof)
+    kv = np.zeros(g.nnz)
+    g.update_and_assemble(ddu, ff, kv)
+    o.update_secondary_values(ddu)
+    sig, ivs, el = g.get_state()
+    assert np.array_equal(el, o.elastic), "elastic flags differ"
+    assert 0 < (1 - el.mean()) < 1, "expected a mix of elastic and plastic IPs"
+    assert_close(sig, o.sig, what="sigma")
+    assert_close(ivs, o.ivs, what="[z, lambda]")
+    assert_close(ff, o.assemble_f_int(), what="f_int")
+    assert_close(kv, oracle_csr_values(o, indptr, indices), what="K")
+
+
+@pytest.mark.parametrize("kind", [M.QUA8, M.HEX20], ids=["qua8", "hex20"])
+def test_separate_calls_match_fused(kind):
+    """update_secondary + assemble_f_int + assemble_kk == fused call (to rounding: the two kernel
+    instantiations may fuse multiply-adds differently)."""
+    m, g, o = make(kind, seed=3)
+    ddu = plastic_ddu(m, seed=5)
+    g.initialize_internal_values()
+    g.backup_secondary_values()
+    ff1, kv1 = np.zeros(g.ndof), np.zeros(g.nnz)
+    g.update_and_assemble(ddu, ff1, kv1)
+    s1 = g.get_state()
+    g.restore_secondary_values()
+    g.update_secondary_values(ddu)
+    ff2 = g.assemble_f_int()
+    kv2 = g.assemble_kk()
+    s2 = g.get_state()
+    assert_close(ff1, ff2, tol=1e-13, what="f_int")
+    assert_close(kv1, kv2, tol=1e-13, what="K")
+    assert_close(s1[0], s2[0], tol=1e-13, what="sigma")
+    assert_close(s1[1], s2[1], tol=1e-13, what="[z, lambda]")
+    assert np.array_equal(s1[2], s2[2])
+
+
+@pytest.mark.parametrize("kind", [M.QUA4, M.QUA8, M.HEX8, M.HEX20], ids=["qua4", "qua8", "hex8", "hex20"])
+def test_per_cell_calls_match_oracle(kind):
+    m, g, o = make(kind, seed=7)
+    ddu = plastic_ddu(m, seed=9)
+    g.initialize_internal_values()
+    g.update_secondary_values(ddu)
+    o.initialize()
+    o.update_secondary_values(ddu)
+    ng, nc = g.ngauss, g.ncomp
+    for cell in [0, m.ncell // 2, m.ncell - 1]:
+        X = m.coords[m.cells[cell]]
+        sl = slice(cell * ng, (cell + 1) * ng)
+        kf = oracle.elem_jacobian(kind, ng, X, 1, oracle.Params(E, NU, H, Z0), o.sig[sl], o.ivs[sl], o.elastic[sl])
+        assert_close(g.calc_jacobian(cell), kf, what=f"K_e cell {cell}")
+        assert_close(g.calc_f_int(cell), oracle.elem_f_int(kind, ng, X, o.sig[sl]), what=f"f_e cell {cell}")
+
+
+def test_csr_bit_reproducible():
+    m, g, o = make(M.HEX20, seed=1)
+    ddu = plastic_ddu(m, seed=2)
+    g.initialize_internal_values()
+    g.backup_secondary_values()
+    outs = []
+    for _ in range(3):
+        ff, kv = np.zeros(g.ndof), np.zeros(g.nnz)
+        g.update_and_assemble(ddu, ff, kv)
+        outs.append((ff.tobytes(), kv.tobytes()))
+    assert outs[0] == outs[1] == outs[2]
+
+
+@pytest.mark.parametrize("ngauss", [4, 9])
+def test_qua8_gauss_rules(ngauss):
+    m, g, o = make(M.QUA8, ngauss=ngauss, seed=4)
+    ddu = plastic_ddu(m, seed=4)
+    g.initialize_internal_values()
+    g.update_secondary_values(ddu)
+    o.initialize()
+    o.update_secondary_values(ddu)
+    sig, ivs, el = g.get_state()
+    assert_close(sig, o.sig, what="sigma")
+    assert_close(g.assemble_kk(), oracle_csr_values(o, *g.csr_pattern()), what="K")
+
+
+def test_linear_elastic_and_materials_per_cell():
+    """cell_material selects the parameters per cell (cell attribute -> ParamSolid)."""
+    from pmsim_b200.elements import Elements, Material
+    m = perturbed_mesh(M.QUA8, seed=8, n=(4, 2, 1))
+    cm = (np.arange(m.ncell) % 2).astype(np.int32)
+    mats = [Material.von_mises(E, NU, H, Z0), Material.linear_elastic(2 * E, 0.25)]
+    g = Elements(m, mats, cell_material=cm)
+    ddu = plastic_ddu(m, seed=8)
+    g.initialize_internal_values()
+    g.update_secondary_values(ddu)
+    sig, ivs, el = g.get_state()
+    ng = g.ngauss
+    for c in range(m.ncell):
+        model = 1 if cm[c] == 0 else 0
+        prm = oracle.Params(E, NU, H, Z0) if model == 1 else oracle.Params(2 * E, 0.25)
+        sub = oracle.OracleElements(M.Mesh(2, m.coords, m.cells[c:c + 1], M.QUA8), model, prm)
+        sub.initialize()
+        sub.update_secondary_values(ddu)
+        assert_close(sig[c * ng:(c + 1) * ng], sub.sig, what=f"cell {c}")
+
+
+def test_errors_are_reported_with_location():
+    """A collapsed cell gives the Jacobian error with its cell id (no GPU fault)."""
+    from pmsim_b200.elements import Elements, Material
+    from pmsim_b200._lib import PmsError
+    m = M.structured_2d(M.QUA4, 2, 1, 2.0, 1.0)
+    c = m.coords.copy()
+    c[m.cells[1][2]] = c[m.cells[1][0]]  # fold cell 1
+    g = Elements(M.Mesh(2, c, m.cells, M.QUA4), Material.von_mises(E, NU, H, Z0))
+    with pytest.raises(PmsError) as ei:
+        g.assemble_kk()
+    assert "Jacobian" in str(ei.value)
+    assert g.error_location()[0] == 1

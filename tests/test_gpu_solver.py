@@ -1,0 +1,54 @@
+"""Newton-level parity: the reference's SPO/HYPLAS runs through the B200 elements.
+
+Same boundary conditions, steps and tolerances as the reference tests
+(tests/test_von_mises_single_element_2d.rs, test_von_mises_2x2_elements_2d.rs,
+test_spo_754_footing.rs, test_spo_755_tensile.rs); the iteration counts must equal those of
+the oracle driver on the same problem.
+"""
+import numpy as np
+import pytest
+
+import oracle
+import problems
+from oracle.driver import OracleSolver
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("name", list(problems.SPO_PROBLEMS))
+def test_spo_golden_on_gpu(name):
+    from pmsim_b200.elements import Elements, Material
+    from pmsim_b200.solver import SolverImplicit
+    pb = problems.SPO_PROBLEMS[name]()
+    m = pb["mesh"]
+    el = Elements(m, Material.von_mises(*pb["params"]), ngauss=pb["ngauss"])
+    solver = SolverImplicit(el, pb["essential"], n_max_iterations=20, t_fin=float(pb["nsteps"]))
+    worst = [0.0, 0.0]
+
+    def cb(step, t, u, el):
+        sig = el.get_state()[0]
+        du, ds = problems.compare_step(pb["golden"], step, u, sig, pb["ngauss"])
+        worst[0] = max(worst[0], du)
+        worst[1] = max(worst[1], ds)
+
+    assert solver.solve(cb) == pb["nsteps"]
+    assert worst[0] <= pb["tol_u"], worst
+    assert worst[1] <= pb["tol_s"], worst
+    # same Newton history as the oracle driver
+    oel = oracle.OracleElements(m, oracle.MODEL_VON_MISES, oracle.Params(*pb["params"]), ngauss=pb["ngauss"],
+                                sym_tol=pb["sym_tol"])
+    osol = OracleSolver(oel, m.ndof, pb["essential"], n_max_iterations=20, t_fin=float(pb["nsteps"]))
+    osol.solve()
+    assert [len(h) for h in solver.history] == [len(h) for h in osol.history]
+    for hg, ho in zip(solver.history, osol.history):
+        assert hg[-1][1] < 1e-10 or (hg[-1][2] is not None and hg[-1][2] < 1e-8)
+
+
+def test_smith_5d11_linear_elastic_on_gpu():
+    from pmsim_b200.elements import Elements, Material
+    from pmsim_b200.solver import SolverImplicit
+    pb = problems.smith_5d11()
+    el = Elements(pb["mesh"], Material.linear_elastic(1e6, 0.3))
+    out = {}
+    SolverImplicit(el, pb["essential"], t_fin=1.0).solve(lambda s, t, u, e: out.setdefault("u", u))
+    np.testing.assert_allclose(out["u"], pb["golden"]["uu_correct"], rtol=0, atol=1e-13)
