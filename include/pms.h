@@ -32,7 +32,8 @@ enum pms_status_code {
                                  (norm_s < 1e-10)"  src/material/von_mises.rs:147-150 */
     PMS_ERR_JACOBIAN = 5,     /* non-positive Jacobian determinant at an IP (gemlab calc_gradient) */
     PMS_ERR_NOMEM = 6,        /* device allocation failed */
-    PMS_ERR_UNSUPPORTED = 7   /* idealization/kind not implemented (plane stress, axisymmetric) */
+    PMS_ERR_UNSUPPORTED = 7,  /* idealization/kind not implemented (plane stress, axisymmetric) */
+    PMS_ERR_TOO_LARGE = 8     /* batch does not fit the fixed scratch of pms_element_calc_noalloc */
 };
 
 /* ---- element kinds (gemlab GeoKind subset used by solids) ---------------------------------- */
@@ -180,6 +181,26 @@ int pms_vm_update_and_stiffness_host(const pms_material* mat, int32_t ndim, int6
 /* Measures the FP64 FMA pipe: blocks x 256 threads, 8 independent FMA chains of `iters` each
  * (16*iters FLOP per thread); out[blocks*256] receives the chain sums.  Used as the FP64 peak. */
 int pms_probe_fp64_fma(int64_t iters, int32_t blocks, double* out, void* stream);
+
+/* Element vectors and matrices for a batch of cells WITHOUT ANY DEVICE ALLOCATION.
+ * No counterpart in the reference: it exists for callers that cannot call cudaMalloc -- a program
+ * running inside another framework that owns the whole device-memory budget, a real-time loop
+ * where an allocation would stall or synchronise the GPU, or a foreign-language element loop (for
+ * example Rust behind an FFI) that has no CUDA allocator.  It computes what
+ * ElementTrait::calc_f_int / calc_jacobian compute, for ncell independent cells given on the
+ * host:  X[ncell][nnode][ndim] coordinates; the IP state structure-of-arrays with stride
+ * nip = ncell*ngauss: sig[ncomp][nip] (Mandel), ivs[2][nip] (z then lambda), elastic[nip].
+ * Outputs (host, nullable, at least one): f[ncell][nnode*ndim] and kk[ncell][ne][ne] row-major.
+ * All device work uses one file-scope array of 16 MiB, held by every GPU that loads the library
+ * until the process exits; *max_cells (nullable) receives the largest batch that fits for this
+ * kind, rule and choice of outputs, and a larger batch returns PMS_ERR_TOO_LARGE (split it).
+ * The array is shared by every call and keeps the last call's contents: calls that overlap on the
+ * GPU (from two threads, or on two streams without ordering) race, so serialise them.  The first
+ * call on a device looks up the array's address for that device; make that first call before any
+ * stream capture.  stream: cudaStream_t or NULL; the call returns after its results are on the host. */
+int pms_element_calc_noalloc(int32_t kind, int32_t ngauss, double thickness, const pms_material* mat,
+                             int64_t ncell, const double* X, const double* sig, const double* ivs,
+                             const uint8_t* elastic, double* f, double* kk, int64_t* max_cells, void* stream);
 
 /* Library version string and the number of kernels launched by the material entry points. */
 const char* pms_version(void);

@@ -27,6 +27,7 @@ ERRORS = {
     5: "the determinant of the Jacobian must be positive",
     6: "out of device memory",
     7: "unsupported idealization or element kind",
+    8: "batch too large for the fixed scratch of the no-allocation entry point",
 }
 
 
@@ -93,6 +94,8 @@ SIGNATURES = {
     "pms_elements_set_timing": (_I, [_V, _I]),
     "pms_elements_kernel_times": (_I, [_V, _V, _V]),
     "pms_probe_fp64_fma": (_I, [_I64, _I, _V, _V]),
+    "pms_element_calc_noalloc": (_I, [_I, _I, _D, ctypes.POINTER(Material_), _I64, _V, _V, _V, _V, _V, _V,
+                                      ctypes.POINTER(_I64), _V]),
     "pms_version": (ctypes.c_char_p, []),
     "pms_material_launch_count": (_I64, []),
 }

@@ -1070,3 +1070,211 @@ int pms_mesh_csr_pattern(const pms_mesh* mesh, int64_t* indptr, int32_t* indices
 }
 
 }  // extern "C"
+
+// ------------------------------------------------------------------------------------------
+// Element matrices without any device allocation.
+//
+// Some callers cannot call cudaMalloc: a host program that runs inside another framework's
+// fixed device-memory budget (the framework owns every allocation), a real-time loop where an
+// allocation would stall or synchronise the device, or a foreign-language caller (for example a
+// Rust element loop behind an FFI) that has no CUDA allocator at all.  For them this entry point
+// takes host inputs and host outputs and keeps everything it needs on the device in one
+// file-scope array of fixed size, so it never allocates.  Limit: NOALLOC_SCRATCH_BYTES per
+// device, held by every GPU that loads this library until the process exits; a call whose cells
+// do not fit is rejected (the largest batch that fits is reported back).  All calls share the
+// array and it keeps the last call's contents, so calls that overlap on the GPU (two host
+// threads, or two streams without ordering) race: serialise them.  The first call on a device
+// looks up the array's device address (cudaGetSymbolAddress) for that device; make that first
+// call before any stream capture.
+namespace {
+
+constexpr size_t NOALLOC_SCRATCH_BYTES = size_t(16) << 20;  // 16 MiB
+static __device__ __align__(256) unsigned char g_noalloc_scratch[NOALLOC_SCRATCH_BYTES];
+
+constexpr int NOALLOC_MAX_DEVICES = 64;
+void* g_noalloc_addr[NOALLOC_MAX_DEVICES] = {nullptr};
+
+__global__ void iota_kernel(int64_t n, int32_t* out) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        out[i] = (int32_t)i;
+}
+
+inline size_t up256(size_t b) { return (b + 255) & ~size_t(255); }
+
+struct NoallocLayout {
+    size_t status, tab, mat, coords, conn, sig, z, lam, el, fe, ke, total;
+};
+
+NoallocLayout noalloc_layout(int nn, int nd, int ng, int64_t ncell, bool want_f, bool want_k) {
+    const int nc = 2 * nd, npair = nn * (nn + 1) / 2;
+    const int64_t nip = ncell * ng;
+    NoallocLayout L;
+    size_t o = 0;
+    L.status = o; o += 256;
+    L.tab = o; o += up256(sizeof(double) * ((size_t)ng * nn * nd + ng));
+    L.mat = o; o += up256(sizeof(MatConst));
+    L.coords = o; o += up256(sizeof(double) * (size_t)ncell * nn * nd);
+    L.conn = o; o += up256(sizeof(int32_t) * (size_t)ncell * nn);
+    L.sig = o; o += up256(sizeof(double) * (size_t)nip * nc);
+    L.z = o; o += up256(sizeof(double) * (size_t)nip);
+    L.lam = o; o += up256(sizeof(double) * (size_t)nip);
+    L.el = o; o += up256((size_t)nip);
+    L.fe = o; o += want_f ? up256(sizeof(double) * (size_t)ncell * nn * nd) : 0;
+    L.ke = o; o += want_k ? up256(sizeof(double) * (size_t)ncell * npair * nd * nd) : 0;
+    L.total = o;
+    return L;
+}
+
+template <int ND, int NN>
+void noalloc_launch(const ElemArgs& a, bool dof, bool dok, int smem, cudaStream_t st) {
+    const unsigned blocks = (unsigned)((a.ncell + WPB - 1) / WPB);
+    if (dof && dok) element_kernel<ND, NN, UPD_NONE, true, true><<<blocks, WPB * 32, smem, st>>>(a);
+    else if (dof) element_kernel<ND, NN, UPD_NONE, true, false><<<blocks, WPB * 32, smem, st>>>(a);
+    else element_kernel<ND, NN, UPD_NONE, false, true><<<blocks, WPB * 32, smem, st>>>(a);
+}
+
+}  // namespace
+
+extern "C" int pms_element_calc_noalloc(int32_t kind, int32_t ngauss, double thickness, const pms_material* mat,
+                                        int64_t ncell, const double* X, const double* sig, const double* ivs,
+                                        const uint8_t* elastic, double* f, double* kk, int64_t* max_cells,
+                                        void* stream) {
+    if (kind < 0 || kind > 8 || !mat || ncell < 0 || (!f && !kk)) return PMS_ERR_INVALID;
+    if (mat->model != PMS_LINEAR_ELASTIC && mat->model != PMS_VON_MISES) return PMS_ERR_INVALID;
+    if (mat->model == PMS_VON_MISES && !(mat->z_ini > F_TOL)) return PMS_ERR_INVALID;
+    const int nn = kind_nnode(kind), nd = kind_ndim(kind), nc = 2 * nd, npair = nn * (nn + 1) / 2;
+    // integration rule and shape table on the stack (no heap): at most 27 x 20 x 3 + 27 doubles
+    double ksi_buf[27 * 3], w_buf[27];
+    const int ng = integration_rule_into(kind, ngauss, ksi_buf, w_buf);
+    if (ng <= 0 || ng > 27) return PMS_ERR_INVALID;
+    // largest batch that fits (binary search on the layout size)
+    {
+        int64_t lo = 0, hi = (int64_t)(NOALLOC_SCRATCH_BYTES / 64);
+        while (lo < hi) {
+            const int64_t mid = (lo + hi + 1) / 2;
+            if (noalloc_layout(nn, nd, ng, mid, f != nullptr, kk != nullptr).total <= NOALLOC_SCRATCH_BYTES)
+                lo = mid;
+            else
+                hi = mid - 1;
+        }
+        if (max_cells) *max_cells = lo;
+        if (ncell > lo) return PMS_ERR_TOO_LARGE;  // batch larger than the fixed scratch: split it
+    }
+    if (ncell == 0) return PMS_OK;
+    if (!X || !sig || !ivs || !elastic) return PMS_ERR_INVALID;
+    // device address of the scratch array, looked up once per device
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= NOALLOC_MAX_DEVICES) return PMS_ERR_CUDA;
+    if (!g_noalloc_addr[dev]) {
+        void* p = nullptr;
+        if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) return PMS_ERR_CUDA;
+        g_noalloc_addr[dev] = p;
+    }
+    unsigned char* base = (unsigned char*)g_noalloc_addr[dev];
+    cudaStream_t st = (cudaStream_t)stream;
+    const NoallocLayout L = noalloc_layout(nn, nd, ng, ncell, f != nullptr, kk != nullptr);
+    const int64_t nip = ncell * ng;
+    // shape table
+    double tab[27 * 20 * 3 + 27];
+    {
+        double N[20], dN[60];
+        for (int p = 0; p < ng; p++) {
+            shape_eval(kind, &ksi_buf[3 * p], N, dN);
+            for (int m = 0; m < nn; m++)
+                for (int j = 0; j < nd; j++) tab[(p * nn + m) * nd + j] = dN[m * nd + j];
+            tab[ng * nn * nd + p] = w_buf[p];
+        }
+    }
+    const MatConst mc = make_matconst(mat->model, mat->young, mat->poisson, mat->hh, mat->z_ini);
+    const int tab_len = ng * nn * nd + ng;
+    bool ok = cudaMemsetAsync(base + L.status, 0, 16, st) == cudaSuccess;  // status must start at zero
+    ok = ok && cudaMemcpyAsync(base + L.tab, tab, sizeof(double) * tab_len, cudaMemcpyHostToDevice, st) == cudaSuccess;
+    ok = ok && cudaMemcpyAsync(base + L.mat, &mc, sizeof(MatConst), cudaMemcpyHostToDevice, st) == cudaSuccess;
+    ok = ok && cudaMemcpyAsync(base + L.coords, X, sizeof(double) * (size_t)ncell * nn * nd, cudaMemcpyHostToDevice,
+                               st) == cudaSuccess;
+    ok = ok && cudaMemcpyAsync(base + L.sig, sig, sizeof(double) * (size_t)nip * nc, cudaMemcpyHostToDevice, st) ==
+                   cudaSuccess;
+    ok = ok && cudaMemcpyAsync(base + L.z, ivs, sizeof(double) * (size_t)nip, cudaMemcpyHostToDevice, st) ==
+                   cudaSuccess;
+    ok = ok && cudaMemcpyAsync(base + L.lam, ivs + nip, sizeof(double) * (size_t)nip, cudaMemcpyHostToDevice, st) ==
+                   cudaSuccess;
+    ok = ok && cudaMemcpyAsync(base + L.el, elastic, (size_t)nip, cudaMemcpyHostToDevice, st) == cudaSuccess;
+    if (!ok) return PMS_ERR_CUDA;
+    iota_kernel<<<(unsigned)std::min<int64_t>((ncell * nn + 255) / 256, 1024), 256, 0, st>>>(
+        ncell * nn, (int32_t*)(base + L.conn));
+    ElemArgs a;
+    a.ncell = ncell;
+    a.cell0 = 0;
+    a.nip = nip;
+    a.ngauss = ng;
+    a.thickness = thickness > 0 ? thickness : 1.0;
+    a.coords = (const double*)(base + L.coords);
+    a.conn = (const int32_t*)(base + L.conn);
+    a.cmat = nullptr;
+    a.mats = (const MatConst*)(base + L.mat);
+    a.ddu = nullptr;
+    a.tab = (const double*)(base + L.tab);
+    a.sig_src = nullptr;
+    a.z_src = nullptr;
+    a.lam_src = nullptr;
+    a.el_src = nullptr;
+    a.sig = (double*)(base + L.sig);
+    a.z = (double*)(base + L.z);
+    a.lam = (double*)(base + L.lam);
+    a.el = (uint8_t*)(base + L.el);
+    a.fe = (double*)(base + L.fe);
+    a.ke = (double*)(base + L.ke);
+    a.status = (int32_t*)(base + L.status);
+    const int smem = (((tab_len + 1) & ~1) + WPB * 2 * nn * 5 * nd) * (int)sizeof(double);
+    const bool dof = f != nullptr, dok = kk != nullptr;
+    switch (kind) {
+    case PMS_TRI3: noalloc_launch<2, 3>(a, dof, dok, smem, st); break;
+    case PMS_TRI6: noalloc_launch<2, 6>(a, dof, dok, smem, st); break;
+    case PMS_QUA4: noalloc_launch<2, 4>(a, dof, dok, smem, st); break;
+    case PMS_QUA8: noalloc_launch<2, 8>(a, dof, dok, smem, st); break;
+    case PMS_QUA9: noalloc_launch<2, 9>(a, dof, dok, smem, st); break;
+    case PMS_TET4: noalloc_launch<3, 4>(a, dof, dok, smem, st); break;
+    case PMS_TET10: noalloc_launch<3, 10>(a, dof, dok, smem, st); break;
+    case PMS_HEX8: noalloc_launch<3, 8>(a, dof, dok, smem, st); break;
+    case PMS_HEX20: noalloc_launch<3, 20>(a, dof, dok, smem, st); break;
+    }
+    if (cudaGetLastError() != cudaSuccess) return PMS_ERR_CUDA;
+    const int ne = nn * nd;
+    const size_t packed = (size_t)npair * nd * nd;  // doubles of one cell's upper node-pair blocks
+    if (dof && cudaMemcpyAsync(f, base + L.fe, sizeof(double) * (size_t)ncell * ne, cudaMemcpyDeviceToHost, st) !=
+                   cudaSuccess)
+        return PMS_ERR_CUDA;
+    // packed blocks land at the front of kk and are expanded in place below
+    if (dok && cudaMemcpyAsync(kk, base + L.ke, sizeof(double) * (size_t)ncell * packed, cudaMemcpyDeviceToHost,
+                               st) != cudaSuccess)
+        return PMS_ERR_CUDA;
+    int32_t hst[4] = {0, 0, 0, 0};
+    if (cudaMemcpyAsync(hst, base + L.status, 16, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+        cudaStreamSynchronize(st) != cudaSuccess)
+        return PMS_ERR_CUDA;
+    if (dok) {
+        // cell c's dense matrix starts at c*ne*ne >= c*packed, so going backwards never overwrites a
+        // packed cell that is still to be expanded; the cell's own blocks are copied aside first
+        double blk[210 * 9];
+        for (int64_t c = ncell - 1; c >= 0; c--) {
+            std::memcpy(blk, kk + (size_t)c * packed, sizeof(double) * packed);
+            double* K = kk + (size_t)c * ne * ne;
+            for (int p = 0; p < nn; p++)
+                for (int q = p; q < nn; q++) {
+                    const double* B = blk + (size_t)pair_index(nn, p, q) * nd * nd;
+                    for (int i = 0; i < nd; i++)
+                        for (int j = 0; j < nd; j++) {
+                            K[(p * nd + i) * ne + q * nd + j] = B[i * nd + j];
+                            K[(q * nd + j) * ne + p * nd + i] = B[i * nd + j];
+                        }
+                }
+        }
+    }
+    switch (hst[0]) {
+    case 0: return PMS_OK;
+    case E_ZERO_NORM_S: return PMS_ERR_ZERO_NORM_S;
+    case E_JACOBIAN: return PMS_ERR_JACOBIAN;
+    case E_ZERO_SIGMA_D: return PMS_ERR_ZERO_SIGMA_D;
+    default: return PMS_ERR_INVALID;
+    }
+}

@@ -100,6 +100,56 @@ int integration_rule(int kind, int ngauss, std::vector<double>& ksi, std::vector
     return -1;
 }
 
+int integration_rule_into(int kind, int ngauss, double* ksi, double* w) {
+    if (kind < 0 || kind > 8) return -1;
+    if (ngauss <= 0) ngauss = NGAUSS_DEFAULT[kind];
+    if (ngauss > 27) return -1;
+    const int nd = NDIM[kind];
+    for (int i = 0; i < 3 * ngauss; i++) ksi[i] = 0.0;
+    const bool simplex = (kind == 0 || kind == 1 || kind == 5 || kind == 6);
+    if (!simplex) {
+        int n1 = 0;
+        for (int c = 1; c <= 3; c++)
+            if ((nd == 2 ? c * c : c * c * c) == ngauss) n1 = c;
+        if (n1 == 0) return -1;
+        double x[3], ww[3];
+        gauss_legendre(n1, x, ww);
+        for (int p = 0; p < ngauss; p++) {
+            int i = p % n1, j = (p / n1) % n1, k = p / (n1 * n1);
+            ksi[3 * p] = x[i];
+            ksi[3 * p + 1] = x[j];
+            ksi[3 * p + 2] = nd == 3 ? x[k] : 0.0;
+            w[p] = ww[i] * ww[j] * (nd == 3 ? ww[k] : 1.0);
+        }
+        return ngauss;
+    }
+    if (ngauss == 1) {
+        ksi[0] = ksi[1] = (nd == 2) ? 1.0 / 3.0 : 0.25;
+        if (nd == 3) ksi[2] = 0.25;
+        w[0] = (nd == 2) ? 0.5 : 1.0 / 6.0;
+        return 1;
+    }
+    if (nd == 2 && ngauss == 3) {
+        const double lo = 1.0 / 6.0, hi = 2.0 / 3.0;
+        const double pts[3][2] = {{lo, lo}, {hi, lo}, {lo, hi}};
+        for (int p = 0; p < 3; p++) {
+            ksi[3 * p] = pts[p][0];
+            ksi[3 * p + 1] = pts[p][1];
+            w[p] = 1.0 / 6.0;
+        }
+        return 3;
+    }
+    if (nd == 3 && ngauss == 4) {
+        const double hi = (5.0 + 3.0 * std::sqrt(5.0)) / 20.0, lo = (5.0 - std::sqrt(5.0)) / 20.0;
+        for (int p = 0; p < 4; p++) {
+            for (int d = 0; d < 3; d++) ksi[3 * p + d] = (p > 0 && d == p - 1) ? hi : lo;
+            w[p] = 1.0 / 24.0;
+        }
+        return 4;
+    }
+    return -1;
+}
+
 void shape_eval(int kind, const double* k, double* N, double* dN) {
     const double r = k[0], s = k[1], t = k[2];
     switch (kind) {

@@ -20,6 +20,9 @@ int kind_default_ngauss(int kind);
 // Fills ksi[ngauss*3], w[ngauss].  Returns the number of points or -1.
 int integration_rule(int kind, int ngauss, std::vector<double>& ksi, std::vector<double>& w);
 
+// Same rules written into caller-provided arrays ksi[3*27], w[27] (no heap use).
+int integration_rule_into(int kind, int ngauss, double* ksi, double* w);
+
 // N[nn], dN[nn*nd] (dN_m/dksi_j) at one natural point.
 void shape_eval(int kind, const double* ksi, double* N, double* dN);
 
