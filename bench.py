@@ -12,7 +12,7 @@ Also measured in the same run: the stand-alone von Mises batch kernel on 16,777,
 (``k1_microbench``), the FP64 FMA peak of the GPU (``fp64_peak``), and the CPU restatement of
 the reference (oracle port, all host cores) on a bounded sample (``cpu_baseline``).
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference] [--small]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference] [--size small|medium|full]
 Multi-GPU (torchrun): every rank processes its own block (weak scaling, no data-path
 collective); the time is the max over ranks.
 """
@@ -42,7 +42,8 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--small", action="store_true", help="16x16x8 Hex20 block (profiling captures)")
+    ap.add_argument("--size", default="full", choices=["small", "medium", "full"],
+                    help="Hex20 block 16x16x8 / 32x32x16 (profiling captures) / 64x64x32")
     ap.add_argument("--no-k1", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
@@ -50,21 +51,21 @@ def parse():
     return ap.parse_args()
 
 
-def workload_dims(small):
-    return (16, 16, 8) if small else (64, 64, 32)
+def workload_dims(size):
+    return {"small": (16, 16, 8), "medium": (32, 32, 16), "full": (64, 64, 32)}[size]
 
 
-def make_problem(small):
+def make_problem(size):
     from pmsim_b200 import mesh as M
-    nx, ny, nz = workload_dims(small)
+    nx, ny, nz = workload_dims(size)
     m = M.structured_3d(M.HEX20, nx, ny, nz, float(nx), float(ny), float(nz))
     return m
 
 
-def synthetic_ddu(m, small, seed=20241203):
+def synthetic_ddu(m, size, seed=20241203):
     """Seeded mid-load increment of the footing indentation: the central quarter of the top face is
     pushed down (prescribed uz), decaying with depth and across the footing edge, plus noise."""
-    nx, ny, nz = workload_dims(small)
+    nx, ny, nz = workload_dims(size)
     x, y, z = m.coords[:, 0], m.coords[:, 1], m.coords[:, 2]
     cx, cy = nx / 2.0, ny / 2.0
     hx, hy = nx / 4.0, ny / 4.0
@@ -222,10 +223,10 @@ def reference_arm(args, rank):
     if rank != 0:
         return
     import oracle
-    m = make_problem(args.small)
-    ddu = synthetic_ddu(m, args.small)
+    m = make_problem(args.size)
+    ddu = synthetic_ddu(m, args.size)
     nthreads = oracle.lib().orc_max_threads()
-    ncs = args.cpu_cells or (512 if args.small else 4096)
+    ncs = args.cpu_cells or (512 if args.size == "small" else 4096)
     cpu_sample(m, ddu, min(ncs, 256), nthreads)  # warm-up (page-in, thread pool)
     tot, ips = 0.0, 0
     for _ in range(args.steps):
@@ -233,7 +234,7 @@ def reference_arm(args, rank):
         tot += dt
         ips += n
     value = ips / tot
-    nx, ny, nz = workload_dims(args.small)
+    nx, ny, nz = workload_dims(args.size)
     line = {
         "impl": "reference", "metric": "IP stress-update+tangent/s FP64", "value": value, "unit": "IP/s",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot / args.steps,
@@ -266,8 +267,8 @@ def main():
     dev = torch.device("cuda", local)
     stream = torch.cuda.Stream(device=dev)
 
-    m = make_problem(args.small)
-    ddu_h = synthetic_ddu(m, args.small, seed=20241203 + rank)
+    m = make_problem(args.size)
+    ddu_h = synthetic_ddu(m, args.size, seed=20241203 + rank)
     el = Elements(m, Material.von_mises(E, NU, HH, Z0))
     el.set_stream(stream)
     ng, nnz, ndof = el.ngauss, el.nnz, el.ndof
@@ -348,7 +349,7 @@ def main():
     peaks, peaks_kind = measured_peaks()
     fp64 = fp64_peak(torch, L, stream)
     k1 = None
-    if not args.no_k1 and not args.small:
+    if not args.no_k1 and args.size == "full":
         del d_csr
         torch.cuda.empty_cache()
         k1 = run_k1(torch, stream, max(3, args.steps), args.warmup)
@@ -364,14 +365,14 @@ def main():
     if not args.no_cpu:
         import oracle
         nthreads = oracle.lib().orc_max_threads()
-        ncs = args.cpu_cells or (512 if args.small else 4096)
+        ncs = args.cpu_cells or (512 if args.size == "small" else 4096)
         cpu_sample(m, ddu_h, 256, nthreads)
         dt, n = cpu_sample(m, ddu_h, ncs, nthreads)
         dt1, n1 = cpu_sample(m, ddu_h, max(ncs // 8, 64), 1)
         cpu = {"value": n / dt, "unit": "IP/s", "cores": nthreads, "kind": "port",
                "sample": f"first {ncs} cells ({n} IPs): update + F_int + K COO + CSR sum, all threads",
                "single_thread_ip_per_s": n1 / dt1}
-    nx, ny, nz = workload_dims(args.small)
+    nx, ny, nz = workload_dims(args.size)
     line = {
         "metric": "IP stress-update+tangent/s FP64",
         "value": value, "unit": "IP/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,

@@ -116,21 +116,50 @@ __device__ __forceinline__ double inv_jacobian(const double* J, double* Ji) {
     }
 }
 
+// Register tile of node pairs per lane: rows (a) x cols (b) of the upper node-pair triangle.
+// The tile shapes keep the number of tiles <= 32 (one tile per lane).
+template <int NN> struct TileShape {
+    static constexpr int RT = NN >= 16 ? 2 : 1;
+    static constexpr int CT = NN >= 16 ? 4 : (NN >= 7 ? 2 : 1);
+    static constexpr int NRG = (NN + RT - 1) / RT;
+    static constexpr int NCG = (NN + CT - 1) / CT;
+};
+
+// Shared memory (doubles): block-wide dN table [m][j][32] + w[32], then per warp
+// X[NN*ND], dU[NN*ND], G[ng][NN*ND+1] (gradients), TC[ng][10] (alpha, gamma, beta, S), CS[ng][6].
+__host__ __device__ constexpr int smem_table_doubles(int nn, int nd) { return nn * nd * 32 + 32; }
+__host__ __device__ constexpr int smem_warp_doubles(int nn, int nd, int ng) {
+    return 2 * nn * nd + ng * (nn * nd + 1) + ng * 10 + ng * 6;
+}
+__host__ __device__ constexpr int smem_bytes_for(int nn, int nd, int ng, int wpb) {
+    return (smem_table_doubles(nn, nd) + wpb * smem_warp_doubles(nn, nd, ng)) * 8;
+}
+
 template <int ND, int NN, int UPD, bool DOF, bool DOK>
 __global__ void __launch_bounds__(WPB * 32) element_kernel(ElemArgs A) {
     constexpr int NC = 2 * ND;
-    constexpr int NPAIR = NN * (NN + 1) / 2;
-    constexpr int P = (NPAIR + 31) / 32;  // pair slots per lane
-    constexpr int NODE_STRIDE = 5 * ND;   // per node in smem: Ag, Cg, Hh (scaled), g, h
+    constexpr int NE = NN * ND;
+    constexpr int GS = NE + 1;  // gradient row stride (odd: spreads the banks of phase-1 stores)
+    using TS = TileShape<NN>;
+    constexpr int RT = TS::RT, CT = TS::CT;
     extern __shared__ double smem[];
     const int ng = A.ngauss;
-    double* tab = smem;                                   // ng*NN*ND + ng
-    const int tab_len = ng * NN * ND + ng;
-    const int tab_pad = (tab_len + 1) & ~1;
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    double* nbuf = smem + tab_pad + wid * 2 * NN * NODE_STRIDE;  // double buffer per warp
+    double* dNs = smem;                        // [m][j][32]
+    double* ws = smem + NE * 32;               // [32]
+    double* wbase = smem + smem_table_doubles(NN, ND) + wid * smem_warp_doubles(NN, ND, ng);
+    double* Xs = wbase;                        // [m][d]
+    double* Us = Xs + NE;                      // [m][d]
+    double* G = Us + NE;                       // [p][GS]
+    double* TC = G + ng * GS;                  // [p][10]
+    double* CS = TC + ng * 10;                 // [p][6]
 
-    for (int i = threadIdx.x; i < tab_len; i += blockDim.x) tab[i] = A.tab[i];
+    // stage dN transposed (IP index fastest) so that lane p reads its IP without bank conflicts
+    for (int i = threadIdx.x; i < ng * NE; i += blockDim.x) {
+        const int p = i / NE, r = i % NE;
+        dNs[r * 32 + p] = A.tab[i];
+    }
+    for (int i = threadIdx.x; i < ng; i += blockDim.x) ws[i] = A.tab[ng * NE + i];
     __syncthreads();
 
     const int64_t cl = (int64_t)blockIdx.x * WPB + wid;
@@ -138,229 +167,255 @@ __global__ void __launch_bounds__(WPB * 32) element_kernel(ElemArgs A) {
     const int64_t cell = A.cell0 + cl;
     const MatConst mc = A.mats[A.cmat ? A.cmat[cell] : 0];
 
-    // node data (lane m < NN)
-    double X[ND], du[ND];
-#pragma unroll
-    for (int i = 0; i < ND; i++) { X[i] = 0.0; du[i] = 0.0; }
     if (lane < NN) {
         const int pt = A.conn[cell * NN + lane];
 #pragma unroll
         for (int i = 0; i < ND; i++) {
-            X[i] = A.coords[(int64_t)pt * ND + i];
-            if (UPD != UPD_NONE) du[i] = A.ddu[(int64_t)pt * ND + i];
+            Xs[lane * ND + i] = A.coords[(int64_t)pt * ND + i];
+            Us[lane * ND + i] = (UPD != UPD_NONE) ? A.ddu[(int64_t)pt * ND + i] : 0.0;
         }
     }
-    // IP state (lane p < ng)
+    __syncwarp();
+
+    // ---------------- phase 1: lane p owns integration point p ----------------
     const int64_t ip0 = cell * ng;
-    double st_sig[NC], st_z = 0.0, st_lam = 0.0;
-    int st_el = 1;
+    int err = OK;
+    const bool has_ip = lane < ng;
+    double sig[NC], z = 0.0, lam = 0.0;
+    int el = 1;
 #pragma unroll
-    for (int c = 0; c < NC; c++) st_sig[c] = 0.0;
-    if (lane < ng) {
+    for (int c = 0; c < NC; c++) sig[c] = 0.0;
+    if (has_ip) {
         const double* ssrc = (UPD == UPD_BACKUP) ? A.sig_src : A.sig;
         const double* zsrc = (UPD == UPD_BACKUP) ? A.z_src : A.z;
         const double* lsrc = (UPD == UPD_BACKUP) ? A.lam_src : A.lam;
         const uint8_t* esrc = (UPD == UPD_BACKUP) ? A.el_src : A.el;
 #pragma unroll
-        for (int c = 0; c < NC; c++) st_sig[c] = ssrc[(int64_t)c * A.nip + ip0 + lane];
-        st_z = zsrc[ip0 + lane];
-        st_lam = lsrc[ip0 + lane];
-        st_el = esrc[ip0 + lane];
-    }
-
-    // pair slots of this lane: q = lane + 32*k
-    int pa[P], pb[P];
+        for (int c = 0; c < NC; c++) sig[c] = ssrc[(int64_t)c * A.nip + ip0 + lane];
+        z = zsrc[ip0 + lane];
+        lam = lsrc[ip0 + lane];
+        el = esrc[ip0 + lane];
+        const int p = lane;
+        double J[ND * ND];
 #pragma unroll
-    for (int k = 0; k < P; k++) {
-        int q = lane + 32 * k;
-        int a = 0;
-        if (q < NPAIR) {
-            while (q >= (a + 1) * NN - (a + 1) * a / 2) a++;
-            pa[k] = a;
-            pb[k] = a + (q - (a * NN - a * (a - 1) / 2));
-        } else {
-            pa[k] = -1;
-            pb[k] = -1;
-        }
-    }
-    double acc[DOK ? P : 1][ND][ND];
+        for (int k = 0; k < ND * ND; k++) J[k] = 0.0;
 #pragma unroll
-    for (int k = 0; k < (DOK ? P : 1); k++)
+        for (int m = 0; m < NN; m++)
 #pragma unroll
-        for (int i = 0; i < ND; i++)
+            for (int i = 0; i < ND; i++)
 #pragma unroll
-            for (int j = 0; j < ND; j++) acc[k][i][j] = 0.0;
-    double f[ND];
-#pragma unroll
-    for (int i = 0; i < ND; i++) f[i] = 0.0;
-    int err = OK, err_ip = -1;
-
-    for (int p = 0; p < ng; p++) {
-        const double* dN = tab + (p * NN + (lane < NN ? lane : 0)) * ND;
-        const double wp = tab[ng * NN * ND + p];
-        // Jacobian J[i][j] = sum_m X_m[i] dN_m[j]
-        double J[ND * ND], Ji[ND * ND];
-#pragma unroll
-        for (int i = 0; i < ND; i++)
-#pragma unroll
-            for (int j = 0; j < ND; j++) J[i * ND + j] = warp_sum(lane < NN ? X[i] * dN[j] : 0.0);
+                for (int j = 0; j < ND; j++) J[i * ND + j] = fma(Xs[m * ND + i], dNs[(m * ND + j) * 32 + p], J[i * ND + j]);
+        double Ji[ND * ND];
         const double det = inv_jacobian<ND>(J, Ji);
-        if (!(det > 0.0) && err == OK) { err = E_JACOBIAN; err_ip = p; }
-        // gradient g_m = J^-T dN_m
-        double g[ND];
+        if (!(det > 0.0)) err = E_JACOBIAN;
+        const double coef = det * ws[p] * A.thickness;
+        double eps[NC];
 #pragma unroll
-        for (int i = 0; i < ND; i++) {
-            double v = 0.0;
+        for (int c = 0; c < NC; c++) eps[c] = 0.0;
+        double* Gp = G + p * GS;
 #pragma unroll
-            for (int j = 0; j < ND; j++) v += dN[j] * Ji[j * ND + i];
-            g[i] = (lane < NN) ? v : 0.0;
-        }
-        const double coef = det * wp * A.thickness;
-        // state of IP p
-        double sig[NC], z, lam;
-        int el;
-#pragma unroll
-        for (int c = 0; c < NC; c++) sig[c] = __shfl_sync(FULL, st_sig[c], p);
-        z = __shfl_sync(FULL, st_z, p);
-        lam = __shfl_sync(FULL, st_lam, p);
-        el = __shfl_sync(FULL, st_el, p);
-        if (UPD != UPD_NONE) {
-            // strain increment (Mandel) = sum_m sym(g_m (x) du_m)
-            double eps[NC];
-            eps[0] = warp_sum(du[0] * g[0]);
-            eps[1] = warp_sum(du[1] * g[1]);
-            if constexpr (ND == 2) {
-                eps[2] = 0.0;
-                eps[3] = warp_sum(SQRT2 * ((du[0] * g[1] + du[1] * g[0]) / 2.0));
-            } else {
-                eps[2] = warp_sum(du[ND - 1] * g[ND - 1]);
-                eps[3] = warp_sum(SQRT2 * ((du[0] * g[1] + du[1] * g[0]) / 2.0));
-                eps[4 % NC] = warp_sum(SQRT2 * ((du[1] * g[ND - 1] + du[ND - 1] * g[1]) / 2.0));
-                eps[5 % NC] = warp_sum(SQRT2 * ((du[0] * g[ND - 1] + du[ND - 1] * g[0]) / 2.0));
-            }
-            const double hh = mc.hh;
-            int st = ip_update<NC>(mc, hh, sig, z, lam, el, eps);
-            if (st != OK && err == OK) { err = st; err_ip = p; }
-            if (lane == p) {
-#pragma unroll
-                for (int c = 0; c < NC; c++) st_sig[c] = sig[c];
-                st_z = z;
-                st_lam = lam;
-                st_el = el;
-            }
-        }
-        if (DOF) {
-            // f_m[i] += coef * sum_j sigma_ij g_m[j]
-            double S[ND][ND];
-            S[0][0] = sig[0];
-            S[1][1] = sig[1];
-            S[0][1] = S[1][0] = sig[3] * INV_SQRT2;
-            if constexpr (ND == 3) {
-                S[ND - 1][ND - 1] = sig[2];
-                S[1][ND - 1] = S[ND - 1][1] = sig[4 % NC] * INV_SQRT2;
-                S[0][ND - 1] = S[ND - 1][0] = sig[5 % NC] * INV_SQRT2;
-            }
+        for (int m = 0; m < NN; m++) {
+            double g[ND];
 #pragma unroll
             for (int i = 0; i < ND; i++) {
                 double v = 0.0;
 #pragma unroll
-                for (int j = 0; j < ND; j++) v += S[i][j] * g[j];
-                f[i] += coef * v;
+                for (int j = 0; j < ND; j++) v = fma(dNs[(m * ND + j) * 32 + p], Ji[j * ND + i], v);
+                g[i] = v;
+                Gp[m * ND + i] = v;
+            }
+            if (UPD != UPD_NONE) {
+                const double* u = Us + m * ND;
+                eps[0] += u[0] * g[0];
+                eps[1] += u[1] * g[1];
+                if constexpr (ND == 2) {
+                    eps[3] += SQRT2 * ((u[0] * g[1] + u[1] * g[0]) / 2.0);
+                } else {
+                    eps[2] += u[2] * g[2];
+                    eps[3] += SQRT2 * ((u[0] * g[1] + u[1] * g[0]) / 2.0);
+                    eps[4 % NC] += SQRT2 * ((u[1] * g[2 % ND] + u[2 % ND] * g[1]) / 2.0);
+                    eps[5 % NC] += SQRT2 * ((u[0] * g[2 % ND] + u[2 % ND] * g[0]) / 2.0);
+                }
+            }
+        }
+        if (UPD != UPD_NONE) {
+            const int st = ip_update<NC>(mc, mc.hh, sig, z, lam, el, eps);
+            if (st != OK && err == OK) err = st;
+        }
+        if (DOF) {  // coef * sigma as a symmetric ND x ND tensor: xx, yy, xy (, zz, yz, xz)
+            double* c6 = CS + p * 6;
+            c6[0] = coef * sig[0];
+            c6[1] = coef * sig[1];
+            c6[2] = coef * sig[3] * INV_SQRT2;
+            if constexpr (ND == 3) {
+                c6[3] = coef * sig[2];
+                c6[4] = coef * sig[4 % NC] * INV_SQRT2;
+                c6[5] = coef * sig[5 % NC] * INV_SQRT2;
             }
         }
         if (DOK) {
             double a, b, s[NC];
-            int st = tangent_coefs<NC>(mc, mc.hh, sig, lam, el, a, b, s);
-            if (st != OK && err == OK) { err = st; err_ip = p; }
-            const double al = coef * 0.5 * a, ga = coef * (mc.kk - a / 3.0), be = coef * b;
-            double Sd[ND][ND];
-            Sd[0][0] = s[0];
-            Sd[1][1] = s[1];
-            Sd[0][1] = Sd[1][0] = s[3] * INV_SQRT2;
+            const int st = tangent_coefs<NC>(mc, mc.hh, sig, lam, el, a, b, s);
+            if (st != OK && err == OK) err = st;
+            double* t = TC + p * 10;
+            t[0] = coef * 0.5 * a;
+            t[1] = coef * (mc.kk - a / 3.0);
+            t[2] = coef * b;
+            t[3] = s[0];
+            t[4] = s[1];
+            t[5] = s[3] * INV_SQRT2;
             if constexpr (ND == 3) {
-                Sd[ND - 1][ND - 1] = s[2];
-                Sd[1][ND - 1] = Sd[ND - 1][1] = s[4 % NC] * INV_SQRT2;
-                Sd[0][ND - 1] = Sd[ND - 1][0] = s[5 % NC] * INV_SQRT2;
+                t[6] = s[2];
+                t[7] = s[4 % NC] * INV_SQRT2;
+                t[8] = s[5 % NC] * INV_SQRT2;
             }
-            double* buf = nbuf + (p & 1) * NN * NODE_STRIDE;
-            if (lane < NN) {
-                double h[ND];
-#pragma unroll
-                for (int i = 0; i < ND; i++) {
-                    double v = 0.0;
-#pragma unroll
-                    for (int j = 0; j < ND; j++) v += Sd[i][j] * g[j];
-                    h[i] = v;
-                }
-                double* nb = buf + lane * NODE_STRIDE;
-#pragma unroll
-                for (int i = 0; i < ND; i++) {
-                    nb[i] = al * g[i];
-                    nb[ND + i] = ga * g[i];
-                    nb[2 * ND + i] = be * h[i];
-                    nb[3 * ND + i] = g[i];
-                    nb[4 * ND + i] = h[i];
-                }
-            }
-            __syncwarp();
-#pragma unroll
-            for (int k = 0; k < P; k++) {
-                if (pa[k] >= 0) {
-                    const double* ra = buf + pa[k] * NODE_STRIDE;
-                    const double* cb = buf + pb[k] * NODE_STRIDE;
-                    double Aa[ND], Ca[ND], Ha[ND], gb[ND], hb[ND];
-#pragma unroll
-                    for (int i = 0; i < ND; i++) {
-                        Aa[i] = ra[i];
-                        Ca[i] = ra[ND + i];
-                        Ha[i] = ra[2 * ND + i];
-                        gb[i] = cb[3 * ND + i];
-                        hb[i] = cb[4 * ND + i];
-                    }
-                    double dot = 0.0;
-#pragma unroll
-                    for (int i = 0; i < ND; i++) dot += Aa[i] * gb[i];
-#pragma unroll
-                    for (int i = 0; i < ND; i++)
-#pragma unroll
-                        for (int j = 0; j < ND; j++) {
-                            double v = acc[k][i][j];
-                            v = fma(Aa[j], gb[i], v);
-                            v = fma(Ca[i], gb[j], v);
-                            v = fma(Ha[i], hb[j], v);
-                            if (i == j) v += dot;
-                            acc[k][i][j] = v;
-                        }
-                }
-            }
-            // the other buffer is rewritten at p+1; p+2 reuses this one after a full pair pass,
-            // which every lane finishes before reaching the __syncwarp of p+1
         }
     }
-
-    if (lane == 0 && err != OK) report(A.status, err, cell, err_ip);
-    if (UPD != UPD_NONE && lane < ng) {
-#pragma unroll
-        for (int c = 0; c < NC; c++) A.sig[(int64_t)c * A.nip + ip0 + lane] = st_sig[c];
-        A.z[ip0 + lane] = st_z;
-        A.lam[ip0 + lane] = st_lam;
-        A.el[ip0 + lane] = (uint8_t)st_el;
+    // first failing IP of the cell (lowest p) reports
+    {
+        const unsigned bad = __ballot_sync(FULL, err != OK);
+        if (bad) {
+            const int p = __ffs(bad) - 1;
+            const int code = __shfl_sync(FULL, err, p);
+            if (lane == 0) report(A.status, code, cell, p);
+        }
     }
+    if (UPD != UPD_NONE && has_ip) {
+#pragma unroll
+        for (int c = 0; c < NC; c++) A.sig[(int64_t)c * A.nip + ip0 + lane] = sig[c];
+        A.z[ip0 + lane] = z;
+        A.lam[ip0 + lane] = lam;
+        A.el[ip0 + lane] = (uint8_t)el;
+    }
+    __syncwarp();
+
+    // ---------------- F_int: lane m owns node m ----------------
     if (DOF && lane < NN) {
+        double f[ND];
+#pragma unroll
+        for (int i = 0; i < ND; i++) f[i] = 0.0;
+        for (int p = 0; p < ng; p++) {
+            const double* c6 = CS + p * 6;
+            const double* g = G + p * GS + lane * ND;
+            if constexpr (ND == 2) {
+                f[0] += c6[0] * g[0] + c6[2] * g[1];
+                f[1] += c6[2] * g[0] + c6[1] * g[1];
+            } else {
+                f[0] += c6[0] * g[0] + c6[2] * g[1] + c6[5 % 6] * g[2 % ND];
+                f[1] += c6[2] * g[0] + c6[1] * g[1] + c6[4 % 6] * g[2 % ND];
+                f[2 % ND] += c6[5 % 6] * g[0] + c6[4 % 6] * g[1] + c6[3 % 6] * g[2 % ND];
+            }
+        }
 #pragma unroll
         for (int i = 0; i < ND; i++) A.fe[(cell * NN + lane) * ND + i] = f[i];
     }
+
+    // ---------------- phase 2: lane owns a tile of node-pair blocks ----------------
     if (DOK) {
+        // the lane-th tile (i, j) with i*RT <= min(j*CT + CT - 1, NN - 1), row-major
+        int ti = -1, tj = -1;
+        {
+            int k = 0;
+            for (int i = 0; i < TS::NRG; i++)
+                for (int j = 0; j < TS::NCG; j++) {
+                    const int jmax = min(j * CT + CT - 1, NN - 1);
+                    if (i * RT <= jmax) {
+                        if (k == lane) { ti = i; tj = j; }
+                        k++;
+                    }
+                }
+        }
+        if (ti >= 0) {
+            const int a0 = ti * RT, b0 = tj * CT;
+            double acc[RT][CT][ND][ND];
 #pragma unroll
-        for (int k = 0; k < P; k++) {
-            if (pa[k] >= 0) {
-                const int q = lane + 32 * k;
-                double* dst = A.ke + (cell * NPAIR + q) * (ND * ND);
+            for (int r = 0; r < RT; r++)
 #pragma unroll
-                for (int i = 0; i < ND; i++)
+                for (int c = 0; c < CT; c++)
 #pragma unroll
-                    for (int j = 0; j < ND; j++) dst[i * ND + j] = acc[k][i][j];
+                    for (int i = 0; i < ND; i++)
+#pragma unroll
+                        for (int j = 0; j < ND; j++) acc[r][c][i][j] = 0.0;
+            for (int p = 0; p < ng; p++) {
+                const double* t = TC + p * 10;
+                const double al = t[0], ga = t[1], be = t[2];
+                double S[ND][ND];
+                S[0][0] = t[3];
+                S[1][1] = t[4];
+                S[0][1] = S[1][0] = t[5];
+                if constexpr (ND == 3) {
+                    S[2 % ND][2 % ND] = t[6];
+                    S[1][2 % ND] = S[2 % ND][1] = t[7];
+                    S[0][2 % ND] = S[2 % ND][0] = t[8];
+                }
+                const bool plastic = be != 0.0;  // same value on every lane: uniform branch
+                const double* Gp = G + p * GS;
+                double Ar[RT][ND], Cr[RT][ND], Hr[RT][ND];
+#pragma unroll
+                for (int r = 0; r < RT; r++) {
+                    const int a = min(a0 + r, NN - 1);
+                    double g[ND];
+#pragma unroll
+                    for (int i = 0; i < ND; i++) g[i] = Gp[a * ND + i];
+#pragma unroll
+                    for (int i = 0; i < ND; i++) {
+                        Ar[r][i] = al * g[i];
+                        Cr[r][i] = ga * g[i];
+                        double h = 0.0;
+                        if (plastic) {
+#pragma unroll
+                            for (int j = 0; j < ND; j++) h = fma(S[i][j], g[j], h);
+                        }
+                        Hr[r][i] = be * h;
+                    }
+                }
+#pragma unroll
+                for (int c = 0; c < CT; c++) {
+                    const int b = min(b0 + c, NN - 1);
+                    double gb[ND], hb[ND];
+#pragma unroll
+                    for (int i = 0; i < ND; i++) gb[i] = Gp[b * ND + i];
+                    if (plastic) {
+#pragma unroll
+                        for (int i = 0; i < ND; i++) {
+                            double h = 0.0;
+#pragma unroll
+                            for (int j = 0; j < ND; j++) h = fma(S[i][j], gb[j], h);
+                            hb[i] = h;
+                        }
+                    }
+#pragma unroll
+                    for (int r = 0; r < RT; r++) {
+                        double dot = 0.0;
+#pragma unroll
+                        for (int k = 0; k < ND; k++) dot = fma(Ar[r][k], gb[k], dot);
+#pragma unroll
+                        for (int i = 0; i < ND; i++)
+#pragma unroll
+                            for (int j = 0; j < ND; j++) {
+                                double v = acc[r][c][i][j];
+                                v = fma(Ar[r][j], gb[i], v);
+                                v = fma(Cr[r][i], gb[j], v);
+                                if (plastic) v = fma(Hr[r][i], hb[j], v);
+                                if (i == j) v += dot;
+                                acc[r][c][i][j] = v;
+                            }
+                    }
+                }
             }
+#pragma unroll
+            for (int r = 0; r < RT; r++)
+#pragma unroll
+                for (int c = 0; c < CT; c++) {
+                    const int a = a0 + r, b = b0 + c;
+                    if (a < NN && b < NN && a <= b) {
+                        double* dst = A.ke + (cell * (NN * (NN + 1) / 2) + (a * NN - a * (a - 1) / 2 + (b - a))) * (ND * ND);
+#pragma unroll
+                        for (int i = 0; i < ND; i++)
+#pragma unroll
+                            for (int j = 0; j < ND; j++) dst[i * ND + j] = acc[r][c][i][j];
+                    }
+                }
         }
     }
 }
@@ -729,8 +784,7 @@ int pms_elements_create(const pms_mesh* mesh, const pms_material* materials, int
         return PMS_ERR_CUDA;
     }
     h->stream = h->own_stream;
-    int tab_len = h->ng * h->nn * h->nd + h->ng;
-    h->smem_bytes = (((tab_len + 1) & ~1) + WPB * 2 * h->nn * 5 * h->nd) * (int)sizeof(double);
+    h->smem_bytes = smem_bytes_for(h->nn, h->nd, h->ng, WPB);
     // the state starts as LocalState::new: zero stress, elastic, zero internal variables
     init_state_kernel<<<grid_1d(h->nip), 256, 0, h->stream>>>(h->nip, h->nc, h->d_mats, h->d_cmat, h->ng, h->d_sig,
                                                               h->d_z, h->d_lam, h->d_el);
@@ -1125,12 +1179,18 @@ NoallocLayout noalloc_layout(int nn, int nd, int ng, int64_t ncell, bool want_f,
     return L;
 }
 
+template <int ND, int NN, bool DOF, bool DOK>
+void noalloc_launch_t(const ElemArgs& a, int smem, cudaStream_t st) {
+    auto kern = element_kernel<ND, NN, UPD_NONE, DOF, DOK>;
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
+    kern<<<(unsigned)((a.ncell + WPB - 1) / WPB), WPB * 32, smem, st>>>(a);
+}
+
 template <int ND, int NN>
 void noalloc_launch(const ElemArgs& a, bool dof, bool dok, int smem, cudaStream_t st) {
-    const unsigned blocks = (unsigned)((a.ncell + WPB - 1) / WPB);
-    if (dof && dok) element_kernel<ND, NN, UPD_NONE, true, true><<<blocks, WPB * 32, smem, st>>>(a);
-    else if (dof) element_kernel<ND, NN, UPD_NONE, true, false><<<blocks, WPB * 32, smem, st>>>(a);
-    else element_kernel<ND, NN, UPD_NONE, false, true><<<blocks, WPB * 32, smem, st>>>(a);
+    if (dof && dok) noalloc_launch_t<ND, NN, true, true>(a, smem, st);
+    else if (dof) noalloc_launch_t<ND, NN, true, false>(a, smem, st);
+    else noalloc_launch_t<ND, NN, false, true>(a, smem, st);
 }
 
 }  // namespace
@@ -1225,7 +1285,7 @@ extern "C" int pms_element_calc_noalloc(int32_t kind, int32_t ngauss, double thi
     a.fe = (double*)(base + L.fe);
     a.ke = (double*)(base + L.ke);
     a.status = (int32_t*)(base + L.status);
-    const int smem = (((tab_len + 1) & ~1) + WPB * 2 * nn * 5 * nd) * (int)sizeof(double);
+    const int smem = smem_bytes_for(nn, nd, ng, WPB);
     const bool dof = f != nullptr, dok = kk != nullptr;
     switch (kind) {
     case PMS_TRI3: noalloc_launch<2, 3>(a, dof, dok, smem, st); break;
