@@ -27,8 +27,8 @@
 // dN (9), h = S g (9), three scaled copies (9).
 //
 // Assembly: element blocks go to a scratch buffer ke[cell][pair][nd*nd]; kk_gather_kernel owns
-// each node-pair block (A <= B) with one thread, sums its contributions in ascending cell order
-// and writes K_AB and K_BA.  No atomics: bit-identical on every run.
+// each node-pair block (A <= B) with one lane (one warp per block row), sums its contributions
+// in ascending cell order and writes K_AB and K_BA.  No atomics: bit-identical on every run.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -420,50 +420,73 @@ __global__ void __launch_bounds__(WPB * 32) element_kernel(ElemArgs A) {
     }
 }
 
-// One thread per node-pair block (A <= B): fixed-order sum of the element blocks, written to
-// both (A, B) and (B, A) positions of the scalar CSR.
+// One warp per block row A, one lane per upper block (A, B >= A) of that row: fixed-order sum of
+// its element blocks (ascending cell), written to (A, B) -- consecutive lanes write consecutive
+// blocks of the row -- and, transposed, to (B, A).
 template <int ND>
-__global__ void __launch_bounds__(256) kk_gather_kernel(int64_t nupper, const int32_t* __restrict__ u_row,
-                                                        const int32_t* __restrict__ u_col,
-                                                        const int32_t* __restrict__ u_kab,
+__global__ void __launch_bounds__(256) kk_gather_kernel(int64_t npoint, const int64_t* __restrict__ uptr,
+                                                        const int32_t* __restrict__ kdiag,
+                                                        const int64_t* __restrict__ bptr,
+                                                        const int32_t* __restrict__ bcol,
                                                         const int32_t* __restrict__ u_kba,
                                                         const int64_t* __restrict__ u_cptr,
                                                         const int32_t* __restrict__ u_contrib,
-                                                        const int64_t* __restrict__ bptr,
                                                         const double* __restrict__ ke, double* __restrict__ csr) {
-    for (int64_t u = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; u < nupper;
-         u += (int64_t)gridDim.x * blockDim.x) {
-        double s[ND * ND];
-#pragma unroll
-        for (int i = 0; i < ND * ND; i++) s[i] = 0.0;
-        const int64_t c0 = u_cptr[u], c1 = u_cptr[u + 1];
-        for (int64_t c = c0; c < c1; c++) {
-            const uint32_t code = (uint32_t)u_contrib[c];
-            const double* blk = ke + (int64_t)(code & 0x7fffffffu) * (ND * ND);
-            if (code & 0x80000000u) {
-#pragma unroll
-                for (int i = 0; i < ND; i++)
-#pragma unroll
-                    for (int j = 0; j < ND; j++) s[i * ND + j] += blk[j * ND + i];
-            } else {
-#pragma unroll
-                for (int i = 0; i < ND * ND; i++) s[i] += blk[i];
-            }
-        }
-        const int32_t Ar = u_row[u], Bc = u_col[u];
+    const int lane = threadIdx.x & 31;
+    const int64_t nwarp = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t Ar = (((int64_t)blockIdx.x * blockDim.x) + threadIdx.x) >> 5; Ar < npoint; Ar += nwarp) {
+        const int64_t u0 = uptr[Ar], nu = uptr[Ar + 1] - u0;
         const int64_t ba = bptr[Ar], nba = bptr[Ar + 1] - ba;
-        const int64_t posAB = (int64_t)ND * ND * ba + (int64_t)u_kab[u] * ND;
+        const int kd = kdiag[Ar];
+        for (int64_t t = lane; t < nu; t += 32) {
+            const int64_t u = u0 + t;
+            const int64_t kab = kd + t;
+            const int32_t Bc = bcol[ba + kab];
+            double s[ND * ND];
 #pragma unroll
-        for (int i = 0; i < ND; i++)
+            for (int i = 0; i < ND * ND; i++) s[i] = 0.0;
+            const int64_t c0 = u_cptr[u], c1 = u_cptr[u + 1];
+            // batches of GB contributions: all codes, then all blocks in flight, then the ordered sum
+            constexpr int GB = 4;
+            for (int64_t cb = c0; cb < c1; cb += GB) {
+                uint32_t code[GB];
 #pragma unroll
-            for (int j = 0; j < ND; j++) csr[posAB + i * ND * nba + j] = s[i * ND + j];
-        if (Bc != Ar) {
-            const int64_t bb = bptr[Bc], nbb = bptr[Bc + 1] - bb;
-            const int64_t posBA = (int64_t)ND * ND * bb + (int64_t)u_kba[u] * ND;
+                for (int k = 0; k < GB; k++) code[k] = (cb + k < c1) ? (uint32_t)__ldg(u_contrib + cb + k) : 0u;
+                double v[GB][ND * ND];
+#pragma unroll
+                for (int k = 0; k < GB; k++) {
+                    const double* blk = ke + (int64_t)(code[k] & 0x7fffffffu) * (ND * ND);
+#pragma unroll
+                    for (int i = 0; i < ND * ND; i++) v[k][i] = (cb + k < c1) ? __ldg(blk + i) : 0.0;
+                }
+#pragma unroll
+                for (int k = 0; k < GB; k++) {
+                    if (cb + k < c1) {
+                        if (code[k] & 0x80000000u) {
+#pragma unroll
+                            for (int i = 0; i < ND; i++)
+#pragma unroll
+                                for (int j = 0; j < ND; j++) s[i * ND + j] += v[k][j * ND + i];
+                        } else {
+#pragma unroll
+                            for (int i = 0; i < ND * ND; i++) s[i] += v[k][i];
+                        }
+                    }
+                }
+            }
+            const int64_t posAB = (int64_t)ND * ND * ba + kab * ND;
 #pragma unroll
             for (int i = 0; i < ND; i++)
 #pragma unroll
-                for (int j = 0; j < ND; j++) csr[posBA + j * ND * nbb + i] = s[i * ND + j];
+                for (int j = 0; j < ND; j++) csr[posAB + i * ND * nba + j] = s[i * ND + j];
+            if (Bc != Ar) {
+                const int64_t bb = bptr[Bc], nbb = bptr[Bc + 1] - bb;
+                const int64_t posBA = (int64_t)ND * ND * bb + (int64_t)u_kba[u] * ND;
+#pragma unroll
+                for (int i = 0; i < ND; i++)
+#pragma unroll
+                    for (int j = 0; j < ND; j++) csr[posBA + j * ND * nbb + i] = s[i * ND + j];
+            }
         }
     }
 }
@@ -529,7 +552,9 @@ struct pms_elements {
     int64_t* d_inc_ptr = nullptr;
     int32_t* d_inc = nullptr;
     int64_t* d_bptr = nullptr;
-    int32_t *d_urow = nullptr, *d_ucol = nullptr, *d_ukab = nullptr, *d_ukba = nullptr, *d_ucontrib = nullptr;
+    int32_t* d_bcol = nullptr;
+    int64_t* d_uptr = nullptr;
+    int32_t *d_kdiag = nullptr, *d_ukba = nullptr, *d_ucontrib = nullptr;
     int64_t* d_ucptr = nullptr;
     double *d_ddu = nullptr, *d_ff = nullptr, *d_csr = nullptr;  // staging for host-memory calls
     int32_t* d_status = nullptr;
@@ -674,13 +699,14 @@ ElemArgs make_args(pms_elements* h, const double* ddu) {
 }
 
 void launch_kk_gather(pms_elements* h, double* csr) {
-    int64_t nu = h->pat.nupper();
+    const int64_t np = h->npoint;
+    const int blocks = (int)std::min<int64_t>((np + 7) / 8, 148 * 32);  // 8 warps (rows) per block
     if (h->nd == 2)
-        kk_gather_kernel<2><<<grid_1d(nu), 256, 0, h->stream>>>(nu, h->d_urow, h->d_ucol, h->d_ukab, h->d_ukba,
-                                                                 h->d_ucptr, h->d_ucontrib, h->d_bptr, h->d_ke, csr);
+        kk_gather_kernel<2><<<blocks, 256, 0, h->stream>>>(np, h->d_uptr, h->d_kdiag, h->d_bptr, h->d_bcol, h->d_ukba,
+                                                            h->d_ucptr, h->d_ucontrib, h->d_ke, csr);
     else
-        kk_gather_kernel<3><<<grid_1d(nu), 256, 0, h->stream>>>(nu, h->d_urow, h->d_ucol, h->d_ukab, h->d_ukba,
-                                                                 h->d_ucptr, h->d_ucontrib, h->d_bptr, h->d_ke, csr);
+        kk_gather_kernel<3><<<blocks, 256, 0, h->stream>>>(np, h->d_uptr, h->d_kdiag, h->d_bptr, h->d_bcol, h->d_ukba,
+                                                            h->d_ucptr, h->d_ucontrib, h->d_ke, csr);
     h->launches++;
 }
 
@@ -767,9 +793,9 @@ int pms_elements_create(const pms_mesh* mesh, const pms_material* materials, int
          h->upload(&h->d_inc_ptr, h->pat.inc_ptr.data(), h->pat.inc_ptr.size()) &&
          h->upload(&h->d_inc, h->pat.inc.data(), h->pat.inc.size()) &&
          h->upload(&h->d_bptr, h->pat.bptr.data(), h->pat.bptr.size()) &&
-         h->upload(&h->d_urow, h->pat.u_row.data(), h->pat.u_row.size()) &&
-         h->upload(&h->d_ucol, h->pat.u_col.data(), h->pat.u_col.size()) &&
-         h->upload(&h->d_ukab, h->pat.u_kab.data(), h->pat.u_kab.size()) &&
+         h->upload(&h->d_bcol, h->pat.bcol.data(), h->pat.bcol.size()) &&
+         h->upload(&h->d_uptr, h->pat.uptr.data(), h->pat.uptr.size()) &&
+         h->upload(&h->d_kdiag, h->pat.kdiag.data(), h->pat.kdiag.size()) &&
          h->upload(&h->d_ukba, h->pat.u_kba.data(), h->pat.u_kba.size()) &&
          h->upload(&h->d_ucptr, h->pat.u_cptr.data(), h->pat.u_cptr.size()) &&
          h->upload(&h->d_ucontrib, h->pat.u_contrib.data(), h->pat.u_contrib.size()) &&

@@ -128,6 +128,9 @@ bool build_pattern(int nd, int nn, int64_t npoint, int64_t ncell, const int64_t*
         }
     }
     p.u_cptr[NU] = NC;
+    p.uptr = uptr;
+    p.kdiag.assign(npoint, 0);
+    for (int64_t A = 0; A < npoint; A++) p.kdiag[A] = (uptr[A + 1] > uptr[A]) ? p.u_kab[uptr[A]] : 0;
     // position of A in block row B
 #pragma omp parallel for schedule(static)
     for (int64_t u = 0; u < NU; u++) {

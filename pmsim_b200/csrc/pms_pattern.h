@@ -29,6 +29,8 @@ struct Pattern {
     std::vector<int32_t> u_col;   // B
     std::vector<int64_t> u_cptr;  // contributions of upper block u: [u_cptr[u], u_cptr[u+1])
     std::vector<int32_t> u_contrib;  // (cell*npair + pair) | transpose<<31
+    std::vector<int64_t> uptr;       // upper blocks of block row A: [uptr[A], uptr[A+1])
+    std::vector<int32_t> kdiag;      // position of A in its own block row (first upper block)
     int64_t nblock() const { return (int64_t)bcol.size(); }
     int64_t nupper() const { return (int64_t)u_row.size(); }
 };
