@@ -157,6 +157,48 @@ int pms_elements_error_location(const pms_elements* h, int64_t* cell, int32_t* i
 /* Number of kernels this handle has launched since creation (instrumentation). */
 int64_t pms_elements_launch_count(const pms_elements* h);
 
+/* ---- batched Newton solver on the device --------------------------------------------------
+ * Many independent problems share one pms_elements handle: problem p owns the points
+ * [point_ptr[p], point_ptr[p+1]) and the cells [cell_ptr[p], cell_ptr[p+1]) (disjoint ranges, so
+ * the handle's CSR matrix is block diagonal).  Every Newton iteration is one element launch for all
+ * problems and one batched PCG solve; the sequencing, the Lagrange-multiplier treatment of the
+ * prescribed equations and the convergence tests are those of SolverImplicit::iterate
+ * (src/fem/solver_implicit.rs:187-272, src/fem/bc_prescribed.rs:99-134,
+ * src/fem/convergence_control.rs:52-128).  The reference's direct solve (UMFPACK,
+ * src/fem/linear_system.rs:185-201) is replaced by FP64 PCG with a node-block Jacobi preconditioner
+ * on the system with the prescribed equations eliminated; it reproduces the augmented system's
+ * iterates.  Each problem's arithmetic is independent of the other problems in the batch. */
+typedef struct pms_batch_config {
+    double tol_rr_abs;          /* max|R| < tol_rr_abs: converged (reference default 1e-10) */
+    double tol_mdu_rel;         /* rel(mdu) < tol_mdu_rel (iteration > 0): converged (default 1e-8) */
+    int32_t n_max_iterations;   /* Newton iterations per step (reference default 10) */
+    double pcg_rtol;            /* PCG stops at |r|_2 <= pcg_rtol |r0|_2 (default 1e-12) */
+    int32_t pcg_max_iterations; /* PCG iteration cap per solve (default 20000) */
+} pms_batch_config;
+
+typedef struct pms_batch pms_batch;
+
+/* pres_eq[npres]: sorted, unique global equations with prescribed values (Essential);
+ * ff_ext[ndof] (host, nullable): constant external forces (loading factor 1). */
+int pms_batch_create(pms_elements* el, int32_t nproblem, const int64_t* point_ptr, const int64_t* cell_ptr,
+                     int64_t npres, const int64_t* pres_eq, const double* ff_ext, const pms_batch_config* cfg,
+                     pms_batch** out);
+void pms_batch_destroy(pms_batch* b);
+/* U = 0, multipliers = 0 and pms_elements_initialize of the handle */
+int pms_batch_reset(pms_batch* b);
+/* One load step for the problems with active[p] != 0: dU = 0, lambda = 0 at the IPs, then Newton
+ * iterations until each problem converges.  c_values[npres] (host) are the prescribed values at the
+ * new time of each problem.  Per problem (host, nullable): iterations (residual evaluations, as the
+ * reference counts them), final max|R|, status (0 ok, 1 NaN/Inf in R, 2 NaN/Inf in mdu,
+ * 3 "Newton-Raphson did not converge") and the PCG iterations spent. */
+int pms_batch_solve_step(pms_batch* b, const double* c_values, const uint8_t* active, int32_t* iterations,
+                         double* norm_rr, int32_t* status, int32_t* pcg_iterations);
+int pms_batch_get_u(pms_batch* b, double* u);                 /* host u[ndof] */
+int pms_batch_get_multipliers(pms_batch* b, double* lam);     /* host lambda[npres] (reactions) */
+/* kernels launched by the solver (PCG iterations captured in graphs count once per kernel) */
+int64_t pms_batch_counters(const pms_batch* b, int64_t* pcg_iterations_total);
+const char* pms_batch_last_error(const pms_batch* b);
+
 /* ---- material batch (StressStrainTrait::update_stress + stiffness over n IPs) -------------
  * Device buffers, structure-of-arrays with component stride n:
  *   sig[ncomp*n] (in/out), z[n] (in/out), lambda[n] (out), elastic[n] (out), deps[ncomp*n] (in),

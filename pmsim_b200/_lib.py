@@ -53,6 +53,12 @@ class Config_(ctypes.Structure):
                 ("thickness", ctypes.c_double)]
 
 
+class BatchConfig_(ctypes.Structure):
+    _fields_ = [("tol_rr_abs", ctypes.c_double), ("tol_mdu_rel", ctypes.c_double),
+                ("n_max_iterations", ctypes.c_int32), ("pcg_rtol", ctypes.c_double),
+                ("pcg_max_iterations", ctypes.c_int32)]
+
+
 class Info_(ctypes.Structure):
     _fields_ = [("ndim", ctypes.c_int32), ("kind", ctypes.c_int32), ("nnode", ctypes.c_int32),
                 ("ngauss", ctypes.c_int32), ("ncomp", ctypes.c_int32), ("npoint", ctypes.c_int64),
@@ -96,6 +102,14 @@ SIGNATURES = {
     "pms_probe_fp64_fma": (_I, [_I64, _I, _V, _V]),
     "pms_element_calc_noalloc": (_I, [_I, _I, _D, ctypes.POINTER(Material_), _I64, _V, _V, _V, _V, _V, _V,
                                       ctypes.POINTER(_I64), _V]),
+    "pms_batch_create": (_I, [_V, _I, _V, _V, _I64, _V, _V, ctypes.POINTER(BatchConfig_), ctypes.POINTER(_V)]),
+    "pms_batch_destroy": (None, [_V]),
+    "pms_batch_reset": (_I, [_V]),
+    "pms_batch_solve_step": (_I, [_V, _V, _V, _V, _V, _V, _V]),
+    "pms_batch_get_u": (_I, [_V, _V]),
+    "pms_batch_get_multipliers": (_I, [_V, _V]),
+    "pms_batch_counters": (_I64, [_V, ctypes.POINTER(_I64)]),
+    "pms_batch_last_error": (ctypes.c_char_p, [_V]),
     "pms_version": (ctypes.c_char_p, []),
     "pms_material_launch_count": (_I64, []),
 }

@@ -39,6 +39,7 @@
 
 #include "../../include/pms.h"
 #include "pms_device.cuh"
+#include "pms_internal.h"
 #include "pms_pattern.h"
 #include "pms_shapes.h"
 
@@ -50,7 +51,10 @@ constexpr unsigned FULL = 0xffffffffu;
 constexpr int WPB = 4;  // warps (cells) per block
 
 // Modes of the element kernel
-enum { UPD_NONE = 0, UPD_CURRENT = 1, UPD_BACKUP = 2 };
+// UPD_MODE: the mode comes at run time from the cell's problem (batched solver):
+//   0 = inactive (cell skipped), 1 = step start: assemble from the current state with lambda = 0
+//   and copy it to the backup, 2 = update from the backup with ddu, then assemble.
+enum { UPD_NONE = 0, UPD_CURRENT = 1, UPD_BACKUP = 2, UPD_MODE = 3 };
 
 struct ElemArgs {
     int64_t ncell;     // cells in this launch
@@ -70,6 +74,8 @@ struct ElemArgs {
     double* fe;   // [cell][nn][nd]
     double* ke;   // [cell][npair][nd*nd]
     int32_t* status;  // {code, cell, ip, 0}
+    const int32_t* cell_prob = nullptr;  // UPD_MODE: problem of each cell
+    const uint8_t* pmode = nullptr;      // UPD_MODE: mode of each problem
 };
 
 __device__ __forceinline__ void report(int32_t* status, int code, int64_t cell, int ip) {
@@ -78,13 +84,6 @@ __device__ __forceinline__ void report(int32_t* status, int code, int64_t cell, 
         status[1] = (int32_t)cell;
         status[2] = ip;
     }
-}
-
-// sum over the warp, result identical on every lane (tree to lane 0, then broadcast)
-__device__ __forceinline__ double warp_sum(double v) {
-#pragma unroll
-    for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(FULL, v, off);
-    return __shfl_sync(FULL, v, 0);
 }
 
 template <int ND>
@@ -165,6 +164,13 @@ __global__ void __launch_bounds__(WPB * 32) element_kernel(ElemArgs A) {
     const int64_t cl = (int64_t)blockIdx.x * WPB + wid;
     if (cl >= A.ncell) return;  // whole warp exits together
     const int64_t cell = A.cell0 + cl;
+    int mode = (UPD == UPD_NONE) ? 0 : 2;
+    if (UPD == UPD_MODE) {
+        mode = A.pmode[A.cell_prob[cell]];
+        if (mode == 0) return;  // inactive problem: whole warp exits
+    }
+    const bool do_update = (UPD == UPD_MODE) ? (mode == 2) : (UPD != UPD_NONE);
+    const bool from_backup = (UPD == UPD_BACKUP) || (UPD == UPD_MODE && mode == 2);
     const MatConst mc = A.mats[A.cmat ? A.cmat[cell] : 0];
 
     if (lane < NN) {
@@ -172,7 +178,7 @@ __global__ void __launch_bounds__(WPB * 32) element_kernel(ElemArgs A) {
 #pragma unroll
         for (int i = 0; i < ND; i++) {
             Xs[lane * ND + i] = A.coords[(int64_t)pt * ND + i];
-            Us[lane * ND + i] = (UPD != UPD_NONE) ? A.ddu[(int64_t)pt * ND + i] : 0.0;
+            Us[lane * ND + i] = do_update ? A.ddu[(int64_t)pt * ND + i] : 0.0;
         }
     }
     __syncwarp();
@@ -186,15 +192,25 @@ __global__ void __launch_bounds__(WPB * 32) element_kernel(ElemArgs A) {
 #pragma unroll
     for (int c = 0; c < NC; c++) sig[c] = 0.0;
     if (has_ip) {
-        const double* ssrc = (UPD == UPD_BACKUP) ? A.sig_src : A.sig;
-        const double* zsrc = (UPD == UPD_BACKUP) ? A.z_src : A.z;
-        const double* lsrc = (UPD == UPD_BACKUP) ? A.lam_src : A.lam;
-        const uint8_t* esrc = (UPD == UPD_BACKUP) ? A.el_src : A.el;
+        const double* ssrc = from_backup ? A.sig_src : A.sig;
+        const double* zsrc = from_backup ? A.z_src : A.z;
+        const double* lsrc = from_backup ? A.lam_src : A.lam;
+        const uint8_t* esrc = from_backup ? A.el_src : A.el;
 #pragma unroll
         for (int c = 0; c < NC; c++) sig[c] = ssrc[(int64_t)c * A.nip + ip0 + lane];
         z = zsrc[ip0 + lane];
         lam = lsrc[ip0 + lane];
         el = esrc[ip0 + lane];
+        if (UPD == UPD_MODE && mode == 1) {
+            // reset_algorithmic_variables + backup_secondary_values of a new load step
+            lam = 0.0;
+#pragma unroll
+            for (int c = 0; c < NC; c++) const_cast<double*>(A.sig_src)[(int64_t)c * A.nip + ip0 + lane] = sig[c];
+            const_cast<double*>(A.z_src)[ip0 + lane] = z;
+            const_cast<double*>(A.lam_src)[ip0 + lane] = 0.0;
+            const_cast<uint8_t*>(A.el_src)[ip0 + lane] = (uint8_t)el;
+            A.lam[ip0 + lane] = 0.0;
+        }
         const int p = lane;
         double J[ND * ND];
 #pragma unroll
@@ -224,7 +240,7 @@ __global__ void __launch_bounds__(WPB * 32) element_kernel(ElemArgs A) {
                 g[i] = v;
                 Gp[m * ND + i] = v;
             }
-            if (UPD != UPD_NONE) {
+            if (do_update) {
                 const double* u = Us + m * ND;
                 eps[0] += u[0] * g[0];
                 eps[1] += u[1] * g[1];
@@ -238,7 +254,7 @@ __global__ void __launch_bounds__(WPB * 32) element_kernel(ElemArgs A) {
                 }
             }
         }
-        if (UPD != UPD_NONE) {
+        if (do_update) {
             const int st = ip_update<NC>(mc, mc.hh, sig, z, lam, el, eps);
             if (st != OK && err == OK) err = st;
         }
@@ -280,7 +296,7 @@ __global__ void __launch_bounds__(WPB * 32) element_kernel(ElemArgs A) {
             if (lane == 0) report(A.status, code, cell, p);
         }
     }
-    if (UPD != UPD_NONE && has_ip) {
+    if (do_update && has_ip) {
 #pragma unroll
         for (int c = 0; c < NC; c++) A.sig[(int64_t)c * A.nip + ip0 + lane] = sig[c];
         A.z[ip0 + lane] = z;
@@ -557,6 +573,8 @@ struct pms_elements {
     int32_t *d_kdiag = nullptr, *d_ukba = nullptr, *d_ucontrib = nullptr;
     int64_t* d_ucptr = nullptr;
     double *d_ddu = nullptr, *d_ff = nullptr, *d_csr = nullptr;  // staging for host-memory calls
+    int64_t* d_indptr = nullptr;  // device CSR pattern (built on first request)
+    int32_t* d_indices = nullptr;
     int32_t* d_status = nullptr;
     int64_t device_bytes = 0;
     cudaStream_t stream = nullptr;
@@ -656,7 +674,27 @@ void launch_elem_nn(pms_elements* h, const ElemArgs& a, int upd, bool dof, bool 
     }
 }
 
+template <int ND, int NN>
+void launch_elem_modes(pms_elements* h, const ElemArgs& a) {
+    launch_elem_t<ND, NN, UPD_MODE, true, true>(h, a);
+}
+
 void launch_elem(pms_elements* h, const ElemArgs& a, int upd, bool dof, bool dok) {
+    if (upd == UPD_MODE) {
+        switch (h->kind) {
+        case PMS_TRI3: launch_elem_modes<2, 3>(h, a); break;
+        case PMS_TRI6: launch_elem_modes<2, 6>(h, a); break;
+        case PMS_QUA4: launch_elem_modes<2, 4>(h, a); break;
+        case PMS_QUA8: launch_elem_modes<2, 8>(h, a); break;
+        case PMS_QUA9: launch_elem_modes<2, 9>(h, a); break;
+        case PMS_TET4: launch_elem_modes<3, 4>(h, a); break;
+        case PMS_TET10: launch_elem_modes<3, 10>(h, a); break;
+        case PMS_HEX8: launch_elem_modes<3, 8>(h, a); break;
+        case PMS_HEX20: launch_elem_modes<3, 20>(h, a); break;
+        }
+        h->launches++;
+        return;
+    }
     switch (h->kind) {
     case PMS_TRI3: launch_elem_nn<2, 3>(h, a, upd, dof, dok); break;
     case PMS_TRI6: launch_elem_nn<2, 6>(h, a, upd, dof, dok); break;
@@ -1150,6 +1188,52 @@ int pms_mesh_csr_pattern(const pms_mesh* mesh, int64_t* indptr, int32_t* indices
 }
 
 }  // extern "C"
+
+// ------------------------------------------------------------------------------------------
+// Internal interface used by the batched solver (pms_internal.h).
+namespace pms {
+
+ElementsView elements_view(pms_elements* h) {
+    ElementsView v;
+    v.nd = h->nd;
+    v.nn = h->nn;
+    v.ng = h->ng;
+    v.npoint = h->npoint;
+    v.ncell = h->ncell;
+    v.ndof = h->ndof;
+    v.nnz = h->nnz;
+    v.d_bptr = h->d_bptr;
+    v.d_kdiag = h->d_kdiag;
+    v.stream = h->stream;
+    return v;
+}
+
+int elements_device_pattern(pms_elements* h, const int64_t** indptr, const int32_t** indices) {
+    if (!h->d_indptr) {
+        if (!h->alloc(&h->d_indptr, (size_t)h->ndof + 1) || !h->alloc(&h->d_indices, (size_t)h->nnz))
+            return fail(h, PMS_ERR_NOMEM, "out of device memory for the CSR pattern");
+        int rc = pms_elements_csr_pattern(h, h->d_indptr, h->d_indices, PMS_MEM_DEVICE);
+        if (rc) return rc;
+    }
+    *indptr = h->d_indptr;
+    *indices = h->d_indices;
+    return PMS_OK;
+}
+
+int elements_run_modes(pms_elements* h, const int32_t* cell_prob, const uint8_t* pmode, const double* ddu,
+                       double* ff, double* csr) {
+    ElemArgs a = make_args(h, ddu);
+    a.cell_prob = cell_prob;
+    a.pmode = pmode;
+    launch_elem(h, a, UPD_MODE, true, true);
+    launch_f_gather(h, ff);
+    launch_kk_gather(h, csr);
+    return cuda_check(h);
+}
+
+int elements_status(pms_elements* h) { return finish_host(h); }
+
+}  // namespace pms
 
 // ------------------------------------------------------------------------------------------
 // Element matrices without any device allocation.

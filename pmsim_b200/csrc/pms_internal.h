@@ -1,0 +1,32 @@
+// pms_internal.h -- C++ interface between the element handle (pms_elements.cu) and the batched
+// Newton/PCG solver (pms_solver.cu).  Not part of the C ABI.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "../../include/pms.h"
+
+namespace pms {
+
+struct ElementsView {
+    int nd, nn, ng;
+    int64_t npoint, ncell, ndof, nnz;
+    const int64_t* d_bptr;   // block-row pointers (npoint + 1)
+    const int32_t* d_kdiag;  // position of the diagonal block in each block row
+    cudaStream_t stream;
+};
+
+ElementsView elements_view(pms_elements* h);
+
+// Device CSR pattern of K (allocated by the handle on first use, kept until destroy).
+int elements_device_pattern(pms_elements* h, const int64_t** indptr, const int32_t** indices);
+
+// One launch of the element kernel in per-problem mode (0 skip, 1 step start, 2 update) followed by
+// the F_int and CSR gathers; all pointers are device pointers on the handle's stream.
+int elements_run_modes(pms_elements* h, const int32_t* cell_prob, const uint8_t* pmode, const double* ddu,
+                       double* ff, double* csr);
+
+// Sets lambda = 0 ... not needed: mode 1 resets it.  Status of the last launches (syncs the stream).
+int elements_status(pms_elements* h);
+
+}  // namespace pms

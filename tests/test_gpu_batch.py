@@ -1,0 +1,102 @@
+"""Batched device Newton + PCG (pms_batch_*): parity with the golden runs and with the oracle driver,
+and results independent of the batch composition (same bits alone and in the mix).
+
+Reference: SolverImplicit::iterate (src/fem/solver_implicit.rs:187-272) with LMM prescribed values
+(src/fem/bc_prescribed.rs:99-134); golden data as in test_gpu_solver.py.
+"""
+import numpy as np
+import pytest
+
+import oracle
+import problems
+from oracle.driver import OracleSolver
+from pmsim_b200 import mesh as M
+
+pytestmark = pytest.mark.gpu
+
+
+def as_problem(pb):
+    from pmsim_b200.batch import Problem
+    from pmsim_b200.elements import Material
+    return Problem(pb["mesh"], Material.von_mises(*pb["params"]), pb["essential"], nsteps=pb["nsteps"],
+                   ngauss=pb["ngauss"])
+
+
+def footing(nx, ny, E, z0, width, nsteps=10, seed=0):
+    """The plane-strain strip footing of the small benchmark configuration: 10 m x 5 m, Qua8, 3x3
+    Gauss, von Mises nu=0.3 H=0, bottom fixed, sides roller, top nodes with x <= width pressed
+    down by 0.005 m per step."""
+    from pmsim_b200.batch import Problem
+    from pmsim_b200.elements import Material
+    m = M.structured_2d(M.QUA8, nx, ny, 10.0, 5.0)
+    tol = 1e-8
+    ess = []
+    for p in m.points_where(lambda x, y: np.abs(y) < tol):
+        ess += [(2 * p, 0.0, None), (2 * p + 1, 0.0, None)]
+    for p in m.points_where(lambda x, y: (np.abs(x) < tol) | (np.abs(x - 10.0) < tol)):
+        ess += [(2 * p, 0.0, None)]
+    for p in m.points_where(lambda x, y: (np.abs(y - 5.0) < tol) & (x <= width + tol)):
+        ess += [(2 * p + 1, -0.005, lambda t: t)]
+    return Problem(m, Material.von_mises(E, 0.3, 0.0, z0), ess, nsteps=nsteps, ngauss=9)
+
+
+@pytest.mark.parametrize("name", ["single_element_2d", "2x2_elements_2d", "tensile_755"])
+def test_batch_spo_golden(name):
+    from pmsim_b200.batch import BatchSolver
+    pb = problems.SPO_PROBLEMS[name]()
+    bs = BatchSolver([as_problem(pb)], n_max_iterations=20)
+    worst = [0.0, 0.0]
+
+    def cb(step, b):
+        sig = b.state_of(0)[0]
+        du, ds = problems.compare_step(pb["golden"], step, b.u_of(0), sig, pb["ngauss"])
+        worst[0] = max(worst[0], du)
+        worst[1] = max(worst[1], ds)
+
+    bs.solve(cb)
+    assert worst[0] <= pb["tol_u"], worst
+    assert worst[1] <= pb["tol_s"], worst
+    m = pb["mesh"]
+    oel = oracle.OracleElements(m, 1, oracle.Params(*pb["params"]), ngauss=pb["ngauss"], sym_tol=-1.0)
+    osol = OracleSolver(oel, m.ndof, pb["essential"], n_max_iterations=20, t_fin=float(pb["nsteps"]))
+    osol.solve()
+    assert bs.history[0] == [len(h) for h in osol.history]
+
+
+def test_batch_footing_matches_oracle_driver():
+    """Small footing (the CPU-runnable configuration at reduced size) against the oracle driver:
+    displacements, IP stresses and the Newton iteration count of every step."""
+    from pmsim_b200.batch import BatchSolver
+    pb = footing(8, 4, 1e4, 9.0, 1.0, nsteps=10)
+    bs = BatchSolver([pb], n_max_iterations=20)
+    got = []
+    bs.solve(lambda s, b: got.append((b.u_of(0).copy(), b.state_of(0)[0].copy())))
+    m = pb.mesh
+    oel = oracle.OracleElements(m, 1, oracle.Params(1e4, 0.3, 0.0, 9.0), ngauss=9, sym_tol=-1.0)
+    ref = []
+    osol = OracleSolver(oel, m.ndof, pb.essential, n_max_iterations=20, t_fin=10.0)
+    osol.solve(lambda step, t, u, el: ref.append((u.copy(), el.sig.copy())))
+    assert bs.history[0] == [len(h) for h in osol.history]
+    for (ug, sg), (uo, so) in zip(got, ref):
+        assert np.max(np.abs(ug - uo)) <= 1e-9 * max(np.max(np.abs(uo)), 1e-30)
+        assert np.max(np.abs(sg - so)) <= 1e-7 * np.max(np.abs(so))
+
+
+def test_batch_results_do_not_depend_on_the_mix():
+    from pmsim_b200.batch import BatchSolver
+    rng = np.random.default_rng(5)
+    probs = [footing(int(rng.integers(4, 10)), int(rng.integers(2, 6)), float(1e4 * np.exp(rng.normal(0, 0.5))),
+                     float(rng.uniform(5, 20)), float(rng.uniform(0.5, 2.0)), nsteps=4) for _ in range(5)]
+    mix = BatchSolver(probs)
+    mix.solve()
+    u_mix = mix.u()
+    st_mix = mix.elements.get_state()
+    for i, p in enumerate(probs):
+        alone = BatchSolver([p])
+        alone.solve()
+        assert np.array_equal(alone.u(), mix.u_of(i, u_mix)), f"problem {i}: U differs alone vs in the mix"
+        a = alone.elements.get_state()
+        b = mix.state_of(i, st_mix)
+        for x, y in zip(a, b):
+            assert np.array_equal(x, y)
+        assert alone.history[0] == mix.history[i]
