@@ -190,7 +190,8 @@ int pms_batch_reset(pms_batch* b);
  * iterations until each problem converges.  c_values[npres] (host) are the prescribed values at the
  * new time of each problem.  Per problem (host, nullable): iterations (residual evaluations, as the
  * reference counts them), final max|R|, status (0 ok, 1 NaN/Inf in R, 2 NaN/Inf in mdu,
- * 3 "Newton-Raphson did not converge") and the PCG iterations spent. */
+ * 3 "Newton-Raphson did not converge", 4/5/6 the stress-update, tangent or Jacobian error of the
+ * element path -- a failing problem stops, the others go on) and the PCG iterations spent. */
 int pms_batch_solve_step(pms_batch* b, const double* c_values, const uint8_t* active, int32_t* iterations,
                          double* norm_rr, int32_t* status, int32_t* pcg_iterations);
 int pms_batch_get_u(pms_batch* b, double* u);                 /* host u[ndof] */

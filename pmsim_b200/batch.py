@@ -139,17 +139,30 @@ class BatchSolver:
             self.pcg_history[p].append(int(pcg[p]))
         return iters, norm, status, pcg
 
-    def solve(self, on_step=None):
-        """Runs every problem through its load steps (problems with fewer steps drop out)."""
+    MESSAGES = {1: "Found NaN or Inf", 2: "Found NaN or Inf in mdu", 3: "Newton-Raphson did not converge",
+                4: "von Mises plastic update must not lead to zero sigma_d (sigma_d < 1e-10)",
+                5: "von Mises stiffness cannot be computed with zero deviatoric norm (norm_s < 1e-10)",
+                6: "the determinant of the Jacobian must be positive"}
+
+    def solve(self, on_step=None, on_fail="raise"):
+        """Runs every problem through its load steps (problems with fewer steps drop out).
+
+        on_fail="raise" stops at the first failing problem with the reference's message;
+        on_fail="drop" removes failing problems and records them in ``self.failed``."""
         self.reset()
+        self.failed = {}
         nmax = max(p.nsteps for p in self.problems)
         for s in range(nmax):
-            act = np.array([1 if s < p.nsteps else 0 for p in self.problems], np.uint8)
+            act = np.array([1 if (s < p.nsteps and i not in self.failed) else 0
+                            for i, p in enumerate(self.problems)], np.uint8)
+            if not act.any():
+                break
             iters, norm, status, pcg = self.solve_step(act)
-            bad = np.nonzero(status * act)[0]
-            if len(bad):
-                msgs = {1: "Found NaN or Inf", 2: "Found NaN or Inf in mdu", 3: "Newton-Raphson did not converge"}
-                raise RuntimeError(f"problem {bad[0]}: {msgs.get(int(status[bad[0]]), 'error')}")
+            for i in np.nonzero(status * act)[0]:
+                msg = self.MESSAGES.get(int(status[i]), "error")
+                if on_fail == "raise":
+                    raise RuntimeError(f"problem {i}: {msg}")
+                self.failed[int(i)] = (s, msg)
             if on_step is not None:
                 on_step(s, self)
 

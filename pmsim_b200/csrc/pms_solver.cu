@@ -417,7 +417,7 @@ struct pms_batch {
     int np = 0;
     int64_t nnode = 0, ndof = 0, npres = 0, nchunk = 0;
     pms_batch_config cfg{};
-    std::vector<int64_t> point_ptr, pres_ptr;
+    std::vector<int64_t> point_ptr, cell_ptr, pres_ptr;
     std::vector<void*> allocs;
     // device
     int32_t *d_node_prob = nullptr, *d_cell_prob = nullptr, *d_chunk_nnode = nullptr, *d_chunk_prob = nullptr;
@@ -552,6 +552,7 @@ int pms_batch_create(pms_elements* el, int32_t nproblem, const int64_t* point_pt
     b->graph_iters = 8;
     const int nd = b->v.nd;
     b->point_ptr.assign(point_ptr, point_ptr + nproblem + 1);
+    b->cell_ptr.assign(cell_ptr, cell_ptr + nproblem + 1);
     if (point_ptr[0] != 0 || point_ptr[nproblem] != b->nnode || cell_ptr[0] != 0 || cell_ptr[nproblem] != b->v.ncell) {
         delete b;
         return PMS_ERR_INVALID;
@@ -694,8 +695,20 @@ int pms_batch_solve_step(pms_batch* b, const double* c_values, const uint8_t* ac
         finalize_kernel<<<grid_of(np, 128), 128, 0, st>>>(np, b->d_pchunk, b->d_part_a, b->d_norm, 0);
         cudaMemcpyAsync(hnorm.data(), b->d_norm, np * 8, cudaMemcpyDeviceToHost, st);
         if (cudaStreamSynchronize(st) != cudaSuccess) return bfail(b, PMS_ERR_CUDA, "residual failed");
+        // a material or geometry error in one problem stops that problem only
         rc = elements_status(b->el);
-        if (rc) return rc;
+        if (rc == PMS_ERR_ZERO_SIGMA_D || rc == PMS_ERR_ZERO_NORM_S || rc == PMS_ERR_JACOBIAN) {
+            int64_t cell = -1;
+            int32_t ip = -1;
+            pms_elements_error_location(b->el, &cell, &ip);
+            const int p = (int)(std::upper_bound(b->cell_ptr.begin(), b->cell_ptr.end(), cell) - b->cell_ptr.begin()) - 1;
+            if (p >= 0 && p < np) {
+                stat[p] = 1 + rc;  // 4: zero sigma_d, 5: zero norm_s, 6: Jacobian
+                running[p] = 0;
+            }
+        } else if (rc) {
+            return rc;
+        }
         for (int p = 0; p < np; p++) {
             if (!running[p]) continue;
             iters[p] = it + 1;
@@ -764,7 +777,7 @@ int pms_batch_solve_step(pms_batch* b, const double* c_values, const uint8_t* ac
     }
     if (cudaStreamSynchronize(st) != cudaSuccess) return bfail(b, PMS_ERR_CUDA, "step failed");
     rc = elements_status(b->el);
-    if (rc) return rc;
+    if (rc && rc != PMS_ERR_ZERO_SIGMA_D && rc != PMS_ERR_ZERO_NORM_S && rc != PMS_ERR_JACOBIAN) return rc;
     for (int p = 0; p < np; p++) {
         if (act[p] && !conv[p] && stat[p] == 0) stat[p] = 3;  // "Newton-Raphson did not converge"
         if (iterations) iterations[p] = iters[p];
