@@ -50,6 +50,8 @@ def parse():
     ap.add_argument("--cpu-cells", type=int, default=0)
     ap.add_argument("--batched", type=int, default=512, help="footing problems in the batched solve (0: skip)")
     ap.add_argument("--alone-sample", type=int, default=8, help="problems solved one at a time for the ratio")
+    ap.add_argument("--served", type=int, default=64, help="requests in the served run (0: skip)")
+    ap.add_argument("--rate", type=float, default=200.0, help="Poisson arrival rate of the served run (req/s)")
     return ap.parse_args()
 
 
@@ -216,7 +218,7 @@ def run_batched(nprob, nalone, seed=2024):
     t_setup = time.perf_counter() - t0
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    bs.solve(on_fail="drop")
+    bs.solve_independent(on_fail="drop")
     torch.cuda.synchronize()
     t_batch = time.perf_counter() - t0
     nfail = len(bs.failed)
@@ -235,7 +237,7 @@ def run_batched(nprob, nalone, seed=2024):
         b1 = BatchSolver([probs[i]], n_max_iterations=20, pcg_max_iterations=5000)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        b1.solve(on_fail="drop")
+        b1.solve_independent(on_fail="drop")
         torch.cuda.synchronize()
         t_alone += time.perf_counter() - t0
         ok_alone += 0 if b1.failed else 1
@@ -268,6 +270,44 @@ def run_batched(nprob, nalone, seed=2024):
             "ratio_vs_direct": batched / direct if direct > 0 else None,
             "note": "solves/s counts converged problems (max|R| <= 1e-10); failures are Newton divergence "
                     "of the reference scheme on the finest meshes (the CPU oracle fails them too)"}
+
+
+def run_served(nreq, rate, nalone, seed=7):
+    """Served configuration: Poisson arrivals (rate req/s) of footing (70%, 1k-50k DOF) and Hex8
+    block (30%, up to 206,763 DOF) requests, 10 load steps each, admitted under a 120 GB device
+    budget into device batches that overlap on the GPU (continuous batching); throughput and
+    latency percentiles, and the same requests solved one at a time for the ratio."""
+    import torch
+    from pmsim_b200.batch import BatchSolver
+    from pmsim_b200.footing import request_population
+    from pmsim_b200.serve import Request, Server, poisson_arrivals, summarize
+    probs = request_population(nreq, seed=seed)
+    arr = poisson_arrivals(nreq, rate, seed=seed + 1)
+    reqs = [Request(i, p, float(a)) for i, (p, a) in enumerate(zip(probs, arr))]
+    srv = Server(budget_bytes=120e9, n_max_iterations=20, pcg_max_iterations=5000)
+    torch.cuda.synchronize()
+    srv.serve(reqs)
+    torch.cuda.synchronize()
+    out = summarize(reqs)
+    out.update({"rate_req_per_s": rate, "batches": srv.batches, "peak_concurrent_batches": srv.peak_concurrent,
+                "peak_admitted_bytes": srv.peak_in_use, "budget_bytes": 120e9,
+                "ndof_min": int(min(p.mesh.ndof for p in probs)), "ndof_max": int(max(p.mesh.ndof for p in probs))})
+    rng = np.random.default_rng(seed + 2)
+    sample = sorted(rng.choice(nreq, size=min(nalone, nreq), replace=False).tolist())
+    t_alone, ok = 0.0, 0
+    for i in sample:
+        b1 = BatchSolver([probs[i]], n_max_iterations=20, pcg_max_iterations=5000)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        b1.solve_independent(on_fail="drop")
+        torch.cuda.synchronize()
+        t_alone += time.perf_counter() - t0
+        ok += 0 if b1.failed else 1
+        b1.close()
+    out["alone_sample"] = len(sample)
+    out["alone_solves_per_s"] = ok / t_alone if t_alone > 0 else None
+    out["ratio_vs_alone"] = (out["solves_per_s"] / out["alone_solves_per_s"]) if ok else None
+    return out
 
 
 def cpu_sample(m, ddu, ncell_sample, nthreads):
@@ -432,6 +472,10 @@ def main():
     if args.batched > 0 and args.size == "full":
         torch.cuda.empty_cache()
         batched = run_batched(args.batched, args.alone_sample)
+    served = None
+    if args.served > 0 and args.size == "full":
+        torch.cuda.empty_cache()
+        served = run_served(args.served, args.rate, args.alone_sample)
     ms_elem = kt[0] / max(kc[0], 1)
     fl_ip = flops_per_ip_hex20()
     achieved_tf = nip * fl_ip / (ms_elem * 1e-3) / 1e12
@@ -469,7 +513,7 @@ def main():
         "kernels_ms_per_step": {"element": ms_elem, "f_gather": kt[1] / max(kc[1], 1),
                                 "kk_gather": kt[2] / max(kc[2], 1)},
         "gpu_launches": int(launches),
-        "e2e": e2e, "cpu_baseline": cpu, "k1_microbench": k1, "batched": batched, "fp64_peak_tflops": fp64,
+        "e2e": e2e, "cpu_baseline": cpu, "k1_microbench": k1, "batched": batched, "served": served, "fp64_peak_tflops": fp64,
         "clocks": clk,
     }
     print(json.dumps(line), flush=True)

@@ -194,6 +194,14 @@ int pms_batch_reset(pms_batch* b);
  * element path -- a failing problem stops, the others go on) and the PCG iterations spent. */
 int pms_batch_solve_step(pms_batch* b, const double* c_values, const uint8_t* active, int32_t* iterations,
                          double* norm_rr, int32_t* status, int32_t* pcg_iterations);
+/* One Newton iteration of every problem with cmd[p] != 0, each at its own load step and iteration
+ * (continuous batching): cmd 1 = start a new load step (dU = 0, lambda = 0 at the IPs; c_values hold
+ * its prescribed values), cmd 2 = continue the step (stress update with the current dU, then the
+ * next iteration).  result[p]: -1 idle, 0 still iterating (send cmd 2), 1 converged (state and U are
+ * the step's solution), 100 + status on failure (status codes as for pms_batch_solve_step).
+ * iteration[p] (0-based), norm_rr[p] and pcg_iterations[p] of this tick are optional outputs. */
+int pms_batch_tick(pms_batch* b, const uint8_t* cmd, const double* c_values, int32_t* result, int32_t* iteration,
+                   double* norm_rr, int32_t* pcg_iterations);
 int pms_batch_get_u(pms_batch* b, double* u);                 /* host u[ndof] */
 int pms_batch_get_multipliers(pms_batch* b, double* lam);     /* host lambda[npres] (reactions) */
 /* kernels launched by the solver (PCG iterations captured in graphs count once per kernel) */

@@ -106,6 +106,7 @@ SIGNATURES = {
     "pms_batch_destroy": (None, [_V]),
     "pms_batch_reset": (_I, [_V]),
     "pms_batch_solve_step": (_I, [_V, _V, _V, _V, _V, _V, _V]),
+    "pms_batch_tick": (_I, [_V, _V, _V, _V, _V, _V, _V]),
     "pms_batch_get_u": (_I, [_V, _V]),
     "pms_batch_get_multipliers": (_I, [_V, _V]),
     "pms_batch_counters": (_I64, [_V, ctypes.POINTER(_I64)]),

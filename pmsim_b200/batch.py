@@ -166,6 +166,62 @@ class BatchSolver:
             if on_step is not None:
                 on_step(s, self)
 
+    def tick(self, cmd):
+        """One Newton iteration of every problem with cmd[p] != 0 (1: start its next load step,
+        2: continue).  Returns (result, iteration, norm_rr, pcg_iterations) per problem."""
+        cmd = np.ascontiguousarray(cmd, np.uint8)
+        res = np.full(self.np, -1, np.int32)
+        it = np.zeros(self.np, np.int32)
+        norm = np.zeros(self.np)
+        pcg = np.zeros(self.np, np.int32)
+        c = self.c_values(self.t)
+        self._check(self.L.pms_batch_tick(self.h, _lib.ptr(cmd), _lib.ptr(c), _lib.ptr(res), _lib.ptr(it),
+                                          _lib.ptr(norm), _lib.ptr(pcg)))
+        return res, it, norm, pcg
+
+    def solve_independent(self, on_step=None, on_fail="drop", clock=None):
+        """Every problem runs through its load steps at its own pace: each tick advances every running
+        problem by one Newton iteration, and a problem that converges starts its next step at the next
+        tick (no waiting for slower problems).  Records self.history / self.failed / self.finish."""
+        import time as _time
+        clock = clock or _time.perf_counter
+        self.reset()
+        self.failed, self.finish = {}, {}
+        counts = np.zeros(self.np, np.int64)
+        cmd = np.array([1 if p.nsteps > 0 else 0 for p in self.problems], np.uint8)
+        self.t = cmd.astype(float)  # the first step's time
+        self.step[:] = 0
+        self.ticks = 0
+        while cmd.any():
+            res, it, norm, pcg = self.tick(cmd)
+            self.ticks += 1
+            for p in np.nonzero(cmd)[0]:
+                counts[p] += 1
+                if pcg[p]:
+                    self.pcg_history[p].append(int(pcg[p]))
+                r = int(res[p])
+                if r == 0:
+                    cmd[p] = 2
+                elif r == 1:
+                    self.history[p].append(int(counts[p]))
+                    counts[p] = 0
+                    self.step[p] += 1
+                    if on_step is not None:
+                        on_step(int(p), int(self.step[p]) - 1, self)
+                    if self.step[p] < self.problems[p].nsteps:
+                        self.t[p] += 1.0
+                        cmd[p] = 1
+                    else:
+                        cmd[p] = 0
+                        self.finish[int(p)] = clock()
+                else:
+                    msg = self.MESSAGES.get(r - 100, "error")
+                    if on_fail == "raise":
+                        raise RuntimeError(f"problem {p}: {msg}")
+                    self.failed[int(p)] = (int(self.step[p]), msg)
+                    cmd[p] = 0
+                    self.finish[int(p)] = clock()
+
     def u(self):
         out = np.zeros(self.mesh.ndof)
         self._check(self.L.pms_batch_get_u(self.h, _lib.ptr(out)))

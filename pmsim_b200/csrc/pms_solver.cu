@@ -441,6 +441,7 @@ struct pms_batch {
     std::string last_error;
     int64_t launches = 0;
     int64_t pcg_total = 0;
+    std::vector<int32_t> it;  // Newton iteration of each problem within its current load step
 
     template <typename T>
     bool alloc(T** p, size_t count) {
@@ -666,64 +667,70 @@ int pms_batch_reset(pms_batch* b) {
     return cudaStreamSynchronize(st) == cudaSuccess ? PMS_OK : PMS_ERR_CUDA;
 }
 
-int pms_batch_solve_step(pms_batch* b, const double* c_values, const uint8_t* active, int32_t* iterations,
-                         double* norm_rr, int32_t* status, int32_t* pcg_iterations) {
-    if (!b || !active) return PMS_ERR_INVALID;
+int pms_batch_tick(pms_batch* b, const uint8_t* cmd, const double* c_values, int32_t* result, int32_t* iteration,
+                   double* norm_rr, int32_t* pcg_iterations) {
+    if (!b || !cmd || !result) return PMS_ERR_INVALID;
     if (b->npres > 0 && !c_values) return PMS_ERR_INVALID;
     cudaStream_t st = b->v.stream;
     const int np = b->np;
-    std::vector<uint8_t> act(active, active + np), conv(np, 0), mode(np, 0), first(np, 0), upd(np, 0);
-    std::vector<int32_t> iters(np, 0), stat(np, 0), pcgi(np, 0), pcg_step(np, 0);
+    std::vector<uint8_t> running(np, 0), mode(np, 0), first(np, 0), upd(np, 0), start(np, 0);
+    std::vector<int32_t> pcg_step(np, 0);
     std::vector<double> hnorm(np, 0.0), hrel(np, 0.0);
+    if ((int)b->it.size() != np) b->it.assign(np, 0);
+    for (int p = 0; p < np; p++) {
+        result[p] = -1;
+        if (cmd[p] == 1) {
+            b->it[p] = 0;
+            start[p] = 1;
+        }
+        running[p] = cmd[p] != 0;
+        mode[p] = cmd[p] == 1 ? 1 : (cmd[p] == 2 ? 2 : 0);
+    }
     if (b->npres > 0) cudaMemcpyAsync(b->d_c, c_values, b->npres * 8, cudaMemcpyHostToDevice, st);
-    // dU = 0 for the active problems (state t += dt happens on the host: c_values)
-    cudaMemcpyAsync(b->d_upd, act.data(), np, cudaMemcpyHostToDevice, st);
+    // a new load step: dU = 0 (the loading time t += dt is in c_values)
+    cudaMemcpyAsync(b->d_upd, start.data(), np, cudaMemcpyHostToDevice, st);
     zero_masked_kernel<<<grid_of(b->ndof), 256, 0, st>>>(b->S, b->d_upd, b->d_ddu);
-    // iteration 0: assemble from the current state with lambda = 0 (and back it up)
-    for (int p = 0; p < np; p++) mode[p] = act[p] ? 1 : 0;
+    // element pass: step start (assemble with lambda = 0, backup) or stress update + assemble
     cudaMemcpyAsync(b->d_pmode, mode.data(), np, cudaMemcpyHostToDevice, st);
     int rc = elements_run_modes(b->el, b->d_cell_prob, b->d_pmode, b->d_ddu, b->d_ff, b->d_csr);
     if (rc) return rc;
-    std::vector<uint8_t> running = act;
-    for (int it = 0; it < b->cfg.n_max_iterations; it++) {
-        bool any = false;
-        for (int p = 0; p < np; p++) any = any || running[p];
-        if (!any) break;
-        cudaMemcpyAsync(b->d_active, running.data(), np, cudaMemcpyHostToDevice, st);
-        residual_kernel<<<(unsigned)b->nchunk, CHN, 0, st>>>(b->S, b->d_ff, b->d_fext, b->d_u, b->d_lam, b->d_c,
-                                                             b->d_rr, b->d_part_a);
-        finalize_kernel<<<grid_of(np, 128), 128, 0, st>>>(np, b->d_pchunk, b->d_part_a, b->d_norm, 0);
-        cudaMemcpyAsync(hnorm.data(), b->d_norm, np * 8, cudaMemcpyDeviceToHost, st);
-        if (cudaStreamSynchronize(st) != cudaSuccess) return bfail(b, PMS_ERR_CUDA, "residual failed");
-        // a material or geometry error in one problem stops that problem only
-        rc = elements_status(b->el);
-        if (rc == PMS_ERR_ZERO_SIGMA_D || rc == PMS_ERR_ZERO_NORM_S || rc == PMS_ERR_JACOBIAN) {
-            int64_t cell = -1;
-            int32_t ip = -1;
-            pms_elements_error_location(b->el, &cell, &ip);
-            const int p = (int)(std::upper_bound(b->cell_ptr.begin(), b->cell_ptr.end(), cell) - b->cell_ptr.begin()) - 1;
-            if (p >= 0 && p < np) {
-                stat[p] = 1 + rc;  // 4: zero sigma_d, 5: zero norm_s, 6: Jacobian
-                running[p] = 0;
-            }
-        } else if (rc) {
-            return rc;
+    // residual and its max norm per problem
+    cudaMemcpyAsync(b->d_active, running.data(), np, cudaMemcpyHostToDevice, st);
+    residual_kernel<<<(unsigned)b->nchunk, CHN, 0, st>>>(b->S, b->d_ff, b->d_fext, b->d_u, b->d_lam, b->d_c, b->d_rr,
+                                                         b->d_part_a);
+    finalize_kernel<<<grid_of(np, 128), 128, 0, st>>>(np, b->d_pchunk, b->d_part_a, b->d_norm, 0);
+    cudaMemcpyAsync(hnorm.data(), b->d_norm, np * 8, cudaMemcpyDeviceToHost, st);
+    if (cudaStreamSynchronize(st) != cudaSuccess) return bfail(b, PMS_ERR_CUDA, "residual failed");
+    // a material or geometry error in one problem stops that problem only
+    rc = elements_status(b->el);
+    if (rc == PMS_ERR_ZERO_SIGMA_D || rc == PMS_ERR_ZERO_NORM_S || rc == PMS_ERR_JACOBIAN) {
+        int64_t cell = -1;
+        int32_t ip = -1;
+        pms_elements_error_location(b->el, &cell, &ip);
+        const int p = (int)(std::upper_bound(b->cell_ptr.begin(), b->cell_ptr.end(), cell) - b->cell_ptr.begin()) - 1;
+        if (p >= 0 && p < np && running[p]) {
+            result[p] = 100 + 1 + rc;  // 104: zero sigma_d, 105: zero norm_s, 106: Jacobian
+            running[p] = 0;
         }
-        for (int p = 0; p < np; p++) {
-            if (!running[p]) continue;
-            iters[p] = it + 1;
-            if (!std::isfinite(hnorm[p])) {
-                stat[p] = 1;  // "Found NaN or Inf"
-                running[p] = 0;
-            } else if (hnorm[p] < b->cfg.tol_rr_abs) {
-                conv[p] = 1;
-                running[p] = 0;
-            }
+    } else if (rc) {
+        return rc;
+    }
+    bool any = false;
+    for (int p = 0; p < np; p++) {
+        if (!running[p]) continue;
+        if (iteration) iteration[p] = b->it[p];
+        if (norm_rr) norm_rr[p] = hnorm[p];
+        if (!std::isfinite(hnorm[p])) {
+            result[p] = 101;  // "Found NaN or Inf"
+            running[p] = 0;
+        } else if (hnorm[p] < b->cfg.tol_rr_abs) {
+            result[p] = 1;
+            running[p] = 0;
         }
-        any = false;
-        for (int p = 0; p < np; p++) any = any || running[p];
-        if (!any) break;
-        // linear solve for the problems still running
+        any = any || running[p];
+    }
+    if (any) {
+        // linear solve (mdu, mdl) for the problems still iterating
         cudaMemcpyAsync(b->d_active, running.data(), np, cudaMemcpyHostToDevice, st);
         block_jacobi_kernel<<<grid_of(b->nnode), 256, 0, st>>>(b->S, b->v.d_bptr, b->v.d_kdiag, b->d_csr, b->d_binv);
         pres_increment_kernel<<<grid_of(b->ndof), 256, 0, st>>>(b->S, b->d_u, b->d_c, b->d_mdu);
@@ -741,7 +748,7 @@ int pms_batch_solve_step(pms_batch* b, const double* c_values, const uint8_t* ac
             multiplier_kernel<<<grid_of(b->npres), 256, 0, st>>>(b->npres, b->d_pres_eq, b->d_pres_prob, b->d_active,
                                                                   b->d_indptr, b->d_indices, b->d_csr, b->d_mdu,
                                                                   b->d_rr, b->d_mdl);
-        for (int p = 0; p < np; p++) first[p] = (it == 0);
+        for (int p = 0; p < np; p++) first[p] = (b->it[p] == 0);
         cudaMemcpyAsync(b->d_first, first.data(), np, cudaMemcpyHostToDevice, st);
         rel_mdu_kernel<<<(unsigned)b->nchunk, CHN, 0, st>>>(b->S, b->d_first, b->d_mdu, b->d_mdu0, b->d_part_a);
         finalize_kernel<<<grid_of(np, 128), 128, 0, st>>>(np, b->d_pchunk, b->d_part_a, b->d_rel, 0);
@@ -752,16 +759,16 @@ int pms_batch_solve_step(pms_batch* b, const double* c_values, const uint8_t* ac
         for (int p = 0; p < np; p++) {
             upd[p] = 0;
             if (!running[p]) continue;
-            pcgi[p] += pcg_step[p];
+            if (pcg_iterations) pcg_iterations[p] = pcg_step[p];
             b->pcg_total += pcg_step[p];
             if (!std::isfinite(hrel[p])) {
-                stat[p] = 2;  // "Found NaN or Inf in mdu"
-                running[p] = 0;
-            } else if (it > 0 && hrel[p] < b->cfg.tol_mdu_rel) {
-                conv[p] = 1;  // converged without applying this correction
-                running[p] = 0;
+                result[p] = 102;  // "Found NaN or Inf in mdu"
+            } else if (b->it[p] > 0 && hrel[p] < b->cfg.tol_mdu_rel) {
+                result[p] = 1;  // converged without applying this correction
             } else {
                 upd[p] = 1;
+                b->it[p] += 1;
+                result[p] = (b->it[p] >= b->cfg.n_max_iterations) ? 103 : 0;  // 103: did not converge
             }
         }
         cudaMemcpyAsync(b->d_upd, upd.data(), np, cudaMemcpyHostToDevice, st);
@@ -769,21 +776,46 @@ int pms_batch_solve_step(pms_batch* b, const double* c_values, const uint8_t* ac
         if (b->npres > 0)
             update_multipliers_kernel<<<grid_of(b->npres), 256, 0, st>>>(b->npres, b->d_pres_prob, b->d_upd, b->d_mdl,
                                                                           b->d_lam);
-        for (int p = 0; p < np; p++) mode[p] = upd[p] ? 2 : 0;
-        cudaMemcpyAsync(b->d_pmode, mode.data(), np, cudaMemcpyHostToDevice, st);
-        rc = elements_run_modes(b->el, b->d_cell_prob, b->d_pmode, b->d_ddu, b->d_ff, b->d_csr);
-        if (rc) return rc;
         b->launches += 12;
     }
-    if (cudaStreamSynchronize(st) != cudaSuccess) return bfail(b, PMS_ERR_CUDA, "step failed");
-    rc = elements_status(b->el);
-    if (rc && rc != PMS_ERR_ZERO_SIGMA_D && rc != PMS_ERR_ZERO_NORM_S && rc != PMS_ERR_JACOBIAN) return rc;
+    b->launches += 4;
+    if (cudaStreamSynchronize(st) != cudaSuccess) return bfail(b, PMS_ERR_CUDA, "tick failed");
+    return PMS_OK;
+}
+
+int pms_batch_solve_step(pms_batch* b, const double* c_values, const uint8_t* active, int32_t* iterations,
+                         double* norm_rr, int32_t* status, int32_t* pcg_iterations) {
+    if (!b || !active) return PMS_ERR_INVALID;
+    const int np = b->np;
+    std::vector<uint8_t> cmd(np, 0);
+    std::vector<int32_t> res(np, -1), iter(np, 0), pcg(np, 0), pcg_sum(np, 0), stat(np, 0), count(np, 0);
+    std::vector<double> norm(np, 0.0), last_norm(np, 0.0);
+    for (int p = 0; p < np; p++) cmd[p] = active[p] ? 1 : 0;
+    for (;;) {
+        bool any = false;
+        for (int p = 0; p < np; p++) any = any || cmd[p];
+        if (!any) break;
+        std::fill(pcg.begin(), pcg.end(), 0);
+        int rc = pms_batch_tick(b, cmd.data(), c_values, res.data(), iter.data(), norm.data(), pcg.data());
+        if (rc) return rc;
+        for (int p = 0; p < np; p++) {
+            if (!cmd[p]) continue;
+            count[p] += 1;  // residual evaluations, as the reference counts iterations
+            pcg_sum[p] += pcg[p];
+            last_norm[p] = norm[p];
+            if (res[p] == 0) {
+                cmd[p] = 2;
+            } else {
+                cmd[p] = 0;
+                stat[p] = (res[p] >= 100) ? res[p] - 100 : 0;
+            }
+        }
+    }
     for (int p = 0; p < np; p++) {
-        if (act[p] && !conv[p] && stat[p] == 0) stat[p] = 3;  // "Newton-Raphson did not converge"
-        if (iterations) iterations[p] = iters[p];
-        if (norm_rr) norm_rr[p] = hnorm[p];
+        if (iterations) iterations[p] = count[p];
+        if (norm_rr) norm_rr[p] = last_norm[p];
         if (status) status[p] = stat[p];
-        if (pcg_iterations) pcg_iterations[p] = pcgi[p];
+        if (pcg_iterations) pcg_iterations[p] = pcg_sum[p];
     }
     return PMS_OK;
 }

@@ -100,3 +100,20 @@ def test_batch_results_do_not_depend_on_the_mix():
         for x, y in zip(a, b):
             assert np.array_equal(x, y)
         assert alone.history[0] == mix.history[i]
+
+
+def test_independent_progress_matches_lock_step():
+    """Ticks (each problem at its own step) give the same bits as lock-step load steps."""
+    from pmsim_b200.batch import BatchSolver
+    rng = np.random.default_rng(11)
+    probs = [footing(int(rng.integers(4, 10)), int(rng.integers(2, 6)), float(1e4 * np.exp(rng.normal(0, 0.5))),
+                     float(rng.uniform(5, 20)), float(rng.uniform(0.5, 2.0)), nsteps=int(rng.integers(2, 5)))
+             for _ in range(4)]
+    a = BatchSolver(probs)
+    a.solve()
+    b = BatchSolver(probs)
+    b.solve_independent(on_fail="raise")
+    assert np.array_equal(a.u(), b.u())
+    for x, y in zip(a.elements.get_state(), b.elements.get_state()):
+        assert np.array_equal(x, y)
+    assert a.history == b.history
