@@ -52,6 +52,7 @@ def parse():
     ap.add_argument("--alone-sample", type=int, default=8, help="problems solved one at a time for the ratio")
     ap.add_argument("--served", type=int, default=64, help="requests in the served run (0: skip)")
     ap.add_argument("--rate", type=float, default=200.0, help="Poisson arrival rate of the served run (req/s)")
+    ap.add_argument("--no-c0", action="store_true")
     return ap.parse_args()
 
 
@@ -272,6 +273,48 @@ def run_batched(nprob, nalone, seed=2024):
                     "of the reference scheme on the finest meshes (the CPU oracle fails them too)"}
 
 
+def run_c0():
+    """The reference's CPU-runnable case: the 20x10 Qua8 strip footing (9 IP, 1322 DOF, 10 steps)
+    solved end to end by (a) the drop-in path (device element calls + host sparse LU), (b) the
+    device Newton/PCG solver, (c) the CPU oracle (C++ restatement, one thread, SuperLU), with the
+    Newton iteration counts of every step."""
+    import oracle
+    import torch
+    from oracle.driver import OracleSolver
+    from pmsim_b200.batch import BatchSolver
+    from pmsim_b200.elements import Elements
+    from pmsim_b200.footing import footing_problem
+    from pmsim_b200.solver import SolverImplicit
+    p = footing_problem(20, 10, 1e4, 9.0, 1.0, nsteps=10)
+    el = Elements(p.mesh, p.material, ngauss=9)
+    sol = SolverImplicit(el, p.essential, n_max_iterations=20, t_fin=10.0)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    sol.solve()
+    t_dropin = time.perf_counter() - t0
+    it_dropin = [len(h) for h in sol.history]
+    el.close()
+    bs = BatchSolver([p], n_max_iterations=20)
+    t0 = time.perf_counter()
+    bs.solve_independent(on_fail="raise")
+    torch.cuda.synchronize()
+    t_dev = time.perf_counter() - t0
+    it_dev = list(bs.history[0])
+    bs.close()
+    mt = p.material
+    oel = oracle.OracleElements(p.mesh, 1, oracle.Params(mt.young, mt.poisson, mt.hh, mt.z_ini), ngauss=9,
+                                sym_tol=-1.0, nthreads=1)
+    osol = OracleSolver(oel, p.mesh.ndof, p.essential, n_max_iterations=20, t_fin=10.0)
+    t0 = time.perf_counter()
+    osol.solve()
+    t_cpu = time.perf_counter() - t0
+    it_cpu = [len(h) for h in osol.history]
+    return {"workload": "footing 20x10 Qua8, 9 IP, 1322 DOF, 10 steps (LMM)", "dropin_s": t_dropin,
+            "device_newton_pcg_s": t_dev, "oracle_cpu_1thread_s": t_cpu, "iterations_dropin": it_dropin,
+            "iterations_device": it_dev, "iterations_oracle": it_cpu,
+            "dropin_elements_s": sol.timing["elements"], "dropin_solve_s": sol.timing["solve"]}
+
+
 def run_served(nreq, rate, nalone, seed=7):
     """Served configuration: Poisson arrivals (rate req/s) of footing (70%, 1k-50k DOF) and Hex8
     block (30%, up to 206,763 DOF) requests, 10 load steps each, admitted under a 120 GB device
@@ -369,10 +412,10 @@ def main():
         reference_arm(args, rank)
         return
     import torch
-    import torch.distributed as dist
+    from pmsim_b200 import dist
     if world > 1:
         torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+        dist.init("nccl", timeout_s=120)
     from pmsim_b200 import _lib
     from pmsim_b200.elements import Elements, Material
     L = _lib.load()
@@ -390,9 +433,7 @@ def main():
     el.initialize_internal_values()
     el.backup_secondary_values()
 
-    def barrier():
-        if world > 1:
-            dist.barrier()
+    barrier = dist.barrier
 
     # warm-up
     for _ in range(args.warmup):
@@ -424,11 +465,7 @@ def main():
     L.pms_elements_kernel_times(el.h, _lib.ptr(kt), _lib.ptr(kc))
     L.pms_elements_set_timing(el.h, 0)
     el.sync()
-    ms_max = ms
-    if world > 1:
-        t = torch.tensor([ms], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_max = float(t.item())
+    ms_max = dist.max_over_ranks(ms, dev)
     nip = m.ncell * ng
     value = world * nip / (ms_max * 1e-3)
 
@@ -443,18 +480,13 @@ def main():
         t0 = time.perf_counter()
         for _ in range(args.steps):
             el.update_and_assemble(h_ddu, h_ff, h_csr)
-        t_e2e = (time.perf_counter() - t0) / args.steps
-        if world > 1:
-            t = torch.tensor([t_e2e], device=dev, dtype=torch.float64)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            t_e2e = float(t.item())
+        t_e2e = dist.max_over_ranks((time.perf_counter() - t0) / args.steps, dev)
         e2e = {"value": world * nip / t_e2e, "unit": "IP/s", "h2d_bytes_per_step": ndof * 8,
                "d2h_bytes_per_step": (ndof + nnz) * 8, "ms_per_step": t_e2e * 1e3}
         del h_csr
 
     if world > 1:
-        dist.barrier()
-        dist.destroy_process_group()
+        dist.finalize()
     if rank != 0:
         return
 
@@ -472,6 +504,9 @@ def main():
     if args.batched > 0 and args.size == "full":
         torch.cuda.empty_cache()
         batched = run_batched(args.batched, args.alone_sample)
+    c0 = None
+    if not args.no_c0 and args.size == "full":
+        c0 = run_c0()
     served = None
     if args.served > 0 and args.size == "full":
         torch.cuda.empty_cache()
@@ -513,7 +548,7 @@ def main():
         "kernels_ms_per_step": {"element": ms_elem, "f_gather": kt[1] / max(kc[1], 1),
                                 "kk_gather": kt[2] / max(kc[2], 1)},
         "gpu_launches": int(launches),
-        "e2e": e2e, "cpu_baseline": cpu, "k1_microbench": k1, "batched": batched, "served": served, "fp64_peak_tflops": fp64,
+        "e2e": e2e, "cpu_baseline": cpu, "k1_microbench": k1, "batched": batched, "served": served, "c0_footing": c0, "fp64_peak_tflops": fp64,
         "clocks": clk,
     }
     print(json.dumps(line), flush=True)

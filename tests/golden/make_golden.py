@@ -10,7 +10,8 @@ Sources (paths inside the pmsim project):
   * data/spo/test_von_mises_2x2_elements_2d_ref.json     (HYPLAS, Qua8 4 IP, 5 steps)
   * data/spo/spo_754_footing_ref.json + spo_754_footing.msh (HYPLAS, Qua8 4 IP, 14 steps)
   * data/spo/spo_755_tensile_perf_plast_ref.json + spo_755_tensile.msh (Qua8 4 IP, 15 steps)
-  * data/results/artificial/*.json, *.msh  (pmsim's own FemState output, uniform fields)
+  * data/results/artificial/*.json, *.msh  (pmsim's own FemState output, uniform fields; the
+    raw files are kept as femstate_*.json for the byte-level checkpoint test)
   * tests/test_solid_smith_5d11_qua4_plane_strain_uy.rs (inline expected displacements) and
     src/base/sample_meshes.rs (smith_example_5d11_qua4, smith_example_5d24_hex20 meshes)
 """
@@ -91,6 +92,13 @@ def main(ref):
     artificial(ref, "artificial-elastic-2d-qua8", "artificial_2d_qua8.npz")
     artificial(ref, "artificial-elastic-2d", "artificial_2d_tri3.npz")
     artificial(ref, "artificial-elastic-3d", "artificial_3d_hex8.npz")
+    # raw FemState files written by pmsim itself (byte-level checkpoint compatibility)
+    import shutil
+    for stem in ("artificial-elastic-2d-qua8", "artificial-elastic-3d"):
+        for i in range(3):
+            src = os.path.join(ref, "data/results/artificial", f"{stem}-{i:020d}.json")
+            shutil.copyfile(src, os.path.join(HERE, f"femstate_{stem}_{i}.json"))
+    print("copied FemState json files")
     coords, conn, kind = rust_mesh(ref, "smith_example_5d11_qua4")
     uu = rust_array(os.path.join(ref, "tests/test_solid_smith_5d11_qua4_plane_strain_uy.rs"), "uu_correct")
     np.savez_compressed(os.path.join(HERE, "smith_5d11_qua4.npz"), coords=coords, cells=conn, kind=np.array(kind),

@@ -158,3 +158,20 @@ def test_errors_are_reported_with_location():
         g.assemble_kk()
     assert "Jacobian" in str(ei.value)
     assert g.error_location()[0] == 1
+
+
+def test_femstate_checkpoint_round_trip_on_device():
+    """Export the device IP state in pmsim's FemState JSON layout and import it into a fresh handle."""
+    from pmsim_b200 import state_io
+    m, g, o = make(M.QUA8, seed=12)
+    ddu = plastic_ddu(m, seed=12)
+    g.initialize_internal_values()
+    g.update_secondary_values(ddu)
+    text = state_io.export_state(g, u=ddu, ddu=ddu, t=1.0)
+    from pmsim_b200.elements import Elements, Material
+    h = Elements(m, Material.von_mises(E, NU, H, Z0))
+    u, du, t = state_io.import_state(h, text)
+    assert t == 1.0 and np.array_equal(u, ddu)
+    for a, b in zip(g.get_state(), h.get_state()):
+        assert np.array_equal(a, b)
+    assert state_io.export_state(h, u=u, ddu=du, t=t) == text
