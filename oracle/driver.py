@@ -30,7 +30,7 @@ class OracleSolver:
 
     def __init__(self, elements, ndof, essential, loads=(), lagrange_mult_method=True, n_max_iterations=10,
                  tol_rr_abs=1e-10, tol_mdu_rel=1e-8, t_ini=0.0, t_fin=1.0, ddt=1.0, constant_tangent=False,
-                 linear_problem=False):
+                 linear_problem=False, ff_ext_fn=None):
         self.el = elements
         self.ndof = ndof
         # Essential is a map keyed by (point, dof) (src/base/essential.rs:22): a later entry
@@ -43,6 +43,7 @@ class OracleSolver:
         self.consts = [e[1] for e in ess]
         self.fns = [e[2] for e in ess]
         self.loads = list(loads)
+        self.ff_ext_fn = ff_ext_fn  # t -> F_ext over the DOFs (distributed loads), or None
         self.lmm = lagrange_mult_method
         if not self.lmm and any(c != 0.0 for c in self.consts):
             raise NewtonError("the Lagrange multiplier method is required for non-zero prescribed values")
@@ -66,10 +67,12 @@ class OracleSolver:
         f = self.fns[p]
         return self.consts[p] * f(t) if f is not None else self.consts[p]
 
-    def _ff_ext(self):
+    def _ff_ext(self, t):
         ff = np.zeros(self.neq_total)
         for eq, v in self.loads:
             ff[eq] += v
+        if self.ff_ext_fn is not None:
+            ff[: self.ndof] += self.ff_ext_fn(t)
         return ff
 
     def solve(self, on_step=None):
@@ -99,7 +102,7 @@ class OracleSolver:
                     rr[: self.ndof] = fi
                 else:
                     rr[: self.ndof] = np.where(self.flags, 0.0, fi)
-                ffe = self._ff_ext()
+                ffe = self._ff_ext(t)
                 if not self.lmm:
                     ffe[: self.ndof][self.flags] = 0.0
                 rr -= ell * ffe

@@ -56,7 +56,7 @@ class Essential:
 
 class SolverImplicit:
     def __init__(self, elements: Elements, essential, loads=(), lagrange_mult_method=True, n_max_iterations=10,
-                 tol_rr_abs=1e-10, tol_mdu_rel=1e-8, t_ini=0.0, t_fin=1.0, ddt=1.0, verbose=False):
+                 tol_rr_abs=1e-10, tol_mdu_rel=1e-8, t_ini=0.0, t_fin=1.0, ddt=1.0, verbose=False, natural=None):
         self.el = elements
         self.ndof = elements.ndof
         ess = essential if isinstance(essential, Essential) else Essential.from_list(essential)
@@ -80,12 +80,17 @@ class SolverImplicit:
         self.history = []
         self.timing = {"elements": 0.0, "solve": 0.0}
         self.verbose = verbose
+        self.natural = natural  # object with ff_ext(t) -> F_ext over the DOFs (pmsim_b200.natural.Natural)
+
+    def _ff_ext(self, t):
         ffe = np.zeros(self.neq_total)
         for eq, v in self.loads:
             ffe[eq] += v
+        if self.natural is not None:
+            ffe[: self.ndof] += self.natural.ff_ext(t)
         if not self.lmm:
             ffe[: self.ndof][self.flags] = 0.0
-        self.ff_ext = ffe
+        return ffe
 
     def _bc_values(self, t):
         return np.array([c * fn(t) if fn is not None else c for c, fn in zip(self.consts, self.fns)])
@@ -115,6 +120,7 @@ class SolverImplicit:
             ddu[:] = 0.0
             el.reset_algorithmic_variables()
             c = self._bc_values(t)
+            ff_ext = self._ff_ext(t)
             hist = []
             t0 = time.perf_counter()
             el.assemble_f_int(ff)
@@ -123,7 +129,7 @@ class SolverImplicit:
             mdu0 = None
             converged = False
             for it in range(self.n_max_iterations):
-                rr = -self.ff_ext.copy()
+                rr = -ff_ext.copy()
                 rr[: self.ndof] += np.where(self.flags, 0.0, ff) if not self.lmm else ff
                 if self.lmm:
                     rr[self.eq_p] += u[self.ndof:]

@@ -108,6 +108,25 @@ def main(ref):
     np.savez_compressed(os.path.join(HERE, "smith_5d24_hex20_mesh.npz"), coords=coords, cells=conn,
                         kind=np.array(kind))
     print("wrote smith_5d24_hex20_mesh.npz", coords.shape, conn.shape)
+    # linear-elastic SGM runs with natural boundary conditions: mesh, cell attributes, expected U
+    for fn, test, out in [("smith_example_5d2_tri3", "test_solid_smith_5d2_tri3_plane_strain.rs", "smith_5d2_tri3"),
+                          ("smith_example_5d15_qua8", "test_solid_smith_5d15_qua8_plane_strain.rs",
+                           "smith_5d15_qua8"),
+                          ("smith_example_5d30_tet4", "test_solid_smith_5d30_tet4_3d.rs", "smith_5d30_tet4"),
+                          ("smith_example_5d24_hex20", "test_solid_smith_5d24_hex20_3d.rs", "smith_5d24_hex20"),
+                          ("smith_example_5d27_qua9", "test_solid_smith_5d27_qua9_plane_strain.rs",
+                           "smith_5d27_qua9")]:
+        coords, conn, kind = rust_mesh(ref, fn)
+        src = open(os.path.join(ref, "src/base/sample_meshes.rs")).read()
+        i = src.index(f"pub fn {fn}()")
+        body = src[i:src.index("\n    }\n", i)]
+        attr = np.array([int(a) for a in re.findall(r"Cell\s*\{\s*id:\s*\d+,\s*attribute:\s*(\d+)", body)])
+        uu = rust_array(os.path.join(ref, "tests", test), "uu_correct")
+        np.savez_compressed(os.path.join(HERE, out + ".npz"), coords=coords, cells=conn, kind=np.array(kind),
+                            attribute=attr, uu_correct=uu)
+        print("wrote", out, coords.shape, conn.shape, uu.shape)
+    # SPO 7.5.1 pressurised cylinder (reduced-system method, internal pressure, von Mises)
+    spo(ref, "spo_751_pres_cylin_ref.json", "spo_751_pres_cylin.npz", mesh="data/spo/spo_751_pres_cylin_qua4.msh")
 
 
 if __name__ == "__main__":

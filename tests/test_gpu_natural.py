@@ -1,0 +1,44 @@
+"""Natural boundary conditions through the device element path: the linear-elastic SGM runs
+(tests/test_solid_smith_5d{2,15,27,30,24}_*.rs, two materials in the Hex20 case) and SPO 7.5.1
+(tests/test_spo_751_pres_cylin.rs: reduced-system method, internal pressure, von Mises), each at the
+reference test's tolerance (SPO 7.5.1 stresses: see tests/problems.py) and, for 7.5.1, pmsim's own
+logged Newton iteration counts."""
+import numpy as np
+import pytest
+
+import problems
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("case", problems.SGM_NATURAL)
+def test_sgm_natural_bcs_on_device(case):
+    from pmsim_b200.elements import Elements, Material
+    from pmsim_b200.solver import SolverImplicit
+    pb = problems.sgm_natural(case)
+    mats = [Material.linear_elastic(E, nu) for E, nu in pb["mats"]]
+    el = Elements(pb["mesh"], mats, ngauss=pb["ngauss"], cell_material=pb["cmat"])
+    out = {}
+    SolverImplicit(el, pb["essential"], lagrange_mult_method=False, t_fin=1.0, natural=pb["natural"]).solve(
+        lambda s, t, u, e: out.setdefault("u", u))
+    np.testing.assert_allclose(out["u"], pb["golden"]["uu_correct"], rtol=0, atol=pb["tol"])
+
+
+def test_spo_751_pressurised_cylinder_on_device():
+    from pmsim_b200.elements import Elements, Material
+    from pmsim_b200.solver import SolverImplicit
+    pb = problems.pres_cylin_751()
+    el = Elements(pb["mesh"], Material.von_mises(*pb["params"]), ngauss=4)
+    solver = SolverImplicit(el, pb["essential"], lagrange_mult_method=False, tol_mdu_rel=1e-10,
+                            t_fin=float(pb["nsteps"]), natural=pb["natural"])
+    worst = [0.0, 0.0]
+
+    def cb(step, t, u, e):
+        du, ds = problems.compare_step(pb["golden"], step, u, e.get_state()[0], 4)
+        worst[0] = max(worst[0], du)
+        worst[1] = max(worst[1], ds)
+
+    assert solver.solve(cb) == pb["nsteps"]
+    assert worst[0] <= pb["tol_u"], worst
+    assert worst[1] <= pb["tol_s"], worst
+    assert [len(h) for h in solver.history] == pb["iterations"]

@@ -208,3 +208,38 @@ def test_oracle_fd_jacobian():
         e[j] = h
         Kfd[:, j] = (fint(du + e)[0] - fint(du - e)[0]) / (2 * h)
     assert np.max(np.abs(K - Kfd)) / np.max(np.abs(K)) < 1e-6
+
+
+@pytest.mark.parametrize("case", problems.SGM_NATURAL)
+def test_oracle_sgm_natural_bcs(case):
+    """Distributed and point loads (Natural) with the reduced-system method, linear elastic."""
+    pb = problems.sgm_natural(case)
+    m = pb["mesh"]
+    if pb["cmat"] is None:
+        el = oracle.OracleElements(m, 0, oracle.Params(*pb["mats"][0]), ngauss=pb["ngauss"])
+    else:  # two materials: assemble per material subset (the oracle mesh is homogeneous)
+        pytest.skip("per-cell materials are covered on the device (test_gpu_natural.py)")
+    out = {}
+    solver = OracleSolver(el, m.ndof, pb["essential"], lagrange_mult_method=False, t_fin=1.0,
+                          ff_ext_fn=pb["natural"].ff_ext)
+    solver.solve(lambda step, t, u, el: out.setdefault("u", u))
+    np.testing.assert_allclose(out["u"], pb["golden"]["uu_correct"], rtol=0, atol=pb["tol"])
+
+
+def test_oracle_spo_751_pressurised_cylinder():
+    pb = problems.pres_cylin_751()
+    m = pb["mesh"]
+    el = oracle.OracleElements(m, 1, oracle.Params(*pb["params"]), ngauss=4, sym_tol=-1.0)
+    solver = OracleSolver(el, m.ndof, pb["essential"], lagrange_mult_method=False, tol_mdu_rel=1e-10,
+                          t_fin=float(pb["nsteps"]), ff_ext_fn=pb["natural"].ff_ext)
+    worst = [0.0, 0.0]
+
+    def cb(step, t, u, el):
+        du, ds = problems.compare_step(pb["golden"], step, u, el.sig, 4)
+        worst[0] = max(worst[0], du)
+        worst[1] = max(worst[1], ds)
+
+    assert solver.solve(cb) == pb["nsteps"]
+    assert worst[0] <= pb["tol_u"], worst
+    assert worst[1] <= pb["tol_s"], worst
+    assert [len(h) for h in solver.history] == pb["iterations"]
