@@ -24,7 +24,6 @@ import os
 import statistics
 import subprocess
 import sys
-import tempfile
 import time
 
 import numpy as np
@@ -39,7 +38,7 @@ PEAKS_FALLBACK = {"hbm_gbs": 6650.0}
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=30)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--size", default="full", choices=["small", "medium", "full"],
@@ -106,44 +105,71 @@ def algorithmic_bytes_step(m, ng, nnz):
 
 
 class Clocks:
-    """nvidia-smi sampling during the timed region."""
+    """SM clock and clock-event reasons sampled every ~2 ms by an NVML polling thread (read-only
+    queries); ``mark()`` brackets the timed region and only samples inside it are reported.
+    Falls back to one ``nvidia-smi`` reading when NVML is unavailable."""
 
-    def __init__(self, index):
-        self.f = tempfile.NamedTemporaryFile(prefix="clk", suffix=".csv", delete=False)
-        self.p = None
+    REASONS = {0x4: "sw_power_cap", 0x8: "hw_slowdown", 0x20: "sw_thermal_slowdown", 0x40: "hw_thermal_slowdown",
+               0x80: "hw_power_brake_slowdown"}
+
+    def __init__(self, device):
+        import threading
+        self.samples, self.t0, self.t1, self.h, self.nv = [], None, None, None, None
         try:
-            self.p = subprocess.Popen(
-                ["nvidia-smi", "-i", str(index),
-                 "--query-gpu=clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-                 "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-                 "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
-                 "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+            import pynvml as nv
+            nv.nvmlInit()
+            props = __import__("torch").cuda.get_device_properties(device)
+            bus = f"{props.pci_domain_id:08X}:{props.pci_bus_id:02X}:{props.pci_device_id:02X}.0"
+            self.h = nv.nvmlDeviceGetHandleByPciBusId(bus)
+            self.nv = nv
+            self.max_mhz = float(nv.nvmlDeviceGetMaxClockInfo(self.h, nv.NVML_CLOCK_SM))
         except Exception:
-            self.p = None
+            self.h = None
+        self.stop_flag = threading.Event()
+        self.th = None
+        if self.h is not None:
+            self.th = threading.Thread(target=self._poll, daemon=True)
+            self.th.start()
+
+    def _poll(self):
+        nv = self.nv
+        while not self.stop_flag.is_set():
+            try:
+                mhz = float(nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM))
+                rs = int(nv.nvmlDeviceGetCurrentClocksEventReasons(self.h))
+                self.samples.append((time.perf_counter(), mhz, rs))
+            except Exception:
+                pass
+            time.sleep(0.002)
+
+    def mark(self, start=True):
+        if start:
+            self.t0 = time.perf_counter()
+        else:
+            self.t1 = time.perf_counter()
 
     def stop(self):
-        if self.p is None:
-            return None
-        self.p.terminate()
-        try:
-            self.p.wait(timeout=5)
-        except Exception:
-            self.p.kill()
-        self.f.close()
-        rows = []
-        for line in open(self.f.name):
-            parts = [x.strip() for x in line.split(",")]
-            if len(parts) >= 8:
-                rows.append(parts)
-        os.unlink(self.f.name)
+        if self.th is None:
+            return _smi_clocks()
+        self.stop_flag.set()
+        self.th.join(timeout=5)
+        t1 = self.t1 if self.t1 is not None else float("inf")
+        rows = [(m, r) for t, m, r in self.samples if (self.t0 is None or t >= self.t0) and t <= t1]
         if not rows:
             return None
-        sm = [float(r[0]) for r in rows if r[0].replace(".", "").isdigit()]
-        mx = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[k] for r in rows for k in range(4) if "Active" in r[4 + k] and "Not" not in r[4 + k]})
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(rows)}
+        reasons = sorted({name for _, r in rows for bit, name in self.REASONS.items() if r & bit})
+        return {"sm_mhz": statistics.median(m for m, _ in rows), "sm_max_mhz": self.max_mhz,
+                "sm_min_mhz": min(m for m, _ in rows), "reasons": reasons, "samples": len(rows), "source": "nvml"}
+
+
+def _smi_clocks():
+    try:
+        out = subprocess.run(["nvidia-smi", "--query-gpu=clocks.sm,clocks.max.sm", "--format=csv,noheader,nounits"],
+                             capture_output=True, text=True, timeout=20).stdout.split("\n")[0].split(",")
+        return {"sm_mhz": float(out[0]), "sm_max_mhz": float(out[1]), "reasons": [], "samples": 1,
+                "source": "nvidia-smi after the timed region"}
+    except Exception:
+        return None
 
 
 def measured_peaks():
@@ -446,16 +472,18 @@ def main():
     # timed region: device-resident inputs (every buffer is far larger than the 126 MB L2)
     L.pms_elements_set_timing(el.h, 1)
     L.pms_elements_kernel_times(el.h, None, None)
-    clocks = Clocks(local)
+    clocks = Clocks(dev)
     launches0 = el.launch_count()
     barrier()
     torch.cuda.synchronize(dev)
+    clocks.mark(True)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
     for _ in range(args.steps):
         el.update_and_assemble(d_ddu, d_ff, d_csr)
     e1.record(stream)
     torch.cuda.synchronize(dev)
+    clocks.mark(False)
     barrier()
     clk = clocks.stop()
     launches = el.launch_count() - launches0

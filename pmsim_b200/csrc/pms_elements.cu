@@ -26,9 +26,11 @@
 // FLOPs per IP and pair (3D): 3 (dot) + 9*3 (entries) + 3 (diagonal) = 33 FMA; per node: J^-T
 // dN (9), h = S g (9), three scaled copies (9).
 //
-// Assembly: element blocks go to a scratch buffer ke[cell][pair][nd*nd]; kk_gather_kernel owns
-// each node-pair block (A <= B) with one lane (one warp per block row), sums its contributions
-// in ascending cell order and writes K_AB and K_BA.  No atomics: bit-identical on every run.
+// Assembly: each cell's dense element matrix goes to a scratch buffer ke[cell][NE][NE] (the
+// reference's GenericElement::kke, src/fem/elements.rs:13-14); kk_gather_kernel owns one block
+// row A of K per warp, adds the node-row slabs (a, all b) of the cells incident to A in ascending
+// cell order in shared memory and writes the CSR row once, coalesced.  No atomics: bit-identical
+// on every run.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -72,7 +74,7 @@ struct ElemArgs {
     const double* sig_src; const double* z_src; const double* lam_src; const uint8_t* el_src;
     double* sig; double* z; double* lam; uint8_t* el;
     double* fe;   // [cell][nn][nd]
-    double* ke;   // [cell][npair][nd*nd]
+    double* ke;   // [cell][NE][NE] dense element matrices
     int32_t* status;  // {code, cell, ip, 0}
     const int32_t* cell_prob = nullptr;  // UPD_MODE: problem of each cell
     const uint8_t* pmode = nullptr;      // UPD_MODE: mode of each problem
@@ -419,91 +421,100 @@ __global__ void __launch_bounds__(WPB * 32) element_kernel(ElemArgs A) {
                     }
                 }
             }
+            // the dense element matrix K_e (row-major NE x NE): block (a, b) and its mirror (b, a)
+            double* kc = A.ke + cell * (int64_t)(NE * NE);
 #pragma unroll
             for (int r = 0; r < RT; r++)
 #pragma unroll
                 for (int c = 0; c < CT; c++) {
                     const int a = a0 + r, b = b0 + c;
                     if (a < NN && b < NN && a <= b) {
-                        double* dst = A.ke + (cell * (NN * (NN + 1) / 2) + (a * NN - a * (a - 1) / 2 + (b - a))) * (ND * ND);
 #pragma unroll
                         for (int i = 0; i < ND; i++)
 #pragma unroll
-                            for (int j = 0; j < ND; j++) dst[i * ND + j] = acc[r][c][i][j];
+                            for (int j = 0; j < ND; j++) kc[(a * ND + i) * NE + b * ND + j] = acc[r][c][i][j];
+                        if (a != b) {
+#pragma unroll
+                            for (int j = 0; j < ND; j++)
+#pragma unroll
+                                for (int i = 0; i < ND; i++) kc[(b * ND + j) * NE + a * ND + i] = acc[r][c][i][j];
+                        }
                     }
                 }
         }
     }
 }
 
-// One warp per block row A, one lane per upper block (A, B >= A) of that row: fixed-order sum of
-// its element blocks (ascending cell), written to (A, B) -- consecutive lanes write consecutive
-// blocks of the row -- and, transposed, to (B, A).
-template <int ND>
-__global__ void __launch_bounds__(256) kk_gather_kernel(int64_t npoint, const int64_t* __restrict__ uptr,
-                                                        const int32_t* __restrict__ kdiag,
-                                                        const int64_t* __restrict__ bptr,
-                                                        const int32_t* __restrict__ bcol,
-                                                        const int32_t* __restrict__ u_kba,
-                                                        const int64_t* __restrict__ u_cptr,
-                                                        const int32_t* __restrict__ u_contrib,
-                                                        const double* __restrict__ ke, double* __restrict__ csr) {
-    const int lane = threadIdx.x & 31;
-    const int64_t nwarp = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    for (int64_t Ar = (((int64_t)blockIdx.x * blockDim.x) + threadIdx.x) >> 5; Ar < npoint; Ar += nwarp) {
-        const int64_t u0 = uptr[Ar], nu = uptr[Ar + 1] - u0;
-        const int64_t ba = bptr[Ar], nba = bptr[Ar + 1] - ba;
-        const int kd = kdiag[Ar];
-        for (int64_t t = lane; t < nu; t += 32) {
-            const int64_t u = u0 + t;
-            const int64_t kab = kd + t;
-            const int32_t Bc = bcol[ba + kab];
-            double s[ND * ND];
+// One warp per block row A of K.  Lanes form G = 32/NN groups of NN lanes; lane (g, b) of round r
+// loads, for incidence k = k0 + r*G + g of A (cell c, local index a), the ND x ND block (a, b) of
+// c's dense element matrix -- the NN lanes of a group read one contiguous node-row slab -- and
+// adds it at column slot[k*NN + b] of the row buffer in shared memory.  The adds go group by group
+// and round by round, i.e. in ascending incidence (= ascending cell) order, so every entry of K is
+// the fixed-order sum over its cells.  The buffer holds the row in CSR order and is written out
+// coalesced.  Rows of problems whose mode is 0 are skipped (per-problem batches).
+template <int ND, int NN>
+__global__ void __launch_bounds__(256) kk_gather_kernel(int64_t npoint, int nbmax, const int64_t* __restrict__ bptr,
+                                                        const int64_t* __restrict__ inc_ptr,
+                                                        const int32_t* __restrict__ inc,
+                                                        const int16_t* __restrict__ slot,
+                                                        const double* __restrict__ ke, double* __restrict__ csr,
+                                                        const int32_t* __restrict__ node_prob,
+                                                        const uint8_t* __restrict__ pmode) {
+    constexpr int NE = NN * ND, BB = ND * ND;
+    constexpr int G = NN >= 32 ? 1 : 32 / NN;          // incidences per round
+    constexpr int NB = G >= 8 ? 1 : (G >= 3 ? 2 : 4);  // rounds loaded before they are added
+    extern __shared__ double rowbuf[];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, wpb = blockDim.x >> 5;
+    double* buf = rowbuf + (int64_t)wid * nbmax * BB;
+    const int g = lane / NN, b = lane - (lane / NN) * NN;
+    const bool lane_on = g < G;
+    const int64_t nwarp = (int64_t)gridDim.x * wpb;
+    for (int64_t A = (int64_t)blockIdx.x * wpb + wid; A < npoint; A += nwarp) {
+        if (pmode && pmode[node_prob[A]] == 0) continue;  // warp-uniform
+        const int64_t ba = bptr[A];
+        const int nba = (int)(bptr[A + 1] - ba);
+        const int nrow = ND * nba;
+        for (int t = lane; t < nba * BB; t += 32) buf[t] = 0.0;
+        const int64_t k0 = inc_ptr[A], k1 = inc_ptr[A + 1];
+        for (int64_t kb = k0; kb < k1; kb += G * NB) {
+            double v[NB][BB];
+            int pos[NB];
 #pragma unroll
-            for (int i = 0; i < ND * ND; i++) s[i] = 0.0;
-            const int64_t c0 = u_cptr[u], c1 = u_cptr[u + 1];
-            // batches of GB contributions: all codes, then all blocks in flight, then the ordered sum
-            constexpr int GB = 4;
-            for (int64_t cb = c0; cb < c1; cb += GB) {
-                uint32_t code[GB];
+            for (int r = 0; r < NB; r++) {
+                const int64_t k = kb + r * G + g;
+                pos[r] = -1;
+                if (lane_on && k < k1) {
+                    const int32_t code = __ldg(inc + k);
+                    const int64_t cell = code / NN;
+                    const int a = code - (int)cell * NN;
+                    pos[r] = __ldg(slot + k * NN + b);
+                    const double* src = ke + (cell * NE + a * ND) * NE + b * ND;
 #pragma unroll
-                for (int k = 0; k < GB; k++) code[k] = (cb + k < c1) ? (uint32_t)__ldg(u_contrib + cb + k) : 0u;
-                double v[GB][ND * ND];
+                    for (int i = 0; i < ND; i++)
 #pragma unroll
-                for (int k = 0; k < GB; k++) {
-                    const double* blk = ke + (int64_t)(code[k] & 0x7fffffffu) * (ND * ND);
+                        for (int j = 0; j < ND; j++) v[r][i * ND + j] = __ldg(src + i * NE + j);
+                } else {
 #pragma unroll
-                    for (int i = 0; i < ND * ND; i++) v[k][i] = (cb + k < c1) ? __ldg(blk + i) : 0.0;
+                    for (int i = 0; i < BB; i++) v[r][i] = 0.0;
                 }
+            }
 #pragma unroll
-                for (int k = 0; k < GB; k++) {
-                    if (cb + k < c1) {
-                        if (code[k] & 0x80000000u) {
+            for (int r = 0; r < NB; r++)
 #pragma unroll
-                            for (int i = 0; i < ND; i++)
+                for (int gg = 0; gg < G; gg++) {
+                    __syncwarp();
+                    if (g == gg && pos[r] >= 0) {
 #pragma unroll
-                                for (int j = 0; j < ND; j++) s[i * ND + j] += v[k][j * ND + i];
-                        } else {
+                        for (int i = 0; i < ND; i++)
 #pragma unroll
-                            for (int i = 0; i < ND * ND; i++) s[i] += v[k][i];
-                        }
+                            for (int j = 0; j < ND; j++) buf[i * nrow + pos[r] * ND + j] += v[r][i * ND + j];
                     }
                 }
-            }
-            const int64_t posAB = (int64_t)ND * ND * ba + kab * ND;
-#pragma unroll
-            for (int i = 0; i < ND; i++)
-#pragma unroll
-                for (int j = 0; j < ND; j++) csr[posAB + i * ND * nba + j] = s[i * ND + j];
-            if (Bc != Ar) {
-                const int64_t bb = bptr[Bc], nbb = bptr[Bc + 1] - bb;
-                const int64_t posBA = (int64_t)ND * ND * bb + (int64_t)u_kba[u] * ND;
-#pragma unroll
-                for (int i = 0; i < ND; i++)
-#pragma unroll
-                    for (int j = 0; j < ND; j++) csr[posBA + j * ND * nbb + i] = s[i * ND + j];
-            }
         }
+        __syncwarp();
+        double* dst = csr + (int64_t)BB * ba;
+        for (int t = lane; t < nba * BB; t += 32) dst[t] = buf[t];
+        __syncwarp();
     }
 }
 
@@ -547,7 +558,8 @@ __global__ void zero_lambda_kernel(int64_t nip, double* lam) {
 
 // ------------------------------------------------------------------------------- handle
 struct pms_elements {
-    int nd = 0, kind = 0, nn = 0, ng = 0, nc = 0, npair = 0;
+    int nd = 0, kind = 0, nn = 0, ng = 0, nc = 0;
+    int gather_wpb = 8, gather_smem = 0;  // rows (warps) per block and shared memory of kk_gather
     int64_t npoint = 0, ncell = 0, ndof = 0, nip = 0, nnz = 0;
     double thickness = 1.0;
     std::vector<MatConst> mats;
@@ -569,9 +581,8 @@ struct pms_elements {
     int32_t* d_inc = nullptr;
     int64_t* d_bptr = nullptr;
     int32_t* d_bcol = nullptr;
-    int64_t* d_uptr = nullptr;
-    int32_t *d_kdiag = nullptr, *d_ukba = nullptr, *d_ucontrib = nullptr;
-    int64_t* d_ucptr = nullptr;
+    int32_t* d_kdiag = nullptr;
+    int16_t* d_slot = nullptr;
     double *d_ddu = nullptr, *d_ff = nullptr, *d_csr = nullptr;  // staging for host-memory calls
     int64_t* d_indptr = nullptr;  // device CSR pattern (built on first request)
     int32_t* d_indices = nullptr;
@@ -736,15 +747,31 @@ ElemArgs make_args(pms_elements* h, const double* ddu) {
     return a;
 }
 
-void launch_kk_gather(pms_elements* h, double* csr) {
-    const int64_t np = h->npoint;
-    const int blocks = (int)std::min<int64_t>((np + 7) / 8, 148 * 32);  // 8 warps (rows) per block
-    if (h->nd == 2)
-        kk_gather_kernel<2><<<blocks, 256, 0, h->stream>>>(np, h->d_uptr, h->d_kdiag, h->d_bptr, h->d_bcol, h->d_ukba,
-                                                            h->d_ucptr, h->d_ucontrib, h->d_ke, csr);
-    else
-        kk_gather_kernel<3><<<blocks, 256, 0, h->stream>>>(np, h->d_uptr, h->d_kdiag, h->d_bptr, h->d_bcol, h->d_ukba,
-                                                            h->d_ucptr, h->d_ucontrib, h->d_ke, csr);
+template <int ND, int NN>
+void launch_kk_gather_t(pms_elements* h, double* csr, const int32_t* node_prob, const uint8_t* pmode) {
+    auto kern = kk_gather_kernel<ND, NN>;
+    if (h->gather_smem > 48 * 1024)
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, h->gather_smem);
+    const int64_t np = h->npoint, wpb = h->gather_wpb;
+    const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>((np + wpb - 1) / wpb, 148 * 32));
+    kern<<<blocks, (unsigned)(32 * wpb), h->gather_smem, h->stream>>>(np, h->pat.nbmax, h->d_bptr, h->d_inc_ptr,
+                                                                      h->d_inc, h->d_slot, h->d_ke, csr, node_prob,
+                                                                      pmode);
+}
+
+void launch_kk_gather(pms_elements* h, double* csr, const int32_t* node_prob = nullptr,
+                      const uint8_t* pmode = nullptr) {
+    switch (h->kind) {
+    case PMS_TRI3: launch_kk_gather_t<2, 3>(h, csr, node_prob, pmode); break;
+    case PMS_TRI6: launch_kk_gather_t<2, 6>(h, csr, node_prob, pmode); break;
+    case PMS_QUA4: launch_kk_gather_t<2, 4>(h, csr, node_prob, pmode); break;
+    case PMS_QUA8: launch_kk_gather_t<2, 8>(h, csr, node_prob, pmode); break;
+    case PMS_QUA9: launch_kk_gather_t<2, 9>(h, csr, node_prob, pmode); break;
+    case PMS_TET4: launch_kk_gather_t<3, 4>(h, csr, node_prob, pmode); break;
+    case PMS_TET10: launch_kk_gather_t<3, 10>(h, csr, node_prob, pmode); break;
+    case PMS_HEX8: launch_kk_gather_t<3, 8>(h, csr, node_prob, pmode); break;
+    case PMS_HEX20: launch_kk_gather_t<3, 20>(h, csr, node_prob, pmode); break;
+    }
     h->launches++;
 }
 
@@ -775,7 +802,6 @@ int pms_elements_create(const pms_mesh* mesh, const pms_material* materials, int
     h->nd = mesh->ndim;
     h->nc = 2 * h->nd;
     h->nn = kind_nnode(kind);
-    h->npair = h->nn * (h->nn + 1) / 2;
     h->npoint = mesh->npoint;
     h->ncell = mesh->ncell;
     h->ndof = h->npoint * h->nd;
@@ -827,16 +853,13 @@ int pms_elements_create(const pms_mesh* mesh, const pms_material* materials, int
          h->alloc(&h->d_sig_b, (size_t)h->nip * h->nc) && h->alloc(&h->d_z_b, h->nip) &&
          h->alloc(&h->d_lam_b, h->nip) && h->alloc(&h->d_el_b, h->nip) &&
          h->alloc(&h->d_fe, (size_t)h->ncell * h->nn * h->nd) &&
-         h->alloc(&h->d_ke, (size_t)h->ncell * h->npair * h->nd * h->nd) &&
+         h->alloc(&h->d_ke, (size_t)h->ncell * h->nn * h->nd * h->nn * h->nd) &&
          h->upload(&h->d_inc_ptr, h->pat.inc_ptr.data(), h->pat.inc_ptr.size()) &&
          h->upload(&h->d_inc, h->pat.inc.data(), h->pat.inc.size()) &&
          h->upload(&h->d_bptr, h->pat.bptr.data(), h->pat.bptr.size()) &&
          h->upload(&h->d_bcol, h->pat.bcol.data(), h->pat.bcol.size()) &&
-         h->upload(&h->d_uptr, h->pat.uptr.data(), h->pat.uptr.size()) &&
          h->upload(&h->d_kdiag, h->pat.kdiag.data(), h->pat.kdiag.size()) &&
-         h->upload(&h->d_ukba, h->pat.u_kba.data(), h->pat.u_kba.size()) &&
-         h->upload(&h->d_ucptr, h->pat.u_cptr.data(), h->pat.u_cptr.size()) &&
-         h->upload(&h->d_ucontrib, h->pat.u_contrib.data(), h->pat.u_contrib.size()) &&
+         h->upload(&h->d_slot, h->pat.slot.data(), h->pat.slot.size()) &&
          h->alloc(&h->d_ddu, h->ndof) && h->alloc(&h->d_ff, h->ndof) && h->alloc(&h->d_status, 4);
     if (!ok) {
         delete h;
@@ -849,6 +872,16 @@ int pms_elements_create(const pms_mesh* mesh, const pms_material* materials, int
     }
     h->stream = h->own_stream;
     h->smem_bytes = smem_bytes_for(h->nn, h->nd, h->ng, WPB);
+    {
+        // kk_gather: one row buffer (largest block row) per warp, up to 8 warps and 48 KB per block
+        const int64_t row_bytes = (int64_t)std::max(h->pat.nbmax, 1) * h->nd * h->nd * 8;
+        if (row_bytes > 200 * 1024) {
+            delete h;
+            return PMS_ERR_TOO_LARGE;
+        }
+        h->gather_wpb = (int)std::max<int64_t>(1, std::min<int64_t>(8, (48 * 1024) / row_bytes));
+        h->gather_smem = (int)(h->gather_wpb * row_bytes);
+    }
     // the state starts as LocalState::new: zero stress, elastic, zero internal variables
     init_state_kernel<<<grid_1d(h->nip), 256, 0, h->stream>>>(h->nip, h->nc, h->d_mats, h->d_cmat, h->ng, h->d_sig,
                                                               h->d_z, h->d_lam, h->d_el);
@@ -875,7 +908,7 @@ int pms_elements_get_info(const pms_elements* h, pms_elements_info* o) {
     o->nip = h->nip;
     o->nnz = h->nnz;
     o->nblock_upper = h->pat.nupper();
-    o->ncontrib = (int64_t)h->pat.u_contrib.size();
+    o->ncontrib = h->ncell * h->nn * h->nn;
     o->device_bytes = h->device_bytes;
     return PMS_OK;
 }
@@ -1072,20 +1105,9 @@ int pms_element_calc_jacobian(pms_elements* h, int64_t cell, double* kk) {
     if (!kk) return PMS_ERR_INVALID;
     int rc = one_cell(h, cell, false, true);
     if (rc) return rc;
-    const int nd = h->nd, nn = h->nn, ne = nn * nd;
-    std::vector<double> blk((size_t)h->npair * nd * nd);
-    if (cudaMemcpy(blk.data(), h->d_ke + cell * h->npair * nd * nd, blk.size() * 8, cudaMemcpyDeviceToHost) !=
-        cudaSuccess)
+    const int64_t ne = h->nn * h->nd;
+    if (cudaMemcpy(kk, h->d_ke + cell * ne * ne, (size_t)(ne * ne) * 8, cudaMemcpyDeviceToHost) != cudaSuccess)
         return fail(h, PMS_ERR_CUDA, "copy failed");
-    for (int a = 0; a < nn; a++)
-        for (int b = a; b < nn; b++) {
-            const double* B = blk.data() + (size_t)pair_index(nn, a, b) * nd * nd;
-            for (int i = 0; i < nd; i++)
-                for (int j = 0; j < nd; j++) {
-                    kk[(a * nd + i) * ne + b * nd + j] = B[i * nd + j];
-                    kk[(b * nd + j) * ne + a * nd + i] = B[i * nd + j];
-                }
-        }
     return PMS_OK;
 }
 
@@ -1220,14 +1242,14 @@ int elements_device_pattern(pms_elements* h, const int64_t** indptr, const int32
     return PMS_OK;
 }
 
-int elements_run_modes(pms_elements* h, const int32_t* cell_prob, const uint8_t* pmode, const double* ddu,
-                       double* ff, double* csr) {
+int elements_run_modes(pms_elements* h, const int32_t* cell_prob, const int32_t* node_prob, const uint8_t* pmode,
+                       const double* ddu, double* ff, double* csr) {
     ElemArgs a = make_args(h, ddu);
     a.cell_prob = cell_prob;
     a.pmode = pmode;
     launch_elem(h, a, UPD_MODE, true, true);
     launch_f_gather(h, ff);
-    launch_kk_gather(h, csr);
+    launch_kk_gather(h, csr, node_prob, pmode);
     return cuda_check(h);
 }
 
@@ -1270,7 +1292,7 @@ struct NoallocLayout {
 };
 
 NoallocLayout noalloc_layout(int nn, int nd, int ng, int64_t ncell, bool want_f, bool want_k) {
-    const int nc = 2 * nd, npair = nn * (nn + 1) / 2;
+    const int nc = 2 * nd, ne = nn * nd;
     const int64_t nip = ncell * ng;
     NoallocLayout L;
     size_t o = 0;
@@ -1284,7 +1306,7 @@ NoallocLayout noalloc_layout(int nn, int nd, int ng, int64_t ncell, bool want_f,
     L.lam = o; o += up256(sizeof(double) * (size_t)nip);
     L.el = o; o += up256((size_t)nip);
     L.fe = o; o += want_f ? up256(sizeof(double) * (size_t)ncell * nn * nd) : 0;
-    L.ke = o; o += want_k ? up256(sizeof(double) * (size_t)ncell * npair * nd * nd) : 0;
+    L.ke = o; o += want_k ? up256(sizeof(double) * (size_t)ncell * ne * ne) : 0;
     L.total = o;
     return L;
 }
@@ -1312,7 +1334,7 @@ extern "C" int pms_element_calc_noalloc(int32_t kind, int32_t ngauss, double thi
     if (kind < 0 || kind > 8 || !mat || ncell < 0 || (!f && !kk)) return PMS_ERR_INVALID;
     if (mat->model != PMS_LINEAR_ELASTIC && mat->model != PMS_VON_MISES) return PMS_ERR_INVALID;
     if (mat->model == PMS_VON_MISES && !(mat->z_ini > F_TOL)) return PMS_ERR_INVALID;
-    const int nn = kind_nnode(kind), nd = kind_ndim(kind), nc = 2 * nd, npair = nn * (nn + 1) / 2;
+    const int nn = kind_nnode(kind), nd = kind_ndim(kind), nc = 2 * nd;
     // integration rule and shape table on the stack (no heap): at most 27 x 20 x 3 + 27 doubles
     double ksi_buf[27 * 3], w_buf[27];
     const int ng = integration_rule_into(kind, ngauss, ksi_buf, w_buf);
@@ -1410,36 +1432,16 @@ extern "C" int pms_element_calc_noalloc(int32_t kind, int32_t ngauss, double thi
     }
     if (cudaGetLastError() != cudaSuccess) return PMS_ERR_CUDA;
     const int ne = nn * nd;
-    const size_t packed = (size_t)npair * nd * nd;  // doubles of one cell's upper node-pair blocks
     if (dof && cudaMemcpyAsync(f, base + L.fe, sizeof(double) * (size_t)ncell * ne, cudaMemcpyDeviceToHost, st) !=
                    cudaSuccess)
         return PMS_ERR_CUDA;
-    // packed blocks land at the front of kk and are expanded in place below
-    if (dok && cudaMemcpyAsync(kk, base + L.ke, sizeof(double) * (size_t)ncell * packed, cudaMemcpyDeviceToHost,
+    if (dok && cudaMemcpyAsync(kk, base + L.ke, sizeof(double) * (size_t)ncell * ne * ne, cudaMemcpyDeviceToHost,
                                st) != cudaSuccess)
         return PMS_ERR_CUDA;
     int32_t hst[4] = {0, 0, 0, 0};
     if (cudaMemcpyAsync(hst, base + L.status, 16, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
         cudaStreamSynchronize(st) != cudaSuccess)
         return PMS_ERR_CUDA;
-    if (dok) {
-        // cell c's dense matrix starts at c*ne*ne >= c*packed, so going backwards never overwrites a
-        // packed cell that is still to be expanded; the cell's own blocks are copied aside first
-        double blk[210 * 9];
-        for (int64_t c = ncell - 1; c >= 0; c--) {
-            std::memcpy(blk, kk + (size_t)c * packed, sizeof(double) * packed);
-            double* K = kk + (size_t)c * ne * ne;
-            for (int p = 0; p < nn; p++)
-                for (int q = p; q < nn; q++) {
-                    const double* B = blk + (size_t)pair_index(nn, p, q) * nd * nd;
-                    for (int i = 0; i < nd; i++)
-                        for (int j = 0; j < nd; j++) {
-                            K[(p * nd + i) * ne + q * nd + j] = B[i * nd + j];
-                            K[(q * nd + j) * ne + p * nd + i] = B[i * nd + j];
-                        }
-                }
-        }
-    }
     switch (hst[0]) {
     case 0: return PMS_OK;
     case E_ZERO_NORM_S: return PMS_ERR_ZERO_NORM_S;

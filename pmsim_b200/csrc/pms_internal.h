@@ -22,9 +22,10 @@ ElementsView elements_view(pms_elements* h);
 int elements_device_pattern(pms_elements* h, const int64_t** indptr, const int32_t** indices);
 
 // One launch of the element kernel in per-problem mode (0 skip, 1 step start, 2 update) followed by
-// the F_int and CSR gathers; all pointers are device pointers on the handle's stream.
-int elements_run_modes(pms_elements* h, const int32_t* cell_prob, const uint8_t* pmode, const double* ddu,
-                       double* ff, double* csr);
+// the F_int and CSR gathers (the CSR rows of mode-0 problems are left as they are); all pointers
+// are device pointers on the handle's stream.
+int elements_run_modes(pms_elements* h, const int32_t* cell_prob, const int32_t* node_prob, const uint8_t* pmode,
+                       const double* ddu, double* ff, double* csr);
 
 // Sets lambda = 0 ... not needed: mode 1 resets it.  Status of the last launches (syncs the stream).
 int elements_status(pms_elements* h);

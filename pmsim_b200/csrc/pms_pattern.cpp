@@ -10,39 +10,32 @@
 namespace pms {
 
 namespace {
-struct Item {
-    int32_t B;
-    int32_t cell;
-    int16_t a, b;
-};
-
-// all (B, cell, a, b) for the incidences of node A, sorted by (B, cell)
-void row_items(const Pattern& p, const int64_t* conn, int64_t A, std::vector<Item>& it) {
-    it.clear();
+// sorted, unique neighbour nodes of A (the nodes of its incident cells)
+void row_nodes(const Pattern& p, const int64_t* conn, int64_t A, std::vector<int32_t>& cols) {
+    cols.clear();
     for (int64_t k = p.inc_ptr[A]; k < p.inc_ptr[A + 1]; k++) {
-        int32_t code = p.inc[k];
-        int32_t cell = code / p.nn;
-        int16_t a = (int16_t)(code % p.nn);
-        const int64_t* c = conn + (int64_t)cell * p.nn;
-        for (int b = 0; b < p.nn; b++) it.push_back(Item{(int32_t)c[b], cell, a, (int16_t)b});
+        const int64_t cell = p.inc[k] / p.nn;
+        const int64_t* c = conn + cell * p.nn;
+        for (int b = 0; b < p.nn; b++) cols.push_back((int32_t)c[b]);
     }
-    std::sort(it.begin(), it.end(), [](const Item& x, const Item& y) {
-        if (x.B != y.B) return x.B < y.B;
-        if (x.cell != y.cell) return x.cell < y.cell;
-        if (x.a != y.a) return x.a < y.a;
-        return x.b < y.b;
-    });
+    std::sort(cols.begin(), cols.end());
+    cols.erase(std::unique(cols.begin(), cols.end()), cols.end());
 }
 }  // namespace
+
+int64_t Pattern::nupper() const {
+    int64_t n = 0;
+    for (int64_t A = 0; A < npoint; A++)
+        for (int64_t k = bptr[A]; k < bptr[A + 1]; k++) n += bcol[k] >= A;
+    return n;
+}
 
 bool build_pattern(int nd, int nn, int64_t npoint, int64_t ncell, const int64_t* conn, Pattern& p, const char** msg) {
     p.nd = nd;
     p.nn = nn;
-    p.npair = nn * (nn + 1) / 2;
     p.npoint = npoint;
     p.ncell = ncell;
-    if (npoint >= (int64_t)1 << 31 || ncell * (int64_t)nn >= (int64_t)1 << 31 ||
-        ncell * (int64_t)p.npair >= (int64_t)1 << 31) {
+    if (npoint >= (int64_t)1 << 31 || ncell * (int64_t)nn >= (int64_t)1 << 31) {
         *msg = "mesh too large for 31-bit gather codes";
         return false;
     }
@@ -61,83 +54,49 @@ bool build_pattern(int nd, int nn, int64_t npoint, int64_t ncell, const int64_t*
         for (int64_t e = 0; e < ncell; e++)
             for (int a = 0; a < nn; a++) p.inc[pos[conn[e * nn + a]]++] = (int32_t)(e * nn + a);
     }
-    // pass 1: counts per block row
-    std::vector<int64_t> nb(npoint, 0), nu(npoint, 0), nc(npoint, 0);
+    // pass 1: block row lengths
+    std::vector<int64_t> nb(npoint, 0);
 #pragma omp parallel
     {
-        std::vector<Item> it;
+        std::vector<int32_t> cols;
 #pragma omp for schedule(dynamic, 256)
         for (int64_t A = 0; A < npoint; A++) {
-            row_items(p, conn, A, it);
-            int64_t cb = 0, cu = 0, cc = 0;
-            for (size_t k = 0; k < it.size(); k++) {
-                bool first = (k == 0 || it[k].B != it[k - 1].B);
-                if (first) cb++;
-                if (it[k].B >= A) {
-                    if (first) cu++;
-                    cc++;
-                }
-            }
-            nb[A] = cb;
-            nu[A] = cu;
-            nc[A] = cc;
+            row_nodes(p, conn, A, cols);
+            nb[A] = (int64_t)cols.size();
         }
     }
     p.bptr.assign(npoint + 1, 0);
-    std::vector<int64_t> uptr(npoint + 1, 0), cptr(npoint + 1, 0);
+    int64_t mx = 0;
     for (int64_t A = 0; A < npoint; A++) {
         p.bptr[A + 1] = p.bptr[A] + nb[A];
-        uptr[A + 1] = uptr[A] + nu[A];
-        cptr[A + 1] = cptr[A] + nc[A];
+        mx = std::max(mx, nb[A]);
     }
+    if (mx > 32767) {
+        *msg = "a block row of the matrix has more than 32767 node blocks";
+        return false;
+    }
+    p.nbmax = (int)mx;
     p.bcol.assign(p.bptr[npoint], 0);
-    int64_t NU = uptr[npoint], NC = cptr[npoint];
-    p.u_row.assign(NU, 0);
-    p.u_kab.assign(NU, 0);
-    p.u_kba.assign(NU, 0);
-    p.u_col.assign(NU, 0);
-    p.u_cptr.assign(NU + 1, 0);
-    p.u_contrib.assign(NC, 0);
-    // pass 2: fill
+    p.kdiag.assign(npoint, 0);
+    p.slot.assign((size_t)ncell * nn * nn, 0);
+    // pass 2: columns, diagonal positions and the slot map
 #pragma omp parallel
     {
-        std::vector<Item> it;
+        std::vector<int32_t> cols;
 #pragma omp for schedule(dynamic, 256)
         for (int64_t A = 0; A < npoint; A++) {
-            row_items(p, conn, A, it);
-            int64_t kb = p.bptr[A] - 1, ku = uptr[A] - 1, kc = cptr[A];
-            for (size_t k = 0; k < it.size(); k++) {
-                const Item& x = it[k];
-                bool first = (k == 0 || x.B != it[k - 1].B);
-                if (first) p.bcol[++kb] = x.B;
-                if (x.B >= A) {
-                    if (first) {
-                        ++ku;
-                        p.u_row[ku] = (int32_t)A;
-                        p.u_col[ku] = x.B;
-                        p.u_kab[ku] = (int32_t)(kb - p.bptr[A]);
-                        p.u_cptr[ku] = kc;
-                    }
-                    int a = x.a, b = x.b;
-                    bool tr = a > b;
-                    int q = tr ? pair_index(nn, b, a) : pair_index(nn, a, b);
-                    uint32_t code = (uint32_t)((int64_t)x.cell * p.npair + q) | (tr ? 0x80000000u : 0u);
-                    p.u_contrib[kc++] = (int32_t)code;
-                }
+            row_nodes(p, conn, A, cols);
+            std::copy(cols.begin(), cols.end(), p.bcol.begin() + p.bptr[A]);
+            auto it = std::lower_bound(cols.begin(), cols.end(), (int32_t)A);
+            p.kdiag[A] = (it != cols.end() && *it == A) ? (int32_t)(it - cols.begin()) : 0;
+            for (int64_t k = p.inc_ptr[A]; k < p.inc_ptr[A + 1]; k++) {
+                const int64_t cell = p.inc[k] / nn;
+                const int64_t* c = conn + cell * nn;
+                for (int b = 0; b < nn; b++)
+                    p.slot[(size_t)k * nn + b] =
+                        (int16_t)(std::lower_bound(cols.begin(), cols.end(), (int32_t)c[b]) - cols.begin());
             }
         }
-    }
-    p.u_cptr[NU] = NC;
-    p.uptr = uptr;
-    p.kdiag.assign(npoint, 0);
-    for (int64_t A = 0; A < npoint; A++) p.kdiag[A] = (uptr[A + 1] > uptr[A]) ? p.u_kab[uptr[A]] : 0;
-    // position of A in block row B
-#pragma omp parallel for schedule(static)
-    for (int64_t u = 0; u < NU; u++) {
-        int32_t A = p.u_row[u], B = p.u_col[u];
-        const int32_t* b0 = p.bcol.data() + p.bptr[B];
-        const int32_t* b1 = p.bcol.data() + p.bptr[B + 1];
-        p.u_kba[u] = (int32_t)(std::lower_bound(b0, b1, A) - b0);
     }
     return true;
 }

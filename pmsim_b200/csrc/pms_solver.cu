@@ -692,7 +692,7 @@ int pms_batch_tick(pms_batch* b, const uint8_t* cmd, const double* c_values, int
     zero_masked_kernel<<<grid_of(b->ndof), 256, 0, st>>>(b->S, b->d_upd, b->d_ddu);
     // element pass: step start (assemble with lambda = 0, backup) or stress update + assemble
     cudaMemcpyAsync(b->d_pmode, mode.data(), np, cudaMemcpyHostToDevice, st);
-    int rc = elements_run_modes(b->el, b->d_cell_prob, b->d_pmode, b->d_ddu, b->d_ff, b->d_csr);
+    int rc = elements_run_modes(b->el, b->d_cell_prob, b->d_node_prob, b->d_pmode, b->d_ddu, b->d_ff, b->d_csr);
     if (rc) return rc;
     // residual and its max norm per problem
     cudaMemcpyAsync(b->d_active, running.data(), np, cudaMemcpyHostToDevice, st);

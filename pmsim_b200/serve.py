@@ -22,7 +22,7 @@ from .batch import BatchSolver, Problem
 
 
 def footprint_bytes(problem: Problem) -> int:
-    """Device bytes of a request: CSR values + indices, element-block scratch, gather maps, IP state
+    """Device bytes of a request: CSR values + indices, dense element matrices, gather maps, IP state
     (current + backup) and the solver vectors (from the CSR pattern built on the host)."""
     m = problem.mesh
     L = _lib.load()
@@ -33,9 +33,8 @@ def footprint_bytes(problem: Problem) -> int:
         raise _lib.PmsError(rc)
     nd, nn = m.ndim, m.nnode
     ng = problem.ngauss or 9
-    npair = nn * (nn + 1) // 2
     nip = m.ncell * ng
-    return int(nnz.value * 20 + m.ncell * npair * nd * nd * 8 + nip * (2 * nd * 8 + 24) * 2
+    return int(nnz.value * 20 + m.ncell * (nn * nd) ** 2 * 8 + m.ncell * nn * nn * 2 + nip * (2 * nd * 8 + 24) * 2
                + m.ndof * 8 * 16 + m.ncell * nn * 12 + (64 << 20))
 
 
