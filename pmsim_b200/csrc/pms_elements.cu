@@ -343,17 +343,17 @@ __global__ void __launch_bounds__(WPB * 32) element_kernel(ElemArgs A) {
                     }
                 }
         }
+        const int a0 = ti * RT, b0 = tj * CT;
+        double acc[RT][CT][ND][ND];
+#pragma unroll
+        for (int r = 0; r < RT; r++)
+#pragma unroll
+            for (int c = 0; c < CT; c++)
+#pragma unroll
+                for (int i = 0; i < ND; i++)
+#pragma unroll
+                    for (int j = 0; j < ND; j++) acc[r][c][i][j] = 0.0;
         if (ti >= 0) {
-            const int a0 = ti * RT, b0 = tj * CT;
-            double acc[RT][CT][ND][ND];
-#pragma unroll
-            for (int r = 0; r < RT; r++)
-#pragma unroll
-                for (int c = 0; c < CT; c++)
-#pragma unroll
-                    for (int i = 0; i < ND; i++)
-#pragma unroll
-                        for (int j = 0; j < ND; j++) acc[r][c][i][j] = 0.0;
             for (int p = 0; p < ng; p++) {
                 const double* t = TC + p * 10;
                 const double al = t[0], ga = t[1], be = t[2];
@@ -421,26 +421,43 @@ __global__ void __launch_bounds__(WPB * 32) element_kernel(ElemArgs A) {
                     }
                 }
             }
-            // the dense element matrix K_e (row-major NE x NE): block (a, b) and its mirror (b, a)
-            double* kc = A.ke + cell * (int64_t)(NE * NE);
+        }
+        // write K_e (row-major NE x NE) through the warp's shared memory, RS node rows at a time:
+        // each lane drops its blocks (a, b) and mirrors (b, a) into the staged rows, then the warp
+        // copies the rows out with contiguous stores
+        const int RS = min(NN, smem_warp_doubles(NN, ND, ng) / (ND * NE));
+        double* stage = wbase;
+        double* kc = A.ke + cell * (int64_t)(NE * NE);
+        for (int r0 = 0; r0 < NN; r0 += RS) {
+            __syncwarp();
+            if (ti >= 0) {
 #pragma unroll
-            for (int r = 0; r < RT; r++)
+                for (int r = 0; r < RT; r++)
 #pragma unroll
-                for (int c = 0; c < CT; c++) {
-                    const int a = a0 + r, b = b0 + c;
-                    if (a < NN && b < NN && a <= b) {
+                    for (int c = 0; c < CT; c++) {
+                        const int a = a0 + r, b = b0 + c;
+                        if (a < NN && b < NN && a <= b) {
+                            if (a >= r0 && a < r0 + RS) {
 #pragma unroll
-                        for (int i = 0; i < ND; i++)
+                                for (int i = 0; i < ND; i++)
 #pragma unroll
-                            for (int j = 0; j < ND; j++) kc[(a * ND + i) * NE + b * ND + j] = acc[r][c][i][j];
-                        if (a != b) {
+                                    for (int j = 0; j < ND; j++)
+                                        stage[((a - r0) * ND + i) * NE + b * ND + j] = acc[r][c][i][j];
+                            }
+                            if (a != b && b >= r0 && b < r0 + RS) {
 #pragma unroll
-                            for (int j = 0; j < ND; j++)
+                                for (int j = 0; j < ND; j++)
 #pragma unroll
-                                for (int i = 0; i < ND; i++) kc[(b * ND + j) * NE + a * ND + i] = acc[r][c][i][j];
+                                    for (int i = 0; i < ND; i++)
+                                        stage[((b - r0) * ND + j) * NE + a * ND + i] = acc[r][c][i][j];
+                            }
                         }
                     }
-                }
+            }
+            __syncwarp();
+            const int n = min(RS, NN - r0) * ND * NE;
+            double* dst = kc + (int64_t)r0 * ND * NE;
+            for (int t = lane; t < n; t += 32) dst[t] = stage[t];
         }
     }
 }
@@ -604,6 +621,7 @@ struct pms_elements {
     bool alloc(T** p, size_t count) {
         *p = nullptr;
         if (count == 0) count = 1;
+        std::lock_guard<std::mutex> lock(device_mutex());
         if (cudaMalloc((void**)p, count * sizeof(T)) != cudaSuccess) return false;
         allocs.push_back((void*)*p);
         device_bytes += (int64_t)(count * sizeof(T));
@@ -628,6 +646,7 @@ struct pms_elements {
     }
     ~pms_elements() {
         if (own_stream) cudaStreamSynchronize(own_stream);
+        std::lock_guard<std::mutex> lock(device_mutex());
         for (auto& v : ev_pending)
             for (auto& e : v) ev_pool.push_back(e);
         for (auto& e : ev_pool) {
@@ -1228,6 +1247,11 @@ ElementsView elements_view(pms_elements* h) {
     v.d_kdiag = h->d_kdiag;
     v.stream = h->stream;
     return v;
+}
+
+std::mutex& device_mutex() {
+    static std::mutex m;
+    return m;
 }
 
 int elements_device_pattern(pms_elements* h, const int64_t** indptr, const int32_t** indices) {

@@ -2,11 +2,18 @@
 // Newton/PCG solver (pms_solver.cu).  Not part of the C ABI.
 #pragma once
 #include <cstdint>
+#include <mutex>
 #include <cuda_runtime.h>
 
 #include "../../include/pms.h"
 
 namespace pms {
+
+// Serialises CUDA graph capture against device allocation and release across host threads: a
+// cudaFree (which synchronises the device) issued by one thread while another thread captures a
+// graph would invalidate that capture.  Handles in different threads (served batches) take it
+// around cudaMalloc/cudaFree and around each capture.
+std::mutex& device_mutex();
 
 struct ElementsView {
     int nd, nn, ng;

@@ -447,6 +447,7 @@ struct pms_batch {
     bool alloc(T** p, size_t count) {
         *p = nullptr;
         if (count == 0) count = 1;
+        std::lock_guard<std::mutex> lock(device_mutex());
         if (cudaMalloc((void**)p, count * sizeof(T)) != cudaSuccess) return false;
         allocs.push_back((void*)*p);
         return true;
@@ -457,8 +458,9 @@ struct pms_batch {
         return count == 0 || cudaMemcpy(*p, src, count * sizeof(T), cudaMemcpyHostToDevice) == cudaSuccess;
     }
     ~pms_batch() {
-        if (graph) cudaGraphExecDestroy(graph);
         cudaStreamSynchronize(v.stream);
+        std::lock_guard<std::mutex> lock(device_mutex());
+        if (graph) cudaGraphExecDestroy(graph);
         for (void* p : allocs) cudaFree(p);
     }
 };
@@ -508,6 +510,7 @@ void pcg_iteration(pms_batch* b) {
 int run_pcg(pms_batch* b) {
     cudaStream_t st = b->v.stream;
     if (!b->graph) {
+        std::lock_guard<std::mutex> lock(device_mutex());
         cudaGraph_t g;
         if (cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
             return bfail(b, PMS_ERR_CUDA, "stream capture failed");

@@ -39,9 +39,9 @@ def test_serve_results_same_alone_and_in_mix():
         alone = BatchSolver([r.problem])
         alone.solve_independent(on_fail="drop")
         if r.error is not None:
-            assert 0 in alone.failed
+            assert 0 in alone.failed, f"request {r.rid} failed in the mix ({r.error}) but not alone"
             continue
-        assert not alone.failed
+        assert not alone.failed, f"request {r.rid} failed alone ({alone.failed}) but not in the mix"
         assert np.array_equal(alone.u(), r.u), f"request {r.rid}: U differs alone vs in the mix"
         for x, y in zip(alone.elements.get_state(), r.meta["state"]):
             assert np.array_equal(x, y)
