@@ -52,6 +52,7 @@ def parse():
     ap.add_argument("--served", type=int, default=64, help="requests in the served run (0: skip)")
     ap.add_argument("--rate", type=float, default=200.0, help="Poisson arrival rate of the served run (req/s)")
     ap.add_argument("--no-c0", action="store_true")
+    ap.add_argument("--served-detail", default="", help="write per-request served records (JSON) to this file")
     return ap.parse_args()
 
 
@@ -94,6 +95,12 @@ def flops_per_ip_hex20():
     fma = 20 * 9 * 5 + 210 * 33
     mul = 20 * 9
     return 2 * fma + mul
+
+
+# DRAM bytes (read + write) of one element_kernel<3,20> launch per cell, from the ncu capture of the
+# 32x32x16 block (profiles/element_kernel_hex20_32x32x16.md: 33.6 MB read + 449.1 MB written for
+# 16,384 cells); traffic grows with the cell count, so a launch over n cells moves n times this.
+ELEMENT_DRAM_BYTES_PER_CELL = (33.590272e6 + 449.112320e6) / 16384
 
 
 def algorithmic_bytes_step(m, ng, nnz):
@@ -243,6 +250,9 @@ def run_batched(nprob, nalone, seed=2024):
     t0 = time.perf_counter()
     bs = BatchSolver(probs, n_max_iterations=20, pcg_max_iterations=5000)
     t_setup = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    tuning = bs.autotune()
+    t_tune = time.perf_counter() - t0
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     bs.solve_independent(on_fail="drop")
@@ -288,7 +298,8 @@ def run_batched(nprob, nalone, seed=2024):
     alone = ok_alone / t_alone
     direct = ok_direct / t_direct
     return {"problems": nprob, "converged": nconv, "failed": nfail, "ndof_total": ndof,
-            "seconds": t_batch, "setup_seconds": t_setup, "solves_per_s": batched,
+            "seconds": t_batch, "setup_seconds": t_setup, "autotune_seconds": t_tune, "tuning": tuning,
+            "solves_per_s": batched,
             "newton_iterations_total": int(sum(newton)), "pcg_iterations_total": int(pcg_t.value),
             "attempts_per_s": nprob / t_batch, "alone_attempts_per_s": len(sample) / t_alone,
             "alone_sample": len(sample), "alone_converged": ok_alone, "alone_solves_per_s": alone,
@@ -341,7 +352,7 @@ def run_c0():
             "dropin_elements_s": sol.timing["elements"], "dropin_solve_s": sol.timing["solve"]}
 
 
-def run_served(nreq, rate, nalone, seed=7):
+def run_served(nreq, rate, nalone, seed=7, detail_file=""):
     """Served configuration: Poisson arrivals (rate req/s) of footing (70%, 1k-50k DOF) and Hex8
     block (30%, up to 206,763 DOF) requests, 10 load steps each, admitted under a 120 GB device
     budget into device batches that overlap on the GPU (continuous batching); throughput and
@@ -373,6 +384,11 @@ def run_served(nreq, rate, nalone, seed=7):
         t_alone += time.perf_counter() - t0
         ok += 0 if b1.failed else 1
         b1.close()
+    if detail_file:
+        with open(detail_file, "w") as f:
+            json.dump([{"rid": r.rid, "kind": r.problem.mesh.kind, "ndof": int(r.problem.mesh.ndof),
+                        "arrival": r.arrival, "admitted": r.admitted, "finished": r.finished, "error": r.error,
+                        **r.meta} for r in reqs], f)
     out["alone_sample"] = len(sample)
     out["alone_solves_per_s"] = ok / t_alone if t_alone > 0 else None
     out["ratio_vs_alone"] = (out["solves_per_s"] / out["alone_solves_per_s"]) if ok else None
@@ -538,7 +554,7 @@ def main():
     served = None
     if args.served > 0 and args.size == "full":
         torch.cuda.empty_cache()
-        served = run_served(args.served, args.rate, args.alone_sample)
+        served = run_served(args.served, args.rate, args.alone_sample, detail_file=args.served_detail)
     ms_elem = kt[0] / max(kc[0], 1)
     fl_ip = flops_per_ip_hex20()
     achieved_tf = nip * fl_ip / (ms_elem * 1e-3) / 1e12
@@ -567,7 +583,9 @@ def main():
                    "plastic_fraction": plastic, "l2": "inputs larger than L2 (no flush)",
                    "parallelism": f"replica per GPU x{world}"},
         "roofline": {"bound": "fp64", "achieved": achieved_tf, "peak": fp64, "unit": "TFLOP/s",
-                     "frac": achieved_tf / fp64, "traffic": None,
+                     "frac": achieved_tf / fp64, "traffic": ELEMENT_DRAM_BYTES_PER_CELL * m.ncell,
+                     "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of the 32x32x16 "
+                                       "capture, scaled by cells to this launch",
                      "kernel": "element_kernel<3,20> (fused update + B^T sigma + B^T D B)",
                      "flop_per_ip": fl_ip, "peak_source": "FP64 FMA probe measured in this run"},
         "roofline_hbm": {"bound": "hbm", "achieved": step_gbs, "peak": peaks["hbm_gbs"], "unit": "GB/s",

@@ -199,9 +199,35 @@ int pms_batch_solve_step(pms_batch* b, const double* c_values, const uint8_t* ac
  * its prescribed values), cmd 2 = continue the step (stress update with the current dU, then the
  * next iteration).  result[p]: -1 idle, 0 still iterating (send cmd 2), 1 converged (state and U are
  * the step's solution), 100 + status on failure (status codes as for pms_batch_solve_step).
- * iteration[p] (0-based), norm_rr[p] and pcg_iterations[p] of this tick are optional outputs. */
+ * iteration[p] (0-based), norm_rr[p] and pcg_iterations[p] of this tick are optional outputs.
+ * A tick advances each problem by one stage of its own iteration (element pass and residual test;
+ * PCG iterations; completion of the iteration), so a problem never waits for another problem's
+ * linear solve: result 2 = the problem's linear solve is still under way (send cmd 2 again; no
+ * iteration is completed by this tick). */
 int pms_batch_tick(pms_batch* b, const uint8_t* cmd, const double* c_values, int32_t* result, int32_t* iteration,
                    double* norm_rr, int32_t* pcg_iterations);
+/* Launch shapes of the PCG (they change speed only: both engines compute bit-identical iterates).
+ * Problems with at most block_max_ndof DOFs run their whole PCG in one thread block of
+ * block_threads threads (128, 256, 512 or 1024) at their own pace; larger problems run the
+ * batch-wide kernels, graph_iters iterations per CUDA-graph launch.  pcg_budget bounds the PCG
+ * iterations a problem gets per tick.  No counterpart in the reference (its solve is a direct
+ * factorisation, src/fem/linear_system.rs:185-201). */
+typedef struct pms_batch_tuning {
+    int64_t block_max_ndof;
+    int32_t block_threads;
+    int32_t pcg_budget;
+    int32_t graph_iters;
+} pms_batch_tuning;
+int pms_batch_set_tuning(pms_batch* b, const pms_batch_tuning* t);
+int pms_batch_get_tuning(const pms_batch* b, pms_batch_tuning* t);
+/* Autotuner: times 32 PCG iterations of every problem on its initial tangent (unit right-hand
+ * side) for each candidate engine threshold and block size, keeps the fastest, then resets the
+ * batch (pms_batch_reset).  *out (nullable) receives the choice. */
+int pms_batch_autotune(pms_batch* b, pms_batch_tuning* out);
+/* Instrumentation (the autotuner's measurement): device time in ms of `iterations` PCG iterations
+ * of every problem, on its initial tangent, with the launch shapes *t; resets the batch and keeps
+ * its own tuning. */
+int pms_batch_time_pcg(pms_batch* b, const pms_batch_tuning* t, int32_t iterations, double* ms);
 int pms_batch_get_u(pms_batch* b, double* u);                 /* host u[ndof] */
 int pms_batch_get_multipliers(pms_batch* b, double* lam);     /* host lambda[npres] (reactions) */
 /* kernels launched by the solver (PCG iterations captured in graphs count once per kernel) */

@@ -59,6 +59,11 @@ class BatchConfig_(ctypes.Structure):
                 ("pcg_max_iterations", ctypes.c_int32)]
 
 
+class BatchTuning_(ctypes.Structure):
+    _fields_ = [("block_max_ndof", ctypes.c_int64), ("block_threads", ctypes.c_int32),
+                ("pcg_budget", ctypes.c_int32), ("graph_iters", ctypes.c_int32)]
+
+
 class Info_(ctypes.Structure):
     _fields_ = [("ndim", ctypes.c_int32), ("kind", ctypes.c_int32), ("nnode", ctypes.c_int32),
                 ("ngauss", ctypes.c_int32), ("ncomp", ctypes.c_int32), ("npoint", ctypes.c_int64),
@@ -107,6 +112,10 @@ SIGNATURES = {
     "pms_batch_reset": (_I, [_V]),
     "pms_batch_solve_step": (_I, [_V, _V, _V, _V, _V, _V, _V]),
     "pms_batch_tick": (_I, [_V, _V, _V, _V, _V, _V, _V]),
+    "pms_batch_set_tuning": (_I, [_V, ctypes.POINTER(BatchTuning_)]),
+    "pms_batch_get_tuning": (_I, [_V, ctypes.POINTER(BatchTuning_)]),
+    "pms_batch_autotune": (_I, [_V, ctypes.POINTER(BatchTuning_)]),
+    "pms_batch_time_pcg": (_I, [_V, ctypes.POINTER(BatchTuning_), _I, ctypes.POINTER(_D)]),
     "pms_batch_get_u": (_I, [_V, _V]),
     "pms_batch_get_multipliers": (_I, [_V, _V]),
     "pms_batch_counters": (_I64, [_V, ctypes.POINTER(_I64)]),

@@ -166,9 +166,30 @@ class BatchSolver:
             if on_step is not None:
                 on_step(s, self)
 
+    def tuning(self):
+        t = _lib.BatchTuning_()
+        self._check(self.L.pms_batch_get_tuning(self.h, ctypes.byref(t)))
+        return {k: getattr(t, k) for k, _ in t._fields_}
+
+    def set_tuning(self, **kw):
+        cur = self.tuning()
+        cur.update(kw)
+        t = _lib.BatchTuning_(**cur)
+        self._check(self.L.pms_batch_set_tuning(self.h, ctypes.byref(t)))
+
+    def autotune(self):
+        """Times the PCG launch shapes on this batch (pms_batch_autotune) and keeps the fastest; the
+        iterates do not depend on the choice.  Resets the batch."""
+        t = _lib.BatchTuning_()
+        self._check(self.L.pms_batch_autotune(self.h, ctypes.byref(t)))
+        self.t[:] = 0.0
+        self.step[:] = 0
+        return {k: getattr(t, k) for k, _ in t._fields_}
+
     def tick(self, cmd):
-        """One Newton iteration of every problem with cmd[p] != 0 (1: start its next load step,
-        2: continue).  Returns (result, iteration, norm_rr, pcg_iterations) per problem."""
+        """One stage of the Newton iteration of every problem with cmd[p] != 0 (1: start its next
+        load step, 2: continue).  Returns (result, iteration, norm_rr, pcg_iterations) per problem;
+        result 2 means the problem's linear solve is still under way (send 2 again)."""
         cmd = np.ascontiguousarray(cmd, np.uint8)
         res = np.full(self.np, -1, np.int32)
         it = np.zeros(self.np, np.int32)
@@ -196,10 +217,12 @@ class BatchSolver:
             res, it, norm, pcg = self.tick(cmd)
             self.ticks += 1
             for p in np.nonzero(cmd)[0]:
+                r = int(res[p])
+                if r == 2:  # linear solve still under way
+                    continue
                 counts[p] += 1
                 if pcg[p]:
                     self.pcg_history[p].append(int(pcg[p]))
-                r = int(res[p])
                 if r == 0:
                     cmd[p] = 2
                 elif r == 1:

@@ -78,7 +78,23 @@ struct ElemArgs {
     int32_t* status;  // {code, cell, ip, 0}
     const int32_t* cell_prob = nullptr;  // UPD_MODE: problem of each cell
     const uint8_t* pmode = nullptr;      // UPD_MODE: mode of each problem
+    // work queue (nq > 0): the launch covers ncell queued cells, range k from q_first[k]
+    int32_t nq = 0;
+    const int64_t* q_off = nullptr;
+    const int64_t* q_first = nullptr;
 };
+
+// Item i of a range queue: off[k] <= i < off[k+1] maps to first[k] + (i - off[k]).
+__device__ __forceinline__ int64_t queue_item(int64_t i, int n, const int64_t* __restrict__ off,
+                                              const int64_t* __restrict__ first) {
+    int lo = 0, hi = n;
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (__ldg(off + mid) <= i) lo = mid;
+        else hi = mid;
+    }
+    return __ldg(first + lo) + (i - __ldg(off + lo));
+}
 
 __device__ __forceinline__ void report(int32_t* status, int code, int64_t cell, int ip) {
     if (code == OK) return;
@@ -127,10 +143,11 @@ template <int NN> struct TileShape {
 };
 
 // Shared memory (doubles): block-wide dN table [m][j][32] + w[32], then per warp
-// X[NN*ND], dU[NN*ND], G[ng][NN*ND+1] (gradients), TC[ng][10] (alpha, gamma, beta, S), CS[ng][6].
+// X[NN*ND], dU[NN*ND], G[ng][NN*ND+1] (gradients), TC[ng][10] (alpha, gamma, beta, S), CS[ng][6],
+// V[NN][5*ND] (per node at the current IP: alpha g, gamma g, beta h, g, h with h = S g).
 __host__ __device__ constexpr int smem_table_doubles(int nn, int nd) { return nn * nd * 32 + 32; }
 __host__ __device__ constexpr int smem_warp_doubles(int nn, int nd, int ng) {
-    return 2 * nn * nd + ng * (nn * nd + 1) + ng * 10 + ng * 6;
+    return 2 * nn * nd + ng * (nn * nd + 1) + ng * 10 + ng * 6 + nn * 5 * nd;
 }
 __host__ __device__ constexpr int smem_bytes_for(int nn, int nd, int ng, int wpb) {
     return (smem_table_doubles(nn, nd) + wpb * smem_warp_doubles(nn, nd, ng)) * 8;
@@ -154,6 +171,7 @@ __global__ void __launch_bounds__(WPB * 32) element_kernel(ElemArgs A) {
     double* G = Us + NE;                       // [p][GS]
     double* TC = G + ng * GS;                  // [p][10]
     double* CS = TC + ng * 10;                 // [p][6]
+    double* V = CS + ng * 6;                   // [m][5*ND]
 
     // stage dN transposed (IP index fastest) so that lane p reads its IP without bank conflicts
     for (int i = threadIdx.x; i < ng * NE; i += blockDim.x) {
@@ -165,7 +183,7 @@ __global__ void __launch_bounds__(WPB * 32) element_kernel(ElemArgs A) {
 
     const int64_t cl = (int64_t)blockIdx.x * WPB + wid;
     if (cl >= A.ncell) return;  // whole warp exits together
-    const int64_t cell = A.cell0 + cl;
+    const int64_t cell = A.nq ? queue_item(cl, A.nq, A.q_off, A.q_first) : A.cell0 + cl;
     int mode = (UPD == UPD_NONE) ? 0 : 2;
     if (UPD == UPD_MODE) {
         mode = A.pmode[A.cell_prob[cell]];
@@ -353,9 +371,13 @@ __global__ void __launch_bounds__(WPB * 32) element_kernel(ElemArgs A) {
                 for (int i = 0; i < ND; i++)
 #pragma unroll
                     for (int j = 0; j < ND; j++) acc[r][c][i][j] = 0.0;
-        if (ti >= 0) {
-            for (int p = 0; p < ng; p++) {
-                const double* t = TC + p * 10;
+        constexpr int VS = 5 * ND;
+        for (int p = 0; p < ng; p++) {
+            const double* t = TC + p * 10;
+            const bool plastic = t[2] != 0.0;  // beta: same value on every lane, uniform branch
+            // node lanes: the scaled gradients of their node at this IP
+            __syncwarp();
+            if (lane < NN) {
                 const double al = t[0], ga = t[1], be = t[2];
                 double S[ND][ND];
                 S[0][0] = t[3];
@@ -366,60 +388,79 @@ __global__ void __launch_bounds__(WPB * 32) element_kernel(ElemArgs A) {
                     S[1][2 % ND] = S[2 % ND][1] = t[7];
                     S[0][2 % ND] = S[2 % ND][0] = t[8];
                 }
-                const bool plastic = be != 0.0;  // same value on every lane: uniform branch
-                const double* Gp = G + p * GS;
-                double Ar[RT][ND], Cr[RT][ND], Hr[RT][ND];
+                const double* g = G + p * GS + lane * ND;
+                double* v = V + lane * VS;
+                double gv[ND];
 #pragma unroll
-                for (int r = 0; r < RT; r++) {
-                    const int a = min(a0 + r, NN - 1);
-                    double g[ND];
+                for (int i = 0; i < ND; i++) gv[i] = g[i];
 #pragma unroll
-                    for (int i = 0; i < ND; i++) g[i] = Gp[a * ND + i];
-#pragma unroll
-                    for (int i = 0; i < ND; i++) {
-                        Ar[r][i] = al * g[i];
-                        Cr[r][i] = ga * g[i];
-                        double h = 0.0;
-                        if (plastic) {
-#pragma unroll
-                            for (int j = 0; j < ND; j++) h = fma(S[i][j], g[j], h);
-                        }
-                        Hr[r][i] = be * h;
-                    }
-                }
-#pragma unroll
-                for (int c = 0; c < CT; c++) {
-                    const int b = min(b0 + c, NN - 1);
-                    double gb[ND], hb[ND];
-#pragma unroll
-                    for (int i = 0; i < ND; i++) gb[i] = Gp[b * ND + i];
+                for (int i = 0; i < ND; i++) {
+                    double h = 0.0;
                     if (plastic) {
 #pragma unroll
-                        for (int i = 0; i < ND; i++) {
-                            double h = 0.0;
-#pragma unroll
-                            for (int j = 0; j < ND; j++) h = fma(S[i][j], gb[j], h);
-                            hb[i] = h;
-                        }
+                        for (int j = 0; j < ND; j++) h = fma(S[i][j], gv[j], h);
                     }
+                    v[i] = al * gv[i];
+                    v[ND + i] = ga * gv[i];
+                    v[2 * ND + i] = be * h;
+                    v[3 * ND + i] = gv[i];
+                    v[4 * ND + i] = h;
+                }
+            }
+            __syncwarp();
+            if (ti < 0) continue;
+            double Ar[RT][ND], Cr[RT][ND], Hr[RT][ND];
 #pragma unroll
-                    for (int r = 0; r < RT; r++) {
-                        double dot = 0.0;
+            for (int r = 0; r < RT; r++) {
+                const double* v = V + min(a0 + r, NN - 1) * VS;
 #pragma unroll
-                        for (int k = 0; k < ND; k++) dot = fma(Ar[r][k], gb[k], dot);
+                for (int i = 0; i < ND; i++) {
+                    Ar[r][i] = v[i];
+                    Cr[r][i] = v[ND + i];
+                    Hr[r][i] = v[2 * ND + i];
+                }
+            }
+#pragma unroll
+            for (int c = 0; c < CT; c++) {
+                const double* v = V + min(b0 + c, NN - 1) * VS;
+                double gb[ND], hb[ND];
+#pragma unroll
+                for (int i = 0; i < ND; i++) {
+                    gb[i] = v[3 * ND + i];
+                    hb[i] = v[4 * ND + i];
+                }
+                double dot[RT];
+#pragma unroll
+                for (int r = 0; r < RT; r++) {
+                    dot[r] = 0.0;
+#pragma unroll
+                    for (int k = 0; k < ND; k++) dot[r] = fma(Ar[r][k], gb[k], dot[r]);
+                }
+                // term by term over the tile column (each entry keeps its own operation order)
+#pragma unroll
+                for (int r = 0; r < RT; r++)
+#pragma unroll
+                    for (int i = 0; i < ND; i++)
+#pragma unroll
+                        for (int j = 0; j < ND; j++) acc[r][c][i][j] = fma(Ar[r][j], gb[i], acc[r][c][i][j]);
+#pragma unroll
+                for (int r = 0; r < RT; r++)
+#pragma unroll
+                    for (int i = 0; i < ND; i++)
+#pragma unroll
+                        for (int j = 0; j < ND; j++) acc[r][c][i][j] = fma(Cr[r][i], gb[j], acc[r][c][i][j]);
+                if (plastic) {
+#pragma unroll
+                    for (int r = 0; r < RT; r++)
 #pragma unroll
                         for (int i = 0; i < ND; i++)
 #pragma unroll
-                            for (int j = 0; j < ND; j++) {
-                                double v = acc[r][c][i][j];
-                                v = fma(Ar[r][j], gb[i], v);
-                                v = fma(Cr[r][i], gb[j], v);
-                                if (plastic) v = fma(Hr[r][i], hb[j], v);
-                                if (i == j) v += dot;
-                                acc[r][c][i][j] = v;
-                            }
-                    }
+                            for (int j = 0; j < ND; j++) acc[r][c][i][j] = fma(Hr[r][i], hb[j], acc[r][c][i][j]);
                 }
+#pragma unroll
+                for (int r = 0; r < RT; r++)
+#pragma unroll
+                    for (int i = 0; i < ND; i++) acc[r][c][i][i] += dot[r];
             }
         }
         // write K_e (row-major NE x NE) through the warp's shared memory, RS node rows at a time:
@@ -476,7 +517,9 @@ __global__ void __launch_bounds__(256) kk_gather_kernel(int64_t npoint, int nbma
                                                         const int16_t* __restrict__ slot,
                                                         const double* __restrict__ ke, double* __restrict__ csr,
                                                         const int32_t* __restrict__ node_prob,
-                                                        const uint8_t* __restrict__ pmode) {
+                                                        const uint8_t* __restrict__ pmode, int nq,
+                                                        const int64_t* __restrict__ q_off,
+                                                        const int64_t* __restrict__ q_first, int64_t node0) {
     constexpr int NE = NN * ND, BB = ND * ND;
     constexpr int G = NN >= 32 ? 1 : 32 / NN;          // incidences per round
     constexpr int NB = G >= 8 ? 1 : (G >= 3 ? 2 : 4);  // rounds loaded before they are added
@@ -486,7 +529,8 @@ __global__ void __launch_bounds__(256) kk_gather_kernel(int64_t npoint, int nbma
     const int g = lane / NN, b = lane - (lane / NN) * NN;
     const bool lane_on = g < G;
     const int64_t nwarp = (int64_t)gridDim.x * wpb;
-    for (int64_t A = (int64_t)blockIdx.x * wpb + wid; A < npoint; A += nwarp) {
+    for (int64_t Ai = (int64_t)blockIdx.x * wpb + wid; Ai < npoint; Ai += nwarp) {
+        const int64_t A = nq ? queue_item(Ai, nq, q_off, q_first) : node0 + Ai;
         if (pmode && pmode[node_prob[A]] == 0) continue;  // warp-uniform
         const int64_t ba = bptr[A];
         const int nba = (int)(bptr[A + 1] - ba);
@@ -539,9 +583,12 @@ __global__ void __launch_bounds__(256) kk_gather_kernel(int64_t npoint, int nbma
 template <int ND>
 __global__ void __launch_bounds__(256) f_gather_kernel(int64_t npoint, const int64_t* __restrict__ inc_ptr,
                                                        const int32_t* __restrict__ inc,
-                                                       const double* __restrict__ fe, double* __restrict__ ff) {
-    for (int64_t A = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; A < npoint;
-         A += (int64_t)gridDim.x * blockDim.x) {
+                                                       const double* __restrict__ fe, double* __restrict__ ff,
+                                                       int nq = 0, const int64_t* __restrict__ q_off = nullptr,
+                                                       const int64_t* __restrict__ q_first = nullptr) {
+    for (int64_t Ai = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; Ai < npoint;
+         Ai += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t A = nq ? queue_item(Ai, nq, q_off, q_first) : Ai;
         double s[ND];
 #pragma unroll
         for (int i = 0; i < ND; i++) s[i] = 0.0;
@@ -613,6 +660,10 @@ struct pms_elements {
     int64_t launches = 0;
     int smem_bytes = 0;
     std::vector<void*> allocs;
+    // host-memory calls: the CSR values leave in row slabs on copy_stream while later slabs gather
+    static constexpr int NSLAB = 8;
+    cudaStream_t copy_stream = nullptr;
+    cudaEvent_t slab_ev[NSLAB + 1] = {};
     // optional CUDA-event timing of the three kernels of a batched call
     bool timing = false;
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev_pool, ev_pending[3];
@@ -652,6 +703,12 @@ struct pms_elements {
         for (auto& e : ev_pool) {
             cudaEventDestroy(e.first);
             cudaEventDestroy(e.second);
+        }
+        if (copy_stream) {
+            cudaStreamSynchronize(copy_stream);
+            for (auto& e : slab_ev)
+                if (e) cudaEventDestroy(e);
+            cudaStreamDestroy(copy_stream);
         }
         for (void* p : allocs) cudaFree(p);
         if (own_stream) cudaStreamDestroy(own_stream);
@@ -767,38 +824,45 @@ ElemArgs make_args(pms_elements* h, const double* ddu) {
 }
 
 template <int ND, int NN>
-void launch_kk_gather_t(pms_elements* h, double* csr, const int32_t* node_prob, const uint8_t* pmode) {
+void launch_kk_gather_t(pms_elements* h, double* csr, const int32_t* node_prob, const uint8_t* pmode,
+                        const pms::WorkQueue* q, int64_t node0, int64_t nrows) {
     auto kern = kk_gather_kernel<ND, NN>;
     if (h->gather_smem > 48 * 1024)
         cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, h->gather_smem);
-    const int64_t np = h->npoint, wpb = h->gather_wpb;
+    const int64_t np = q ? q->nnode : (nrows >= 0 ? nrows : h->npoint), wpb = h->gather_wpb;
     const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>((np + wpb - 1) / wpb, 148 * 32));
-    kern<<<blocks, (unsigned)(32 * wpb), h->gather_smem, h->stream>>>(np, h->pat.nbmax, h->d_bptr, h->d_inc_ptr,
-                                                                      h->d_inc, h->d_slot, h->d_ke, csr, node_prob,
-                                                                      pmode);
+    kern<<<blocks, (unsigned)(32 * wpb), h->gather_smem, h->stream>>>(
+        np, h->pat.nbmax, h->d_bptr, h->d_inc_ptr, h->d_inc, h->d_slot, h->d_ke, csr, node_prob, pmode,
+        q ? q->nq : 0, q ? q->node_off : nullptr, q ? q->node_first : nullptr, node0);
 }
 
+// CSR gather of the block rows [node0, node0 + nrows) (nrows < 0: all), or of a work queue
 void launch_kk_gather(pms_elements* h, double* csr, const int32_t* node_prob = nullptr,
-                      const uint8_t* pmode = nullptr) {
+                      const uint8_t* pmode = nullptr, const pms::WorkQueue* q = nullptr, int64_t node0 = 0,
+                      int64_t nrows = -1) {
     switch (h->kind) {
-    case PMS_TRI3: launch_kk_gather_t<2, 3>(h, csr, node_prob, pmode); break;
-    case PMS_TRI6: launch_kk_gather_t<2, 6>(h, csr, node_prob, pmode); break;
-    case PMS_QUA4: launch_kk_gather_t<2, 4>(h, csr, node_prob, pmode); break;
-    case PMS_QUA8: launch_kk_gather_t<2, 8>(h, csr, node_prob, pmode); break;
-    case PMS_QUA9: launch_kk_gather_t<2, 9>(h, csr, node_prob, pmode); break;
-    case PMS_TET4: launch_kk_gather_t<3, 4>(h, csr, node_prob, pmode); break;
-    case PMS_TET10: launch_kk_gather_t<3, 10>(h, csr, node_prob, pmode); break;
-    case PMS_HEX8: launch_kk_gather_t<3, 8>(h, csr, node_prob, pmode); break;
-    case PMS_HEX20: launch_kk_gather_t<3, 20>(h, csr, node_prob, pmode); break;
+    case PMS_TRI3: launch_kk_gather_t<2, 3>(h, csr, node_prob, pmode, q, node0, nrows); break;
+    case PMS_TRI6: launch_kk_gather_t<2, 6>(h, csr, node_prob, pmode, q, node0, nrows); break;
+    case PMS_QUA4: launch_kk_gather_t<2, 4>(h, csr, node_prob, pmode, q, node0, nrows); break;
+    case PMS_QUA8: launch_kk_gather_t<2, 8>(h, csr, node_prob, pmode, q, node0, nrows); break;
+    case PMS_QUA9: launch_kk_gather_t<2, 9>(h, csr, node_prob, pmode, q, node0, nrows); break;
+    case PMS_TET4: launch_kk_gather_t<3, 4>(h, csr, node_prob, pmode, q, node0, nrows); break;
+    case PMS_TET10: launch_kk_gather_t<3, 10>(h, csr, node_prob, pmode, q, node0, nrows); break;
+    case PMS_HEX8: launch_kk_gather_t<3, 8>(h, csr, node_prob, pmode, q, node0, nrows); break;
+    case PMS_HEX20: launch_kk_gather_t<3, 20>(h, csr, node_prob, pmode, q, node0, nrows); break;
     }
     h->launches++;
 }
 
-void launch_f_gather(pms_elements* h, double* ff) {
+void launch_f_gather(pms_elements* h, double* ff, const pms::WorkQueue* q = nullptr) {
+    const int64_t n = q ? q->nnode : h->npoint;
+    const int nq = q ? q->nq : 0;
+    const int64_t* off = q ? q->node_off : nullptr;
+    const int64_t* first = q ? q->node_first : nullptr;
     if (h->nd == 2)
-        f_gather_kernel<2><<<grid_1d(h->npoint), 256, 0, h->stream>>>(h->npoint, h->d_inc_ptr, h->d_inc, h->d_fe, ff);
+        f_gather_kernel<2><<<grid_1d(n), 256, 0, h->stream>>>(n, h->d_inc_ptr, h->d_inc, h->d_fe, ff, nq, off, first);
     else
-        f_gather_kernel<3><<<grid_1d(h->npoint), 256, 0, h->stream>>>(h->npoint, h->d_inc_ptr, h->d_inc, h->d_fe, ff);
+        f_gather_kernel<3><<<grid_1d(n), 256, 0, h->stream>>>(n, h->d_inc_ptr, h->d_inc, h->d_fe, ff, nq, off, first);
     h->launches++;
 }
 
@@ -1069,15 +1133,44 @@ static int run(pms_elements* h, const double* ddu, double* ff, double* csr, int 
     };
     if (upd != UPD_NONE || dof || dok) timed(0, [&] { launch_elem(h, a, upd, dof, dok); });
     if (dof) timed(1, [&] { launch_f_gather(h, d_ff); });
-    if (dok) timed(2, [&] { launch_kk_gather(h, d_csr); });
+    if (mem == PMS_MEM_DEVICE || !dok) {
+        if (dok) timed(2, [&] { launch_kk_gather(h, d_csr); });
+        int rc = cuda_check(h);
+        if (rc) return rc;
+        if (mem == PMS_MEM_HOST) {
+            if (dof) cudaMemcpyAsync(ff, d_ff, (size_t)h->ndof * 8, cudaMemcpyDeviceToHost, h->stream);
+            return finish_host(h);
+        }
+        return PMS_OK;
+    }
+    // host CSR: gather NSLAB row slabs; each slab's values go out on the copy stream as soon as
+    // the slab is written, overlapping the transfer with the later slabs (and R)
+    if (!h->copy_stream) {
+        if (cudaStreamCreateWithFlags(&h->copy_stream, cudaStreamNonBlocking) != cudaSuccess)
+            return fail(h, PMS_ERR_CUDA, "stream creation failed");
+        for (auto& e : h->slab_ev)
+            if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess)
+                return fail(h, PMS_ERR_CUDA, "event creation failed");
+    }
+    constexpr int NS = pms_elements::NSLAB;
+    const int64_t BB = (int64_t)h->nd * h->nd;
+    timed(2, [&] {
+        for (int k = 0; k < NS; k++) {
+            const int64_t A0 = h->npoint * k / NS, A1 = h->npoint * (k + 1) / NS;
+            if (A1 > A0) launch_kk_gather(h, d_csr, nullptr, nullptr, nullptr, A0, A1 - A0);
+            cudaEventRecord(h->slab_ev[k], h->stream);
+            cudaStreamWaitEvent(h->copy_stream, h->slab_ev[k], 0);
+            const int64_t v0 = BB * h->pat.bptr[A0], v1 = BB * h->pat.bptr[A1];
+            if (v1 > v0)
+                cudaMemcpyAsync(csr + v0, d_csr + v0, (size_t)(v1 - v0) * 8, cudaMemcpyDeviceToHost, h->copy_stream);
+        }
+    });
     int rc = cuda_check(h);
     if (rc) return rc;
-    if (mem == PMS_MEM_HOST) {
-        if (dof) cudaMemcpyAsync(ff, d_ff, (size_t)h->ndof * 8, cudaMemcpyDeviceToHost, h->stream);
-        if (dok) cudaMemcpyAsync(csr, d_csr, (size_t)h->nnz * 8, cudaMemcpyDeviceToHost, h->stream);
-        return finish_host(h);
-    }
-    return PMS_OK;
+    if (dof) cudaMemcpyAsync(ff, d_ff, (size_t)h->ndof * 8, cudaMemcpyDeviceToHost, h->stream);
+    cudaEventRecord(h->slab_ev[NS], h->copy_stream);
+    cudaStreamWaitEvent(h->stream, h->slab_ev[NS], 0);
+    return finish_host(h);
 }
 
 int pms_elements_update_secondary(pms_elements* h, const double* ddu, int32_t mem) {
@@ -1267,13 +1360,20 @@ int elements_device_pattern(pms_elements* h, const int64_t** indptr, const int32
 }
 
 int elements_run_modes(pms_elements* h, const int32_t* cell_prob, const int32_t* node_prob, const uint8_t* pmode,
-                       const double* ddu, double* ff, double* csr) {
+                       const double* ddu, double* ff, double* csr, const WorkQueue* queue) {
     ElemArgs a = make_args(h, ddu);
     a.cell_prob = cell_prob;
     a.pmode = pmode;
+    if (queue) {
+        if (queue->nq <= 0 || queue->ncell <= 0) return PMS_OK;  // nothing queued
+        a.ncell = queue->ncell;
+        a.nq = queue->nq;
+        a.q_off = queue->cell_off;
+        a.q_first = queue->cell_first;
+    }
     launch_elem(h, a, UPD_MODE, true, true);
-    launch_f_gather(h, ff);
-    launch_kk_gather(h, csr, node_prob, pmode);
+    launch_f_gather(h, ff, queue);
+    launch_kk_gather(h, csr, node_prob, pmode, queue);
     return cuda_check(h);
 }
 

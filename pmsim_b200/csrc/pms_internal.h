@@ -28,13 +28,25 @@ ElementsView elements_view(pms_elements* h);
 // Device CSR pattern of K (allocated by the handle on first use, kept until destroy).
 int elements_device_pattern(pms_elements* h, const int64_t** indptr, const int32_t** indices);
 
+// Work queue of a batched element pass: the cell ranges and node ranges of the problems that take
+// part (device arrays; range k covers off[k] .. off[k+1]-1 of the queue, starting at first[k]).
+struct WorkQueue {
+    int32_t nq = 0;
+    int64_t ncell = 0, nnode = 0;  // queued cells and nodes (off[nq])
+    const int64_t* cell_off = nullptr;
+    const int64_t* cell_first = nullptr;
+    const int64_t* node_off = nullptr;
+    const int64_t* node_first = nullptr;
+};
+
 // One launch of the element kernel in per-problem mode (0 skip, 1 step start, 2 update) followed by
 // the F_int and CSR gathers (the CSR rows of mode-0 problems are left as they are); all pointers
-// are device pointers on the handle's stream.
+// are device pointers on the handle's stream.  With a queue, only its cells and nodes are visited
+// (every queued problem must have a non-zero mode); F_int rows outside the queue are left as they are.
 int elements_run_modes(pms_elements* h, const int32_t* cell_prob, const int32_t* node_prob, const uint8_t* pmode,
-                       const double* ddu, double* ff, double* csr);
+                       const double* ddu, double* ff, double* csr, const WorkQueue* queue = nullptr);
 
-// Sets lambda = 0 ... not needed: mode 1 resets it.  Status of the last launches (syncs the stream).
+// Status of the last launches (waits for the handle's stream).
 int elements_status(pms_elements* h);
 
 }  // namespace pms

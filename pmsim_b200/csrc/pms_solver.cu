@@ -11,9 +11,21 @@
 // max|R| over free rows, prescribed rows (R_p + l) and constraint rows (u_p - c), and
 // rel(mdu) = max |mdu_i| / (1 + |mdu0_i|) over the DOFs and the multipliers.
 //
-// Determinism: every reduction is split into chunks that never straddle two problems; a chunk is
-// reduced by a fixed tree and a problem sums its chunks in order, so a problem's results do not
-// depend on which other problems share the batch (bit-identical alone and in the mix).
+// Continuous progress.  A tick advances every running problem by one stage of its own Newton
+// iteration: problems waiting for an element pass get it (all of them in one launch), problems
+// whose linear solve is under way get up to `pcg_budget` more PCG iterations, and problems whose
+// PCG converged in this tick finish their Newton iteration (multipliers, rel(mdu), U update).  A
+// problem never waits for the PCG of another problem to finish.
+//
+// Two PCG engines, one arithmetic.  Small problems run the whole PCG loop in one thread block each
+// (pcg_block_kernel: no grid-wide synchronisation, every problem at its own pace, resumable
+// across ticks); large problems run the batch-wide kernels (spmv+dot, update, beta, direction),
+// captured in a CUDA graph.  Both engines call the same per-node and per-row functions and reduce
+// through the same trees: 128-node chunks that never straddle two problems, each summed by the
+// fixed pairing (t, t+s), s = 64..1, and a problem's chunk partials summed in chunk order.  A
+// problem's iterates are therefore bit-identical whichever engine runs it and whichever problems
+// share the batch, so the engine threshold and launch shapes (chosen by pms_batch_autotune) change
+// speed only.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -30,10 +42,14 @@ using namespace pms;
 
 namespace {
 
-constexpr int CHN = 128;  // nodes per reduction chunk (= threads per block of the node kernels)
+constexpr unsigned FULL = 0xffffffffu;
+constexpr int CHN = 128;        // nodes per reduction chunk (= threads per block of the node kernels)
+constexpr int WIDE_SPMV_THREADS = 512;
+constexpr int CTA_MAX_CHUNKS = 2048;  // chunk partials a block-engine problem may keep in shared memory
 
 struct SolverArgs {
     int nd;
+    int np;
     int64_t nnode, ndof;
     const int32_t* node_prob;    // problem of each node
     const int64_t* chunk_node0;  // first node of each chunk
@@ -41,33 +57,211 @@ struct SolverArgs {
     const int32_t* chunk_prob;   // problem of each chunk
     const int64_t* pchunk;       // chunks of problem p: [pchunk[p], pchunk[p+1])
     const int32_t* pres_idx;     // per DOF: index into the prescribed arrays, or -1
-    const uint8_t* active;       // per problem: Newton iteration running
-    uint8_t* pcg_active;         // per problem: PCG still iterating
+    const uint8_t* active;       // per problem: selected for the current Newton-level stage
+    uint8_t* pcg_active;         // [2][np]: PCG still iterating on the batch-wide engine (by parity)
+    const uint8_t* engine;       // per problem: 1 = block engine, 0 = batch-wide engine
 };
 
-__device__ __forceinline__ double block_sum(double v, double* sh) {
-    const int t = threadIdx.x;
-    sh[t] = v;
+// ---- canonical reductions ----------------------------------------------------------------
+// Reduces the 128 values of a thread group (threads [128g, 128g + 128) of the block) by the fixed
+// pairing (t, t+s), s = 64, 32, ..., 1 (the last five levels by warp shuffles, which pair the same
+// operands).  Every block-level PCG and Newton reduction goes through here.  All threads of the
+// block must call it; sh holds blockDim.x doubles.
+template <bool MAX>
+__device__ __forceinline__ double group_reduce(double v, double* sh) {
+    const int t = threadIdx.x & (CHN - 1);
+    double* s = sh + (threadIdx.x & ~(CHN - 1));
+    s[t] = v;
     __syncthreads();
-    for (int s = CHN / 2; s > 0; s >>= 1) {
-        if (t < s) sh[t] += sh[t + s];
-        __syncthreads();
+    if (t < 64) s[t] = MAX ? fmax(s[t], s[t + 64]) : s[t] + s[t + 64];
+    __syncthreads();
+    if (t < 32) {
+        double r = MAX ? fmax(s[t], s[t + 32]) : s[t] + s[t + 32];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            const double w = __shfl_down_sync(FULL, r, o);
+            r = MAX ? fmax(r, w) : r + w;
+        }
+        if (t == 0) s[0] = r;
     }
-    const double r = sh[0];
+    __syncthreads();
+    const double r = s[0];
     __syncthreads();
     return r;
 }
-__device__ __forceinline__ double block_max(double v, double* sh) {
-    const int t = threadIdx.x;
-    sh[t] = v;
+
+// Two sums at once (same trees as two group_reduce<false> calls); sh holds 2*blockDim.x doubles.
+__device__ __forceinline__ void group_reduce2(double& a, double& b, double* sh) {
+    const int t = threadIdx.x & (CHN - 1);
+    double* s = sh + 2 * (threadIdx.x & ~(CHN - 1));
+    double* u = s + CHN;
+    s[t] = a;
+    u[t] = b;
     __syncthreads();
-    for (int s = CHN / 2; s > 0; s >>= 1) {
-        if (t < s) sh[t] = fmax(sh[t], sh[t + s]);
-        __syncthreads();
+    if (t < 64) {
+        s[t] = s[t] + s[t + 64];
+        u[t] = u[t] + u[t + 64];
     }
-    const double r = sh[0];
     __syncthreads();
-    return r;
+    if (t < 32) {
+        double x = s[t] + s[t + 32], y = u[t] + u[t + 32];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            x = x + __shfl_down_sync(FULL, x, o);
+            y = y + __shfl_down_sync(FULL, y, o);
+        }
+        if (t == 0) {
+            s[0] = x;
+            u[0] = y;
+        }
+    }
+    __syncthreads();
+    a = s[0];
+    b = u[0];
+    __syncthreads();
+}
+
+// Total of a problem's chunk partials (the per-problem half of every PCG reduction), computed by a
+// group of 128 threads: thread t adds the partials t, t+128, ... in order, then the group tree.
+// Every PCG engine computes its totals this way, so they agree to the bit.
+__device__ __forceinline__ double problem_total(const double* part, int64_t c0, int64_t c1, double* sh) {
+    double s = 0.0;
+    for (int64_t c = c0 + (threadIdx.x & (CHN - 1)); c < c1; c += CHN) s += part[c];
+    return group_reduce<false>(s, sh);
+}
+
+__device__ __forceinline__ void problem_total2(const double* pa, const double* pb, int64_t c0, int64_t c1,
+                                               double& a, double& b, double* sh) {
+    a = 0.0;
+    b = 0.0;
+    for (int64_t c = c0 + (threadIdx.x & (CHN - 1)); c < c1; c += CHN) {
+        a += pa[c];
+        b += pb[c];
+    }
+    group_reduce2(a, b, sh);
+}
+
+// ---- per-row / per-node PCG arithmetic shared by both engines -----------------------------
+// (K x)_row by TPR lanes: lane `sub` takes the entries sub, sub+TPR, ... (FMA chain), then a
+// shuffle tree over the TPR lanes.  Every lane of the warp must call it (on = false: no entries).
+template <int TPR>
+__device__ __forceinline__ double row_dot(int64_t row, int sub, bool on, const int64_t* __restrict__ indptr,
+                                          const int32_t* __restrict__ indices, const double* __restrict__ val,
+                                          const double* __restrict__ x) {
+    double s = 0.0;
+    if (on)
+        for (int64_t k = indptr[row] + sub; k < indptr[row + 1]; k += TPR) s = fma(val[k], x[indices[k]], s);
+#pragma unroll
+    for (int o = TPR / 2; o > 0; o >>= 1) s += __shfl_down_sync(FULL, s, o, TPR);
+    return s;
+}
+
+// R rows at once by the same lanes (row j: the same FMA chain and shuffle tree as row_dot), so
+// that the loads of R rows are in flight together.
+template <int TPR, int R>
+__device__ __forceinline__ void rows_dot(const int64_t (&row)[R], const bool (&on)[R], int sub,
+                                         const int64_t* __restrict__ indptr, const int32_t* __restrict__ indices,
+                                         const double* __restrict__ val, const double* __restrict__ x,
+                                         double (&s)[R]) {
+    int64_t k[R], e[R];
+#pragma unroll
+    for (int j = 0; j < R; j++) {
+        s[j] = 0.0;
+        k[j] = on[j] ? indptr[row[j]] + sub : 0;
+        e[j] = on[j] ? indptr[row[j] + 1] : 0;
+    }
+    bool more = true;
+    while (more) {
+        more = false;
+#pragma unroll
+        for (int j = 0; j < R; j++)
+            if (k[j] < e[j]) {
+                s[j] = fma(val[k[j]], x[indices[k[j]]], s[j]);
+                k[j] += TPR;
+                more = more || k[j] < e[j];
+            }
+    }
+#pragma unroll
+    for (int j = 0; j < R; j++)
+#pragma unroll
+        for (int o = TPR / 2; o > 0; o >>= 1) s[j] += __shfl_down_sync(FULL, s[j], o, TPR);
+}
+
+// q = K p (prescribed rows: 0) on rows [row0, row1) by BD threads, R rows per lane group per pass
+template <int BD, int TPR, int R>
+__device__ __forceinline__ void spmv_rows(const int32_t* pres_idx, int64_t row0, int64_t row1,
+                                          const int64_t* __restrict__ indptr, const int32_t* __restrict__ indices,
+                                          const double* __restrict__ val, const double* p, double* q) {
+    constexpr int GR = BD / TPR;  // lane groups
+    const int sub = threadIdx.x % TPR, grp = threadIdx.x / TPR;
+    for (int64_t base = row0; base < row1; base += (int64_t)R * GR) {
+        int64_t row[R];
+        bool on[R];
+        double sv[R];
+#pragma unroll
+        for (int j = 0; j < R; j++) {
+            row[j] = base + j * GR + grp;
+            on[j] = row[j] < row1;
+        }
+        rows_dot<TPR, R>(row, on, sub, indptr, indices, val, p, sv);
+        if (sub == 0) {
+#pragma unroll
+            for (int j = 0; j < R; j++)
+                if (on[j]) q[row[j]] = (pres_idx[row[j]] >= 0) ? 0.0 : sv[j];
+        }
+    }
+}
+
+// a.b over the free DOFs of a node
+__device__ __forceinline__ double node_dot(const SolverArgs& S, int64_t node, const double* a, const double* b) {
+    double s = 0.0;
+    for (int d = 0; d < S.nd; d++) {
+        const int64_t i = node * S.nd + d;
+        if (S.pres_idx[i] < 0) s = fma(a[i], b[i], s);
+    }
+    return s;
+}
+
+// x += alpha p, r -= alpha q (free DOFs), z = M r with the node's inverse diagonal block;
+// accumulates the node's r.z and r.r
+__device__ __forceinline__ void node_update(const SolverArgs& S, int64_t node, double alpha, const double* p,
+                                            const double* q, const double* binv, double* x, double* r, double* z,
+                                            double& rz, double& r2) {
+    const int nd = S.nd;
+    double rv[3];
+    for (int d = 0; d < nd; d++) {
+        const int64_t i = node * nd + d;
+        if (S.pres_idx[i] < 0) {
+            x[i] = fma(alpha, p[i], x[i]);
+            rv[d] = fma(-alpha, q[i], r[i]);
+            r[i] = rv[d];
+        } else {
+            rv[d] = 0.0;
+        }
+    }
+    const double* B = binv + node * nd * nd;
+    for (int d = 0; d < nd; d++) {
+        double zv = 0.0;
+        for (int e = 0; e < nd; e++) zv = fma(B[d * nd + e], rv[e], zv);
+        z[node * nd + d] = zv;
+        rz = fma(rv[d], zv, rz);
+        r2 = fma(rv[d], rv[d], r2);
+    }
+}
+
+// p = z + beta p on a DOF (0 on prescribed DOFs)
+__device__ __forceinline__ void dof_direction(const SolverArgs& S, int64_t i, double beta, const double* z,
+                                              double* p) {
+    p[i] = (S.pres_idx[i] >= 0) ? 0.0 : fma(beta, p[i], z[i]);
+}
+
+// scalar step of one PCG iteration: beta, rho, iteration count and the stopping test
+__device__ __forceinline__ bool pcg_scalar_step(double rz, double rr, double& rho, double r0, int32_t& iters,
+                                                double rtol, int32_t max_iter, double& beta) {
+    beta = (rho != 0.0) ? rz / rho : 0.0;
+    rho = rz;
+    iters += 1;
+    return !(sqrt(rr) > rtol * r0) || iters >= max_iter;  // true: done
 }
 
 // ---- Newton-level kernels ----------------------------------------------------------------
@@ -94,7 +288,7 @@ __global__ void residual_kernel(SolverArgs S, const double* ff, const double* fe
             m = fmax(m, isfinite(v) ? fabs(v) : INFINITY);
         }
     }
-    m = block_max(m, sh);
+    m = group_reduce<true>(m, sh);
     if (threadIdx.x == 0) part_max[ch] = m;
 }
 
@@ -144,21 +338,17 @@ __global__ void block_jacobi_kernel(SolverArgs S, const int64_t* bptr, const int
         for (int j = 0; j < nf; j++) out[fr[i] * nd + fr[j]] = ok ? a[i][nf + j] : (i == j ? 1.0 / fmax(fabs(a[i][i]), 1e-300) : 0.0);
 }
 
-// y = K x on the rows of active problems (tpr threads per row); masked: y_p = 0 on prescribed rows
-// when mask_pres, and only problems with flag[p] set take part.
+// y = K x on the rows of the problems with flag[p] set (TPR threads per row); y_p = 0 on
+// prescribed rows when mask_pres.
 template <int TPR>
 __global__ void spmv_kernel(SolverArgs S, const int64_t* indptr, const int32_t* indices, const double* val,
                             const double* x, double* y, const uint8_t* flag, bool mask_pres) {
     const int64_t gid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     const int64_t row = gid / TPR;
     const int sub = (int)(gid % TPR);
-    // no early exit: every lane of the warp takes part in the shuffles below
+    // no early exit: every lane of the warp takes part in the shuffles
     const bool on = row < S.ndof && flag[S.node_prob[row < S.ndof ? row / S.nd : 0]];
-    double s = 0.0;
-    if (on)
-        for (int64_t k = indptr[row] + sub; k < indptr[row + 1]; k += TPR) s = fma(val[k], x[indices[k]], s);
-#pragma unroll
-    for (int o = TPR / 2; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o, TPR);
+    const double s = row_dot<TPR>(row, sub, on, indptr, indices, val, x);
     if (on && sub == 0) y[row] = (mask_pres && S.pres_idx[row] >= 0) ? 0.0 : s;
 }
 
@@ -174,7 +364,7 @@ __global__ void pres_increment_kernel(SolverArgs S, const double* u, const doubl
 // PCG start: r = R_f - (K mdu_p)_f, x = 0, z = M r, p = z; partials of r.z and r.r
 __global__ void pcg_start_kernel(SolverArgs S, const double* rr, const double* kt, const double* binv, double* r,
                                  double* x, double* z, double* p, double* part_rz, double* part_rr) {
-    __shared__ double sh[CHN];
+    __shared__ double sh[2 * CHN];
     const int64_t ch = blockIdx.x;
     const int pr = S.chunk_prob[ch];
     double rz = 0.0, r2 = 0.0;
@@ -192,136 +382,199 @@ __global__ void pcg_start_kernel(SolverArgs S, const double* rr, const double* k
         const double* B = binv + node * nd * nd;
         for (int d = 0; d < nd; d++) {
             double zv = 0.0;
-            for (int e = 0; e < nd; e++) zv += B[d * nd + e] * rv[e];
+            for (int e = 0; e < nd; e++) zv = fma(B[d * nd + e], rv[e], zv);
             z[node * nd + d] = zv;
             p[node * nd + d] = zv;
-            rz += rv[d] * zv;
-            r2 += rv[d] * rv[d];
+            rz = fma(rv[d], zv, rz);
+            r2 = fma(rv[d], rv[d], r2);
         }
     }
-    rz = block_sum(rz, sh);
-    r2 = block_sum(r2, sh);
-    if (threadIdx.x == 0) {
+    group_reduce2(rz, r2, sh);
+    if (threadIdx.x == 0 && S.active[pr]) {
         part_rz[ch] = rz;
         part_rr[ch] = r2;
     }
 }
 
-__global__ void pcg_init_scalars_kernel(int np, const uint8_t* active, const int64_t* pchunk, const double* part_rz,
-                                        const double* part_rr, double* rho, double* r0, uint8_t* pcg_active,
-                                        int32_t* pcg_iters) {
-    const int p = blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= np) return;
-    double a = 0.0, b = 0.0;
-    for (int64_t c = pchunk[p]; c < pchunk[p + 1]; c++) {
-        a += part_rz[c];
-        b += part_rr[c];
-    }
-    rho[p] = a;
+// per problem selected by `active` (one block of 128 threads each): rho = r.z, r0 = |r|_2, iteration
+// count 0, and the engine that runs its PCG (block engine: cta_active, batch-wide: pcg_active)
+__global__ void __launch_bounds__(CHN)
+pcg_init_scalars_kernel(int np, const uint8_t* active, const uint8_t* engine, const int64_t* pchunk,
+                        const double* part_rz, const double* part_rr, double* rho, double* r0, uint8_t* pcg_active,
+                        uint8_t* cta_active, int32_t* pcg_iters) {
+    __shared__ double sh[2 * CHN];
+    const int p = blockIdx.x;
+    if (!active[p]) return;
+    double a, b;
+    problem_total2(part_rz, part_rr, pchunk[p], pchunk[p + 1], a, b, sh);
+    if (threadIdx.x != 0) return;
     r0[p] = sqrt(b);
-    pcg_active[p] = (active[p] && b > 0.0) ? 1 : 0;
-    pcg_iters[p] = 0;
-}
-
-// partials of p.q
-__global__ void pcg_dot_kernel(SolverArgs S, const double* a, const double* b, double* part) {
-    __shared__ double sh[CHN];
-    const int64_t ch = blockIdx.x;
-    const int pr = S.chunk_prob[ch];
-    double s = 0.0;
-    if (S.pcg_active[pr] && threadIdx.x < S.chunk_nnode[ch]) {
-        const int64_t node = S.chunk_node0[ch] + threadIdx.x;
-        for (int d = 0; d < S.nd; d++) {
-            const int64_t i = node * S.nd + d;
-            if (S.pres_idx[i] < 0) s += a[i] * b[i];
-        }
+    const uint8_t go = b > 0.0 ? 1 : 0;
+    for (int e = 0; e < 2; e++) {  // both parity buffers of the batch-wide engine
+        rho[e * np + p] = a;
+        pcg_active[e * np + p] = engine[p] ? 0 : go;
+        pcg_iters[e * np + p] = 0;
     }
-    s = block_sum(s, sh);
-    if (threadIdx.x == 0) part[ch] = s;
+    cta_active[p] = engine[p] ? go : 0;
 }
 
-__global__ void pcg_alpha_kernel(int np, const uint8_t* pcg_active, const int64_t* pchunk, const double* part,
-                                 const double* rho, double* alpha) {
-    const int p = blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= np) return;
-    double pq = 0.0;
-    for (int64_t c = pchunk[p]; c < pchunk[p + 1]; c++) pq += part[c];
-    alpha[p] = (pcg_active[p] && pq != 0.0) ? rho[p] / pq : 0.0;
-}
+// ---- batch-wide PCG engine (one CUDA graph node per kernel) --------------------------------
 
-// x += a p, r -= a q, z = M r; partials of r.z and r.r
-__global__ void pcg_update_kernel(SolverArgs S, const double* alpha, const double* p, const double* q,
-                                  const double* binv, double* x, double* r, double* z, double* part_rz,
-                                  double* part_rr) {
-    __shared__ double sh[CHN];
+// q = K p on the rows of one chunk (TPR lanes per row, all threads of the block over the chunk's
+// rows), then the chunk's partial of p.q
+template <int TPR>
+__global__ void __launch_bounds__(WIDE_SPMV_THREADS)
+pcg_spmv_dot_kernel(SolverArgs S, int par, const int64_t* __restrict__ indptr, const int32_t* __restrict__ indices,
+                    const double* __restrict__ val, const double* p, double* q, double* part) {
+    __shared__ double sh[WIDE_SPMV_THREADS];
     const int64_t ch = blockIdx.x;
     const int pr = S.chunk_prob[ch];
+    if (!S.pcg_active[par * S.np + pr]) return;  // whole block
+    const int64_t node0 = S.chunk_node0[ch];
+    const int nn = S.chunk_nnode[ch];
+    spmv_rows<WIDE_SPMV_THREADS, TPR, 4>(S.pres_idx, node0 * S.nd, (node0 + nn) * S.nd, indptr, indices, val, p, q);
+    __syncthreads();
+    const double v = (threadIdx.x < nn) ? node_dot(S, node0 + threadIdx.x, p, q) : 0.0;
+    const double t = group_reduce<false>(v, sh);  // group 0 holds the chunk's nodes
+    if (threadIdx.x == 0) part[ch] = t;
+}
+
+// alpha = rho / p.q (every block of a problem sums the same partials in the same order), then
+// x, r, z and the chunk's partials of r.z and r.r
+__global__ void __launch_bounds__(CHN)
+pcg_update_kernel(SolverArgs S, int par, const double* part_pq, const double* rho, const double* p, const double* q,
+                  const double* binv, double* x, double* r, double* z, double* part_rz, double* part_rr,
+                  int32_t* nactive) {
+    __shared__ double sh[2 * CHN];
+    if (blockIdx.x == 0 && threadIdx.x == 0) *nactive = 0;  // counted again by pcg_beta_direction_kernel
+    const int64_t ch = blockIdx.x;
+    const int pr = S.chunk_prob[ch];
+    if (!S.pcg_active[par * S.np + pr]) return;  // whole block
+    const double pq = problem_total(part_pq, S.pchunk[pr], S.pchunk[pr + 1], sh);
+    const double alpha = (pq != 0.0) ? rho[par * S.np + pr] / pq : 0.0;
     double rz = 0.0, r2 = 0.0;
-    if (S.pcg_active[pr] && threadIdx.x < S.chunk_nnode[ch]) {
-        const int64_t node = S.chunk_node0[ch] + threadIdx.x;
-        const int nd = S.nd;
-        const double a = alpha[pr];
-        double rv[3];
-        for (int d = 0; d < nd; d++) {
-            const int64_t i = node * nd + d;
-            if (S.pres_idx[i] < 0) {
-                x[i] += a * p[i];
-                rv[d] = r[i] - a * q[i];
-                r[i] = rv[d];
-            } else {
-                rv[d] = 0.0;
-            }
-        }
-        const double* B = binv + node * nd * nd;
-        for (int d = 0; d < nd; d++) {
-            double zv = 0.0;
-            for (int e = 0; e < nd; e++) zv += B[d * nd + e] * rv[e];
-            z[node * nd + d] = zv;
-            rz += rv[d] * zv;
-            r2 += rv[d] * rv[d];
-        }
-    }
-    rz = block_sum(rz, sh);
-    r2 = block_sum(r2, sh);
+    if (threadIdx.x < S.chunk_nnode[ch])
+        node_update(S, S.chunk_node0[ch] + threadIdx.x, alpha, p, q, binv, x, r, z, rz, r2);
+    group_reduce2(rz, r2, sh);
     if (threadIdx.x == 0) {
         part_rz[ch] = rz;
         part_rr[ch] = r2;
     }
 }
 
-__global__ void pcg_beta_kernel(int np, uint8_t* pcg_active, const int64_t* pchunk, const double* part_rz,
-                                const double* part_rr, double* rho, double* beta, const double* r0, double rtol,
-                                int32_t max_iter, int32_t* iters, int32_t* nactive) {
-    const int p = blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= np) return;
-    if (!pcg_active[p]) {
-        beta[p] = 0.0;
+// beta (every block of a problem from the same partials), the direction p = z + beta p on the
+// chunk, and -- by the problem's first chunk -- rho, the iteration count and the stopping test.
+// The per-problem scalars are double-buffered by iteration parity (read `par`, write the other),
+// so no block reads a value that another block of the same launch writes; graphs hold an even
+// number of iterations, so buffer 0 is current between launches.
+__global__ void __launch_bounds__(CHN)
+pcg_beta_direction_kernel(SolverArgs S, int par, const double* part_rz, const double* part_rr, double* rho,
+                          const double* r0, double rtol, int32_t max_iter, int32_t* iters, const double* z, double* p,
+                          int32_t* nactive) {
+    __shared__ double sh[2 * CHN];
+    const int64_t ch = blockIdx.x;
+    const int pr = S.chunk_prob[ch];
+    if (S.engine[pr]) return;  // block-engine problem: its state is not ours
+    const int cur = par * S.np + pr, nxt = (par ^ 1) * S.np + pr;
+    const bool lead = ch == S.pchunk[pr];
+    if (!S.pcg_active[cur]) {
+        if (lead && threadIdx.x == 0) {
+            S.pcg_active[nxt] = 0;
+            rho[nxt] = rho[cur];
+            iters[nxt] = iters[cur];
+        }
         return;
     }
-    double a = 0.0, b = 0.0;
-    for (int64_t c = pchunk[p]; c < pchunk[p + 1]; c++) {
-        a += part_rz[c];
-        b += part_rr[c];
+    double a, b;
+    problem_total2(part_rz, part_rr, S.pchunk[pr], S.pchunk[pr + 1], a, b, sh);
+    double rh = rho[cur], beta;
+    int32_t it = iters[cur];
+    const bool done = pcg_scalar_step(a, b, rh, r0[pr], it, rtol, max_iter, beta);
+    if (lead && threadIdx.x == 0) {
+        rho[nxt] = rh;
+        iters[nxt] = it;
+        S.pcg_active[nxt] = done ? 0 : 1;
+        if (!done) atomicAdd(nactive, 1);
     }
-    beta[p] = (rho[p] != 0.0) ? a / rho[p] : 0.0;
-    rho[p] = a;
-    iters[p] += 1;
-    const bool done = !(sqrt(b) > rtol * r0[p]) || iters[p] >= max_iter;
-    if (done) {
-        pcg_active[p] = 0;
-    } else {
-        atomicAdd(nactive, 1);
+    if (threadIdx.x < S.chunk_nnode[ch]) {
+        const int64_t node = S.chunk_node0[ch] + threadIdx.x;
+        for (int d = 0; d < S.nd; d++) dof_direction(S, node * S.nd + d, beta, z, p);
     }
 }
 
-__global__ void pcg_p_kernel(SolverArgs S, const uint8_t* was_active, const double* beta, const double* z,
-                             double* p) {
-    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= S.ndof) return;
-    const int pr = S.node_prob[i / S.nd];
-    if (!was_active[pr]) return;
-    p[i] = (S.pres_idx[i] >= 0) ? 0.0 : z[i] + beta[pr] * p[i];
+// ---- block PCG engine: one thread block runs one problem's PCG ------------------------------
+// Up to `budget` iterations (or to convergence) of the problem list[blockIdx.x]; its state (x, r,
+// z, p, q, rho, iteration count, active flag) lives in global memory, so the next launch resumes
+// where this one stopped.  Same arithmetic as the batch-wide kernels: rows by row_dot<TPR>, chunk
+// partials by the 128-thread trees (group g of the block takes chunks g, g+G, ...), problem totals
+// in chunk order.
+template <int BD, int TPR>
+__global__ void __launch_bounds__(BD)
+pcg_block_kernel(SolverArgs S, const int32_t* list, const int64_t* __restrict__ indptr,
+                 const int32_t* __restrict__ indices, const double* __restrict__ val, const double* binv, double* x,
+                 double* r, double* z, double* p, double* q, double* rho_g, const double* r0_g, int32_t* iters_g,
+                 uint8_t* cta_active, double rtol, int32_t max_iter, int32_t budget) {
+    constexpr int G = BD / CHN;
+    extern __shared__ double smem[];
+    double* red = smem;                 // 2*BD
+    double* pq_part = red + 2 * BD;     // CTA_MAX_CHUNKS each
+    double* rz_part = pq_part + CTA_MAX_CHUNKS;
+    double* rr_part = rz_part + CTA_MAX_CHUNKS;
+    const int pr = list[blockIdx.x];
+    if (!cta_active[pr]) return;  // whole block
+    const int64_t c0 = S.pchunk[pr], c1 = S.pchunk[pr + 1];
+    const int nch = (int)(c1 - c0);
+    const int nd = S.nd;
+    const int64_t row0 = S.chunk_node0[c0] * nd;
+    const int64_t row1 = (S.chunk_node0[c1 - 1] + S.chunk_nnode[c1 - 1]) * nd;
+    const int g = threadIdx.x / CHN, tg = threadIdx.x % CHN;
+    double rho = rho_g[pr];
+    const double r0 = r0_g[pr];
+    int32_t it = iters_g[pr];
+    bool active = true;
+    for (int k = 0; k < budget && active; k++) {
+        // q = K p on the problem's rows
+        spmv_rows<BD, TPR, 4>(S.pres_idx, row0, row1, indptr, indices, val, p, q);
+        __syncthreads();
+        // chunk partials of p.q
+        for (int cb = 0; cb < nch; cb += G) {
+            const int c = cb + g;
+            double v = 0.0;
+            if (c < nch && tg < S.chunk_nnode[c0 + c]) v = node_dot(S, S.chunk_node0[c0 + c] + tg, p, q);
+            v = group_reduce<false>(v, red);
+            if (tg == 0 && c < nch) pq_part[c] = v;
+        }
+        __syncthreads();
+        const double pq = problem_total(pq_part, 0, nch, red);  // every group computes the same total
+        const double alpha = (pq != 0.0) ? rho / pq : 0.0;
+        // x, r, z and the chunk partials of r.z, r.r
+        for (int cb = 0; cb < nch; cb += G) {
+            const int c = cb + g;
+            double rz = 0.0, r2 = 0.0;
+            if (c < nch && tg < S.chunk_nnode[c0 + c])
+                node_update(S, S.chunk_node0[c0 + c] + tg, alpha, p, q, binv, x, r, z, rz, r2);
+            group_reduce2(rz, r2, red);
+            if (tg == 0 && c < nch) {
+                rz_part[c] = rz;
+                rr_part[c] = r2;
+            }
+        }
+        __syncthreads();
+        double rzt, rrt, beta;
+        problem_total2(rz_part, rr_part, 0, nch, rzt, rrt, red);
+        const bool done = pcg_scalar_step(rzt, rrt, rho, r0, it, rtol, max_iter, beta);
+        for (int64_t i = row0 + threadIdx.x; i < row1; i += BD) dof_direction(S, i, beta, z, p);
+        active = !done;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        rho_g[pr] = rho;
+        iters_g[pr] = it;
+        cta_active[pr] = active ? 1 : 0;
+    }
 }
+
+size_t block_engine_smem(int bd) { return (size_t)(2 * bd + 3 * CTA_MAX_CHUNKS) * sizeof(double); }
 
 // mdu = x on free rows (mdu already holds u_p - c on prescribed rows); mdl = (R_p + l) - (K mdu)_p
 __global__ void assemble_mdu_kernel(SolverArgs S, const double* x, double* mdu) {
@@ -364,7 +617,7 @@ __global__ void rel_mdu_kernel(SolverArgs S, const uint8_t* first, const double*
             }
         }
     }
-    m = block_max(m, sh);
+    m = group_reduce<true>(m, sh);
     if (threadIdx.x == 0) part_max[ch] = m;
 }
 
@@ -408,6 +661,12 @@ __global__ void zero_masked_kernel(SolverArgs S, const uint8_t* flag, double* v)
     if (flag[S.node_prob[i / S.nd]]) v[i] = 0.0;
 }
 
+__global__ void fill_masked_kernel(SolverArgs S, const uint8_t* flag, double* v, double value) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= S.ndof) return;
+    if (flag[S.node_prob[i / S.nd]]) v[i] = value;
+}
+
 }  // namespace
 
 // ------------------------------------------------------------------------------------ handle
@@ -417,31 +676,39 @@ struct pms_batch {
     int np = 0;
     int64_t nnode = 0, ndof = 0, npres = 0, nchunk = 0;
     pms_batch_config cfg{};
+    pms_batch_tuning tune{};
     std::vector<int64_t> point_ptr, cell_ptr, pres_ptr;
     std::vector<void*> allocs;
     // device
     int32_t *d_node_prob = nullptr, *d_cell_prob = nullptr, *d_chunk_nnode = nullptr, *d_chunk_prob = nullptr;
     int64_t *d_chunk_node0 = nullptr, *d_pchunk = nullptr, *d_ppres = nullptr, *d_pres_eq = nullptr;
-    int32_t *d_pres_idx = nullptr, *d_pres_prob = nullptr;
-    uint8_t *d_active = nullptr, *d_pcg_active = nullptr, *d_pcg_was = nullptr, *d_pmode = nullptr,
-            *d_first = nullptr, *d_upd = nullptr;
+    int32_t *d_pres_idx = nullptr, *d_pres_prob = nullptr, *d_list = nullptr;
+    uint8_t *d_active = nullptr, *d_pcg_active = nullptr, *d_cta_active = nullptr, *d_pmode = nullptr,
+            *d_first = nullptr, *d_upd = nullptr, *d_engine = nullptr;
     double *d_u = nullptr, *d_ddu = nullptr, *d_ff = nullptr, *d_fext = nullptr, *d_csr = nullptr, *d_rr = nullptr;
     double *d_mdu = nullptr, *d_mdu0 = nullptr, *d_kt = nullptr, *d_r = nullptr, *d_z = nullptr, *d_p = nullptr,
            *d_q = nullptr, *d_x = nullptr, *d_binv = nullptr;
     double *d_lam = nullptr, *d_c = nullptr, *d_mdl = nullptr, *d_mdl0 = nullptr;
-    double *d_part_a = nullptr, *d_part_b = nullptr;
-    double *d_rho = nullptr, *d_r0 = nullptr, *d_alpha = nullptr, *d_beta = nullptr, *d_norm = nullptr,
-           *d_rel = nullptr;
+    double *d_part_a = nullptr, *d_part_b = nullptr, *d_part_c = nullptr;
+    double *d_rho = nullptr, *d_r0 = nullptr, *d_norm = nullptr, *d_rel = nullptr;
     int32_t *d_iters = nullptr, *d_nactive = nullptr;
+    int64_t* d_queue = nullptr;    // work queue of the element pass: 4 arrays of np + 1
+    std::vector<int64_t> h_queue;
     const int64_t* d_indptr = nullptr;
     const int32_t* d_indices = nullptr;
     SolverArgs S{};
+    cudaStream_t st2 = nullptr;  // block-engine PCG, overlapped with the batch-wide engine
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     cudaGraphExec_t graph = nullptr;
-    int graph_iters = 0;
+    int graph_iters_captured = 0;
     std::string last_error;
     int64_t launches = 0;
     int64_t pcg_total = 0;
-    std::vector<int32_t> it;  // Newton iteration of each problem within its current load step
+    std::vector<int32_t> it;       // Newton iteration of each problem within its current load step
+    std::vector<uint8_t> solving;  // per problem: linear solve under way
+    std::vector<uint8_t> engine;   // per problem: 1 = block engine, 0 = batch-wide engine
+    std::vector<int64_t> pndof;    // DOFs of each problem
+    std::vector<int32_t> h_list;
 
     template <typename T>
     bool alloc(T** p, size_t count) {
@@ -459,8 +726,12 @@ struct pms_batch {
     }
     ~pms_batch() {
         cudaStreamSynchronize(v.stream);
+        if (st2) cudaStreamSynchronize(st2);
         std::lock_guard<std::mutex> lock(device_mutex());
         if (graph) cudaGraphExecDestroy(graph);
+        if (ev_fork) cudaEventDestroy(ev_fork);
+        if (ev_join) cudaEventDestroy(ev_join);
+        if (st2) cudaStreamDestroy(st2);
         for (void* p : allocs) cudaFree(p);
     }
 };
@@ -474,8 +745,10 @@ int bfail(pms_batch* b, int code, const char* msg) {
 
 inline unsigned grid_of(int64_t n, int t = 256) { return (unsigned)std::max<int64_t>((n + t - 1) / t, 1); }
 
+int tpr_of(int nd) { return nd == 2 ? 8 : 16; }
+
 void launch_spmv(pms_batch* b, const double* x, double* y, const uint8_t* flag, bool mask) {
-    const int tpr = b->v.nd == 2 ? 8 : 16;
+    const int tpr = tpr_of(b->v.nd);
     const int64_t threads = b->ndof * tpr;
     if (tpr == 8)
         spmv_kernel<8><<<grid_of(threads), 256, 0, b->v.stream>>>(b->S, b->d_indptr, b->d_indices, b->d_csr, x, y,
@@ -486,48 +759,144 @@ void launch_spmv(pms_batch* b, const double* x, double* y, const uint8_t* flag, 
     b->launches++;
 }
 
-// one PCG iteration for every problem with pcg_active set
-void pcg_iteration(pms_batch* b) {
+// one batch-wide PCG iteration (parity par) for every problem with pcg_active set (3 kernels)
+void wide_iteration(pms_batch* b, int par) {
     cudaStream_t st = b->v.stream;
-    const int np = b->np;
-    const unsigned gp = grid_of(np, 128);
-    cudaMemsetAsync(b->d_nactive, 0, sizeof(int32_t), st);  // counts the problems still active after this iteration
-    cudaMemcpyAsync(b->d_pcg_was, b->d_pcg_active, np, cudaMemcpyDeviceToDevice, st);
-    launch_spmv(b, b->d_p, b->d_q, b->d_pcg_active, true);
-    pcg_dot_kernel<<<(unsigned)b->nchunk, CHN, 0, st>>>(b->S, b->d_p, b->d_q, b->d_part_a);
-    pcg_alpha_kernel<<<gp, 128, 0, st>>>(np, b->d_pcg_active, b->d_pchunk, b->d_part_a, b->d_rho, b->d_alpha);
-    pcg_update_kernel<<<(unsigned)b->nchunk, CHN, 0, st>>>(b->S, b->d_alpha, b->d_p, b->d_q, b->d_binv, b->d_x,
-                                                           b->d_r, b->d_z, b->d_part_a, b->d_part_b);
-    pcg_beta_kernel<<<gp, 128, 0, st>>>(np, b->d_pcg_active, b->d_pchunk, b->d_part_a, b->d_part_b, b->d_rho,
-                                        b->d_beta, b->d_r0, b->cfg.pcg_rtol, b->cfg.pcg_max_iterations, b->d_iters,
-                                        b->d_nactive);
-    pcg_p_kernel<<<grid_of(b->ndof), 256, 0, st>>>(b->S, b->d_pcg_was, b->d_beta, b->d_z, b->d_p);
-    b->launches += 5;
+    const unsigned nch = (unsigned)b->nchunk;
+    if (tpr_of(b->v.nd) == 8)
+        pcg_spmv_dot_kernel<8><<<nch, WIDE_SPMV_THREADS, 0, st>>>(b->S, par, b->d_indptr, b->d_indices, b->d_csr,
+                                                                   b->d_p, b->d_q, b->d_part_c);
+    else
+        pcg_spmv_dot_kernel<16><<<nch, WIDE_SPMV_THREADS, 0, st>>>(b->S, par, b->d_indptr, b->d_indices, b->d_csr,
+                                                                    b->d_p, b->d_q, b->d_part_c);
+    pcg_update_kernel<<<nch, CHN, 0, st>>>(b->S, par, b->d_part_c, b->d_rho, b->d_p, b->d_q, b->d_binv, b->d_x,
+                                           b->d_r, b->d_z, b->d_part_a, b->d_part_b, b->d_nactive);
+    pcg_beta_direction_kernel<<<nch, CHN, 0, st>>>(b->S, par, b->d_part_a, b->d_part_b, b->d_rho, b->d_r0,
+                                                   b->cfg.pcg_rtol, b->cfg.pcg_max_iterations, b->d_iters, b->d_z,
+                                                   b->d_p, b->d_nactive);
+    b->launches += 3;
 }
 
-// PCG until every problem has converged (or reached the iteration cap); iterations run in CUDA
-// graphs of graph_iters iterations between host checks of the number of active problems.
-int run_pcg(pms_batch* b) {
+int ensure_graph(pms_batch* b) {
+    const int gi = std::max(2, b->tune.graph_iters + (b->tune.graph_iters & 1));  // even
+    if (b->graph && b->graph_iters_captured == gi) return PMS_OK;
+    std::lock_guard<std::mutex> lock(device_mutex());
+    if (b->graph) {
+        cudaGraphExecDestroy(b->graph);
+        b->graph = nullptr;
+    }
     cudaStream_t st = b->v.stream;
-    if (!b->graph) {
-        std::lock_guard<std::mutex> lock(device_mutex());
-        cudaGraph_t g;
-        if (cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
-            return bfail(b, PMS_ERR_CUDA, "stream capture failed");
-        for (int i = 0; i < b->graph_iters; i++) pcg_iteration(b);
-        if (cudaStreamEndCapture(st, &g) != cudaSuccess) return bfail(b, PMS_ERR_CUDA, "stream capture failed");
-        if (cudaGraphInstantiate(&b->graph, g, 0) != cudaSuccess) {
-            cudaGraphDestroy(g);
-            return bfail(b, PMS_ERR_CUDA, "graph instantiation failed");
-        }
+    cudaGraph_t g;
+    if (cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
+        return bfail(b, PMS_ERR_CUDA, "stream capture failed");
+    for (int i = 0; i < gi; i++) wide_iteration(b, i & 1);
+    if (cudaStreamEndCapture(st, &g) != cudaSuccess) return bfail(b, PMS_ERR_CUDA, "stream capture failed");
+    if (cudaGraphInstantiate(&b->graph, g, 0) != cudaSuccess) {
         cudaGraphDestroy(g);
+        return bfail(b, PMS_ERR_CUDA, "graph instantiation failed");
     }
-    int32_t nact = 1;
-    for (int64_t it = 0; it < b->cfg.pcg_max_iterations && nact > 0; it += b->graph_iters) {
-        if (cudaGraphLaunch(b->graph, st) != cudaSuccess) return bfail(b, PMS_ERR_CUDA, "graph launch failed");
-        cudaMemcpyAsync(&nact, b->d_nactive, sizeof(int32_t), cudaMemcpyDeviceToHost, st);
-        if (cudaStreamSynchronize(st) != cudaSuccess) return bfail(b, PMS_ERR_CUDA, cudaGetErrorString(cudaGetLastError()));
+    cudaGraphDestroy(g);
+    b->graph_iters_captured = gi;
+    return PMS_OK;
+}
+
+template <int BD>
+void launch_block_engine_bd(pms_batch* b, int nlist, int budget, cudaStream_t st) {
+    const size_t sm = block_engine_smem(BD);
+    if (tpr_of(b->v.nd) == 8)
+        pcg_block_kernel<BD, 8><<<nlist, BD, sm, st>>>(b->S, b->d_list, b->d_indptr, b->d_indices, b->d_csr,
+                                                        b->d_binv, b->d_x, b->d_r, b->d_z, b->d_p, b->d_q, b->d_rho,
+                                                        b->d_r0, b->d_iters, b->d_cta_active, b->cfg.pcg_rtol,
+                                                        b->cfg.pcg_max_iterations, budget);
+    else
+        pcg_block_kernel<BD, 16><<<nlist, BD, sm, st>>>(b->S, b->d_list, b->d_indptr, b->d_indices, b->d_csr,
+                                                         b->d_binv, b->d_x, b->d_r, b->d_z, b->d_p, b->d_q, b->d_rho,
+                                                         b->d_r0, b->d_iters, b->d_cta_active, b->cfg.pcg_rtol,
+                                                         b->cfg.pcg_max_iterations, budget);
+}
+
+int launch_block_engine(pms_batch* b, int nlist, int budget, cudaStream_t st) {
+    switch (b->tune.block_threads) {
+        case 128: launch_block_engine_bd<128>(b, nlist, budget, st); break;
+        case 256: launch_block_engine_bd<256>(b, nlist, budget, st); break;
+        case 1024: launch_block_engine_bd<1024>(b, nlist, budget, st); break;
+        default: launch_block_engine_bd<512>(b, nlist, budget, st); break;
     }
+    b->launches++;
+    return PMS_OK;
+}
+
+template <int BD>
+bool set_block_smem_bd() {
+    const int sm = (int)block_engine_smem(BD);
+    bool ok = cudaFuncSetAttribute(pcg_block_kernel<BD, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm) ==
+              cudaSuccess;
+    ok = ok && cudaFuncSetAttribute(pcg_block_kernel<BD, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm) ==
+                   cudaSuccess;
+    return ok;
+}
+
+bool set_block_smem() {
+    return set_block_smem_bd<128>() && set_block_smem_bd<256>() && set_block_smem_bd<512>() &&
+           set_block_smem_bd<1024>();
+}
+
+// Which engine runs each problem's PCG (host and device copies).
+int assign_engines(pms_batch* b) {
+    for (int p = 0; p < b->np; p++) b->engine[p] = (b->pndof[p] <= b->tune.block_max_ndof) ? 1 : 0;
+    return cudaMemcpyAsync(b->d_engine, b->engine.data(), b->np, cudaMemcpyHostToDevice, b->v.stream) ==
+                   cudaSuccess
+               ? PMS_OK
+               : bfail(b, PMS_ERR_CUDA, "engine upload failed");
+}
+
+// Starts the PCG of the problems selected in d_active: preconditioner, prescribed increments,
+// r = R_f - K_fp mdu_p, z, p and the scalars.
+void pcg_start(pms_batch* b) {
+    cudaStream_t st = b->v.stream;
+    block_jacobi_kernel<<<grid_of(b->nnode), 256, 0, st>>>(b->S, b->v.d_bptr, b->v.d_kdiag, b->d_csr, b->d_binv);
+    pres_increment_kernel<<<grid_of(b->ndof), 256, 0, st>>>(b->S, b->d_u, b->d_c, b->d_mdu);
+    launch_spmv(b, b->d_mdu, b->d_kt, b->d_active, false);
+    pcg_start_kernel<<<(unsigned)b->nchunk, CHN, 0, st>>>(b->S, b->d_rr, b->d_kt, b->d_binv, b->d_r, b->d_x, b->d_z,
+                                                           b->d_p, b->d_part_a, b->d_part_b);
+    pcg_init_scalars_kernel<<<(unsigned)b->np, CHN, 0, st>>>(b->np, b->d_active, b->d_engine, b->d_pchunk,
+                                                                  b->d_part_a, b->d_part_b, b->d_rho, b->d_r0,
+                                                                  b->d_pcg_active, b->d_cta_active, b->d_iters);
+    b->launches += 4;
+}
+
+// PCG iterations of every solving problem: the block engine (one launch, on the second stream) and
+// the batch-wide engine (graph launches on the handle's stream) run side by side.  The batch-wide
+// loop keeps going while the block engine is busy; once it is idle, the loop stops when an eighth
+// of its problems (at least one) have finished or after `budget` iterations.  `exact` runs exactly
+// `budget` iterations on both engines (timing).
+int pcg_phase(pms_batch* b, int nblock, int nwide, int budget, bool exact) {
+    cudaStream_t st = b->v.stream;
+    if (nblock > 0) {
+        if (cudaEventRecord(b->ev_fork, st) != cudaSuccess || cudaStreamWaitEvent(b->st2, b->ev_fork, 0) != cudaSuccess)
+            return bfail(b, PMS_ERR_CUDA, "stream fork failed");
+        launch_block_engine(b, nblock, budget, b->st2);
+        if (cudaEventRecord(b->ev_join, b->st2) != cudaSuccess) return bfail(b, PMS_ERR_CUDA, "stream join failed");
+    }
+    if (nwide > 0) {
+        int rc = ensure_graph(b);
+        if (rc) return rc;
+        int32_t nact = nwide;
+        const int32_t stop_at = nwide - std::max(1, nwide / 8);
+        for (int64_t done = 0; nact > 0;) {
+            if (exact && done >= budget) break;
+            if (cudaGraphLaunch(b->graph, st) != cudaSuccess) return bfail(b, PMS_ERR_CUDA, "graph launch failed");
+            done += b->graph_iters_captured;
+            if (exact) continue;
+            cudaMemcpyAsync(&nact, b->d_nactive, sizeof(int32_t), cudaMemcpyDeviceToHost, st);
+            if (cudaStreamSynchronize(st) != cudaSuccess)
+                return bfail(b, PMS_ERR_CUDA, cudaGetErrorString(cudaGetLastError()));
+            const bool block_busy = nblock > 0 && cudaEventQuery(b->ev_join) == cudaErrorNotReady;
+            if (!block_busy && (nact <= stop_at || done >= budget)) break;
+        }
+    }
+    if (nblock > 0 && cudaStreamWaitEvent(st, b->ev_join, 0) != cudaSuccess)
+        return bfail(b, PMS_ERR_CUDA, "stream join failed");
     return PMS_OK;
 }
 
@@ -553,7 +922,10 @@ int pms_batch_create(pms_elements* el, int32_t nproblem, const int64_t* point_pt
     if (b->cfg.pcg_max_iterations <= 0) b->cfg.pcg_max_iterations = 20000;
     if (!(b->cfg.pcg_rtol > 0)) b->cfg.pcg_rtol = 1e-12;
     if (b->cfg.n_max_iterations <= 0) b->cfg.n_max_iterations = 10;
-    b->graph_iters = 8;
+    b->tune.block_max_ndof = 2048;
+    b->tune.block_threads = 512;
+    b->tune.pcg_budget = 128;
+    b->tune.graph_iters = 8;
     const int nd = b->v.nd;
     b->point_ptr.assign(point_ptr, point_ptr + nproblem + 1);
     b->cell_ptr.assign(cell_ptr, cell_ptr + nproblem + 1);
@@ -570,6 +942,7 @@ int pms_batch_create(pms_elements* el, int32_t nproblem, const int64_t* point_pt
     std::vector<int32_t> node_prob(b->nnode), cell_prob(b->v.ncell);
     std::vector<int64_t> chunk_node0, pchunk(nproblem + 1, 0);
     std::vector<int32_t> chunk_nnode, chunk_prob;
+    b->pndof.assign(nproblem, 0);
     for (int p = 0; p < nproblem; p++) {
         for (int64_t i = point_ptr[p]; i < point_ptr[p + 1]; i++) node_prob[i] = p;
         for (int64_t c = cell_ptr[p]; c < cell_ptr[p + 1]; c++) cell_prob[c] = p;
@@ -579,6 +952,7 @@ int pms_batch_create(pms_elements* el, int32_t nproblem, const int64_t* point_pt
             chunk_nnode.push_back((int32_t)std::min<int64_t>(CHN, point_ptr[p + 1] - i));
             chunk_prob.push_back(p);
         }
+        b->pndof[p] = (point_ptr[p + 1] - point_ptr[p]) * nd;
     }
     pchunk[nproblem] = (int64_t)chunk_node0.size();
     b->nchunk = (int64_t)chunk_node0.size();
@@ -612,18 +986,21 @@ int pms_batch_create(pms_elements* el, int32_t nproblem, const int64_t* point_pt
               b->upload(&b->d_pres_eq, peq.data(), peq.size()) &&
               b->upload(&b->d_pres_idx, pres_idx.data(), pres_idx.size()) &&
               b->upload(&b->d_pres_prob, pres_prob.data(), pres_prob.size()) &&
-              b->alloc(&b->d_active, nproblem) && b->alloc(&b->d_pcg_active, nproblem) &&
-              b->alloc(&b->d_pcg_was, nproblem) && b->alloc(&b->d_pmode, nproblem) &&
-              b->alloc(&b->d_first, nproblem) && b->alloc(&b->d_upd, nproblem) && b->alloc(&b->d_u, n) &&
+              b->alloc(&b->d_list, nproblem) && b->alloc(&b->d_active, nproblem) &&
+              b->alloc(&b->d_pcg_active, 2 * (size_t)nproblem) && b->alloc(&b->d_cta_active, nproblem) &&
+              b->alloc(&b->d_pmode, nproblem) && b->alloc(&b->d_first, nproblem) &&
+              b->alloc(&b->d_upd, nproblem) && b->alloc(&b->d_engine, nproblem) && b->alloc(&b->d_u, n) &&
               b->alloc(&b->d_ddu, n) && b->alloc(&b->d_ff, n) && b->alloc(&b->d_csr, (size_t)b->v.nnz) &&
               b->alloc(&b->d_rr, n) && b->alloc(&b->d_mdu, n) && b->alloc(&b->d_mdu0, n) &&
               b->alloc(&b->d_kt, n) && b->alloc(&b->d_r, n) && b->alloc(&b->d_z, n) && b->alloc(&b->d_p, n) &&
               b->alloc(&b->d_q, n) && b->alloc(&b->d_x, n) && b->alloc(&b->d_binv, (size_t)b->nnode * nd * nd) &&
               b->alloc(&b->d_lam, npres) && b->alloc(&b->d_c, npres) && b->alloc(&b->d_mdl, npres) &&
-              b->alloc(&b->d_mdl0, npres) && b->alloc(&b->d_part_a, b->nchunk) && b->alloc(&b->d_part_b, b->nchunk) &&
-              b->alloc(&b->d_rho, nproblem) && b->alloc(&b->d_r0, nproblem) && b->alloc(&b->d_alpha, nproblem) &&
-              b->alloc(&b->d_beta, nproblem) && b->alloc(&b->d_norm, nproblem) && b->alloc(&b->d_rel, nproblem) &&
-              b->alloc(&b->d_iters, nproblem) && b->alloc(&b->d_nactive, 1);
+              b->alloc(&b->d_mdl0, npres) && b->alloc(&b->d_part_a, b->nchunk) &&
+              b->alloc(&b->d_part_b, b->nchunk) && b->alloc(&b->d_part_c, b->nchunk) &&
+              b->alloc(&b->d_rho, 2 * (size_t)nproblem) && b->alloc(&b->d_r0, nproblem) &&
+              b->alloc(&b->d_norm, nproblem) && b->alloc(&b->d_rel, nproblem) &&
+              b->alloc(&b->d_iters, 2 * (size_t)nproblem) &&
+              b->alloc(&b->d_nactive, 1) && b->alloc(&b->d_queue, 4 * ((size_t)nproblem + 1));
     if (ok && ff_ext) ok = b->upload(&b->d_fext, ff_ext, n);
     if (!ok) {
         delete b;
@@ -634,11 +1011,21 @@ int pms_batch_create(pms_elements* el, int32_t nproblem, const int64_t* point_pt
         delete b;
         return rc;
     }
+    if (cudaStreamCreateWithFlags(&b->st2, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&b->ev_join, cudaEventDisableTiming) != cudaSuccess || !set_block_smem()) {
+        delete b;
+        return PMS_ERR_CUDA;
+    }
     cudaMemset(b->d_u, 0, n * 8);
     cudaMemset(b->d_ddu, 0, n * 8);
     cudaMemset(b->d_lam, 0, std::max<int64_t>(npres, 1) * 8);
     cudaMemset(b->d_p, 0, n * 8);
+    cudaMemset(b->d_pcg_active, 0, 2 * (size_t)nproblem);
+    cudaMemset(b->d_cta_active, 0, nproblem);
     b->S.nd = nd;
+    b->S.np = nproblem;
+    b->S.engine = b->d_engine;
     b->S.nnode = b->nnode;
     b->S.ndof = b->ndof;
     b->S.node_prob = b->d_node_prob;
@@ -649,7 +1036,13 @@ int pms_batch_create(pms_elements* el, int32_t nproblem, const int64_t* point_pt
     b->S.pres_idx = b->d_pres_idx;
     b->S.active = b->d_active;
     b->S.pcg_active = b->d_pcg_active;
-    if (cudaDeviceSynchronize() != cudaSuccess) {
+    b->solving.assign(nproblem, 0);
+    b->engine.assign(nproblem, 0);
+    b->it.assign(nproblem, 0);
+    // a problem on the block engine keeps its chunk partials in shared memory
+    for (int p = 0; p < nproblem; p++)
+        if (pchunk[p + 1] - pchunk[p] > CTA_MAX_CHUNKS) b->pndof[p] = INT64_MAX;
+    if (assign_engines(b) || cudaDeviceSynchronize() != cudaSuccess) {
         delete b;
         return PMS_ERR_CUDA;
     }
@@ -665,6 +1058,10 @@ int pms_batch_reset(pms_batch* b) {
     cudaMemsetAsync(b->d_u, 0, b->ndof * 8, st);
     cudaMemsetAsync(b->d_ddu, 0, b->ndof * 8, st);
     cudaMemsetAsync(b->d_lam, 0, std::max<int64_t>(b->npres, 1) * 8, st);
+    cudaMemsetAsync(b->d_pcg_active, 0, 2 * (size_t)b->np, st);
+    cudaMemsetAsync(b->d_cta_active, 0, b->np, st);
+    std::fill(b->solving.begin(), b->solving.end(), 0);
+    std::fill(b->it.begin(), b->it.end(), 0);
     int rc = pms_elements_initialize(b->el);
     if (rc) return rc;
     return cudaStreamSynchronize(st) == cudaSuccess ? PMS_OK : PMS_ERR_CUDA;
@@ -676,112 +1073,164 @@ int pms_batch_tick(pms_batch* b, const uint8_t* cmd, const double* c_values, int
     if (b->npres > 0 && !c_values) return PMS_ERR_INVALID;
     cudaStream_t st = b->v.stream;
     const int np = b->np;
-    std::vector<uint8_t> running(np, 0), mode(np, 0), first(np, 0), upd(np, 0), start(np, 0);
+    std::vector<uint8_t> elem(np, 0), mode(np, 0), start(np, 0), sel(np, 0), upd(np, 0), first(np, 0);
     std::vector<int32_t> pcg_step(np, 0);
     std::vector<double> hnorm(np, 0.0), hrel(np, 0.0);
-    if ((int)b->it.size() != np) b->it.assign(np, 0);
+    bool any_elem = false;
     for (int p = 0; p < np; p++) {
         result[p] = -1;
+        if (cmd[p] == 0 || b->solving[p]) continue;  // solving problems go on with their PCG below
         if (cmd[p] == 1) {
             b->it[p] = 0;
             start[p] = 1;
         }
-        running[p] = cmd[p] != 0;
-        mode[p] = cmd[p] == 1 ? 1 : (cmd[p] == 2 ? 2 : 0);
+        elem[p] = 1;
+        mode[p] = cmd[p] == 1 ? 1 : 2;
+        any_elem = true;
     }
     if (b->npres > 0) cudaMemcpyAsync(b->d_c, c_values, b->npres * 8, cudaMemcpyHostToDevice, st);
-    // a new load step: dU = 0 (the loading time t += dt is in c_values)
-    cudaMemcpyAsync(b->d_upd, start.data(), np, cudaMemcpyHostToDevice, st);
-    zero_masked_kernel<<<grid_of(b->ndof), 256, 0, st>>>(b->S, b->d_upd, b->d_ddu);
-    // element pass: step start (assemble with lambda = 0, backup) or stress update + assemble
-    cudaMemcpyAsync(b->d_pmode, mode.data(), np, cudaMemcpyHostToDevice, st);
-    int rc = elements_run_modes(b->el, b->d_cell_prob, b->d_node_prob, b->d_pmode, b->d_ddu, b->d_ff, b->d_csr);
-    if (rc) return rc;
-    // residual and its max norm per problem
-    cudaMemcpyAsync(b->d_active, running.data(), np, cudaMemcpyHostToDevice, st);
-    residual_kernel<<<(unsigned)b->nchunk, CHN, 0, st>>>(b->S, b->d_ff, b->d_fext, b->d_u, b->d_lam, b->d_c, b->d_rr,
-                                                         b->d_part_a);
-    finalize_kernel<<<grid_of(np, 128), 128, 0, st>>>(np, b->d_pchunk, b->d_part_a, b->d_norm, 0);
-    cudaMemcpyAsync(hnorm.data(), b->d_norm, np * 8, cudaMemcpyDeviceToHost, st);
-    if (cudaStreamSynchronize(st) != cudaSuccess) return bfail(b, PMS_ERR_CUDA, "residual failed");
-    // a material or geometry error in one problem stops that problem only
-    rc = elements_status(b->el);
-    if (rc == PMS_ERR_ZERO_SIGMA_D || rc == PMS_ERR_ZERO_NORM_S || rc == PMS_ERR_JACOBIAN) {
-        int64_t cell = -1;
-        int32_t ip = -1;
-        pms_elements_error_location(b->el, &cell, &ip);
-        const int p = (int)(std::upper_bound(b->cell_ptr.begin(), b->cell_ptr.end(), cell) - b->cell_ptr.begin()) - 1;
-        if (p >= 0 && p < np && running[p]) {
-            result[p] = 100 + 1 + rc;  // 104: zero sigma_d, 105: zero norm_s, 106: Jacobian
-            running[p] = 0;
-        }
-    } else if (rc) {
-        return rc;
-    }
-    bool any = false;
-    for (int p = 0; p < np; p++) {
-        if (!running[p]) continue;
-        if (iteration) iteration[p] = b->it[p];
-        if (norm_rr) norm_rr[p] = hnorm[p];
-        if (!std::isfinite(hnorm[p])) {
-            result[p] = 101;  // "Found NaN or Inf"
-            running[p] = 0;
-        } else if (hnorm[p] < b->cfg.tol_rr_abs) {
-            result[p] = 1;
-            running[p] = 0;
-        }
-        any = any || running[p];
-    }
-    if (any) {
-        // linear solve (mdu, mdl) for the problems still iterating
-        cudaMemcpyAsync(b->d_active, running.data(), np, cudaMemcpyHostToDevice, st);
-        block_jacobi_kernel<<<grid_of(b->nnode), 256, 0, st>>>(b->S, b->v.d_bptr, b->v.d_kdiag, b->d_csr, b->d_binv);
-        pres_increment_kernel<<<grid_of(b->ndof), 256, 0, st>>>(b->S, b->d_u, b->d_c, b->d_mdu);
-        launch_spmv(b, b->d_mdu, b->d_kt, b->d_active, false);
-        pcg_start_kernel<<<(unsigned)b->nchunk, CHN, 0, st>>>(b->S, b->d_rr, b->d_kt, b->d_binv, b->d_r, b->d_x,
-                                                               b->d_z, b->d_p, b->d_part_a, b->d_part_b);
-        pcg_init_scalars_kernel<<<grid_of(np, 128), 128, 0, st>>>(np, b->d_active, b->d_pchunk, b->d_part_a,
-                                                                   b->d_part_b, b->d_rho, b->d_r0, b->d_pcg_active,
-                                                                   b->d_iters);
-        rc = run_pcg(b);
-        if (rc) return rc;
-        cudaMemcpyAsync(pcg_step.data(), b->d_iters, np * 4, cudaMemcpyDeviceToHost, st);
-        assemble_mdu_kernel<<<grid_of(b->ndof), 256, 0, st>>>(b->S, b->d_x, b->d_mdu);
-        if (b->npres > 0)
-            multiplier_kernel<<<grid_of(b->npres), 256, 0, st>>>(b->npres, b->d_pres_eq, b->d_pres_prob, b->d_active,
-                                                                  b->d_indptr, b->d_indices, b->d_csr, b->d_mdu,
-                                                                  b->d_rr, b->d_mdl);
-        for (int p = 0; p < np; p++) first[p] = (b->it[p] == 0);
-        cudaMemcpyAsync(b->d_first, first.data(), np, cudaMemcpyHostToDevice, st);
-        rel_mdu_kernel<<<(unsigned)b->nchunk, CHN, 0, st>>>(b->S, b->d_first, b->d_mdu, b->d_mdu0, b->d_part_a);
-        finalize_kernel<<<grid_of(np, 128), 128, 0, st>>>(np, b->d_pchunk, b->d_part_a, b->d_rel, 0);
-        rel_multipliers_kernel<<<grid_of(np, 128), 128, 0, st>>>(np, b->d_active, b->d_first, b->d_ppres, b->d_mdl,
-                                                                  b->d_mdl0, b->d_rel);
-        cudaMemcpyAsync(hrel.data(), b->d_rel, np * 8, cudaMemcpyDeviceToHost, st);
-        if (cudaStreamSynchronize(st) != cudaSuccess) return bfail(b, PMS_ERR_CUDA, "solve failed");
+    int rc;
+    // ---- stage 1: element pass, residual and its test for the problems that need them
+    if (any_elem) {
+        cudaMemcpyAsync(b->d_upd, start.data(), np, cudaMemcpyHostToDevice, st);
+        zero_masked_kernel<<<grid_of(b->ndof), 256, 0, st>>>(b->S, b->d_upd, b->d_ddu);  // new step: dU = 0
+        cudaMemcpyAsync(b->d_pmode, mode.data(), np, cudaMemcpyHostToDevice, st);
+        // work queue: the cell and node ranges of these problems only
+        const size_t W = (size_t)np + 1;
+        b->h_queue.assign(4 * W, 0);
+        WorkQueue q;
         for (int p = 0; p < np; p++) {
-            upd[p] = 0;
-            if (!running[p]) continue;
-            if (pcg_iterations) pcg_iterations[p] = pcg_step[p];
-            b->pcg_total += pcg_step[p];
-            if (!std::isfinite(hrel[p])) {
-                result[p] = 102;  // "Found NaN or Inf in mdu"
-            } else if (b->it[p] > 0 && hrel[p] < b->cfg.tol_mdu_rel) {
-                result[p] = 1;  // converged without applying this correction
+            if (!elem[p]) continue;
+            const int k = q.nq++;
+            b->h_queue[k + 1] = b->h_queue[k] + (b->cell_ptr[p + 1] - b->cell_ptr[p]);
+            b->h_queue[W + k] = b->cell_ptr[p];
+            b->h_queue[2 * W + k + 1] = b->h_queue[2 * W + k] + (b->point_ptr[p + 1] - b->point_ptr[p]);
+            b->h_queue[3 * W + k] = b->point_ptr[p];
+        }
+        q.ncell = b->h_queue[q.nq];
+        q.nnode = b->h_queue[2 * W + q.nq];
+        q.cell_off = b->d_queue;
+        q.cell_first = b->d_queue + W;
+        q.node_off = b->d_queue + 2 * W;
+        q.node_first = b->d_queue + 3 * W;
+        cudaMemcpyAsync(b->d_queue, b->h_queue.data(), 4 * W * 8, cudaMemcpyHostToDevice, st);
+        rc = elements_run_modes(b->el, b->d_cell_prob, b->d_node_prob, b->d_pmode, b->d_ddu, b->d_ff, b->d_csr, &q);
+        if (rc) return rc;
+        cudaMemcpyAsync(b->d_active, elem.data(), np, cudaMemcpyHostToDevice, st);
+        residual_kernel<<<(unsigned)b->nchunk, CHN, 0, st>>>(b->S, b->d_ff, b->d_fext, b->d_u, b->d_lam, b->d_c,
+                                                             b->d_rr, b->d_part_a);
+        finalize_kernel<<<grid_of(np, 128), 128, 0, st>>>(np, b->d_pchunk, b->d_part_a, b->d_norm, 0);
+        cudaMemcpyAsync(hnorm.data(), b->d_norm, np * 8, cudaMemcpyDeviceToHost, st);
+        if (cudaStreamSynchronize(st) != cudaSuccess) return bfail(b, PMS_ERR_CUDA, "residual failed");
+        b->launches += 4;
+        // a material or geometry error in one problem stops that problem only
+        rc = elements_status(b->el);
+        if (rc == PMS_ERR_ZERO_SIGMA_D || rc == PMS_ERR_ZERO_NORM_S || rc == PMS_ERR_JACOBIAN) {
+            int64_t cell = -1;
+            int32_t ip = -1;
+            pms_elements_error_location(b->el, &cell, &ip);
+            const int p =
+                (int)(std::upper_bound(b->cell_ptr.begin(), b->cell_ptr.end(), cell) - b->cell_ptr.begin()) - 1;
+            if (p >= 0 && p < np && elem[p]) {
+                result[p] = 100 + 1 + rc;  // 104: zero sigma_d, 105: zero norm_s, 106: Jacobian
+                elem[p] = 0;
+            }
+        } else if (rc) {
+            return rc;
+        }
+        bool any_start = false;
+        for (int p = 0; p < np; p++) {
+            if (!elem[p]) continue;
+            if (iteration) iteration[p] = b->it[p];
+            if (norm_rr) norm_rr[p] = hnorm[p];
+            if (!std::isfinite(hnorm[p])) {
+                result[p] = 101;  // "Found NaN or Inf"
+            } else if (hnorm[p] < b->cfg.tol_rr_abs) {
+                result[p] = 1;
             } else {
-                upd[p] = 1;
-                b->it[p] += 1;
-                result[p] = (b->it[p] >= b->cfg.n_max_iterations) ? 103 : 0;  // 103: did not converge
+                sel[p] = 1;  // needs the linear solve
+                b->solving[p] = 1;
+                any_start = true;
             }
         }
-        cudaMemcpyAsync(b->d_upd, upd.data(), np, cudaMemcpyHostToDevice, st);
-        update_kernel<<<grid_of(b->ndof), 256, 0, st>>>(b->S, b->d_upd, b->d_mdu, b->d_u, b->d_ddu);
-        if (b->npres > 0)
-            update_multipliers_kernel<<<grid_of(b->npres), 256, 0, st>>>(b->npres, b->d_pres_prob, b->d_upd, b->d_mdl,
-                                                                          b->d_lam);
-        b->launches += 12;
+        // ---- stage 2: start the linear solve (mdu, mdl) of those problems
+        if (any_start) {
+            cudaMemcpyAsync(b->d_active, sel.data(), np, cudaMemcpyHostToDevice, st);
+            pcg_start(b);
+        }
     }
-    b->launches += 4;
+    // ---- stage 3: PCG iterations of every solving problem
+    int nblock = 0, nwide = 0;
+    b->h_list.clear();
+    for (int p = 0; p < np; p++) {
+        if (!b->solving[p]) continue;
+        if (b->engine[p]) {
+            b->h_list.push_back(p);
+            nblock++;
+        } else {
+            nwide++;
+        }
+    }
+    if (nblock > 0) cudaMemcpyAsync(b->d_list, b->h_list.data(), nblock * 4, cudaMemcpyHostToDevice, st);
+    if (nblock + nwide > 0) {
+        rc = pcg_phase(b, nblock, nwide, std::max(1, b->tune.pcg_budget), false);
+        if (rc) return rc;
+        std::vector<uint8_t> wa(np), ca(np);
+        cudaMemcpyAsync(wa.data(), b->d_pcg_active, np, cudaMemcpyDeviceToHost, st);
+        cudaMemcpyAsync(ca.data(), b->d_cta_active, np, cudaMemcpyDeviceToHost, st);
+        cudaMemcpyAsync(pcg_step.data(), b->d_iters, np * 4, cudaMemcpyDeviceToHost, st);
+        if (cudaStreamSynchronize(st) != cudaSuccess) return bfail(b, PMS_ERR_CUDA, "PCG failed");
+        // ---- stage 4: problems whose PCG finished complete their Newton iteration
+        bool any_fin = false;
+        for (int p = 0; p < np; p++) {
+            sel[p] = 0;
+            if (!b->solving[p]) continue;
+            if (wa[p] || ca[p]) {
+                result[p] = 2;  // still solving
+                continue;
+            }
+            sel[p] = 1;
+            first[p] = (b->it[p] == 0);
+            any_fin = true;
+        }
+        if (any_fin) {
+            cudaMemcpyAsync(b->d_active, sel.data(), np, cudaMemcpyHostToDevice, st);
+            assemble_mdu_kernel<<<grid_of(b->ndof), 256, 0, st>>>(b->S, b->d_x, b->d_mdu);
+            if (b->npres > 0)
+                multiplier_kernel<<<grid_of(b->npres), 256, 0, st>>>(b->npres, b->d_pres_eq, b->d_pres_prob,
+                                                                      b->d_active, b->d_indptr, b->d_indices,
+                                                                      b->d_csr, b->d_mdu, b->d_rr, b->d_mdl);
+            cudaMemcpyAsync(b->d_first, first.data(), np, cudaMemcpyHostToDevice, st);
+            rel_mdu_kernel<<<(unsigned)b->nchunk, CHN, 0, st>>>(b->S, b->d_first, b->d_mdu, b->d_mdu0, b->d_part_a);
+            finalize_kernel<<<grid_of(np, 128), 128, 0, st>>>(np, b->d_pchunk, b->d_part_a, b->d_rel, 0);
+            rel_multipliers_kernel<<<grid_of(np, 128), 128, 0, st>>>(np, b->d_active, b->d_first, b->d_ppres,
+                                                                      b->d_mdl, b->d_mdl0, b->d_rel);
+            cudaMemcpyAsync(hrel.data(), b->d_rel, np * 8, cudaMemcpyDeviceToHost, st);
+            if (cudaStreamSynchronize(st) != cudaSuccess) return bfail(b, PMS_ERR_CUDA, "solve failed");
+            for (int p = 0; p < np; p++) {
+                if (!sel[p]) continue;
+                b->solving[p] = 0;
+                if (iteration) iteration[p] = b->it[p];
+                if (pcg_iterations) pcg_iterations[p] = pcg_step[p];
+                b->pcg_total += pcg_step[p];
+                if (!std::isfinite(hrel[p])) {
+                    result[p] = 102;  // "Found NaN or Inf in mdu"
+                } else if (b->it[p] > 0 && hrel[p] < b->cfg.tol_mdu_rel) {
+                    result[p] = 1;  // converged without applying this correction
+                } else {
+                    upd[p] = 1;
+                    b->it[p] += 1;
+                    result[p] = (b->it[p] >= b->cfg.n_max_iterations) ? 103 : 0;  // 103: did not converge
+                }
+            }
+            cudaMemcpyAsync(b->d_upd, upd.data(), np, cudaMemcpyHostToDevice, st);
+            update_kernel<<<grid_of(b->ndof), 256, 0, st>>>(b->S, b->d_upd, b->d_mdu, b->d_u, b->d_ddu);
+            if (b->npres > 0)
+                update_multipliers_kernel<<<grid_of(b->npres), 256, 0, st>>>(b->npres, b->d_pres_prob, b->d_upd,
+                                                                              b->d_mdl, b->d_lam);
+            b->launches += 7;
+        }
+    }
     if (cudaStreamSynchronize(st) != cudaSuccess) return bfail(b, PMS_ERR_CUDA, "tick failed");
     return PMS_OK;
 }
@@ -803,8 +1252,12 @@ int pms_batch_solve_step(pms_batch* b, const double* c_values, const uint8_t* ac
         if (rc) return rc;
         for (int p = 0; p < np; p++) {
             if (!cmd[p]) continue;
-            count[p] += 1;  // residual evaluations, as the reference counts iterations
             pcg_sum[p] += pcg[p];
+            if (res[p] == 2) {  // linear solve still under way
+                cmd[p] = 2;
+                continue;
+            }
+            count[p] += 1;  // one Newton iteration (residual evaluation, as the reference counts them)
             last_norm[p] = norm[p];
             if (res[p] == 0) {
                 cmd[p] = 2;
@@ -821,6 +1274,142 @@ int pms_batch_solve_step(pms_batch* b, const double* c_values, const uint8_t* ac
         if (pcg_iterations) pcg_iterations[p] = pcg_sum[p];
     }
     return PMS_OK;
+}
+
+int pms_batch_set_tuning(pms_batch* b, const pms_batch_tuning* t) {
+    if (!b || !t) return PMS_ERR_INVALID;
+    if (t->block_threads != 128 && t->block_threads != 256 && t->block_threads != 512 && t->block_threads != 1024)
+        return PMS_ERR_INVALID;
+    if (t->pcg_budget < 1 || t->graph_iters < 1 || t->graph_iters > 64 || t->block_max_ndof < 0)
+        return PMS_ERR_INVALID;
+    for (int p = 0; p < b->np; p++)
+        if (b->solving[p]) return bfail(b, PMS_ERR_INVALID, "tuning cannot change while a linear solve is under way");
+    b->tune = *t;
+    if (cudaStreamSynchronize(b->v.stream) != cudaSuccess) return PMS_ERR_CUDA;
+    return assign_engines(b);
+}
+
+int pms_batch_get_tuning(const pms_batch* b, pms_batch_tuning* t) {
+    if (!b || !t) return PMS_ERR_INVALID;
+    *t = b->tune;
+    return PMS_OK;
+}
+
+namespace {
+
+// Sets up every problem's PCG on its initial tangent with a unit right-hand side (after
+// pms_batch_reset): step-start element pass, block-Jacobi, r = 1 on the free rows.
+int timing_setup(pms_batch* b) {
+    for (int p = 0; p < b->np; p++)
+        if (b->solving[p]) return bfail(b, PMS_ERR_INVALID, "timing needs a batch with no solve under way");
+    cudaStream_t st = b->v.stream;
+    const int np = b->np;
+    int rc = pms_batch_reset(b);
+    if (rc) return rc;
+    std::vector<uint8_t> all(np, 1);
+    cudaMemcpyAsync(b->d_pmode, all.data(), np, cudaMemcpyHostToDevice, st);
+    rc = elements_run_modes(b->el, b->d_cell_prob, b->d_node_prob, b->d_pmode, b->d_ddu, b->d_ff, b->d_csr);
+    if (rc) return rc;
+    rc = elements_status(b->el);
+    if (rc) return rc;
+    cudaMemcpyAsync(b->d_active, all.data(), np, cudaMemcpyHostToDevice, st);
+    fill_masked_kernel<<<grid_of(b->ndof), 256, 0, st>>>(b->S, b->d_active, b->d_rr, 1.0);
+    std::vector<double> zc(std::max<int64_t>(b->npres, 1), 0.0);
+    cudaMemcpyAsync(b->d_c, zc.data(), std::max<int64_t>(b->npres, 1) * 8, cudaMemcpyHostToDevice, st);
+    return cudaStreamSynchronize(st) == cudaSuccess ? PMS_OK : bfail(b, PMS_ERR_CUDA, "timing setup failed");
+}
+
+// Device time (ms) of `iters` PCG iterations of every problem with the given launch shapes (second
+// of two runs, the first warms up), after timing_setup.
+int time_candidate(pms_batch* b, const pms_batch_tuning& cand, int iters, float* ms_out) {
+    cudaStream_t st = b->v.stream;
+    const int np = b->np;
+    b->tune = cand;
+    int rc = assign_engines(b);
+    if (rc) return rc;
+    int nblock = 0, nwide = 0;
+    b->h_list.clear();
+    for (int p = 0; p < np; p++) {
+        if (b->engine[p]) {
+            b->h_list.push_back(p);
+            nblock++;
+        } else {
+            nwide++;
+        }
+    }
+    if (nblock > 0) cudaMemcpyAsync(b->d_list, b->h_list.data(), nblock * 4, cudaMemcpyHostToDevice, st);
+    std::vector<uint8_t> all(np, 1);
+    cudaMemcpyAsync(b->d_active, all.data(), np, cudaMemcpyHostToDevice, st);
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    float ms = 0.0f;
+    for (int rep = 0; rep < 2 && !rc; rep++) {
+        pcg_start(b);
+        cudaEventRecord(e0, st);
+        rc = pcg_phase(b, nblock, nwide, iters, true);
+        cudaEventRecord(e1, st);
+        if (cudaEventSynchronize(e1) != cudaSuccess) rc = bfail(b, PMS_ERR_CUDA, "timing run failed");
+        cudaEventElapsedTime(&ms, e0, e1);
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    *ms_out = ms;
+    return rc;
+}
+
+}  // namespace
+
+int pms_batch_time_pcg(pms_batch* b, const pms_batch_tuning* t, int32_t iterations, double* ms) {
+    if (!b || !t || !ms || iterations < 1) return PMS_ERR_INVALID;
+    const pms_batch_tuning keep = b->tune;
+    int rc = pms_batch_set_tuning(b, t);
+    if (rc) return rc;
+    rc = timing_setup(b);
+    float m = 0.0f;
+    if (!rc) rc = time_candidate(b, *t, iterations, &m);
+    *ms = m;
+    b->tune = keep;
+    int rc2 = assign_engines(b);
+    int rc3 = pms_batch_reset(b);
+    return rc ? rc : (rc2 ? rc2 : rc3);
+}
+
+int pms_batch_autotune(pms_batch* b, pms_batch_tuning* out) {
+    if (!b) return PMS_ERR_INVALID;
+    int rc = timing_setup(b);
+    if (rc) return rc;
+    const int np = b->np;
+    // candidates: engine threshold x block size; the batch-wide engine alone first
+    int64_t maxdof = 0;
+    for (int p = 0; p < np; p++)
+        if (b->pndof[p] != INT64_MAX) maxdof = std::max(maxdof, b->pndof[p]);
+    std::vector<int64_t> thr = {0};
+    for (int64_t t = 1024; t < maxdof; t *= 2) thr.push_back(t);
+    if (maxdof > 0) thr.push_back(maxdof);
+    const int sizes[3] = {256, 512, 1024};
+    const pms_batch_tuning keep = b->tune;
+    pms_batch_tuning best = keep;
+    float best_ms = 1e30f;
+    for (int64_t t : thr) {
+        for (int si = 0; si < (t == 0 ? 1 : 3) && !rc; si++) {
+            pms_batch_tuning cand = keep;
+            cand.block_max_ndof = t;
+            cand.block_threads = t == 0 ? keep.block_threads : sizes[si];
+            float ms = 0.0f;
+            rc = time_candidate(b, cand, 32, &ms);
+            if (!rc && ms < best_ms) {
+                best_ms = ms;
+                best = cand;
+            }
+        }
+        if (rc) break;
+    }
+    b->tune = rc ? keep : best;
+    int rc2 = assign_engines(b);
+    int rc3 = pms_batch_reset(b);
+    if (!rc && out) *out = b->tune;
+    return rc ? rc : (rc2 ? rc2 : rc3);
 }
 
 int pms_batch_get_u(pms_batch* b, double* u) {

@@ -52,10 +52,16 @@ class Request:
 
 
 class Server:
-    def __init__(self, budget_bytes=120e9, max_batch=256, max_concurrent=4, keep_results=False, **solver_kw):
+    """``admit_window``: a waiting request is admitted once it has waited this long (seconds), together
+    with everything that arrived since (one batch per element kind), so that bursts share a batch;
+    ``max_concurrent`` batches run at a time, each on its own stream and host thread."""
+
+    def __init__(self, budget_bytes=120e9, max_batch=256, max_concurrent=16, admit_window=0.025,
+                 keep_results=False, **solver_kw):
         self.budget = float(budget_bytes)
         self.max_batch = max_batch
         self.max_concurrent = max_concurrent
+        self.admit_window = float(admit_window)
         self.keep_results = keep_results
         self.solver_kw = solver_kw
         self.in_use = 0.0
@@ -74,6 +80,9 @@ class Server:
             u = bs.u() if self.keep_results else None
             for i, r in enumerate(reqs):
                 r.finished = bs.finish.get(i, clock())
+                r.meta["newton"] = int(sum(bs.history[i]))
+                r.meta["pcg"] = int(sum(bs.pcg_history[i]))
+                r.meta["batch_size"] = len(reqs)
                 if i in bs.failed:
                     r.error = bs.failed[i][1]
                 if u is not None:
@@ -110,7 +119,10 @@ class Server:
             groups = {}
             with self.lock:
                 keep = []
-                if self.live >= self.max_concurrent:
+                # hold the wave until its oldest request has waited admit_window (or the stream ended)
+                ready = bool(waiting) and (now - min(r.arrival for r in waiting) >= self.admit_window
+                                           or k >= len(pending) or not realtime)
+                if self.live >= self.max_concurrent or not ready:
                     keep, waiting = waiting, []
                 for r in waiting:
                     kind = (r.problem.mesh.kind, r.problem.ngauss)

@@ -117,3 +117,36 @@ def test_independent_progress_matches_lock_step():
     for x, y in zip(a.elements.get_state(), b.elements.get_state()):
         assert np.array_equal(x, y)
     assert a.history == b.history
+
+
+def test_pcg_engines_give_the_same_bits():
+    """The block engine (one thread block per problem) and the batch-wide engine run the same
+    arithmetic: forcing either one, or letting the autotuner choose, gives identical U, IP state
+    and Newton/PCG iteration histories."""
+    from pmsim_b200.batch import BatchSolver
+    rng = np.random.default_rng(21)
+    probs = [footing(int(rng.integers(4, 16)), int(rng.integers(2, 8)), float(1e4 * np.exp(rng.normal(0, 0.5))),
+                     float(rng.uniform(5, 20)), float(rng.uniform(0.5, 2.0)), nsteps=3) for _ in range(6)]
+    runs = []
+    for setting in ("wide", "block", "mixed", "auto"):
+        bs = BatchSolver(probs)
+        if setting == "wide":
+            bs.set_tuning(block_max_ndof=0)
+        elif setting == "block":
+            bs.set_tuning(block_max_ndof=10 ** 9, block_threads=256, pcg_budget=7)
+        elif setting == "mixed":
+            nd = sorted(p.mesh.ndof for p in probs)
+            bs.set_tuning(block_max_ndof=nd[len(nd) // 2], block_threads=1024, graph_iters=2, pcg_budget=16)
+        else:
+            bs.autotune()
+        bs.solve_independent(on_fail="drop")
+        runs.append((setting, bs.u(), bs.elements.get_state(), bs.history, bs.pcg_history, dict(bs.failed)))
+        bs.close()
+    _, u0, st0, h0, pc0, f0 = runs[0]
+    for name, u, st, h, pc, f in runs[1:]:
+        assert f == f0, name
+        assert np.array_equal(u, u0), f"{name}: U differs from the batch-wide engine"
+        for x, y in zip(st, st0):
+            assert np.array_equal(x, y), name
+        assert h == h0, name
+        assert pc == pc0, name
