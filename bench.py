@@ -272,8 +272,8 @@ def run_batched(nprob, nalone, seed=2024):
     t_alone, ok_alone = 0.0, 0
     for i in sample:
         b1 = BatchSolver([probs[i]], n_max_iterations=20, pcg_max_iterations=5000)
-        torch.cuda.synchronize()
         t0 = time.perf_counter()
+        b1.autotune()  # its own best launch shapes, timed with the solve
         b1.solve_independent(on_fail="drop")
         torch.cuda.synchronize()
         t_alone += time.perf_counter() - t0
@@ -377,8 +377,8 @@ def run_served(nreq, rate, nalone, seed=7, detail_file=""):
     t_alone, ok = 0.0, 0
     for i in sample:
         b1 = BatchSolver([probs[i]], n_max_iterations=20, pcg_max_iterations=5000)
-        torch.cuda.synchronize()
         t0 = time.perf_counter()
+        b1.autotune()  # its own best launch shapes, timed with the solve
         b1.solve_independent(on_fail="drop")
         torch.cuda.synchronize()
         t_alone += time.perf_counter() - t0

@@ -206,23 +206,27 @@ int pms_batch_solve_step(pms_batch* b, const double* c_values, const uint8_t* ac
  * iteration is completed by this tick). */
 int pms_batch_tick(pms_batch* b, const uint8_t* cmd, const double* c_values, int32_t* result, int32_t* iteration,
                    double* norm_rr, int32_t* pcg_iterations);
-/* Launch shapes of the PCG (they change speed only: both engines compute bit-identical iterates).
- * Problems with at most block_max_ndof DOFs run their whole PCG in one thread block of
- * block_threads threads (128, 256, 512 or 1024) at their own pace; larger problems run the
- * batch-wide kernels, graph_iters iterations per CUDA-graph launch.  pcg_budget bounds the PCG
- * iterations a problem gets per tick.  No counterpart in the reference (its solve is a direct
- * factorisation, src/fem/linear_system.rs:185-201). */
+/* Launch shapes of the PCG (they change speed only: every engine computes bit-identical iterates).
+ * A problem with at most team_max_ndof DOFs runs its whole PCG on a thread-block cluster ("team")
+ * of C = 1, 2, 4, 8 or 16 CTAs of team_threads threads (256, 512 or 1024), its vectors resident in
+ * the CTAs' shared memory; C is the smallest team whose CTAs hold at most team_chunks 128-node
+ * chunks each (0: as many as fit).  Other problems run the batch-wide kernels, graph_iters
+ * iterations per CUDA-graph launch.  pcg_budget bounds the PCG iterations a problem gets per tick.
+ * No counterpart in the reference (its solve is a direct factorisation,
+ * src/fem/linear_system.rs:185-201). */
 typedef struct pms_batch_tuning {
-    int64_t block_max_ndof;
-    int32_t block_threads;
+    int64_t team_max_ndof;
+    int32_t team_threads;
+    int32_t team_chunks;
     int32_t pcg_budget;
     int32_t graph_iters;
 } pms_batch_tuning;
 int pms_batch_set_tuning(pms_batch* b, const pms_batch_tuning* t);
 int pms_batch_get_tuning(const pms_batch* b, pms_batch_tuning* t);
 /* Autotuner: times 32 PCG iterations of every problem on its initial tangent (unit right-hand
- * side) for each candidate engine threshold and block size, keeps the fastest, then resets the
- * batch (pms_batch_reset).  *out (nullable) receives the choice. */
+ * side) for each candidate (batch-wide only; teams up to several sizes, CTA sizes and chunks per
+ * CTA), keeps the fastest, then resets the batch (pms_batch_reset).  *out (nullable) receives the
+ * choice. */
 int pms_batch_autotune(pms_batch* b, pms_batch_tuning* out);
 /* Instrumentation (the autotuner's measurement): device time in ms of `iterations` PCG iterations
  * of every problem, on its initial tangent, with the launch shapes *t; resets the batch and keeps

@@ -60,8 +60,8 @@ class BatchConfig_(ctypes.Structure):
 
 
 class BatchTuning_(ctypes.Structure):
-    _fields_ = [("block_max_ndof", ctypes.c_int64), ("block_threads", ctypes.c_int32),
-                ("pcg_budget", ctypes.c_int32), ("graph_iters", ctypes.c_int32)]
+    _fields_ = [("team_max_ndof", ctypes.c_int64), ("team_threads", ctypes.c_int32),
+                ("team_chunks", ctypes.c_int32), ("pcg_budget", ctypes.c_int32), ("graph_iters", ctypes.c_int32)]
 
 
 class Info_(ctypes.Structure):

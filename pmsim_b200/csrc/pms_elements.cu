@@ -133,45 +133,53 @@ __device__ __forceinline__ double inv_jacobian(const double* J, double* Ji) {
     }
 }
 
+// Warps per cell: the 20-node kinds split the node-pair triangle over two warps (2x2 register
+// tiles), which halves the registers of a thread and doubles the warps an SM can hold.
+__host__ __device__ constexpr int warps_per_cell(int nn) { return nn >= 16 ? 2 : 1; }
+__host__ __device__ constexpr int cells_per_block(int nn) { return WPB / warps_per_cell(nn); }
+
 // Register tile of node pairs per lane: rows (a) x cols (b) of the upper node-pair triangle.
-// The tile shapes keep the number of tiles <= 32 (one tile per lane).
+// The tile shapes keep the number of tiles <= 32 per warp of the cell.
 template <int NN> struct TileShape {
     static constexpr int RT = NN >= 16 ? 2 : 1;
-    static constexpr int CT = NN >= 16 ? 4 : (NN >= 7 ? 2 : 1);
+    static constexpr int CT = warps_per_cell(NN) == 2 ? 2 : (NN >= 7 ? 2 : 1);
     static constexpr int NRG = (NN + RT - 1) / RT;
     static constexpr int NCG = (NN + CT - 1) / CT;
 };
 
-// Shared memory (doubles): block-wide dN table [m][j][32] + w[32], then per warp
+// Shared memory (doubles): block-wide dN table [m][j][32] + w[32], then per cell
 // X[NN*ND], dU[NN*ND], G[ng][NN*ND+1] (gradients), TC[ng][10] (alpha, gamma, beta, S), CS[ng][6],
-// V[NN][5*ND] (per node at the current IP: alpha g, gamma g, beta h, g, h with h = S g).
+// V[2][NN][5*ND] (per node at the current IP, double-buffered: alpha g, gamma g, beta h, g, h with
+// h = S g).
 __host__ __device__ constexpr int smem_table_doubles(int nn, int nd) { return nn * nd * 32 + 32; }
-__host__ __device__ constexpr int smem_warp_doubles(int nn, int nd, int ng) {
-    return 2 * nn * nd + ng * (nn * nd + 1) + ng * 10 + ng * 6 + nn * 5 * nd;
+__host__ __device__ constexpr int smem_cell_doubles(int nn, int nd, int ng) {
+    return 2 * nn * nd + ng * (nn * nd + 1) + ng * 10 + ng * 6 + 2 * nn * 5 * nd;
 }
 __host__ __device__ constexpr int smem_bytes_for(int nn, int nd, int ng, int wpb) {
-    return (smem_table_doubles(nn, nd) + wpb * smem_warp_doubles(nn, nd, ng)) * 8;
+    return (smem_table_doubles(nn, nd) + (wpb / warps_per_cell(nn)) * smem_cell_doubles(nn, nd, ng)) * 8;
 }
 
 template <int ND, int NN, int UPD, bool DOF, bool DOK>
-__global__ void __launch_bounds__(WPB * 32) element_kernel(ElemArgs A) {
+__global__ void __launch_bounds__(WPB * 32, warps_per_cell(NN) == 2 ? 3 : 1) element_kernel(ElemArgs A) {
     constexpr int NC = 2 * ND;
     constexpr int NE = NN * ND;
     constexpr int GS = NE + 1;  // gradient row stride (odd: spreads the banks of phase-1 stores)
     using TS = TileShape<NN>;
     constexpr int RT = TS::RT, CT = TS::CT;
+    constexpr int WPC = warps_per_cell(NN), CPB = WPB / WPC;
     extern __shared__ double smem[];
     const int ng = A.ngauss;
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int cs = wid / WPC, half = wid % WPC;  // cell slot in the block, warp within the cell
     double* dNs = smem;                        // [m][j][32]
     double* ws = smem + NE * 32;               // [32]
-    double* wbase = smem + smem_table_doubles(NN, ND) + wid * smem_warp_doubles(NN, ND, ng);
+    double* wbase = smem + smem_table_doubles(NN, ND) + cs * smem_cell_doubles(NN, ND, ng);
     double* Xs = wbase;                        // [m][d]
     double* Us = Xs + NE;                      // [m][d]
     double* G = Us + NE;                       // [p][GS]
     double* TC = G + ng * GS;                  // [p][10]
     double* CS = TC + ng * 10;                 // [p][6]
-    double* V = CS + ng * 6;                   // [m][5*ND]
+    double* V0 = CS + ng * 6;                  // [2][m][5*ND]
 
     // stage dN transposed (IP index fastest) so that lane p reads its IP without bank conflicts
     for (int i = threadIdx.x; i < ng * NE; i += blockDim.x) {
@@ -181,18 +189,24 @@ __global__ void __launch_bounds__(WPB * 32) element_kernel(ElemArgs A) {
     for (int i = threadIdx.x; i < ng; i += blockDim.x) ws[i] = A.tab[ng * NE + i];
     __syncthreads();
 
-    const int64_t cl = (int64_t)blockIdx.x * WPB + wid;
-    if (cl >= A.ncell) return;  // whole warp exits together
+    // the warps of one cell meet at a named barrier (id 1 + cell slot)
+    auto cell_sync = [&]() {
+        if constexpr (WPC == 1) __syncwarp();
+        else asm volatile("bar.sync %0, %1;" ::"r"(1 + cs), "r"(32 * WPC) : "memory");
+    };
+    const int64_t cl = (int64_t)blockIdx.x * CPB + cs;
+    if (cl >= A.ncell) return;  // the cell's warps exit together
     const int64_t cell = A.nq ? queue_item(cl, A.nq, A.q_off, A.q_first) : A.cell0 + cl;
     int mode = (UPD == UPD_NONE) ? 0 : 2;
     if (UPD == UPD_MODE) {
         mode = A.pmode[A.cell_prob[cell]];
-        if (mode == 0) return;  // inactive problem: whole warp exits
+        if (mode == 0) return;  // inactive problem: the cell's warps exit together
     }
     const bool do_update = (UPD == UPD_MODE) ? (mode == 2) : (UPD != UPD_NONE);
     const bool from_backup = (UPD == UPD_BACKUP) || (UPD == UPD_MODE && mode == 2);
     const MatConst mc = A.mats[A.cmat ? A.cmat[cell] : 0];
 
+    if (half == 0) {  // warp 0 of the cell: node data, integration points, F_int
     if (lane < NN) {
         const int pt = A.conn[cell * NN + lane];
 #pragma unroll
@@ -346,17 +360,21 @@ __global__ void __launch_bounds__(WPB * 32) element_kernel(ElemArgs A) {
         for (int i = 0; i < ND; i++) A.fe[(cell * NN + lane) * ND + i] = f[i];
     }
 
+    }  // warp 0
+    cell_sync();  // G and TC are visible to every warp of the cell
+
     // ---------------- phase 2: lane owns a tile of node-pair blocks ----------------
     if (DOK) {
-        // the lane-th tile (i, j) with i*RT <= min(j*CT + CT - 1, NN - 1), row-major
+        // tile number lane + 32*half: (i, j) with i*RT <= min(j*CT + CT - 1, NN - 1), row-major
         int ti = -1, tj = -1;
         {
+            const int me = lane + 32 * half;
             int k = 0;
             for (int i = 0; i < TS::NRG; i++)
                 for (int j = 0; j < TS::NCG; j++) {
                     const int jmax = min(j * CT + CT - 1, NN - 1);
                     if (i * RT <= jmax) {
-                        if (k == lane) { ti = i; tj = j; }
+                        if (k == me) { ti = i; tj = j; }
                         k++;
                     }
                 }
@@ -375,9 +393,9 @@ __global__ void __launch_bounds__(WPB * 32) element_kernel(ElemArgs A) {
         for (int p = 0; p < ng; p++) {
             const double* t = TC + p * 10;
             const bool plastic = t[2] != 0.0;  // beta: same value on every lane, uniform branch
-            // node lanes: the scaled gradients of their node at this IP
-            __syncwarp();
-            if (lane < NN) {
+            double* V = V0 + (p & 1) * NN * VS;  // double buffer: one barrier per IP
+            // node lanes of warp 0: the scaled gradients of their node at this IP
+            if (half == 0 && lane < NN) {
                 const double al = t[0], ga = t[1], be = t[2];
                 double S[ND][ND];
                 S[0][0] = t[3];
@@ -407,7 +425,7 @@ __global__ void __launch_bounds__(WPB * 32) element_kernel(ElemArgs A) {
                     v[4 * ND + i] = h;
                 }
             }
-            __syncwarp();
+            cell_sync();
             if (ti < 0) continue;
             double Ar[RT][ND], Cr[RT][ND], Hr[RT][ND];
 #pragma unroll
@@ -466,11 +484,11 @@ __global__ void __launch_bounds__(WPB * 32) element_kernel(ElemArgs A) {
         // write K_e (row-major NE x NE) through the warp's shared memory, RS node rows at a time:
         // each lane drops its blocks (a, b) and mirrors (b, a) into the staged rows, then the warp
         // copies the rows out with contiguous stores
-        const int RS = min(NN, smem_warp_doubles(NN, ND, ng) / (ND * NE));
+        const int RS = min(NN, smem_cell_doubles(NN, ND, ng) / (ND * NE));
         double* stage = wbase;
         double* kc = A.ke + cell * (int64_t)(NE * NE);
         for (int r0 = 0; r0 < NN; r0 += RS) {
-            __syncwarp();
+            cell_sync();
             if (ti >= 0) {
 #pragma unroll
                 for (int r = 0; r < RT; r++)
@@ -495,10 +513,10 @@ __global__ void __launch_bounds__(WPB * 32) element_kernel(ElemArgs A) {
                         }
                     }
             }
-            __syncwarp();
+            cell_sync();
             const int n = min(RS, NN - r0) * ND * NE;
             double* dst = kc + (int64_t)r0 * ND * NE;
-            for (int t = lane; t < n; t += 32) dst[t] = stage[t];
+            for (int t = lane + 32 * half; t < n; t += 32 * WPC) dst[t] = stage[t];
         }
     }
 }
@@ -742,7 +760,7 @@ void launch_elem_t(pms_elements* h, const ElemArgs& a) {
         cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
         configured = true;
     }
-    int64_t blocks = (a.ncell + WPB - 1) / WPB;
+    int64_t blocks = (a.ncell + cells_per_block(NN) - 1) / cells_per_block(NN);
     kern<<<(unsigned)blocks, WPB * 32, h->smem_bytes, h->stream>>>(a);
 }
 
@@ -1439,7 +1457,7 @@ template <int ND, int NN, bool DOF, bool DOK>
 void noalloc_launch_t(const ElemArgs& a, int smem, cudaStream_t st) {
     auto kern = element_kernel<ND, NN, UPD_NONE, DOF, DOK>;
     cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
-    kern<<<(unsigned)((a.ncell + WPB - 1) / WPB), WPB * 32, smem, st>>>(a);
+    kern<<<(unsigned)((a.ncell + cells_per_block(NN) - 1) / cells_per_block(NN)), WPB * 32, smem, st>>>(a);
 }
 
 template <int ND, int NN>

@@ -17,15 +17,16 @@
 // PCG converged in this tick finish their Newton iteration (multipliers, rel(mdu), U update).  A
 // problem never waits for the PCG of another problem to finish.
 //
-// Two PCG engines, one arithmetic.  Small problems run the whole PCG loop in one thread block each
-// (pcg_block_kernel: no grid-wide synchronisation, every problem at its own pace, resumable
-// across ticks); large problems run the batch-wide kernels (spmv+dot, update, beta, direction),
-// captured in a CUDA graph.  Both engines call the same per-node and per-row functions and reduce
+// Two PCG engines, one arithmetic.  A problem whose vectors fit the shared memory of up to 16 CTAs
+// runs its whole PCG loop on a thread-block cluster (pcg_team_kernel: distributed shared memory,
+// hardware cluster barriers, every problem at its own pace, resumable across ticks); larger
+// problems run the batch-wide kernels (spmv+dot, update, beta+direction), captured in a CUDA graph.  Both engines call the same per-node and per-row functions and reduce
 // through the same trees: 128-node chunks that never straddle two problems, each summed by the
 // fixed pairing (t, t+s), s = 64..1, and a problem's chunk partials summed in chunk order.  A
 // problem's iterates are therefore bit-identical whichever engine runs it and whichever problems
 // share the batch, so the engine threshold and launch shapes (chosen by pms_batch_autotune) change
 // speed only.
+#include <cooperative_groups.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -45,7 +46,6 @@ namespace {
 constexpr unsigned FULL = 0xffffffffu;
 constexpr int CHN = 128;        // nodes per reduction chunk (= threads per block of the node kernels)
 constexpr int WIDE_SPMV_THREADS = 512;
-constexpr int CTA_MAX_CHUNKS = 2048;  // chunk partials a block-engine problem may keep in shared memory
 
 struct SolverArgs {
     int nd;
@@ -156,30 +156,46 @@ __device__ __forceinline__ double row_dot(int64_t row, int sub, bool on, const i
     return s;
 }
 
-// R rows at once by the same lanes (row j: the same FMA chain and shuffle tree as row_dot), so
-// that the loads of R rows are in flight together.
-template <int TPR, int R>
-__device__ __forceinline__ void rows_dot(const int64_t (&row)[R], const bool (&on)[R], int sub,
-                                         const int64_t* __restrict__ indptr, const int32_t* __restrict__ indices,
-                                         const double* __restrict__ val, const double* __restrict__ x,
-                                         double (&s)[R]) {
-    int64_t k[R], e[R];
+// Rows with entries [k0[j], k1[j]) by TPR lanes (row j: the same FMA chain and shuffle tree as
+// row_dot), M entries per lane loaded ahead of each round of FMAs, so that the loads of R rows x M
+// entries are in flight together; gather(col) supplies x[col].
+template <int TPR, int R, int M, class Gather>
+__device__ __forceinline__ void rows_dot_pf(const int64_t (&k0)[R], const int64_t (&k1)[R], int sub,
+                                            const double* __restrict__ val, const int32_t* __restrict__ indices,
+                                            const Gather& gather, double (&s)[R]) {
+    int64_t k[R];
+    bool more = false;
 #pragma unroll
     for (int j = 0; j < R; j++) {
         s[j] = 0.0;
-        k[j] = on[j] ? indptr[row[j]] + sub : 0;
-        e[j] = on[j] ? indptr[row[j] + 1] : 0;
+        k[j] = k0[j] + sub;
+        more = more || k[j] < k1[j];
     }
-    bool more = true;
     while (more) {
-        more = false;
+        double v[R][M], x[R][M];
+        int32_t c[R][M];
 #pragma unroll
         for (int j = 0; j < R; j++)
-            if (k[j] < e[j]) {
-                s[j] = fma(val[k[j]], x[indices[k[j]]], s[j]);
-                k[j] += TPR;
-                more = more || k[j] < e[j];
+#pragma unroll
+            for (int m = 0; m < M; m++) {
+                const int64_t kk = k[j] + (int64_t)m * TPR;
+                const bool ok = kk < k1[j];
+                v[j][m] = ok ? val[kk] : 0.0;
+                c[j][m] = ok ? indices[kk] : -1;
             }
+#pragma unroll
+        for (int j = 0; j < R; j++)
+#pragma unroll
+            for (int m = 0; m < M; m++) x[j][m] = (c[j][m] >= 0) ? gather(c[j][m]) : 0.0;
+        more = false;
+#pragma unroll
+        for (int j = 0; j < R; j++) {
+#pragma unroll
+            for (int m = 0; m < M; m++)
+                if (c[j][m] >= 0) s[j] = fma(v[j][m], x[j][m], s[j]);
+            k[j] += (int64_t)M * TPR;
+            more = more || k[j] < k1[j];
+        }
     }
 #pragma unroll
     for (int j = 0; j < R; j++)
@@ -187,72 +203,73 @@ __device__ __forceinline__ void rows_dot(const int64_t (&row)[R], const bool (&o
         for (int o = TPR / 2; o > 0; o >>= 1) s[j] += __shfl_down_sync(FULL, s[j], o, TPR);
 }
 
-// q = K p (prescribed rows: 0) on rows [row0, row1) by BD threads, R rows per lane group per pass
-template <int BD, int TPR, int R>
+// q = K p on rows [row0, row1) by BD threads, R rows per lane group per pass; store(row, v)
+// receives q_row (0 on prescribed rows).
+template <int BD, int TPR, int R, class Gather, class Store>
 __device__ __forceinline__ void spmv_rows(const int32_t* pres_idx, int64_t row0, int64_t row1,
                                           const int64_t* __restrict__ indptr, const int32_t* __restrict__ indices,
-                                          const double* __restrict__ val, const double* p, double* q) {
+                                          const double* __restrict__ val, const Gather& gather, const Store& store) {
     constexpr int GR = BD / TPR;  // lane groups
     const int sub = threadIdx.x % TPR, grp = threadIdx.x / TPR;
     for (int64_t base = row0; base < row1; base += (int64_t)R * GR) {
         int64_t row[R];
         bool on[R];
         double sv[R];
+        int64_t k0[R], k1[R];
 #pragma unroll
         for (int j = 0; j < R; j++) {
             row[j] = base + j * GR + grp;
             on[j] = row[j] < row1;
+            k0[j] = on[j] ? indptr[row[j]] : 0;
+            k1[j] = on[j] ? indptr[row[j] + 1] : 0;
         }
-        rows_dot<TPR, R>(row, on, sub, indptr, indices, val, p, sv);
+        rows_dot_pf<TPR, R, 4>(k0, k1, sub, val, indices, gather, sv);
         if (sub == 0) {
 #pragma unroll
             for (int j = 0; j < R; j++)
-                if (on[j]) q[row[j]] = (pres_idx[row[j]] >= 0) ? 0.0 : sv[j];
+                if (on[j]) store(row[j], (pres_idx[row[j]] >= 0) ? 0.0 : sv[j]);
         }
     }
 }
 
-// a.b over the free DOFs of a node
-__device__ __forceinline__ double node_dot(const SolverArgs& S, int64_t node, const double* a, const double* b) {
+// a.b over the free DOFs of a node; pres, a, b point at the node's first DOF
+template <class P>
+__device__ __forceinline__ double node_dot(const P* pres, int nd, const double* a, const double* b) {
     double s = 0.0;
-    for (int d = 0; d < S.nd; d++) {
-        const int64_t i = node * S.nd + d;
-        if (S.pres_idx[i] < 0) s = fma(a[i], b[i], s);
-    }
+    for (int d = 0; d < nd; d++)
+        if (pres[d] < 0) s = fma(a[d], b[d], s);
     return s;
 }
 
-// x += alpha p, r -= alpha q (free DOFs), z = M r with the node's inverse diagonal block;
-// accumulates the node's r.z and r.r
-__device__ __forceinline__ void node_update(const SolverArgs& S, int64_t node, double alpha, const double* p,
-                                            const double* q, const double* binv, double* x, double* r, double* z,
+// x += alpha p, r -= alpha q (free DOFs), z = M r with the node's inverse diagonal block B;
+// accumulates the node's r.z and r.r (all pointers at the node's first DOF / block)
+template <class P>
+__device__ __forceinline__ void node_update(const P* pres, int nd, double alpha, const double* p,
+                                            const double* q, const double* B, double* x, double* r, double* z,
                                             double& rz, double& r2) {
-    const int nd = S.nd;
     double rv[3];
     for (int d = 0; d < nd; d++) {
-        const int64_t i = node * nd + d;
-        if (S.pres_idx[i] < 0) {
-            x[i] = fma(alpha, p[i], x[i]);
-            rv[d] = fma(-alpha, q[i], r[i]);
-            r[i] = rv[d];
+        if (pres[d] < 0) {
+            x[d] = fma(alpha, p[d], x[d]);
+            rv[d] = fma(-alpha, q[d], r[d]);
+            r[d] = rv[d];
         } else {
             rv[d] = 0.0;
         }
     }
-    const double* B = binv + node * nd * nd;
     for (int d = 0; d < nd; d++) {
         double zv = 0.0;
         for (int e = 0; e < nd; e++) zv = fma(B[d * nd + e], rv[e], zv);
-        z[node * nd + d] = zv;
+        z[d] = zv;
         rz = fma(rv[d], zv, rz);
         r2 = fma(rv[d], rv[d], r2);
     }
 }
 
 // p = z + beta p on a DOF (0 on prescribed DOFs)
-__device__ __forceinline__ void dof_direction(const SolverArgs& S, int64_t i, double beta, const double* z,
-                                              double* p) {
-    p[i] = (S.pres_idx[i] >= 0) ? 0.0 : fma(beta, p[i], z[i]);
+template <class P>
+__device__ __forceinline__ void dof_direction(P pres, double beta, const double* z, double* p) {
+    *p = (pres >= 0) ? 0.0 : fma(beta, *p, *z);
 }
 
 // scalar step of one PCG iteration: beta, rho, iteration count and the stopping test
@@ -432,9 +449,12 @@ pcg_spmv_dot_kernel(SolverArgs S, int par, const int64_t* __restrict__ indptr, c
     if (!S.pcg_active[par * S.np + pr]) return;  // whole block
     const int64_t node0 = S.chunk_node0[ch];
     const int nn = S.chunk_nnode[ch];
-    spmv_rows<WIDE_SPMV_THREADS, TPR, 4>(S.pres_idx, node0 * S.nd, (node0 + nn) * S.nd, indptr, indices, val, p, q);
+    spmv_rows<WIDE_SPMV_THREADS, TPR, 4>(
+        S.pres_idx, node0 * S.nd, (node0 + nn) * S.nd, indptr, indices, val, [&](int32_t c) { return p[c]; },
+        [&](int64_t row, double v) { q[row] = v; });
     __syncthreads();
-    const double v = (threadIdx.x < nn) ? node_dot(S, node0 + threadIdx.x, p, q) : 0.0;
+    const int64_t i0 = (node0 + threadIdx.x) * S.nd;
+    const double v = (threadIdx.x < nn) ? node_dot(S.pres_idx + i0, S.nd, p + i0, q + i0) : 0.0;
     const double t = group_reduce<false>(v, sh);  // group 0 holds the chunk's nodes
     if (threadIdx.x == 0) part[ch] = t;
 }
@@ -453,8 +473,11 @@ pcg_update_kernel(SolverArgs S, int par, const double* part_pq, const double* rh
     const double pq = problem_total(part_pq, S.pchunk[pr], S.pchunk[pr + 1], sh);
     const double alpha = (pq != 0.0) ? rho[par * S.np + pr] / pq : 0.0;
     double rz = 0.0, r2 = 0.0;
-    if (threadIdx.x < S.chunk_nnode[ch])
-        node_update(S, S.chunk_node0[ch] + threadIdx.x, alpha, p, q, binv, x, r, z, rz, r2);
+    if (threadIdx.x < S.chunk_nnode[ch]) {
+        const int nd = S.nd;
+        const int64_t node = S.chunk_node0[ch] + threadIdx.x, i0 = node * nd;
+        node_update(S.pres_idx + i0, nd, alpha, p + i0, q + i0, binv + node * nd * nd, x + i0, r + i0, z + i0, rz, r2);
+    }
     group_reduce2(rz, r2, sh);
     if (threadIdx.x == 0) {
         part_rz[ch] = rz;
@@ -498,83 +521,191 @@ pcg_beta_direction_kernel(SolverArgs S, int par, const double* part_rz, const do
     }
     if (threadIdx.x < S.chunk_nnode[ch]) {
         const int64_t node = S.chunk_node0[ch] + threadIdx.x;
-        for (int d = 0; d < S.nd; d++) dof_direction(S, node * S.nd + d, beta, z, p);
+        for (int d = 0; d < S.nd; d++) {
+            const int64_t i = node * S.nd + d;
+            dof_direction(S.pres_idx[i], beta, z + i, p + i);
+        }
     }
 }
 
-// ---- block PCG engine: one thread block runs one problem's PCG ------------------------------
-// Up to `budget` iterations (or to convergence) of the problem list[blockIdx.x]; its state (x, r,
-// z, p, q, rho, iteration count, active flag) lives in global memory, so the next launch resumes
-// where this one stopped.  Same arithmetic as the batch-wide kernels: rows by row_dot<TPR>, chunk
-// partials by the 128-thread trees (group g of the block takes chunks g, g+G, ...), problem totals
-// in chunk order.
+// ---- team PCG engine: a thread-block cluster runs one problem's PCG --------------------------
+// Problem list[blockIdx.x / C] runs on the C CTAs of one cluster (C = 1..16).  CTA k owns a
+// contiguous run of the problem's 128-node chunks and keeps x, r, z, p, q and the preconditioner of
+// its nodes in shared memory; the SpMV reads the p of nodes owned by other CTAs of the cluster
+// through distributed shared memory.  Chunk partials are stored into every CTA's copy of the
+// partial arrays, so that each CTA forms the same problem totals.  Hardware cluster barriers order
+// the phases (no spin waits).  Up to `budget` iterations (or to convergence) per launch; the state
+// goes back to global memory at the end, so the next launch resumes.  Same arithmetic as the
+// batch-wide kernels: bit-identical iterates.
+constexpr int TEAM_MAX = 16;
+constexpr int TEAM_MAX_CHUNKS = 256;  // chunks of a team problem
+constexpr size_t TEAM_SMEM_LIMIT = 200 * 1024;
+
+// Shared memory of a team CTA: doubles p, q, r, z, x (npc*nd each), the inverse diagonal blocks
+// (npc*nd*nd), three chunk-partial arrays and the reduction scratch (2*bd); then int32 row
+// pointers of its rows (npc*nd + 1) and the CTAs' node offsets (TEAM_MAX + 1); then one byte per
+// DOF (-1 free, 0 prescribed).
+__host__ __device__ inline size_t team_fixed_bytes(int bd) {
+    return (size_t)8 * (3 * TEAM_MAX_CHUNKS + 2 * bd) + 4 * (TEAM_MAX + 2) + 16;
+}
+__host__ __device__ inline size_t team_node_bytes(int nd) { return (size_t)8 * (5 * nd + nd * nd) + 5 * nd; }
+// nodes per CTA a team kernel can hold (a multiple of the chunk size)
+__host__ __device__ inline int team_node_capacity(int nd, int bd) {
+    const int nodes = (int)((TEAM_SMEM_LIMIT - team_fixed_bytes(bd)) / team_node_bytes(nd));
+    return (nodes / CHN) * CHN;
+}
+__host__ __device__ inline size_t team_smem_bytes(int nd, int bd) {
+    return team_fixed_bytes(bd) + (size_t)team_node_capacity(nd, bd) * team_node_bytes(nd);
+}
+
 template <int BD, int TPR>
-__global__ void __launch_bounds__(BD)
-pcg_block_kernel(SolverArgs S, const int32_t* list, const int64_t* __restrict__ indptr,
-                 const int32_t* __restrict__ indices, const double* __restrict__ val, const double* binv, double* x,
-                 double* r, double* z, double* p, double* q, double* rho_g, const double* r0_g, int32_t* iters_g,
-                 uint8_t* cta_active, double rtol, int32_t max_iter, int32_t budget) {
+__global__ void __launch_bounds__(BD, 1)
+pcg_team_kernel(SolverArgs S, const int32_t* list, const int64_t* __restrict__ indptr,
+                const int32_t* __restrict__ indices, const double* __restrict__ val, const double* binv_g,
+                double* x_g, double* r_g, double* z_g, double* p_g, double* rho_g, const double* r0_g,
+                int32_t* iters_g, uint8_t* cta_active, double rtol, int32_t max_iter, int32_t budget) {
+    namespace cg = cooperative_groups;
     constexpr int G = BD / CHN;
+    constexpr int RT = BD >= 1024 ? 2 : 4;  // rows per lane group per SpMV pass
+    constexpr int nd = TPR == 8 ? 2 : 3;    // DOFs per node (the lanes per row follow the dimension)
+    cg::cluster_group cl = cg::this_cluster();
+    const int C = (int)cl.num_blocks();
+    const int me = (int)cl.block_rank();
+    const int pr = list[blockIdx.x / C];
+    if (!cta_active[pr]) return;  // the whole cluster reads the same flag
+    // a one-CTA team needs no cluster barrier (its partials are its own shared memory)
+    auto team_sync = [&]() {
+        if (C == 1) __syncthreads();
+        else cl.sync();
+    };
+    const int npc = team_node_capacity(nd, BD);
     extern __shared__ double smem[];
-    double* red = smem;                 // 2*BD
-    double* pq_part = red + 2 * BD;     // CTA_MAX_CHUNKS each
-    double* rz_part = pq_part + CTA_MAX_CHUNKS;
-    double* rr_part = rz_part + CTA_MAX_CHUNKS;
-    const int pr = list[blockIdx.x];
-    if (!cta_active[pr]) return;  // whole block
-    const int64_t c0 = S.pchunk[pr], c1 = S.pchunk[pr + 1];
-    const int nch = (int)(c1 - c0);
-    const int nd = S.nd;
-    const int64_t row0 = S.chunk_node0[c0] * nd;
-    const int64_t row1 = (S.chunk_node0[c1 - 1] + S.chunk_nnode[c1 - 1]) * nd;
-    const int g = threadIdx.x / CHN, tg = threadIdx.x % CHN;
+    double* ps = smem;
+    double* qs = ps + npc * nd;
+    double* rs = qs + npc * nd;
+    double* zs = rs + npc * nd;
+    double* xs = zs + npc * nd;
+    double* bs = xs + npc * nd;                  // npc * nd * nd
+    double* part_pq = bs + npc * nd * nd;        // TEAM_MAX_CHUNKS each
+    double* part_rz = part_pq + TEAM_MAX_CHUNKS;
+    double* part_rr = part_rz + TEAM_MAX_CHUNKS;
+    double* red = part_rr + TEAM_MAX_CHUNKS;     // 2 * BD
+    int32_t* rp = (int32_t*)(red + 2 * BD);      // npc * nd + 1 row pointers (relative)
+    int32_t* kb = rp + npc * nd + 1;             // TEAM_MAX + 1 node offsets of the CTAs' runs
+    int8_t* fr = (int8_t*)(kb + TEAM_MAX + 1);   // npc * nd: -1 free DOF, 0 prescribed
+    const int64_t c0 = S.pchunk[pr];
+    const int nch = (int)(S.pchunk[pr + 1] - c0);
+    const int64_t n0 = S.chunk_node0[c0];
+    const int N = (int)(S.chunk_node0[c0 + nch - 1] + S.chunk_nnode[c0 + nch - 1] - n0);  // nodes
+    if (threadIdx.x <= C) {
+        const int k = (int)threadIdx.x;
+        kb[k] = min(N, CHN * (int)((int64_t)k * nch / C));
+    }
+    __syncthreads();
+    const int cb = (int)((int64_t)me * nch / C), ce = (int)((int64_t)(me + 1) * nch / C);  // my chunks
+    const int nb = kb[me], ne = kb[me + 1];                                               // my nodes
+    const int64_t gd0 = (n0 + nb) * nd;  // my first DOF (= first row)
+    const int ndl = (ne - nb) * nd;
+    const int64_t kbase = indptr[gd0];
+    for (int i = threadIdx.x; i < ndl; i += BD) {
+        ps[i] = p_g[gd0 + i];
+        rs[i] = r_g[gd0 + i];
+        zs[i] = z_g[gd0 + i];
+        xs[i] = x_g[gd0 + i];
+        fr[i] = S.pres_idx[gd0 + i] < 0 ? -1 : 0;
+        rp[i] = (int32_t)(indptr[gd0 + i] - kbase);
+    }
+    if (threadIdx.x == 0) rp[ndl] = (int32_t)(indptr[gd0 + ndl] - kbase);
+    for (int i = threadIdx.x; i < ndl * nd; i += BD) bs[i] = binv_g[gd0 * nd + i];
     double rho = rho_g[pr];
     const double r0 = r0_g[pr];
     int32_t it = iters_g[pr];
     bool active = true;
-    for (int k = 0; k < budget && active; k++) {
-        // q = K p on the problem's rows
-        spmv_rows<BD, TPR, 4>(S.pres_idx, row0, row1, indptr, indices, val, p, q);
-        __syncthreads();
-        // chunk partials of p.q
-        for (int cb = 0; cb < nch; cb += G) {
-            const int c = cb + g;
-            double v = 0.0;
-            if (c < nch && tg < S.chunk_nnode[c0 + c]) v = node_dot(S, S.chunk_node0[c0 + c] + tg, p, q);
-            v = group_reduce<false>(v, red);
-            if (tg == 0 && c < nch) pq_part[c] = v;
-        }
-        __syncthreads();
-        const double pq = problem_total(pq_part, 0, nch, red);  // every group computes the same total
-        const double alpha = (pq != 0.0) ? rho / pq : 0.0;
-        // x, r, z and the chunk partials of r.z, r.r
-        for (int cb = 0; cb < nch; cb += G) {
-            const int c = cb + g;
-            double rz = 0.0, r2 = 0.0;
-            if (c < nch && tg < S.chunk_nnode[c0 + c])
-                node_update(S, S.chunk_node0[c0 + c] + tg, alpha, p, q, binv, x, r, z, rz, r2);
-            group_reduce2(rz, r2, red);
-            if (tg == 0 && c < nch) {
-                rz_part[c] = rz;
-                rr_part[c] = r2;
+    const int g = threadIdx.x / CHN, tg = threadIdx.x % CHN;
+    const int sub = threadIdx.x % TPR, grp = threadIdx.x / TPR;
+    // x[col] of the problem: from my shared memory or from the owning CTA's
+    auto gather = [&](int32_t col) -> double {
+        const int64_t l = col - gd0;
+        if (l >= 0 && l < ndl) return ps[l];
+        const int node = col / nd - (int)n0;
+        // owner of chunk c: the largest k with floor(k*nch/C) <= c
+        const int k = (int)(((int64_t)(node / CHN + 1) * C - 1) / nch);
+        const double* rpk = cl.map_shared_rank(ps, k);
+        return rpk[(node - kb[k]) * nd + col % nd];
+    };
+    team_sync();  // every CTA holds its p before the first remote read
+    for (int step = 0; step < budget && active; step++) {
+        // q = K p on my rows
+        for (int base = 0; base < ndl; base += RT * (BD / TPR)) {
+            int row[RT];
+            bool on[RT];
+            int64_t k0[RT], k1[RT];
+            double sv[RT];
+#pragma unroll
+            for (int j = 0; j < RT; j++) {
+                row[j] = base + j * (BD / TPR) + grp;
+                on[j] = row[j] < ndl;
+                k0[j] = on[j] ? kbase + rp[row[j]] : 0;
+                k1[j] = on[j] ? kbase + rp[row[j] + 1] : 0;
+            }
+            rows_dot_pf<TPR, RT, 4>(k0, k1, sub, val, indices, gather, sv);
+            if (sub == 0) {
+#pragma unroll
+                for (int j = 0; j < RT; j++)
+                    if (on[j]) qs[row[j]] = (fr[row[j]] >= 0) ? 0.0 : sv[j];
             }
         }
         __syncthreads();
+        // p.q partials of my chunks, stored into every CTA's array
+        for (int j0 = cb; j0 < ce; j0 += G) {
+            const int j = j0 + g;
+            double v = 0.0;
+            if (j < ce && tg < min(CHN, N - CHN * j)) {
+                const int l = (CHN * j - nb + tg) * nd;
+                v = node_dot(fr + l, nd, ps + l, qs + l);
+            }
+            v = group_reduce<false>(v, red);
+            if (tg == 0 && j < ce)
+                for (int k = 0; k < C; k++) cl.map_shared_rank(part_pq, k)[j] = v;
+        }
+        team_sync();
+        const double pq = problem_total(part_pq, 0, nch, red);
+        const double alpha = (pq != 0.0) ? rho / pq : 0.0;
+        for (int j0 = cb; j0 < ce; j0 += G) {
+            const int j = j0 + g;
+            double rz = 0.0, r2 = 0.0;
+            if (j < ce && tg < min(CHN, N - CHN * j)) {
+                const int ln = CHN * j - nb + tg, l = ln * nd;
+                node_update(fr + l, nd, alpha, ps + l, qs + l, bs + ln * nd * nd, xs + l, rs + l, zs + l, rz, r2);
+            }
+            group_reduce2(rz, r2, red);
+            if (tg == 0 && j < ce)
+                for (int k = 0; k < C; k++) {
+                    cl.map_shared_rank(part_rz, k)[j] = rz;
+                    cl.map_shared_rank(part_rr, k)[j] = r2;
+                }
+        }
+        team_sync();
         double rzt, rrt, beta;
-        problem_total2(rz_part, rr_part, 0, nch, rzt, rrt, red);
+        problem_total2(part_rz, part_rr, 0, nch, rzt, rrt, red);
         const bool done = pcg_scalar_step(rzt, rrt, rho, r0, it, rtol, max_iter, beta);
-        for (int64_t i = row0 + threadIdx.x; i < row1; i += BD) dof_direction(S, i, beta, z, p);
+        for (int i = threadIdx.x; i < ndl; i += BD) dof_direction(fr[i], beta, zs + i, ps + i);
         active = !done;
-        __syncthreads();
+        team_sync();  // p complete (and every remote read of this iteration done) before the next SpMV
     }
-    if (threadIdx.x == 0) {
+    for (int i = threadIdx.x; i < ndl; i += BD) {
+        p_g[gd0 + i] = ps[i];
+        r_g[gd0 + i] = rs[i];
+        z_g[gd0 + i] = zs[i];
+        x_g[gd0 + i] = xs[i];
+    }
+    if (me == 0 && threadIdx.x == 0) {
         rho_g[pr] = rho;
         iters_g[pr] = it;
         cta_active[pr] = active ? 1 : 0;
     }
+    team_sync();  // no CTA leaves while another may still address its shared memory
 }
-
-size_t block_engine_smem(int bd) { return (size_t)(2 * bd + 3 * CTA_MAX_CHUNKS) * sizeof(double); }
 
 // mdu = x on free rows (mdu already holds u_p - c on prescribed rows); mdl = (R_p + l) - (K mdu)_p
 __global__ void assemble_mdu_kernel(SolverArgs S, const double* x, double* mdu) {
@@ -697,8 +828,10 @@ struct pms_batch {
     const int64_t* d_indptr = nullptr;
     const int32_t* d_indices = nullptr;
     SolverArgs S{};
-    cudaStream_t st2 = nullptr;  // block-engine PCG, overlapped with the batch-wide engine
-    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+    cudaStream_t st_cls[5] = {};  // team launches (one stream per team size), beside the batch-wide engine
+    cudaEvent_t ev_fork = nullptr, ev_cls[5] = {};
+    int cls_off[6] = {};
+    int team_cmax = 8;
     cudaGraphExec_t graph = nullptr;
     int graph_iters_captured = 0;
     std::string last_error;
@@ -708,6 +841,7 @@ struct pms_batch {
     std::vector<uint8_t> solving;  // per problem: linear solve under way
     std::vector<uint8_t> engine;   // per problem: 1 = block engine, 0 = batch-wide engine
     std::vector<int64_t> pndof;    // DOFs of each problem
+    std::vector<int64_t> pnch;     // reduction chunks of each problem
     std::vector<int32_t> h_list;
 
     template <typename T>
@@ -726,12 +860,15 @@ struct pms_batch {
     }
     ~pms_batch() {
         cudaStreamSynchronize(v.stream);
-        if (st2) cudaStreamSynchronize(st2);
+        for (auto c : st_cls)
+            if (c) cudaStreamSynchronize(c);
         std::lock_guard<std::mutex> lock(device_mutex());
         if (graph) cudaGraphExecDestroy(graph);
         if (ev_fork) cudaEventDestroy(ev_fork);
-        if (ev_join) cudaEventDestroy(ev_join);
-        if (st2) cudaStreamDestroy(st2);
+        for (auto e : ev_cls)
+            if (e) cudaEventDestroy(e);
+        for (auto c : st_cls)
+            if (c) cudaStreamDestroy(c);
         for (void* p : allocs) cudaFree(p);
     }
 };
@@ -800,50 +937,91 @@ int ensure_graph(pms_batch* b) {
     return PMS_OK;
 }
 
-template <int BD>
-void launch_block_engine_bd(pms_batch* b, int nlist, int budget, cudaStream_t st) {
-    const size_t sm = block_engine_smem(BD);
-    if (tpr_of(b->v.nd) == 8)
-        pcg_block_kernel<BD, 8><<<nlist, BD, sm, st>>>(b->S, b->d_list, b->d_indptr, b->d_indices, b->d_csr,
-                                                        b->d_binv, b->d_x, b->d_r, b->d_z, b->d_p, b->d_q, b->d_rho,
-                                                        b->d_r0, b->d_iters, b->d_cta_active, b->cfg.pcg_rtol,
-                                                        b->cfg.pcg_max_iterations, budget);
-    else
-        pcg_block_kernel<BD, 16><<<nlist, BD, sm, st>>>(b->S, b->d_list, b->d_indptr, b->d_indices, b->d_csr,
-                                                         b->d_binv, b->d_x, b->d_r, b->d_z, b->d_p, b->d_q, b->d_rho,
-                                                         b->d_r0, b->d_iters, b->d_cta_active, b->cfg.pcg_rtol,
-                                                         b->cfg.pcg_max_iterations, budget);
+constexpr int NCLASS = 5;  // team sizes 1, 2, 4, 8, 16
+
+template <int BD, int TPR>
+cudaError_t launch_team_t(pms_batch* b, const int32_t* list, int n, int C, int budget, cudaStream_t st) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)(n * C));
+    cfg.blockDim = dim3(BD);
+    cfg.dynamicSmemBytes = team_smem_bytes(b->v.nd, BD);
+    cfg.stream = st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = (unsigned)C;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, pcg_team_kernel<BD, TPR>, b->S, list, b->d_indptr, b->d_indices,
+                              (const double*)b->d_csr, (const double*)b->d_binv, b->d_x, b->d_r, b->d_z, b->d_p,
+                              b->d_rho, (const double*)b->d_r0, b->d_iters, b->d_cta_active, b->cfg.pcg_rtol,
+                              b->cfg.pcg_max_iterations, budget);
 }
 
-int launch_block_engine(pms_batch* b, int nlist, int budget, cudaStream_t st) {
-    switch (b->tune.block_threads) {
-        case 128: launch_block_engine_bd<128>(b, nlist, budget, st); break;
-        case 256: launch_block_engine_bd<256>(b, nlist, budget, st); break;
-        case 1024: launch_block_engine_bd<1024>(b, nlist, budget, st); break;
-        default: launch_block_engine_bd<512>(b, nlist, budget, st); break;
+int launch_team(pms_batch* b, const int32_t* list, int n, int C, int budget, cudaStream_t st) {
+    const bool two = tpr_of(b->v.nd) == 8;
+    cudaError_t e;
+    switch (b->tune.team_threads) {
+        case 256: e = two ? launch_team_t<256, 8>(b, list, n, C, budget, st) : launch_team_t<256, 16>(b, list, n, C, budget, st); break;
+        case 1024: e = two ? launch_team_t<1024, 8>(b, list, n, C, budget, st) : launch_team_t<1024, 16>(b, list, n, C, budget, st); break;
+        default: e = two ? launch_team_t<512, 8>(b, list, n, C, budget, st) : launch_team_t<512, 16>(b, list, n, C, budget, st); break;
     }
     b->launches++;
+    return e == cudaSuccess ? PMS_OK : bfail(b, PMS_ERR_CUDA, cudaGetErrorString(e));
+}
+
+template <int BD, int TPR>
+bool team_attrs_t() {
+    const int sm = (int)team_smem_bytes(TPR == 8 ? 2 : 3, BD);
+    return cudaFuncSetAttribute(pcg_team_kernel<BD, TPR>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm) ==
+               cudaSuccess &&
+           cudaFuncSetAttribute(pcg_team_kernel<BD, TPR>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) ==
+               cudaSuccess;
+}
+
+// Kernel attributes of every team variant, and the largest cluster this device schedules
+// (16 where the non-portable size is available, else 8).  Once per process.
+int team_setup(int* cmax) {
+    static int cached = -1;
+    static std::mutex m;
+    std::lock_guard<std::mutex> lock(m);
+    if (cached < 0) {
+        const bool ok = team_attrs_t<256, 8>() && team_attrs_t<256, 16>() && team_attrs_t<512, 8>() &&
+                        team_attrs_t<512, 16>() && team_attrs_t<1024, 8>() && team_attrs_t<1024, 16>();
+        if (!ok) return PMS_ERR_CUDA;
+        int c = 16;
+        for (int nd = 2; nd <= 3; nd++) {
+            cudaLaunchConfig_t cfg = {};
+            cfg.gridDim = dim3(16);
+            cfg.blockDim = dim3(1024);
+            cfg.dynamicSmemBytes = team_smem_bytes(nd, 1024);
+            cudaLaunchAttribute at[1];
+            at[0].id = cudaLaunchAttributeClusterDimension;
+            at[0].val.clusterDim.x = 16;
+            at[0].val.clusterDim.y = 1;
+            at[0].val.clusterDim.z = 1;
+            cfg.attrs = at;
+            cfg.numAttrs = 1;
+            int n16 = 0;
+            const cudaError_t e = (nd == 2) ? cudaOccupancyMaxActiveClusters(&n16, pcg_team_kernel<1024, 8>, &cfg)
+                                            : cudaOccupancyMaxActiveClusters(&n16, pcg_team_kernel<1024, 16>, &cfg);
+            if (e != cudaSuccess) cudaGetLastError();
+            if (e != cudaSuccess || n16 < 1) c = 8;
+        }
+        cached = c;
+    }
+    *cmax = cached;
     return PMS_OK;
 }
 
-template <int BD>
-bool set_block_smem_bd() {
-    const int sm = (int)block_engine_smem(BD);
-    bool ok = cudaFuncSetAttribute(pcg_block_kernel<BD, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm) ==
-              cudaSuccess;
-    ok = ok && cudaFuncSetAttribute(pcg_block_kernel<BD, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm) ==
-                   cudaSuccess;
-    return ok;
-}
+// Team size of a problem: the smallest power of two whose CTAs hold at most the target number of
+// chunks each; 0 (batch-wide engine) when it needs more than the largest cluster.
+int team_size_of(const pms_batch* b, int p);
 
-bool set_block_smem() {
-    return set_block_smem_bd<128>() && set_block_smem_bd<256>() && set_block_smem_bd<512>() &&
-           set_block_smem_bd<1024>();
-}
-
-// Which engine runs each problem's PCG (host and device copies).
+// Which engine runs each problem's PCG (host and device copies): 0 = batch-wide, C = a team of C.
 int assign_engines(pms_batch* b) {
-    for (int p = 0; p < b->np; p++) b->engine[p] = (b->pndof[p] <= b->tune.block_max_ndof) ? 1 : 0;
+    for (int p = 0; p < b->np; p++) b->engine[p] = (b->pndof[p] <= b->tune.team_max_ndof) ? team_size_of(b, p) : 0;
     return cudaMemcpyAsync(b->d_engine, b->engine.data(), b->np, cudaMemcpyHostToDevice, b->v.stream) ==
                    cudaSuccess
                ? PMS_OK
@@ -865,19 +1043,35 @@ void pcg_start(pms_batch* b) {
     b->launches += 4;
 }
 
-// PCG iterations of every solving problem: the block engine (one launch, on the second stream) and
-// the batch-wide engine (graph launches on the handle's stream) run side by side.  The batch-wide
-// loop keeps going while the block engine is busy; once it is idle, the loop stops when an eighth
-// of its problems (at least one) have finished or after `budget` iterations.  `exact` runs exactly
-// `budget` iterations on both engines (timing).
-int pcg_phase(pms_batch* b, int nblock, int nwide, int budget, bool exact) {
+// PCG iterations of every solving problem: one team launch per team size (each on its own stream)
+// and the batch-wide engine (graph launches on the handle's stream) run side by side.  The team
+// lists are in b->h_list, grouped by team size (b->cls_off).  The batch-wide loop keeps going while
+// a team launch is busy; once they are idle, it stops when an eighth of its problems (at least
+// one) have finished or after `budget` iterations.  `exact` runs exactly `budget` iterations on
+// every engine (timing).
+int pcg_phase(pms_batch* b, int nteam, int nwide, int budget, bool exact) {
     cudaStream_t st = b->v.stream;
-    if (nblock > 0) {
-        if (cudaEventRecord(b->ev_fork, st) != cudaSuccess || cudaStreamWaitEvent(b->st2, b->ev_fork, 0) != cudaSuccess)
-            return bfail(b, PMS_ERR_CUDA, "stream fork failed");
-        launch_block_engine(b, nblock, budget, b->st2);
-        if (cudaEventRecord(b->ev_join, b->st2) != cudaSuccess) return bfail(b, PMS_ERR_CUDA, "stream join failed");
+    bool launched[NCLASS] = {};
+    if (nteam > 0) {
+        cudaMemcpyAsync(b->d_list, b->h_list.data(), nteam * 4, cudaMemcpyHostToDevice, st);
+        if (cudaEventRecord(b->ev_fork, st) != cudaSuccess) return bfail(b, PMS_ERR_CUDA, "stream fork failed");
+        for (int c = 0; c < NCLASS; c++) {
+            const int n = b->cls_off[c + 1] - b->cls_off[c];
+            if (n == 0) continue;
+            if (cudaStreamWaitEvent(b->st_cls[c], b->ev_fork, 0) != cudaSuccess)
+                return bfail(b, PMS_ERR_CUDA, "stream fork failed");
+            int rc = launch_team(b, b->d_list + b->cls_off[c], n, 1 << c, budget, b->st_cls[c]);
+            if (rc) return rc;
+            if (cudaEventRecord(b->ev_cls[c], b->st_cls[c]) != cudaSuccess)
+                return bfail(b, PMS_ERR_CUDA, "stream join failed");
+            launched[c] = true;
+        }
     }
+    auto teams_busy = [&]() {
+        for (int c = 0; c < NCLASS; c++)
+            if (launched[c] && cudaEventQuery(b->ev_cls[c]) == cudaErrorNotReady) return true;
+        return false;
+    };
     if (nwide > 0) {
         int rc = ensure_graph(b);
         if (rc) return rc;
@@ -891,13 +1085,39 @@ int pcg_phase(pms_batch* b, int nblock, int nwide, int budget, bool exact) {
             cudaMemcpyAsync(&nact, b->d_nactive, sizeof(int32_t), cudaMemcpyDeviceToHost, st);
             if (cudaStreamSynchronize(st) != cudaSuccess)
                 return bfail(b, PMS_ERR_CUDA, cudaGetErrorString(cudaGetLastError()));
-            const bool block_busy = nblock > 0 && cudaEventQuery(b->ev_join) == cudaErrorNotReady;
-            if (!block_busy && (nact <= stop_at || done >= budget)) break;
+            if (!teams_busy() && (nact <= stop_at || done >= budget)) break;
         }
     }
-    if (nblock > 0 && cudaStreamWaitEvent(st, b->ev_join, 0) != cudaSuccess)
-        return bfail(b, PMS_ERR_CUDA, "stream join failed");
+    for (int c = 0; c < NCLASS; c++)
+        if (launched[c] && cudaStreamWaitEvent(st, b->ev_cls[c], 0) != cudaSuccess)
+            return bfail(b, PMS_ERR_CUDA, "stream join failed");
     return PMS_OK;
+}
+
+// Team lists of the problems selected by `want` (grouped by team size) and the count of
+// batch-wide ones.
+void build_lists(pms_batch* b, const std::vector<uint8_t>& want, int& nteam, int& nwide) {
+    b->h_list.clear();
+    nwide = 0;
+    for (int c = 0; c < NCLASS; c++) {
+        b->cls_off[c] = (int)b->h_list.size();
+        for (int p = 0; p < b->np; p++)
+            if (want[p] && b->engine[p] == (1 << c)) b->h_list.push_back(p);
+    }
+    b->cls_off[NCLASS] = (int)b->h_list.size();
+    for (int p = 0; p < b->np; p++)
+        if (want[p] && b->engine[p] == 0) nwide++;
+    nteam = (int)b->h_list.size();
+}
+
+int team_size_of(const pms_batch* b, int p) {
+    const int64_t nch = b->pnch[p];
+    const int cap = team_node_capacity(b->v.nd, b->tune.team_threads) / CHN;
+    const int per = b->tune.team_chunks > 0 ? std::min(cap, b->tune.team_chunks) : cap;
+    if (nch > TEAM_MAX_CHUNKS) return 0;
+    for (int c = 1; c <= b->team_cmax; c *= 2)
+        if ((nch + c - 1) / c <= per) return c;
+    return 0;
 }
 
 }  // namespace
@@ -922,8 +1142,9 @@ int pms_batch_create(pms_elements* el, int32_t nproblem, const int64_t* point_pt
     if (b->cfg.pcg_max_iterations <= 0) b->cfg.pcg_max_iterations = 20000;
     if (!(b->cfg.pcg_rtol > 0)) b->cfg.pcg_rtol = 1e-12;
     if (b->cfg.n_max_iterations <= 0) b->cfg.n_max_iterations = 10;
-    b->tune.block_max_ndof = 2048;
-    b->tune.block_threads = 512;
+    b->tune.team_max_ndof = INT64_MAX;
+    b->tune.team_threads = 1024;
+    b->tune.team_chunks = 1;
     b->tune.pcg_budget = 128;
     b->tune.graph_iters = 8;
     const int nd = b->v.nd;
@@ -1011,9 +1232,12 @@ int pms_batch_create(pms_elements* el, int32_t nproblem, const int64_t* point_pt
         delete b;
         return rc;
     }
-    if (cudaStreamCreateWithFlags(&b->st2, cudaStreamNonBlocking) != cudaSuccess ||
-        cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
-        cudaEventCreateWithFlags(&b->ev_join, cudaEventDisableTiming) != cudaSuccess || !set_block_smem()) {
+    bool sok = cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming) == cudaSuccess &&
+               team_setup(&b->team_cmax) == PMS_OK;
+    for (int c = 0; c < NCLASS && sok; c++)
+        sok = cudaStreamCreateWithFlags(&b->st_cls[c], cudaStreamNonBlocking) == cudaSuccess &&
+              cudaEventCreateWithFlags(&b->ev_cls[c], cudaEventDisableTiming) == cudaSuccess;
+    if (!sok) {
         delete b;
         return PMS_ERR_CUDA;
     }
@@ -1039,9 +1263,8 @@ int pms_batch_create(pms_elements* el, int32_t nproblem, const int64_t* point_pt
     b->solving.assign(nproblem, 0);
     b->engine.assign(nproblem, 0);
     b->it.assign(nproblem, 0);
-    // a problem on the block engine keeps its chunk partials in shared memory
-    for (int p = 0; p < nproblem; p++)
-        if (pchunk[p + 1] - pchunk[p] > CTA_MAX_CHUNKS) b->pndof[p] = INT64_MAX;
+    b->pnch.assign(nproblem, 0);
+    for (int p = 0; p < nproblem; p++) b->pnch[p] = pchunk[p + 1] - pchunk[p];
     if (assign_engines(b) || cudaDeviceSynchronize() != cudaSuccess) {
         delete b;
         return PMS_ERR_CUDA;
@@ -1160,20 +1383,10 @@ int pms_batch_tick(pms_batch* b, const uint8_t* cmd, const double* c_values, int
         }
     }
     // ---- stage 3: PCG iterations of every solving problem
-    int nblock = 0, nwide = 0;
-    b->h_list.clear();
-    for (int p = 0; p < np; p++) {
-        if (!b->solving[p]) continue;
-        if (b->engine[p]) {
-            b->h_list.push_back(p);
-            nblock++;
-        } else {
-            nwide++;
-        }
-    }
-    if (nblock > 0) cudaMemcpyAsync(b->d_list, b->h_list.data(), nblock * 4, cudaMemcpyHostToDevice, st);
-    if (nblock + nwide > 0) {
-        rc = pcg_phase(b, nblock, nwide, std::max(1, b->tune.pcg_budget), false);
+    int nteam = 0, nwide = 0;
+    build_lists(b, b->solving, nteam, nwide);
+    if (nteam + nwide > 0) {
+        rc = pcg_phase(b, nteam, nwide, std::max(1, b->tune.pcg_budget), false);
         if (rc) return rc;
         std::vector<uint8_t> wa(np), ca(np);
         cudaMemcpyAsync(wa.data(), b->d_pcg_active, np, cudaMemcpyDeviceToHost, st);
@@ -1278,9 +1491,9 @@ int pms_batch_solve_step(pms_batch* b, const double* c_values, const uint8_t* ac
 
 int pms_batch_set_tuning(pms_batch* b, const pms_batch_tuning* t) {
     if (!b || !t) return PMS_ERR_INVALID;
-    if (t->block_threads != 128 && t->block_threads != 256 && t->block_threads != 512 && t->block_threads != 1024)
-        return PMS_ERR_INVALID;
-    if (t->pcg_budget < 1 || t->graph_iters < 1 || t->graph_iters > 64 || t->block_max_ndof < 0)
+    if (t->team_threads != 256 && t->team_threads != 512 && t->team_threads != 1024) return PMS_ERR_INVALID;
+    if (t->pcg_budget < 1 || t->graph_iters < 1 || t->graph_iters > 64 || t->team_max_ndof < 0 ||
+        t->team_chunks < 0)
         return PMS_ERR_INVALID;
     for (int p = 0; p < b->np; p++)
         if (b->solving[p]) return bfail(b, PMS_ERR_INVALID, "tuning cannot change while a linear solve is under way");
@@ -1327,18 +1540,9 @@ int time_candidate(pms_batch* b, const pms_batch_tuning& cand, int iters, float*
     b->tune = cand;
     int rc = assign_engines(b);
     if (rc) return rc;
-    int nblock = 0, nwide = 0;
-    b->h_list.clear();
-    for (int p = 0; p < np; p++) {
-        if (b->engine[p]) {
-            b->h_list.push_back(p);
-            nblock++;
-        } else {
-            nwide++;
-        }
-    }
-    if (nblock > 0) cudaMemcpyAsync(b->d_list, b->h_list.data(), nblock * 4, cudaMemcpyHostToDevice, st);
     std::vector<uint8_t> all(np, 1);
+    int nteam = 0, nwide = 0;
+    build_lists(b, all, nteam, nwide);
     cudaMemcpyAsync(b->d_active, all.data(), np, cudaMemcpyHostToDevice, st);
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
@@ -1347,7 +1551,7 @@ int time_candidate(pms_batch* b, const pms_batch_tuning& cand, int iters, float*
     for (int rep = 0; rep < 2 && !rc; rep++) {
         pcg_start(b);
         cudaEventRecord(e0, st);
-        rc = pcg_phase(b, nblock, nwide, iters, true);
+        rc = pcg_phase(b, nteam, nwide, iters, true);
         cudaEventRecord(e1, st);
         if (cudaEventSynchronize(e1) != cudaSuccess) rc = bfail(b, PMS_ERR_CUDA, "timing run failed");
         cudaEventElapsedTime(&ms, e0, e1);
@@ -1380,30 +1584,38 @@ int pms_batch_autotune(pms_batch* b, pms_batch_tuning* out) {
     int rc = timing_setup(b);
     if (rc) return rc;
     const int np = b->np;
-    // candidates: engine threshold x block size; the batch-wide engine alone first
+    // candidates: the batch-wide engine alone, then teams for every problem that fits (or only for
+    // the problems up to a size) with several CTA sizes and chunks per CTA
     int64_t maxdof = 0;
-    for (int p = 0; p < np; p++)
-        if (b->pndof[p] != INT64_MAX) maxdof = std::max(maxdof, b->pndof[p]);
-    std::vector<int64_t> thr = {0};
-    for (int64_t t = 1024; t < maxdof; t *= 2) thr.push_back(t);
-    if (maxdof > 0) thr.push_back(maxdof);
-    const int sizes[3] = {256, 512, 1024};
+    for (int p = 0; p < np; p++) maxdof = std::max(maxdof, b->pndof[p]);
     const pms_batch_tuning keep = b->tune;
+    std::vector<pms_batch_tuning> cands;
+    {
+        pms_batch_tuning c = keep;
+        c.team_max_ndof = 0;
+        cands.push_back(c);
+    }
+    for (int64_t t : {(int64_t)2048, (int64_t)8192, INT64_MAX}) {
+        if (t != INT64_MAX && t >= maxdof) continue;
+        for (int threads : {512, 1024})
+            for (int chunks : {0, 1, 4}) {
+                pms_batch_tuning c = keep;
+                c.team_max_ndof = t;
+                c.team_threads = threads;
+                c.team_chunks = chunks;
+                cands.push_back(c);
+            }
+    }
     pms_batch_tuning best = keep;
     float best_ms = 1e30f;
-    for (int64_t t : thr) {
-        for (int si = 0; si < (t == 0 ? 1 : 3) && !rc; si++) {
-            pms_batch_tuning cand = keep;
-            cand.block_max_ndof = t;
-            cand.block_threads = t == 0 ? keep.block_threads : sizes[si];
-            float ms = 0.0f;
-            rc = time_candidate(b, cand, 32, &ms);
-            if (!rc && ms < best_ms) {
-                best_ms = ms;
-                best = cand;
-            }
-        }
+    for (const auto& cand : cands) {
+        float ms = 0.0f;
+        rc = time_candidate(b, cand, 32, &ms);
         if (rc) break;
+        if (ms < best_ms) {
+            best_ms = ms;
+            best = cand;
+        }
     }
     b->tune = rc ? keep : best;
     int rc2 = assign_engines(b);

@@ -54,14 +54,16 @@ class Request:
 class Server:
     """``admit_window``: a waiting request is admitted once it has waited this long (seconds), together
     with everything that arrived since (one batch per element kind), so that bursts share a batch;
-    ``max_concurrent`` batches run at a time, each on its own stream and host thread."""
+    ``max_concurrent`` batches run at a time, each on its own stream and host thread; ``autotune``
+    picks each batch's PCG launch shapes (which change speed, never results)."""
 
     def __init__(self, budget_bytes=120e9, max_batch=256, max_concurrent=16, admit_window=0.025,
-                 keep_results=False, **solver_kw):
+                 keep_results=False, autotune=True, **solver_kw):
         self.budget = float(budget_bytes)
         self.max_batch = max_batch
         self.max_concurrent = max_concurrent
         self.admit_window = float(admit_window)
+        self.autotune = autotune
         self.keep_results = keep_results
         self.solver_kw = solver_kw
         self.in_use = 0.0
@@ -75,6 +77,8 @@ class Server:
     def _run_batch(self, reqs, t0):
         try:
             bs = BatchSolver([r.problem for r in reqs], **self.solver_kw)
+            if self.autotune:
+                bs.autotune()  # launch shapes only: the results do not depend on them
             clock = lambda: time.perf_counter() - t0  # noqa: E731
             bs.solve_independent(on_fail="drop", clock=clock)
             u = bs.u() if self.keep_results else None

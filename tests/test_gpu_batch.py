@@ -119,34 +119,49 @@ def test_independent_progress_matches_lock_step():
     assert a.history == b.history
 
 
-def test_pcg_engines_give_the_same_bits():
-    """The block engine (one thread block per problem) and the batch-wide engine run the same
-    arithmetic: forcing either one, or letting the autotuner choose, gives identical U, IP state
-    and Newton/PCG iteration histories."""
+def _solve_with(probs, setting):
     from pmsim_b200.batch import BatchSolver
-    rng = np.random.default_rng(21)
-    probs = [footing(int(rng.integers(4, 16)), int(rng.integers(2, 8)), float(1e4 * np.exp(rng.normal(0, 0.5))),
-                     float(rng.uniform(5, 20)), float(rng.uniform(0.5, 2.0)), nsteps=3) for _ in range(6)]
-    runs = []
-    for setting in ("wide", "block", "mixed", "auto"):
-        bs = BatchSolver(probs)
-        if setting == "wide":
-            bs.set_tuning(block_max_ndof=0)
-        elif setting == "block":
-            bs.set_tuning(block_max_ndof=10 ** 9, block_threads=256, pcg_budget=7)
-        elif setting == "mixed":
-            nd = sorted(p.mesh.ndof for p in probs)
-            bs.set_tuning(block_max_ndof=nd[len(nd) // 2], block_threads=1024, graph_iters=2, pcg_budget=16)
-        else:
-            bs.autotune()
-        bs.solve_independent(on_fail="drop")
-        runs.append((setting, bs.u(), bs.elements.get_state(), bs.history, bs.pcg_history, dict(bs.failed)))
-        bs.close()
-    _, u0, st0, h0, pc0, f0 = runs[0]
-    for name, u, st, h, pc, f in runs[1:]:
+    bs = BatchSolver(probs)
+    if setting == "wide":
+        bs.set_tuning(team_max_ndof=0)
+    elif setting == "teams1":  # one 128-node chunk per CTA: clusters of 1..16 CTAs
+        bs.set_tuning(team_max_ndof=10 ** 12, team_threads=256, team_chunks=1, pcg_budget=7)
+    elif setting == "teams4":
+        bs.set_tuning(team_max_ndof=10 ** 12, team_threads=1024, team_chunks=4, pcg_budget=33)
+    elif setting == "mixed":
+        nd = sorted(p.mesh.ndof for p in probs)
+        bs.set_tuning(team_max_ndof=nd[len(nd) // 2], team_threads=512, team_chunks=0, graph_iters=2, pcg_budget=16)
+    else:
+        bs.autotune()
+    bs.solve_independent(on_fail="drop")
+    out = (bs.u(), bs.elements.get_state(), bs.history, bs.pcg_history, dict(bs.failed))
+    bs.close()
+    return out
+
+
+def _assert_same(runs):
+    (n0, (u0, st0, h0, pc0, f0)) = runs[0]
+    for name, (u, st, h, pc, f) in runs[1:]:
         assert f == f0, name
-        assert np.array_equal(u, u0), f"{name}: U differs from the batch-wide engine"
+        assert np.array_equal(u, u0), f"{name}: U differs from {n0}"
         for x, y in zip(st, st0):
             assert np.array_equal(x, y), name
         assert h == h0, name
         assert pc == pc0, name
+
+
+def test_pcg_engines_give_the_same_bits():
+    """The team engine (a thread-block cluster per problem, vectors in shared memory) and the
+    batch-wide engine run the same arithmetic: forcing either one, any team shape, or letting the
+    autotuner choose gives identical U, IP state and Newton/PCG iteration histories."""
+    rng = np.random.default_rng(21)
+    probs = [footing(int(rng.integers(4, 16)), int(rng.integers(2, 8)), float(1e4 * np.exp(rng.normal(0, 0.5))),
+                     float(rng.uniform(5, 20)), float(rng.uniform(0.5, 2.0)), nsteps=3) for _ in range(6)]
+    _assert_same([(s, _solve_with(probs, s)) for s in ("wide", "teams1", "teams4", "mixed", "auto")])
+
+
+def test_pcg_sixteen_cta_team_matches_batch_wide():
+    """A 64x32 footing (50 chunks) on a 16-CTA cluster (4 chunks per CTA, p read across CTAs
+    through distributed shared memory) next to a small one: same bits as the batch-wide engine."""
+    probs = [footing(64, 32, 1e4, 9.0, 1.0, nsteps=2), footing(6, 3, 2e4, 12.0, 1.5, nsteps=2)]
+    _assert_same([(s, _solve_with(probs, s)) for s in ("wide", "teams4")])
