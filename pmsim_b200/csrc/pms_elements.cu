@@ -133,9 +133,11 @@ __device__ __forceinline__ double inv_jacobian(const double* J, double* Ji) {
     }
 }
 
-// Warps per cell: the 20-node kinds split the node-pair triangle over two warps (2x2 register
-// tiles), which halves the registers of a thread and doubles the warps an SM can hold.
-__host__ __device__ constexpr int warps_per_cell(int nn) { return nn >= 16 ? 2 : 1; }
+// Warps per cell.  The kernel can split a cell's node-pair triangle over two warps (2x2 register
+// tiles: fewer registers per thread, more warps per SM), but for Hex20 that measured slower (4.55
+// vs 4.27 ms on the 64x64x32 block: 40% more shared-memory loads per pair, and the second warp
+// idles during the integration-point phase), so every kind uses one warp per cell.
+__host__ __device__ constexpr int warps_per_cell(int) { return 1; }
 __host__ __device__ constexpr int cells_per_block(int nn) { return WPB / warps_per_cell(nn); }
 
 // Register tile of node pairs per lane: rows (a) x cols (b) of the upper node-pair triangle.

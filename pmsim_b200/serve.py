@@ -57,7 +57,7 @@ class Server:
     ``max_concurrent`` batches run at a time, each on its own stream and host thread; ``autotune``
     picks each batch's PCG launch shapes (which change speed, never results)."""
 
-    def __init__(self, budget_bytes=120e9, max_batch=256, max_concurrent=16, admit_window=0.025,
+    def __init__(self, budget_bytes=120e9, max_batch=256, max_concurrent=4, admit_window=0.1,
                  keep_results=False, autotune=True, **solver_kw):
         self.budget = float(budget_bytes)
         self.max_batch = max_batch
