@@ -405,13 +405,29 @@ def cpu_sample(m, ddu, ncell_sample, nthreads):
     el = oracle.OracleElements(sub, oracle.MODEL_VON_MISES, oracle.Params(E, NU, HH, Z0), sym_tol=-1.0,
                                nthreads=nthreads)
     el.initialize()
-    t0 = time.perf_counter()
+    t = [time.perf_counter()]
     el.update_secondary_values(ddu)
+    t.append(time.perf_counter())
     el.assemble_f_int()
+    t.append(time.perf_counter())
     rows, cols, vals = el.assemble_kk_coo()
+    t.append(time.perf_counter())
     oracle.coo_to_csr(m.ndof, rows, cols, vals)
-    dt = time.perf_counter() - t0
-    return dt, ncell_sample * el.ngauss
+    t.append(time.perf_counter())
+    cpu_sample.phases = dict(zip(("update_secondary", "f_int", "k_coo", "csr_sum"),
+                                 (t[i + 1] - t[i] for i in range(4))))
+    return t[-1] - t[0], ncell_sample * el.ngauss
+
+
+def cpu_model():
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
 
 
 def reference_arm(args, rank):
@@ -439,7 +455,8 @@ def reference_arm(args, rank):
         "config": {"workload": f"hex20 {nx}x{ny}x{nz} block, 27 IP, von Mises (one Newton iteration)",
                    "parallelism": "host threads"},
         "cpu_baseline": {"value": value, "unit": "IP/s", "cores": nthreads, "kind": "port",
-                         "sample": f"first {ncs} cells ({ncs * 27} IPs) per step: update + F_int + K COO + CSR"},
+                         "sample": f"first {ncs} cells ({ncs * 27} IPs) per step: update + F_int + K COO + CSR",
+                         "cpu_model": cpu_model(), "nproc": os.cpu_count()},
         "e2e": {"value": value, "unit": "IP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -567,10 +584,12 @@ def main():
         ncs = args.cpu_cells or (512 if args.size == "small" else 4096)
         cpu_sample(m, ddu_h, 256, nthreads)
         dt, n = cpu_sample(m, ddu_h, ncs, nthreads)
+        phases = {k: v / n * 1e6 for k, v in cpu_sample.phases.items()}
         dt1, n1 = cpu_sample(m, ddu_h, max(ncs // 8, 64), 1)
         cpu = {"value": n / dt, "unit": "IP/s", "cores": nthreads, "kind": "port",
                "sample": f"first {ncs} cells ({n} IPs): update + F_int + K COO + CSR sum, all threads",
-               "single_thread_ip_per_s": n1 / dt1}
+               "single_thread_ip_per_s": n1 / dt1, "us_per_ip_by_phase": phases,
+               "cpu_model": cpu_model(), "nproc": os.cpu_count()}
     nx, ny, nz = workload_dims(args.size)
     line = {
         "metric": "IP stress-update+tangent/s FP64",

@@ -142,20 +142,31 @@ __host__ __device__ constexpr int cells_per_block(int nn) { return WPB / warps_p
 
 // Register tile of node pairs per lane: rows (a) x cols (b) of the upper node-pair triangle.
 // The tile shapes keep the number of tiles <= 32 per warp of the cell.
+template <int NN> struct TileShape;
+template <int NN> __host__ __device__ constexpr int tile_count() {
+    int k = 0;
+    for (int i = 0; i < TileShape<NN>::NRG; i++)
+        for (int j = 0; j < TileShape<NN>::NCG; j++) {
+            const int jmax = (j * TileShape<NN>::CT + TileShape<NN>::CT - 1) < (NN - 1)
+                                 ? (j * TileShape<NN>::CT + TileShape<NN>::CT - 1) : (NN - 1);
+            if (i * TileShape<NN>::RT <= jmax) k++;
+        }
+    return k;
+}
 template <int NN> struct TileShape {
     static constexpr int RT = NN >= 16 ? 2 : 1;
-    static constexpr int CT = warps_per_cell(NN) == 2 ? 2 : (NN >= 7 ? 2 : 1);
+    static constexpr int CT = warps_per_cell(NN) == 2 ? 2 : (NN >= 16 ? 4 : (NN >= 7 ? 2 : 1));
     static constexpr int NRG = (NN + RT - 1) / RT;
     static constexpr int NCG = (NN + CT - 1) / CT;
 };
 
 // Shared memory (doubles): block-wide dN table [m][j][32] + w[32], then per cell
 // X[NN*ND], dU[NN*ND], G[ng][NN*ND+1] (gradients), TC[ng][10] (alpha, gamma, beta, S), CS[ng][6],
-// V[2][NN][5*ND] (per node at the current IP, double-buffered: alpha g, gamma g, beta h, g, h with
-// h = S g).
+// V[WPC][NN][5*ND] (per node at the current IP: alpha g, gamma g, beta h, g, h with h = S g;
+// double-buffered when two warps share the cell).
 __host__ __device__ constexpr int smem_table_doubles(int nn, int nd) { return nn * nd * 32 + 32; }
 __host__ __device__ constexpr int smem_cell_doubles(int nn, int nd, int ng) {
-    return 2 * nn * nd + ng * (nn * nd + 1) + ng * 10 + ng * 6 + 2 * nn * 5 * nd;
+    return 2 * nn * nd + ng * (nn * nd + 1) + ng * 10 + ng * 6 + warps_per_cell(nn) * nn * 5 * nd;
 }
 __host__ __device__ constexpr int smem_bytes_for(int nn, int nd, int ng, int wpb) {
     return (smem_table_doubles(nn, nd) + (wpb / warps_per_cell(nn)) * smem_cell_doubles(nn, nd, ng)) * 8;
@@ -169,6 +180,7 @@ __global__ void __launch_bounds__(WPB * 32, warps_per_cell(NN) == 2 ? 3 : 1) ele
     using TS = TileShape<NN>;
     constexpr int RT = TS::RT, CT = TS::CT;
     constexpr int WPC = warps_per_cell(NN), CPB = WPB / WPC;
+    static_assert(tile_count<NN>() <= 32 * WPC, "every node-pair tile needs a lane");
     extern __shared__ double smem[];
     const int ng = A.ngauss;
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
@@ -395,7 +407,10 @@ __global__ void __launch_bounds__(WPB * 32, warps_per_cell(NN) == 2 ? 3 : 1) ele
         for (int p = 0; p < ng; p++) {
             const double* t = TC + p * 10;
             const bool plastic = t[2] != 0.0;  // beta: same value on every lane, uniform branch
-            double* V = V0 + (p & 1) * NN * VS;  // double buffer: one barrier per IP
+            // two warps: double buffer, one barrier per IP; one warp: every lane is done with the
+            // previous IP's vectors before the node lanes overwrite them
+            double* V = V0 + (WPC == 2 ? (p & 1) * NN * VS : 0);
+            if constexpr (WPC == 1) __syncwarp();
             // node lanes of warp 0: the scaled gradients of their node at this IP
             if (half == 0 && lane < NN) {
                 const double al = t[0], ga = t[1], be = t[2];
