@@ -155,13 +155,13 @@ def elem_jacobian(kind, ngauss, X, model, params, sig, ivs, elastic, thickness=1
 class OracleElements:
     """Mirror of ``Elements`` (src/fem/elements.rs) over a homogeneous mesh, AoS IP state."""
 
-    def __init__(self, mesh, model, params, ngauss=0, thickness=1.0, sym_tol=1e-10, nthreads=1):
+    def __init__(self, mesh, model, params, ngauss=0, thickness=1.0, sym_tol=1e-10, nthreads=1, axisymmetric=False):
         self.mesh = mesh
         self.kind = mesh.kind
         self.model = model
         self.params = params
         self.ngauss = ngauss if ngauss > 0 else lib().orc_default_ngauss(mesh.kind)
-        self.thickness = thickness
+        self.thickness = -1.0 if axisymmetric else thickness  # < 0: axisymmetric (weight = radius)
         self.sym_tol = sym_tol
         self.nthreads = nthreads
         self.nc = 2 * mesh.ndim

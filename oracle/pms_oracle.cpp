@@ -404,8 +404,20 @@ struct ElemCtx {
     int kind, nn, nd, nc, ngauss;
     double ksi[27 * 3], w[27];
     double thickness;
+    bool axisym;  // 2D axisymmetric idealization (x = radius): weight |J| w r, hoop strain u_r / r
 };
 
+// Integration weight of an IP: |J| w t, or |J| w r in the axisymmetric idealization (r = sum N_m x_m,
+// gemlab's integrators with args.axisymmetric, called by src/fem/element_solid.rs:128,150,171).
+inline double ip_coef(const ElemCtx& c, const IpGeo& g, const double* X, int p, double* radius) {
+    if (!c.axisym) return g.det * c.w[p] * c.thickness;
+    double r = 0.0;
+    for (int m = 0; m < c.nn; m++) r += g.N[m] * X[m * 2];
+    *radius = r;
+    return g.det * c.w[p] * r;
+}
+
+// thickness < 0 selects the axisymmetric idealization (2D kinds only)
 bool make_ctx(int kind, int ngauss, double thickness, ElemCtx& c) {
     c.kind = kind;
     c.nn = kind_nnode(kind);
@@ -414,7 +426,9 @@ bool make_ctx(int kind, int ngauss, double thickness, ElemCtx& c) {
     c.nc = 2 * c.nd;
     if (ngauss <= 0) ngauss = default_ngauss(kind);
     c.ngauss = gauss_rule(kind, ngauss, c.ksi, c.w);
-    c.thickness = thickness;
+    c.axisym = thickness < 0.0;
+    c.thickness = c.axisym ? 1.0 : thickness;
+    if (c.axisym && c.nd != 2) return false;
     return c.ngauss > 0;
 }
 
@@ -426,7 +440,8 @@ int elem_f_int(const ElemCtx& c, const double* X, const double* sig /*ngauss*nc*
     for (int p = 0; p < c.ngauss; p++) {
         int st = ip_geometry(c.kind, X, c.ksi + 3 * p, g);
         if (st) return st;
-        double coef = g.det * c.w[p] * c.thickness;
+        double r = 1.0;
+        double coef = ip_coef(c, g, X, p, &r);
         const double* v = sig + p * c.nc;
         double S[3][3];
         S[0][0] = v[0]; S[1][1] = v[1]; S[2][2] = v[2];
@@ -436,6 +451,7 @@ int elem_f_int(const ElemCtx& c, const double* X, const double* sig /*ngauss*nc*
             for (int i = 0; i < c.nd; i++) {
                 double s = 0;
                 for (int j = 0; j < c.nd; j++) s += S[i][j] * g.G[m * c.nd + j];
+                if (c.axisym && i == 0) s += v[2] * g.N[m] / r;  // hoop row of B: N/r on u_r
                 f[m * c.nd + i] += coef * s;
             }
     }
@@ -455,8 +471,11 @@ int elem_jacobian(const ElemCtx& c, const double* X, int model, const Params& pr
         if (st) return st;
         st = model_stiffness(model, prm, c.nc, sig + p * c.nc, ivs + 2 * p, elastic[p], dd);
         if (st) return st;
-        double coef = g.det * c.w[p] * c.thickness;
+        double r = 1.0;
+        double coef = ip_coef(c, g, X, p, &r);
         b_matrix(c.nn, c.nd, g.G, B.data());
+        if (c.axisym)
+            for (int m = 0; m < c.nn; m++) B[2 * ne + 2 * m] = g.N[m] / r;  // eps_zz = u_r / r
         for (int k = 0; k < c.nc; k++)
             for (int col = 0; col < ne; col++) {
                 double s = 0;
@@ -490,6 +509,11 @@ int elem_update(const ElemCtx& c, const double* X, int model, const Params& prm,
                 eps[0] += ux * gx;
                 eps[1] += uy * gy;
                 eps[3] += SQRT2 * ((ux * gy + uy * gx) / 2.0);
+            }
+            if (c.axisym) {  // src/base/calculate_strain.rs:36-48: out-of-plane strain u_r / r
+                double r = 0.0;
+                for (int m = 0; m < c.nn; m++) r += g.N[m] * X[2 * m];
+                for (int m = 0; m < c.nn; m++) eps[2] += du[2 * m] * g.N[m] / r;
             }
         } else {
             for (int m = 0; m < c.nn; m++) {

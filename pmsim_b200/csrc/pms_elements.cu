@@ -61,6 +61,7 @@ enum { UPD_NONE = 0, UPD_CURRENT = 1, UPD_BACKUP = 2, UPD_MODE = 3 };
 struct ElemArgs {
     int64_t ncell;     // cells in this launch
     int64_t cell0;     // first cell of this launch
+    int axisym = 0;    // 2D axisymmetric idealization (x = radius)
     int64_t nip;       // total IPs of the mesh (SoA stride)
     int ngauss;
     double thickness;
@@ -69,7 +70,7 @@ struct ElemArgs {
     const int32_t* cmat;    // per-cell material (nullable)
     const MatConst* mats;
     const double* ddu;      // ndof
-    const double* tab;      // dN[ngauss][nn][nd], then w[ngauss]
+    const double* tab;      // dN[ngauss][nn][nd], then w[ngauss], then N[ngauss][nn] (axisymmetric)
     // IP state, SoA with stride nip: sig[c*nip + ip]
     const double* sig_src; const double* z_src; const double* lam_src; const uint8_t* el_src;
     double* sig; double* z; double* lam; uint8_t* el;
@@ -160,13 +161,17 @@ template <int NN> struct TileShape {
     static constexpr int NCG = (NN + CT - 1) / CT;
 };
 
-// Shared memory (doubles): block-wide dN table [m][j][32] + w[32], then per cell
+// Shared memory (doubles): block-wide dN table [m][j][32] + w[32] (+ N table [m][32] in 2D), then per cell
 // X[NN*ND], dU[NN*ND], G[ng][NN*ND+1] (gradients), TC[ng][10] (alpha, gamma, beta, S), CS[ng][6],
-// V[WPC][NN][5*ND] (per node at the current IP: alpha g, gamma g, beta h, g, h with h = S g;
-// double-buffered when two warps share the cell).
-__host__ __device__ constexpr int smem_table_doubles(int nn, int nd) { return nn * nd * 32 + 32; }
+// V[WPC][NN][VS] (per node at the current IP: alpha g, gamma g^, beta h, g, h, and in 2D g^,
+// 2 (a/2)|J|w r q and q, with h = S g (+ q s_zz e_x), g^ = g (+ q e_x) and q = N/r in the axisymmetric
+// idealization; double-buffered when two warps share the cell).
+__host__ __device__ constexpr int node_vec_doubles(int nd) { return 5 * nd + (nd == 2 ? 4 : 0); }
+__host__ __device__ constexpr int smem_table_doubles(int nn, int nd) {
+    return nn * nd * 32 + 32 + (nd == 2 ? nn * 32 : 0);
+}
 __host__ __device__ constexpr int smem_cell_doubles(int nn, int nd, int ng) {
-    return 2 * nn * nd + ng * (nn * nd + 1) + ng * 10 + ng * 6 + warps_per_cell(nn) * nn * 5 * nd;
+    return 2 * nn * nd + ng * (nn * nd + 1) + ng * 10 + ng * 6 + warps_per_cell(nn) * nn * node_vec_doubles(nd);
 }
 __host__ __device__ constexpr int smem_bytes_for(int nn, int nd, int ng, int wpb) {
     return (smem_table_doubles(nn, nd) + (wpb / warps_per_cell(nn)) * smem_cell_doubles(nn, nd, ng)) * 8;
@@ -187,6 +192,7 @@ __global__ void __launch_bounds__(WPB * 32, warps_per_cell(NN) == 2 ? 3 : 1) ele
     const int cs = wid / WPC, half = wid % WPC;  // cell slot in the block, warp within the cell
     double* dNs = smem;                        // [m][j][32]
     double* ws = smem + NE * 32;               // [32]
+    double* Ns = ws + 32;                      // [m][32] (2D)
     double* wbase = smem + smem_table_doubles(NN, ND) + cs * smem_cell_doubles(NN, ND, ng);
     double* Xs = wbase;                        // [m][d]
     double* Us = Xs + NE;                      // [m][d]
@@ -201,6 +207,11 @@ __global__ void __launch_bounds__(WPB * 32, warps_per_cell(NN) == 2 ? 3 : 1) ele
         dNs[r * 32 + p] = A.tab[i];
     }
     for (int i = threadIdx.x; i < ng; i += blockDim.x) ws[i] = A.tab[ng * NE + i];
+    if (ND == 2 && A.axisym)
+        for (int i = threadIdx.x; i < ng * NN; i += blockDim.x) {
+            const int p = i / NN, m = i % NN;
+            Ns[m * 32 + p] = A.tab[ng * NE + ng + i];
+        }
     __syncthreads();
 
     // the warps of one cell meet at a named barrier (id 1 + cell slot)
@@ -272,7 +283,14 @@ __global__ void __launch_bounds__(WPB * 32, warps_per_cell(NN) == 2 ? 3 : 1) ele
         double Ji[ND * ND];
         const double det = inv_jacobian<ND>(J, Ji);
         if (!(det > 0.0)) err = E_JACOBIAN;
-        const double coef = det * ws[p] * A.thickness;
+        // integration weight |J| w t, or |J| w r with r = sum N_m x_m (axisymmetric)
+        double rad = 1.0;
+        if (ND == 2 && A.axisym) {
+            rad = 0.0;
+#pragma unroll
+            for (int m = 0; m < NN; m++) rad += Ns[m * 32 + p] * Xs[m * ND];
+        }
+        const double coef = det * ws[p] * ((ND == 2 && A.axisym) ? rad : A.thickness);
         double eps[NC];
 #pragma unroll
         for (int c = 0; c < NC; c++) eps[c] = 0.0;
@@ -302,6 +320,9 @@ __global__ void __launch_bounds__(WPB * 32, warps_per_cell(NN) == 2 ? 3 : 1) ele
                 }
             }
         }
+        if (ND == 2 && A.axisym && do_update)  // out-of-plane strain u_r / r (calculate_strain.rs:36-48)
+#pragma unroll
+            for (int m = 0; m < NN; m++) eps[2] += Us[m * ND] * Ns[m * 32 + p] / rad;
         if (do_update) {
             const int st = ip_update<NC>(mc, mc.hh, sig, z, lam, el, eps);
             if (st != OK && err == OK) err = st;
@@ -311,6 +332,10 @@ __global__ void __launch_bounds__(WPB * 32, warps_per_cell(NN) == 2 ? 3 : 1) ele
             c6[0] = coef * sig[0];
             c6[1] = coef * sig[1];
             c6[2] = coef * sig[3] * INV_SQRT2;
+            if constexpr (ND == 2) {
+                c6[3] = coef * sig[2];  // hoop stress (axisymmetric)
+                c6[4] = rad;
+            }
             if constexpr (ND == 3) {
                 c6[3] = coef * sig[2];
                 c6[4] = coef * sig[4 % NC] * INV_SQRT2;
@@ -328,6 +353,10 @@ __global__ void __launch_bounds__(WPB * 32, warps_per_cell(NN) == 2 ? 3 : 1) ele
             t[3] = s[0];
             t[4] = s[1];
             t[5] = s[3] * INV_SQRT2;
+            if constexpr (ND == 2) {
+                t[6] = s[2];  // deviatoric s_zz (axisymmetric hoop row)
+                t[9] = rad;
+            }
             if constexpr (ND == 3) {
                 t[6] = s[2];
                 t[7] = s[4 % NC] * INV_SQRT2;
@@ -364,6 +393,7 @@ __global__ void __launch_bounds__(WPB * 32, warps_per_cell(NN) == 2 ? 3 : 1) ele
             if constexpr (ND == 2) {
                 f[0] += c6[0] * g[0] + c6[2] * g[1];
                 f[1] += c6[2] * g[0] + c6[1] * g[1];
+                if (A.axisym) f[0] += c6[3] * Ns[lane * 32 + p] / c6[4];
             } else {
                 f[0] += c6[0] * g[0] + c6[2] * g[1] + c6[5 % 6] * g[2 % ND];
                 f[1] += c6[2] * g[0] + c6[1] * g[1] + c6[4 % 6] * g[2 % ND];
@@ -403,7 +433,7 @@ __global__ void __launch_bounds__(WPB * 32, warps_per_cell(NN) == 2 ? 3 : 1) ele
                 for (int i = 0; i < ND; i++)
 #pragma unroll
                     for (int j = 0; j < ND; j++) acc[r][c][i][j] = 0.0;
-        constexpr int VS = 5 * ND;
+        constexpr int VS = node_vec_doubles(ND);
         for (int p = 0; p < ng; p++) {
             const double* t = TC + p * 10;
             const bool plastic = t[2] != 0.0;  // beta: same value on every lane, uniform branch
@@ -425,26 +455,38 @@ __global__ void __launch_bounds__(WPB * 32, warps_per_cell(NN) == 2 ? 3 : 1) ele
                 }
                 const double* g = G + p * GS + lane * ND;
                 double* v = V + lane * VS;
-                double gv[ND];
+                double gv[ND], gh[ND];  // gradient and volumetric row B^T I (with the hoop term)
 #pragma unroll
-                for (int i = 0; i < ND; i++) gv[i] = g[i];
+                for (int i = 0; i < ND; i++) gh[i] = gv[i] = g[i];
+                double q = 0.0;  // N/r of this node (axisymmetric)
+                if (ND == 2 && A.axisym) {
+                    q = Ns[lane * 32 + p] / t[9];
+                    gh[0] = gv[0] + q;
+                }
 #pragma unroll
                 for (int i = 0; i < ND; i++) {
                     double h = 0.0;
                     if (plastic) {
 #pragma unroll
                         for (int j = 0; j < ND; j++) h = fma(S[i][j], gv[j], h);
+                        if (ND == 2 && A.axisym && i == 0) h = fma(q, t[6], h);
                     }
                     v[i] = al * gv[i];
-                    v[ND + i] = ga * gv[i];
+                    v[ND + i] = ga * gh[i];
                     v[2 * ND + i] = be * h;
                     v[3 * ND + i] = gv[i];
                     v[4 * ND + i] = h;
                 }
+                if constexpr (ND == 2) {
+                    v[5 * ND] = gh[0];
+                    v[5 * ND + 1] = gh[1];
+                    v[5 * ND + 2] = 2.0 * al * q;
+                    v[5 * ND + 3] = q;
+                }
             }
             cell_sync();
             if (ti < 0) continue;
-            double Ar[RT][ND], Cr[RT][ND], Hr[RT][ND];
+            double Ar[RT][ND], Cr[RT][ND], Hr[RT][ND], Qr[RT];
 #pragma unroll
             for (int r = 0; r < RT; r++) {
                 const double* v = V + min(a0 + r, NN - 1) * VS;
@@ -454,16 +496,19 @@ __global__ void __launch_bounds__(WPB * 32, warps_per_cell(NN) == 2 ? 3 : 1) ele
                     Cr[r][i] = v[ND + i];
                     Hr[r][i] = v[2 * ND + i];
                 }
+                Qr[r] = (ND == 2) ? v[(5 * ND + 2) % VS] : 0.0;
             }
 #pragma unroll
             for (int c = 0; c < CT; c++) {
                 const double* v = V + min(b0 + c, NN - 1) * VS;
-                double gb[ND], hb[ND];
+                double gb[ND], hb[ND], gc[ND];  // g, h and the volumetric row of the column node
 #pragma unroll
                 for (int i = 0; i < ND; i++) {
                     gb[i] = v[3 * ND + i];
                     hb[i] = v[4 * ND + i];
+                    gc[i] = (ND == 2) ? v[(5 * ND + i) % VS] : gb[i];
                 }
+                const double qb = (ND == 2) ? v[(5 * ND + 3) % VS] : 0.0;
                 double dot[RT];
 #pragma unroll
                 for (int r = 0; r < RT; r++) {
@@ -483,7 +528,7 @@ __global__ void __launch_bounds__(WPB * 32, warps_per_cell(NN) == 2 ? 3 : 1) ele
 #pragma unroll
                     for (int i = 0; i < ND; i++)
 #pragma unroll
-                        for (int j = 0; j < ND; j++) acc[r][c][i][j] = fma(Cr[r][i], gb[j], acc[r][c][i][j]);
+                        for (int j = 0; j < ND; j++) acc[r][c][i][j] = fma(Cr[r][i], gc[j], acc[r][c][i][j]);
                 if (plastic) {
 #pragma unroll
                     for (int r = 0; r < RT; r++)
@@ -496,6 +541,9 @@ __global__ void __launch_bounds__(WPB * 32, warps_per_cell(NN) == 2 ? 3 : 1) ele
                 for (int r = 0; r < RT; r++)
 #pragma unroll
                     for (int i = 0; i < ND; i++) acc[r][c][i][i] += dot[r];
+                if (ND == 2 && A.axisym)  // hoop row: a (N_a/r)(N_b/r) on the radial-radial entry
+#pragma unroll
+                    for (int r = 0; r < RT; r++) acc[r][c][0][0] = fma(Qr[r], qb, acc[r][c][0][0]);
             }
         }
         // write K_e (row-major NE x NE) through the warp's shared memory, RS node rows at a time:
@@ -661,6 +709,7 @@ struct pms_elements {
     int gather_wpb = 8, gather_smem = 0;  // rows (warps) per block and shared memory of kk_gather
     int64_t npoint = 0, ncell = 0, ndof = 0, nip = 0, nnz = 0;
     double thickness = 1.0;
+    int axisym = 0;
     std::vector<MatConst> mats;
     Pattern pat;
     std::vector<double> tab;  // dN table + weights
@@ -838,6 +887,7 @@ ElemArgs make_args(pms_elements* h, const double* ddu) {
     a.nip = h->nip;
     a.ngauss = h->ng;
     a.thickness = h->thickness;
+    a.axisym = h->axisym;
     a.coords = h->d_coords;
     a.conn = h->d_conn;
     a.cmat = h->d_cmat;
@@ -913,7 +963,7 @@ int pms_elements_create(const pms_mesh* mesh, const pms_material* materials, int
     int kind = mesh->kind;
     if (kind < 0 || kind > 8 || kind_ndim(kind) != mesh->ndim) return PMS_ERR_INVALID;
     if (config->plane_stress) return PMS_ERR_UNSUPPORTED;
-    if (config->axisymmetric) return PMS_ERR_UNSUPPORTED;
+    if (config->axisymmetric && mesh->ndim != 2) return PMS_ERR_UNSUPPORTED;
     if (mesh->npoint < 1 || mesh->ncell < 1) return PMS_ERR_INVALID;
     auto* h = new pms_elements();
     h->kind = kind;
@@ -924,6 +974,7 @@ int pms_elements_create(const pms_mesh* mesh, const pms_material* materials, int
     h->ncell = mesh->ncell;
     h->ndof = h->npoint * h->nd;
     h->thickness = config->thickness > 0 ? config->thickness : 1.0;
+    h->axisym = config->axisymmetric ? 1 : 0;
     std::vector<double> ksi, w;
     h->ng = integration_rule(kind, config->ngauss, ksi, w);
     if (h->ng <= 0 || h->ng > 32) {
@@ -942,7 +993,7 @@ int pms_elements_create(const pms_mesh* mesh, const pms_material* materials, int
             if (mesh->cell_material[c] < 0 || mesh->cell_material[c] >= nmaterial) { delete h; return PMS_ERR_INVALID; }
     }
     // shape tables
-    h->tab.assign((size_t)h->ng * h->nn * h->nd + h->ng, 0.0);
+    h->tab.assign((size_t)h->ng * h->nn * h->nd + h->ng + (size_t)h->ng * h->nn, 0.0);
     {
         double N[20], dN[60];
         for (int p = 0; p < h->ng; p++) {
@@ -950,6 +1001,7 @@ int pms_elements_create(const pms_mesh* mesh, const pms_material* materials, int
             for (int m = 0; m < h->nn; m++)
                 for (int j = 0; j < h->nd; j++) h->tab[(p * h->nn + m) * h->nd + j] = dN[m * h->nd + j];
             h->tab[(size_t)h->ng * h->nn * h->nd + p] = w[p];
+            for (int m = 0; m < h->nn; m++) h->tab[(size_t)h->ng * h->nn * h->nd + h->ng + p * h->nn + m] = N[m];
         }
     }
     const char* msg = nullptr;

@@ -896,24 +896,21 @@ void launch_spmv(pms_batch* b, const double* x, double* y, const uint8_t* flag, 
     b->launches++;
 }
 
-// one batch-wide PCG iteration (parity par) for every problem with pcg_active set (3 kernels)
-void wide_iteration(pms_batch* b, int par) {
-    cudaStream_t st = b->v.stream;
-    const unsigned nch = (unsigned)b->nchunk;
-    if (tpr_of(b->v.nd) == 8)
-        pcg_spmv_dot_kernel<8><<<nch, WIDE_SPMV_THREADS, 0, st>>>(b->S, par, b->d_indptr, b->d_indices, b->d_csr,
-                                                                   b->d_p, b->d_q, b->d_part_c);
-    else
-        pcg_spmv_dot_kernel<16><<<nch, WIDE_SPMV_THREADS, 0, st>>>(b->S, par, b->d_indptr, b->d_indices, b->d_csr,
-                                                                    b->d_p, b->d_q, b->d_part_c);
-    pcg_update_kernel<<<nch, CHN, 0, st>>>(b->S, par, b->d_part_c, b->d_rho, b->d_p, b->d_q, b->d_binv, b->d_x,
-                                           b->d_r, b->d_z, b->d_part_a, b->d_part_b, b->d_nactive);
-    pcg_beta_direction_kernel<<<nch, CHN, 0, st>>>(b->S, par, b->d_part_a, b->d_part_b, b->d_rho, b->d_r0,
-                                                   b->cfg.pcg_rtol, b->cfg.pcg_max_iterations, b->d_iters, b->d_z,
-                                                   b->d_p, b->d_nactive);
-    b->launches += 3;
+// Appends a kernel node (after `dep`, if any) to graph g; args point at the argument values.
+cudaError_t add_kernel_node(cudaGraph_t g, cudaGraphNode_t* node, cudaGraphNode_t dep, void* fn, unsigned grid,
+                            unsigned block, void** args) {
+    cudaKernelNodeParams kp = {};
+    kp.func = fn;
+    kp.gridDim = dim3(grid);
+    kp.blockDim = dim3(block);
+    kp.sharedMemBytes = 0;
+    kp.kernelParams = args;
+    kp.extra = nullptr;
+    return cudaGraphAddKernelNode(node, g, dep ? &dep : nullptr, dep ? 1 : 0, &kp);
 }
 
+// The batch-wide PCG graph: graph_iters iterations (even) of the three kernels, built node by node
+// (no stream capture, so other host threads that launch work meanwhile cannot disturb it).
 int ensure_graph(pms_batch* b) {
     const int gi = std::max(2, b->tune.graph_iters + (b->tune.graph_iters & 1));  // even
     if (b->graph && b->graph_iters_captured == gi) return PMS_OK;
@@ -922,15 +919,34 @@ int ensure_graph(pms_batch* b) {
         cudaGraphExecDestroy(b->graph);
         b->graph = nullptr;
     }
-    cudaStream_t st = b->v.stream;
     cudaGraph_t g;
-    if (cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
-        return bfail(b, PMS_ERR_CUDA, "stream capture failed");
-    for (int i = 0; i < gi; i++) wide_iteration(b, i & 1);
-    if (cudaStreamEndCapture(st, &g) != cudaSuccess) return bfail(b, PMS_ERR_CUDA, "stream capture failed");
-    if (cudaGraphInstantiate(&b->graph, g, 0) != cudaSuccess) {
+    if (cudaGraphCreate(&g, 0) != cudaSuccess) return bfail(b, PMS_ERR_CUDA, "graph creation failed");
+    const unsigned nch = (unsigned)b->nchunk;
+    void* spmv = tpr_of(b->v.nd) == 8 ? (void*)pcg_spmv_dot_kernel<8> : (void*)pcg_spmv_dot_kernel<16>;
+    cudaGraphNode_t prev = nullptr;
+    bool ok = true;
+    for (int i = 0; i < gi && ok; i++) {
+        int par = i & 1;
+        const double* val = b->d_csr;
+        double rtol = b->cfg.pcg_rtol;
+        int32_t max_iter = b->cfg.pcg_max_iterations;
+        void* a1[] = {&b->S, &par, (void*)&b->d_indptr, (void*)&b->d_indices, (void*)&val, &b->d_p, &b->d_q,
+                      &b->d_part_c};
+        void* a2[] = {&b->S, &par, &b->d_part_c, &b->d_rho, &b->d_p, &b->d_q, &b->d_binv, &b->d_x, &b->d_r,
+                      &b->d_z, &b->d_part_a, &b->d_part_b, &b->d_nactive};
+        void* a3[] = {&b->S, &par, &b->d_part_a, &b->d_part_b, &b->d_rho, &b->d_r0, &rtol, &max_iter,
+                      &b->d_iters, &b->d_z, &b->d_p, &b->d_nactive};
+        cudaGraphNode_t n1, n2, n3;
+        ok = add_kernel_node(g, &n1, prev, spmv, nch, WIDE_SPMV_THREADS, a1) == cudaSuccess &&
+             add_kernel_node(g, &n2, n1, (void*)pcg_update_kernel, nch, CHN, a2) == cudaSuccess &&
+             add_kernel_node(g, &n3, n2, (void*)pcg_beta_direction_kernel, nch, CHN, a3) == cudaSuccess;
+        prev = n3;
+        b->launches += 3;
+    }
+    if (!ok || cudaGraphInstantiate(&b->graph, g, 0) != cudaSuccess) {
+        b->graph = nullptr;
         cudaGraphDestroy(g);
-        return bfail(b, PMS_ERR_CUDA, "graph instantiation failed");
+        return bfail(b, PMS_ERR_CUDA, "graph construction failed");
     }
     cudaGraphDestroy(g);
     b->graph_iters_captured = gi;

@@ -12,6 +12,7 @@ Sources (paths inside the pmsim project):
   * data/spo/spo_755_tensile_perf_plast_ref.json + spo_755_tensile.msh (Qua8 4 IP, 15 steps)
   * data/results/artificial/*.json, *.msh  (pmsim's own FemState output, uniform fields; the
     raw files are kept as femstate_*.json for the byte-level checkpoint test)
+  * data/sgm/sgm_5d17_ref.json and tests/test_solid_smith_5d17_qua4_axisym.rs (axisymmetric Qua4)
   * tests/test_solid_smith_5d11_qua4_plane_strain_uy.rs (inline expected displacements) and
     src/base/sample_meshes.rs (smith_example_5d11_qua4, smith_example_5d24_hex20 meshes)
 """
@@ -125,6 +126,20 @@ def main(ref):
         np.savez_compressed(os.path.join(HERE, out + ".npz"), coords=coords, cells=conn, kind=np.array(kind),
                             attribute=attr, uu_correct=uu)
         print("wrote", out, coords.shape, conn.shape, uu.shape)
+    # SGM 5.17 axisymmetric Qua4 (9 IP, two layers, point loads): mesh, cell attributes, expected U of
+    # the test, and Smith-Griffiths' own element stiffness matrices, displacements and IP stresses
+    coords, conn, kind = rust_mesh(ref, "smith_example_5d17_qua4")
+    src = open(os.path.join(ref, "src/base/sample_meshes.rs")).read()
+    i = src.index("pub fn smith_example_5d17_qua4()")
+    body = src[i:src.index("\n    }\n", i)]
+    attr = np.array([int(a) for a in re.findall(r"Cell\s*\{\s*id:\s*\d+,\s*attribute:\s*(\d+)", body)])
+    uu = rust_array(os.path.join(ref, "tests", "test_solid_smith_5d17_qua4_axisym.rs"), "uu_correct")
+    sgm = json.load(open(os.path.join(ref, "data/sgm/sgm_5d17_ref.json")))["all"][0]
+    np.savez_compressed(os.path.join(HERE, "smith_5d17_qua4_axisym.npz"), coords=coords, cells=conn,
+                        kind=np.array(kind), attribute=attr, uu_correct=uu,
+                        sgm_stiffness=np.array(sgm["stiffness"]), sgm_displacement=np.array(sgm["displacement"]),
+                        sgm_stresses=np.array(sgm["stresses"]))
+    print("wrote smith_5d17_qua4_axisym", coords.shape, conn.shape, uu.shape)
     # SPO 7.5.1 pressurised cylinder (reduced-system method, internal pressure, von Mises)
     spo(ref, "spo_751_pres_cylin_ref.json", "spo_751_pres_cylin.npz", mesh="data/spo/spo_751_pres_cylin_qua4.msh")
 

@@ -162,3 +162,64 @@ def pres_cylin_751():
     # iterations: pmsim's own Newton history of this run (data/log-nonlin-tests.txt, SPO-751 block).
     return dict(mesh=m, params=(210.0, 0.3, 0.0, 0.24), ngauss=4, essential=ess, natural=nat, nsteps=5, golden=g,
                 tol_u=1e-11, tol_s=2e-14, iterations=[2, 5, 6, 5, 9])
+
+
+class MultiMaterialOracle:
+    """The oracle's element calls over a mesh whose cells use several materials: one homogeneous
+    OracleElements per material on its subset of cells (all points kept), summed like the
+    reference's Elements loop over cells (src/fem/elements.rs:132-163)."""
+
+    def __init__(self, mesh, cmat, mats, ngauss=0, axisymmetric=False):
+        import oracle
+        self.groups = []
+        for k, (E, nu) in enumerate(mats):
+            sub = Mesh(mesh.ndim, mesh.coords, mesh.cells[cmat == k], mesh.kind)
+            self.groups.append(oracle.OracleElements(sub, 0, oracle.Params(E, nu, 0.0, 1.0), ngauss=ngauss,
+                                                     axisymmetric=axisymmetric))
+        self.ndof = mesh.ndof
+
+    def _each(self, name, *a):
+        for g in self.groups:
+            getattr(g, name)(*a)
+
+    def initialize(self):
+        self._each("initialize")
+
+    def reset_algorithmic_variables(self):
+        self._each("reset_algorithmic_variables")
+
+    def backup_secondary_values(self):
+        self._each("backup_secondary_values")
+
+    def restore_secondary_values(self):
+        self._each("restore_secondary_values")
+
+    def update_secondary_values(self, ddu):
+        self._each("update_secondary_values", ddu)
+
+    def assemble_f_int(self):
+        return sum(g.assemble_f_int() for g in self.groups)
+
+    def assemble_kk_csr(self):
+        import scipy.sparse as sp
+        k = None
+        for g in self.groups:
+            ip, ix, v = g.assemble_kk_csr()
+            m = sp.csr_matrix((v, ix, ip), shape=(self.ndof, self.ndof))
+            k = m if k is None else k + m
+        k = k.tocsr()
+        k.sort_indices()
+        return k.indptr, k.indices, k.data
+
+
+def sgm_5d17_axisym():
+    """tests/test_solid_smith_5d17_qua4_axisym.rs: axisymmetric Qua4 (9 IP), two linear-elastic layers
+    (E=100, nu=0.3 on top; E=1000, nu=0.45 below), sides and base on rollers/fixed, point loads Fy on
+    points 0, 3, 6; reduced-system method, one step."""
+    g = load("smith_5d17_qua4_axisym.npz")
+    m = Mesh(2, g["coords"], g["cells"], kind_from_name(str(g["kind"])))
+    ess = (_ess(m.points_where(lambda x, y: abs(x) < TOL), 0, 2) + _ess(m.points_where(lambda x, y: abs(x - 30) < TOL), 0, 2)
+           + _ess(m.points_where(lambda x, y: abs(y + 10) < TOL), 0, 2) + _ess(m.points_where(lambda x, y: abs(y + 10) < TOL), 1, 2))
+    loads = [(2 * 0 + 1, -2.6667), (2 * 3 + 1, -23.3333), (2 * 6 + 1, -24.0)]
+    return dict(mesh=m, mats=[(100.0, 0.3), (1000.0, 0.45)], cmat=(g["attribute"] - 1).astype(np.int32), ngauss=9,
+                essential=ess, loads=loads, golden=g)

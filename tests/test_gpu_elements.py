@@ -175,3 +175,50 @@ def test_femstate_checkpoint_round_trip_on_device():
     for a, b in zip(g.get_state(), h.get_state()):
         assert np.array_equal(a, b)
     assert state_io.export_state(h, u=u, ddu=du, t=t) == text
+
+
+KINDS_2D = [M.TRI3, M.TRI6, M.QUA4, M.QUA8, M.QUA9]
+
+
+@pytest.mark.parametrize("kind", KINDS_2D, ids=[M.KIND_NAMES[k] for k in KINDS_2D])
+def test_axisymmetric_update_and_assemble_matches_oracle(kind):
+    """Axisymmetric idealization (x = radius): weight |J| w r, hoop strain u_r/r, hoop rows of B in
+    F_int and K (src/base/calculate_strain.rs:36-48, gemlab integrators with args.axisymmetric,
+    src/fem/element_solid.rs:128-171), von Mises with plastic and elastic IPs, against the oracle."""
+    from pmsim_b200.elements import Elements, Material
+    m = perturbed_mesh(kind, seed=7, n=GRID[2])
+    m.coords[:, 0] += 0.5  # keep every point off the axis
+    g = Elements(m, Material.von_mises(E, NU, H, Z0), axisymmetric=True)
+    o = oracle.OracleElements(m, 1, oracle.Params(E, NU, H, Z0), sym_tol=-1.0, axisymmetric=True)
+    indptr, indices = g.csr_pattern()
+    g.initialize_internal_values()
+    o.initialize()
+    assert_close(g.assemble_kk(), oracle_csr_values(o, indptr, indices), what="K elastic")
+    ddu = plastic_ddu(m, seed=kind + 40)
+    g.backup_secondary_values()
+    ff = np.zeros(g.ndof)
+    kv = np.zeros(g.nnz)
+    g.update_and_assemble(ddu, ff, kv)
+    o.update_secondary_values(ddu)
+    sig, ivs, el = g.get_state()
+    assert np.array_equal(el, o.elastic), "elastic flags differ"
+    assert 0 < (1 - el.mean()) < 1, "expected a mix of elastic and plastic IPs"
+    assert_close(sig, o.sig, what="sigma")
+    assert_close(ivs, o.ivs, what="[z, lambda]")
+    assert_close(ff, o.assemble_f_int(), what="f_int")
+    assert_close(kv, oracle_csr_values(o, indptr, indices), what="K")
+
+
+def test_sgm_5d17_axisymmetric_on_device():
+    """tests/test_solid_smith_5d17_qua4_axisym.rs on the device elements (two layers, 9 IP, point
+    loads, reduced-system method): the reference test's displacements at its tolerance 1e-9."""
+    import problems
+    from pmsim_b200.elements import Elements, Material
+    from pmsim_b200.solver import SolverImplicit
+    pb = problems.sgm_5d17_axisym()
+    mats = [Material.linear_elastic(E_, nu) for E_, nu in pb["mats"]]
+    el = Elements(pb["mesh"], mats, ngauss=9, cell_material=pb["cmat"], axisymmetric=True)
+    sol = SolverImplicit(el, pb["essential"], loads=pb["loads"], lagrange_mult_method=False, t_fin=1.0)
+    out = {}
+    sol.solve(lambda step, t, u, e: out.setdefault("u", u.copy()))
+    np.testing.assert_allclose(out["u"], pb["golden"]["uu_correct"], rtol=0, atol=1e-9)

@@ -243,3 +243,36 @@ def test_oracle_spo_751_pressurised_cylinder():
     assert worst[0] <= pb["tol_u"], worst
     assert worst[1] <= pb["tol_s"], worst
     assert [len(h) for h in solver.history] == pb["iterations"]
+
+
+def test_oracle_sgm_5d17_axisymmetric_element_matrices():
+    """Axisymmetric K_e (weight |J| w r, hoop row N/r in B) of the six Qua4 cells against the
+    stiffness matrices of Smith & Griffiths' run (data/sgm/sgm_5d17_ref.json; the first equals
+    pmsim's inline kk_e0_ref).  Those printed values carry about 1e-7 relative noise in single
+    entries (12.82051135 where the exact value is 500/39 = 12.82051282...), and the reference's own
+    check of kk_e0_ref used 1e-5; the six matrices agree to 3.4e-8 of their largest entry, and the
+    bar here is 1e-7.  The displacements of the solve are pinned at 1e-9 below."""
+    pb = problems.sgm_5d17_axisym()
+    g, m = pb["golden"], pb["mesh"]
+    for e in range(m.ncell):
+        E, nu = pb["mats"][pb["cmat"][e]]
+        X = m.coords[m.cells[e]].reshape(-1).copy()
+        sig = np.zeros((9, 4))
+        ivs = np.zeros((9, 2))
+        el = np.ones(9, np.uint8)
+        K = oracle.elem_jacobian(m.kind, 9, X, 0, oracle.Params(E, nu, 0.0, 1.0), sig, ivs, el, thickness=-1.0)
+        ref = g["sgm_stiffness"][e]
+        assert np.max(np.abs(K - ref)) <= 1e-7 * np.max(np.abs(ref)), e
+
+
+def test_oracle_sgm_5d17_axisymmetric_solution():
+    """Displacements of tests/test_solid_smith_5d17_qua4_axisym.rs (the reference test's tolerance,
+    1e-9) and Smith & Griffiths' IP stresses (xx, yy, xy, zz printed order) on the axisymmetric
+    oracle."""
+    pb = problems.sgm_5d17_axisym()
+    m, g = pb["mesh"], pb["golden"]
+    el = problems.MultiMaterialOracle(m, pb["cmat"], pb["mats"], ngauss=9, axisymmetric=True)
+    out = {}
+    solver = OracleSolver(el, m.ndof, pb["essential"], loads=pb["loads"], lagrange_mult_method=False, t_fin=1.0)
+    solver.solve(lambda step, t, u, e: out.setdefault("u", u))
+    np.testing.assert_allclose(out["u"], g["uu_correct"], rtol=0, atol=1e-9)
