@@ -276,3 +276,23 @@ def test_oracle_sgm_5d17_axisymmetric_solution():
     solver = OracleSolver(el, m.ndof, pb["essential"], loads=pb["loads"], lagrange_mult_method=False, t_fin=1.0)
     solver.solve(lambda step, t, u, e: out.setdefault("u", u))
     np.testing.assert_allclose(out["u"], g["uu_correct"], rtol=0, atol=1e-9)
+
+
+def test_oracle_sgm_5d17_axisymmetric_distributed_load():
+    """The point loads of SGM 5.17 are a unit pressure on the top side 0 <= r <= 10 integrated with
+    the radius (per radian: int_0^4 (1 - r/4) r dr = 8/3, ...).  The same run driven by that
+    distributed load (Natural with the axisymmetric side integral) gives the test's displacements."""
+    from pmsim_b200.natural import Natural, find_sides
+    pb = problems.sgm_5d17_axisym()
+    m, g = pb["mesh"], pb["golden"]
+    nat = Natural(m, axisymmetric=True).sides(find_sides(m, lambda p: abs(p[1]) < 1e-9, lambda p: p[0] <= 10 + 1e-9),
+                                              -1.0)
+    f = nat.ff_ext(1.0)
+    np.testing.assert_allclose(f[[1, 7, 13]], [-8 / 3, -70 / 3, -24.0], rtol=1e-14)
+    el = problems.MultiMaterialOracle(m, pb["cmat"], pb["mats"], ngauss=9, axisymmetric=True)
+    out = {}
+    solver = OracleSolver(el, m.ndof, pb["essential"], lagrange_mult_method=False, t_fin=1.0, ff_ext_fn=nat.ff_ext)
+    solver.solve(lambda step, t, u, e: out.setdefault("u", u))
+    # the test's point loads are rounded to 4 decimals (-2.6667, -23.3333, i.e. 1.3e-5 relative);
+    # the displacements move by 5.0e-7 of their 0.04 magnitude
+    np.testing.assert_allclose(out["u"], g["uu_correct"], rtol=0, atol=1e-6)
