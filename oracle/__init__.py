@@ -28,6 +28,7 @@ c_int_p = ctypes.POINTER(ctypes.c_int)
 
 MODEL_LINEAR_ELASTIC = 0
 MODEL_VON_MISES = 1
+MODEL_LINEAR_ELASTIC_PLANE_STRESS = 2  # 2D only
 
 
 def build():

@@ -279,14 +279,27 @@ void elastic_modulus(const Params& p, int nc, double* dd) {
     for (int i = 3; i < nc; i++) dd[i * nc + i] = c * (1.0 - 2.0 * p.poisson);
 }
 
-// model: 0 = LinearElastic, 1 = VonMises.  ivs = [z, lambda]. returns 0 ok, else error code
+// Plane-stress Hooke modulus (2D, Mandel xx, yy, zz, xy): c = E/(1-nu^2) on the in-plane normal
+// block, zz row and column zero, shear c(1-nu) = 2G (russell_tensor LinElasticity with plane_stress,
+// used by src/material/linear_elastic.rs:17).
+void elastic_modulus_plane_stress(const Params& p, double* dd) {
+    double c = p.young / (1.0 - p.poisson * p.poisson);
+    for (int i = 0; i < 16; i++) dd[i] = 0;
+    dd[0] = dd[5] = c;
+    dd[1] = dd[4] = c * p.poisson;
+    dd[15] = c * (1.0 - p.poisson);
+}
+
+// model: 0 = LinearElastic, 1 = VonMises, 2 = LinearElastic in plane stress (2D).
+// ivs = [z, lambda]. returns 0 ok, else error code
 //   2: "von Mises plastic update must not lead to zero sigma_d (sigma_d < 1e-10)"
 //   3: "von Mises stiffness cannot be computed with zero deviatoric norm (norm_s < 1e-10)"
 int model_update_stress(int model, const Params& p, int nc, double* sig, double* ivs, uint8_t* elastic,
                         const double* deps) {
     double dd[36];
-    elastic_modulus(p, nc, dd);
-    if (model == 0) {  // src/material/linear_elastic.rs:61-71
+    if (model == 2) elastic_modulus_plane_stress(p, dd);
+    else elastic_modulus(p, nc, dd);
+    if (model == 0 || model == 2) {  // src/material/linear_elastic.rs:61-71
         double ds[6];
         for (int i = 0; i < nc; i++) { ds[i] = 0; for (int j = 0; j < nc; j++) ds[i] += dd[i * nc + j] * deps[j]; }
         for (int i = 0; i < nc; i++) sig[i] += ds[i];
@@ -317,6 +330,7 @@ int model_update_stress(int model, const Params& p, int nc, double* sig, double*
 
 int model_stiffness(int model, const Params& p, int nc, const double* sig, const double* ivs, uint8_t elastic,
                     double* dd) {
+    if (model == 2) { elastic_modulus_plane_stress(p, dd); return 0; }
     if (model == 0 || elastic) { elastic_modulus(p, nc, dd); return 0; }
     // src/material/von_mises.rs:124-167
     double kk, gg;

@@ -18,14 +18,21 @@ enum Err : int { OK = 0, E_INVALID = 1, E_CUDA = 2, E_ZERO_SIGMA_D = 3, E_ZERO_N
 // Material constants in the form the kernels use.
 struct MatConst {
     int model;       // 0 linear elastic, 1 von Mises
+    int plane_stress;  // linear elastic in plane stress (2D): in-plane normal block c(1, nu; nu, 1),
+                       // c = E/(1-nu^2), no out-of-plane stress (russell_tensor LinElasticity)
     double kk, gg;   // bulk and shear moduli: K = E/(3(1-2nu)), G = E/(2(1+nu))
     double hh, z_ini;
     double c11, c12, c44;  // Hooke in Mandel form: c(1-nu), c nu, c(1-2nu) with c = E/((1+nu)(1-2nu))
+    double ps11, ps12;     // plane stress: E/(1-nu^2), E nu/(1-nu^2) (= the effective Lame lambda*)
 };
 
-inline MatConst make_matconst(int model, double young, double poisson, double hh, double z_ini) {
+inline MatConst make_matconst(int model, double young, double poisson, double hh, double z_ini,
+                              bool plane_stress = false) {
     MatConst m;
     m.model = model;
+    m.plane_stress = plane_stress ? 1 : 0;
+    m.ps11 = young / (1.0 - poisson * poisson);
+    m.ps12 = m.ps11 * poisson;
     m.kk = young / (3.0 * (1.0 - 2.0 * poisson));
     m.gg = young / (2.0 * (1.0 + poisson));
     m.hh = hh;
@@ -54,6 +61,12 @@ __device__ __forceinline__ double sigma_d(const double* v) {
 // sigma += D_e : deps  (t4_ddot_t2_update with the Hooke modulus)
 template <int NC>
 __device__ __forceinline__ void hooke_add(const MatConst& m, double* sig, const double* de) {
+    if (NC == 4 && m.plane_stress) {  // sigma_zz stays zero
+        sig[0] += m.ps11 * de[0] + m.ps12 * de[1];
+        sig[1] += m.ps12 * de[0] + m.ps11 * de[1];
+        sig[3 % NC] += m.c44 * de[3 % NC];
+        return;
+    }
     double d0 = m.c11 * de[0] + m.c12 * de[1] + m.c12 * de[2];
     double d1 = m.c12 * de[0] + m.c11 * de[1] + m.c12 * de[2];
     double d2 = m.c12 * de[0] + m.c12 * de[1] + m.c11 * de[2];

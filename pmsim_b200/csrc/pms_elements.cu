@@ -348,7 +348,8 @@ __global__ void __launch_bounds__(WPB * 32, warps_per_cell(NN) == 2 ? 3 : 1) ele
             if (st != OK && err == OK) err = st;
             double* t = TC + p * 10;
             t[0] = coef * 0.5 * a;
-            t[1] = coef * (mc.kk - a / 3.0);
+            // volumetric coefficient: K - a/3 (= Lame lambda when elastic); plane stress: lambda*
+            t[1] = coef * ((ND == 2 && mc.plane_stress) ? mc.ps12 : (mc.kk - a / 3.0));
             t[2] = coef * b;
             t[3] = s[0];
             t[4] = s[1];
@@ -962,8 +963,14 @@ int pms_elements_create(const pms_mesh* mesh, const pms_material* materials, int
     if (!mesh || !materials || nmaterial < 1 || !config || !mesh->coords || !mesh->cells) return PMS_ERR_INVALID;
     int kind = mesh->kind;
     if (kind < 0 || kind > 8 || kind_ndim(kind) != mesh->ndim) return PMS_ERR_INVALID;
-    if (config->plane_stress) return PMS_ERR_UNSUPPORTED;
     if (config->axisymmetric && mesh->ndim != 2) return PMS_ERR_UNSUPPORTED;
+    // plane stress: 2D linear elastic only ("von Mises model does not work in plane-stress",
+    // src/material/von_mises.rs:60-62)
+    if (config->plane_stress) {
+        if (mesh->ndim != 2 || config->axisymmetric) return PMS_ERR_UNSUPPORTED;
+        for (int i = 0; i < nmaterial; i++)
+            if (materials[i].model != PMS_LINEAR_ELASTIC) return PMS_ERR_UNSUPPORTED;
+    }
     if (mesh->npoint < 1 || mesh->ncell < 1) return PMS_ERR_INVALID;
     auto* h = new pms_elements();
     h->kind = kind;
@@ -986,7 +993,7 @@ int pms_elements_create(const pms_mesh* mesh, const pms_material* materials, int
         const pms_material& m = materials[i];
         if (m.model != PMS_LINEAR_ELASTIC && m.model != PMS_VON_MISES) { delete h; return PMS_ERR_INVALID; }
         if (m.model == PMS_VON_MISES && !(m.z_ini > F_TOL)) { delete h; return PMS_ERR_INVALID; }
-        h->mats.push_back(make_matconst(m.model, m.young, m.poisson, m.hh, m.z_ini));
+        h->mats.push_back(make_matconst(m.model, m.young, m.poisson, m.hh, m.z_ini, config->plane_stress != 0));
     }
     if (mesh->cell_material) {
         for (int64_t c = 0; c < h->ncell; c++)

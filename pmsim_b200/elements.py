@@ -39,7 +39,7 @@ class Material:
 
 class Elements:
     def __init__(self, mesh: Mesh, materials, ngauss: int = 0, thickness: float = 1.0, cell_material=None,
-                 axisymmetric: bool = False):
+                 axisymmetric: bool = False, plane_stress: bool = False):
         self.L = _lib.load()
         if isinstance(materials, Material):
             materials = [materials]
@@ -51,7 +51,7 @@ class Elements:
             self._cm = np.ascontiguousarray(cell_material, dtype=np.int32)
         cmesh = _lib.Mesh_(mesh.ndim, mesh.kind, mesh.npoint, mesh.ncell, _lib.ptr(mesh.coords), _lib.ptr(mesh.cells),
                            _lib.ptr(self._cm))
-        cfg = _lib.Config_(int(ngauss), 0, 1 if axisymmetric else 0, float(thickness))
+        cfg = _lib.Config_(int(ngauss), 1 if plane_stress else 0, 1 if axisymmetric else 0, float(thickness))
         h = ctypes.c_void_p()
         rc = self.L.pms_elements_create(ctypes.byref(cmesh), mats, len(materials), ctypes.byref(cfg), ctypes.byref(h))
         if rc != _lib.PMS_OK:

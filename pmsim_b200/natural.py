@@ -103,11 +103,12 @@ def find_sides(mesh: M.Mesh, on_locus, filt=None):
     return out
 
 
-def side_forces(mesh: M.Mesh, sides, component=None, axisymmetric=False):
+def side_forces(mesh: M.Mesh, sides, component=None, axisymmetric=False, thickness=1.0):
     """Consistent nodal forces of a unit load on the sides: component=None -> unit outward normal
     pressure (qn = 1), else unit traction along axis `component`.  In the axisymmetric idealization
     (2D, x = radius) the side integral carries the radius, f_m = int N_m q r dl (per radian), as the
-    element integrals do."""
+    element integrals do; otherwise a 2D side integral carries the thickness (args.alpha in
+    src/fem/bc_distributed.rs:139-165)."""
     nd = mesh.ndim
     f = np.zeros(mesh.ndof)
     for c, k in sides:
@@ -127,6 +128,8 @@ def side_forces(mesh: M.Mesh, sides, component=None, axisymmetric=False):
                 q = normal if component is None else np.eye(2)[component] * np.linalg.norm(t)
                 if axisymmetric:
                     q = q * (N @ X[:, 0])
+                elif thickness != 1.0:
+                    q = q * thickness
                 for m in range(n):
                     f[nd * pts[m]: nd * pts[m] + nd] += ws * N[m] * q
         else:
@@ -145,15 +148,17 @@ def side_forces(mesh: M.Mesh, sides, component=None, axisymmetric=False):
 class Natural:
     """Loads as (unit force vector, value, f(t) or None); ff_ext(t) = sum value * f(t) * unit."""
 
-    def __init__(self, mesh: M.Mesh, axisymmetric=False):
+    def __init__(self, mesh: M.Mesh, axisymmetric=False, thickness=1.0):
         self.mesh = mesh
         self.axisymmetric = bool(axisymmetric)
+        self.thickness = float(thickness)
         if self.axisymmetric and mesh.ndim != 2:
             raise ValueError("the axisymmetric idealization is two-dimensional")
         self.items = []
 
     def sides(self, sides, value, fn=None, component=None):
-        self.items.append((side_forces(self.mesh, sides, component, self.axisymmetric), float(value), fn))
+        self.items.append((side_forces(self.mesh, sides, component, self.axisymmetric, self.thickness), float(value),
+                           fn))
         return self
 
     def points(self, point_ids, dof, value, fn=None):

@@ -13,6 +13,7 @@ Sources (paths inside the pmsim project):
   * data/results/artificial/*.json, *.msh  (pmsim's own FemState output, uniform fields; the
     raw files are kept as femstate_*.json for the byte-level checkpoint test)
   * data/sgm/sgm_5d17_ref.json and tests/test_solid_smith_5d17_qua4_axisym.rs (axisymmetric Qua4)
+  * tests/test_solid_bhatti_1d6_plane_stress.rs and the bhatti_example_1d6_bracket mesh (plane stress)
   * tests/test_solid_smith_5d11_qua4_plane_strain_uy.rs (inline expected displacements) and
     src/base/sample_meshes.rs (smith_example_5d11_qua4, smith_example_5d24_hex20 meshes)
 """
@@ -140,6 +141,12 @@ def main(ref):
                         sgm_stiffness=np.array(sgm["stiffness"]), sgm_displacement=np.array(sgm["displacement"]),
                         sgm_stresses=np.array(sgm["stresses"]))
     print("wrote smith_5d17_qua4_axisym", coords.shape, conn.shape, uu.shape)
+    # Bhatti 1.6 bracket in plane stress (Tri3, thickness 0.25, linear elastic)
+    coords, conn, kind = rust_mesh(ref, "bhatti_example_1d6_bracket")
+    uu = rust_array(os.path.join(ref, "tests", "test_solid_bhatti_1d6_plane_stress.rs"), "uu_correct")
+    np.savez_compressed(os.path.join(HERE, "bhatti_1d6_plane_stress.npz"), coords=coords, cells=conn,
+                        kind=np.array(kind), uu_correct=uu)
+    print("wrote bhatti_1d6_plane_stress", coords.shape, conn.shape, uu.shape)
     # SPO 7.5.1 pressurised cylinder (reduced-system method, internal pressure, von Mises)
     spo(ref, "spo_751_pres_cylin_ref.json", "spo_751_pres_cylin.npz", mesh="data/spo/spo_751_pres_cylin_qua4.msh")
 

@@ -223,3 +223,15 @@ def sgm_5d17_axisym():
     loads = [(2 * 0 + 1, -2.6667), (2 * 3 + 1, -23.3333), (2 * 6 + 1, -24.0)]
     return dict(mesh=m, mats=[(100.0, 0.3), (1000.0, 0.45)], cmat=(g["attribute"] - 1).astype(np.int32), ngauss=9,
                 essential=ess, loads=loads, golden=g)
+
+
+def bhatti_1d6_plane_stress():
+    """tests/test_solid_bhatti_1d6_plane_stress.rs: Tri3 bracket in plane stress (thickness 0.25),
+    linear elastic E=1e4, nu=0.2, points 0 and 1 fixed, Qn = -20 on the top sides (1,3) and (3,5)."""
+    from pmsim_b200.natural import Natural, find_sides
+    g = load("bhatti_1d6_plane_stress.npz")
+    m = Mesh(2, g["coords"], g["cells"], kind_from_name(str(g["kind"])))
+    ess = [(2 * p + d, 0.0, None) for p in (0, 1) for d in range(2)]
+    top = find_sides(m, lambda p: abs(p[1] - (2.0 - p[0] / 4.0)) < TOL)
+    nat = Natural(m, thickness=0.25).sides(top, -20.0)
+    return dict(mesh=m, young=1e4, poisson=0.2, thickness=0.25, essential=ess, natural=nat, golden=g, nsides=len(top))

@@ -76,3 +76,21 @@ def test_invalid_arguments_are_rejected_without_gpu():
     cells[0, 0] = 100  # point out of range
     cm = _lib.Mesh_(2, M.QUA4, m.npoint, 1, _lib.ptr(m.coords), _lib.ptr(cells), None)
     assert L.pms_mesh_csr_pattern(ctypes.byref(cm), None, None, None) == 1
+
+
+def test_unsupported_idealizations_are_rejected_without_gpu():
+    """Plane stress with von Mises is refused as the reference refuses it ("von Mises model does not
+    work in plane-stress", src/material/von_mises.rs:60-62), and so are 3D axisymmetric or plane-stress
+    configurations; these checks come before any device work."""
+    L = _lib.load()
+    m = M.structured_2d(M.QUA4, 1, 1)
+    cm = _lib.Mesh_(2, M.QUA4, m.npoint, m.ncell, _lib.ptr(m.coords), _lib.ptr(m.cells), None)
+    vm = _lib.material(_lib.VON_MISES, 1e4, 0.3, 0.0, 9.0)
+    h = ctypes.c_void_p()
+    assert L.pms_elements_create(ctypes.byref(cm), ctypes.byref(vm), 1, ctypes.byref(_lib.Config_(0, 1, 0, 1.0)),
+                                 ctypes.byref(h)) == 7
+    m3 = M.structured_3d(M.HEX8, 1, 1, 1)
+    cm3 = _lib.Mesh_(3, M.HEX8, m3.npoint, m3.ncell, _lib.ptr(m3.coords), _lib.ptr(m3.cells), None)
+    le = _lib.material(_lib.LINEAR_ELASTIC, 1e4, 0.3, 0.0, 1.0)
+    for cfg in (_lib.Config_(0, 1, 0, 1.0), _lib.Config_(0, 0, 1, 1.0)):
+        assert L.pms_elements_create(ctypes.byref(cm3), ctypes.byref(le), 1, ctypes.byref(cfg), ctypes.byref(h)) == 7

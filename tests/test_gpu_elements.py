@@ -222,3 +222,42 @@ def test_sgm_5d17_axisymmetric_on_device():
     out = {}
     sol.solve(lambda step, t, u, e: out.setdefault("u", u.copy()))
     np.testing.assert_allclose(out["u"], pb["golden"]["uu_correct"], rtol=0, atol=1e-9)
+
+
+@pytest.mark.parametrize("kind", KINDS_2D, ids=[M.KIND_NAMES[k] for k in KINDS_2D])
+def test_plane_stress_update_and_assemble_matches_oracle(kind):
+    """Plane stress (linear elastic; in-plane normal block E/(1-nu^2) (1, nu; nu, 1), no sigma_zz) with
+    thickness 0.25, against the oracle."""
+    from pmsim_b200.elements import Elements, Material
+    m = perturbed_mesh(kind, seed=9, n=GRID[2])
+    g = Elements(m, Material.linear_elastic(E, NU), thickness=0.25, plane_stress=True)
+    o = oracle.OracleElements(m, oracle.MODEL_LINEAR_ELASTIC_PLANE_STRESS, oracle.Params(E, NU, 0.0, 1.0), thickness=0.25)
+    indptr, indices = g.csr_pattern()
+    g.initialize_internal_values()
+    o.initialize()
+    ddu = plastic_ddu(m, seed=kind + 60)
+    g.backup_secondary_values()
+    ff = np.zeros(g.ndof)
+    kv = np.zeros(g.nnz)
+    g.update_and_assemble(ddu, ff, kv)
+    o.update_secondary_values(ddu)
+    sig = g.get_state()[0]
+    assert np.all(sig[:, 2] == 0.0), "plane stress keeps sigma_zz = 0"
+    assert_close(sig, o.sig, what="sigma")
+    assert_close(ff, o.assemble_f_int(), what="f_int")
+    assert_close(kv, oracle_csr_values(o, indptr, indices), what="K")
+
+
+def test_bhatti_1d6_plane_stress_on_device():
+    """tests/test_solid_bhatti_1d6_plane_stress.rs on the device elements: the reference test's
+    displacements (its tolerance is 1e-15; the device sums in another order, so 1e-14 here)."""
+    import problems
+    from pmsim_b200.elements import Elements, Material
+    from pmsim_b200.solver import SolverImplicit
+    pb = problems.bhatti_1d6_plane_stress()
+    el = Elements(pb["mesh"], Material.linear_elastic(pb["young"], pb["poisson"]), thickness=pb["thickness"],
+                  plane_stress=True)
+    sol = SolverImplicit(el, pb["essential"], lagrange_mult_method=False, t_fin=1.0, natural=pb["natural"])
+    out = {}
+    sol.solve(lambda step, t, u, e: out.setdefault("u", u.copy()))
+    np.testing.assert_allclose(out["u"], pb["golden"]["uu_correct"], rtol=0, atol=1e-14)

@@ -296,3 +296,17 @@ def test_oracle_sgm_5d17_axisymmetric_distributed_load():
     # the test's point loads are rounded to 4 decimals (-2.6667, -23.3333, i.e. 1.3e-5 relative);
     # the displacements move by 5.0e-7 of their 0.04 magnitude
     np.testing.assert_allclose(out["u"], g["uu_correct"], rtol=0, atol=1e-6)
+
+
+def test_oracle_bhatti_1d6_plane_stress():
+    """Plane stress (linear elastic, thickness 0.25, pressure on two sides) against the displacements
+    of tests/test_solid_bhatti_1d6_plane_stress.rs at the reference test's tolerance, 1e-15."""
+    pb = problems.bhatti_1d6_plane_stress()
+    m = pb["mesh"]
+    assert pb["nsides"] == 2
+    el = oracle.OracleElements(m, oracle.MODEL_LINEAR_ELASTIC_PLANE_STRESS, oracle.Params(pb["young"], pb["poisson"], 0.0, 1.0),
+                               thickness=pb["thickness"])
+    out = {}
+    solver = OracleSolver(el, m.ndof, pb["essential"], lagrange_mult_method=False, t_fin=1.0, ff_ext_fn=pb["natural"].ff_ext)
+    solver.solve(lambda step, t, u, e: out.setdefault("u", u))
+    np.testing.assert_allclose(out["u"], pb["golden"]["uu_correct"], rtol=0, atol=1e-15)
