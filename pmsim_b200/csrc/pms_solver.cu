@@ -45,7 +45,6 @@ namespace {
 
 constexpr unsigned FULL = 0xffffffffu;
 constexpr int CHN = 128;        // nodes per reduction chunk (= threads per block of the node kernels)
-constexpr int WIDE_SPMV_THREADS = 512;
 
 struct SolverArgs {
     int nd;
@@ -63,61 +62,50 @@ struct SolverArgs {
 };
 
 // ---- canonical reductions ----------------------------------------------------------------
-// Reduces the 128 values of a thread group (threads [128g, 128g + 128) of the block) by the fixed
-// pairing (t, t+s), s = 64, 32, ..., 1 (the last five levels by warp shuffles, which pair the same
-// operands).  Every block-level PCG and Newton reduction goes through here.  All threads of the
-// block must call it; sh holds blockDim.x doubles.
+// A 128-node chunk is summed as four 32-node quarters, each by the warp shuffle tree (pairs t, t+16,
+// t+8, ..., t+1), and the quarters as ((q0 + q1) + (q2 + q3)).  Every block-level PCG and Newton
+// reduction goes through here (threads [128g, 128g + 128) of a block form group g and hold the
+// chunk's nodes in order), and a kernel that gives each quarter its own block reproduces the same
+// value; so a problem's dot products do not depend on the engine that computes them.
+template <bool MAX>
+__device__ __forceinline__ double warp_tree(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const double w = __shfl_down_sync(FULL, v, o);
+        v = MAX ? fmax(v, w) : v + w;
+    }
+    return v;  // lane 0 holds the quarter's value
+}
+
+template <bool MAX>
+__device__ __forceinline__ double quarters(double q0, double q1, double q2, double q3) {
+    return MAX ? fmax(fmax(q0, q1), fmax(q2, q3)) : (q0 + q1) + (q2 + q3);
+}
+
+// All threads of the block must call it; sh holds at least 4 doubles per group.
 template <bool MAX>
 __device__ __forceinline__ double group_reduce(double v, double* sh) {
-    const int t = threadIdx.x & (CHN - 1);
-    double* s = sh + (threadIdx.x & ~(CHN - 1));
-    s[t] = v;
+    const double w = warp_tree<MAX>(v);
+    double* s = sh + 4 * (threadIdx.x / CHN);
+    if ((threadIdx.x & 31) == 0) s[(threadIdx.x & (CHN - 1)) >> 5] = w;
     __syncthreads();
-    if (t < 64) s[t] = MAX ? fmax(s[t], s[t + 64]) : s[t] + s[t + 64];
-    __syncthreads();
-    if (t < 32) {
-        double r = MAX ? fmax(s[t], s[t + 32]) : s[t] + s[t + 32];
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-            const double w = __shfl_down_sync(FULL, r, o);
-            r = MAX ? fmax(r, w) : r + w;
-        }
-        if (t == 0) s[0] = r;
-    }
-    __syncthreads();
-    const double r = s[0];
+    const double r = quarters<MAX>(s[0], s[1], s[2], s[3]);
     __syncthreads();
     return r;
 }
 
-// Two sums at once (same trees as two group_reduce<false> calls); sh holds 2*blockDim.x doubles.
+// Two sums at once (same trees as two group_reduce<false> calls); sh holds 8 doubles per group.
 __device__ __forceinline__ void group_reduce2(double& a, double& b, double* sh) {
-    const int t = threadIdx.x & (CHN - 1);
-    double* s = sh + 2 * (threadIdx.x & ~(CHN - 1));
-    double* u = s + CHN;
-    s[t] = a;
-    u[t] = b;
-    __syncthreads();
-    if (t < 64) {
-        s[t] = s[t] + s[t + 64];
-        u[t] = u[t] + u[t + 64];
+    const double wa = warp_tree<false>(a), wb = warp_tree<false>(b);
+    double* s = sh + 8 * (threadIdx.x / CHN);
+    if ((threadIdx.x & 31) == 0) {
+        const int k = (threadIdx.x & (CHN - 1)) >> 5;
+        s[k] = wa;
+        s[4 + k] = wb;
     }
     __syncthreads();
-    if (t < 32) {
-        double x = s[t] + s[t + 32], y = u[t] + u[t + 32];
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-            x = x + __shfl_down_sync(FULL, x, o);
-            y = y + __shfl_down_sync(FULL, y, o);
-        }
-        if (t == 0) {
-            s[0] = x;
-            u[0] = y;
-        }
-    }
-    __syncthreads();
-    a = s[0];
-    b = u[0];
+    a = quarters<false>(s[0], s[1], s[2], s[3]);
+    b = quarters<false>(s[4], s[5], s[6], s[7]);
     __syncthreads();
 }
 
@@ -127,6 +115,14 @@ __device__ __forceinline__ void group_reduce2(double& a, double& b, double* sh) 
 __device__ __forceinline__ double problem_total(const double* part, int64_t c0, int64_t c1, double* sh) {
     double s = 0.0;
     for (int64_t c = c0 + (threadIdx.x & (CHN - 1)); c < c1; c += CHN) s += part[c];
+    return group_reduce<false>(s, sh);
+}
+
+// The same total from quarter partials (four per chunk, in chunk order).
+__device__ __forceinline__ double problem_total_quarters(const double* part4, int64_t c0, int64_t c1, double* sh) {
+    double s = 0.0;
+    for (int64_t c = c0 + (threadIdx.x & (CHN - 1)); c < c1; c += CHN)
+        s += quarters<false>(part4[4 * c], part4[4 * c + 1], part4[4 * c + 2], part4[4 * c + 3]);
     return group_reduce<false>(s, sh);
 }
 
@@ -437,32 +433,40 @@ pcg_init_scalars_kernel(int np, const uint8_t* active, const uint8_t* engine, co
 
 // ---- batch-wide PCG engine (one CUDA graph node per kernel) --------------------------------
 
-// q = K p on the rows of one chunk (TPR lanes per row, all threads of the block over the chunk's
-// rows), then the chunk's partial of p.q
+// q = K p on the rows of one chunk quarter (32 nodes; one pass of TPR lanes x 4 rows per lane group),
+// then the quarter's partial of p.q by the warp tree.  Block b covers quarter b % 4 of chunk b / 4.
 template <int TPR>
-__global__ void __launch_bounds__(WIDE_SPMV_THREADS)
+__host__ __device__ constexpr int quarter_threads() { return 32 * (TPR == 8 ? 2 : 3) * TPR / 4; }
+
+template <int TPR>
+__global__ void __launch_bounds__(quarter_threads<TPR>())
 pcg_spmv_dot_kernel(SolverArgs S, int par, const int64_t* __restrict__ indptr, const int32_t* __restrict__ indices,
-                    const double* __restrict__ val, const double* p, double* q, double* part) {
-    __shared__ double sh[WIDE_SPMV_THREADS];
-    const int64_t ch = blockIdx.x;
+                    const double* __restrict__ val, const double* p, double* q, double* part4) {
+    constexpr int QB = quarter_threads<TPR>();
+    const int64_t ch = blockIdx.x >> 2;
+    const int k = blockIdx.x & 3;
     const int pr = S.chunk_prob[ch];
     if (!S.pcg_active[par * S.np + pr]) return;  // whole block
-    const int64_t node0 = S.chunk_node0[ch];
-    const int nn = S.chunk_nnode[ch];
-    spmv_rows<WIDE_SPMV_THREADS, TPR, 4>(
-        S.pres_idx, node0 * S.nd, (node0 + nn) * S.nd, indptr, indices, val, [&](int32_t c) { return p[c]; },
-        [&](int64_t row, double v) { q[row] = v; });
+    const int nn = max(0, min(32, S.chunk_nnode[ch] - 32 * k));
+    const int64_t node0 = S.chunk_node0[ch] + 32 * k;
+    if (nn > 0)
+        spmv_rows<QB, TPR, 4>(
+            S.pres_idx, node0 * S.nd, (node0 + nn) * S.nd, indptr, indices, val, [&](int32_t c) { return p[c]; },
+            [&](int64_t row, double v) { q[row] = v; });
     __syncthreads();
-    const int64_t i0 = (node0 + threadIdx.x) * S.nd;
-    const double v = (threadIdx.x < nn) ? node_dot(S.pres_idx + i0, S.nd, p + i0, q + i0) : 0.0;
-    const double t = group_reduce<false>(v, sh);  // group 0 holds the chunk's nodes
-    if (threadIdx.x == 0) part[ch] = t;
+    if (threadIdx.x < 32) {
+        const int64_t i0 = (node0 + threadIdx.x) * S.nd;
+        const double v = (threadIdx.x < nn) ? node_dot(S.pres_idx + i0, S.nd, p + i0, q + i0) : 0.0;
+        const double t = warp_tree<false>(v);
+        if (threadIdx.x == 0) part4[4 * ch + k] = t;
+    }
 }
 
 // alpha = rho / p.q (every block of a problem sums the same partials in the same order), then
 // x, r, z and the chunk's partials of r.z and r.r
 __global__ void __launch_bounds__(CHN)
-pcg_update_kernel(SolverArgs S, int par, const double* part_pq, const double* rho, const double* p, const double* q,
+pcg_update_kernel(SolverArgs S, int par, const double* part_pq /*4 per chunk*/, const double* rho, const double* p,
+                  const double* q,
                   const double* binv, double* x, double* r, double* z, double* part_rz, double* part_rr,
                   int32_t* nactive) {
     __shared__ double sh[2 * CHN];
@@ -470,7 +474,7 @@ pcg_update_kernel(SolverArgs S, int par, const double* part_pq, const double* rh
     const int64_t ch = blockIdx.x;
     const int pr = S.chunk_prob[ch];
     if (!S.pcg_active[par * S.np + pr]) return;  // whole block
-    const double pq = problem_total(part_pq, S.pchunk[pr], S.pchunk[pr + 1], sh);
+    const double pq = problem_total_quarters(part_pq, S.pchunk[pr], S.pchunk[pr + 1], sh);
     const double alpha = (pq != 0.0) ? rho[par * S.np + pr] / pq : 0.0;
     double rz = 0.0, r2 = 0.0;
     if (threadIdx.x < S.chunk_nnode[ch]) {
@@ -923,6 +927,7 @@ int ensure_graph(pms_batch* b) {
     if (cudaGraphCreate(&g, 0) != cudaSuccess) return bfail(b, PMS_ERR_CUDA, "graph creation failed");
     const unsigned nch = (unsigned)b->nchunk;
     void* spmv = tpr_of(b->v.nd) == 8 ? (void*)pcg_spmv_dot_kernel<8> : (void*)pcg_spmv_dot_kernel<16>;
+    const unsigned qthreads = tpr_of(b->v.nd) == 8 ? quarter_threads<8>() : quarter_threads<16>();
     cudaGraphNode_t prev = nullptr;
     bool ok = true;
     for (int i = 0; i < gi && ok; i++) {
@@ -937,7 +942,7 @@ int ensure_graph(pms_batch* b) {
         void* a3[] = {&b->S, &par, &b->d_part_a, &b->d_part_b, &b->d_rho, &b->d_r0, &rtol, &max_iter,
                       &b->d_iters, &b->d_z, &b->d_p, &b->d_nactive};
         cudaGraphNode_t n1, n2, n3;
-        ok = add_kernel_node(g, &n1, prev, spmv, nch, WIDE_SPMV_THREADS, a1) == cudaSuccess &&
+        ok = add_kernel_node(g, &n1, prev, spmv, 4 * nch, qthreads, a1) == cudaSuccess &&
              add_kernel_node(g, &n2, n1, (void*)pcg_update_kernel, nch, CHN, a2) == cudaSuccess &&
              add_kernel_node(g, &n3, n2, (void*)pcg_beta_direction_kernel, nch, CHN, a3) == cudaSuccess;
         prev = n3;
@@ -1233,7 +1238,7 @@ int pms_batch_create(pms_elements* el, int32_t nproblem, const int64_t* point_pt
               b->alloc(&b->d_q, n) && b->alloc(&b->d_x, n) && b->alloc(&b->d_binv, (size_t)b->nnode * nd * nd) &&
               b->alloc(&b->d_lam, npres) && b->alloc(&b->d_c, npres) && b->alloc(&b->d_mdl, npres) &&
               b->alloc(&b->d_mdl0, npres) && b->alloc(&b->d_part_a, b->nchunk) &&
-              b->alloc(&b->d_part_b, b->nchunk) && b->alloc(&b->d_part_c, b->nchunk) &&
+              b->alloc(&b->d_part_b, b->nchunk) && b->alloc(&b->d_part_c, 4 * (size_t)b->nchunk) &&
               b->alloc(&b->d_rho, 2 * (size_t)nproblem) && b->alloc(&b->d_r0, nproblem) &&
               b->alloc(&b->d_norm, nproblem) && b->alloc(&b->d_rel, nproblem) &&
               b->alloc(&b->d_iters, 2 * (size_t)nproblem) &&
