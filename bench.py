@@ -52,6 +52,8 @@ def parse():
     ap.add_argument("--served", type=int, default=64, help="requests in the served run (0: skip)")
     ap.add_argument("--rate", type=float, default=200.0, help="Poisson arrival rate of the served run (req/s)")
     ap.add_argument("--no-c0", action="store_true")
+    ap.add_argument("--no-qua8", action="store_true")
+    ap.add_argument("--qua8-n", type=int, default=1024, help="Qua8 mesh of n x n cells for the memory-bound step")
     ap.add_argument("--served-detail", default="", help="write per-request served records (JSON) to this file")
     return ap.parse_args()
 
@@ -234,6 +236,72 @@ def run_k1(torch, stream, steps, warmup):
     bytes_ip = 112 + 233
     return {"ips": n, "ms": ms, "ip_per_s": n / (ms * 1e-3), "gbs": n * bytes_ip / (ms * 1e-3) / 1e9,
             "bytes_per_ip": bytes_ip, "yield_fraction": yielded}
+
+
+def run_qua8_step(torch, stream, steps, warmup, hbm_peak, n=1024):
+    """The fused Newton iteration on a large 2D mesh, where it is memory-bound: n x n Qua8 cells
+    (9 IP) of the footing material (E=1e4, nu=0.3, z0=9, H=0) under a seeded smooth increment that
+    leaves a mix of elastic and plastic IPs.  Reports the element kernel's DRAM bytes per second
+    (its inputs, IP state, F_e and the dense K_e it writes) and the step's algorithmic bytes per
+    second, against the measured HBM peak."""
+    from pmsim_b200 import _lib
+    from pmsim_b200 import mesh as M
+    from pmsim_b200.elements import Elements, Material
+    L = _lib.load()
+    m = M.structured_2d(M.QUA8, n, n, float(n), float(n))
+    x, y = m.coords[:, 0] / n, m.coords[:, 1] / n
+    rng = np.random.default_rng(99)
+    u = np.zeros_like(m.coords)
+    u[:, 0] = 1.5e-3 * n * np.sin(3.0 * x) * np.cos(2.0 * y) / 3.0
+    u[:, 1] = -2.0e-3 * n * y * (1.0 + 0.5 * np.sin(5.0 * x)) / 1.0
+    u += rng.normal(0.0, 1e-4, u.shape)
+    el = Elements(m, Material.von_mises(1e4, 0.3, 0.0, 9.0), ngauss=9)
+    el.set_stream(stream)
+    dev = torch.device("cuda", torch.cuda.current_device())
+    d_ddu = torch.tensor(u.reshape(-1), device=dev)
+    d_ff = torch.empty(el.ndof, device=dev, dtype=torch.float64)
+    d_csr = torch.empty(el.nnz, device=dev, dtype=torch.float64)
+    el.initialize_internal_values()
+    el.backup_secondary_values()
+    for _ in range(warmup):
+        el.update_and_assemble(d_ddu, d_ff, d_csr)
+    el.sync()
+    plastic = float(1.0 - el.get_state()[2].mean())
+    L.pms_elements_set_timing(el.h, 1)
+    L.pms_elements_kernel_times(el.h, None, None)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        el.update_and_assemble(d_ddu, d_ff, d_csr)
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    ms = e0.elapsed_time(e1) / steps
+    kt = np.zeros(3)
+    kc = np.zeros(3, np.int64)
+    L.pms_elements_kernel_times(el.h, _lib.ptr(kt), _lib.ptr(kc))
+    L.pms_elements_set_timing(el.h, 0)
+    ms_el = kt[0] / max(kc[0], 1)
+    ng, nip, ne = 9, m.ncell * 9, 16
+    # element kernel DRAM bytes: node data (coords + dU gathered per cell, conn), IP state read
+    # (backup: sigma 4 + z + lambda + flag) and written (current state), F_e and the dense K_e
+    el_bytes = (m.ncell * (8 * 2 * 8 * 2 + 8 * 4) + nip * (6 * 8 + 1) * 2 + m.ncell * ne * 8
+                + m.ncell * ne * ne * 8)
+    # the fused step's algorithmic bytes in 2D: coordinates, connectivity, dU, IP state read (sigma 4 +
+    # z) and written (sigma 4 + z + lambda + flag), R and the CSR values once
+    step_bytes = (m.npoint * 16 + m.ncell * 8 * 4 + m.ndof * 8 + nip * 40 + nip * 49 + m.ndof * 8
+                  + int(el.nnz) * 8)
+    del d_csr
+    el.close()
+    gbs_el = el_bytes / (ms_el * 1e-3) / 1e9
+    gbs_step = step_bytes / (ms * 1e-3) / 1e9
+    return {"workload": f"qua8 {n}x{n} footing material, 9 IP, one fused Newton iteration", "ncell": m.ncell,
+            "nip": nip, "nnz": int(el.nnz), "plastic_fraction": plastic, "ms_per_step": ms,
+            "kernels_ms_per_step": {"element": ms_el, "f_gather": kt[1] / max(kc[1], 1),
+                                    "kk_gather": kt[2] / max(kc[2], 1)},
+            "element_roofline": {"bound": "hbm", "achieved": gbs_el, "peak": hbm_peak, "unit": "GB/s",
+                                 "frac": gbs_el / hbm_peak, "bytes_per_launch": el_bytes},
+            "step_roofline": {"bound": "hbm", "achieved": gbs_step, "peak": hbm_peak, "unit": "GB/s",
+                              "frac": gbs_step / hbm_peak, "algorithmic_bytes_per_step": step_bytes}}
 
 
 def run_batched(nprob, nalone, seed=2024):
@@ -561,6 +629,11 @@ def main():
         k1["roofline"] = {"bound": "hbm", "achieved": k1["gbs"], "peak": peaks["hbm_gbs"], "unit": "GB/s",
                           "frac": k1["gbs"] / peaks["hbm_gbs"], "peak_source": peaks_kind}
 
+    qua8 = None
+    if not args.no_qua8:
+        torch.cuda.empty_cache()
+        qua8 = run_qua8_step(torch, stream, max(3, min(args.steps, 10)), args.warmup, peaks["hbm_gbs"], n=args.qua8_n)
+
     batched = None
     if args.batched > 0 and args.size == "full":
         torch.cuda.empty_cache()
@@ -613,7 +686,7 @@ def main():
         "kernels_ms_per_step": {"element": ms_elem, "f_gather": kt[1] / max(kc[1], 1),
                                 "kk_gather": kt[2] / max(kc[2], 1)},
         "gpu_launches": int(launches),
-        "e2e": e2e, "cpu_baseline": cpu, "k1_microbench": k1, "batched": batched, "served": served, "c0_footing": c0, "fp64_peak_tflops": fp64,
+        "e2e": e2e, "cpu_baseline": cpu, "k1_microbench": k1, "qua8_step": qua8, "batched": batched, "served": served, "c0_footing": c0, "fp64_peak_tflops": fp64,
         "clocks": clk,
     }
     print(json.dumps(line), flush=True)

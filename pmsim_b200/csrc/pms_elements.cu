@@ -219,13 +219,15 @@ __global__ void __launch_bounds__(WPB * 32, warps_per_cell(NN) == 2 ? 3 : 1) ele
         if constexpr (WPC == 1) __syncwarp();
         else asm volatile("bar.sync %0, %1;" ::"r"(1 + cs), "r"(32 * WPC) : "memory");
     };
-    const int64_t cl = (int64_t)blockIdx.x * CPB + cs;
-    if (cl >= A.ncell) return;  // the cell's warps exit together
+    // persistent: the block's cell slots walk the queue with a stride of the whole grid
+    const int64_t cstride = (int64_t)gridDim.x * CPB;
+    for (int64_t cl = (int64_t)blockIdx.x * CPB + cs; cl < A.ncell; cl += cstride) {
+    cell_sync();  // the previous cell's write-out is done with the cell's shared memory
     const int64_t cell = A.nq ? queue_item(cl, A.nq, A.q_off, A.q_first) : A.cell0 + cl;
     int mode = (UPD == UPD_NONE) ? 0 : 2;
     if (UPD == UPD_MODE) {
         mode = A.pmode[A.cell_prob[cell]];
-        if (mode == 0) return;  // inactive problem: the cell's warps exit together
+        if (mode == 0) continue;  // inactive problem: the cell's warps skip it together
     }
     const bool do_update = (UPD == UPD_MODE) ? (mode == 2) : (UPD != UPD_NONE);
     const bool from_backup = (UPD == UPD_BACKUP) || (UPD == UPD_MODE && mode == 2);
@@ -585,6 +587,7 @@ __global__ void __launch_bounds__(WPB * 32, warps_per_cell(NN) == 2 ? 3 : 1) ele
             for (int t = lane + 32 * half; t < n; t += 32 * WPC) dst[t] = stage[t];
         }
     }
+    }  // cells
 }
 
 // One warp per block row A of K.  Lanes form G = 32/NN groups of NN lanes; lane (g, b) of round r
@@ -819,6 +822,16 @@ int grid_1d(int64_t n) {
     return (int)std::max<int64_t>(b, 1);
 }
 
+// Blocks of a kernel that the GPU holds at once (one wave of the persistent element kernel).
+int64_t resident_blocks(const void* kern, int smem) {
+    int dev = 0, sms = 0, per_sm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, WPB * 32, smem) != cudaSuccess || per_sm < 1)
+        per_sm = 1;
+    return (int64_t)std::max(sms, 1) * per_sm;
+}
+
 template <int ND, int NN, int UPD, bool DOF, bool DOK>
 void launch_elem_t(pms_elements* h, const ElemArgs& a) {
     auto kern = element_kernel<ND, NN, UPD, DOF, DOK>;
@@ -828,6 +841,7 @@ void launch_elem_t(pms_elements* h, const ElemArgs& a) {
         configured = true;
     }
     int64_t blocks = (a.ncell + cells_per_block(NN) - 1) / cells_per_block(NN);
+    blocks = std::min<int64_t>(blocks, resident_blocks((const void*)kern, h->smem_bytes));
     kern<<<(unsigned)blocks, WPB * 32, h->smem_bytes, h->stream>>>(a);
 }
 
