@@ -178,7 +178,7 @@ __host__ __device__ constexpr int smem_bytes_for(int nn, int nd, int ng, int wpb
 }
 
 template <int ND, int NN, int UPD, bool DOF, bool DOK>
-__global__ void __launch_bounds__(WPB * 32, warps_per_cell(NN) == 2 ? 3 : 1) element_kernel(ElemArgs A) {
+__global__ void __launch_bounds__(WPB * 32, warps_per_cell(NN) == 2 ? 3 : (ND == 2 ? 4 : 1)) element_kernel(ElemArgs A) {
     constexpr int NC = 2 * ND;
     constexpr int NE = NN * ND;
     constexpr int GS = NE + 1;  // gradient row stride (odd: spreads the banks of phase-1 stores)
