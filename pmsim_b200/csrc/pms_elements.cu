@@ -590,6 +590,384 @@ __global__ void __launch_bounds__(WPB * 32, warps_per_cell(NN) == 2 ? 3 : (ND ==
     }  // cells
 }
 
+// ------------------------------------------------------------------------------------------------
+// 2D kernel: two cells per warp, one half-warp (16 lanes) per cell.
+//
+// The 2D cells have at most 9 nodes and, in the rules used here, at most 16 integration points,
+// so element_kernel (one warp per cell) keeps most lanes idle.  Here half h of warp w owns cell
+// 2(w-th pair) + h: lane p < ngauss of the half owns integration point p (phase 1, as in
+// element_kernel), lane m < nnode owns node m (F_int), and in phase 2 lane t owns tile t of the
+// upper node-pair triangle (2x2 node pairs for Tri6/Qua8/Qua9, single pairs for Tri3/Qua4).
+// Phase 1 also forms, per integration point and node, h = S g (+ q s_zz e_x) and q = N/r, so
+// phase 2 reads its operands from shared memory with no per-point staging or barrier.  Every
+// entry of K_e and f_e takes the same operations in the same order as in element_kernel, so the
+// two kernels give the same bits.  A half without a cell (odd count, inactive problem) repeats
+// its partner's cell and writes nothing: both halves run the same loop trips, so the warp-wide
+// syncs below are always reached by all 32 lanes.
+constexpr int WPB2 = 4;      // warps per block (two cells each)
+constexpr int NG2_MAX = 16;  // integration points per cell that the half-warp layout holds
+
+template <int NN> struct Tile2 {
+    static constexpr int T = NN * (NN + 1) / 2 > 16 ? 2 : 1;  // tile side in nodes
+    static constexpr int NG = (NN + T - 1) / T;                // node groups
+    static constexpr int NT = NG * (NG + 1) / 2;               // tiles of the upper triangle
+};
+
+// Shared memory (doubles): table dN[m*2+j][16], w[16], N[m][16]; then per cell X[NE], dU[NE],
+// G[ng][NE+2], H[ng][NE+2], Q[ng][NN], TC[ng][4] (alpha, gamma, beta), CS[ng][6]; the cell area
+// also stages K_e (NE x NE) for the write-out.
+__host__ __device__ constexpr int table2_doubles(int nn) { return 2 * nn * 16 + 16 + nn * 16; }
+__host__ __device__ constexpr int cell2_doubles(int nn, int ng) {
+    return ((4 * nn + 2 * ng * (2 * nn + 2) + ng * nn + 10 * ng > 4 * nn * nn
+                 ? 4 * nn + 2 * ng * (2 * nn + 2) + ng * nn + 10 * ng
+                 : 4 * nn * nn) + 1) & ~1;
+}
+__host__ __device__ constexpr int smem2_bytes(int nn, int ng) {
+    return (table2_doubles(nn) + 2 * WPB2 * cell2_doubles(nn, ng)) * 8;
+}
+
+template <int NN, int UPD, bool DOF, bool DOK>
+__global__ void __launch_bounds__(WPB2 * 32, 4) element2d_kernel(ElemArgs A) {
+    constexpr int NE = 2 * NN, GS = NE + 2;
+    using TL = Tile2<NN>;
+    constexpr int T = TL::T;
+    static_assert(TL::NT <= 16, "every node-pair tile needs a lane of the half-warp");
+    extern __shared__ __align__(16) double smem2[];
+    const int ng = A.ngauss;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int hh = lane >> 4, hl = lane & 15;
+    const int cd = cell2_doubles(NN, ng);
+    double* dNs = smem2;          // [m*2+j][16]
+    double* ws = dNs + NE * 16;   // [16]
+    double* Ns = ws + 16;         // [m][16]
+    double* Xs = smem2 + table2_doubles(NN) + (2 * wid + hh) * cd;
+    double* Us = Xs + NE;
+    double* G = Us + NE;       // [p][GS]
+    double* H = G + ng * GS;   // [p][GS]
+    double* Q = H + ng * GS;   // [p][NN]
+    double* TC = Q + ng * NN;  // [p][4]
+    double* CS = TC + ng * 4;  // [p][6]
+
+    for (int i = threadIdx.x; i < ng * NE; i += blockDim.x) {
+        const int p = i / NE, r = i % NE;
+        dNs[r * 16 + p] = A.tab[i];
+    }
+    for (int i = threadIdx.x; i < ng; i += blockDim.x) ws[i] = A.tab[ng * NE + i];
+    if (A.axisym)
+        for (int i = threadIdx.x; i < ng * NN; i += blockDim.x) {
+            const int p = i / NN, m = i % NN;
+            Ns[m * 16 + p] = A.tab[ng * NE + ng + i];
+        }
+    __syncthreads();
+
+    // this lane's tile (ti <= tj), row-major over the upper triangle of node groups
+    int ti = -1, tj = -1;
+    {
+        int k = 0;
+        for (int i = 0; i < TL::NG; i++)
+            for (int j = i; j < TL::NG; j++) {
+                if (k == hl) {
+                    ti = i;
+                    tj = j;
+                }
+                k++;
+            }
+    }
+
+    const int64_t npair = (A.ncell + 1) / 2;
+    for (int64_t pr = (int64_t)blockIdx.x * WPB2 + wid; pr < npair; pr += (int64_t)gridDim.x * WPB2) {
+        __syncwarp();  // the previous pair's write-out is done with the cells' shared memory
+        // every lane looks at both cells of the pair, so the choices below agree across the warp
+        int64_t cellv0 = 0, cellv1 = 0;
+        int mode0 = (UPD == UPD_NONE) ? 0 : 2, mode1 = mode0;
+        bool on0 = 2 * pr < A.ncell, on1 = 2 * pr + 1 < A.ncell;
+        if (on0) cellv0 = A.nq ? queue_item(2 * pr, A.nq, A.q_off, A.q_first) : A.cell0 + 2 * pr;
+        if (on1) cellv1 = A.nq ? queue_item(2 * pr + 1, A.nq, A.q_off, A.q_first) : A.cell0 + 2 * pr + 1;
+        if (UPD == UPD_MODE) {  // cells of inactive problems are left out
+            if (on0) mode0 = A.pmode[A.cell_prob[cellv0]];
+            if (on1) mode1 = A.pmode[A.cell_prob[cellv1]];
+            on0 = on0 && mode0 != 0;
+            on1 = on1 && mode1 != 0;
+        }
+        if (!on0 && !on1) continue;
+        const bool active = hh ? on1 : on0;  // a half without a cell repeats its partner's and writes nothing
+        const bool take1 = hh ? on1 : !on0;
+        const int64_t cell = take1 ? cellv1 : cellv0;
+        const int mode = take1 ? mode1 : mode0;
+        const bool do_update = (UPD == UPD_MODE) ? (mode == 2) : (UPD != UPD_NONE);
+        const bool from_backup = (UPD == UPD_BACKUP) || (UPD == UPD_MODE && mode == 2);
+        const MatConst mc = A.mats[A.cmat ? A.cmat[cell] : 0];
+
+        if (hl < NN) {
+            const int pt = A.conn[cell * NN + hl];
+#pragma unroll
+            for (int i = 0; i < 2; i++) {
+                Xs[hl * 2 + i] = A.coords[(int64_t)pt * 2 + i];
+                Us[hl * 2 + i] = do_update ? A.ddu[(int64_t)pt * 2 + i] : 0.0;
+            }
+        }
+        __syncwarp();
+
+        // ---------------- phase 1: lane p of the half owns integration point p ----------------
+        const int64_t ip0 = cell * ng;
+        int err = OK;
+        const bool has_ip = hl < ng;
+        double sig[4], z = 0.0, lam = 0.0;
+        int el = 1;
+#pragma unroll
+        for (int c = 0; c < 4; c++) sig[c] = 0.0;
+        if (has_ip) {
+            const double* ssrc = from_backup ? A.sig_src : A.sig;
+            const double* zsrc = from_backup ? A.z_src : A.z;
+            const double* lsrc = from_backup ? A.lam_src : A.lam;
+            const uint8_t* esrc = from_backup ? A.el_src : A.el;
+#pragma unroll
+            for (int c = 0; c < 4; c++) sig[c] = ssrc[(int64_t)c * A.nip + ip0 + hl];
+            z = zsrc[ip0 + hl];
+            lam = lsrc[ip0 + hl];
+            el = esrc[ip0 + hl];
+            if (UPD == UPD_MODE && mode == 1) {
+                // reset_algorithmic_variables + backup_secondary_values of a new load step
+                lam = 0.0;
+                if (active) {
+#pragma unroll
+                    for (int c = 0; c < 4; c++) const_cast<double*>(A.sig_src)[(int64_t)c * A.nip + ip0 + hl] = sig[c];
+                    const_cast<double*>(A.z_src)[ip0 + hl] = z;
+                    const_cast<double*>(A.lam_src)[ip0 + hl] = 0.0;
+                    const_cast<uint8_t*>(A.el_src)[ip0 + hl] = (uint8_t)el;
+                    A.lam[ip0 + hl] = 0.0;
+                }
+            }
+            const int p = hl;
+            double J[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+            for (int m = 0; m < NN; m++)
+#pragma unroll
+                for (int i = 0; i < 2; i++)
+#pragma unroll
+                    for (int j = 0; j < 2; j++) J[i * 2 + j] = fma(Xs[m * 2 + i], dNs[(m * 2 + j) * 16 + p], J[i * 2 + j]);
+            double Ji[4];
+            const double det = inv_jacobian<2>(J, Ji);
+            if (!(det > 0.0)) err = E_JACOBIAN;
+            double rad = 1.0;
+            if (A.axisym) {
+                rad = 0.0;
+#pragma unroll
+                for (int m = 0; m < NN; m++) rad += Ns[m * 16 + p] * Xs[m * 2];
+            }
+            const double coef = det * ws[p] * (A.axisym ? rad : A.thickness);
+            double eps[4] = {0.0, 0.0, 0.0, 0.0};
+            double* Gp = G + p * GS;
+#pragma unroll
+            for (int m = 0; m < NN; m++) {
+                double g[2];
+#pragma unroll
+                for (int i = 0; i < 2; i++) {
+                    double v = 0.0;
+#pragma unroll
+                    for (int j = 0; j < 2; j++) v = fma(dNs[(m * 2 + j) * 16 + p], Ji[j * 2 + i], v);
+                    g[i] = v;
+                }
+                Gp[m * 2] = g[0];
+                Gp[m * 2 + 1] = g[1];
+                if (do_update) {
+                    const double* u = Us + m * 2;
+                    eps[0] += u[0] * g[0];
+                    eps[1] += u[1] * g[1];
+                    eps[3] += SQRT2 * ((u[0] * g[1] + u[1] * g[0]) / 2.0);
+                }
+            }
+            if (A.axisym && do_update)  // out-of-plane strain u_r / r (calculate_strain.rs:36-48)
+#pragma unroll
+                for (int m = 0; m < NN; m++) eps[2] += Us[m * 2] * Ns[m * 16 + p] / rad;
+            if (do_update) {
+                const int st = ip_update<4>(mc, mc.hh, sig, z, lam, el, eps);
+                if (st != OK && err == OK) err = st;
+            }
+            if (DOF) {  // coef * sigma: xx, yy, xy, hoop (axisymmetric), and the radius
+                double* c6 = CS + p * 6;
+                c6[0] = coef * sig[0];
+                c6[1] = coef * sig[1];
+                c6[2] = coef * sig[3] * INV_SQRT2;
+                c6[3] = coef * sig[2];
+                c6[4] = rad;
+            }
+            if (DOK) {
+                double a, b, s[4];
+                const int st = tangent_coefs<4>(mc, mc.hh, sig, lam, el, a, b, s);
+                if (st != OK && err == OK) err = st;
+                double* t = TC + p * 4;
+                t[0] = coef * 0.5 * a;
+                // volumetric coefficient: K - a/3 (= Lame lambda when elastic); plane stress: lambda*
+                t[1] = coef * (mc.plane_stress ? mc.ps12 : (mc.kk - a / 3.0));
+                t[2] = coef * b;
+                const bool plastic = t[2] != 0.0;
+                const double s00 = s[0], s11 = s[1], s01 = s[3] * INV_SQRT2, szz = s[2];
+                double* Hp = H + p * GS;
+                double* Qp = Q + p * NN;
+#pragma unroll
+                for (int m = 0; m < NN; m++) {
+                    const double g0 = Gp[m * 2], g1 = Gp[m * 2 + 1];
+                    double q = 0.0;  // N/r of node m (axisymmetric)
+                    if (A.axisym) {
+                        q = Ns[m * 16 + p] / rad;
+                        Qp[m] = q;
+                    }
+                    double h0 = 0.0, h1 = 0.0;  // h = S g (+ q s_zz e_x)
+                    if (plastic) {
+                        h0 = fma(s00, g0, h0);
+                        h0 = fma(s01, g1, h0);
+                        h1 = fma(s01, g0, h1);
+                        h1 = fma(s11, g1, h1);
+                        if (A.axisym) h0 = fma(q, szz, h0);
+                    }
+                    Hp[m * 2] = h0;
+                    Hp[m * 2 + 1] = h1;
+                }
+            }
+        }
+        // first failing IP of each cell (lowest p) reports
+        {
+            const unsigned bad = __ballot_sync(FULL, err != OK);
+            const unsigned mine = (bad >> (16 * hh)) & 0xffffu;
+            const int first = mine ? __ffs(mine) - 1 : 0;
+            const int code = __shfl_sync(FULL, err, 16 * hh + first);
+            if (active && mine && hl == 0) report(A.status, code, cell, first);
+        }
+        if (active && do_update && has_ip) {
+#pragma unroll
+            for (int c = 0; c < 4; c++) A.sig[(int64_t)c * A.nip + ip0 + hl] = sig[c];
+            A.z[ip0 + hl] = z;
+            A.lam[ip0 + hl] = lam;
+            A.el[ip0 + hl] = (uint8_t)el;
+        }
+        __syncwarp();
+
+        // ---------------- F_int: lane m of the half owns node m ----------------
+        if (DOF && hl < NN) {
+            double f[2] = {0.0, 0.0};
+            for (int p = 0; p < ng; p++) {
+                const double* c6 = CS + p * 6;
+                const double* g = G + p * GS + hl * 2;
+                f[0] += c6[0] * g[0] + c6[2] * g[1];
+                f[1] += c6[2] * g[0] + c6[1] * g[1];
+                if (A.axisym) f[0] += c6[3] * Ns[hl * 16 + p] / c6[4];
+            }
+            if (active) {
+                A.fe[(cell * NN + hl) * 2] = f[0];
+                A.fe[(cell * NN + hl) * 2 + 1] = f[1];
+            }
+        }
+
+        // ---------------- phase 2: lane owns a tile of node-pair blocks ----------------
+        if (DOK) {
+            const int a0 = ti * T, b0 = tj * T;
+            double acc[T][T][2][2];
+#pragma unroll
+            for (int r = 0; r < T; r++)
+#pragma unroll
+                for (int c = 0; c < T; c++)
+#pragma unroll
+                    for (int i = 0; i < 2; i++)
+#pragma unroll
+                        for (int j = 0; j < 2; j++) acc[r][c][i][j] = 0.0;
+            if (ti >= 0) {
+                for (int p = 0; p < ng; p++) {
+                    const double* t = TC + p * 4;
+                    const double al = t[0], ga = t[1], be = t[2];
+                    const bool plastic = be != 0.0;
+                    const double* Gp = G + p * GS;
+                    const double* Hp = H + p * GS;
+                    const double* Qp = Q + p * NN;
+                    double Ar[T][2], Cr[T][2], Hr[T][2], Qr[T];
+#pragma unroll
+                    for (int r = 0; r < T; r++) {
+                        const int a = min(a0 + r, NN - 1);
+                        const double g0 = Gp[a * 2], g1 = Gp[a * 2 + 1];
+                        const double q = A.axisym ? Qp[a] : 0.0;
+                        Ar[r][0] = al * g0;
+                        Ar[r][1] = al * g1;
+                        Cr[r][0] = ga * (A.axisym ? g0 + q : g0);
+                        Cr[r][1] = ga * g1;
+                        Hr[r][0] = be * Hp[a * 2];
+                        Hr[r][1] = be * Hp[a * 2 + 1];
+                        Qr[r] = 2.0 * al * q;
+                    }
+#pragma unroll
+                    for (int c = 0; c < T; c++) {
+                        const int b = min(b0 + c, NN - 1);
+                        const double gb[2] = {Gp[b * 2], Gp[b * 2 + 1]};
+                        const double hb[2] = {Hp[b * 2], Hp[b * 2 + 1]};
+                        const double qb = A.axisym ? Qp[b] : 0.0;
+                        const double gc[2] = {A.axisym ? gb[0] + qb : gb[0], gb[1]};
+                        double dot[T];
+#pragma unroll
+                        for (int r = 0; r < T; r++) {
+                            dot[r] = 0.0;
+#pragma unroll
+                            for (int k = 0; k < 2; k++) dot[r] = fma(Ar[r][k], gb[k], dot[r]);
+                        }
+#pragma unroll
+                        for (int r = 0; r < T; r++)
+#pragma unroll
+                            for (int i = 0; i < 2; i++)
+#pragma unroll
+                                for (int j = 0; j < 2; j++) acc[r][c][i][j] = fma(Ar[r][j], gb[i], acc[r][c][i][j]);
+#pragma unroll
+                        for (int r = 0; r < T; r++)
+#pragma unroll
+                            for (int i = 0; i < 2; i++)
+#pragma unroll
+                                for (int j = 0; j < 2; j++) acc[r][c][i][j] = fma(Cr[r][i], gc[j], acc[r][c][i][j]);
+                        if (plastic) {
+#pragma unroll
+                            for (int r = 0; r < T; r++)
+#pragma unroll
+                                for (int i = 0; i < 2; i++)
+#pragma unroll
+                                    for (int j = 0; j < 2; j++) acc[r][c][i][j] = fma(Hr[r][i], hb[j], acc[r][c][i][j]);
+                        }
+#pragma unroll
+                        for (int r = 0; r < T; r++)
+#pragma unroll
+                            for (int i = 0; i < 2; i++) acc[r][c][i][i] += dot[r];
+                        if (A.axisym)  // hoop row: a (N_a/r)(N_b/r) on the radial-radial entry
+#pragma unroll
+                            for (int r = 0; r < T; r++) acc[r][c][0][0] = fma(Qr[r], qb, acc[r][c][0][0]);
+                    }
+                }
+            }
+            __syncwarp();  // both halves are done reading the cell areas that the staging overwrites
+            // stage K_e row-major in the cell area (blocks (a, b) and their mirrors (b, a)), then
+            // copy it out with 16-byte stores, 256 contiguous bytes per half-warp store
+            double* stage = Xs;
+            if (ti >= 0) {
+#pragma unroll
+                for (int r = 0; r < T; r++)
+#pragma unroll
+                    for (int c = 0; c < T; c++) {
+                        const int a = a0 + r, b = b0 + c;
+                        if (a < NN && b < NN && a <= b) {
+#pragma unroll
+                            for (int i = 0; i < 2; i++)
+#pragma unroll
+                                for (int j = 0; j < 2; j++) {
+                                    stage[(a * 2 + i) * NE + b * 2 + j] = acc[r][c][i][j];
+                                    if (a != b) stage[(b * 2 + j) * NE + a * 2 + i] = acc[r][c][i][j];
+                                }
+                        }
+                    }
+            }
+            __syncwarp();
+            if (active) {
+                double2* dst = reinterpret_cast<double2*>(A.ke + cell * (int64_t)(NE * NE));
+                const double2* s2 = reinterpret_cast<const double2*>(stage);
+                for (int t = hl; t < NE * NE / 2; t += 16) dst[t] = s2[t];
+            }
+        }
+    }  // pairs
+}
+
 // One warp per block row A of K.  Lanes form G = 32/NN groups of NN lanes; lane (g, b) of round r
 // loads, for incidence k = k0 + r*G + g of A (cell c, local index a), the ND x ND block (a, b) of
 // c's dense element matrix -- the NN lanes of a group read one contiguous node-row slab -- and
@@ -823,17 +1201,38 @@ int grid_1d(int64_t n) {
 }
 
 // Blocks of a kernel that the GPU holds at once (one wave of the persistent element kernel).
-int64_t resident_blocks(const void* kern, int smem) {
+int64_t resident_blocks(const void* kern, int smem, int threads = WPB * 32) {
     int dev = 0, sms = 0, per_sm = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, WPB * 32, smem) != cudaSuccess || per_sm < 1)
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem) != cudaSuccess || per_sm < 1)
         per_sm = 1;
     return (int64_t)std::max(sms, 1) * per_sm;
 }
 
+// 2D cells with at most 16 integration points: two cells per warp
+template <int NN, int UPD, bool DOF, bool DOK>
+void launch_elem2d_t(const ElemArgs& a, cudaStream_t st, bool persistent) {
+    auto kern = element2d_kernel<NN, UPD, DOF, DOK>;
+    const int smem = smem2_bytes(NN, a.ngauss);
+    static thread_local bool configured = false;
+    if (!configured) {
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem2_bytes(NN, NG2_MAX));
+        configured = true;
+    }
+    int64_t blocks = ((a.ncell + 1) / 2 + WPB2 - 1) / WPB2;
+    if (persistent) blocks = std::min<int64_t>(blocks, resident_blocks((const void*)kern, smem, WPB2 * 32));
+    kern<<<(unsigned)std::max<int64_t>(blocks, 1), WPB2 * 32, smem, st>>>(a);
+}
+
 template <int ND, int NN, int UPD, bool DOF, bool DOK>
 void launch_elem_t(pms_elements* h, const ElemArgs& a) {
+    if constexpr (ND == 2) {
+        if (a.ngauss <= NG2_MAX) {
+            launch_elem2d_t<NN, UPD, DOF, DOK>(a, h->stream, true);
+            return;
+        }
+    }
     auto kern = element_kernel<ND, NN, UPD, DOF, DOK>;
     static thread_local bool configured = false;
     if (!configured) {
@@ -1545,6 +1944,12 @@ NoallocLayout noalloc_layout(int nn, int nd, int ng, int64_t ncell, bool want_f,
 
 template <int ND, int NN, bool DOF, bool DOK>
 void noalloc_launch_t(const ElemArgs& a, int smem, cudaStream_t st) {
+    if constexpr (ND == 2) {
+        if (a.ngauss <= NG2_MAX) {
+            launch_elem2d_t<NN, UPD_NONE, DOF, DOK>(a, st, false);
+            return;
+        }
+    }
     auto kern = element_kernel<ND, NN, UPD_NONE, DOF, DOK>;
     cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
     kern<<<(unsigned)((a.ncell + cells_per_block(NN) - 1) / cells_per_block(NN)), WPB * 32, smem, st>>>(a);
