@@ -968,13 +968,20 @@ __global__ void __launch_bounds__(WPB2 * 32, 4) element2d_kernel(ElemArgs A) {
     }  // pairs
 }
 
-// One warp per block row A of K.  Lanes form G = 32/NN groups of NN lanes; lane (g, b) of round r
-// loads, for incidence k = k0 + r*G + g of A (cell c, local index a), the ND x ND block (a, b) of
-// c's dense element matrix -- the NN lanes of a group read one contiguous node-row slab -- and
-// adds it at column slot[k*NN + b] of the row buffer in shared memory.  The adds go group by group
-// and round by round, i.e. in ascending incidence (= ascending cell) order, so every entry of K is
-// the fixed-order sum over its cells.  The buffer holds the row in CSR order and is written out
-// coalesced.  Rows of problems whose mode is 0 are skipped (per-problem batches).
+// One warp per G = 32/NN consecutive block rows of K (a work-queue range may cut the run); group g
+// of NN lanes owns row A_g.  Lane b of the group loads, for each incidence k of A_g (cell c, local
+// index a), the ND x ND block (a, b) of c's dense element matrix -- the NN lanes read one contiguous
+// node-row slab -- and adds it at column slot[k*NN + b] of the row's buffer in shared memory.  Up
+// to NB incidences are loaded before they are added; the adds go in ascending incidence (= cell)
+// order with a group barrier between incidences, so every entry of K is the fixed-order sum over
+// its cells: bit-identical on every run.  The G buffers lie back to back in CSR order, so when the
+// rows are consecutive the warp writes them out as one contiguous run.  Rows of problems whose mode
+// is 0 are skipped (per-problem batches).
+template <int ND, int NN> struct GatherShape {
+    static constexpr int G = NN >= 32 ? 1 : 32 / NN;  // rows per warp
+    static constexpr int NB = 4;                      // incidences loaded before they are added
+};
+
 template <int ND, int NN>
 __global__ void __launch_bounds__(256) kk_gather_kernel(int64_t npoint, int nbmax, const int64_t* __restrict__ bptr,
                                                         const int64_t* __restrict__ inc_ptr,
@@ -986,60 +993,98 @@ __global__ void __launch_bounds__(256) kk_gather_kernel(int64_t npoint, int nbma
                                                         const int64_t* __restrict__ q_off,
                                                         const int64_t* __restrict__ q_first, int64_t node0) {
     constexpr int NE = NN * ND, BB = ND * ND;
-    constexpr int G = NN >= 32 ? 1 : 32 / NN;          // incidences per round
-    constexpr int NB = G >= 8 ? 1 : (G >= 3 ? 2 : 4);  // rounds loaded before they are added
+    constexpr int G = GatherShape<ND, NN>::G, NB = GatherShape<ND, NN>::NB;
     extern __shared__ double rowbuf[];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, wpb = blockDim.x >> 5;
-    double* buf = rowbuf + (int64_t)wid * nbmax * BB;
+    double* buf = rowbuf + (int64_t)wid * G * nbmax * BB;
     const int g = lane / NN, b = lane - (lane / NN) * NN;
     const bool lane_on = g < G;
+    const unsigned gmask = lane_on ? (((NN >= 32) ? 0xffffffffu : ((1u << NN) - 1u)) << (g * NN)) : (1u << lane);
+    const int64_t ngroup = (npoint + G - 1) / G;
     const int64_t nwarp = (int64_t)gridDim.x * wpb;
-    for (int64_t Ai = (int64_t)blockIdx.x * wpb + wid; Ai < npoint; Ai += nwarp) {
-        const int64_t A = nq ? queue_item(Ai, nq, q_off, q_first) : node0 + Ai;
-        if (pmode && pmode[node_prob[A]] == 0) continue;  // warp-uniform
-        const int64_t ba = bptr[A];
-        const int nba = (int)(bptr[A + 1] - ba);
-        const int nrow = ND * nba;
-        for (int t = lane; t < nba * BB; t += 32) buf[t] = 0.0;
-        const int64_t k0 = inc_ptr[A], k1 = inc_ptr[A + 1];
-        for (int64_t kb = k0; kb < k1; kb += G * NB) {
-            double v[NB][BB];
-            int pos[NB];
+    for (int64_t w = (int64_t)blockIdx.x * wpb + wid; w < ngroup; w += nwarp) {
+        const int64_t Ai = w * G + g;
+        bool on = lane_on && Ai < npoint;
+        int64_t A = 0;
+        if (on) {
+            A = nq ? queue_item(Ai, nq, q_off, q_first) : node0 + Ai;
+            if (pmode && pmode[node_prob[A]] == 0) on = false;
+        }
+        int64_t ba = 0;
+        int nba = 0;
+        if (on) {
+            ba = bptr[A];
+            nba = (int)(bptr[A + 1] - ba);
+        }
+        // buffer offsets of the group rows (exclusive scan over the groups) and the run test
+        int off = 0, total = 0;
+        int nbg[G], offg[G];
+        int64_t bag[G];
 #pragma unroll
-            for (int r = 0; r < NB; r++) {
-                const int64_t k = kb + r * G + g;
-                pos[r] = -1;
-                if (lane_on && k < k1) {
-                    const int32_t code = __ldg(inc + k);
-                    const int64_t cell = code / NN;
-                    const int a = code - (int)cell * NN;
-                    pos[r] = __ldg(slot + k * NN + b);
-                    const double* src = ke + (cell * NE + a * ND) * NE + b * ND;
+        for (int q = 0; q < G; q++) {
+            nbg[q] = __shfl_sync(FULL, nba, q * NN);
+            bag[q] = __shfl_sync(FULL, ba, q * NN);
+            offg[q] = total;
+            if (q < g) off += nbg[q];
+            total += nbg[q];
+        }
+        const int64_t A0 = __shfl_sync(FULL, A, 0);
+        const bool on0 = __shfl_sync(FULL, on, 0);
+        const bool fits = !lane_on || Ai >= npoint || (on && A == A0 + g);
+        const bool run = __all_sync(FULL, fits) && on0;
+        for (int t = lane; t < total * BB; t += 32) buf[t] = 0.0;
+        __syncwarp();
+        if (on) {
+            double* rb = buf + (int64_t)off * BB;
+            const int nrow = ND * nba;
+            const int64_t k0 = inc_ptr[A], k1 = inc_ptr[A + 1];
+            for (int64_t kb = k0; kb < k1; kb += NB) {
+                double v[NB][BB];
+                int pos[NB];
 #pragma unroll
-                    for (int i = 0; i < ND; i++)
-#pragma unroll
-                        for (int j = 0; j < ND; j++) v[r][i * ND + j] = __ldg(src + i * NE + j);
-                } else {
-#pragma unroll
-                    for (int i = 0; i < BB; i++) v[r][i] = 0.0;
-                }
-            }
-#pragma unroll
-            for (int r = 0; r < NB; r++)
-#pragma unroll
-                for (int gg = 0; gg < G; gg++) {
-                    __syncwarp();
-                    if (g == gg && pos[r] >= 0) {
+                for (int r = 0; r < NB; r++) {
+                    const int64_t k = kb + r;
+                    pos[r] = -1;
+                    if (k < k1) {
+                        const int32_t code = __ldg(inc + k);
+                        const int64_t cell = code / NN;
+                        const int a = code - (int)cell * NN;
+                        pos[r] = __ldg(slot + k * NN + b);
+                        const double* src = ke + (cell * NE + a * ND) * NE + b * ND;
 #pragma unroll
                         for (int i = 0; i < ND; i++)
 #pragma unroll
-                            for (int j = 0; j < ND; j++) buf[i * nrow + pos[r] * ND + j] += v[r][i * ND + j];
+                            for (int j = 0; j < ND; j++) v[r][i * ND + j] = __ldg(src + i * NE + j);
+                    } else {
+#pragma unroll
+                        for (int i = 0; i < BB; i++) v[r][i] = 0.0;
                     }
                 }
+#pragma unroll
+                for (int r = 0; r < NB; r++) {
+                    __syncwarp(gmask);  // the group's previous incidence is added
+                    if (pos[r] >= 0) {
+#pragma unroll
+                        for (int i = 0; i < ND; i++)
+#pragma unroll
+                            for (int j = 0; j < ND; j++) rb[i * nrow + pos[r] * ND + j] += v[r][i * ND + j];
+                    }
+                }
+            }
         }
         __syncwarp();
-        double* dst = csr + (int64_t)BB * ba;
-        for (int t = lane; t < nba * BB; t += 32) dst[t] = buf[t];
+        if (run) {
+            double* dst = csr + (int64_t)BB * bag[0];
+            for (int t = lane; t < total * BB; t += 32) dst[t] = buf[t];
+        } else {
+#pragma unroll
+            for (int q = 0; q < G; q++) {
+                if (nbg[q] == 0) continue;  // absent or inactive row (warp-uniform)
+                double* dst = csr + (int64_t)BB * bag[q];
+                const double* s = buf + (int64_t)offg[q] * BB;
+                for (int t = lane; t < nbg[q] * BB; t += 32) dst[t] = s[t];
+            }
+        }
         __syncwarp();
     }
 }
@@ -1329,7 +1374,8 @@ void launch_kk_gather_t(pms_elements* h, double* csr, const int32_t* node_prob, 
     if (h->gather_smem > 48 * 1024)
         cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, h->gather_smem);
     const int64_t np = q ? q->nnode : (nrows >= 0 ? nrows : h->npoint), wpb = h->gather_wpb;
-    const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>((np + wpb - 1) / wpb, 148 * 32));
+    const int64_t nw = (np + GatherShape<ND, NN>::G - 1) / GatherShape<ND, NN>::G;  // warps of rows
+    const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>((nw + wpb - 1) / wpb, 148 * 32));
     kern<<<blocks, (unsigned)(32 * wpb), h->gather_smem, h->stream>>>(
         np, h->pat.nbmax, h->d_bptr, h->d_inc_ptr, h->d_inc, h->d_slot, h->d_ke, csr, node_prob, pmode,
         q ? q->nq : 0, q ? q->node_off : nullptr, q ? q->node_first : nullptr, node0);
@@ -1463,8 +1509,10 @@ int pms_elements_create(const pms_mesh* mesh, const pms_material* materials, int
     h->stream = h->own_stream;
     h->smem_bytes = smem_bytes_for(h->nn, h->nd, h->ng, WPB);
     {
-        // kk_gather: one row buffer (largest block row) per warp, up to 8 warps and 48 KB per block
-        const int64_t row_bytes = (int64_t)std::max(h->pat.nbmax, 1) * h->nd * h->nd * 8;
+        // kk_gather: buffers for G = 32/nnode rows (largest block row each) per warp, up to 8
+        // warps and 48 KB per block
+        const int64_t row_bytes =
+            (int64_t)(h->nn >= 32 ? 1 : 32 / h->nn) * std::max(h->pat.nbmax, 1) * h->nd * h->nd * 8;
         if (row_bytes > 200 * 1024) {
             delete h;
             return PMS_ERR_TOO_LARGE;
