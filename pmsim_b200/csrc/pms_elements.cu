@@ -614,12 +614,14 @@ template <int NN> struct Tile2 {
 };
 
 // Shared memory (doubles): table dN[m*2+j][16], w[16], N[m][16]; then per cell X[NE], dU[NE],
-// G[ng][NE+2], H[ng][NE+2], Q[ng][NN], TC[ng][4] (alpha, gamma, beta), CS[ng][6]; the cell area
+// G[ng][NE+2], H[ng][NE+2], Q[ng][NN] (+1 to an even count), TC[ng][4] (alpha, gamma, beta),
+// CS[ng][6]; the cell area
 // also stages K_e (NE x NE) for the write-out.
 __host__ __device__ constexpr int table2_doubles(int nn) { return 2 * nn * 16 + 16 + nn * 16; }
+// (every array starts on a 16-byte boundary: Q is padded to an even count)
 __host__ __device__ constexpr int cell2_doubles(int nn, int ng) {
-    return ((4 * nn + 2 * ng * (2 * nn + 2) + ng * nn + 10 * ng > 4 * nn * nn
-                 ? 4 * nn + 2 * ng * (2 * nn + 2) + ng * nn + 10 * ng
+    return ((4 * nn + 2 * ng * (2 * nn + 2) + ((ng * nn + 1) & ~1) + 10 * ng > 4 * nn * nn
+                 ? 4 * nn + 2 * ng * (2 * nn + 2) + ((ng * nn + 1) & ~1) + 10 * ng
                  : 4 * nn * nn) + 1) & ~1;
 }
 __host__ __device__ constexpr int smem2_bytes(int nn, int ng) {
@@ -645,7 +647,7 @@ __global__ void __launch_bounds__(WPB2 * 32, 4) element2d_kernel(ElemArgs A) {
     double* G = Us + NE;       // [p][GS]
     double* H = G + ng * GS;   // [p][GS]
     double* Q = H + ng * GS;   // [p][NN]
-    double* TC = Q + ng * NN;  // [p][4]
+    double* TC = Q + ((ng * NN + 1) & ~1);  // [p][4]
     double* CS = TC + ng * 4;  // [p][6]
 
     for (int i = threadIdx.x; i < ng * NE; i += blockDim.x) {
@@ -768,8 +770,7 @@ __global__ void __launch_bounds__(WPB2 * 32, 4) element2d_kernel(ElemArgs A) {
                     for (int j = 0; j < 2; j++) v = fma(dNs[(m * 2 + j) * 16 + p], Ji[j * 2 + i], v);
                     g[i] = v;
                 }
-                Gp[m * 2] = g[0];
-                Gp[m * 2 + 1] = g[1];
+                reinterpret_cast<double2*>(Gp)[m] = make_double2(g[0], g[1]);
                 if (do_update) {
                     const double* u = Us + m * 2;
                     eps[0] += u[0] * g[0];
@@ -807,7 +808,8 @@ __global__ void __launch_bounds__(WPB2 * 32, 4) element2d_kernel(ElemArgs A) {
                 double* Qp = Q + p * NN;
 #pragma unroll
                 for (int m = 0; m < NN; m++) {
-                    const double g0 = Gp[m * 2], g1 = Gp[m * 2 + 1];
+                    const double2 gm = reinterpret_cast<const double2*>(Gp)[m];
+                    const double g0 = gm.x, g1 = gm.y;
                     double q = 0.0;  // N/r of node m (axisymmetric)
                     if (A.axisym) {
                         q = Ns[m * 16 + p] / rad;
@@ -821,8 +823,7 @@ __global__ void __launch_bounds__(WPB2 * 32, 4) element2d_kernel(ElemArgs A) {
                         h1 = fma(s11, g1, h1);
                         if (A.axisym) h0 = fma(q, szz, h0);
                     }
-                    Hp[m * 2] = h0;
-                    Hp[m * 2 + 1] = h1;
+                    reinterpret_cast<double2*>(Hp)[m] = make_double2(h0, h1);
                 }
             }
         }
@@ -873,8 +874,8 @@ __global__ void __launch_bounds__(WPB2 * 32, 4) element2d_kernel(ElemArgs A) {
                         for (int j = 0; j < 2; j++) acc[r][c][i][j] = 0.0;
             if (ti >= 0) {
                 for (int p = 0; p < ng; p++) {
-                    const double* t = TC + p * 4;
-                    const double al = t[0], ga = t[1], be = t[2];
+                    const double2 t01 = reinterpret_cast<const double2*>(TC)[2 * p];
+                    const double al = t01.x, ga = t01.y, be = TC[p * 4 + 2];
                     const bool plastic = be != 0.0;
                     const double* Gp = G + p * GS;
                     const double* Hp = H + p * GS;
@@ -883,21 +884,25 @@ __global__ void __launch_bounds__(WPB2 * 32, 4) element2d_kernel(ElemArgs A) {
 #pragma unroll
                     for (int r = 0; r < T; r++) {
                         const int a = min(a0 + r, NN - 1);
-                        const double g0 = Gp[a * 2], g1 = Gp[a * 2 + 1];
+                        const double2 ga2 = reinterpret_cast<const double2*>(Gp)[a];
+                        const double2 ha2 = reinterpret_cast<const double2*>(Hp)[a];
+                        const double g0 = ga2.x, g1 = ga2.y;
                         const double q = A.axisym ? Qp[a] : 0.0;
                         Ar[r][0] = al * g0;
                         Ar[r][1] = al * g1;
                         Cr[r][0] = ga * (A.axisym ? g0 + q : g0);
                         Cr[r][1] = ga * g1;
-                        Hr[r][0] = be * Hp[a * 2];
-                        Hr[r][1] = be * Hp[a * 2 + 1];
+                        Hr[r][0] = be * ha2.x;
+                        Hr[r][1] = be * ha2.y;
                         Qr[r] = 2.0 * al * q;
                     }
 #pragma unroll
                     for (int c = 0; c < T; c++) {
                         const int b = min(b0 + c, NN - 1);
-                        const double gb[2] = {Gp[b * 2], Gp[b * 2 + 1]};
-                        const double hb[2] = {Hp[b * 2], Hp[b * 2 + 1]};
+                        const double2 gb2 = reinterpret_cast<const double2*>(Gp)[b];
+                        const double2 hb2 = reinterpret_cast<const double2*>(Hp)[b];
+                        const double gb[2] = {gb2.x, gb2.y};
+                        const double hb[2] = {hb2.x, hb2.y};
                         const double qb = A.axisym ? Qp[b] : 0.0;
                         const double gc[2] = {A.axisym ? gb[0] + qb : gb[0], gb[1]};
                         double dot[T];
@@ -983,7 +988,7 @@ template <int ND, int NN> struct GatherShape {
 };
 
 template <int ND, int NN>
-__global__ void __launch_bounds__(256) kk_gather_kernel(int64_t npoint, int nbmax, const int64_t* __restrict__ bptr,
+__global__ void __launch_bounds__(256, ND == 2 ? 4 : 1) kk_gather_kernel(int64_t npoint, int nbmax, const int64_t* __restrict__ bptr,
                                                         const int64_t* __restrict__ inc_ptr,
                                                         const int32_t* __restrict__ inc,
                                                         const int16_t* __restrict__ slot,
@@ -1018,15 +1023,11 @@ __global__ void __launch_bounds__(256) kk_gather_kernel(int64_t npoint, int nbma
         }
         // buffer offsets of the group rows (exclusive scan over the groups) and the run test
         int off = 0, total = 0;
-        int nbg[G], offg[G];
-        int64_t bag[G];
 #pragma unroll
         for (int q = 0; q < G; q++) {
-            nbg[q] = __shfl_sync(FULL, nba, q * NN);
-            bag[q] = __shfl_sync(FULL, ba, q * NN);
-            offg[q] = total;
-            if (q < g) off += nbg[q];
-            total += nbg[q];
+            const int nq_ = __shfl_sync(FULL, nba, q * NN);
+            if (q < g) off += nq_;
+            total += nq_;
         }
         const int64_t A0 = __shfl_sync(FULL, A, 0);
         const bool on0 = __shfl_sync(FULL, on, 0);
@@ -1074,15 +1075,18 @@ __global__ void __launch_bounds__(256) kk_gather_kernel(int64_t npoint, int nbma
         }
         __syncwarp();
         if (run) {
-            double* dst = csr + (int64_t)BB * bag[0];
+            double* dst = csr + (int64_t)BB * __shfl_sync(FULL, ba, 0);
             for (int t = lane; t < total * BB; t += 32) dst[t] = buf[t];
         } else {
-#pragma unroll
+            int oq = 0;
+#pragma unroll 1
             for (int q = 0; q < G; q++) {
-                if (nbg[q] == 0) continue;  // absent or inactive row (warp-uniform)
-                double* dst = csr + (int64_t)BB * bag[q];
-                const double* s = buf + (int64_t)offg[q] * BB;
-                for (int t = lane; t < nbg[q] * BB; t += 32) dst[t] = s[t];
+                const int nq_ = __shfl_sync(FULL, nba, q * NN);
+                const int64_t bq = __shfl_sync(FULL, ba, q * NN);
+                double* dst = csr + (int64_t)BB * bq;  // rows that are absent or inactive have nq_ = 0
+                const double* src = buf + (int64_t)oq * BB;
+                for (int t = lane; t < nq_ * BB; t += 32) dst[t] = src[t];
+                oq += nq_;
             }
         }
         __syncwarp();
