@@ -591,21 +591,22 @@ __global__ void __launch_bounds__(WPB * 32, warps_per_cell(NN) == 2 ? 3 : (ND ==
 }
 
 // ------------------------------------------------------------------------------------------------
-// 2D kernel: two cells per warp, one half-warp (16 lanes) per cell.
+// 2D kernel: several cells per warp, LPC lanes per cell.
 //
 // The 2D cells have at most 9 nodes and, in the rules used here, at most 16 integration points,
-// so element_kernel (one warp per cell) keeps most lanes idle.  Here half h of warp w owns cell
-// 2(w-th pair) + h: lane p < ngauss of the half owns integration point p (phase 1, as in
-// element_kernel), lane m < nnode owns node m (F_int), and in phase 2 lane t owns tile t of the
-// upper node-pair triangle (2x2 node pairs for Tri6/Qua8/Qua9, single pairs for Tri3/Qua4).
+// so element_kernel (one warp per cell) keeps most lanes idle.  Here slot h of a warp owns cell
+// CPW*(group) + h, CPW = 32/LPC: lane p < ngauss of the slot owns integration point p (phase 1, as
+// in element_kernel), lane m < nnode owns node m (F_int), and in phase 2 lane t owns tile t of the
+// upper node-pair triangle (2x2 node pairs for Tri6/Qua8/Qua9, single pairs for Tri3/Qua4).  Qua8
+// with 9 points runs three cells of 10 lanes per warp (30 of 32 lanes hold a tile in phase 2).
 // Phase 1 also forms, per integration point and node, h = S g (+ q s_zz e_x) and q = N/r, so
 // phase 2 reads its operands from shared memory with no per-point staging or barrier.  Every
 // entry of K_e and f_e takes the same operations in the same order as in element_kernel, so the
-// two kernels give the same bits.  A half without a cell (odd count, inactive problem) repeats
-// its partner's cell and writes nothing: both halves run the same loop trips, so the warp-wide
-// syncs below are always reached by all 32 lanes.
-constexpr int WPB2 = 4;      // warps per block (two cells each)
-constexpr int NG2_MAX = 16;  // integration points per cell that the half-warp layout holds
+// kernels give the same bits.  A slot without a cell (ragged end, inactive problem) repeats the
+// group's first cell and writes nothing: all slots run the same loop trips, so the warp-wide syncs
+// below are always reached by all 32 lanes.
+constexpr int WPB2 = 4;      // warps per block
+constexpr int NG2_MAX = 16;  // integration points per cell that the 2D layouts hold
 
 template <int NN> struct Tile2 {
     static constexpr int T = NN * (NN + 1) / 2 > 16 ? 2 : 1;  // tile side in nodes
@@ -624,25 +625,37 @@ __host__ __device__ constexpr int cell2_doubles(int nn, int ng) {
                  ? 4 * nn + 2 * ng * (2 * nn + 2) + ((ng * nn + 1) & ~1) + 10 * ng
                  : 4 * nn * nn) + 1) & ~1;
 }
-__host__ __device__ constexpr int smem2_bytes(int nn, int ng) {
-    return (table2_doubles(nn) + 2 * WPB2 * cell2_doubles(nn, ng)) * 8;
+__host__ __device__ constexpr int smem2_bytes(int nn, int ng, int cpw) {
+    return (table2_doubles(nn) + cpw * WPB2 * cell2_doubles(nn, ng)) * 8;
 }
 
-template <int NN, int UPD, bool DOF, bool DOK>
+// Lanes per cell of the packed layout: enough for every node, every node-pair tile and (checked at
+// launch) every integration point.  It is used when it packs three or more cells into a warp
+// (Tri3, Tri6, Qua4, Qua8: 3 to 5 cells); otherwise, and for rules with more points than lanes,
+// the kernel runs with 16 lanes (two cells) per warp.
+template <int NN> __host__ __device__ constexpr int lanes_packed() {
+    return Tile2<NN>::NT > NN ? Tile2<NN>::NT : NN;
+}
+template <int NN> __host__ __device__ constexpr bool packed_layout() { return 32 / lanes_packed<NN>() >= 3; }
+
+template <int NN, int LPC, int UPD, bool DOF, bool DOK>
 __global__ void __launch_bounds__(WPB2 * 32, 4) element2d_kernel(ElemArgs A) {
     constexpr int NE = 2 * NN, GS = NE + 2;
+    constexpr int CPW = 32 / LPC;  // cells per warp
     using TL = Tile2<NN>;
     constexpr int T = TL::T;
-    static_assert(TL::NT <= 16, "every node-pair tile needs a lane of the half-warp");
+    static_assert(TL::NT <= LPC && NN <= LPC && LPC <= 16, "every node and node-pair tile needs a lane of the cell");
     extern __shared__ __align__(16) double smem2[];
     const int ng = A.ngauss;
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    const int hh = lane >> 4, hl = lane & 15;
+    // cell slot of the lane in its warp and lane within the cell; the lanes past CPW*LPC join the
+    // last slot with hl >= LPC, so they own no node, point or tile
+    const int hh = min(lane / LPC, CPW - 1), hl = lane - hh * LPC;
     const int cd = cell2_doubles(NN, ng);
     double* dNs = smem2;          // [m*2+j][16]
     double* ws = dNs + NE * 16;   // [16]
     double* Ns = ws + 16;         // [m][16]
-    double* Xs = smem2 + table2_doubles(NN) + (2 * wid + hh) * cd;
+    double* Xs = smem2 + table2_doubles(NN) + (CPW * wid + hh) * cd;
     double* Us = Xs + NE;
     double* G = Us + NE;       // [p][GS]
     double* H = G + ng * GS;   // [p][GS]
@@ -676,26 +689,41 @@ __global__ void __launch_bounds__(WPB2 * 32, 4) element2d_kernel(ElemArgs A) {
             }
     }
 
-    const int64_t npair = (A.ncell + 1) / 2;
-    for (int64_t pr = (int64_t)blockIdx.x * WPB2 + wid; pr < npair; pr += (int64_t)gridDim.x * WPB2) {
-        __syncwarp();  // the previous pair's write-out is done with the cells' shared memory
-        // every lane looks at both cells of the pair, so the choices below agree across the warp
-        int64_t cellv0 = 0, cellv1 = 0;
-        int mode0 = (UPD == UPD_NONE) ? 0 : 2, mode1 = mode0;
-        bool on0 = 2 * pr < A.ncell, on1 = 2 * pr + 1 < A.ncell;
-        if (on0) cellv0 = A.nq ? queue_item(2 * pr, A.nq, A.q_off, A.q_first) : A.cell0 + 2 * pr;
-        if (on1) cellv1 = A.nq ? queue_item(2 * pr + 1, A.nq, A.q_off, A.q_first) : A.cell0 + 2 * pr + 1;
-        if (UPD == UPD_MODE) {  // cells of inactive problems are left out
-            if (on0) mode0 = A.pmode[A.cell_prob[cellv0]];
-            if (on1) mode1 = A.pmode[A.cell_prob[cellv1]];
-            on0 = on0 && mode0 != 0;
-            on1 = on1 && mode1 != 0;
+    const int64_t ngroup = (A.ncell + CPW - 1) / CPW;
+    for (int64_t pr = (int64_t)blockIdx.x * WPB2 + wid; pr < ngroup; pr += (int64_t)gridDim.x * WPB2) {
+        __syncwarp();  // the previous group's write-out is done with the cells' shared memory
+        // every lane looks at all cells of the group, so the choices below agree across the warp;
+        // a slot without a cell repeats the group's first cell and writes nothing
+        bool active = false, any = false;
+        int64_t cell = 0, cell_first = 0;
+        int mode = 0, mode_first = 0;
+#pragma unroll
+        for (int k = 0; k < CPW; k++) {
+            const int64_t cl = (int64_t)CPW * pr + k;
+            bool on = cl < A.ncell;
+            int64_t ck = 0;
+            int mk = (UPD == UPD_NONE) ? 0 : 2;
+            if (on) ck = A.nq ? queue_item(cl, A.nq, A.q_off, A.q_first) : A.cell0 + cl;
+            if (UPD == UPD_MODE && on) {  // cells of inactive problems are left out
+                mk = A.pmode[A.cell_prob[ck]];
+                on = mk != 0;
+            }
+            if (on && !any) {
+                any = true;
+                cell_first = ck;
+                mode_first = mk;
+            }
+            if (k == hh) {
+                active = on;
+                cell = ck;
+                mode = mk;
+            }
         }
-        if (!on0 && !on1) continue;
-        const bool active = hh ? on1 : on0;  // a half without a cell repeats its partner's and writes nothing
-        const bool take1 = hh ? on1 : !on0;
-        const int64_t cell = take1 ? cellv1 : cellv0;
-        const int mode = take1 ? mode1 : mode0;
+        if (!any) continue;
+        if (!active) {
+            cell = cell_first;
+            mode = mode_first;
+        }
         const bool do_update = (UPD == UPD_MODE) ? (mode == 2) : (UPD != UPD_NONE);
         const bool from_backup = (UPD == UPD_BACKUP) || (UPD == UPD_MODE && mode == 2);
         const MatConst mc = A.mats[A.cmat ? A.cmat[cell] : 0];
@@ -830,9 +858,9 @@ __global__ void __launch_bounds__(WPB2 * 32, 4) element2d_kernel(ElemArgs A) {
         // first failing IP of each cell (lowest p) reports
         {
             const unsigned bad = __ballot_sync(FULL, err != OK);
-            const unsigned mine = (bad >> (16 * hh)) & 0xffffu;
+            const unsigned mine = (bad >> (LPC * hh)) & ((1u << LPC) - 1u);
             const int first = mine ? __ffs(mine) - 1 : 0;
-            const int code = __shfl_sync(FULL, err, 16 * hh + first);
+            const int code = __shfl_sync(FULL, err, LPC * hh + first);
             if (active && mine && hl == 0) report(A.status, code, cell, first);
         }
         if (active && do_update && has_ip) {
@@ -944,7 +972,7 @@ __global__ void __launch_bounds__(WPB2 * 32, 4) element2d_kernel(ElemArgs A) {
             }
             __syncwarp();  // both halves are done reading the cell areas that the staging overwrites
             // stage K_e row-major in the cell area (blocks (a, b) and their mirrors (b, a)), then
-            // copy it out with 16-byte stores, 256 contiguous bytes per half-warp store
+            // copy it out with 16-byte stores, LPC*16 contiguous bytes per cell and store
             double* stage = Xs;
             if (ti >= 0) {
 #pragma unroll
@@ -964,10 +992,10 @@ __global__ void __launch_bounds__(WPB2 * 32, 4) element2d_kernel(ElemArgs A) {
                     }
             }
             __syncwarp();
-            if (active) {
+            if (active && hl < LPC) {
                 double2* dst = reinterpret_cast<double2*>(A.ke + cell * (int64_t)(NE * NE));
                 const double2* s2 = reinterpret_cast<const double2*>(stage);
-                for (int t = hl; t < NE * NE / 2; t += 16) dst[t] = s2[t];
+                for (int t = hl; t < NE * NE / 2; t += LPC) dst[t] = s2[t];
             }
         }
     }  // pairs
@@ -1259,19 +1287,32 @@ int64_t resident_blocks(const void* kern, int smem, int threads = WPB * 32) {
     return (int64_t)std::max(sms, 1) * per_sm;
 }
 
-// 2D cells with at most 16 integration points: two cells per warp
-template <int NN, int UPD, bool DOF, bool DOK>
-void launch_elem2d_t(const ElemArgs& a, cudaStream_t st, bool persistent) {
-    auto kern = element2d_kernel<NN, UPD, DOF, DOK>;
-    const int smem = smem2_bytes(NN, a.ngauss);
+// 2D cells with at most 16 integration points: LPC lanes per cell, 32/LPC cells per warp
+template <int NN, int LPC, int UPD, bool DOF, bool DOK>
+void launch_elem2d_lpc(const ElemArgs& a, cudaStream_t st, bool persistent) {
+    constexpr int CPW = 32 / LPC;
+    auto kern = element2d_kernel<NN, LPC, UPD, DOF, DOK>;
+    const int smem = smem2_bytes(NN, a.ngauss, CPW);
     static thread_local bool configured = false;
     if (!configured) {
-        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem2_bytes(NN, NG2_MAX));
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem2_bytes(NN, LPC, CPW));
+        cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
         configured = true;
     }
-    int64_t blocks = ((a.ncell + 1) / 2 + WPB2 - 1) / WPB2;
+    int64_t blocks = ((a.ncell + CPW - 1) / CPW + WPB2 - 1) / WPB2;
     if (persistent) blocks = std::min<int64_t>(blocks, resident_blocks((const void*)kern, smem, WPB2 * 32));
     kern<<<(unsigned)std::max<int64_t>(blocks, 1), WPB2 * 32, smem, st>>>(a);
+}
+
+template <int NN, int UPD, bool DOF, bool DOK>
+void launch_elem2d_t(const ElemArgs& a, cudaStream_t st, bool persistent) {
+    if constexpr (packed_layout<NN>()) {
+        if (a.ngauss <= lanes_packed<NN>()) {
+            launch_elem2d_lpc<NN, lanes_packed<NN>(), UPD, DOF, DOK>(a, st, persistent);
+            return;
+        }
+    }
+    launch_elem2d_lpc<NN, 16, UPD, DOF, DOK>(a, st, persistent);
 }
 
 template <int ND, int NN, int UPD, bool DOF, bool DOK>
