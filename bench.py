@@ -9,7 +9,8 @@ The displacement increment is a seeded synthetic footing indentation of the bloc
 (mid-load), so that plastic and elastic IPs mix.  Metric: IP stress-update+tangent per second.
 
 Also measured in the same run: the stand-alone von Mises batch kernel on 16,777,216 IPs
-(``k1_microbench``), the FP64 FMA peak of the GPU (``fp64_peak``), and the CPU restatement of
+(``k1_microbench``), the general (ODE-based) elastoplastic update on 4,194,304 IPs
+(``ep_microbench``), the FP64 FMA peak of the GPU (``fp64_peak``), and the CPU restatement of
 the reference (oracle port, all host cores) on a bounded sample (``cpu_baseline``).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference] [--size small|medium|full]
@@ -236,6 +237,66 @@ def run_k1(torch, stream, steps, warmup):
     bytes_ip = 112 + 233
     return {"ips": n, "ms": ms, "ip_per_s": n / (ms * 1e-3), "gbs": n * bytes_ip / (ms * 1e-3) / 1e9,
             "bytes_per_ip": bytes_ip, "yield_fraction": yielded}
+
+
+def run_ep(torch, stream, steps, warmup, n=4_194_304, cpu_sample=20_000):
+    """General elastoplastic update (Elastoplastic::update_stress with von Mises: yield-surface
+    crossing + Dormand-Prince 5(4) integration of the elastoplastic rates) on n 3D IPs: half start
+    on the yield surface (random deviatoric direction, random mean stress), half at zero stress;
+    deps ~ N(0, (1.5 z0/(2G))^2) per Mandel component, H = 1e3.  Also times the oracle (C++
+    restatement, one thread) on the first cpu_sample IPs."""
+    import oracle
+    from pmsim_b200.material import EP_CASES, ElastoplasticBatch
+    gg = E / (2 * (1 + NU))
+    g = torch.Generator(device="cuda").manual_seed(4321)
+    sig0 = torch.randn((6, n), generator=g, device="cuda", dtype=torch.float64)
+    mean = sig0[:3].mean(0)
+    dev = sig0.clone()
+    dev[:3] -= mean
+    sd = torch.sqrt(1.5 * (dev * dev).sum(0))
+    sig0 = dev * (Z0 / sd)
+    sig0[:3] += torch.randn(n, generator=g, device="cuda", dtype=torch.float64) * 50.0
+    sig0[:, n // 2:] = 0.0
+    deps = torch.randn((6, n), generator=g, device="cuda", dtype=torch.float64) * (1.5 * Z0 / (2 * gg))
+    sig = torch.empty_like(sig0)
+    z = torch.empty(n, device="cuda", dtype=torch.float64)
+    el = torch.zeros(n, device="cuda", dtype=torch.uint8)
+    cases = torch.empty(n, device="cuda", dtype=torch.int32)
+    nst = torch.empty(n, device="cuda", dtype=torch.int32)
+    status = torch.zeros(4, device="cuda", dtype=torch.int32)
+    ep = ElastoplasticBatch(E, NU, 1e3, Z0, ndim=3)
+    times = []
+    with torch.cuda.stream(stream):
+        for i in range(warmup + steps):
+            sig.copy_(sig0)
+            z.fill_(Z0)
+            status.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            ep.update_stress(sig, z, el, deps, cases, nst, status, stream=stream)
+            e1.record(stream)
+            if i >= warmup:
+                times.append((e0, e1))
+    torch.cuda.synchronize()
+    ms = statistics.mean(a.elapsed_time(b) for a, b in times)
+    cnt = torch.bincount((cases + 1).long(), minlength=6).cpu().tolist()
+    mix = {"failed": cnt[0] / n, **{c: cnt[k + 1] / n for k, c in enumerate(EP_CASES)}}
+    ok = cases >= 0
+    mean_steps = float(nst[ok & (el == 0)].double().mean().item())
+    # oracle on a sample, one thread
+    m = cpu_sample
+    osig = sig0[:, :m].T.contiguous().cpu().numpy().copy()
+    odeps = deps[:, :m].T.contiguous().cpu().numpy().copy()
+    oz = np.full(m, Z0)
+    oel = np.zeros(m, dtype=np.uint8)
+    t0 = time.perf_counter()
+    oracle.ep_update(oracle.Params(E, NU, 1e3, Z0), 3, osig, oz, oel, odeps)
+    t_cpu = time.perf_counter() - t0
+    return {"ips": n, "ms": ms, "ip_per_s": n / (ms * 1e-3), "case_fraction": mix,
+            "mean_ode_steps_plastic": mean_steps, "tol_rel": 1e-10,
+            "cpu_oracle_1thread_ip_per_s": m / t_cpu, "cpu_sample_ips": m,
+            "workload": "3D, half on the yield surface (random direction), half at zero stress, "
+                        "deps ~ N(0, (1.5 z0/2G)^2), E=2e5, nu=0.3, z0=250, H=1e3"}
 
 
 def run_qua8_step(torch, stream, steps, warmup, hbm_peak, n=1024):
@@ -622,10 +683,12 @@ def main():
     peaks, peaks_kind = measured_peaks()
     fp64 = fp64_peak(torch, L, stream)
     k1 = None
+    ep = None
     if not args.no_k1 and args.size == "full":
         del d_csr
         torch.cuda.empty_cache()
         k1 = run_k1(torch, stream, max(3, args.steps), args.warmup)
+        ep = run_ep(torch, stream, 3, args.warmup)
         k1["roofline"] = {"bound": "hbm", "achieved": k1["gbs"], "peak": peaks["hbm_gbs"], "unit": "GB/s",
                           "frac": k1["gbs"] / peaks["hbm_gbs"], "peak_source": peaks_kind}
 
@@ -686,7 +749,7 @@ def main():
         "kernels_ms_per_step": {"element": ms_elem, "f_gather": kt[1] / max(kc[1], 1),
                                 "kk_gather": kt[2] / max(kc[2], 1)},
         "gpu_launches": int(launches),
-        "e2e": e2e, "cpu_baseline": cpu, "k1_microbench": k1, "qua8_step": qua8, "batched": batched, "served": served, "c0_footing": c0, "fp64_peak_tflops": fp64,
+        "e2e": e2e, "cpu_baseline": cpu, "k1_microbench": k1, "ep_microbench": ep, "qua8_step": qua8, "batched": batched, "served": served, "c0_footing": c0, "fp64_peak_tflops": fp64,
         "clocks": clk,
     }
     print(json.dumps(line), flush=True)

@@ -33,7 +33,13 @@ enum pms_status_code {
     PMS_ERR_JACOBIAN = 5,     /* non-positive Jacobian determinant at an IP (gemlab calc_gradient) */
     PMS_ERR_NOMEM = 6,        /* device allocation failed */
     PMS_ERR_UNSUPPORTED = 7,  /* idealization/kind not implemented (plane stress, axisymmetric) */
-    PMS_ERR_TOO_LARGE = 8     /* batch does not fit the fixed scratch of pms_element_calc_noalloc */
+    PMS_ERR_TOO_LARGE = 8,    /* batch does not fit the fixed scratch of pms_element_calc_noalloc */
+    PMS_ERR_DF_DSIGMA = 9,    /* "cannot compute df/dsigma due to singularity" (von_mises.rs:254-260) */
+    PMS_ERR_NUMERATOR = 10,   /* "plastic numerator (df/dsigma : De : deps) is overly negative"
+                                 (elastoplastic.rs:193-195) */
+    PMS_ERR_ODE = 11,         /* the elastoplastic ODE took more than max_steps steps */
+    PMS_ERR_INTERSECTION = 12 /* no crossing found although the trial point lies outside the yield
+                                 surface (the reference asserts, elastoplastic.rs:484) */
 };
 
 /* ---- element kinds (gemlab GeoKind subset used by solids) ---------------------------------- */
@@ -258,6 +264,29 @@ int pms_vm_stiffness_batch(const pms_material* mat, int32_t ndim, int64_t n, con
 int pms_vm_update_and_stiffness_host(const pms_material* mat, int32_t ndim, int64_t n, double* sig, double* z,
                                      double* lambda, uint8_t* elastic, const double* deps, const double* hh,
                                      double* dd);
+
+/* ---- general elastoplastic update (Elastoplastic::update_stress over n IPs) ----------------
+ * Replaces Elastoplastic::update_stress (src/material/elastoplastic.rs:539-641) with the von Mises
+ * plasticity model (src/material/von_mises.rs:229-282), the only model Elastoplastic accepts:
+ * yield-surface intersection along the elastic path, then the ODE dsigma/dt = Dep : deps,
+ * dz/dt = Lambda_d H integrated from the crossing to the end of the increment.  mat->model must be
+ * PMS_VON_MISES (else PMS_ERR_INVALID); mat->hh is the hardening H.  Device buffers as in
+ * pms_vm_update_and_stiffness_batch: sig[ncomp*n], z[n], elastic[n] in/out, deps[ncomp*n] in.
+ * cases[n] (nullable) receives the case of each IP (pms_ep_case; -1 where the IP failed) and
+ * steps[n] (nullable) the ODE steps taken (accepted and rejected).  On an error the IP's state is
+ * left as it was and status {code, ip_lo, ip_hi, 0} names the first failing IP.  No tangent: the
+ * reference's Elastoplastic::stiffness is not implemented either (elastoplastic.rs:528-537). */
+typedef struct pms_ep_settings {
+    double tol_rel;     /* relative tolerance of the ODE error control (default 1e-10) */
+    double tol_abs;     /* absolute tolerance (default 1e-10) */
+    double h_ini;       /* first trial step in pseudo-time, clipped to the interval (default 1) */
+    int32_t max_steps;  /* step limit per IP (default 1000); beyond it PMS_ERR_ODE */
+    int32_t pad_;
+} pms_ep_settings;
+enum pms_ep_case { PMS_EP_AE = 0, PMS_EP_AXB = 1, PMS_EP_BE = 2, PMS_EP_BXP = 3, PMS_EP_BP = 4 };
+int pms_ep_update_stress_batch(const pms_material* mat, int32_t ndim, int64_t n, double* sig, double* z,
+                               uint8_t* elastic, const double* deps, const pms_ep_settings* settings,
+                               int32_t* cases, int32_t* steps, int32_t* status, void* stream);
 
 /* Measures the FP64 FMA pipe: blocks x 256 threads, 8 independent FMA chains of `iters` each
  * (16*iters FLOP per thread); out[blocks*256] receives the chain sums.  Used as the FP64 peak. */

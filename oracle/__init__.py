@@ -65,6 +65,10 @@ def lib():
         L.orc_coo_to_csr.argtypes = [ctypes.c_int64, ctypes.c_int64, c_int64_p, c_int64_p, c_double_p, c_int64_p,
                                      c_int64_p, c_double_p]
         L.orc_coo_to_csr.restype = ctypes.c_int64
+        L.orc_ep_update_batch.argtypes = [c_double_p, ctypes.c_int, ctypes.c_int64, c_double_p, c_double_p,
+                                          c_uint8_p, c_double_p, c_double_p, ctypes.c_int,
+                                          ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int32),
+                                          c_int64_p]
         L.orc_update_secondary.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_double, c_double_p, ctypes.c_int64,
                                            c_int64_p, ctypes.c_int, c_double_p, c_double_p, c_double_p, c_double_p,
                                            c_uint8_p, ctypes.c_int, c_int64_p, c_int_p]
@@ -130,6 +134,26 @@ def model_batch(model, params, ndim, sig, ivs, elastic, deps, with_tangent=True,
     if st:
         raise RuntimeError(f"material batch error {st}")
     return dd
+
+
+EP_CASES = ("AE", "AXB", "BE", "BXP", "BP")
+
+
+def ep_update(params, ndim, sig, z, elastic, deps, tol_rel=1e-10, tol_abs=1e-10, h_ini=1.0, max_steps=1000):
+    """General elastoplastic update (Elastoplastic::update_stress with the von Mises model) of n
+    IPs in place: sig (n, nc), z (n), elastic (n, uint8), deps (n, nc).  Returns (code, cases,
+    steps, first failing IP or -1)."""
+    n = sig.shape[0]
+    cases = np.zeros(n, dtype=np.int32)
+    steps = np.zeros(n, dtype=np.int32)
+    bad = np.array([-1], dtype=np.int64)
+    st = lib().orc_ep_update_batch(_dp(params.arr), ndim, n, _dp(sig), _dp(z), _p(elastic, c_uint8_p),
+                                   _dp(np.ascontiguousarray(deps, dtype=np.float64)),
+                                   _dp(np.array([tol_rel, tol_abs, h_ini], dtype=np.float64)), max_steps,
+                                   cases.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)),
+                                   steps.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)),
+                                   bad.ctypes.data_as(c_int64_p))
+    return st, cases, steps, int(bad[0])
 
 
 def elem_f_int(kind, ngauss, X, sig, thickness=1.0):

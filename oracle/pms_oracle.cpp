@@ -556,6 +556,225 @@ void gather_X(const ElemCtx& c, const double* coords, const int64_t* conn, int64
 
 }  // namespace
 
+// ------------------------------------------------------------------ general elastoplasticity
+// Elastoplastic::update_stress (src/material/elastoplastic.rs:376-641) with the von Mises
+// plasticity model (src/material/von_mises.rs:229-282), restated with dense Mandel matrices:
+// D_e from elastic_modulus, D_ep = D_e - (D_e n)(n D_e)/N_p formed as a matrix
+// (t4_ddot_t2_dyad_t2_ddot_t4), dsigma/dt = D_ep deps.  Intersection finding brackets the
+// crossings of f(t) = sigma_d(sigma0 + t D_e deps) - z on the two monotone pieces of the convex f
+// and refines them by bisection (the reference interpolates f with a Chebyshev series and finds
+// its roots).
+// The ODE is integrated with the Dormand-Prince 5(4) pair and the standard step controller (the
+// reference uses DoPri8 from russell_ode, which is not available here).
+// Returns 0, or 9 (df/dsigma singular), 10 (negative plastic numerator), 11 (ODE step limit),
+// 12 (no crossing although the trial point is outside).  case: 0 AE, 1 AXB, 2 BE, 3 BXP, 4 BP.
+namespace ep {
+
+const double NUMERATOR_TOL = 1e-8;    // elastoplastic.rs:17
+const double PSEUDO_TIME_TOL = 1e-7;  // elastoplastic.rs:23
+
+double sigma_d_of(int nc, const double* v) {
+    double m = (v[0] + v[1] + v[2]) / 3.0, q = 0;
+    for (int i = 0; i < 3; i++) q += (v[i] - m) * (v[i] - m);
+    for (int i = 3; i < nc; i++) q += v[i] * v[i];
+    return std::sqrt(1.5 * q);
+}
+
+// f along the elastic path with z frozen
+double f_path(int nc, const double* s0, const double* dse, double z, double t) {
+    double v[6];
+    for (int i = 0; i < nc; i++) v[i] = s0[i] + t * dse[i];
+    return sigma_d_of(nc, v) - z;
+}
+
+// roots of f_path in [0, 1].  sigma_d is a norm of an affine function of t, so f is convex: it
+// has at most one root on each side of its minimiser t_v.  Each monotone piece [0, t_v], [t_v, 1]
+// is checked for a sign change and refined by bisection.
+int roots(int nc, const double* s0, const double* dse, double z, double* r) {
+    double m0 = (s0[0] + s0[1] + s0[2]) / 3.0, md = (dse[0] + dse[1] + dse[2]) / 3.0, sd = 0, dd = 0;
+    for (int i = 0; i < nc; i++) {
+        double a = (i < 3) ? s0[i] - m0 : s0[i], b = (i < 3) ? dse[i] - md : dse[i];
+        sd += a * b;
+        dd += b * b;
+    }
+    double tv = dd > 0 ? std::min(1.0, std::max(0.0, -sd / dd)) : 0.0;
+    double cuts[3] = {0.0, tv, 1.0};
+    int k = 0;
+    for (int piece = 0; piece < 2; piece++) {
+        double lo = cuts[piece], hi = cuts[piece + 1];
+        if (!(hi > lo)) continue;
+        double flo = f_path(nc, s0, dse, z, lo), fhi = f_path(nc, s0, dse, z, hi);
+        bool change = (flo < 0.0) != (fhi < 0.0);
+        if (piece == 0 && lo == 0.0 && flo == 0.0 && fhi < 0.0) {  // starts exactly on the surface
+            r[k++] = 0.0;
+            continue;
+        }
+        if (!change) continue;
+        for (int it = 0; it < 200 && hi - lo > 1e-17; it++) {
+            double mid = 0.5 * (lo + hi), fm = f_path(nc, s0, dse, z, mid);
+            if ((fm < 0.0) == (flo < 0.0)) { lo = mid; flo = fm; } else hi = mid;
+        }
+        r[k++] = 0.5 * (lo + hi);
+    }
+    return k;
+}
+
+// dy/dt of y = [sigma, z] (elastoplastic.rs:159-205)
+int rates(const Params& p, int nc, const double* De, const double* y, const double* deps, double* dy) {
+    double m = (y[0] + y[1] + y[2]) / 3.0, s[6];
+    for (int i = 0; i < nc; i++) s[i] = (i < 3) ? y[i] - m : y[i];
+    double sd = sigma_d_of(nc, y);
+    if (!(sd > 1e-10)) return 9;  // deriv1_invariant_sigma_d fails at sigma_d = 0
+    double n[6], Den[6], nDe[6];
+    for (int i = 0; i < nc; i++) n[i] = 1.5 * s[i] / sd;  // df/dsigma
+    for (int i = 0; i < nc; i++) {
+        Den[i] = 0; nDe[i] = 0;
+        for (int j = 0; j < nc; j++) { Den[i] += De[i * nc + j] * n[j]; nDe[i] += n[j] * De[j * nc + i]; }
+    }
+    double mp = -(-1.0) * p.hh;  // M_p = -(df/dz) H_yf
+    double nn = 0;
+    for (int i = 0; i < nc; i++) nn += n[i] * Den[i];
+    double np = mp + nn;
+    double Dep[36];
+    for (int i = 0; i < nc; i++)
+        for (int j = 0; j < nc; j++) Dep[i * nc + j] = De[i * nc + j] - Den[i] * nDe[j] / np;
+    double numerator = 0;
+    for (int i = 0; i < nc; i++) numerator += nDe[i] * deps[i];
+    for (int i = 0; i < nc; i++) {
+        dy[i] = 0;
+        for (int j = 0; j < nc; j++) dy[i] += Dep[i * nc + j] * deps[j];
+    }
+    if (numerator < -NUMERATOR_TOL) return 10;
+    double lam_d = std::max(0.0, numerator) / np;
+    dy[nc] = lam_d * p.hh;
+    return 0;
+}
+
+int integrate(const Params& p, int nc, const double* De, double t0, double* y, const double* deps,
+              double rtol, double atol, double h_ini, int max_steps, int* nstep) {
+    static const double c_a[7][6] = {
+        {0, 0, 0, 0, 0, 0},
+        {1.0 / 5.0, 0, 0, 0, 0, 0},
+        {3.0 / 40.0, 9.0 / 40.0, 0, 0, 0, 0},
+        {44.0 / 45.0, -56.0 / 15.0, 32.0 / 9.0, 0, 0, 0},
+        {19372.0 / 6561.0, -25360.0 / 2187.0, 64448.0 / 6561.0, -212.0 / 729.0, 0, 0},
+        {9017.0 / 3168.0, -355.0 / 33.0, 46732.0 / 5247.0, 49.0 / 176.0, -5103.0 / 18656.0, 0},
+        {35.0 / 384.0, 0, 500.0 / 1113.0, 125.0 / 192.0, -2187.0 / 6784.0, 11.0 / 84.0}};
+    static const double c_e[7] = {71.0 / 57600.0, 0, -71.0 / 16695.0, 71.0 / 1920.0, -17253.0 / 339200.0,
+                                  22.0 / 525.0, -1.0 / 40.0};
+    const int D = nc + 1;
+    double k[7][7], yt[7], y5[7];
+    double t = t0, h = std::min(h_ini, 1.0 - t0);
+    int rc = rates(p, nc, De, y, deps, k[0]);
+    if (rc) return rc;
+    bool rejected = false;
+    int steps = 0;
+    while (t < 1.0) {
+        if (steps >= max_steps) { *nstep = steps; return 11; }
+        steps++;
+        bool last = t + h >= 1.0;
+        if (last) h = 1.0 - t;
+        for (int st = 1; st < 7; st++) {
+            for (int i = 0; i < D; i++) {
+                double acc = 0;
+                for (int j = 0; j < st; j++) acc += c_a[st][j] * k[j][i];
+                yt[i] = y[i] + h * acc;
+            }
+            if (st == 6) for (int i = 0; i < D; i++) y5[i] = yt[i];
+            rc = rates(p, nc, De, yt, deps, k[st]);
+            if (rc) { *nstep = steps; return rc; }
+        }
+        double err = 0;
+        for (int i = 0; i < D; i++) {
+            double ei = 0;
+            for (int j = 0; j < 7; j++) ei += c_e[j] * k[j][i];
+            ei *= h;
+            double sc = atol + rtol * std::max(std::fabs(y[i]), std::fabs(y5[i]));
+            err += (ei / sc) * (ei / sc);
+        }
+        err = std::sqrt(err / D);
+        double fac = err > 0 ? 0.9 * std::pow(err, -0.2) : 10.0;
+        if (err <= 1.0) {
+            t = last ? 1.0 : t + h;
+            for (int i = 0; i < D; i++) { y[i] = y5[i]; k[0][i] = k[6][i]; }
+            fac = std::min(rejected ? 1.0 : 10.0, std::max(0.2, fac));
+            rejected = false;
+        } else {
+            fac = std::min(1.0, std::max(0.2, fac));
+            rejected = true;
+        }
+        h *= fac;
+    }
+    *nstep = steps;
+    return 0;
+}
+
+int update(const Params& p, int nc, double* sig, double* z, uint8_t* elastic, const double* deps, double rtol,
+           double atol, double h_ini, int max_steps, int* cs, int* nstep) {
+    double De[36], dse[6];
+    elastic_modulus(p, nc, De);
+    for (int i = 0; i < nc; i++) {
+        dse[i] = 0;
+        for (int j = 0; j < nc; j++) dse[i] += De[i * nc + j] * deps[j];
+    }
+    *nstep = 0;
+    const double f0 = sigma_d_of(nc, sig) - *z;  // yield_function (von_mises.rs:236-240)
+    double r[2], t_int = 0;
+    int c;
+    if (f0 < 0.0) {  // select_case: A (elastoplastic.rs:442-470)
+        int nr = roots(nc, sig, dse, *z, r);
+        if (nr == 0) {
+            if (f_path(nc, sig, dse, *z, 1.0) > 0.0) return 12;
+            c = 0;
+        } else {
+            t_int = r[0];
+            c = (t_int <= PSEUDO_TIME_TOL) ? 4 : (t_int >= 1.0 - PSEUDO_TIME_TOL) ? 0 : 1;
+        }
+    } else {  // B (elastoplastic.rs:471-498); going_inside (:379-389)
+        double sd = f0 + *z, indicator = 0;
+        if (!(sd > 1e-10)) return 9;
+        double m = (sig[0] + sig[1] + sig[2]) / 3.0, md = (dse[0] + dse[1] + dse[2]) / 3.0, nn = 0, dd = 0;
+        for (int i = 0; i < nc; i++) {
+            double ni = 1.5 * ((i < 3) ? sig[i] - m : sig[i]) / sd, di = (i < 3) ? dse[i] - md : dse[i];
+            indicator += ni * dse[i];
+            nn += ni * ni;
+            dd += di * di;
+        }
+        // tangential loading (indicator zero up to rounding) does not count as going inside
+        if (indicator < -1e-10 * std::sqrt(nn * dd)) {
+            // the start (on or just outside the surface) gives the first crossing; a second one is
+            // where the path leaves the surface again (elastoplastic.rs:420-427)
+            int nr = roots(nc, sig, dse, *z, r);
+            if (nr == 2) {
+                t_int = r[1];
+                c = (t_int <= PSEUDO_TIME_TOL) ? 4 : (t_int >= 1.0 - PSEUDO_TIME_TOL) ? 2 : 3;
+            } else {
+                if (f_path(nc, sig, dse, *z, 1.0) > 0.0) return 12;
+                c = 2;
+            }
+        } else {
+            c = 4;
+        }
+    }
+    *cs = c;
+    if (c == 0 || c == 2) {
+        for (int i = 0; i < nc; i++) sig[i] += dse[i];
+        *elastic = 1;
+        return 0;
+    }
+    double y[7], t0 = (c == 4) ? 0.0 : t_int;
+    for (int i = 0; i < nc; i++) y[i] = sig[i] + t0 * dse[i];
+    y[nc] = *z;
+    int rc = integrate(p, nc, De, t0, y, deps, rtol, atol, h_ini, max_steps, nstep);
+    if (rc) return rc;
+    for (int i = 0; i < nc; i++) sig[i] = y[i];
+    *z = y[nc];
+    *elastic = 0;
+    return 0;
+}
+
+}  // namespace ep
+
 extern "C" {
 
 int orc_default_ngauss(int kind) { return default_ngauss(kind); }
@@ -762,6 +981,34 @@ int orc_update_secondary(int kind, int ngauss, double thickness, const double* c
     (void)nthreads;
     if (bad_cell) *bad_cell = bc;
     if (bad_ip) *bad_ip = bi;
+    return err;
+}
+
+// General elastoplastic update over n IPs (AoS: sig n*nc, z n, elastic n, deps n*nc);
+// settings = [rtol, atol, h_ini]; cases/steps per IP.  Returns the first error code (its IP in *bad).
+int orc_ep_update_batch(const double* prm, int ndim, int64_t n, double* sig, double* z, uint8_t* elastic,
+                        const double* deps, const double* settings, int max_steps, int32_t* cases, int32_t* steps,
+                        int64_t* bad) {
+    Params p{prm[0], prm[1], prm[2], prm[3]};
+    int nc = 2 * ndim, err = 0;
+    for (int64_t i = 0; i < n; i++) {
+        double s[6], zi = z[i];
+        uint8_t el = elastic[i];
+        for (int c = 0; c < nc; c++) s[c] = sig[i * nc + c];
+        int cs = -1, ns = 0;
+        int st = ep::update(p, nc, s, &zi, &el, deps + i * nc, settings[0], settings[1], settings[2], max_steps,
+                            &cs, &ns);
+        if (st) {
+            if (!err) { err = st; if (bad) *bad = i; }
+            cs = -1;
+        } else {
+            for (int c = 0; c < nc; c++) sig[i * nc + c] = s[c];
+            z[i] = zi;
+            elastic[i] = el;
+        }
+        cases[i] = cs;
+        steps[i] = ns;
+    }
     return err;
 }
 

@@ -64,6 +64,11 @@ class BatchTuning_(ctypes.Structure):
                 ("team_chunks", ctypes.c_int32), ("pcg_budget", ctypes.c_int32), ("graph_iters", ctypes.c_int32)]
 
 
+class EpSettings_(ctypes.Structure):
+    _fields_ = [("tol_rel", ctypes.c_double), ("tol_abs", ctypes.c_double), ("h_ini", ctypes.c_double),
+                ("max_steps", ctypes.c_int32), ("pad_", ctypes.c_int32)]
+
+
 class Info_(ctypes.Structure):
     _fields_ = [("ndim", ctypes.c_int32), ("kind", ctypes.c_int32), ("nnode", ctypes.c_int32),
                 ("ngauss", ctypes.c_int32), ("ncomp", ctypes.c_int32), ("npoint", ctypes.c_int64),
@@ -100,6 +105,8 @@ SIGNATURES = {
     "pms_vm_update_and_stiffness_batch": (_I, [ctypes.POINTER(Material_), _I, _I64, _V, _V, _V, _V, _V, _V, _V,
                                                _V, _V]),
     "pms_vm_stiffness_batch": (_I, [ctypes.POINTER(Material_), _I, _I64, _V, _V, _V, _V, _V, _V, _V]),
+    "pms_ep_update_stress_batch": (_I, [ctypes.POINTER(Material_), _I, _I64, _V, _V, _V, _V,
+                                        ctypes.POINTER(EpSettings_), _V, _V, _V, _V]),
     "pms_vm_update_and_stiffness_host": (_I, [ctypes.POINTER(Material_), _I, _I64, _V, _V, _V, _V, _V, _V, _V]),
     "pms_mesh_csr_pattern": (_I, [ctypes.POINTER(Mesh_), _V, _V, ctypes.POINTER(_I64)]),
     "pms_elements_set_timing": (_I, [_V, _I]),

@@ -26,11 +26,14 @@
 // FLOPs per IP and pair (3D): 3 (dot) + 9*3 (entries) + 3 (diagonal) = 33 FMA; per node: J^-T
 // dN (9), h = S g (9), three scaled copies (9).
 //
+// 2D cells (at most 9 nodes) run in element2d_kernel instead: the same arithmetic with several
+// cells per warp (three 10-lane Qua8 cells), so that most lanes hold work.
+//
 // Assembly: each cell's dense element matrix goes to a scratch buffer ke[cell][NE][NE] (the
-// reference's GenericElement::kke, src/fem/elements.rs:13-14); kk_gather_kernel owns one block
-// row A of K per warp, adds the node-row slabs (a, all b) of the cells incident to A in ascending
-// cell order in shared memory and writes the CSR row once, coalesced.  No atomics: bit-identical
-// on every run.
+// reference's GenericElement::kke, src/fem/elements.rs:13-14); in kk_gather_kernel a group of
+// nnode lanes owns one block row A of K (32/nnode rows per warp), adds the node-row slabs (a, all
+// b) of the cells incident to A in ascending cell order in shared memory and writes the CSR row
+// once, coalesced.  No atomics: bit-identical on every run.
 #include <cuda_runtime.h>
 
 #include <algorithm>

@@ -74,3 +74,36 @@ class VonMisesBatch:
                                                      _lib.ptr(deps), _lib.ptr(hh), _lib.ptr(dd))
         _lib.check(rc)
         return dd
+
+
+EP_CASES = ("AE", "AXB", "BE", "BXP", "BP")
+
+
+class ElastoplasticBatch:
+    """``Elastoplastic::update_stress`` (``src/material/elastoplastic.rs:539-641``) over n IPs.
+
+    The general elastoplastic update of the reference with its one plasticity model, von Mises
+    (``src/material/von_mises.rs:229-282``): the crossing of the yield surface along the elastic
+    path, then the ODE ``dsigma/dt = Dep : deps``, ``dz/dt = Lambda_d H`` integrated (Dormand-Prince
+    5(4), adaptive) from the crossing to the end of the increment.  Device buffers, structure of
+    arrays: sig[ncomp, n], z[n], elastic[n] (uint8) updated in place from deps[ncomp, n]; cases[n]
+    (int32, optional) receives the index into ``EP_CASES`` (-1 where the IP failed) and steps[n]
+    the ODE steps.  There is no tangent, as in the reference (``Elastoplastic::stiffness`` is a
+    TODO there).
+    """
+
+    def __init__(self, young, poisson, hh, z_ini, ndim=3, tol_rel=1e-10, tol_abs=1e-10, h_ini=1.0,
+                 max_steps=1000):
+        self.L = _lib.load()
+        self.mat = _lib.material(_lib.VON_MISES, young, poisson, hh, z_ini)
+        self.ndim = ndim
+        self.ncomp = 2 * ndim
+        self.settings = _lib.EpSettings_(tol_rel, tol_abs, h_ini, max_steps, 0)
+
+    def update_stress(self, sig, z, elastic, deps, cases=None, steps=None, status=None, stream=None):
+        n = sig.shape[-1]
+        raw = getattr(stream, "cuda_stream", stream)
+        rc = self.L.pms_ep_update_stress_batch(ctypes.byref(self.mat), self.ndim, n, _lib.ptr(sig), _lib.ptr(z),
+                                               _lib.ptr(elastic), _lib.ptr(deps), ctypes.byref(self.settings),
+                                               _lib.ptr(cases), _lib.ptr(steps), _lib.ptr(status), raw)
+        _lib.check(rc)

@@ -94,3 +94,21 @@ def test_unsupported_idealizations_are_rejected_without_gpu():
     le = _lib.material(_lib.LINEAR_ELASTIC, 1e4, 0.3, 0.0, 1.0)
     for cfg in (_lib.Config_(0, 1, 0, 1.0), _lib.Config_(0, 0, 1, 1.0)):
         assert L.pms_elements_create(ctypes.byref(cm3), ctypes.byref(le), 1, ctypes.byref(cfg), ctypes.byref(h)) == 7
+
+
+def test_general_elastoplastic_rejects_other_models_without_gpu():
+    """Elastoplastic::new accepts only the von Mises plasticity model (elastoplastic.rs:129-135):
+    the batched entry refuses a linear-elastic material and bad sizes before touching the GPU."""
+    L = _lib.load()
+    s = _lib.EpSettings_(1e-10, 1e-10, 1.0, 1000, 0)
+    lin = _lib.material(_lib.LINEAR_ELASTIC, 1500.0, 0.25, 0.0, 1.0)
+    vm = _lib.material(_lib.VON_MISES, 1500.0, 0.25, 800.0, 9.0)
+    assert L.pms_ep_update_stress_batch(ctypes.byref(lin), 2, 1, None, None, None, None, ctypes.byref(s),
+                                        None, None, None, None) == 1
+    assert L.pms_ep_update_stress_batch(ctypes.byref(vm), 4, 1, None, None, None, None, ctypes.byref(s),
+                                        None, None, None, None) == 1
+    assert L.pms_ep_update_stress_batch(ctypes.byref(vm), 2, 0, None, None, None, None, ctypes.byref(s),
+                                        None, None, None, None) == 0
+    bad = _lib.EpSettings_(0.0, 1e-10, 1.0, 1000, 0)
+    assert L.pms_ep_update_stress_batch(ctypes.byref(vm), 2, 1, None, None, None, None, ctypes.byref(bad),
+                                        None, None, None, None) == 1

@@ -310,3 +310,52 @@ def test_oracle_bhatti_1d6_plane_stress():
     solver = OracleSolver(el, m.ndof, pb["essential"], lagrange_mult_method=False, t_fin=1.0, ff_ext_fn=pb["natural"].ff_ext)
     solver.solve(lambda step, t, u, e: out.setdefault("u", u))
     np.testing.assert_allclose(out["u"], pb["golden"]["uu_correct"], rtol=0, atol=1e-15)
+
+
+# ---------------------------------------------------------------- general elastoplasticity
+def _ep_oracle(sig0, z0, deps, ndim=2, **kw):
+    import ep_cases as E
+    prm = oracle.Params(E.YOUNG, E.POISSON, E.HH, E.Z_INI)
+    sig = np.array(sig0, dtype=float).reshape(1, -1).copy()
+    z = np.array([z0], dtype=float)
+    el = np.zeros(1, dtype=np.uint8)
+    st, cases, steps, bad = oracle.ep_update(prm, ndim, sig, z, el, np.array(deps).reshape(1, -1), **kw)
+    return st, sig[0], z[0], int(el[0]), oracle.EP_CASES[cases[0]] if cases[0] >= 0 else None, int(steps[0])
+
+
+@pytest.mark.parametrize("idx", range(11))
+def test_oracle_elastoplastic_reference_paths(idx):
+    """The general update on the paths of elastoplastic.rs's von Mises tests: same case keys and,
+    where the reference asserts them, the closed-form invariants (radial paths: the ODE is exact).
+    Tolerance 1e-12 absolute on stresses of order 10 (the reference asserts 1e-13 to 1e-15)."""
+    import ep_cases as E
+    name, s0, z0, d, case, check = E.scenarios()[idx]
+    st, s, z, el, got, _ = _ep_oracle(s0, z0, d)
+    assert st == 0, name
+    assert got == case, (name, got)
+    for v, want in check(s, z, el):
+        assert abs(v - want) <= 1e-12, (name, v, want)
+
+
+def test_oracle_elastoplastic_stays_on_the_yield_surface():
+    """Continuum consistency: along the plastic part f(sigma, z) = sigma_d - z does not change up
+    to the ODE tolerance (df/dt = n : dsigma/dt - dz/dt = 0 along the exact solution), on
+    non-radial paths where the closed-form return map does not apply."""
+    import ep_cases as E
+    sig, z, deps = E.random_states(300, 2, seed=11)
+    prm = oracle.Params(E.YOUNG, E.POISSON, E.HH, E.Z_INI)
+    el = np.zeros(len(z), dtype=np.uint8)
+    f0 = np.array([E.sigma_d(s) for s in sig]) - z
+    st, cases, steps, bad = oracle.ep_update(prm, 2, sig, z, el, deps)
+    # increments the reference rejects fail here too: turning back inside during the plastic part
+    # ("plastic numerator (df/dsigma : De : deps) is overly negative", code 10), or starting outside
+    # and heading inwards without ever reaching the surface (the reference asserts; code 12)
+    ok = cases >= 0
+    assert st in (0, 10, 12) and ok.sum() >= 0.9 * len(z)
+    plastic = ok & (el == 0)
+    assert plastic.sum() > 50 and (ok & (el == 1)).sum() > 20
+    # f is constant along the plastic part: 0 after a crossing, the initial drift for BP
+    for i in np.flatnonzero(plastic):
+        f_start = f0[i] if cases[i] == 4 else 0.0
+        assert abs(E.sigma_d(sig[i]) - z[i] - f_start) <= 1e-8 * z[i], i
+    assert set(cases[ok].tolist()) >= {0, 1, 4}
