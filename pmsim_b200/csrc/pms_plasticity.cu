@@ -29,7 +29,6 @@
 // sigma, z, flag); a few thousand FP64 flops per plastic IP otherwise.
 #include <cuda_runtime.h>
 
-#include <atomic>
 #include <cstdint>
 
 #include "../../include/pms.h"
@@ -38,8 +37,6 @@
 using namespace pms;
 
 namespace {
-
-std::atomic<int64_t> g_ep_launches{0};
 
 constexpr double NUMERATOR_TOL = 1e-8;     // elastoplastic.rs:17
 constexpr double PSEUDO_TIME_TOL = 1e-7;   // elastoplastic.rs:23
@@ -333,6 +330,5 @@ extern "C" int pms_ep_update_stress_batch(const pms_material* mat, int32_t ndim,
         ep_update_kernel<4><<<(unsigned)blocks, 128, 0, st>>>(m, e, n, sig, z, elastic, deps, cases, steps, status);
     else
         ep_update_kernel<6><<<(unsigned)blocks, 128, 0, st>>>(m, e, n, sig, z, elastic, deps, cases, steps, status);
-    g_ep_launches++;
     return cudaGetLastError() == cudaSuccess ? PMS_OK : PMS_ERR_CUDA;
 }

@@ -359,3 +359,37 @@ def test_oracle_elastoplastic_stays_on_the_yield_surface():
         f_start = f0[i] if cases[i] == 4 else 0.0
         assert abs(E.sigma_d(sig[i]) - z[i] - f_start) <= 1e-8 * z[i], i
     assert set(cases[ok].tolist()) >= {0, 1, 4}
+
+
+@pytest.mark.parametrize("ndim", [2, 3])
+def test_oracle_elastoplastic_equals_return_map_on_radial_paths(ndim):
+    """On a radial increment from a point on the yield surface (deviatoric strain along the current
+    deviatoric stress, any volumetric part) D_ep : deps is constant along the path, so the general
+    update must give the closed-form radial return of VonMises::update_stress (von_mises.rs:170-226)
+    -- the relation the reference's elastoplastic tests assert.  Tolerance 1e-10 relative."""
+    import ep_cases as E
+    rng = np.random.default_rng(100 + ndim)
+    nc = 2 * ndim
+    prm = oracle.Params(E.YOUNG, E.POISSON, E.HH, E.Z_INI)
+    for _ in range(200):
+        s = rng.normal(0.0, 1.0, nc)
+        m = (s[0] + s[1] + s[2]) / 3.0
+        dev = s.copy()
+        dev[:3] -= m
+        dev *= E.Z_INI / E.sigma_d(dev)  # on the surface, z = z_ini
+        sig0 = dev.copy()
+        sig0[:3] += rng.normal(0.0, 5.0)
+        unit = dev / np.linalg.norm(dev)
+        deps = rng.uniform(1e-4, 1e-2) * unit
+        deps[:3] += rng.normal(0.0, 1e-3)
+        # general update
+        sg, zg, eg = sig0.reshape(1, -1).copy(), np.array([E.Z_INI]), np.zeros(1, dtype=np.uint8)
+        st, cases, _, _ = oracle.ep_update(prm, ndim, sg, zg, eg, deps.reshape(1, -1))
+        assert st == 0 and oracle.EP_CASES[cases[0]] in ("BP", "AXB")
+        # closed-form radial return
+        sc, ivs, ec = sig0.copy(), np.array([E.Z_INI, 0.0]), np.zeros(1, dtype=np.uint8)
+        assert oracle.model_update_stress(1, prm, ndim, sc, ivs, ec, deps) == 0
+        scale = np.abs(sc).max()
+        assert np.abs(sg[0] - sc).max() <= 1e-10 * scale
+        assert abs(zg[0] - ivs[0]) <= 1e-10 * ivs[0]
+        assert eg[0] == ec[0] == 0
