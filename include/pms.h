@@ -287,6 +287,12 @@ enum pms_ep_case { PMS_EP_AE = 0, PMS_EP_AXB = 1, PMS_EP_BE = 2, PMS_EP_BXP = 3,
 int pms_ep_update_stress_batch(const pms_material* mat, int32_t ndim, int64_t n, double* sig, double* z,
                                uint8_t* elastic, const double* deps, const pms_ep_settings* settings,
                                int32_t* cases, int32_t* steps, int32_t* status, void* stream);
+/* Same as pms_ep_update_stress_batch on HOST buffers (same layout): copies in, runs, copies out,
+ * and returns the first failing IP's code (PMS_OK if none); the library keeps a device staging
+ * area, grown on demand. */
+int pms_ep_update_stress_host(const pms_material* mat, int32_t ndim, int64_t n, double* sig, double* z,
+                              uint8_t* elastic, const double* deps, const pms_ep_settings* settings,
+                              int32_t* cases, int32_t* steps);
 
 /* Measures the FP64 FMA pipe: blocks x 256 threads, 8 independent FMA chains of `iters` each
  * (16*iters FLOP per thread); out[blocks*256] receives the chain sums.  Used as the FP64 peak. */

@@ -107,6 +107,8 @@ SIGNATURES = {
     "pms_vm_stiffness_batch": (_I, [ctypes.POINTER(Material_), _I, _I64, _V, _V, _V, _V, _V, _V, _V]),
     "pms_ep_update_stress_batch": (_I, [ctypes.POINTER(Material_), _I, _I64, _V, _V, _V, _V,
                                         ctypes.POINTER(EpSettings_), _V, _V, _V, _V]),
+    "pms_ep_update_stress_host": (_I, [ctypes.POINTER(Material_), _I, _I64, _V, _V, _V, _V,
+                                       ctypes.POINTER(EpSettings_), _V, _V]),
     "pms_vm_update_and_stiffness_host": (_I, [ctypes.POINTER(Material_), _I, _I64, _V, _V, _V, _V, _V, _V, _V]),
     "pms_mesh_csr_pattern": (_I, [ctypes.POINTER(Mesh_), _V, _V, ctypes.POINTER(_I64)]),
     "pms_elements_set_timing": (_I, [_V, _I]),

@@ -30,6 +30,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <mutex>
 
 #include "../../include/pms.h"
 #include "pms_device.cuh"
@@ -331,4 +332,65 @@ extern "C" int pms_ep_update_stress_batch(const pms_material* mat, int32_t ndim,
     else
         ep_update_kernel<6><<<(unsigned)blocks, 128, 0, st>>>(m, e, n, sig, z, elastic, deps, cases, steps, status);
     return cudaGetLastError() == cudaSuccess ? PMS_OK : PMS_ERR_CUDA;
+}
+
+namespace {
+// device staging of the host-buffer entry, grown on demand and kept until exit
+struct EpStage {
+    std::mutex mu;
+    void* buf = nullptr;
+    size_t bytes = 0;
+    cudaStream_t stream = nullptr;
+} g_ep_stage;
+}  // namespace
+
+extern "C" int pms_ep_update_stress_host(const pms_material* mat, int32_t ndim, int64_t n, double* sig, double* z,
+                                         uint8_t* elastic, const double* deps, const pms_ep_settings* settings,
+                                         int32_t* cases, int32_t* steps) {
+    if (!mat || (ndim != 2 && ndim != 3) || n < 0) return PMS_ERR_INVALID;
+    if (n == 0) return PMS_OK;
+    if (!sig || !z || !elastic || !deps) return PMS_ERR_INVALID;
+    const size_t nc = 2 * (size_t)ndim, b_sig = nc * n * 8, b_n = (size_t)n * 8, b_i = (size_t)n * 4;
+    const size_t need = 64 + 2 * b_sig + b_n + (cases ? b_i : 0) + (steps ? b_i : 0) + (size_t)n;
+    std::lock_guard<std::mutex> lock(g_ep_stage.mu);
+    if (!g_ep_stage.stream && cudaStreamCreateWithFlags(&g_ep_stage.stream, cudaStreamNonBlocking) != cudaSuccess)
+        return PMS_ERR_CUDA;
+    if (g_ep_stage.bytes < need) {
+        if (g_ep_stage.buf) cudaFree(g_ep_stage.buf);
+        g_ep_stage.buf = nullptr;
+        g_ep_stage.bytes = 0;
+        if (cudaMalloc(&g_ep_stage.buf, need) != cudaSuccess) return PMS_ERR_NOMEM;
+        g_ep_stage.bytes = need;
+    }
+    char* p = (char*)g_ep_stage.buf;
+    int32_t* d_status = (int32_t*)p; p += 64;
+    double* d_sig = (double*)p; p += b_sig;
+    double* d_deps = (double*)p; p += b_sig;
+    double* d_z = (double*)p; p += b_n;
+    int32_t* d_cases = nullptr;
+    if (cases) { d_cases = (int32_t*)p; p += b_i; }
+    int32_t* d_steps = nullptr;
+    if (steps) { d_steps = (int32_t*)p; p += b_i; }
+    uint8_t* d_el = (uint8_t*)p;
+    cudaStream_t s = g_ep_stage.stream;
+    cudaMemsetAsync(d_status, 0, 16, s);
+    cudaMemcpyAsync(d_sig, sig, b_sig, cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(d_deps, deps, b_sig, cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(d_z, z, b_n, cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(d_el, elastic, (size_t)n, cudaMemcpyHostToDevice, s);
+    int rc = pms_ep_update_stress_batch(mat, ndim, n, d_sig, d_z, d_el, d_deps, settings, d_cases, d_steps,
+                                        d_status, s);
+    if (rc) {
+        cudaStreamSynchronize(s);
+        return rc;
+    }
+    cudaMemcpyAsync(sig, d_sig, b_sig, cudaMemcpyDeviceToHost, s);
+    cudaMemcpyAsync(z, d_z, b_n, cudaMemcpyDeviceToHost, s);
+    cudaMemcpyAsync(elastic, d_el, (size_t)n, cudaMemcpyDeviceToHost, s);
+    if (cases) cudaMemcpyAsync(cases, d_cases, b_i, cudaMemcpyDeviceToHost, s);
+    if (steps) cudaMemcpyAsync(steps, d_steps, b_i, cudaMemcpyDeviceToHost, s);
+    int32_t hst[4] = {0, 0, 0, 0};
+    cudaMemcpyAsync(hst, d_status, 16, cudaMemcpyDeviceToHost, s);
+    if (cudaStreamSynchronize(s) != cudaSuccess) return PMS_ERR_CUDA;
+    return hst[0];
 }

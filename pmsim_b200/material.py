@@ -107,3 +107,19 @@ class ElastoplasticBatch:
                                                _lib.ptr(elastic), _lib.ptr(deps), ctypes.byref(self.settings),
                                                _lib.ptr(cases), _lib.ptr(steps), _lib.ptr(status), raw)
         _lib.check(rc)
+
+    def update_stress_host(self, sig, z, elastic, deps):
+        """Host numpy buffers (SoA as above; copied to the device and back inside the call).
+        Returns (code of the first failing IP or 0, cases, steps)."""
+        n = sig.shape[-1]
+        for a in (sig, z, elastic, deps):
+            if not a.flags["C_CONTIGUOUS"]:
+                raise ValueError("host arrays must be C-contiguous")
+        cases = np.zeros(n, dtype=np.int32)
+        steps = np.zeros(n, dtype=np.int32)
+        rc = self.L.pms_ep_update_stress_host(ctypes.byref(self.mat), self.ndim, n, _lib.ptr(sig), _lib.ptr(z),
+                                              _lib.ptr(elastic), _lib.ptr(deps), ctypes.byref(self.settings),
+                                              _lib.ptr(cases), _lib.ptr(steps))
+        if rc in (1, 2, 6):  # invalid argument, CUDA error, no device memory: not a per-IP outcome
+            _lib.check(rc)
+        return rc, cases, steps

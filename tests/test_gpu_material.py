@@ -206,3 +206,20 @@ def test_elastoplastic_matches_oracle(ndim):
     # failed IPs keep their state
     failed = cases < 0
     assert np.array_equal(s1[failed], sig[failed]) and np.array_equal(z1[failed], z[failed])
+
+
+@pytest.mark.gpu
+def test_elastoplastic_host_entry_equals_device_entry():
+    """pms_ep_update_stress_host (host buffers, staged through the device) gives the same bits as
+    the device entry, and returns the code of the first failing IP (the increments the reference
+    rejects) as its status."""
+    import ep_cases as E
+    from pmsim_b200.material import ElastoplasticBatch
+    sig, z, deps = E.random_states(3000, 3, seed=77)
+    s1, z1, el1, c1, n1, st = _ep_device(3, sig, z, deps)
+    hs, hz, he = np.ascontiguousarray(sig.T), z.copy(), np.zeros(len(z), dtype=np.uint8)
+    rc, c2, n2 = ElastoplasticBatch(E.YOUNG, E.POISSON, E.HH, E.Z_INI, ndim=3).update_stress_host(
+        hs, hz, he, np.ascontiguousarray(deps.T))
+    assert rc == st[0]
+    assert np.array_equal(hs.T, s1) and np.array_equal(hz, z1) and np.array_equal(he, el1)
+    assert np.array_equal(c2, c1) and np.array_equal(n2, n1)
