@@ -514,8 +514,8 @@ def run_served(nreq, rate, nalone, seed=7, detail_file=""):
         t_alone += time.perf_counter() - t0
         ok += 0 if b1.failed else 1
         b1.close()
-    # the plain GPU path of the target -- the drop-in path (device element calls + host sparse LU)
-    # one request at a time -- on a seeded sample of the smaller requests (<= 20,000 DOF).  Larger
+    # the plain GPU path -- the drop-in path (device element calls + host sparse LU) one request
+    # at a time -- on a seeded sample of the smaller requests (<= 20,000 DOF).  Larger
     # requests only take longer on it, so the ratio is a lower bound; a request still running
     # after the load step that passes 20 s is stopped and counted as converged at that time (again
     # in the plain path's favour).
