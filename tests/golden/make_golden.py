@@ -10,6 +10,7 @@ Sources (paths inside the pmsim project):
   * data/spo/test_von_mises_2x2_elements_2d_ref.json     (HYPLAS, Qua8 4 IP, 5 steps)
   * data/spo/spo_754_footing_ref.json + spo_754_footing.msh (HYPLAS, Qua8 4 IP, 14 steps)
   * data/spo/spo_755_tensile_perf_plast_ref.json + spo_755_tensile.msh (Qua8 4 IP, 15 steps)
+  * data/spo/spo_753_circ_plate_ref.json + spo_753_circ_plate.msh (axisymmetric Qua8 4 IP, 12 steps)
   * data/results/artificial/*.json, *.msh  (pmsim's own FemState output, uniform fields; the
     raw files are kept as femstate_*.json for the byte-level checkpoint test)
   * data/sgm/sgm_5d17_ref.json and tests/test_solid_smith_5d17_qua4_axisym.rs (axisymmetric Qua4)
@@ -149,6 +150,7 @@ def main(ref):
     print("wrote bhatti_1d6_plane_stress", coords.shape, conn.shape, uu.shape)
     # SPO 7.5.1 pressurised cylinder (reduced-system method, internal pressure, von Mises)
     spo(ref, "spo_751_pres_cylin_ref.json", "spo_751_pres_cylin.npz", mesh="data/spo/spo_751_pres_cylin_qua4.msh")
+    spo(ref, "spo_753_circ_plate_ref.json", "spo_753_circ_plate.npz", mesh="data/spo/spo_753_circ_plate.msh")
 
 
 if __name__ == "__main__":

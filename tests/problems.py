@@ -164,6 +164,26 @@ def pres_cylin_751():
                 tol_u=1e-11, tol_s=2e-14, iterations=[2, 5, 6, 5, 9])
 
 
+P_753 = [0.0, 100.0, 200.0, 220.0, 230.0, 240.0, 250.0, 255.0, 257.0, 259.0, 259.5, 259.75, 259.77]
+
+
+def circ_plate_753():
+    """tests/test_spo_753_circ_plate.rs: axisymmetric circular plate (radius 10, thickness 1), 10 Qua8
+    cells, 4 IP, von Mises E=1e7, nu=0.24, z0=16000, H=0; u_r = 0 on the axis (x = 0), u_z = 0 at
+    the rim corner (10, 0); normal pressure P(t) on the top face (y = 1) up to 259.77, near the
+    collapse load; Lagrange multipliers, 12 load steps, at most 20 iterations each.  Tolerances as
+    in the reference test: 1e-9 on displacements, 1e-6 on stresses."""
+    from pmsim_b200.natural import Natural, find_sides
+    g = load("spo_753_circ_plate.npz")
+    m = Mesh(2, g["coords"], g["cells"], QUA8)
+    ess = _ess(m.points_where(lambda x, y: abs(x) < TOL), 0, 2) + \
+        _ess(m.points_where(lambda x, y: (np.abs(x - 10.0) < TOL) & (np.abs(y) < TOL)), 1, 2)
+    nat = Natural(m, axisymmetric=True).sides(find_sides(m, lambda p: abs(p[1] - 1.0) < TOL), 1.0,
+                                              lambda t: -P_753[int(t)])
+    return dict(mesh=m, params=(1e7, 0.24, 0.0, 16000.0), ngauss=4, essential=ess, natural=nat, nsteps=12,
+                golden=g, tol_u=1e-9, tol_s=1e-6)
+
+
 class MultiMaterialOracle:
     """The oracle's element calls over a mesh whose cells use several materials: one homogeneous
     OracleElements per material on its subset of cells (all points kept), summed like the

@@ -393,3 +393,27 @@ def test_oracle_elastoplastic_equals_return_map_on_radial_paths(ndim):
         assert np.abs(sg[0] - sc).max() <= 1e-10 * scale
         assert abs(zg[0] - ivs[0]) <= 1e-10 * ivs[0]
         assert eg[0] == ec[0] == 0
+
+
+def test_oracle_spo_753_axisymmetric_circular_plate():
+    """Axisymmetric von Mises plasticity: the SPO circular-plate run (HYPLAS reference data,
+    data/spo/spo_753_circ_plate_ref.json) replayed by the oracle's Newton driver to the collapse
+    load, at the reference test's tolerances."""
+    pb = problems.circ_plate_753()
+    m = pb["mesh"]
+    el = oracle.OracleElements(m, 1, oracle.Params(*pb["params"]), ngauss=pb["ngauss"], sym_tol=-1.0,
+                               axisymmetric=True)
+    solver = OracleSolver(el, m.ndof, pb["essential"], n_max_iterations=20, t_fin=float(pb["nsteps"]),
+                          ff_ext_fn=pb["natural"].ff_ext)
+    worst = [0.0, 0.0]
+
+    def cb(step, t, u, el):
+        du, ds = problems.compare_step(pb["golden"], step, u, el.sig, pb["ngauss"])
+        worst[0] = max(worst[0], du)
+        worst[1] = max(worst[1], ds)
+
+    assert solver.solve(cb) == pb["nsteps"]
+    assert worst[0] <= pb["tol_u"], worst
+    assert worst[1] <= pb["tol_s"], worst
+    # HYPLAS counts the corrections; the Newton loop here also counts the final residual check
+    assert [len(h) for h in solver.history] == [int(k) + 1 for k in pb["golden"]["hyplas_iterations"]]
