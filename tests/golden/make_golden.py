@@ -11,6 +11,7 @@ Sources (paths inside the pmsim project):
   * data/spo/spo_754_footing_ref.json + spo_754_footing.msh (HYPLAS, Qua8 4 IP, 14 steps)
   * data/spo/spo_755_tensile_perf_plast_ref.json + spo_755_tensile.msh (Qua8 4 IP, 15 steps)
   * data/spo/spo_753_circ_plate_ref.json + spo_753_circ_plate.msh (axisymmetric Qua8 4 IP, 12 steps)
+  * data/spo/spo_752_pres_sphere_collapse_ref.json (axisymmetric sphere on the SPO 7.5.1 mesh, 4 steps)
   * data/results/artificial/*.json, *.msh  (pmsim's own FemState output, uniform fields; the
     raw files are kept as femstate_*.json for the byte-level checkpoint test)
   * data/sgm/sgm_5d17_ref.json and tests/test_solid_smith_5d17_qua4_axisym.rs (axisymmetric Qua4)
@@ -151,6 +152,7 @@ def main(ref):
     # SPO 7.5.1 pressurised cylinder (reduced-system method, internal pressure, von Mises)
     spo(ref, "spo_751_pres_cylin_ref.json", "spo_751_pres_cylin.npz", mesh="data/spo/spo_751_pres_cylin_qua4.msh")
     spo(ref, "spo_753_circ_plate_ref.json", "spo_753_circ_plate.npz", mesh="data/spo/spo_753_circ_plate.msh")
+    spo(ref, "spo_752_pres_sphere_collapse_ref.json", "spo_752_pres_sphere_collapse.npz")
 
 
 if __name__ == "__main__":

@@ -184,6 +184,28 @@ def circ_plate_753():
                 golden=g, tol_u=1e-9, tol_s=1e-6)
 
 
+P_752 = [0.0, 0.15, 0.3, 0.33, 0.33269]
+
+
+def pres_sphere_752():
+    """tests/test_spo_752_pres_sphere.rs (the collapse run): the SPO 7.5.1 Qua8 mesh taken as an
+    axisymmetric section of a thick sphere (inner radius 100, outer 200), 4 IP, von Mises E=210,
+    nu=0.3, z0=0.24, H=0, u_r = 0 on the axis (x = 0), u_z = 0 on the equator (y = 0), internal
+    pressure up to 0.33269 (near collapse), Lagrange multipliers, 4 load steps.  The reference test's
+    tolerances are loose (4.33e-2 on displacements, 2.55e-2 on stresses) because the HYPLAS data
+    were computed differently; they are the reference's."""
+    from pmsim_b200.natural import Natural, find_sides
+    gm = load("spo_751_pres_cylin.npz")
+    g = load("spo_752_pres_sphere_collapse.npz")
+    m = Mesh(2, gm["coords"], gm["cells"], QUA8)
+    ess = _ess(m.points_where(lambda x, y: np.abs(x) < TOL), 0, 2) + \
+        _ess(m.points_where(lambda x, y: np.abs(y) < TOL), 1, 2)
+    on_circle = lambda p: abs(np.hypot(p[0], p[1]) - 100.0) < 1e-6  # noqa: E731
+    nat = Natural(m, axisymmetric=True).sides(find_sides(m, on_circle), 1.0, lambda t: -P_752[int(t)])
+    return dict(mesh=m, params=(210.0, 0.3, 0.0, 0.24), ngauss=4, essential=ess, natural=nat, nsteps=4,
+                golden=g, tol_u=4.33e-2, tol_s=2.55e-2)
+
+
 class MultiMaterialOracle:
     """The oracle's element calls over a mesh whose cells use several materials: one homogeneous
     OracleElements per material on its subset of cells (all points kept), summed like the

@@ -417,3 +417,24 @@ def test_oracle_spo_753_axisymmetric_circular_plate():
     assert worst[1] <= pb["tol_s"], worst
     # HYPLAS counts the corrections; the Newton loop here also counts the final residual check
     assert [len(h) for h in solver.history] == [int(k) + 1 for k in pb["golden"]["hyplas_iterations"]]
+
+
+def test_oracle_spo_752_axisymmetric_pressurised_sphere():
+    """The SPO pressurised sphere (axisymmetric von Mises, collapse run,
+    data/spo/spo_752_pres_sphere_collapse_ref.json) replayed by the oracle's Newton driver at the
+    reference test's own (loose) tolerances."""
+    pb = problems.pres_sphere_752()
+    m = pb["mesh"]
+    el = oracle.OracleElements(m, 1, oracle.Params(*pb["params"]), ngauss=pb["ngauss"], sym_tol=-1.0,
+                               axisymmetric=True)
+    solver = OracleSolver(el, m.ndof, pb["essential"], t_fin=float(pb["nsteps"]), ff_ext_fn=pb["natural"].ff_ext)
+    worst = [0.0, 0.0]
+
+    def cb(step, t, u, el):
+        du, ds = problems.compare_step(pb["golden"], step, u, el.sig, pb["ngauss"])
+        worst[0] = max(worst[0], du)
+        worst[1] = max(worst[1], ds)
+
+    assert solver.solve(cb) == pb["nsteps"]
+    assert worst[0] <= pb["tol_u"], worst
+    assert worst[1] <= pb["tol_s"], worst
