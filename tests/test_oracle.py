@@ -488,3 +488,48 @@ def test_oracle_constant_strain_elements_closed_form(three_d):
         K = oracle.elem_jacobian(kind, 1, X, 0, prm, sig, np.zeros((1, 2)), np.ones(1, dtype=np.uint8))
         assert np.max(np.abs(f - f_ref)) <= 1e-13 * np.max(np.abs(f_ref))
         assert np.max(np.abs(K - K_ref)) <= 1e-12 * np.max(np.abs(K_ref))
+
+
+@pytest.mark.parametrize("kind_name,plane_stress", [("tri3", False), ("qua4", False), ("qua8", False),
+                                                    ("hex8", False), ("tri3", True), ("qua4", True), ("qua8", True)])
+def test_oracle_uniform_strain_fields(kind_name, plane_stress):
+    """ElementSolid::update_secondary_values on uniform strain fields (src/fem/element_solid.rs:453-626
+    with the field generators of src/base/testing.rs:34-230): u_x = e x, u_y = e y and u_x = 2 e y with
+    e = 4.56, E = 1, nu = 0.25, plane strain / 3D and plane stress.  Every IP must carry the closed-form
+    stress at the reference's tolerance 1e-13; the meshes here are distorted (isoparametric elements
+    reproduce linear fields exactly on any shape)."""
+    from pmsim_b200.mesh import structured_2d, structured_3d
+    kind = kind_from_name(kind_name)
+    rng = np.random.default_rng(kind + 31)
+    m = structured_3d(kind, 2, 2, 2) if kind_name == "hex8" else structured_2d(kind, 3, 2, 1.5, 1.0)
+    inner = np.all((m.coords > 1e-9) & (m.coords < m.coords.max(axis=0) - 1e-9), axis=1)
+    m.coords[inner] += rng.uniform(-0.05, 0.05, (inner.sum(), m.ndim))
+    nd, E_, nu, e = m.ndim, 1.0, 0.25, 4.56
+    model = oracle.MODEL_LINEAR_ELASTIC_PLANE_STRESS if plane_stress else oracle.MODEL_LINEAR_ELASTIC
+    c = E_ / ((1 + nu) * (1 - 2 * nu))
+    cps = E_ / (1 - nu * nu)
+    G = E_ / (2 * (1 + nu))
+    nc = 2 * nd
+    fields = []
+    u = np.zeros((m.npoint, nd)); u[:, 0] = e * m.coords[:, 0]
+    s = np.zeros(nc)
+    if plane_stress:
+        s[:2] = [cps * e, cps * e * nu]
+    else:
+        s[:3] = c * e * nu; s[0] = c * e * (1 - nu)
+    fields.append((u, s))
+    u = np.zeros((m.npoint, nd)); u[:, 1] = e * m.coords[:, 1]
+    s = np.zeros(nc)
+    if plane_stress:
+        s[:2] = [cps * e * nu, cps * e]
+    else:
+        s[:3] = c * e * nu; s[1] = c * e * (1 - nu)
+    fields.append((u, s))
+    u = np.zeros((m.npoint, nd)); u[:, 0] = 2 * e * m.coords[:, 1]
+    s = np.zeros(nc); s[3] = np.sqrt(2) * 2 * G * e  # Mandel: sqrt2 * sigma_xy, sigma_xy = 2 G eps_xy
+    fields.append((u, s))
+    for u, want in fields:
+        el = oracle.OracleElements(m, model, oracle.Params(E_, nu, 0.0, 1.0))
+        el.initialize()
+        el.update_secondary_values(u.reshape(-1))
+        assert np.max(np.abs(el.sig - want[None, :])) <= 1e-13, (kind_name, want)
