@@ -1,0 +1,184 @@
+"""One problem sharded over ranks: owner-computes partition, halo exchange, distributed CG.
+
+pmsim solves one problem in one process (``src/fem/solver_implicit.rs``); this module has no
+counterpart in the reference.  It splits one mesh over ``nparts`` ranks so that every rank holds
+a disjoint set of CSR block rows of K and R:
+
+* every node (block row) has one owner (``node_owner``: equal-count slabs along the longest axis);
+* a rank computes every cell that touches a node it owns, so its owned rows of K and R are
+  complete without exchanging element matrices (cells on a slab boundary are computed by both
+  ranks); its local sub-mesh holds those cells and every node they touch: the owned nodes first,
+  then the ghost nodes owned by other ranks;
+* per Newton iteration the ranks exchange the ghost values of the displacement increment (and,
+  inside the linear solve, of the search direction) with their neighbours only;
+* the conjugate-gradient solve over the owned rows needs two all-reduces per iteration.
+
+The element work of a rank is the ordinary element path (``Elements`` / ``pms_elements_*``) on its
+sub-mesh: its first ``n_owned`` block rows of K and entries of R are the owned ones.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from .mesh import Mesh
+
+
+def node_owner(mesh: Mesh, nparts: int, axis: int | None = None) -> np.ndarray:
+    """Owner rank of every node: equal-count slabs of the node coordinates along ``axis`` (default:
+    the axis of largest extent); ties keep the node order, so the result is deterministic."""
+    if nparts < 1:
+        raise ValueError("nparts must be >= 1")
+    if axis is None:
+        axis = int(np.argmax(np.ptp(mesh.coords, axis=0)))
+    order = np.argsort(mesh.coords[:, axis], kind="stable")
+    owner = np.empty(mesh.npoint, dtype=np.int32)
+    owner[order] = (np.arange(mesh.npoint, dtype=np.int64) * nparts) // mesh.npoint
+    return owner
+
+
+@dataclass
+class Shard:
+    part: int
+    nparts: int
+    nodes: np.ndarray  # global node ids: owned (ascending), then ghosts (ascending)
+    n_owned: int
+    cells: np.ndarray  # global ids of the cells computed here (ascending)
+    mesh: Mesh  # local sub-mesh over `nodes` and `cells`
+    recv: dict = field(default_factory=dict)  # rank q -> local positions of the ghosts q owns
+    send: dict = field(default_factory=dict)  # rank q -> local positions of owned nodes q needs
+
+    @property
+    def n_local(self) -> int:
+        return len(self.nodes)
+
+
+def build_shards(mesh: Mesh, owner: np.ndarray, nparts: int) -> list[Shard]:
+    """The shards of every rank (each rank may build all and keep its own: the result is the same on
+    every rank).  The ghost lists are sorted by global id on both sides, so rank p's recv[q] and
+    rank q's send[p] name the same nodes in the same order."""
+    owner = np.asarray(owner)
+    if owner.shape != (mesh.npoint,) or owner.min() < 0 or owner.max() >= nparts:
+        raise ValueError("owner must give a rank in [0, nparts) for every node")
+    shards = []
+    for p in range(nparts):
+        owned = np.flatnonzero(owner == p)
+        cells = np.flatnonzero(np.any(owner[mesh.cells] == p, axis=1))
+        used = np.unique(mesh.cells[cells])
+        ghosts = np.setdiff1d(used, owned)
+        nodes = np.concatenate([owned, ghosts])
+        g2l = np.full(mesh.npoint, -1, dtype=np.int64)
+        g2l[nodes] = np.arange(len(nodes))
+        sub = Mesh(mesh.ndim, mesh.coords[nodes], g2l[mesh.cells[cells]], mesh.kind)
+        sh = Shard(p, nparts, nodes, len(owned), cells, sub)
+        for q in np.unique(owner[ghosts]):
+            sh.recv[int(q)] = g2l[ghosts[owner[ghosts] == q]]
+        shards.append(sh)
+    for sh in shards:  # send lists: what every other rank receives from this one, in its order
+        g2l = {int(g): i for i, g in enumerate(sh.nodes[:sh.n_owned])}
+        for other in shards:
+            if sh.part in other.recv:
+                need = other.nodes[other.recv[sh.part]]
+                sh.send[other.part] = np.array([g2l[int(g)] for g in need], dtype=np.int64)
+    return shards
+
+
+def dof_index(node_positions: np.ndarray, ndim: int) -> np.ndarray:
+    """Local DOF indices (node * ndim + d) of the given local node positions."""
+    return (np.asarray(node_positions, dtype=np.int64)[:, None] * ndim + np.arange(ndim)).reshape(-1)
+
+
+class Halo:
+    """Exchange of ghost values over torch.distributed point-to-point calls (gloo on CPU, NCCL on
+    GPUs): x holds the local vector (owned DOFs first); the ghost entries are overwritten with their
+    owners' values.  Every rank posts its sends and receives in ascending neighbour order."""
+
+    def __init__(self, shard: Shard, ndim: int):
+        self.send = {q: dof_index(v, ndim) for q, v in sorted(shard.send.items())}
+        self.recv = {q: dof_index(v, ndim) for q, v in sorted(shard.recv.items())}
+
+    def exchange(self, x):
+        import torch
+        import torch.distributed as dist
+        reqs, bufs = [], {}
+        for q, idx in self.send.items():
+            reqs.append(dist.isend(x[torch.as_tensor(idx, device=x.device)].contiguous(), q))
+        for q, idx in self.recv.items():
+            bufs[q] = torch.empty(len(idx), dtype=x.dtype, device=x.device)
+            reqs.append(dist.irecv(bufs[q], q))
+        for r in reqs:
+            r.wait()
+        for q, idx in self.recv.items():
+            x[torch.as_tensor(idx, device=x.device)] = bufs[q]
+        return x
+
+
+def owned_rows(indptr: np.ndarray, indices: np.ndarray, values: np.ndarray, n_owned_dof: int):
+    """The owned rows of a local CSR matrix (the first n_owned_dof rows of the sub-mesh's K)."""
+    end = int(indptr[n_owned_dof])
+    return indptr[:n_owned_dof + 1].copy(), indices[:end].copy(), values[:end].copy()
+
+
+def _spmv(indptr, indices, values, x):
+    import torch
+    n = len(indptr) - 1
+    rows = torch.repeat_interleave(torch.arange(n, device=x.device), torch.as_tensor(np.diff(indptr), device=x.device))
+    y = torch.zeros(n, dtype=x.dtype, device=x.device)
+    y.index_add_(0, rows, torch.as_tensor(values, device=x.device) * x[torch.as_tensor(indices, device=x.device)])
+    return y
+
+
+def dist_cg(indptr, indices, values, b_owned, halo: Halo, n_local_dof: int, fixed_local: np.ndarray,
+            rtol=1e-12, max_iterations=10000):
+    """Jacobi-preconditioned CG on the owned rows of K with the prescribed DOFs eliminated (their
+    rows and columns replaced by the identity, right-hand side zero there).  indptr/indices/values:
+    the owned rows, columns in local DOF numbering; b_owned: owned right-hand side; fixed_local:
+    prescribed flags of every local DOF (owned and ghost).  Two all-reduces per iteration (r.z and
+    p.q); stops when r.z <= rtol^2 of its initial value.  Returns (x_owned, iterations)."""
+    import torch
+    import torch.distributed as dist
+    n = len(b_owned)
+    dev = b_owned.device
+    fixed_local = np.asarray(fixed_local, dtype=bool)
+    rows = np.repeat(np.arange(n), np.diff(indptr))
+    keep = ~(fixed_local[rows] | fixed_local[indices])
+    fr = np.flatnonzero(fixed_local[:n])
+    r_all = np.concatenate([rows[keep], fr])
+    c_all = np.concatenate([indices[keep], fr])
+    v_all = np.concatenate([values[keep], np.ones(len(fr))])
+    order = np.lexsort((c_all, r_all))
+    r_all, c_all, v_all = r_all[order], c_all[order], v_all[order]
+    ip = np.concatenate([[0], np.cumsum(np.bincount(r_all, minlength=n))]).astype(np.int64)
+    diag = np.zeros(n)
+    d = r_all == c_all
+    np.add.at(diag, r_all[d], v_all[d])
+    dinv = torch.as_tensor(1.0 / diag, device=dev)
+    b = b_owned.clone()
+    b[torch.as_tensor(fr, device=dev)] = 0.0
+
+    def allsum(t):
+        dist.all_reduce(t, op=dist.ReduceOp.SUM)
+        return t
+
+    x = torch.zeros(n, dtype=b.dtype, device=dev)
+    r = b.clone()
+    z = dinv * r
+    p_local = torch.zeros(n_local_dof, dtype=b.dtype, device=dev)
+    p_local[:n] = z
+    rz = allsum((r * z).sum().reshape(1))[0]
+    rz0 = float(rz)
+    it = 0
+    while it < max_iterations and float(rz) > rtol * rtol * rz0:
+        halo.exchange(p_local)
+        q = _spmv(ip, c_all, v_all, p_local)
+        pq = allsum((p_local[:n] * q).sum().reshape(1))[0]
+        alpha = rz / pq
+        x += alpha * p_local[:n]
+        r -= alpha * q
+        z = dinv * r
+        rz_new = allsum((r * z).sum().reshape(1))[0]
+        p_local[:n] = z + (rz_new / rz) * p_local[:n]
+        rz = rz_new
+        it += 1
+    return x, it

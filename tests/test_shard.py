@@ -1,0 +1,159 @@
+"""One problem sharded over ranks (pmsim_b200/shard.py), on the CPU: the owner-computes partition
+gives every rank complete rows of K and R (checked against the whole-mesh assembly, with the oracle
+standing in for the element calls), the halo lists of both sides agree, and the distributed CG over
+two gloo ranks reproduces the single-process solution."""
+import os
+import socket
+
+import numpy as np
+import pytest
+import torch.multiprocessing as mp
+
+import oracle
+from pmsim_b200 import shard as S
+from pmsim_b200.mesh import HEX8, QUA4, QUA8, structured_2d, structured_3d
+
+E, NU, H, Z0 = 1e4, 0.3, 500.0, 9.0
+
+
+def _mesh(kind):
+    m = structured_3d(HEX8, 3, 2, 4, 1.0, 1.0, 2.0) if kind == HEX8 else structured_2d(kind, 6, 4, 3.0, 2.0)
+    rng = np.random.default_rng(kind)
+    inner = np.all((m.coords > 1e-9) & (m.coords < m.coords.max(axis=0) - 1e-9), axis=1)
+    m.coords[inner] += rng.uniform(-0.05, 0.05, (inner.sum(), m.ndim))
+    return m
+
+
+def _plastic_ddu(m, seed):
+    rng = np.random.default_rng(seed)
+    x = m.coords
+    u = np.zeros((m.npoint, m.ndim))
+    u[:, -1] = -0.004 * x[:, -1] * (1.0 + np.sin(2.0 * x[:, 0]))
+    u += rng.normal(0.0, 2e-4, u.shape)
+    return u.reshape(-1)
+
+
+@pytest.mark.parametrize("kind,nparts", [(QUA8, 2), (QUA8, 3), (QUA4, 4), (HEX8, 2), (HEX8, 3)])
+def test_owned_rows_equal_the_whole_mesh_rows(kind, nparts):
+    m = _mesh(kind)
+    nd = m.ndim
+    owner = S.node_owner(m, nparts)
+    shards = S.build_shards(m, owner, nparts)
+    assert np.array_equal(np.sort(np.concatenate([s.nodes[:s.n_owned] for s in shards])), np.arange(m.npoint))
+    prm = oracle.Params(E, NU, H, Z0)
+    ddu = _plastic_ddu(m, kind + nparts)
+    glob = oracle.OracleElements(m, oracle.MODEL_VON_MISES, prm, sym_tol=-1.0)
+    glob.initialize()
+    glob.update_secondary_values(ddu)
+    assert glob.elastic.min() == 0  # plastic IPs present
+    gp, gi, gv = glob.assemble_kk_csr()
+    gf = glob.assemble_f_int()
+    for s in shards:
+        # every cell touching an owned node is computed here
+        touch = np.flatnonzero(np.any(owner[m.cells] == s.part, axis=1))
+        assert np.array_equal(touch, s.cells)
+        loc = oracle.OracleElements(s.mesh, oracle.MODEL_VON_MISES, prm, sym_tol=-1.0)
+        loc.initialize()
+        loc.update_secondary_values(ddu.reshape(-1, nd)[s.nodes].reshape(-1))
+        lp, li, lv = loc.assemble_kk_csr()
+        lf = loc.assemble_f_int()
+        dof_g = S.dof_index(s.nodes, nd)  # local DOF -> global DOF
+        n_own = s.n_owned * nd
+        np.testing.assert_allclose(lf[:n_own], gf[dof_g[:n_own]], rtol=0, atol=1e-12 * np.abs(gf).max())
+        op, oi, ov = S.owned_rows(lp, li, lv, n_own)
+        scale = np.abs(gv).max()
+        for r in range(n_own):
+            g = dof_g[r]
+            want = dict(zip(gi[gp[g]:gp[g + 1]], gv[gp[g]:gp[g + 1]]))
+            got = dict(zip(dof_g[oi[op[r]:op[r + 1]]], ov[op[r]:op[r + 1]]))
+            assert set(got) == set(want), (s.part, r)
+            assert max(abs(got[c] - want[c]) for c in want) <= 1e-13 * scale
+    # halo lists: rank p receives from q exactly what q sends to p, in the same order
+    for p in shards:
+        for q, pos in p.recv.items():
+            assert np.array_equal(p.nodes[pos], shards[q].nodes[shards[q].send[p.part]])
+            assert np.all(owner[p.nodes[pos]] == q)
+
+
+def _free_port():
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    port = s.getsockname()[1]
+    s.close()
+    return port
+
+
+def _problem():
+    """Linear elastic Qua4 plate 8x6, bottom fixed, a parabolic downward load on the top nodes."""
+    m = structured_2d(QUA4, 8, 6, 4.0, 3.0)
+    fixed = np.zeros(m.ndof, dtype=bool)
+    bottom = m.points_where(lambda x, y: np.abs(y) < 1e-9)
+    fixed[S.dof_index(bottom, 2)] = True
+    f = np.zeros(m.ndof)
+    top = m.points_where(lambda x, y: np.abs(y - 3.0) < 1e-9)
+    f[2 * top + 1] = -1.0 - 0.1 * m.coords[top, 0] ** 2
+    return m, fixed, f
+
+
+def _cg_rank(rank, ws, port, q):
+    os.environ.update({"MASTER_ADDR": "127.0.0.1", "MASTER_PORT": str(port), "WORLD_SIZE": str(ws),
+                       "RANK": str(rank), "LOCAL_RANK": str(rank)})
+    import torch
+    from pmsim_b200 import dist
+    dist.init("gloo", timeout_s=60)
+    try:
+        m, fixed, f = _problem()
+        shards = S.build_shards(m, S.node_owner(m, ws), ws)
+        s = shards[rank]
+        loc = oracle.OracleElements(s.mesh, oracle.MODEL_LINEAR_ELASTIC, oracle.Params(E, NU, 0.0, 1.0), sym_tol=-1.0)
+        loc.initialize()
+        lp, li, lv = loc.assemble_kk_csr()
+        dof = S.dof_index(s.nodes, 2)
+        n_own = s.n_owned * 2
+        op, oi, ov = S.owned_rows(lp, li, lv, n_own)
+        halo = S.Halo(s, 2)
+        # the halo exchange returns the owners' values
+        xg = np.arange(m.ndof, dtype=np.float64) * 0.5 + 1.0
+        xl = torch.zeros(len(dof), dtype=torch.float64)
+        xl[:n_own] = torch.as_tensor(xg[dof[:n_own]])
+        halo.exchange(xl)
+        halo_ok = bool(np.array_equal(xl.numpy(), xg[dof]))
+        x, it = S.dist_cg(op, oi, ov, torch.as_tensor(f[dof[:n_own]]), halo, len(dof), fixed[dof], rtol=1e-13)
+        q.put((rank, halo_ok, it, dof[:n_own], x.numpy()))
+    finally:
+        dist.finalize()
+
+
+@pytest.mark.timeout(180)
+def test_distributed_cg_over_two_gloo_ranks():
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_cg_rank, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    out = [q.get(timeout=150) for _ in procs]
+    for p in procs:
+        p.join(timeout=60)
+    # the single-process solution (oracle K, prescribed DOFs eliminated)
+    import scipy.sparse as sp
+    import scipy.sparse.linalg as spla
+    m, fixed, f = _problem()
+    el = oracle.OracleElements(m, oracle.MODEL_LINEAR_ELASTIC, oracle.Params(E, NU, 0.0, 1.0), sym_tol=-1.0)
+    el.initialize()
+    gp, gi, gv = el.assemble_kk_csr()
+    K = sp.csr_matrix((gv, gi, gp), shape=(m.ndof, m.ndof)).tocsc()
+    free = ~fixed
+    u = np.zeros(m.ndof)
+    u[free] = spla.spsolve(K[free][:, free], f[free])
+    got = np.zeros(m.ndof)
+    seen = np.zeros(m.ndof, dtype=bool)
+    iters = set()
+    for rank, halo_ok, it, dofs, x in out:
+        assert halo_ok, rank
+        got[dofs] = x
+        seen[dofs] = True
+        iters.add(it)
+    assert seen.all()
+    assert len(iters) == 1  # every rank takes the same number of iterations (the reductions are global)
+    np.testing.assert_allclose(got, u, rtol=0, atol=1e-9 * np.abs(u).max())
