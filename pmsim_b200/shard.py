@@ -182,3 +182,86 @@ def dist_cg(indptr, indices, values, b_owned, halo: Halo, n_local_dof: int, fixe
         rz = rz_new
         it += 1
     return x, it
+
+
+def _call(el, *names):
+    for n in names:
+        f = getattr(el, n, None)
+        if f is not None:
+            return f
+    raise AttributeError(names[0])
+
+
+def _local_kk(el):
+    if hasattr(el, "assemble_kk_csr"):
+        return el.assemble_kk_csr()
+    indptr, indices = el.csr_pattern()
+    return np.asarray(indptr), np.asarray(indices), np.asarray(el.assemble_kk())
+
+
+def dist_newton(shard: Shard, ndim: int, elements, fixed_local, ff_ext_owned, nsteps, n_max_iterations=10,
+                tol_rr_abs=1e-10, tol_mdu_rel=1e-8, cg_rtol=1e-13, on_step=None):
+    """The reference's implicit Newton loop (src/fem/solver_implicit.rs:187-272) in its reduced-system
+    form (zero prescribed values, src/fem/bc_prescribed.rs:153-157) over the ranks of a sharded
+    problem.  ``elements`` runs the element calls on this rank's sub-mesh (the device ``Elements``
+    or any object with the same calls); ``ff_ext_owned(t)`` gives F_ext on the owned DOFs.
+    Per iteration: R on the owned rows, max|R| over all ranks, K's owned rows, the correction by
+    ``dist_cg``, rel(mdu) over all ranks, the owned dU update and the ghost exchange of dU before
+    the stress update.  Returns the per-step histories [(iteration, max|R|, rel(mdu))...] and the
+    owned displacements."""
+    import torch
+    import torch.distributed as dist
+    nl = shard.n_local * ndim
+    n = shard.n_owned * ndim
+    fixed_local = np.asarray(fixed_local, dtype=bool)
+    fixed_own = fixed_local[:n]
+    halo = Halo(shard, ndim)
+
+    def allmax(x):
+        t = torch.tensor([float(x)], dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t[0])
+
+    _call(elements, "initialize_internal_values", "initialize")()
+    u = np.zeros(n)
+    histories = []
+    for step in range(1, nsteps + 1):
+        t = float(step)
+        ddu = torch.zeros(nl, dtype=torch.float64)
+        elements.reset_algorithmic_variables()
+        ffe = np.where(fixed_own, 0.0, np.asarray(ff_ext_owned(t), dtype=np.float64))
+        hist, mdu0 = [], None
+        for it in range(n_max_iterations):
+            fi = np.asarray(elements.assemble_f_int())[:n]
+            rr = np.where(fixed_own, 0.0, fi) - ffe
+            norm_rr = allmax(np.max(np.abs(rr)) if n else 0.0)
+            if not np.isfinite(norm_rr):
+                raise FloatingPointError("Found NaN or Inf")
+            if norm_rr < tol_rr_abs:
+                hist.append((it, norm_rr, None))
+                break
+            op, oi, ov = owned_rows(*_local_kk(elements), n)
+            mdu, _ = dist_cg(op, oi, ov, torch.as_tensor(rr), halo, nl, fixed_local, rtol=cg_rtol)
+            mdu = mdu.numpy()
+            if it == 0:
+                mdu0, rel = mdu.copy(), 1.0
+            else:
+                rel = allmax(np.max(np.abs(mdu) / (1.0 + np.abs(mdu0))) if n else 0.0)
+            hist.append((it, norm_rr, rel))
+            if it > 0 and rel < tol_mdu_rel:
+                break
+            free = ~fixed_own
+            u[free] -= mdu[free]
+            ddu[:n][torch.as_tensor(free)] -= torch.as_tensor(mdu[free])
+            halo.exchange(ddu)
+            if it == 0:
+                elements.backup_secondary_values()
+            else:
+                elements.restore_secondary_values()
+            elements.update_secondary_values(ddu.numpy())
+            if it == n_max_iterations - 1:
+                raise RuntimeError("Newton-Raphson did not converge")
+        histories.append(hist)
+        if on_step is not None:
+            on_step(step - 1, t, u.copy(), elements)
+    return histories, u

@@ -157,3 +157,57 @@ def test_distributed_cg_over_two_gloo_ranks():
     assert seen.all()
     assert len(iters) == 1  # every rank takes the same number of iterations (the reductions are global)
     np.testing.assert_allclose(got, u, rtol=0, atol=1e-9 * np.abs(u).max())
+
+
+def _newton_rank(rank, ws, port, q):
+    os.environ.update({"MASTER_ADDR": "127.0.0.1", "MASTER_PORT": str(port), "WORLD_SIZE": str(ws),
+                       "RANK": str(rank), "LOCAL_RANK": str(rank)})
+    import problems
+    from pmsim_b200 import dist
+    dist.init("gloo", timeout_s=120)
+    try:
+        pb = problems.pres_cylin_751()
+        m = pb["mesh"]
+        fixed = np.zeros(m.ndof, dtype=bool)
+        fixed[[e[0] for e in pb["essential"]]] = True
+        s = S.build_shards(m, S.node_owner(m, ws), ws)[rank]
+        dof = S.dof_index(s.nodes, 2)
+        n_own = s.n_owned * 2
+        el = oracle.OracleElements(s.mesh, oracle.MODEL_VON_MISES, oracle.Params(*pb["params"]), ngauss=4,
+                                   sym_tol=-1.0)
+        steps = []
+        hist, u = S.dist_newton(s, 2, el, fixed[dof], lambda t: pb["natural"].ff_ext(t)[dof[:n_own]], pb["nsteps"],
+                                tol_mdu_rel=1e-10,
+                                on_step=lambda k, t, u, e: steps.append((u.copy(), e.sig.copy())))
+        q.put((rank, [len(h) for h in hist], dof[:n_own], s.cells, steps))
+    finally:
+        dist.finalize()
+
+
+@pytest.mark.timeout(240)
+def test_sharded_newton_replays_spo_751_over_two_gloo_ranks():
+    """The reference's Newton loop over two ranks (owner-computes rows, dU halo exchange,
+    distributed CG) on the SPO 7.5.1 pressurised cylinder (von Mises, reduced-system method,
+    internal pressure): every step's displacements and IP stresses at the tolerances of the
+    single-process replay, and pmsim's own logged Newton iteration counts."""
+    import problems
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_newton_rank, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    out = [q.get(timeout=200) for _ in procs]
+    for p in procs:
+        p.join(timeout=60)
+    pb = problems.pres_cylin_751()
+    m = pb["mesh"]
+    g = pb["golden"]
+    for rank, iters, dofs, cells, steps in out:
+        assert iters == pb["iterations"], (rank, iters)
+        for k, (u, sig) in enumerate(steps):
+            gu = g["displacement"][k].reshape(-1)
+            assert np.max(np.abs(u - gu[dofs])) <= pb["tol_u"], (rank, k)
+            gs = np.array(g["stresses"][k], dtype=float)[cells]
+            gs[..., 3:] *= np.sqrt(2.0)
+            assert np.max(np.abs(sig.reshape(gs.shape) - gs)) <= pb["tol_s"], (rank, k)
