@@ -125,11 +125,13 @@ def _cg_rank(rank, ws, port, q):
 
 
 @pytest.mark.timeout(180)
-def test_distributed_cg_over_two_gloo_ranks():
+@pytest.mark.parametrize("ws", [2, 3])
+def test_distributed_cg_over_gloo_ranks(ws):
+    """Two ranks (one neighbour each) and three (the middle rank exchanges with two)."""
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
     port = _free_port()
-    procs = [ctx.Process(target=_cg_rank, args=(r, 2, port, q)) for r in range(2)]
+    procs = [ctx.Process(target=_cg_rank, args=(r, ws, port, q)) for r in range(ws)]
     for p in procs:
         p.start()
     out = [q.get(timeout=150) for _ in procs]
