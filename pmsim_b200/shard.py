@@ -200,15 +200,16 @@ def _local_kk(el):
 
 
 def dist_newton(shard: Shard, ndim: int, elements, fixed_local, ff_ext_owned, nsteps, n_max_iterations=10,
-                tol_rr_abs=1e-10, tol_mdu_rel=1e-8, cg_rtol=1e-13, on_step=None):
+                tol_rr_abs=1e-10, tol_mdu_rel=1e-8, cg_rtol=1e-13, on_step=None, device="cpu"):
     """The reference's implicit Newton loop (src/fem/solver_implicit.rs:187-272) in its reduced-system
     form (zero prescribed values, src/fem/bc_prescribed.rs:153-157) over the ranks of a sharded
     problem.  ``elements`` runs the element calls on this rank's sub-mesh (the device ``Elements``
     or any object with the same calls); ``ff_ext_owned(t)`` gives F_ext on the owned DOFs.
     Per iteration: R on the owned rows, max|R| over all ranks, K's owned rows, the correction by
     ``dist_cg``, rel(mdu) over all ranks, the owned dU update and the ghost exchange of dU before
-    the stress update.  Returns the per-step histories [(iteration, max|R|, rel(mdu))...] and the
-    owned displacements."""
+    the stress update.  ``device`` holds the vectors that cross ranks ("cpu" for gloo, the rank's
+    CUDA device for NCCL).  Returns the per-step histories [(iteration, max|R|, rel(mdu))...] and
+    the owned displacements."""
     import torch
     import torch.distributed as dist
     nl = shard.n_local * ndim
@@ -218,7 +219,7 @@ def dist_newton(shard: Shard, ndim: int, elements, fixed_local, ff_ext_owned, ns
     halo = Halo(shard, ndim)
 
     def allmax(x):
-        t = torch.tensor([float(x)], dtype=torch.float64)
+        t = torch.tensor([float(x)], dtype=torch.float64, device=device)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t[0])
 
@@ -227,7 +228,7 @@ def dist_newton(shard: Shard, ndim: int, elements, fixed_local, ff_ext_owned, ns
     histories = []
     for step in range(1, nsteps + 1):
         t = float(step)
-        ddu = torch.zeros(nl, dtype=torch.float64)
+        ddu = torch.zeros(nl, dtype=torch.float64, device=device)
         elements.reset_algorithmic_variables()
         ffe = np.where(fixed_own, 0.0, np.asarray(ff_ext_owned(t), dtype=np.float64))
         hist, mdu0 = [], None
@@ -241,8 +242,8 @@ def dist_newton(shard: Shard, ndim: int, elements, fixed_local, ff_ext_owned, ns
                 hist.append((it, norm_rr, None))
                 break
             op, oi, ov = owned_rows(*_local_kk(elements), n)
-            mdu, _ = dist_cg(op, oi, ov, torch.as_tensor(rr), halo, nl, fixed_local, rtol=cg_rtol)
-            mdu = mdu.numpy()
+            mdu, _ = dist_cg(op, oi, ov, torch.as_tensor(rr, device=device), halo, nl, fixed_local, rtol=cg_rtol)
+            mdu = mdu.cpu().numpy()
             if it == 0:
                 mdu0, rel = mdu.copy(), 1.0
             else:
@@ -252,13 +253,13 @@ def dist_newton(shard: Shard, ndim: int, elements, fixed_local, ff_ext_owned, ns
                 break
             free = ~fixed_own
             u[free] -= mdu[free]
-            ddu[:n][torch.as_tensor(free)] -= torch.as_tensor(mdu[free])
+            ddu[:n][torch.as_tensor(free, device=device)] -= torch.as_tensor(mdu[free], device=device)
             halo.exchange(ddu)
             if it == 0:
                 elements.backup_secondary_values()
             else:
                 elements.restore_secondary_values()
-            elements.update_secondary_values(ddu.numpy())
+            elements.update_secondary_values(ddu.cpu().numpy())
             if it == n_max_iterations - 1:
                 raise RuntimeError("Newton-Raphson did not converge")
         histories.append(hist)
