@@ -97,20 +97,30 @@ class Halo:
     def __init__(self, shard: Shard, ndim: int):
         self.send = {q: dof_index(v, ndim) for q, v in sorted(shard.send.items())}
         self.recv = {q: dof_index(v, ndim) for q, v in sorted(shard.recv.items())}
+        self._dev = {}  # device -> (send, recv) index tensors
+
+    def _index(self, device):
+        import torch
+        key = str(device)
+        if key not in self._dev:
+            self._dev[key] = ({q: torch.as_tensor(i, device=device) for q, i in self.send.items()},
+                              {q: torch.as_tensor(i, device=device) for q, i in self.recv.items()})
+        return self._dev[key]
 
     def exchange(self, x):
         import torch
         import torch.distributed as dist
+        send, recv = self._index(x.device)
         reqs, bufs = [], {}
-        for q, idx in self.send.items():
-            reqs.append(dist.isend(x[torch.as_tensor(idx, device=x.device)].contiguous(), q))
-        for q, idx in self.recv.items():
+        for q, idx in send.items():
+            reqs.append(dist.isend(x[idx].contiguous(), q))
+        for q, idx in recv.items():
             bufs[q] = torch.empty(len(idx), dtype=x.dtype, device=x.device)
             reqs.append(dist.irecv(bufs[q], q))
         for r in reqs:
             r.wait()
-        for q, idx in self.recv.items():
-            x[torch.as_tensor(idx, device=x.device)] = bufs[q]
+        for q, idx in recv.items():
+            x[idx] = bufs[q]
         return x
 
 
@@ -120,12 +130,10 @@ def owned_rows(indptr: np.ndarray, indices: np.ndarray, values: np.ndarray, n_ow
     return indptr[:n_owned_dof + 1].copy(), indices[:end].copy(), values[:end].copy()
 
 
-def _spmv(indptr, indices, values, x):
-    import torch
-    n = len(indptr) - 1
-    rows = torch.repeat_interleave(torch.arange(n, device=x.device), torch.as_tensor(np.diff(indptr), device=x.device))
-    y = torch.zeros(n, dtype=x.dtype, device=x.device)
-    y.index_add_(0, rows, torch.as_tensor(values, device=x.device) * x[torch.as_tensor(indices, device=x.device)])
+def _spmv(rows, cols, vals, n, x):
+    """y = A x for A in coordinate form (row-sorted tensors on x's device)."""
+    y = x.new_zeros(n)
+    y.index_add_(0, rows, vals * x[cols])
     return y
 
 
@@ -149,11 +157,13 @@ def dist_cg(indptr, indices, values, b_owned, halo: Halo, n_local_dof: int, fixe
     v_all = np.concatenate([values[keep], np.ones(len(fr))])
     order = np.lexsort((c_all, r_all))
     r_all, c_all, v_all = r_all[order], c_all[order], v_all[order]
-    ip = np.concatenate([[0], np.cumsum(np.bincount(r_all, minlength=n))]).astype(np.int64)
     diag = np.zeros(n)
     d = r_all == c_all
     np.add.at(diag, r_all[d], v_all[d])
     dinv = torch.as_tensor(1.0 / diag, device=dev)
+    t_rows = torch.as_tensor(r_all, device=dev)
+    t_cols = torch.as_tensor(c_all, device=dev)
+    t_vals = torch.as_tensor(v_all, device=dev)
     b = b_owned.clone()
     b[torch.as_tensor(fr, device=dev)] = 0.0
 
@@ -171,7 +181,7 @@ def dist_cg(indptr, indices, values, b_owned, halo: Halo, n_local_dof: int, fixe
     it = 0
     while it < max_iterations and float(rz) > rtol * rtol * rz0:
         halo.exchange(p_local)
-        q = _spmv(ip, c_all, v_all, p_local)
+        q = _spmv(t_rows, t_cols, t_vals, n, p_local)
         pq = allsum((p_local[:n] * q).sum().reshape(1))[0]
         alpha = rz / pq
         x += alpha * p_local[:n]
