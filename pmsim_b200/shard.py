@@ -210,11 +210,20 @@ def _local_kk(el):
 
 
 def dist_newton(shard: Shard, ndim: int, elements, fixed_local, ff_ext_owned, nsteps, n_max_iterations=10,
-                tol_rr_abs=1e-10, tol_mdu_rel=1e-8, cg_rtol=1e-13, on_step=None, device="cpu"):
-    """The reference's implicit Newton loop (src/fem/solver_implicit.rs:187-272) in its reduced-system
-    form (zero prescribed values, src/fem/bc_prescribed.rs:153-157) over the ranks of a sharded
-    problem.  ``elements`` runs the element calls on this rank's sub-mesh (the device ``Elements``
-    or any object with the same calls); ``ff_ext_owned(t)`` gives F_ext on the owned DOFs.
+                tol_rr_abs=1e-10, tol_mdu_rel=1e-8, cg_rtol=1e-13, on_step=None, device="cpu",
+                prescribed_local=None):
+    """The reference's implicit Newton loop (src/fem/solver_implicit.rs:187-272) over the ranks of a
+    sharded problem.  ``elements`` runs the element calls on this rank's sub-mesh (the device
+    ``Elements`` or any object with the same calls); ``ff_ext_owned(t)`` gives F_ext on the owned
+    DOFs; ``fixed_local`` flags the prescribed DOFs of every local DOF.
+
+    * ``prescribed_local`` None: reduced-system form with zero prescribed values
+      (src/fem/bc_prescribed.rs:153-157).
+    * ``prescribed_local(t)`` -> values at the local DOFs: Lagrange multipliers
+      (src/fem/bc_prescribed.rs:99-134), solved by elimination, which gives the augmented direct
+      solve's iterates: mdu_p = u_p - c, K_ff mdu_f = R_f - K_fp mdu_p, mdl = (R_p + l) - (K mdu)_p.
+      The residual and rel(mdu) include the multiplier rows, as in the reference.
+
     Per iteration: R on the owned rows, max|R| over all ranks, K's owned rows, the correction by
     ``dist_cg``, rel(mdu) over all ranks, the owned dU update and the ghost exchange of dU before
     the stress update.  ``device`` holds the vectors that cross ranks ("cpu" for gloo, the rank's
@@ -226,6 +235,8 @@ def dist_newton(shard: Shard, ndim: int, elements, fixed_local, ff_ext_owned, ns
     n = shard.n_owned * ndim
     fixed_local = np.asarray(fixed_local, dtype=bool)
     fixed_own = fixed_local[:n]
+    pres = np.flatnonzero(fixed_own)  # owned prescribed DOFs (one multiplier each in LMM form)
+    lmm = prescribed_local is not None
     halo = Halo(shard, ndim)
 
     def allmax(x):
@@ -233,37 +244,70 @@ def dist_newton(shard: Shard, ndim: int, elements, fixed_local, ff_ext_owned, ns
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t[0])
 
+    def kmul(rows, v_local):
+        """(K v) on the owned rows for a local vector v (its ghost values exchanged first)."""
+        vt = torch.as_tensor(v_local, device=device).clone()
+        halo.exchange(vt)
+        op, oi, ov = rows
+        return np.bincount(np.repeat(np.arange(n), np.diff(op)), weights=ov * vt.cpu().numpy()[oi], minlength=n)
+
     _call(elements, "initialize_internal_values", "initialize")()
     u = np.zeros(n)
+    lam = np.zeros(len(pres))
     histories = []
     for step in range(1, nsteps + 1):
         t = float(step)
         ddu = torch.zeros(nl, dtype=torch.float64, device=device)
         elements.reset_algorithmic_variables()
-        ffe = np.where(fixed_own, 0.0, np.asarray(ff_ext_owned(t), dtype=np.float64))
+        ffe = np.asarray(ff_ext_owned(t), dtype=np.float64)
+        if not lmm:
+            ffe = np.where(fixed_own, 0.0, ffe)
+        c = np.asarray(prescribed_local(t), dtype=np.float64)[:n][pres] if lmm else None
         hist, mdu0 = [], None
         for it in range(n_max_iterations):
             fi = np.asarray(elements.assemble_f_int())[:n]
-            rr = np.where(fixed_own, 0.0, fi) - ffe
-            norm_rr = allmax(np.max(np.abs(rr)) if n else 0.0)
+            if lmm:
+                rr = fi - ffe
+                rr[pres] += lam
+                rr_p = u[pres] - c
+                norm_own = max(np.max(np.abs(rr)) if n else 0.0, np.max(np.abs(rr_p)) if len(pres) else 0.0)
+            else:
+                rr = np.where(fixed_own, 0.0, fi) - ffe
+                norm_own = np.max(np.abs(rr)) if n else 0.0
+            norm_rr = allmax(norm_own)
             if not np.isfinite(norm_rr):
                 raise FloatingPointError("Found NaN or Inf")
             if norm_rr < tol_rr_abs:
                 hist.append((it, norm_rr, None))
                 break
-            op, oi, ov = owned_rows(*_local_kk(elements), n)
-            mdu, _ = dist_cg(op, oi, ov, torch.as_tensor(rr, device=device), halo, nl, fixed_local, rtol=cg_rtol)
-            mdu = mdu.cpu().numpy()
-            if it == 0:
-                mdu0, rel = mdu.copy(), 1.0
+            rows = owned_rows(*_local_kk(elements), n)
+            if lmm:
+                vp = np.zeros(nl)
+                vp[pres] = rr_p  # mdu on the prescribed DOFs
+                b = rr - kmul(rows, vp)
+                mdu_f, _ = dist_cg(*rows, torch.as_tensor(b, device=device), halo, nl, fixed_local, rtol=cg_rtol)
+                mdu = mdu_f.cpu().numpy()
+                mdu[pres] = rr_p
+                full = np.zeros(nl)
+                full[:n] = mdu
+                mdl = rr[pres] - kmul(rows, full)[pres]
+                mvec = np.concatenate([mdu, mdl])
             else:
-                rel = allmax(np.max(np.abs(mdu) / (1.0 + np.abs(mdu0))) if n else 0.0)
+                mdu_t, _ = dist_cg(*rows, torch.as_tensor(rr, device=device), halo, nl, fixed_local, rtol=cg_rtol)
+                mdu = mdu_t.cpu().numpy()
+                mvec = mdu
+            if it == 0:
+                mdu0, rel = mvec.copy(), 1.0
+            else:
+                rel = allmax(np.max(np.abs(mvec) / (1.0 + np.abs(mdu0))) if len(mvec) else 0.0)
             hist.append((it, norm_rr, rel))
             if it > 0 and rel < tol_mdu_rel:
                 break
-            free = ~fixed_own
-            u[free] -= mdu[free]
-            ddu[:n][torch.as_tensor(free, device=device)] -= torch.as_tensor(mdu[free], device=device)
+            upd = np.ones(n, dtype=bool) if lmm else ~fixed_own
+            u[upd] -= mdu[upd]
+            if lmm:
+                lam -= mdl
+            ddu[:n][torch.as_tensor(upd, device=device)] -= torch.as_tensor(mdu[upd], device=device)
             halo.exchange(ddu)
             if it == 0:
                 elements.backup_secondary_values()

@@ -101,6 +101,7 @@ def _cg_rank(rank, ws, port, q):
     import torch
     from pmsim_b200 import dist
     dist.init("gloo", timeout_s=60)
+    torch.set_num_threads(1)  # two ranks share the cores
     try:
         m, fixed, f = _problem()
         shards = S.build_shards(m, S.node_owner(m, ws), ws)
@@ -199,11 +200,13 @@ class _DeviceStyle:
 
 
 def _newton_rank(rank, ws, port, q):
+    import torch
     os.environ.update({"MASTER_ADDR": "127.0.0.1", "MASTER_PORT": str(port), "WORLD_SIZE": str(ws),
                        "RANK": str(rank), "LOCAL_RANK": str(rank)})
     import problems
     from pmsim_b200 import dist
     dist.init("gloo", timeout_s=120)
+    torch.set_num_threads(1)  # two ranks share the cores
     try:
         pb = problems.pres_cylin_751()
         m = pb["mesh"]
@@ -253,3 +256,70 @@ def test_sharded_newton_replays_spo_751_over_two_gloo_ranks():
             gs = np.array(g["stresses"][k], dtype=float)[cells]
             gs[..., 3:] *= np.sqrt(2.0)
             assert np.max(np.abs(sig.reshape(gs.shape) - gs)) <= pb["tol_s"], (rank, k)
+
+
+def _footing_rank(rank, ws, port, q):
+    import torch
+    os.environ.update({"MASTER_ADDR": "127.0.0.1", "MASTER_PORT": str(port), "WORLD_SIZE": str(ws),
+                       "RANK": str(rank), "LOCAL_RANK": str(rank)})
+    from pmsim_b200 import dist
+    from pmsim_b200.footing import footing_problem
+    dist.init("gloo", timeout_s=120)
+    torch.set_num_threads(1)  # two ranks share the cores
+    try:
+        p = footing_problem(20, 10, 1e4, 9.0, 1.0, nsteps=10)
+        m = p.mesh
+        ess = {int(e[0]): e for e in p.essential}  # a later entry for the same equation wins
+        fixed = np.zeros(m.ndof, dtype=bool)
+        fixed[list(ess)] = True
+
+        def values(t):
+            c = np.zeros(m.ndof)
+            for eq, (_, const, fn) in ess.items():
+                c[eq] = const * fn(t) if fn is not None else const
+            return c
+
+        s = S.build_shards(m, S.node_owner(m, ws), ws)[rank]
+        dof = S.dof_index(s.nodes, 2)
+        n_own = s.n_owned * 2
+        mt = p.material
+        el = oracle.OracleElements(s.mesh, oracle.MODEL_VON_MISES, oracle.Params(mt.young, mt.poisson, mt.hh, mt.z_ini),
+                                   ngauss=9, sym_tol=-1.0)
+        steps = []
+        hist, _ = S.dist_newton(s, 2, el, fixed[dof], lambda t: np.zeros(n_own), 10, n_max_iterations=20,
+                                prescribed_local=lambda t: values(t)[dof],
+                                on_step=lambda k, t, u, e: steps.append(u.copy()))
+        q.put((rank, [len(h) for h in hist], dof[:n_own], steps))
+    finally:
+        dist.finalize()
+
+
+@pytest.mark.timeout(300)
+def test_sharded_newton_with_multipliers_replays_the_footing():
+    """Lagrange multipliers over two ranks: the 20x10 Qua8 footing (9 IP, von Mises, prescribed
+    indentation, the reference's CPU-runnable configuration) takes the single-process oracle's Newton
+    counts at every step (7,7,6,6,6,7,7,5,5,5) and its displacements within 1e-9 of the largest."""
+    from oracle.driver import OracleSolver
+    from pmsim_b200.footing import footing_problem
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_footing_rank, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    out = [q.get(timeout=280) for _ in procs]
+    for p in procs:
+        p.join(timeout=60)
+    p = footing_problem(20, 10, 1e4, 9.0, 1.0, nsteps=10)
+    mt = p.material
+    oel = oracle.OracleElements(p.mesh, oracle.MODEL_VON_MISES, oracle.Params(mt.young, mt.poisson, mt.hh, mt.z_ini),
+                                ngauss=9, sym_tol=-1.0)
+    ref = []
+    osol = OracleSolver(oel, p.mesh.ndof, p.essential, n_max_iterations=20, t_fin=10.0)
+    osol.solve(lambda k, t, u, e: ref.append(u.copy()))
+    want = [len(h) for h in osol.history]
+    assert want == [7, 7, 6, 6, 6, 7, 7, 5, 5, 5]
+    for rank, iters, dofs, steps in out:
+        assert iters == want, (rank, iters)
+        for k, u in enumerate(steps):
+            assert np.max(np.abs(u - ref[k][dofs])) <= 1e-9 * np.abs(ref[k]).max(), (rank, k)
