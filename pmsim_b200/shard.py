@@ -161,8 +161,8 @@ def dist_cg(indptr, indices, values, b_owned, halo: Halo, n_local_dof: int, fixe
     d = r_all == c_all
     np.add.at(diag, r_all[d], v_all[d])
     dinv = torch.as_tensor(1.0 / diag, device=dev)
-    t_rows = torch.as_tensor(r_all, device=dev)
-    t_cols = torch.as_tensor(c_all, device=dev)
+    t_rows = torch.as_tensor(r_all.astype(np.int64), device=dev)
+    t_cols = torch.as_tensor(c_all.astype(np.int64), device=dev)  # the device pattern is int32
     t_vals = torch.as_tensor(v_all, device=dev)
     b = b_owned.clone()
     b[torch.as_tensor(fr, device=dev)] = 0.0
