@@ -189,7 +189,7 @@ class _DeviceStyle:
 
     def csr_pattern(self):
         ip, ix, _ = self.el.assemble_kk_csr()
-        return ip, ix
+        return ip, ix.astype(np.int32)  # the device pattern's column type
 
     def assemble_kk(self):
         return self.el.assemble_kk_csr()[2]
