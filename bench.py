@@ -56,6 +56,12 @@ def parse():
     ap.add_argument("--no-qua8", action="store_true")
     ap.add_argument("--qua8-n", type=int, default=1024, help="Qua8 mesh of n x n cells for the memory-bound step")
     ap.add_argument("--served-detail", default="", help="write per-request served records (JSON) to this file")
+    ap.add_argument("--pcg-time", nargs="+", default=None, metavar="ARG",
+                    help="only time the PCG engines on one problem: ENGINE PROBLEM DIMS... with ENGINE team|wide "
+                         "and PROBLEM foot (nx ny Qua8 footing) | hex (nx ny nz Hex8 block)")
+    ap.add_argument("--pcg-chunks", type=int, default=0, help="--pcg-time: 128-node chunks per team CTA (0: all fit)")
+    ap.add_argument("--pcg-threads", type=int, default=1024, help="--pcg-time: threads per team CTA")
+    ap.add_argument("--pcg-iterations", type=int, default=64, help="--pcg-time: PCG iterations timed")
     return ap.parse_args()
 
 
@@ -100,9 +106,9 @@ def flops_per_ip_hex20():
     return 2 * fma + mul
 
 
-# DRAM bytes (read + write) of one element_kernel<3,20> launch per cell, from the ncu capture of the
-# 32x32x16 block (profiles/element_kernel_hex20_32x32x16.md: 33.6 MB read + 449.1 MB written for
-# 16,384 cells); traffic grows with the cell count, so a launch over n cells moves n times this.
+# DRAM bytes (read + write) of one element_kernel<3,20> launch per cell, from an ncu capture of the
+# 32x32x16 block (33.6 MB read + 449.1 MB written for 16,384 cells); traffic grows with the cell
+# count, so a launch over n cells moves n times this.
 ELEMENT_DRAM_BYTES_PER_CELL = (33.590272e6 + 449.112320e6) / 16384
 
 
@@ -599,6 +605,28 @@ def cpu_model():
     return "unknown"
 
 
+def pcg_time(args):
+    """--pcg-time: device time per PCG iteration of one problem on its initial tangent (unit
+    right-hand side), with the team engine (a thread-block cluster per problem) or the batch-wide
+    engine (pms_batch_time_pcg); the launch shapes of profile captures of the PCG kernels."""
+    import ctypes
+    from pmsim_b200 import _lib
+    from pmsim_b200.batch import BatchSolver
+    from pmsim_b200.footing import block_problem, footing_problem
+    engine, problem, dims = args.pcg_time[0], args.pcg_time[1], [int(v) for v in args.pcg_time[2:]]
+    if engine not in ("team", "wide") or problem not in ("foot", "hex"):
+        raise SystemExit("--pcg-time ENGINE PROBLEM DIMS: ENGINE team|wide, PROBLEM foot|hex")
+    p = footing_problem(*dims[:2]) if problem == "foot" else block_problem(*dims[:3])
+    bs = BatchSolver([p])
+    t = _lib.BatchTuning_(10 ** 12 if engine == "team" else 0, args.pcg_threads, args.pcg_chunks, 128, 8)
+    ms = ctypes.c_double()
+    rc = bs.L.pms_batch_time_pcg(bs.h, ctypes.byref(t), args.pcg_iterations, ctypes.byref(ms))
+    if rc != 0:
+        raise _lib.PmsError(rc)
+    print(f"{engine} {problem} {dims} ndof {p.mesh.ndof}: {ms.value / args.pcg_iterations * 1e3:.2f} us per iteration")
+    bs.close()
+
+
 def reference_arm(args, rank):
     """--impl reference: the reference's CPU path (oracle port; the Rust reference cannot be built
     here) on the host cores, same metric and workload, each step a bounded sample."""
@@ -638,6 +666,9 @@ def main():
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         reference_arm(args, rank)
+        return
+    if args.pcg_time:
+        pcg_time(args)
         return
     import torch
     from pmsim_b200 import dist

@@ -79,9 +79,12 @@ typedef struct pms_mesh {
 /* The Config fields the hot path reads (src/base/config.rs:19-229). */
 typedef struct pms_config {
     int32_t ngauss;        /* 0 = default rule of the kind (ParamSolid::ngauss = None) */
-    int32_t plane_stress;  /* must be 0: von Mises rejects plane stress (von_mises.rs:60-62) */
-    int32_t axisymmetric;  /* must be 0 (not implemented) */
-    double thickness;      /* Idealization::thickness, default 1.0 */
+    int32_t plane_stress;  /* Idealization::plane_stress: 2D linear-elastic materials only; with a von Mises
+                              material the call returns PMS_ERR_UNSUPPORTED, as the reference refuses it
+                              ("von Mises model does not work in plane-stress", von_mises.rs:60-62) */
+    int32_t axisymmetric;  /* Idealization::axisymmetric: 2D kinds (x = radius), any material; 3D kinds
+                              return PMS_ERR_UNSUPPORTED; cannot be combined with plane_stress */
+    double thickness;      /* Idealization::thickness, default 1.0 (ignored when axisymmetric) */
 } pms_config;
 
 typedef struct pms_elements_info {
@@ -302,9 +305,12 @@ int pms_probe_fp64_fma(int64_t iters, int32_t blocks, double* out, void* stream)
  * No counterpart in the reference: it exists for callers that cannot call cudaMalloc -- a program
  * running inside another framework that owns the whole device-memory budget, a real-time loop
  * where an allocation would stall or synchronise the GPU, or a foreign-language element loop (for
- * example Rust behind an FFI) that has no CUDA allocator.  It computes what
- * ElementTrait::calc_f_int / calc_jacobian compute, for ncell independent cells given on the
- * host:  X[ncell][nnode][ndim] coordinates; the IP state structure-of-arrays with stride
+ * example Rust behind an FFI) that has no CUDA allocator.  For ncell independent cells given on
+ * the host it returns each cell's internal-force vector f = sum_p B^T sigma |J| w t and its
+ * tangent matrix K = sum_p B^T D B |J| w t (D the consistent tangent of the IP state: elastic
+ * modulus where elastic[ip] != 0, the von Mises elastoplastic tangent otherwise).  2D cells are
+ * always in plane strain: there is no plane-stress or axisymmetric option here.
+ * Inputs: X[ncell][nnode][ndim] coordinates; the IP state structure-of-arrays with stride
  * nip = ncell*ngauss: sig[ncomp][nip] (Mandel), ivs[2][nip] (z then lambda), elastic[nip].
  * Outputs (host, nullable, at least one): f[ncell][nnode*ndim] and kk[ncell][ne][ne] row-major.
  * All device work uses one file-scope array of 16 MiB, held by every GPU that loads the library

@@ -95,7 +95,10 @@ def block_slots(mesh: Mesh, bptr: np.ndarray, bcol: np.ndarray) -> np.ndarray:
         for a in range(nn):
             A = nodes[a]
             row = bcol[bptr[A]:bptr[A + 1]]
-            slots[c, a] = np.searchsorted(row, nodes)
+            k = np.searchsorted(row, nodes)
+            if np.any(k >= len(row)) or np.any(row[np.minimum(k, len(row) - 1)] != nodes):
+                raise ValueError(f"cell {c}: block row {A} of the pattern lacks a block of the cell")
+            slots[c, a] = k
     return slots
 
 

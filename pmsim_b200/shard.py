@@ -108,17 +108,21 @@ class Halo:
         return self._dev[key]
 
     def exchange(self, x):
+        """Posts every send and receive of this rank as one group (torch.distributed's
+        batch_isend_irecv): NCCL then issues them together, so two neighbours that both send
+        first cannot wait on each other; gloo runs the same list."""
         import torch
         import torch.distributed as dist
         send, recv = self._index(x.device)
-        reqs, bufs = [], {}
+        ops, bufs = [], {}
         for q, idx in send.items():
-            reqs.append(dist.isend(x[idx].contiguous(), q))
+            ops.append(dist.P2POp(dist.isend, x[idx].contiguous(), q))
         for q, idx in recv.items():
             bufs[q] = torch.empty(len(idx), dtype=x.dtype, device=x.device)
-            reqs.append(dist.irecv(bufs[q], q))
-        for r in reqs:
-            r.wait()
+            ops.append(dist.P2POp(dist.irecv, bufs[q], q))
+        if ops:
+            for r in dist.batch_isend_irecv(ops):
+                r.wait()
         for q, idx in recv.items():
             x[idx] = bufs[q]
         return x
@@ -130,11 +134,24 @@ def owned_rows(indptr: np.ndarray, indices: np.ndarray, values: np.ndarray, n_ow
     return indptr[:n_owned_dof + 1].copy(), indices[:end].copy(), values[:end].copy()
 
 
-def _spmv(rows, cols, vals, n, x):
-    """y = A x for A in coordinate form (row-sorted tensors on x's device)."""
-    y = x.new_zeros(n)
-    y.index_add_(0, rows, vals * x[cols])
-    return y
+def _ell(rows, cols, vals, n):
+    """Row-padded (ELL) form of a row-sorted coordinate matrix: cols/vals of shape (n, width),
+    padding entries point at column 0 with value 0."""
+    counts = np.bincount(rows, minlength=n)
+    width = int(counts.max()) if n else 0
+    start = np.concatenate([[0], np.cumsum(counts)[:-1]])
+    slot = np.arange(len(rows)) - start[rows]
+    ec = np.zeros((n, width), dtype=np.int64)
+    ev = np.zeros((n, width))
+    ec[rows, slot] = cols
+    ev[rows, slot] = vals
+    return ec, ev
+
+
+def _spmv(ell_cols, ell_vals, x):
+    """y = A x with A in row-padded form: a fixed-order sum over each row (no atomics), so the
+    product, and the CG iterates built on it, are the same bits on every run."""
+    return (ell_vals * x[ell_cols]).sum(dim=1)
 
 
 def dist_cg(indptr, indices, values, b_owned, halo: Halo, n_local_dof: int, fixed_local: np.ndarray,
@@ -161,9 +178,9 @@ def dist_cg(indptr, indices, values, b_owned, halo: Halo, n_local_dof: int, fixe
     d = r_all == c_all
     np.add.at(diag, r_all[d], v_all[d])
     dinv = torch.as_tensor(1.0 / diag, device=dev)
-    t_rows = torch.as_tensor(r_all.astype(np.int64), device=dev)
-    t_cols = torch.as_tensor(c_all.astype(np.int64), device=dev)  # the device pattern is int32
-    t_vals = torch.as_tensor(v_all, device=dev)
+    ec, ev = _ell(r_all, c_all.astype(np.int64), v_all, n)  # the device pattern is int32
+    t_cols = torch.as_tensor(ec, device=dev)
+    t_vals = torch.as_tensor(ev, device=dev)
     b = b_owned.clone()
     b[torch.as_tensor(fr, device=dev)] = 0.0
 
@@ -181,7 +198,7 @@ def dist_cg(indptr, indices, values, b_owned, halo: Halo, n_local_dof: int, fixe
     it = 0
     while it < max_iterations and float(rz) > rtol * rtol * rz0:
         halo.exchange(p_local)
-        q = _spmv(t_rows, t_cols, t_vals, n, p_local)
+        q = _spmv(t_cols, t_vals, p_local)
         pq = allsum((p_local[:n] * q).sum().reshape(1))[0]
         alpha = rz / pq
         x += alpha * p_local[:n]

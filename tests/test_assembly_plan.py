@@ -60,3 +60,29 @@ def test_plan_reproduces_the_assembled_matrix(kind, ncolor):
     assert np.array_equal(got, again)
     other = P.emulate(m, ke, bptr, slots, np.arange(m.ncell)[::-1])
     assert np.max(np.abs(other - got)) <= 1e-13 * scale
+
+
+def test_block_slots_refuse_a_pattern_without_the_cell_block():
+    """A pattern that lacks one of a cell's node blocks is refused, not mapped to a neighbouring slot."""
+    m = _mesh(QUA8)
+    ip, ix, _ = oracle.coo_to_csr(m.ndof, *[np.asarray(a) for a in _coo(m)])
+    bptr, bcol = P.block_pattern(ip, ix, m.ndim)
+    P.block_slots(m, bptr, bcol)  # the full pattern maps every block
+    A, B = int(m.cells[0, 0]), int(m.cells[0, 2])
+    row = bcol[bptr[A]:bptr[A + 1]]
+    keep = np.ones(len(bcol), bool)
+    keep[bptr[A] + int(np.flatnonzero(row == B)[0])] = False
+    bcol2 = bcol[keep]
+    bptr2 = bptr.copy()
+    bptr2[A + 1:] -= 1
+    with pytest.raises(ValueError):
+        P.block_slots(m, bptr2, bcol2)
+
+
+def _coo(m):
+    """Unit entries at every (cell node, cell node) DOF pair: the pattern of K."""
+    nd, nn = m.ndim, m.nnode
+    dofs = (m.cells[:, :, None] * nd + np.arange(nd)).reshape(m.ncell, nn * nd)
+    rows = np.repeat(dofs, nn * nd, axis=1).ravel().astype(np.int64)
+    cols = np.tile(dofs, (1, nn * nd)).ravel().astype(np.int64)
+    return rows, cols, np.ones(rows.size)
