@@ -573,7 +573,8 @@ def run_served(nreq, rate, nalone, seed=7, detail_file=""):
 def cpu_sample(m, ddu, ncell_sample, nthreads):
     """The oracle (C++ restatement of pmsim's element/material path, structured like the reference:
     per-cell dense B^T D B, COO triplets with duplicates, sort/sum to CSR) on the first
-    ncell_sample cells.  Returns seconds for update + F_int + K(COO) + CSR and the IP count."""
+    ncell_sample cells.  Returns seconds for update + F_int + K(COO) + CSR, the IP count and the
+    oracle's results (elements with their IP state, F_int over all DOFs, CSR of the sample)."""
     import oracle
     from pmsim_b200 import mesh as M
     sub = M.Mesh(3, m.coords, m.cells[:ncell_sample], m.kind)
@@ -583,15 +584,55 @@ def cpu_sample(m, ddu, ncell_sample, nthreads):
     t = [time.perf_counter()]
     el.update_secondary_values(ddu)
     t.append(time.perf_counter())
-    el.assemble_f_int()
+    ff = el.assemble_f_int()
     t.append(time.perf_counter())
     rows, cols, vals = el.assemble_kk_coo()
     t.append(time.perf_counter())
-    oracle.coo_to_csr(m.ndof, rows, cols, vals)
+    csr = oracle.coo_to_csr(m.ndof, rows, cols, vals)
     t.append(time.perf_counter())
     cpu_sample.phases = dict(zip(("update_secondary", "f_int", "k_coo", "csr_sum"),
                                  (t[i + 1] - t[i] for i in range(4))))
-    return t[-1] - t[0], ncell_sample * el.ngauss
+    return t[-1] - t[0], ncell_sample * el.ngauss, (el, ff, csr)
+
+
+def parity_sample(m, ncs, state, ff, csr_values, indptr, indices, ref, tol=1e-12):
+    """The GPU step against the oracle on the first ncs cells of the same mesh and increment.
+
+    state = (sig, ivs, elastic) of the GPU (all IPs), ff its F_int, csr_values/indptr/indices its K;
+    ref = (oracle elements over the first ncs cells, their F_int over all DOFs, their CSR).  Compared:
+    the IP state of the sample's IPs; every R entry and every CSR row of the nodes whose incident
+    cells all lie in the sample (the rows the sample computes completely).  Relative normwise 1e-12;
+    elastic flags and column indices must be identical."""
+    oel, off, (oip, oix, odata) = ref
+    ng = oel.ngauss
+    nip = ncs * ng
+    sig, ivs, el = state
+    out = {"sample_cells": int(ncs), "sample_ips": int(nip), "tol_rel": tol}
+
+    def rel(a, b):
+        scale = float(np.max(np.abs(b))) if b.size else 0.0
+        return float(np.max(np.abs(a - b))) / max(scale, 1e-300) if b.size else 0.0
+
+    errs = {"sigma": rel(sig[:nip], oel.sig), "z_lambda": rel(ivs[:nip], oel.ivs)}
+    flags_ok = bool(np.array_equal(el[:nip], oel.elastic))
+    n_all = np.bincount(m.cells.ravel(), minlength=m.npoint)
+    n_in = np.bincount(m.cells[:ncs].ravel(), minlength=m.npoint)
+    inside = np.flatnonzero((n_all == n_in) & (n_in > 0))
+    rows = (inside[:, None] * m.ndim + np.arange(m.ndim)).ravel()
+    errs["f_int_rows"] = rel(ff[rows], off[rows])
+    lo, hi = indptr[rows], indptr[rows + 1]
+    olo, ohi = oip[rows], oip[rows + 1]
+    pattern_ok = bool(np.array_equal(hi - lo, ohi - olo))
+    if pattern_ok and rows.size:
+        take = np.concatenate([np.arange(x, y) for x, y in zip(lo, hi)])
+        otake = np.concatenate([np.arange(x, y) for x, y in zip(olo, ohi)])
+        pattern_ok = bool(np.array_equal(indices[take], oix[otake]))
+        errs["csr_rows"] = rel(csr_values[take], odata[otake])
+        out["csr_values_compared"] = int(take.size)
+    out.update({"rows_compared": int(rows.size), "max_rel_err": errs, "elastic_flags_equal": flags_ok,
+                "pattern_equal": pattern_ok})
+    out["ok"] = bool(flags_ok and pattern_ok and rows.size > 0 and all(v <= tol for v in errs.values()))
+    return out
 
 
 def cpu_model():
@@ -640,7 +681,7 @@ def reference_arm(args, rank):
     cpu_sample(m, ddu, min(ncs, 256), nthreads)  # warm-up (page-in, thread pool)
     tot, ips = 0.0, 0
     for _ in range(args.steps):
-        dt, n = cpu_sample(m, ddu, ncs, nthreads)
+        dt, n, _ = cpu_sample(m, ddu, ncs, nthreads)
         tot += dt
         ips += n
     value = ips / tot
@@ -729,6 +770,13 @@ def main():
     ms_max = dist.max_over_ranks(ms, dev)
     nip = m.ncell * ng
     value = world * nip / (ms_max * 1e-3)
+    # the step's results, kept for the parity check against the oracle (rank 0, with the CPU leg)
+    gpu_state = gpu_ff = gpu_csr = el_pattern = None
+    if rank == 0 and not args.no_cpu:
+        gpu_state = el.get_state()
+        gpu_ff = d_ff.cpu().numpy()
+        gpu_csr = d_csr.cpu().numpy()
+        el_pattern = el.csr_pattern()
 
     # e2e through the C ABI with host buffers (pinned): dU in, R and CSR values out, every step
     e2e = None
@@ -785,18 +833,23 @@ def main():
     alg_bytes = algorithmic_bytes_step(m, ng, nnz)
     step_gbs = alg_bytes / (ms * 1e-3) / 1e9
     cpu = None
+    parity = None
     if not args.no_cpu:
         import oracle
         nthreads = oracle.lib().orc_max_threads()
         ncs = args.cpu_cells or (512 if args.size == "small" else 4096)
         cpu_sample(m, ddu_h, 256, nthreads)
-        dt, n = cpu_sample(m, ddu_h, ncs, nthreads)
+        dt, n, ref = cpu_sample(m, ddu_h, ncs, nthreads)
         phases = {k: v / n * 1e6 for k, v in cpu_sample.phases.items()}
-        dt1, n1 = cpu_sample(m, ddu_h, max(ncs // 8, 64), 1)
+        dt1, n1, _ = cpu_sample(m, ddu_h, max(ncs // 8, 64), 1)
         cpu = {"value": n / dt, "unit": "IP/s", "cores": nthreads, "kind": "port",
                "sample": f"first {ncs} cells ({n} IPs): update + F_int + K COO + CSR sum, all threads",
                "single_thread_ip_per_s": n1 / dt1, "us_per_ip_by_phase": phases,
                "cpu_model": cpu_model(), "nproc": os.cpu_count()}
+        indptr, indices = el_pattern
+        parity = parity_sample(m, ncs, gpu_state, gpu_ff, gpu_csr, indptr, indices, ref)
+        parity["what"] = ("GPU step vs the oracle on the first cells: IP state of their IPs, R entries and CSR "
+                          "rows of the nodes whose cells all lie in the sample")
     nx, ny, nz = workload_dims(args.size)
     line = {
         "metric": "IP stress-update+tangent/s FP64",
@@ -820,10 +873,12 @@ def main():
         "kernels_ms_per_step": {"element": ms_elem, "f_gather": kt[1] / max(kc[1], 1),
                                 "kk_gather": kt[2] / max(kc[2], 1)},
         "gpu_launches": int(launches),
-        "e2e": e2e, "cpu_baseline": cpu, "k1_microbench": k1, "ep_microbench": ep, "qua8_step": qua8, "batched": batched, "served": served, "c0_footing": c0, "fp64_peak_tflops": fp64,
+        "e2e": e2e, "cpu_baseline": cpu, "parity": parity, "k1_microbench": k1, "ep_microbench": ep, "qua8_step": qua8, "batched": batched, "served": served, "c0_footing": c0, "fp64_peak_tflops": fp64,
         "clocks": clk,
     }
     print(json.dumps(line), flush=True)
+    if parity is not None and not parity["ok"]:
+        sys.exit("parity check against the oracle failed: " + json.dumps(parity))
 
 
 if __name__ == "__main__":

@@ -160,8 +160,14 @@ int pms_mesh_csr_pattern(const pms_mesh* mesh, int64_t* indptr, int32_t* indices
 
 /* Waits for the handle's stream and returns the first device-side error (PMS_OK if none). */
 int pms_elements_sync(pms_elements* h);
+/* Message of the handle's last error; with h = NULL, the message of this thread's last refused
+ * pms_elements_create (for example "von Mises initial size of the yield surface must > 1e-6",
+ * src/material/von_mises.rs:68-70), empty if it succeeded. */
 const char* pms_elements_last_error(const pms_elements* h);
-/* cell and IP of the first failing integration point (-1 if none) */
+/* cell and IP of the failing integration point that the reference would report (-1 if none): its
+ * loops stop at the first error, and they run the stress update of every cell before the tangent of
+ * any cell, each in ascending cell and IP order (src/fem/elements.rs:156-181) -- so an update error
+ * is reported before a tangent error, and the lowest failing cell, then its lowest IP, is named. */
 int pms_elements_error_location(const pms_elements* h, int64_t* cell, int32_t* ip);
 /* Number of kernels this handle has launched since creation (instrumentation). */
 int64_t pms_elements_launch_count(const pms_elements* h);

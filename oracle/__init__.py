@@ -52,6 +52,8 @@ def lib():
         L.orc_model_update_and_stiffness_batch.argtypes = [ctypes.c_int, c_double_p, ctypes.c_int, ctypes.c_int64,
                                                            c_double_p, c_double_p, c_uint8_p, c_double_p,
                                                            c_double_p, ctypes.c_int]
+        L.orc_model_batch_hh.argtypes = [ctypes.c_int, c_double_p, ctypes.c_int, ctypes.c_int64, c_double_p,
+                                          c_double_p, c_double_p, c_uint8_p, c_double_p, c_double_p, ctypes.c_int]
         L.orc_elem_f_int.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_double, c_double_p, c_double_p,
                                      c_double_p]
         L.orc_elem_jacobian.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_double, c_double_p, ctypes.c_int,
@@ -136,6 +138,18 @@ def model_batch(model, params, ndim, sig, ivs, elastic, deps, with_tangent=True,
     return dd
 
 
+def model_batch_hh(model, params, ndim, hh, sig, ivs, elastic, deps, nthreads=0):
+    """model_batch with a hardening modulus per IP (hh[n]); returns the tangents (n, nc, nc)."""
+    n = sig.shape[0]
+    nc = 2 * ndim
+    dd = np.zeros((n, nc, nc))
+    st = lib().orc_model_batch_hh(model, _dp(params.arr), ndim, n, _dp(np.ascontiguousarray(hh, dtype=np.float64)),
+                                  _dp(sig), _dp(ivs), _p(elastic, c_uint8_p), _dp(deps), _dp(dd), nthreads)
+    if st:
+        raise RuntimeError(f"material batch error {st}")
+    return dd
+
+
 EP_CASES = ("AE", "AXB", "BE", "BXP", "BP")
 
 
@@ -175,6 +189,15 @@ def elem_jacobian(kind, ngauss, X, model, params, sig, ivs, elastic, thickness=1
     if st:
         raise RuntimeError(f"jacobian error {st}")
     return K
+
+
+class OracleError(RuntimeError):
+    """An element-loop error with the failing cell (and IP, for the stress update), as the
+    reference's loops report the first one (src/fem/elements.rs:156-181)."""
+
+    def __init__(self, msg, code, cell, ip=-1):
+        super().__init__(msg)
+        self.code, self.cell, self.ip = code, cell, ip
 
 
 class OracleElements:
@@ -222,7 +245,7 @@ class OracleElements:
         st = lib().orc_assemble_f_int(self.kind, self.ngauss, self.thickness, m.npoint, _dp(m.coords), m.ncell,
                                       _p(m.cells, c_int64_p), _dp(self.sig), _dp(ff))
         if st:
-            raise RuntimeError(f"assemble_f_int error {st}")
+            raise OracleError(f"assemble_f_int error {st}", st, -1)
         return ff
 
     def assemble_kk_coo(self):
@@ -239,9 +262,12 @@ class OracleElements:
                                        _p(rows, c_int64_p), _p(cols, c_int64_p), _dp(vals), self.nthreads,
                                        _p(bad, c_int64_p))
         if st == 5:
-            raise RuntimeError("local matrix is not symmetric")
+            raise OracleError("local matrix is not symmetric", st, int(bad[0]))
+        if st == 3:
+            raise OracleError("von Mises stiffness cannot be computed with zero deviatoric norm (norm_s < 1e-10)",
+                              st, int(bad[0]))
         if st:
-            raise RuntimeError(f"assemble_kk error {st} at cell {bad[0]}")
+            raise OracleError(f"assemble_kk error {st} at cell {bad[0]}", st, int(bad[0]))
         return rows, cols, vals
 
     def assemble_kk_csr(self):
@@ -258,9 +284,10 @@ class OracleElements:
                                         _dp(self.sig), _dp(self.ivs), _p(self.elastic, c_uint8_p), self.nthreads,
                                         _p(bc, c_int64_p), _p(bi, c_int_p))
         if st == 2:
-            raise RuntimeError("von Mises plastic update must not lead to zero sigma_d (sigma_d < 1e-10)")
+            raise OracleError("von Mises plastic update must not lead to zero sigma_d (sigma_d < 1e-10)", st,
+                              int(bc[0]), int(bi[0]))
         if st:
-            raise RuntimeError(f"update_secondary error {st} at cell {bc[0]} ip {bi[0]}")
+            raise OracleError(f"update_secondary error {st} at cell {bc[0]} ip {bi[0]}", st, int(bc[0]), int(bi[0]))
 
 
 def coo_to_csr(nrow, rows, cols, vals):

@@ -823,6 +823,25 @@ int orc_model_update_and_stiffness_batch(int model, const double* prm, int ndim,
     return err;
 }
 
+// The same batch with a hardening modulus per IP (hh[n]; prm[2] is ignored).
+int orc_model_batch_hh(int model, const double* prm, int ndim, int64_t n, const double* hh, double* sig, double* ivs,
+                       uint8_t* elastic, const double* deps, double* dd, int nthreads) {
+    int nc = 2 * ndim;
+    int err = 0;
+#ifdef _OPENMP
+    if (nthreads <= 0) nthreads = omp_get_max_threads();
+#pragma omp parallel for num_threads(nthreads) schedule(static) reduction(max : err)
+#endif
+    for (int64_t i = 0; i < n; i++) {
+        Params p{prm[0], prm[1], hh[i], prm[3]};
+        int st = model_update_stress(model, p, nc, sig + i * nc, ivs + 2 * i, elastic + i, deps + i * nc);
+        if (!st && dd) st = model_stiffness(model, p, nc, sig + i * nc, ivs + 2 * i, elastic[i], dd + i * nc * nc);
+        if (st > err) err = st;
+    }
+    (void)nthreads;
+    return err;
+}
+
 int orc_elem_f_int(int kind, int ngauss, double thickness, const double* X, const double* sig, double* f) {
     ElemCtx c;
     if (!make_ctx(kind, ngauss, thickness, c)) return -1;
@@ -896,7 +915,8 @@ int orc_assemble_kk_coo(int kind, int ngauss, double thickness, const double* co
 #ifdef _OPENMP
 #pragma omp critical
 #endif
-                { if (st > err) { err = st; bad = e; } }
+                // the reference's loop stops at the first failing cell (src/fem/elements.rs:156-163)
+                { if (err == 0 || e < bad) { err = st; bad = e; } }
                 continue;
             }
             int64_t o = e * (int64_t)ne * ne;
@@ -975,7 +995,8 @@ int orc_update_secondary(int kind, int ngauss, double thickness, const double* c
 #ifdef _OPENMP
 #pragma omp critical
 #endif
-            { if (st > err) { err = st; bc = e; bi = ip; } }
+            // the first failing cell in the reference's loop order (src/fem/elements.rs:176-181)
+            { if (err == 0 || e < bc) { err = st; bc = e; bi = ip; } }
         }
     }
     (void)nthreads;

@@ -79,7 +79,8 @@ struct ElemArgs {
     double* sig; double* z; double* lam; uint8_t* el;
     double* fe;   // [cell][nn][nd]
     double* ke;   // [cell][NE][NE] dense element matrices
-    int32_t* status;  // {code, cell, ip, 0}
+    unsigned long long* errkey;  // error key of the failing IP the reference would report (0: none)
+    unsigned long long* prob_err = nullptr;  // UPD_MODE (nullable): the same key per problem
     const int32_t* cell_prob = nullptr;  // UPD_MODE: problem of each cell
     const uint8_t* pmode = nullptr;      // UPD_MODE: mode of each problem
     // work queue (nq > 0): the launch covers ncell queued cells, range k from q_first[k]
@@ -100,12 +101,23 @@ __device__ __forceinline__ int64_t queue_item(int64_t i, int n, const int64_t* _
     return __ldg(first + lo) + (i - __ldg(off + lo));
 }
 
-__device__ __forceinline__ void report(int32_t* status, int code, int64_t cell, int ip) {
+// Which failing IP is reported.  The reference stops at the first error of its loops: the stress
+// update of every cell (Elements::update_secondary_values) runs before any tangent
+// (Elements::assemble_kke), and each loop goes through the cells and their IPs in ascending order
+// (src/fem/elements.rs:156-181).  A failing IP offers the key
+//   rank << 56 | (2^40 - 1 - cell) << 16 | (255 - ip) << 8 | code
+// (rank 2: update error, 1: tangent/assembly error) and atomicMax keeps the one the reference
+// would return: update errors first, then the lowest cell, then its lowest IP.
+constexpr int RANK_UPDATE = 2, RANK_TANGENT = 1;
+__host__ __device__ constexpr unsigned long long error_key(int rank, int64_t cell, int ip, int code) {
+    return ((unsigned long long)rank << 56) | ((((1ull << 40) - 1) - (unsigned long long)cell) << 16) |
+           ((unsigned long long)(255 - ip) << 8) | (unsigned long long)(code & 0xff);
+}
+__device__ __forceinline__ void report(const ElemArgs& A, int rank, int code, int64_t cell, int ip) {
     if (code == OK) return;
-    if (atomicCAS(status, 0, code) == 0) {
-        status[1] = (int32_t)cell;
-        status[2] = ip;
-    }
+    const unsigned long long k = error_key(rank, cell, ip, code);
+    atomicMax(A.errkey, k);
+    if (A.prob_err && A.cell_prob) atomicMax(A.prob_err + A.cell_prob[cell], k);
 }
 
 template <int ND>
@@ -249,7 +261,7 @@ __global__ void __launch_bounds__(WPB * 32, warps_per_cell(NN) == 2 ? 3 : (ND ==
 
     // ---------------- phase 1: lane p owns integration point p ----------------
     const int64_t ip0 = cell * ng;
-    int err = OK;
+    int err = OK, err_t = OK;  // stress-update (and geometry) error, tangent error
     const bool has_ip = lane < ng;
     double sig[NC], z = 0.0, lam = 0.0;
     int el = 1;
@@ -349,8 +361,7 @@ __global__ void __launch_bounds__(WPB * 32, warps_per_cell(NN) == 2 ? 3 : (ND ==
         }
         if (DOK) {
             double a, b, s[NC];
-            const int st = tangent_coefs<NC>(mc, mc.hh, sig, lam, el, a, b, s);
-            if (st != OK && err == OK) err = st;
+            err_t = tangent_coefs<NC>(mc, mc.hh, sig, lam, el, a, b, s);
             double* t = TC + p * 10;
             t[0] = coef * 0.5 * a;
             // volumetric coefficient: K - a/3 (= Lame lambda when elastic); plane stress: lambda*
@@ -370,13 +381,18 @@ __global__ void __launch_bounds__(WPB * 32, warps_per_cell(NN) == 2 ? 3 : (ND ==
             }
         }
     }
-    // first failing IP of the cell (lowest p) reports
+    // first failing IP of the cell (lowest p): an update error if any, else a tangent error
     {
         const unsigned bad = __ballot_sync(FULL, err != OK);
+        const unsigned bad_t = __ballot_sync(FULL, err_t != OK);
         if (bad) {
             const int p = __ffs(bad) - 1;
             const int code = __shfl_sync(FULL, err, p);
-            if (lane == 0) report(A.status, code, cell, p);
+            if (lane == 0) report(A, do_update ? RANK_UPDATE : RANK_TANGENT, code, cell, p);
+        } else if (bad_t) {
+            const int p = __ffs(bad_t) - 1;
+            const int code = __shfl_sync(FULL, err_t, p);
+            if (lane == 0) report(A, RANK_TANGENT, code, cell, p);
         }
     }
     if (do_update && has_ip) {
@@ -743,7 +759,7 @@ __global__ void __launch_bounds__(WPB2 * 32, 4) element2d_kernel(ElemArgs A) {
 
         // ---------------- phase 1: lane p of the half owns integration point p ----------------
         const int64_t ip0 = cell * ng;
-        int err = OK;
+        int err = OK, err_t = OK;  // stress-update (and geometry) error, tangent error
         const bool has_ip = hl < ng;
         double sig[4], z = 0.0, lam = 0.0;
         int el = 1;
@@ -826,8 +842,7 @@ __global__ void __launch_bounds__(WPB2 * 32, 4) element2d_kernel(ElemArgs A) {
             }
             if (DOK) {
                 double a, b, s[4];
-                const int st = tangent_coefs<4>(mc, mc.hh, sig, lam, el, a, b, s);
-                if (st != OK && err == OK) err = st;
+                err_t = tangent_coefs<4>(mc, mc.hh, sig, lam, el, a, b, s);
                 double* t = TC + p * 4;
                 t[0] = coef * 0.5 * a;
                 // volumetric coefficient: K - a/3 (= Lame lambda when elastic); plane stress: lambda*
@@ -858,13 +873,20 @@ __global__ void __launch_bounds__(WPB2 * 32, 4) element2d_kernel(ElemArgs A) {
                 }
             }
         }
-        // first failing IP of each cell (lowest p) reports
+        // first failing IP of each cell (lowest p): an update error if any, else a tangent error
         {
             const unsigned bad = __ballot_sync(FULL, err != OK);
+            const unsigned bad_t = __ballot_sync(FULL, err_t != OK);
             const unsigned mine = (bad >> (LPC * hh)) & ((1u << LPC) - 1u);
+            const unsigned mine_t = (bad_t >> (LPC * hh)) & ((1u << LPC) - 1u);
             const int first = mine ? __ffs(mine) - 1 : 0;
+            const int first_t = mine_t ? __ffs(mine_t) - 1 : 0;
             const int code = __shfl_sync(FULL, err, LPC * hh + first);
-            if (active && mine && hl == 0) report(A.status, code, cell, first);
+            const int code_t = __shfl_sync(FULL, err_t, LPC * hh + first_t);
+            if (active && hl == 0) {
+                if (mine) report(A, do_update ? RANK_UPDATE : RANK_TANGENT, code, cell, first);
+                else if (mine_t) report(A, RANK_TANGENT, code_t, cell, first_t);
+            }
         }
         if (active && do_update && has_ip) {
 #pragma unroll
@@ -1411,7 +1433,7 @@ ElemArgs make_args(pms_elements* h, const double* ddu) {
     a.el = h->d_el;
     a.fe = h->d_fe;
     a.ke = h->d_ke;
-    a.status = h->d_status;
+    a.errkey = (unsigned long long*)h->d_status;
     return a;
 }
 
@@ -1461,24 +1483,61 @@ void launch_f_gather(pms_elements* h, double* ff, const pms::WorkQueue* q = null
 
 }  // namespace
 
+namespace pms {
+// Message of this thread's last refused pms_elements_create (pms_elements_last_error(NULL)).
+std::string& create_error() {
+    static thread_local std::string msg;
+    return msg;
+}
+
+// Decodes an error key (error_key above): the element error code, cell and IP.
+int decode_error(unsigned long long key, int64_t* cell, int32_t* ip) {
+    if (cell) *cell = (int64_t)(((1ull << 40) - 1) - ((key >> 16) & ((1ull << 40) - 1)));
+    if (ip) *ip = 255 - (int32_t)((key >> 8) & 0xff);
+    return (int)(key & 0xff);
+}
+}  // namespace pms
+
 extern "C" {
 
 int pms_elements_create(const pms_mesh* mesh, const pms_material* materials, int32_t nmaterial,
                         const pms_config* config, pms_elements** out) {
-    if (!out) return PMS_ERR_INVALID;
+    auto refuse = [](int code, const char* msg) {
+        create_error() = msg;
+        return code;
+    };
+    create_error().clear();
+    if (!out) return refuse(PMS_ERR_INVALID, "out is null");
     *out = nullptr;
-    if (!mesh || !materials || nmaterial < 1 || !config || !mesh->coords || !mesh->cells) return PMS_ERR_INVALID;
+    if (!mesh || !materials || nmaterial < 1 || !config || !mesh->coords || !mesh->cells)
+        return refuse(PMS_ERR_INVALID, "mesh, materials and config are required");
     int kind = mesh->kind;
-    if (kind < 0 || kind > 8 || kind_ndim(kind) != mesh->ndim) return PMS_ERR_INVALID;
-    if (config->axisymmetric && mesh->ndim != 2) return PMS_ERR_UNSUPPORTED;
-    // plane stress: 2D linear elastic only ("von Mises model does not work in plane-stress",
-    // src/material/von_mises.rs:60-62)
+    if (kind < 0 || kind > 8 || kind_ndim(kind) != mesh->ndim)
+        return refuse(PMS_ERR_INVALID, "unknown element kind or kind of another dimension");
+    if (config->axisymmetric && mesh->ndim != 2)
+        return refuse(PMS_ERR_UNSUPPORTED, "the axisymmetric idealization needs a 2D mesh");
+    // plane stress: 2D linear elastic only (src/material/von_mises.rs:60-62)
     if (config->plane_stress) {
-        if (mesh->ndim != 2 || config->axisymmetric) return PMS_ERR_UNSUPPORTED;
+        if (mesh->ndim != 2 || config->axisymmetric)
+            return refuse(PMS_ERR_UNSUPPORTED, "plane stress needs a 2D mesh without axisymmetry");
         for (int i = 0; i < nmaterial; i++)
-            if (materials[i].model != PMS_LINEAR_ELASTIC) return PMS_ERR_UNSUPPORTED;
+            if (materials[i].model != PMS_LINEAR_ELASTIC)
+                return refuse(PMS_ERR_UNSUPPORTED, "von Mises model does not work in plane-stress");
     }
-    if (mesh->npoint < 1 || mesh->ncell < 1) return PMS_ERR_INVALID;
+    if (mesh->npoint < 1 || mesh->ncell < 1) return refuse(PMS_ERR_INVALID, "the mesh has no points or no cells");
+    for (int i = 0; i < nmaterial; i++) {
+        const pms_material& m = materials[i];
+        if (m.model != PMS_LINEAR_ELASTIC && m.model != PMS_VON_MISES)
+            return refuse(PMS_ERR_INVALID, "unknown stress-strain model");
+        // VonMises::new (src/material/von_mises.rs:68-70)
+        if (m.model == PMS_VON_MISES && !(m.z_ini > F_TOL))
+            return refuse(PMS_ERR_INVALID, "von Mises initial size of the yield surface must > 1e-6");
+    }
+    if (mesh->cell_material) {
+        for (int64_t c = 0; c < mesh->ncell; c++)
+            if (mesh->cell_material[c] < 0 || mesh->cell_material[c] >= nmaterial)
+                return refuse(PMS_ERR_INVALID, "cell_material names a material that does not exist");
+    }
     auto* h = new pms_elements();
     h->kind = kind;
     h->nd = mesh->ndim;
@@ -1493,35 +1552,17 @@ int pms_elements_create(const pms_mesh* mesh, const pms_material* materials, int
     h->ng = integration_rule(kind, config->ngauss, ksi, w);
     if (h->ng <= 0 || h->ng > 32) {
         delete h;
-        return PMS_ERR_INVALID;
+        return refuse(PMS_ERR_INVALID, "requested number of integration points is not available");
     }
     h->nip = h->ncell * h->ng;
     for (int i = 0; i < nmaterial; i++) {
         const pms_material& m = materials[i];
-        if (m.model != PMS_LINEAR_ELASTIC && m.model != PMS_VON_MISES) { delete h; return PMS_ERR_INVALID; }
-        if (m.model == PMS_VON_MISES && !(m.z_ini > F_TOL)) { delete h; return PMS_ERR_INVALID; }
         h->mats.push_back(make_matconst(m.model, m.young, m.poisson, m.hh, m.z_ini, config->plane_stress != 0));
-    }
-    if (mesh->cell_material) {
-        for (int64_t c = 0; c < h->ncell; c++)
-            if (mesh->cell_material[c] < 0 || mesh->cell_material[c] >= nmaterial) { delete h; return PMS_ERR_INVALID; }
-    }
-    // shape tables
-    h->tab.assign((size_t)h->ng * h->nn * h->nd + h->ng + (size_t)h->ng * h->nn, 0.0);
-    {
-        double N[20], dN[60];
-        for (int p = 0; p < h->ng; p++) {
-            shape_eval(kind, &ksi[3 * p], N, dN);
-            for (int m = 0; m < h->nn; m++)
-                for (int j = 0; j < h->nd; j++) h->tab[(p * h->nn + m) * h->nd + j] = dN[m * h->nd + j];
-            h->tab[(size_t)h->ng * h->nn * h->nd + p] = w[p];
-            for (int m = 0; m < h->nn; m++) h->tab[(size_t)h->ng * h->nn * h->nd + h->ng + p * h->nn + m] = N[m];
-        }
     }
     const char* msg = nullptr;
     if (!build_pattern(h->nd, h->nn, h->npoint, h->ncell, mesh->cells, h->pat, &msg)) {
         delete h;
-        return PMS_ERR_INVALID;
+        return refuse(PMS_ERR_INVALID, msg ? msg : "invalid connectivity");
     }
     h->nnz = h->pat.nblock() * h->nd * h->nd;
     // device uploads
@@ -1676,15 +1717,14 @@ int pms_elements_backup(pms_elements* h) { return h ? copy_state(h, true) : PMS_
 int pms_elements_restore(pms_elements* h) { return h ? copy_state(h, false) : PMS_ERR_INVALID; }
 
 static int finish_host(pms_elements* h) {
-    int32_t st[4];
-    if (cudaMemcpyAsync(st, h->d_status, 16, cudaMemcpyDeviceToHost, h->stream) != cudaSuccess ||
+    unsigned long long key = 0;
+    if (cudaMemcpyAsync(&key, h->d_status, 8, cudaMemcpyDeviceToHost, h->stream) != cudaSuccess ||
         cudaStreamSynchronize(h->stream) != cudaSuccess)
         return fail(h, PMS_ERR_CUDA, cudaGetErrorString(cudaGetLastError()));
-    if (st[0] != 0) {
-        h->err_cell = st[1];
-        h->err_ip = st[2];
+    if (key != 0) {
+        const int code = decode_error(key, &h->err_cell, &h->err_ip);
         cudaMemsetAsync(h->d_status, 0, 16, h->stream);
-        switch (st[0]) {
+        switch (code) {
         case E_ZERO_SIGMA_D:
             return fail(h, PMS_ERR_ZERO_SIGMA_D,
                         "von Mises plastic update must not lead to zero sigma_d (sigma_d < 1e-10)");
@@ -1865,7 +1905,7 @@ int pms_elements_set_state(pms_elements* h, const double* sig, const double* ivs
     return cuda_check(h);
 }
 
-const char* pms_elements_last_error(const pms_elements* h) { return h ? h->last_error.c_str() : "null handle"; }
+const char* pms_elements_last_error(const pms_elements* h) { return h ? h->last_error.c_str() : create_error().c_str(); }
 
 int pms_elements_error_location(const pms_elements* h, int64_t* cell, int32_t* ip) {
     if (!h) return PMS_ERR_INVALID;
@@ -1963,10 +2003,12 @@ int elements_device_pattern(pms_elements* h, const int64_t** indptr, const int32
 }
 
 int elements_run_modes(pms_elements* h, const int32_t* cell_prob, const int32_t* node_prob, const uint8_t* pmode,
-                       const double* ddu, double* ff, double* csr, const WorkQueue* queue) {
+                       const double* ddu, double* ff, double* csr, const WorkQueue* queue,
+                       unsigned long long* prob_err) {
     ElemArgs a = make_args(h, ddu);
     a.cell_prob = cell_prob;
     a.pmode = pmode;
+    a.prob_err = prob_err;
     if (queue) {
         if (queue->nq <= 0 || queue->ncell <= 0) return PMS_OK;  // nothing queued
         a.ncell = queue->ncell;
@@ -2149,7 +2191,7 @@ extern "C" int pms_element_calc_noalloc(int32_t kind, int32_t ngauss, double thi
     a.el = (uint8_t*)(base + L.el);
     a.fe = (double*)(base + L.fe);
     a.ke = (double*)(base + L.ke);
-    a.status = (int32_t*)(base + L.status);
+    a.errkey = (unsigned long long*)(base + L.status);
     const int smem = smem_bytes_for(nn, nd, ng, WPB);
     const bool dof = f != nullptr, dok = kk != nullptr;
     switch (kind) {
@@ -2171,11 +2213,11 @@ extern "C" int pms_element_calc_noalloc(int32_t kind, int32_t ngauss, double thi
     if (dok && cudaMemcpyAsync(kk, base + L.ke, sizeof(double) * (size_t)ncell * ne * ne, cudaMemcpyDeviceToHost,
                                st) != cudaSuccess)
         return PMS_ERR_CUDA;
-    int32_t hst[4] = {0, 0, 0, 0};
-    if (cudaMemcpyAsync(hst, base + L.status, 16, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+    unsigned long long key = 0;
+    if (cudaMemcpyAsync(&key, base + L.status, 8, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
         cudaStreamSynchronize(st) != cudaSuccess)
         return PMS_ERR_CUDA;
-    switch (hst[0]) {
+    switch (decode_error(key, nullptr, nullptr)) {
     case 0: return PMS_OK;
     case E_ZERO_NORM_S: return PMS_ERR_ZERO_NORM_S;
     case E_JACOBIAN: return PMS_ERR_JACOBIAN;

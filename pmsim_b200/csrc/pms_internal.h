@@ -43,8 +43,14 @@ struct WorkQueue {
 // the F_int and CSR gathers (the CSR rows of mode-0 problems are left as they are); all pointers
 // are device pointers on the handle's stream.  With a queue, only its cells and nodes are visited
 // (every queued problem must have a non-zero mode); F_int rows outside the queue are left as they are.
+// prob_err (device, nullable): per problem, the key of the element error that problem would report
+// (atomicMax; the caller zeroes it before the launch; decode with decode_error).
 int elements_run_modes(pms_elements* h, const int32_t* cell_prob, const int32_t* node_prob, const uint8_t* pmode,
-                       const double* ddu, double* ff, double* csr, const WorkQueue* queue = nullptr);
+                       const double* ddu, double* ff, double* csr, const WorkQueue* queue = nullptr,
+                       unsigned long long* prob_err = nullptr);
+
+// Element error key -> element error code (internal E_* value), cell and IP.
+int decode_error(unsigned long long key, int64_t* cell, int32_t* ip);
 
 // Status of the last launches (waits for the handle's stream).
 int elements_status(pms_elements* h);

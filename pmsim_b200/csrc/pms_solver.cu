@@ -828,6 +828,7 @@ struct pms_batch {
     double *d_rho = nullptr, *d_r0 = nullptr, *d_norm = nullptr, *d_rel = nullptr;
     int32_t *d_iters = nullptr, *d_nactive = nullptr;
     int64_t* d_queue = nullptr;    // work queue of the element pass: 4 arrays of np + 1
+    unsigned long long* d_perr = nullptr;  // per problem: key of its element error in the last pass
     std::vector<int64_t> h_queue;
     const int64_t* d_indptr = nullptr;
     const int32_t* d_indices = nullptr;
@@ -1242,7 +1243,8 @@ int pms_batch_create(pms_elements* el, int32_t nproblem, const int64_t* point_pt
               b->alloc(&b->d_rho, 2 * (size_t)nproblem) && b->alloc(&b->d_r0, nproblem) &&
               b->alloc(&b->d_norm, nproblem) && b->alloc(&b->d_rel, nproblem) &&
               b->alloc(&b->d_iters, 2 * (size_t)nproblem) &&
-              b->alloc(&b->d_nactive, 1) && b->alloc(&b->d_queue, 4 * ((size_t)nproblem + 1));
+              b->alloc(&b->d_nactive, 1) && b->alloc(&b->d_queue, 4 * ((size_t)nproblem + 1)) &&
+              b->alloc(&b->d_perr, (size_t)nproblem);
     if (ok && ff_ext) ok = b->upload(&b->d_fext, ff_ext, n);
     if (!ok) {
         delete b;
@@ -1358,29 +1360,31 @@ int pms_batch_tick(pms_batch* b, const uint8_t* cmd, const double* c_values, int
         q.node_off = b->d_queue + 2 * W;
         q.node_first = b->d_queue + 3 * W;
         cudaMemcpyAsync(b->d_queue, b->h_queue.data(), 4 * W * 8, cudaMemcpyHostToDevice, st);
-        rc = elements_run_modes(b->el, b->d_cell_prob, b->d_node_prob, b->d_pmode, b->d_ddu, b->d_ff, b->d_csr, &q);
+        cudaMemsetAsync(b->d_perr, 0, (size_t)np * 8, st);
+        rc = elements_run_modes(b->el, b->d_cell_prob, b->d_node_prob, b->d_pmode, b->d_ddu, b->d_ff, b->d_csr, &q,
+                                b->d_perr);
         if (rc) return rc;
         cudaMemcpyAsync(b->d_active, elem.data(), np, cudaMemcpyHostToDevice, st);
         residual_kernel<<<(unsigned)b->nchunk, CHN, 0, st>>>(b->S, b->d_ff, b->d_fext, b->d_u, b->d_lam, b->d_c,
                                                              b->d_rr, b->d_part_a);
         finalize_kernel<<<grid_of(np, 128), 128, 0, st>>>(np, b->d_pchunk, b->d_part_a, b->d_norm, 0);
         cudaMemcpyAsync(hnorm.data(), b->d_norm, np * 8, cudaMemcpyDeviceToHost, st);
+        std::vector<unsigned long long> perr(np, 0);
+        cudaMemcpyAsync(perr.data(), b->d_perr, (size_t)np * 8, cudaMemcpyDeviceToHost, st);
         if (cudaStreamSynchronize(st) != cudaSuccess) return bfail(b, PMS_ERR_CUDA, "residual failed");
         b->launches += 4;
-        // a material or geometry error in one problem stops that problem only
+        // a material or geometry error stops its own problem only; every failing problem of this
+        // pass is stopped with the error its own element loop would report first
         rc = elements_status(b->el);
-        if (rc == PMS_ERR_ZERO_SIGMA_D || rc == PMS_ERR_ZERO_NORM_S || rc == PMS_ERR_JACOBIAN) {
-            int64_t cell = -1;
-            int32_t ip = -1;
-            pms_elements_error_location(b->el, &cell, &ip);
-            const int p =
-                (int)(std::upper_bound(b->cell_ptr.begin(), b->cell_ptr.end(), cell) - b->cell_ptr.begin()) - 1;
-            if (p >= 0 && p < np && elem[p]) {
-                result[p] = 100 + 1 + rc;  // 104: zero sigma_d, 105: zero norm_s, 106: Jacobian
+        if (rc != PMS_OK && rc != PMS_ERR_ZERO_SIGMA_D && rc != PMS_ERR_ZERO_NORM_S && rc != PMS_ERR_JACOBIAN)
+            return rc;
+        for (int p = 0; p < np; p++) {
+            if (!elem[p] || perr[p] == 0) continue;
+            const int code = decode_error(perr[p], nullptr, nullptr);
+            if (code == PMS_ERR_ZERO_SIGMA_D || code == PMS_ERR_ZERO_NORM_S || code == PMS_ERR_JACOBIAN) {
+                result[p] = 100 + 1 + code;  // 104: zero sigma_d, 105: zero norm_s, 106: Jacobian
                 elem[p] = 0;
             }
-        } else if (rc) {
-            return rc;
         }
         bool any_start = false;
         for (int p = 0; p < np; p++) {

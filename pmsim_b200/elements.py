@@ -55,7 +55,8 @@ class Elements:
         h = ctypes.c_void_p()
         rc = self.L.pms_elements_create(ctypes.byref(cmesh), mats, len(materials), ctypes.byref(cfg), ctypes.byref(h))
         if rc != _lib.PMS_OK:
-            raise _lib.PmsError(rc)
+            raw = self.L.pms_elements_last_error(None)  # the refusal's message (reference wording)
+            raise _lib.PmsError(rc, raw.decode() if raw else None)
         self.h = h
         info = _lib.Info_()
         self.L.pms_elements_get_info(self.h, ctypes.byref(info))

@@ -537,3 +537,27 @@ def test_oracle_uniform_strain_fields(kind_name, plane_stress):
         el.initialize()
         el.update_secondary_values(u.reshape(-1))
         assert np.max(np.abs(el.sig - want[None, :])) <= 1e-13, (kind_name, want)
+
+
+def test_oracle_reports_the_first_failing_cell_like_the_reference():
+    """The reference's element loops stop at the first failing cell and IP (src/fem/elements.rs:156-181):
+    zero sigma_d in the update (von_mises.rs:212-216) and zero norm_s in the tangent (:147-150), on the
+    host-made shear bands of tests/error_cases.py, with several threads as with one."""
+    import error_cases as C
+    from pmsim_b200 import mesh as M
+    for kind in (M.QUA8, M.HEX8):
+        m = C.shear_mesh(kind)
+        prm = oracle.Params(C.E, C.NU, C.H_SOFT, C.Z0)
+        first = C.cells_inside(m, 4.0, 8.0)[0]
+        for nthreads in (1, 4):
+            o = oracle.OracleElements(m, 1, prm, sym_tol=-1.0, nthreads=nthreads)
+            o.initialize()
+            with pytest.raises(oracle.OracleError) as e:
+                o.update_secondary_values(C.band_shear(m, [(4.0, 8.0, C.GAMMA_ZERO_SIGMA_D)]))
+            assert (e.value.code, e.value.cell, e.value.ip) == (2, first, 0)
+            o.initialize()
+            o.update_secondary_values(C.band_shear(m, [(4.0, 8.0, C.GAMMA_ZERO_NORM_S)]))
+            assert o.elastic.min() == 0
+            with pytest.raises(oracle.OracleError) as e:
+                o.assemble_kk_coo()
+            assert (e.value.code, e.value.cell) == (3, first)
