@@ -106,10 +106,10 @@ def flops_per_ip_hex20():
     return 2 * fma + mul
 
 
-# DRAM bytes (read + write) of one element_kernel<3,20> launch per cell, from an ncu capture of the
-# 32x32x16 block (33.6 MB read + 449.1 MB written for 16,384 cells); traffic grows with the cell
-# count, so a launch over n cells moves n times this.
-ELEMENT_DRAM_BYTES_PER_CELL = (33.590272e6 + 449.112320e6) / 16384
+# DRAM bytes (read + write) per cell of one launch of the direct-assembly element kernel
+# element_kernel<3,20,...,CSR> from an ncu capture of a smaller block (traffic grows with the cell
+# count, so a launch over n cells moves n times this); None until that capture exists.
+ELEMENT_DRAM_BYTES_PER_CELL = None
 
 
 def algorithmic_bytes_step(m, ng, nnz):
@@ -308,9 +308,9 @@ def run_ep(torch, stream, steps, warmup, n=4_194_304, cpu_sample=20_000):
 def run_qua8_step(torch, stream, steps, warmup, hbm_peak, n=1024):
     """The fused Newton iteration on a large 2D mesh, where it is memory-bound: n x n Qua8 cells
     (9 IP) of the footing material (E=1e4, nu=0.3, z0=9, H=0) under a seeded smooth increment that
-    leaves a mix of elastic and plastic IPs.  Reports the element kernel's DRAM bytes per second
-    (its inputs, IP state, F_e and the dense K_e it writes) and the step's algorithmic bytes per
-    second, against the measured HBM peak."""
+    leaves a mix of elastic and plastic IPs.  Reports the step's algorithmic bytes per second
+    against the measured HBM peak (one kernel: the blocks go straight into the CSR values), and the
+    same step with the gather assembly for comparison."""
     from pmsim_b200 import _lib
     from pmsim_b200 import mesh as M
     from pmsim_b200.elements import Elements, Material
@@ -334,41 +334,59 @@ def run_qua8_step(torch, stream, steps, warmup, hbm_peak, n=1024):
         el.update_and_assemble(d_ddu, d_ff, d_csr)
     el.sync()
     plastic = float(1.0 - el.get_state()[2].mean())
-    L.pms_elements_set_timing(el.h, 1)
-    L.pms_elements_kernel_times(el.h, None, None)
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for _ in range(steps):
-        el.update_and_assemble(d_ddu, d_ff, d_csr)
-    e1.record(stream)
-    torch.cuda.synchronize(dev)
-    ms = e0.elapsed_time(e1) / steps
-    kt = np.zeros(3)
-    kc = np.zeros(3, np.int64)
-    L.pms_elements_kernel_times(el.h, _lib.ptr(kt), _lib.ptr(kc))
-    L.pms_elements_set_timing(el.h, 0)
-    ms_el = kt[0] / max(kc[0], 1)
-    ng, nip, ne = 9, m.ncell * 9, 16
-    # element kernel DRAM bytes: node data (coords + dU gathered per cell, conn), IP state read
-    # (backup: sigma 4 + z + lambda + flag) and written (current state), F_e and the dense K_e
-    el_bytes = (m.ncell * (8 * 2 * 8 * 2 + 8 * 4) + nip * (6 * 8 + 1) * 2 + m.ncell * ne * 8
-                + m.ncell * ne * ne * 8)
+    ms = time_steps(torch, el, stream, steps, d_ddu, d_ff, d_csr)
+    ab = assembly_ab(torch, L, el, stream, steps, warmup, d_ddu, d_ff, d_csr)
+    ng, nip = 9, m.ncell * 9
     # the fused step's algorithmic bytes in 2D: coordinates, connectivity, dU, IP state read (sigma 4 +
     # z) and written (sigma 4 + z + lambda + flag), R and the CSR values once
     step_bytes = (m.npoint * 16 + m.ncell * 8 * 4 + m.ndof * 8 + nip * 40 + nip * 49 + m.ndof * 8
                   + int(el.nnz) * 8)
     del d_csr
     el.close()
-    gbs_el = el_bytes / (ms_el * 1e-3) / 1e9
     gbs_step = step_bytes / (ms * 1e-3) / 1e9
     return {"workload": f"qua8 {n}x{n} footing material, 9 IP, one fused Newton iteration", "ncell": m.ncell,
             "nip": nip, "nnz": int(el.nnz), "plastic_fraction": plastic, "ms_per_step": ms,
-            "kernels_ms_per_step": {"element": ms_el, "f_gather": kt[1] / max(kc[1], 1),
-                                    "kk_gather": kt[2] / max(kc[2], 1)},
-            "element_roofline": {"bound": "hbm", "achieved": gbs_el, "peak": hbm_peak, "unit": "GB/s",
-                                 "frac": gbs_el / hbm_peak, "bytes_per_launch": el_bytes},
+            "kernel": "element2d_kernel<8,10,UPD_BACKUP,F,K,CSR> (update + F_int + K added straight into CSR and R)",
+            "assembly_ab": ab,
             "step_roofline": {"bound": "hbm", "achieved": gbs_step, "peak": hbm_peak, "unit": "GB/s",
                               "frac": gbs_step / hbm_peak, "algorithmic_bytes_per_step": step_bytes}}
+
+
+def time_steps(torch, el, stream, steps, d_ddu, d_ff, d_csr):
+    """Mean device time (ms, CUDA events on the handle's stream) of `steps` fused Newton iterations."""
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        el.update_and_assemble(d_ddu, d_ff, d_csr)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / steps
+
+
+def assembly_ab(torch, L, el, stream, steps, warmup, d_ddu, d_ff, d_csr):
+    """The same step with the gather assembly (dense element matrices, then row gathers; the same
+    bits), timed per kernel, beside the direct assembly's step: the gain of adding the blocks
+    straight into the CSR values."""
+    from pmsim_b200 import _lib
+    el.set_assembly("gather")
+    for _ in range(max(2, warmup)):
+        el.update_and_assemble(d_ddu, d_ff, d_csr)
+    ms_g = time_steps(torch, el, stream, steps, d_ddu, d_ff, d_csr)
+    L.pms_elements_set_timing(el.h, 1)
+    L.pms_elements_kernel_times(el.h, None, None)
+    for _ in range(steps):
+        el.update_and_assemble(d_ddu, d_ff, d_csr)
+    kt = np.zeros(3)
+    kc = np.zeros(3, np.int64)
+    L.pms_elements_kernel_times(el.h, _lib.ptr(kt), _lib.ptr(kc))
+    L.pms_elements_set_timing(el.h, 0)
+    el.set_assembly("direct")
+    el.update_and_assemble(d_ddu, d_ff, d_csr)
+    el.sync()
+    return {"gather_ms_per_step": ms_g,
+            "gather_kernels_ms_per_step": {"element_dense": kt[0] / max(kc[0], 1), "f_gather": kt[1] / max(kc[1], 1),
+                                           "kk_gather": kt[2] / max(kc[2], 1)},
+            "note": "gather assembly: element kernel writes dense K_e/F_e, row gathers sum them (same bits)"}
 
 
 def run_batched(nprob, nalone, seed=2024):
@@ -778,6 +796,9 @@ def main():
         gpu_csr = d_csr.cpu().numpy()
         el_pattern = el.csr_pattern()
 
+    # the same step with the gather assembly (same bits), for the A/B of the direct assembly
+    ab = assembly_ab(torch, L, el, stream, min(args.steps, 10), args.warmup, d_ddu, d_ff, d_csr)
+
     # e2e through the C ABI with host buffers (pinned): dU in, R and CSR values out, every step
     e2e = None
     if not args.no_e2e:
@@ -827,7 +848,7 @@ def main():
     if args.served > 0 and args.size == "full":
         torch.cuda.empty_cache()
         served = run_served(args.served, args.rate, args.alone_sample, detail_file=args.served_detail)
-    ms_elem = kt[0] / max(kc[0], 1)
+    ms_elem = kt[0] / max(kc[0], 1)  # the element kernel is the whole step (direct assembly)
     fl_ip = flops_per_ip_hex20()
     achieved_tf = nip * fl_ip / (ms_elem * 1e-3) / 1e12
     alg_bytes = algorithmic_bytes_step(m, ng, nnz)
@@ -862,16 +883,18 @@ def main():
                    "plastic_fraction": plastic, "l2": "inputs larger than L2 (no flush)",
                    "parallelism": f"replica per GPU x{world}"},
         "roofline": {"bound": "fp64", "achieved": achieved_tf, "peak": fp64, "unit": "TFLOP/s",
-                     "frac": achieved_tf / fp64, "traffic": ELEMENT_DRAM_BYTES_PER_CELL * m.ncell,
-                     "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of the 32x32x16 "
-                                       "capture, scaled by cells to this launch",
-                     "kernel": "element_kernel<3,20> (fused update + B^T sigma + B^T D B)",
+                     "frac": achieved_tf / fp64,
+                     "traffic": ELEMENT_DRAM_BYTES_PER_CELL * m.ncell if ELEMENT_DRAM_BYTES_PER_CELL else None,
+                     "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch on a "
+                                       "smaller block, scaled by cells to this launch",
+                     "kernel": "element_kernel<3,20,UPD_BACKUP,F,K,CSR> (fused update + B^T sigma + B^T D B, "
+                               "blocks added straight into the CSR values and R)",
                      "flop_per_ip": fl_ip, "peak_source": "FP64 FMA probe measured in this run"},
         "roofline_hbm": {"bound": "hbm", "achieved": step_gbs, "peak": peaks["hbm_gbs"], "unit": "GB/s",
                          "frac": step_gbs / peaks["hbm_gbs"], "algorithmic_bytes_per_step": alg_bytes,
                          "peak_source": peaks_kind},
-        "kernels_ms_per_step": {"element": ms_elem, "f_gather": kt[1] / max(kc[1], 1),
-                                "kk_gather": kt[2] / max(kc[2], 1)},
+        "kernels_ms_per_step": {"element": ms_elem},
+        "assembly_ab": ab,
         "gpu_launches": int(launches),
         "e2e": e2e, "cpu_baseline": cpu, "parity": parity, "k1_microbench": k1, "ep_microbench": ep, "qua8_step": qua8, "batched": batched, "served": served, "c0_footing": c0, "fp64_peak_tflops": fp64,
         "clocks": clk,

@@ -38,8 +38,9 @@ enum pms_status_code {
     PMS_ERR_NUMERATOR = 10,   /* "plastic numerator (df/dsigma : De : deps) is overly negative"
                                  (elastoplastic.rs:193-195) */
     PMS_ERR_ODE = 11,         /* the elastoplastic ODE took more than max_steps steps */
-    PMS_ERR_INTERSECTION = 12 /* no crossing found although the trial point lies outside the yield
+    PMS_ERR_INTERSECTION = 12, /* no crossing found although the trial point lies outside the yield
                                  surface (the reference asserts, elastoplastic.rs:484) */
+    PMS_ERR_ORDER = 13        /* internal: a wait of the ordered CSR assembly timed out (no counterpart) */
 };
 
 /* ---- element kinds (gemlab GeoKind subset used by solids) ---------------------------------- */
@@ -93,7 +94,7 @@ typedef struct pms_elements_info {
     int64_t nnz;                               /* CSR nonzeros of K (full, both triangles) */
     int64_t nblock_upper;                      /* node-pair blocks with A <= B */
     int64_t ncontrib;                          /* element blocks summed into them */
-    int64_t device_bytes;                      /* device memory held by the handle */
+    int64_t device_bytes;                      /* device memory held by the handle so far */
 } pms_elements_info;
 
 typedef struct pms_elements pms_elements; /* opaque; not thread-safe; one CUDA stream per handle */
@@ -146,6 +147,17 @@ int pms_element_calc_jacobian(pms_elements* h, int64_t cell, double* kk);
  * sig[nip*ncomp] (Mandel), ivs[nip*2] = [z, lambda], elastic[nip]; host buffers */
 int pms_elements_get_state(pms_elements* h, double* sig, double* ivs, uint8_t* elastic);
 int pms_elements_set_state(pms_elements* h, const double* sig, const double* ivs, const uint8_t* elastic);
+
+/* How K and R are assembled (no counterpart in the reference, whose COO triplets are summed by the
+ * sparse solver, src/base/assembly.rs:70-139).  Both give the same bits: every entry is the sum of
+ * its cells' contributions in ascending cell order.
+ *   PMS_ASSEMBLY_DIRECT (default): the element kernel adds each cell's blocks straight into the
+ *     CSR values and R, row by row in ascending cell order (per-row tickets); no element matrices
+ *     are stored.
+ *   PMS_ASSEMBLY_GATHER: the element kernel writes every cell's dense K_e and F_e, then gather
+ *     kernels sum them row by row (needs 8*ncell*(nnode*ndim)^2 bytes more device memory). */
+enum pms_assembly { PMS_ASSEMBLY_DIRECT = 0, PMS_ASSEMBLY_GATHER = 1 };
+int pms_elements_set_assembly(pms_elements* h, int32_t mode);
 
 /* Instrumentation: when on, every batched call records CUDA events around its kernels on the
  * handle's stream; pms_elements_kernel_times waits for the stream and returns the summed device

@@ -16,6 +16,13 @@ LIB_PATH = os.path.join(HERE, "libpms_b200.so")
 PMS_OK = 0
 PMS_MEM_HOST = 0
 PMS_MEM_DEVICE = 1
+PMS_ERR_INVALID = 1
+PMS_ERR_ZERO_SIGMA_D = 3
+PMS_ERR_ZERO_NORM_S = 4
+PMS_ERR_JACOBIAN = 5
+PMS_ERR_ORDER = 13
+PMS_ASSEMBLY_DIRECT = 0
+PMS_ASSEMBLY_GATHER = 1
 LINEAR_ELASTIC = 0
 VON_MISES = 1
 
@@ -28,6 +35,11 @@ ERRORS = {
     6: "out of device memory",
     7: "unsupported idealization or element kind",
     8: "batch too large for the fixed scratch of the no-allocation entry point",
+    9: "cannot compute df/dsigma due to singularity",
+    10: "plastic numerator (df/dsigma : De : deps) is overly negative",
+    11: "the elastoplastic ODE took more than max_steps steps",
+    12: "no yield-surface crossing found",
+    13: "ordered assembly: a wait for an earlier cell timed out (internal error)",
 }
 
 
@@ -112,6 +124,7 @@ SIGNATURES = {
     "pms_vm_update_and_stiffness_host": (_I, [ctypes.POINTER(Material_), _I, _I64, _V, _V, _V, _V, _V, _V, _V]),
     "pms_mesh_csr_pattern": (_I, [ctypes.POINTER(Mesh_), _V, _V, ctypes.POINTER(_I64)]),
     "pms_elements_set_timing": (_I, [_V, _I]),
+    "pms_elements_set_assembly": (_I, [_V, _I]),
     "pms_elements_kernel_times": (_I, [_V, _V, _V]),
     "pms_probe_fp64_fma": (_I, [_I64, _I, _V, _V]),
     "pms_element_calc_noalloc": (_I, [_I, _I, _D, ctypes.POINTER(Material_), _I64, _V, _V, _V, _V, _V, _V,

@@ -13,7 +13,8 @@ constexpr double INV_SQRT2 = 0.7071067811865476;
 constexpr double SQRT_2_BY_3 = 0.816496580927726;
 constexpr double F_TOL = 1e-6;  // elastic-regime tolerance on f/z_ini (von_mises.rs:23)
 
-enum Err : int { OK = 0, E_INVALID = 1, E_CUDA = 2, E_ZERO_SIGMA_D = 3, E_ZERO_NORM_S = 4, E_JACOBIAN = 5 };
+enum Err : int { OK = 0, E_INVALID = 1, E_CUDA = 2, E_ZERO_SIGMA_D = 3, E_ZERO_NORM_S = 4, E_JACOBIAN = 5,
+                 E_ORDER = 13 };
 
 // Material constants in the form the kernels use.
 struct MatConst {

@@ -87,7 +87,61 @@ struct ElemArgs {
     int32_t nq = 0;
     const int64_t* q_off = nullptr;
     const int64_t* q_first = nullptr;
+    // dense outputs (no CSR): the fe / ke rows of cell c are c - ke_cell0
+    int64_t ke_cell0 = 0;
+    // direct assembly (CSR kernels): cell c adds its node-row slab a into block row A = conn[c][a]
+    // and its F_int share into R once ticket[A] equals c's rank among A's cells (crank), then
+    // advances the ticket; cells are taken in ascending order from the counter `next`
+    const int64_t* bptr = nullptr;       // block-row pointers [npoint + 1]
+    const int16_t* cslot = nullptr;      // [cell][a][b]: column slot of node b in block row conn[a]
+    const int32_t* crank = nullptr;      // [cell][a]: rank (bits 0..29), last-cell flag (bit 30)
+    int32_t* ticket = nullptr;           // [npoint]: slabs of this launch already added to the row
+    unsigned long long* next = nullptr;  // in-order work counter, zero at launch
+    double* csr = nullptr;               // CSR values of K (DOK)
+    double* ff = nullptr;                // R = F_int (DOF)
 };
+
+// Ordered-assembly tickets: acquire/release at GPU scope, so the slab a cell adds to a row is
+// visible to the next cell of that row before it reads the row.
+__device__ __forceinline__ int ticket_load(const int32_t* p) {
+    int v;
+    asm volatile("ld.acquire.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void ticket_store(int32_t* p, int v) {
+    asm volatile("st.release.gpu.global.s32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+// Polls of a row ticket before the kernel gives up (each poll sleeps up to ~1 us, so about 0.1 s):
+// far beyond any legitimate wait, which is the time one earlier cell takes to finish.  A wait that
+// runs out reports E_ORDER (rank 3 in the error key) and adds the slab anyway; every other wait of the
+// launch sees that key within 64 polls and stops waiting too, so the kernel always ends promptly.
+constexpr int ORDER_WAIT_LIMIT = 1 << 17;
+__device__ __forceinline__ bool order_aborted(const unsigned long long* errkey) {
+    return (*(volatile const unsigned long long*)errkey >> 56) >= 3;
+}
+
+// Next item of the in-order work counter, for the whole warp.
+__device__ __forceinline__ int64_t dequeue(unsigned long long* next) {
+    unsigned long long v = 0;
+    if ((threadIdx.x & 31) == 0) v = atomicAdd(next, 1ull);
+    return (int64_t)__shfl_sync(0xffffffffu, v, 0);
+}
+
+// One ND x ND block added into the CSR values: rows pos + i*rs, columns at the block's slot;
+// the first cell of the row stores 0 + v, later ones add to what is there (ascending cell order).
+template <int ND>
+__device__ __forceinline__ void csr_add_block(double* __restrict__ csr, int64_t pos, int rs, bool first,
+                                              const double (&v)[ND][ND], bool transpose) {
+    double old[ND][ND];
+#pragma unroll
+    for (int i = 0; i < ND; i++)
+#pragma unroll
+        for (int j = 0; j < ND; j++) old[i][j] = first ? 0.0 : __ldcg(csr + pos + (int64_t)i * rs + j);
+#pragma unroll
+    for (int i = 0; i < ND; i++)
+#pragma unroll
+        for (int j = 0; j < ND; j++) csr[pos + (int64_t)i * rs + j] = old[i][j] + (transpose ? v[j][i] : v[i][j]);
+}
 
 // Item i of a range queue: off[k] <= i < off[k+1] maps to first[k] + (i - off[k]).
 __device__ __forceinline__ int64_t queue_item(int64_t i, int n, const int64_t* __restrict__ off,
@@ -108,7 +162,7 @@ __device__ __forceinline__ int64_t queue_item(int64_t i, int n, const int64_t* _
 //   rank << 56 | (2^40 - 1 - cell) << 16 | (255 - ip) << 8 | code
 // (rank 2: update error, 1: tangent/assembly error) and atomicMax keeps the one the reference
 // would return: update errors first, then the lowest cell, then its lowest IP.
-constexpr int RANK_UPDATE = 2, RANK_TANGENT = 1;
+constexpr int RANK_ORDER = 3, RANK_UPDATE = 2, RANK_TANGENT = 1;
 __host__ __device__ constexpr unsigned long long error_key(int rank, int64_t cell, int ip, int code) {
     return ((unsigned long long)rank << 56) | ((((1ull << 40) - 1) - (unsigned long long)cell) << 16) |
            ((unsigned long long)(255 - ip) << 8) | (unsigned long long)(code & 0xff);
@@ -192,8 +246,9 @@ __host__ __device__ constexpr int smem_bytes_for(int nn, int nd, int ng, int wpb
     return (smem_table_doubles(nn, nd) + (wpb / warps_per_cell(nn)) * smem_cell_doubles(nn, nd, ng)) * 8;
 }
 
-template <int ND, int NN, int UPD, bool DOF, bool DOK>
+template <int ND, int NN, int UPD, bool DOF, bool DOK, bool CSR>
 __global__ void __launch_bounds__(WPB * 32, warps_per_cell(NN) == 2 ? 3 : (ND == 2 ? 4 : 1)) element_kernel(ElemArgs A) {
+    static_assert(!CSR || warps_per_cell(NN) == 1, "the ordered assembly takes one warp per cell");
     constexpr int NC = 2 * ND;
     constexpr int NE = NN * ND;
     constexpr int GS = NE + 1;  // gradient row stride (odd: spreads the banks of phase-1 stores)
@@ -234,9 +289,11 @@ __global__ void __launch_bounds__(WPB * 32, warps_per_cell(NN) == 2 ? 3 : (ND ==
         if constexpr (WPC == 1) __syncwarp();
         else asm volatile("bar.sync %0, %1;" ::"r"(1 + cs), "r"(32 * WPC) : "memory");
     };
-    // persistent: the block's cell slots walk the queue with a stride of the whole grid
+    // persistent: the block's cell slots walk the queue with a stride of the whole grid, or (direct
+    // assembly) take the next cell from the in-order counter
     const int64_t cstride = (int64_t)gridDim.x * CPB;
-    for (int64_t cl = (int64_t)blockIdx.x * CPB + cs; cl < A.ncell; cl += cstride) {
+    for (int64_t cl = CSR ? dequeue(A.next) : (int64_t)blockIdx.x * CPB + cs; cl < A.ncell;
+         cl = CSR ? dequeue(A.next) : cl + cstride) {
     cell_sync();  // the previous cell's write-out is done with the cell's shared memory
     const int64_t cell = A.nq ? queue_item(cl, A.nq, A.q_off, A.q_first) : A.cell0 + cl;
     int mode = (UPD == UPD_NONE) ? 0 : 2;
@@ -422,17 +479,22 @@ __global__ void __launch_bounds__(WPB * 32, warps_per_cell(NN) == 2 ? 3 : (ND ==
                 f[2 % ND] += c6[5 % 6] * g[0] + c6[4 % 6] * g[1] + c6[3 % 6] * g[2 % ND];
             }
         }
+        // direct assembly: kept in the cell's dU slot (free after phase 1) until the scatter
 #pragma unroll
-        for (int i = 0; i < ND; i++) A.fe[(cell * NN + lane) * ND + i] = f[i];
+        for (int i = 0; i < ND; i++) {
+            if (CSR) Us[lane * ND + i] = f[i];
+            else A.fe[((cell - A.ke_cell0) * NN + lane) * ND + i] = f[i];
+        }
     }
 
     }  // warp 0
     cell_sync();  // G and TC are visible to every warp of the cell
 
     // ---------------- phase 2: lane owns a tile of node-pair blocks ----------------
+    int ti = -1, tj = -1;
+    double acc[RT][CT][ND][ND];
     if (DOK) {
         // tile number lane + 32*half: (i, j) with i*RT <= min(j*CT + CT - 1, NN - 1), row-major
-        int ti = -1, tj = -1;
         {
             const int me = lane + 32 * half;
             int k = 0;
@@ -446,7 +508,6 @@ __global__ void __launch_bounds__(WPB * 32, warps_per_cell(NN) == 2 ? 3 : (ND ==
                 }
         }
         const int a0 = ti * RT, b0 = tj * CT;
-        double acc[RT][CT][ND][ND];
 #pragma unroll
         for (int r = 0; r < RT; r++)
 #pragma unroll
@@ -568,12 +629,13 @@ __global__ void __launch_bounds__(WPB * 32, warps_per_cell(NN) == 2 ? 3 : (ND ==
                     for (int r = 0; r < RT; r++) acc[r][c][0][0] = fma(Qr[r], qb, acc[r][c][0][0]);
             }
         }
-        // write K_e (row-major NE x NE) through the warp's shared memory, RS node rows at a time:
+        // dense output: write K_e (row-major NE x NE) through the warp's shared memory, RS node rows at a time:
         // each lane drops its blocks (a, b) and mirrors (b, a) into the staged rows, then the warp
         // copies the rows out with contiguous stores
+        if constexpr (!CSR) {
         const int RS = min(NN, smem_cell_doubles(NN, ND, ng) / (ND * NE));
         double* stage = wbase;
-        double* kc = A.ke + cell * (int64_t)(NE * NE);
+        double* kc = A.ke + (cell - A.ke_cell0) * (int64_t)(NE * NE);
         for (int r0 = 0; r0 < NN; r0 += RS) {
             cell_sync();
             if (ti >= 0) {
@@ -604,6 +666,95 @@ __global__ void __launch_bounds__(WPB * 32, warps_per_cell(NN) == 2 ? 3 : (ND ==
             const int n = min(RS, NN - r0) * ND * NE;
             double* dst = kc + (int64_t)r0 * ND * NE;
             for (int t = lane + 32 * half; t < n; t += 32 * WPC) dst[t] = stage[t];
+        }
+        }  // dense output
+    }
+    // ---------------- direct assembly: ordered scatter into the CSR values and R ----------------
+    // Node lane m adds slab m (block row A = conn[m]) once ticket[A] equals this cell's rank among
+    // A's cells; every lane adds the blocks of its tile that lie in the ready rows -- (a, b) into row
+    // a and the mirror (b, a) into row b -- and node lane m then advances ticket[A] (the last cell of
+    // A puts it back to 0 for the next launch).  Rows become ready in rounds, so this cell never
+    // waits for a row it could already write: no wait chains along the cell order.
+    if constexpr (CSR) {
+        if (DOF || DOK) {
+            int64_t rowA = 0, pos_m = 0;
+            int rs_m = 0, rank_m = 0;
+            bool last_m = false, todo = false;
+            if (lane < NN) {
+                rowA = A.conn[cell * NN + lane];
+                const int64_t r0 = __ldg(A.bptr + rowA), r1 = __ldg(A.bptr + rowA + 1);
+                pos_m = (int64_t)ND * ND * r0;
+                rs_m = ND * (int)(r1 - r0);
+                const int32_t cr = __ldg(A.crank + cell * NN + lane);
+                rank_m = cr & CRANK_MASK;
+                last_m = (cr & CRANK_LAST) != 0;
+                todo = true;
+            }
+            const int a0 = max(ti, 0) * RT, b0 = max(tj, 0) * CT;
+            int64_t posR[RT], posC[CT];
+            int rsR[RT], rsC[CT];
+            bool fR[RT], fC[CT];
+#pragma unroll
+            for (int r = 0; r < RT; r++) {
+                const int src = min(a0 + r, NN - 1);
+                posR[r] = __shfl_sync(FULL, pos_m, src);
+                rsR[r] = __shfl_sync(FULL, rs_m, src);
+                fR[r] = __shfl_sync(FULL, rank_m, src) == 0;
+            }
+#pragma unroll
+            for (int c = 0; c < CT; c++) {
+                const int src = min(b0 + c, NN - 1);
+                posC[c] = __shfl_sync(FULL, pos_m, src);
+                rsC[c] = __shfl_sync(FULL, rs_m, src);
+                fC[c] = __shfl_sync(FULL, rank_m, src) == 0;
+            }
+            const int16_t* cs_cell = A.cslot + cell * (int64_t)(NN * NN);
+            int spins = 0;
+            while (true) {
+                const unsigned todo_mask = __ballot_sync(FULL, todo);
+                if (!todo_mask) break;
+                bool ready = todo && ticket_load(A.ticket + rowA) == rank_m;
+                unsigned rmask = __ballot_sync(FULL, ready);
+                if (!rmask) {
+                    ++spins;
+                    const bool give_up = __shfl_sync(FULL, spins >= ORDER_WAIT_LIMIT || ((spins & 63) == 0 && order_aborted(A.errkey)), 0);
+                    if (!give_up) {
+                        __nanosleep(spins < 16 ? 32 : 1024);
+                        continue;
+                    }
+                    if (lane == 0) report(A, RANK_ORDER, E_ORDER, cell, 0);
+                    ready = todo;
+                    rmask = todo_mask;
+                }
+                __threadfence();  // the rows' earlier slabs are visible to every lane
+                if (DOF && ready) {
+#pragma unroll
+                    for (int i = 0; i < ND; i++) {
+                        double* q = A.ff + rowA * ND + i;
+                        *q = (rank_m == 0 ? 0.0 : __ldcg(q)) + Us[lane * ND + i];
+                    }
+                }
+                if (DOK && ti >= 0) {
+#pragma unroll
+                    for (int r = 0; r < RT; r++)
+#pragma unroll
+                        for (int c = 0; c < CT; c++) {
+                            const int a = a0 + r, b = b0 + c;
+                            if (a < NN && b < NN && a <= b) {
+                                if ((rmask >> a) & 1u)
+                                    csr_add_block<ND>(A.csr, posR[r] + ND * (int64_t)cs_cell[a * NN + b], rsR[r], fR[r],
+                                                      acc[r][c], false);
+                                if (a != b && ((rmask >> b) & 1u))
+                                    csr_add_block<ND>(A.csr, posC[c] + ND * (int64_t)cs_cell[b * NN + a], rsC[c], fC[c],
+                                                      acc[r][c], true);
+                            }
+                        }
+                }
+                __threadfence();  // this round's slabs are visible before their tickets move
+                __syncwarp();
+                if (ready) ticket_store(A.ticket + rowA, last_m ? 0 : rank_m + 1);
+                todo = todo && !ready;
+            }
         }
     }
     }  // cells
@@ -657,7 +808,7 @@ template <int NN> __host__ __device__ constexpr int lanes_packed() {
 }
 template <int NN> __host__ __device__ constexpr bool packed_layout() { return 32 / lanes_packed<NN>() >= 3; }
 
-template <int NN, int LPC, int UPD, bool DOF, bool DOK>
+template <int NN, int LPC, int UPD, bool DOF, bool DOK, bool CSR>
 __global__ void __launch_bounds__(WPB2 * 32, 4) element2d_kernel(ElemArgs A) {
     constexpr int NE = 2 * NN, GS = NE + 2;
     constexpr int CPW = 32 / LPC;  // cells per warp
@@ -709,7 +860,9 @@ __global__ void __launch_bounds__(WPB2 * 32, 4) element2d_kernel(ElemArgs A) {
     }
 
     const int64_t ngroup = (A.ncell + CPW - 1) / CPW;
-    for (int64_t pr = (int64_t)blockIdx.x * WPB2 + wid; pr < ngroup; pr += (int64_t)gridDim.x * WPB2) {
+    // groups of CPW consecutive cells: grid-strided, or (direct assembly) from the in-order counter
+    for (int64_t pr = CSR ? dequeue(A.next) : (int64_t)blockIdx.x * WPB2 + wid; pr < ngroup;
+         pr = CSR ? dequeue(A.next) : pr + (int64_t)gridDim.x * WPB2) {
         __syncwarp();  // the previous group's write-out is done with the cells' shared memory
         // every lane looks at all cells of the group, so the choices below agree across the warp;
         // a slot without a cell repeats the group's first cell and writes nothing
@@ -907,16 +1060,19 @@ __global__ void __launch_bounds__(WPB2 * 32, 4) element2d_kernel(ElemArgs A) {
                 f[1] += c6[2] * g[0] + c6[1] * g[1];
                 if (A.axisym) f[0] += c6[3] * Ns[hl * 16 + p] / c6[4];
             }
-            if (active) {
-                A.fe[(cell * NN + hl) * 2] = f[0];
-                A.fe[(cell * NN + hl) * 2 + 1] = f[1];
+            if (CSR) {  // kept in the cell's dU slot (free after phase 1) until the scatter
+                Us[hl * 2] = f[0];
+                Us[hl * 2 + 1] = f[1];
+            } else if (active) {
+                A.fe[((cell - A.ke_cell0) * NN + hl) * 2] = f[0];
+                A.fe[((cell - A.ke_cell0) * NN + hl) * 2 + 1] = f[1];
             }
         }
 
         // ---------------- phase 2: lane owns a tile of node-pair blocks ----------------
+        double acc[T][T][2][2];
         if (DOK) {
             const int a0 = ti * T, b0 = tj * T;
-            double acc[T][T][2][2];
 #pragma unroll
             for (int r = 0; r < T; r++)
 #pragma unroll
@@ -995,6 +1151,7 @@ __global__ void __launch_bounds__(WPB2 * 32, 4) element2d_kernel(ElemArgs A) {
                     }
                 }
             }
+            if constexpr (!CSR) {  // dense output
             __syncwarp();  // both halves are done reading the cell areas that the staging overwrites
             // stage K_e row-major in the cell area (blocks (a, b) and their mirrors (b, a)), then
             // copy it out with 16-byte stores, LPC*16 contiguous bytes per cell and store
@@ -1018,9 +1175,96 @@ __global__ void __launch_bounds__(WPB2 * 32, 4) element2d_kernel(ElemArgs A) {
             }
             __syncwarp();
             if (active && hl < LPC) {
-                double2* dst = reinterpret_cast<double2*>(A.ke + cell * (int64_t)(NE * NE));
+                double2* dst = reinterpret_cast<double2*>(A.ke + (cell - A.ke_cell0) * (int64_t)(NE * NE));
                 const double2* s2 = reinterpret_cast<const double2*>(stage);
                 for (int t = hl; t < NE * NE / 2; t += LPC) dst[t] = s2[t];
+            }
+            }  // dense output
+        }
+        // ---------------- direct assembly: ordered scatter into the CSR values and R ----------------
+        // As in element_kernel, with the CPW cells of the warp in one round structure: node lane
+        // (slot h, node m) adds slab m of cell h once ticket[conn[m]] equals that cell's rank, the
+        // tile lanes add their blocks of the ready rows, and a row shared by two cells of the warp is
+        // added by the lower one first (its rank is lower).  Slots without a cell add nothing.
+        if constexpr (CSR) {
+            if (DOF || DOK) {
+                const int sb = LPC * hh;  // first lane of this slot
+                int64_t rowA = 0, pos_m = 0;
+                int rs_m = 0, rank_m = 0;
+                bool last_m = false, todo = false;
+                if (active && hl < NN) {
+                    rowA = A.conn[cell * NN + hl];
+                    const int64_t r0 = __ldg(A.bptr + rowA), r1 = __ldg(A.bptr + rowA + 1);
+                    pos_m = 4 * r0;
+                    rs_m = 2 * (int)(r1 - r0);
+                    const int32_t cr = __ldg(A.crank + cell * NN + hl);
+                    rank_m = cr & CRANK_MASK;
+                    last_m = (cr & CRANK_LAST) != 0;
+                    todo = true;
+                }
+                const int a0 = max(ti, 0) * T, b0 = max(tj, 0) * T;
+                int64_t posR[T], posC[T];
+                int rsR[T], rsC[T];
+                bool fR[T], fC[T];
+#pragma unroll
+                for (int r = 0; r < T; r++) {
+                    const int src = sb + min(a0 + r, NN - 1);
+                    posR[r] = __shfl_sync(FULL, pos_m, src);
+                    rsR[r] = __shfl_sync(FULL, rs_m, src);
+                    fR[r] = __shfl_sync(FULL, rank_m, src) == 0;
+                    const int srcc = sb + min(b0 + r, NN - 1);
+                    posC[r] = __shfl_sync(FULL, pos_m, srcc);
+                    rsC[r] = __shfl_sync(FULL, rs_m, srcc);
+                    fC[r] = __shfl_sync(FULL, rank_m, srcc) == 0;
+                }
+                const int16_t* cs_cell = A.cslot + cell * (int64_t)(NN * NN);
+                int spins = 0;
+                while (true) {
+                    const unsigned todo_mask = __ballot_sync(FULL, todo);
+                    if (!todo_mask) break;
+                    bool ready = todo && ticket_load(A.ticket + rowA) == rank_m;
+                    unsigned rmask = __ballot_sync(FULL, ready);
+                    if (!rmask) {
+                        ++spins;
+                        const bool give_up = __shfl_sync(FULL, spins >= ORDER_WAIT_LIMIT || ((spins & 63) == 0 && order_aborted(A.errkey)), 0);
+                        if (!give_up) {
+                            __nanosleep(spins < 16 ? 32 : 1024);
+                            continue;
+                        }
+                        if (lane == 0) report(A, RANK_ORDER, E_ORDER, cell, 0);
+                        ready = todo;
+                        rmask = todo_mask;
+                    }
+                    __threadfence();  // the rows' earlier slabs are visible to every lane
+                    if (DOF && ready) {
+#pragma unroll
+                        for (int i = 0; i < 2; i++) {
+                            double* q = A.ff + rowA * 2 + i;
+                            *q = (rank_m == 0 ? 0.0 : __ldcg(q)) + Us[hl * 2 + i];
+                        }
+                    }
+                    if (DOK && active && ti >= 0) {
+                        const unsigned mine = rmask >> sb;
+#pragma unroll
+                        for (int r = 0; r < T; r++)
+#pragma unroll
+                            for (int c = 0; c < T; c++) {
+                                const int a = a0 + r, b = b0 + c;
+                                if (a < NN && b < NN && a <= b) {
+                                    if ((mine >> a) & 1u)
+                                        csr_add_block<2>(A.csr, posR[r] + 2 * (int64_t)cs_cell[a * NN + b], rsR[r], fR[r],
+                                                         acc[r][c], false);
+                                    if (a != b && ((mine >> b) & 1u))
+                                        csr_add_block<2>(A.csr, posC[c] + 2 * (int64_t)cs_cell[b * NN + a], rsC[c], fC[c],
+                                                         acc[r][c], true);
+                                }
+                            }
+                    }
+                    __threadfence();  // this round's slabs are visible before their tickets move
+                    __syncwarp();
+                    if (ready) ticket_store(A.ticket + rowA, last_m ? 0 : rank_m + 1);
+                    todo = todo && !ready;
+                }
             }
         }
     }  // pairs
@@ -1207,8 +1451,15 @@ struct pms_elements {
     uint8_t* d_el = nullptr;
     double *d_sig_b = nullptr, *d_z_b = nullptr, *d_lam_b = nullptr;
     uint8_t* d_el_b = nullptr;
-    double* d_fe = nullptr;
+    double* d_fe = nullptr;  // dense F_e / K_e of every cell (gather assembly only; allocated on first use)
     double* d_ke = nullptr;
+    double* d_fe1 = nullptr;  // dense F_e / K_e of one cell (per-cell calls)
+    double* d_ke1 = nullptr;
+    int16_t* d_cslot = nullptr;    // direct assembly: per-cell slot map
+    int32_t* d_crank = nullptr;    // direct assembly: per-cell incidence ranks
+    int32_t* d_ticket = nullptr;   // direct assembly: per-node tickets (zero between launches)
+    unsigned long long* d_next = nullptr;  // direct assembly: in-order work counter
+    int assembly = PMS_ASSEMBLY_DIRECT;
     int64_t* d_inc_ptr = nullptr;
     int32_t* d_inc = nullptr;
     int64_t* d_bptr = nullptr;
@@ -1313,10 +1564,10 @@ int64_t resident_blocks(const void* kern, int smem, int threads = WPB * 32) {
 }
 
 // 2D cells with at most 16 integration points: LPC lanes per cell, 32/LPC cells per warp
-template <int NN, int LPC, int UPD, bool DOF, bool DOK>
+template <int NN, int LPC, int UPD, bool DOF, bool DOK, bool CSR>
 void launch_elem2d_lpc(const ElemArgs& a, cudaStream_t st, bool persistent) {
     constexpr int CPW = 32 / LPC;
-    auto kern = element2d_kernel<NN, LPC, UPD, DOF, DOK>;
+    auto kern = element2d_kernel<NN, LPC, UPD, DOF, DOK, CSR>;
     const int smem = smem2_bytes(NN, a.ngauss, CPW);
     static thread_local bool configured = false;
     if (!configured) {
@@ -1325,30 +1576,31 @@ void launch_elem2d_lpc(const ElemArgs& a, cudaStream_t st, bool persistent) {
         configured = true;
     }
     int64_t blocks = ((a.ncell + CPW - 1) / CPW + WPB2 - 1) / WPB2;
-    if (persistent) blocks = std::min<int64_t>(blocks, resident_blocks((const void*)kern, smem, WPB2 * 32));
+    if (persistent || CSR) blocks = std::min<int64_t>(blocks, resident_blocks((const void*)kern, smem, WPB2 * 32));
+    if (CSR) cudaMemsetAsync(a.next, 0, sizeof(unsigned long long), st);
     kern<<<(unsigned)std::max<int64_t>(blocks, 1), WPB2 * 32, smem, st>>>(a);
 }
 
-template <int NN, int UPD, bool DOF, bool DOK>
+template <int NN, int UPD, bool DOF, bool DOK, bool CSR>
 void launch_elem2d_t(const ElemArgs& a, cudaStream_t st, bool persistent) {
     if constexpr (packed_layout<NN>()) {
         if (a.ngauss <= lanes_packed<NN>()) {
-            launch_elem2d_lpc<NN, lanes_packed<NN>(), UPD, DOF, DOK>(a, st, persistent);
+            launch_elem2d_lpc<NN, lanes_packed<NN>(), UPD, DOF, DOK, CSR>(a, st, persistent);
             return;
         }
     }
-    launch_elem2d_lpc<NN, 16, UPD, DOF, DOK>(a, st, persistent);
+    launch_elem2d_lpc<NN, 16, UPD, DOF, DOK, CSR>(a, st, persistent);
 }
 
-template <int ND, int NN, int UPD, bool DOF, bool DOK>
+template <int ND, int NN, int UPD, bool DOF, bool DOK, bool CSR>
 void launch_elem_t(pms_elements* h, const ElemArgs& a) {
     if constexpr (ND == 2) {
         if (a.ngauss <= NG2_MAX) {
-            launch_elem2d_t<NN, UPD, DOF, DOK>(a, h->stream, true);
+            launch_elem2d_t<NN, UPD, DOF, DOK, CSR>(a, h->stream, true);
             return;
         }
     }
-    auto kern = element_kernel<ND, NN, UPD, DOF, DOK>;
+    auto kern = element_kernel<ND, NN, UPD, DOF, DOK, CSR>;
     static thread_local bool configured = false;
     if (!configured) {
         cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
@@ -1356,55 +1608,64 @@ void launch_elem_t(pms_elements* h, const ElemArgs& a) {
     }
     int64_t blocks = (a.ncell + cells_per_block(NN) - 1) / cells_per_block(NN);
     blocks = std::min<int64_t>(blocks, resident_blocks((const void*)kern, h->smem_bytes));
+    if (CSR) cudaMemsetAsync(a.next, 0, sizeof(unsigned long long), h->stream);
     kern<<<(unsigned)blocks, WPB * 32, h->smem_bytes, h->stream>>>(a);
 }
 
+// upd: UPD_NONE / UPD_CURRENT / UPD_BACKUP; csr: direct assembly into a.csr / a.ff (else dense
+// fe / ke outputs).  Update-only launches (no output) have no assembly.
 template <int ND, int NN>
-void launch_elem_nn(pms_elements* h, const ElemArgs& a, int upd, bool dof, bool dok) {
+void launch_elem_nn(pms_elements* h, const ElemArgs& a, int upd, bool dof, bool dok, bool csr) {
+    if (!dof && !dok) {
+        if (upd == UPD_CURRENT) launch_elem_t<ND, NN, UPD_CURRENT, false, false, false>(h, a);
+        else launch_elem_t<ND, NN, UPD_BACKUP, false, false, false>(h, a);
+        return;
+    }
     if (upd == UPD_NONE) {
-        if (dof && dok) launch_elem_t<ND, NN, UPD_NONE, true, true>(h, a);
-        else if (dof) launch_elem_t<ND, NN, UPD_NONE, true, false>(h, a);
-        else launch_elem_t<ND, NN, UPD_NONE, false, true>(h, a);
+        if (csr) {
+            if (dof && dok) launch_elem_t<ND, NN, UPD_NONE, true, true, true>(h, a);
+            else if (dof) launch_elem_t<ND, NN, UPD_NONE, true, false, true>(h, a);
+            else launch_elem_t<ND, NN, UPD_NONE, false, true, true>(h, a);
+        } else {
+            if (dof && dok) launch_elem_t<ND, NN, UPD_NONE, true, true, false>(h, a);
+            else if (dof) launch_elem_t<ND, NN, UPD_NONE, true, false, false>(h, a);
+            else launch_elem_t<ND, NN, UPD_NONE, false, true, false>(h, a);
+        }
     } else if (upd == UPD_CURRENT) {
-        if (dof || dok) launch_elem_t<ND, NN, UPD_CURRENT, true, true>(h, a);
-        else launch_elem_t<ND, NN, UPD_CURRENT, false, false>(h, a);
+        if (csr) launch_elem_t<ND, NN, UPD_CURRENT, true, true, true>(h, a);
+        else launch_elem_t<ND, NN, UPD_CURRENT, true, true, false>(h, a);
     } else {
-        if (dof || dok) launch_elem_t<ND, NN, UPD_BACKUP, true, true>(h, a);
-        else launch_elem_t<ND, NN, UPD_BACKUP, false, false>(h, a);
+        if (csr) launch_elem_t<ND, NN, UPD_BACKUP, true, true, true>(h, a);
+        else launch_elem_t<ND, NN, UPD_BACKUP, true, true, false>(h, a);
     }
 }
 
-template <int ND, int NN>
-void launch_elem_modes(pms_elements* h, const ElemArgs& a) {
-    launch_elem_t<ND, NN, UPD_MODE, true, true>(h, a);
-}
-
-void launch_elem(pms_elements* h, const ElemArgs& a, int upd, bool dof, bool dok) {
-    if (upd == UPD_MODE) {
+void launch_elem(pms_elements* h, const ElemArgs& a, int upd, bool dof, bool dok, bool csr) {
+    if (upd == UPD_MODE) {  // batched solver: always the direct assembly
         switch (h->kind) {
-        case PMS_TRI3: launch_elem_modes<2, 3>(h, a); break;
-        case PMS_TRI6: launch_elem_modes<2, 6>(h, a); break;
-        case PMS_QUA4: launch_elem_modes<2, 4>(h, a); break;
-        case PMS_QUA8: launch_elem_modes<2, 8>(h, a); break;
-        case PMS_QUA9: launch_elem_modes<2, 9>(h, a); break;
-        case PMS_TET4: launch_elem_modes<3, 4>(h, a); break;
-        case PMS_TET10: launch_elem_modes<3, 10>(h, a); break;
-        case PMS_HEX8: launch_elem_modes<3, 8>(h, a); break;
-        case PMS_HEX20: launch_elem_modes<3, 20>(h, a); break;
+        case PMS_TRI3: launch_elem_t<2, 3, UPD_MODE, true, true, true>(h, a); break;
+        case PMS_TRI6: launch_elem_t<2, 6, UPD_MODE, true, true, true>(h, a); break;
+        case PMS_QUA4: launch_elem_t<2, 4, UPD_MODE, true, true, true>(h, a); break;
+        case PMS_QUA8: launch_elem_t<2, 8, UPD_MODE, true, true, true>(h, a); break;
+        case PMS_QUA9: launch_elem_t<2, 9, UPD_MODE, true, true, true>(h, a); break;
+        case PMS_TET4: launch_elem_t<3, 4, UPD_MODE, true, true, true>(h, a); break;
+        case PMS_TET10: launch_elem_t<3, 10, UPD_MODE, true, true, true>(h, a); break;
+        case PMS_HEX8: launch_elem_t<3, 8, UPD_MODE, true, true, true>(h, a); break;
+        case PMS_HEX20: launch_elem_t<3, 20, UPD_MODE, true, true, true>(h, a); break;
         }
         h->launches++;
         return;
     }
     switch (h->kind) {
-    case PMS_TRI3: launch_elem_nn<2, 3>(h, a, upd, dof, dok); break;
-    case PMS_TRI6: launch_elem_nn<2, 6>(h, a, upd, dof, dok); break;
-    case PMS_QUA4: launch_elem_nn<2, 4>(h, a, upd, dof, dok); break;
-    case PMS_QUA8: launch_elem_nn<2, 8>(h, a, upd, dof, dok); break;
-    case PMS_QUA9: launch_elem_nn<2, 9>(h, a, upd, dof, dok); break;
-    case PMS_TET4: launch_elem_nn<3, 4>(h, a, upd, dof, dok); break;
-    case PMS_TET10: launch_elem_nn<3, 10>(h, a, upd, dof, dok); break;
-    case PMS_HEX8: launch_elem_nn<3, 8>(h, a, upd, dof, dok); break;
-    case PMS_HEX20: launch_elem_nn<3, 20>(h, a, upd, dof, dok); break;
+    case PMS_TRI3: launch_elem_nn<2, 3>(h, a, upd, dof, dok, csr); break;
+    case PMS_TRI6: launch_elem_nn<2, 6>(h, a, upd, dof, dok, csr); break;
+    case PMS_QUA4: launch_elem_nn<2, 4>(h, a, upd, dof, dok, csr); break;
+    case PMS_QUA8: launch_elem_nn<2, 8>(h, a, upd, dof, dok, csr); break;
+    case PMS_QUA9: launch_elem_nn<2, 9>(h, a, upd, dof, dok, csr); break;
+    case PMS_TET4: launch_elem_nn<3, 4>(h, a, upd, dof, dok, csr); break;
+    case PMS_TET10: launch_elem_nn<3, 10>(h, a, upd, dof, dok, csr); break;
+    case PMS_HEX8: launch_elem_nn<3, 8>(h, a, upd, dof, dok, csr); break;
+    case PMS_HEX20: launch_elem_nn<3, 20>(h, a, upd, dof, dok, csr); break;
     }
     h->launches++;
 }
@@ -1434,6 +1695,11 @@ ElemArgs make_args(pms_elements* h, const double* ddu) {
     a.fe = h->d_fe;
     a.ke = h->d_ke;
     a.errkey = (unsigned long long*)h->d_status;
+    a.bptr = h->d_bptr;
+    a.cslot = h->d_cslot;
+    a.crank = h->d_crank;
+    a.ticket = h->d_ticket;
+    a.next = h->d_next;
     return a;
 }
 
@@ -1577,20 +1843,22 @@ int pms_elements_create(const pms_mesh* mesh, const pms_material* materials, int
          h->alloc(&h->d_lam, h->nip) && h->alloc(&h->d_el, h->nip) &&
          h->alloc(&h->d_sig_b, (size_t)h->nip * h->nc) && h->alloc(&h->d_z_b, h->nip) &&
          h->alloc(&h->d_lam_b, h->nip) && h->alloc(&h->d_el_b, h->nip) &&
-         h->alloc(&h->d_fe, (size_t)h->ncell * h->nn * h->nd) &&
-         h->alloc(&h->d_ke, (size_t)h->ncell * h->nn * h->nd * h->nn * h->nd) &&
+         h->alloc(&h->d_fe1, (size_t)h->nn * h->nd) &&
+         h->alloc(&h->d_ke1, (size_t)h->nn * h->nd * h->nn * h->nd) &&
          h->upload(&h->d_inc_ptr, h->pat.inc_ptr.data(), h->pat.inc_ptr.size()) &&
-         h->upload(&h->d_inc, h->pat.inc.data(), h->pat.inc.size()) &&
          h->upload(&h->d_bptr, h->pat.bptr.data(), h->pat.bptr.size()) &&
          h->upload(&h->d_bcol, h->pat.bcol.data(), h->pat.bcol.size()) &&
          h->upload(&h->d_kdiag, h->pat.kdiag.data(), h->pat.kdiag.size()) &&
-         h->upload(&h->d_slot, h->pat.slot.data(), h->pat.slot.size()) &&
+         h->upload(&h->d_cslot, h->pat.cslot.data(), h->pat.cslot.size()) &&
+         h->upload(&h->d_crank, h->pat.crank.data(), h->pat.crank.size()) &&
+         h->alloc(&h->d_ticket, (size_t)h->npoint) && h->alloc(&h->d_next, 1) &&
          h->alloc(&h->d_ddu, h->ndof) && h->alloc(&h->d_ff, h->ndof) && h->alloc(&h->d_status, 4);
     if (!ok) {
         delete h;
         return PMS_ERR_NOMEM;
     }
     cudaMemset(h->d_status, 0, 16);
+    cudaMemset(h->d_ticket, 0, (size_t)h->npoint * sizeof(int32_t));
     if (cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking) != cudaSuccess) {
         delete h;
         return PMS_ERR_CUDA;
@@ -1733,6 +2001,10 @@ static int finish_host(pms_elements* h) {
                         "von Mises stiffness cannot be computed with zero deviatoric norm (norm_s < 1e-10)");
         case E_JACOBIAN:
             return fail(h, PMS_ERR_JACOBIAN, "the determinant of the Jacobian must be positive");
+        case E_ORDER:  // the row tickets may be left mid-count: start the next launch from zero
+            cudaMemsetAsync(h->d_ticket, 0, (size_t)h->npoint * sizeof(int32_t), h->stream);
+            cudaStreamSynchronize(h->stream);
+            return fail(h, PMS_ERR_ORDER, "ordered assembly: a wait for an earlier cell timed out (internal error)");
         default:
             return fail(h, PMS_ERR_INVALID, "device error");
         }
@@ -1741,6 +2013,18 @@ static int finish_host(pms_elements* h) {
 }
 
 int pms_elements_sync(pms_elements* h) { return h ? finish_host(h) : PMS_ERR_INVALID; }
+
+// Buffers of the gather assembly (dense F_e / K_e of every cell, incidence and slot maps), made on
+// first use: the direct assembly needs none of them.
+static int ensure_gather(pms_elements* h) {
+    if (h->d_ke) return PMS_OK;
+    const size_t ne = (size_t)h->nn * h->nd;
+    if (!h->alloc(&h->d_fe, (size_t)h->ncell * ne) || !h->alloc(&h->d_ke, (size_t)h->ncell * ne * ne) ||
+        !h->upload(&h->d_inc, h->pat.inc.data(), h->pat.inc.size()) ||
+        !h->upload(&h->d_slot, h->pat.slot.data(), h->pat.slot.size()))
+        return fail(h, PMS_ERR_NOMEM, "out of device memory for the gather assembly");
+    return PMS_OK;
+}
 
 // Common path of the four batched calls.
 static int run(pms_elements* h, const double* ddu, double* ff, double* csr, int mem, int upd, bool dof, bool dok) {
@@ -1762,7 +2046,16 @@ static int run(pms_elements* h, const double* ddu, double* ff, double* csr, int 
     }
     dof = dof && d_ff;
     dok = dok && d_csr;
+    const bool direct = h->assembly == PMS_ASSEMBLY_DIRECT;
+    if (!direct && (dof || dok)) {
+        const int rc = ensure_gather(h);
+        if (rc) return rc;
+    }
     ElemArgs a = make_args(h, d_ddu);
+    if (direct) {
+        a.csr = d_csr;
+        a.ff = d_ff;
+    }
     auto timed = [h](int k, auto&& fn) {
         if (!h->timing) {
             fn();
@@ -1774,14 +2067,16 @@ static int run(pms_elements* h, const double* ddu, double* ff, double* csr, int 
         cudaEventRecord(e.second, h->stream);
         h->ev_pending[k].push_back(e);
     };
-    if (upd != UPD_NONE || dof || dok) timed(0, [&] { launch_elem(h, a, upd, dof, dok); });
-    if (dof) timed(1, [&] { launch_f_gather(h, d_ff); });
-    if (mem == PMS_MEM_DEVICE || !dok) {
-        if (dok) timed(2, [&] { launch_kk_gather(h, d_csr); });
+    if (upd != UPD_NONE || dof || dok) timed(0, [&] { launch_elem(h, a, upd, dof, dok, direct); });
+    if (dof && !direct) timed(1, [&] { launch_f_gather(h, d_ff); });
+    if (mem == PMS_MEM_DEVICE || !dok || direct) {
+        if (dok && !direct) timed(2, [&] { launch_kk_gather(h, d_csr); });
         int rc = cuda_check(h);
         if (rc) return rc;
         if (mem == PMS_MEM_HOST) {
             if (dof) cudaMemcpyAsync(ff, d_ff, (size_t)h->ndof * 8, cudaMemcpyDeviceToHost, h->stream);
+            if (dok && direct)
+                cudaMemcpyAsync(csr, d_csr, (size_t)h->nnz * 8, cudaMemcpyDeviceToHost, h->stream);
             return finish_host(h);
         }
         return PMS_OK;
@@ -1840,7 +2135,10 @@ static int one_cell(pms_elements* h, int64_t cell, bool dof, bool dok) {
     ElemArgs a = make_args(h, nullptr);
     a.ncell = 1;
     a.cell0 = cell;
-    launch_elem(h, a, UPD_NONE, dof, dok);
+    a.fe = h->d_fe1;  // dense outputs of this one cell
+    a.ke = h->d_ke1;
+    a.ke_cell0 = cell;
+    launch_elem(h, a, UPD_NONE, dof, dok, false);
     int rc = cuda_check(h);
     if (rc) return rc;
     return finish_host(h);
@@ -1850,8 +2148,7 @@ int pms_element_calc_f_int(pms_elements* h, int64_t cell, double* f) {
     if (!f) return PMS_ERR_INVALID;
     int rc = one_cell(h, cell, true, false);
     if (rc) return rc;
-    if (cudaMemcpy(f, h->d_fe + cell * h->nn * h->nd, (size_t)h->nn * h->nd * 8, cudaMemcpyDeviceToHost) !=
-        cudaSuccess)
+    if (cudaMemcpy(f, h->d_fe1, (size_t)h->nn * h->nd * 8, cudaMemcpyDeviceToHost) != cudaSuccess)
         return fail(h, PMS_ERR_CUDA, "copy failed");
     return PMS_OK;
 }
@@ -1861,7 +2158,7 @@ int pms_element_calc_jacobian(pms_elements* h, int64_t cell, double* kk) {
     int rc = one_cell(h, cell, false, true);
     if (rc) return rc;
     const int64_t ne = h->nn * h->nd;
-    if (cudaMemcpy(kk, h->d_ke + cell * ne * ne, (size_t)(ne * ne) * 8, cudaMemcpyDeviceToHost) != cudaSuccess)
+    if (cudaMemcpy(kk, h->d_ke1, (size_t)(ne * ne) * 8, cudaMemcpyDeviceToHost) != cudaSuccess)
         return fail(h, PMS_ERR_CUDA, "copy failed");
     return PMS_OK;
 }
@@ -1915,6 +2212,12 @@ int pms_elements_error_location(const pms_elements* h, int64_t* cell, int32_t* i
 }
 
 int64_t pms_elements_launch_count(const pms_elements* h) { return h ? h->launches : 0; }
+
+int pms_elements_set_assembly(pms_elements* h, int32_t mode) {
+    if (!h || (mode != PMS_ASSEMBLY_DIRECT && mode != PMS_ASSEMBLY_GATHER)) return PMS_ERR_INVALID;
+    h->assembly = mode;
+    return PMS_OK;
+}
 
 int pms_elements_set_timing(pms_elements* h, int32_t on) {
     if (!h) return PMS_ERR_INVALID;
@@ -2016,9 +2319,10 @@ int elements_run_modes(pms_elements* h, const int32_t* cell_prob, const int32_t*
         a.q_off = queue->cell_off;
         a.q_first = queue->cell_first;
     }
-    launch_elem(h, a, UPD_MODE, true, true);
-    launch_f_gather(h, ff, queue);
-    launch_kk_gather(h, csr, node_prob, pmode, queue);
+    a.csr = csr;  // direct assembly: rows of problems outside the pass are left as they are
+    a.ff = ff;
+    (void)node_prob;
+    launch_elem(h, a, UPD_MODE, true, true, true);
     return cuda_check(h);
 }
 
@@ -2084,11 +2388,11 @@ template <int ND, int NN, bool DOF, bool DOK>
 void noalloc_launch_t(const ElemArgs& a, int smem, cudaStream_t st) {
     if constexpr (ND == 2) {
         if (a.ngauss <= NG2_MAX) {
-            launch_elem2d_t<NN, UPD_NONE, DOF, DOK>(a, st, false);
+            launch_elem2d_t<NN, UPD_NONE, DOF, DOK, false>(a, st, false);
             return;
         }
     }
-    auto kern = element_kernel<ND, NN, UPD_NONE, DOF, DOK>;
+    auto kern = element_kernel<ND, NN, UPD_NONE, DOF, DOK, false>;
     cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
     kern<<<(unsigned)((a.ncell + cells_per_block(NN) - 1) / cells_per_block(NN)), WPB * 32, smem, st>>>(a);
 }

@@ -4,10 +4,14 @@
 // sparse solver sum them (src/base/assembly.rs:70-139, src/fem/linear_system.rs:132-164).
 // Here the pattern is built once per mesh.  Block row A of K (node A, ND x ND blocks) is the sum,
 // over the cells incident to A in ascending cell order, of the node-row slab (a, all b) of each
-// cell's dense element matrix, where a is A's local index in the cell.  The gather kernel owns
-// one block row, adds the slabs in that fixed order and writes the row once; slot[] says where
-// each local column node b of an incidence lands in the row.  No atomics: the same bits on every
-// run, and the same bits as summing each node-pair block over its cells in ascending order.
+// cell's element matrix, where a is A's local index in the cell.  Two assemblies use it, both
+// without atomics and with the same bits on every run (every node-pair block summed over its cells
+// in ascending order):
+//  * direct: the element kernel adds cell c's slab a into row A once the cells before c in A's
+//    incidence list have added theirs (rank[c*nn + a] = c's position in that list; a ticket per
+//    row counts the slabs added), at the columns cslot[(c*nn + a)*nn + b];
+//  * gather: a kernel owns one block row and adds the slabs of the cells' dense element matrices in
+//    that order (slot[k*nn + b]: where local node b of incidence k of A lands in the row).
 #pragma once
 #include <cstdint>
 #include <vector>
@@ -26,6 +30,11 @@ struct Pattern {
     std::vector<int32_t> kdiag;  // position of A in its own block row
     // slot[k*nn + b]: position, in block row A, of local node b of incidence k of A
     std::vector<int16_t> slot;
+    // per cell (direct assembly): cslot[(c*nn + a)*nn + b] = position, in block row conn[c][a], of
+    // node b; crank[c*nn + a] = position of c among the cells of node conn[c][a] (bits 0..29),
+    // bit 30 set when c is the last of them
+    std::vector<int16_t> cslot;
+    std::vector<int32_t> crank;
     int nbmax = 0;  // largest block row
     int64_t nblock() const { return (int64_t)bcol.size(); }
     int64_t nupper() const;  // blocks with A <= B
@@ -34,5 +43,8 @@ struct Pattern {
 // Returns false (with msg) when the mesh is inconsistent or too large for 31-bit codes.
 bool build_pattern(int nd, int nn, int64_t npoint, int64_t ncell, const int64_t* conn, Pattern& pat,
                    const char** msg);
+
+constexpr int32_t CRANK_LAST = 1 << 30;
+constexpr int32_t CRANK_MASK = CRANK_LAST - 1;
 
 }  // namespace pms

@@ -90,6 +90,12 @@ class Elements:
             self._pattern = (indptr, indices)
         return self._pattern
 
+    def set_assembly(self, mode):
+        """"direct" (default: blocks added straight into the CSR values and R in ascending cell
+        order) or "gather" (dense element matrices, then row gathers); the same bits either way."""
+        code = {"direct": _lib.PMS_ASSEMBLY_DIRECT, "gather": _lib.PMS_ASSEMBLY_GATHER}[mode]
+        self._check(self.L.pms_elements_set_assembly(self.h, code))
+
     def set_stream(self, stream):
         """stream: torch.cuda.Stream, a raw cudaStream_t, or None for the handle's own stream."""
         raw = getattr(stream, "cuda_stream", stream)

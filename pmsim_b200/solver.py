@@ -56,7 +56,8 @@ class Essential:
 
 class SolverImplicit:
     def __init__(self, elements: Elements, essential, loads=(), lagrange_mult_method=True, n_max_iterations=10,
-                 tol_rr_abs=1e-10, tol_mdu_rel=1e-8, t_ini=0.0, t_fin=1.0, ddt=1.0, verbose=False, natural=None):
+                 tol_rr_abs=1e-10, tol_mdu_rel=1e-8, t_ini=0.0, t_fin=1.0, ddt=1.0, verbose=False, natural=None,
+                 constant_tangent=False):
         self.el = elements
         self.ndof = elements.ndof
         ess = essential if isinstance(essential, Essential) else Essential.from_list(essential)
@@ -81,6 +82,9 @@ class SolverImplicit:
         self.timing = {"elements": 0.0, "solve": 0.0}
         self.verbose = verbose
         self.natural = natural  # object with ff_ext(t) -> F_ext over the DOFs (pmsim_b200.natural.Natural)
+        # Config::constant_tangent (src/base/config.rs:38): K is assembled and factorised at the first
+        # iteration of each step only (src/fem/solver_implicit.rs:216), later iterations reuse it
+        self.constant_tangent = constant_tangent
 
     def _ff_ext(self, t):
         ffe = np.zeros(self.neq_total)
@@ -142,7 +146,8 @@ class SolverImplicit:
                     converged = True
                     break
                 t0 = time.perf_counter()
-                lu = self._factorize(kv)
+                if it == 0 or not self.constant_tangent:
+                    lu = self._factorize(kv)
                 mdu = lu.solve(rr)
                 self.timing["solve"] += time.perf_counter() - t0
                 if not np.all(np.isfinite(mdu)):
@@ -165,7 +170,7 @@ class SolverImplicit:
                 if it == 0:
                     el.backup_secondary_values()
                 t0 = time.perf_counter()
-                el.update_and_assemble(ddu[: self.ndof], ff, kv)
+                el.update_and_assemble(ddu[: self.ndof], ff, None if self.constant_tangent else kv)
                 self.timing["elements"] += time.perf_counter() - t0
                 if it == self.n_max_iterations - 1:
                     raise NewtonError("Newton-Raphson did not converge")
