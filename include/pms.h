@@ -342,6 +342,12 @@ int pms_element_calc_noalloc(int32_t kind, int32_t ngauss, double thickness, con
                              int64_t ncell, const double* X, const double* sig, const double* ivs,
                              const uint8_t* elastic, double* f, double* kk, int64_t* max_cells, void* stream);
 
+/* The calling host thread's CUDA device (no counterpart in the reference, which runs on the host):
+ * every handle is created on, and must be used from, the device that is current in the creating
+ * thread.  pms_device_count reports 0 when no device is visible. */
+int pms_set_device(int32_t device);
+int pms_device_count(int32_t* count);
+
 /* Library version string and the number of kernels launched by the material entry points. */
 const char* pms_version(void);
 int64_t pms_material_launch_count(void);

@@ -125,6 +125,8 @@ SIGNATURES = {
     "pms_mesh_csr_pattern": (_I, [ctypes.POINTER(Mesh_), _V, _V, ctypes.POINTER(_I64)]),
     "pms_elements_set_timing": (_I, [_V, _I]),
     "pms_elements_set_assembly": (_I, [_V, _I]),
+    "pms_set_device": (_I, [_I]),
+    "pms_device_count": (_I, [_V]),
     "pms_elements_kernel_times": (_I, [_V, _V, _V]),
     "pms_probe_fp64_fma": (_I, [_I64, _I, _V, _V]),
     "pms_element_calc_noalloc": (_I, [_I, _I, _D, ctypes.POINTER(Material_), _I64, _V, _V, _V, _V, _V, _V,
@@ -194,3 +196,14 @@ def check(code: int, handle=None):
             raw = load().pms_elements_last_error(handle)
             msg = raw.decode() if raw else None
         raise PmsError(code, msg)
+
+
+def set_device(device: int):
+    """Makes `device` current for the calling host thread (handles then live on it)."""
+    check(load().pms_set_device(int(device)))
+
+
+def device_count() -> int:
+    n = ctypes.c_int32(0)
+    load().pms_device_count(ctypes.byref(n))
+    return int(n.value)

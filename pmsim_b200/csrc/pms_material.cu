@@ -220,4 +220,18 @@ int pms_probe_fp64_fma(int64_t iters, int32_t blocks, double* out, void* stream)
 
 const char* pms_version(void) { return "pms_b200 0.1.0 (sm_100a, FP64)"; }
 
+// The calling host thread's device (cudaSetDevice / cudaGetDeviceCount), for callers without a CUDA
+// runtime binding of their own: handles are created on, and run on, the current device of the thread
+// that creates them.
+int pms_set_device(int32_t device) {
+    return cudaSetDevice(device) == cudaSuccess ? PMS_OK : PMS_ERR_CUDA;
+}
+int pms_device_count(int32_t* count) {
+    int n = 0;
+    if (!count) return PMS_ERR_INVALID;
+    if (cudaGetDeviceCount(&n) != cudaSuccess) n = 0;
+    *count = n;
+    return PMS_OK;
+}
+
 }  // extern "C"

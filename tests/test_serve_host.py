@@ -23,7 +23,7 @@ def test_admission_budget_and_grouping(monkeypatch):
     seen = []
     usage = []
 
-    def fake_run(self, reqs, t0):
+    def fake_run(self, reqs, t0, dev=0):
         kinds = {(r.problem.mesh.kind, r.problem.ngauss) for r in reqs}
         seen.append(kinds)
         with self.lock:
@@ -32,7 +32,8 @@ def test_admission_budget_and_grouping(monkeypatch):
         for r in reqs:
             r.finished = time.perf_counter() - t0
         with self.lock:
-            self.in_use -= sum(r.bytes for r in reqs)
+            self.in_use_dev[dev] -= sum(r.bytes for r in reqs)
+            self.live_dev[dev] -= 1
             self.live -= 1
 
     monkeypatch.setattr(serve.Server, "_run_batch", fake_run)
@@ -60,3 +61,53 @@ def test_request_population_matches_the_served_configuration():
         else:
             assert p.mesh.ndof <= 206763
         assert p.nsteps == 10
+
+
+def test_requests_go_whole_to_the_least_loaded_device(monkeypatch):
+    """Several devices (stand-ins: the batch runner is replaced, no GPU is touched): every request goes
+    whole to one device, no device ever holds more than its budget, the devices share the work, and
+    the placement rule picks the least-loaded device that fits."""
+    from pmsim_b200 import placement
+    probs = [fake_problem("q" if i % 3 else "h", 4 + i % 7) for i in range(60)]
+    sizes = [serve.footprint_bytes(p) for p in probs]
+    budget = 2.5 * max(sizes)
+    log = []
+
+    def fake_run(self, reqs, t0, dev=0):
+        with self.lock:
+            log.append((dev, list(self.in_use_dev)))
+        time.sleep(0.005 * len(reqs))
+        for r in reqs:
+            r.finished = time.perf_counter() - t0
+        with self.lock:
+            self.in_use_dev[dev] -= sum(r.bytes for r in reqs)
+            self.live_dev[dev] -= 1
+            self.live -= 1
+
+    monkeypatch.setattr(serve.Server, "_run_batch", fake_run)
+    arr = serve.poisson_arrivals(len(probs), rate=2000.0, seed=3)
+    reqs = [serve.Request(i, p, float(a)) for i, (p, a) in enumerate(zip(probs, arr))]
+    srv = serve.Server(budget_bytes=budget, devices=[0, 1, 2], max_concurrent=2, admit_window=0.002)
+    srv.serve(reqs)
+    assert all(r.finished > 0 for r in reqs)
+    assert all(r.meta["device"] in (0, 1, 2) for r in reqs)
+    for dev, use in log:
+        assert all(u <= budget + 1e-6 for u in use)
+    assert all(n > 0 for n in srv.batches_dev), srv.batches_dev
+    assert srv.in_use == 0.0 and srv.live == 0
+    assert placement.least_loaded(5.0, [3.0, 1.0, 2.0], [10.0, 10.0, 10.0]) == 1
+    assert placement.least_loaded(5.0, [3.0, 6.0, 2.0], [10.0, 10.0, 6.0]) == 0
+    assert placement.least_loaded(5.0, [6.0, 6.0], [10.0, 10.0]) is None
+
+
+def test_partition_balances_work_and_is_deterministic():
+    from pmsim_b200 import placement
+    from pmsim_b200.footing import population
+    probs = population(64, seed=2024)
+    parts = placement.partition(probs, 4)
+    assert parts == placement.partition(probs, 4)
+    assert sorted(set(parts)) == [0, 1, 2, 3]
+    w = np.array([placement.work_estimate(p) for p in probs])
+    load = np.array([w[np.array(parts) == k].sum() for k in range(4)])
+    assert load.max() <= 1.15 * load.mean()
+    assert placement.partition(probs, 1) == [0] * len(probs)
