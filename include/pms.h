@@ -46,7 +46,8 @@ enum pms_status_code {
 /* ---- element kinds (gemlab GeoKind subset used by solids) ---------------------------------- */
 enum pms_kind {
     PMS_TRI3 = 0, PMS_TRI6 = 1, PMS_QUA4 = 2, PMS_QUA8 = 3, PMS_QUA9 = 4,
-    PMS_TET4 = 5, PMS_TET10 = 6, PMS_HEX8 = 7, PMS_HEX20 = 8
+    PMS_TET4 = 5, PMS_TET10 = 6, PMS_HEX8 = 7, PMS_HEX20 = 8,
+    PMS_TRI10 = 9, PMS_TRI15 = 10  /* complete cubic / quartic triangles (default 6 / 12 IPs) */
 };
 
 /* ---- stress-strain models (src/base/parameters.rs:17-35) ---------------------------------- */
@@ -165,6 +166,12 @@ int pms_elements_set_assembly(pms_elements* h, int32_t mode);
  * previous query. */
 int pms_elements_set_timing(pms_elements* h, int32_t on);
 int pms_elements_kernel_times(pms_elements* h, double* ms, int64_t* counts);
+
+/* Host-only (no GPU needed): the element tables pms_elements_create uploads for a kind and rule
+ * (ngauss 0: the default), as gemlab's Scratchpad/Gauss provide them to ElementSolid::new
+ * (src/fem/element_solid.rs:47-92): tab[ng*nnode*ndim] = dN_m/dksi_j at each IP, then the weights
+ * w[ng], then N[ng*nnode].  tab NULL: only *ngauss_out (the number of IPs) is set. */
+int pms_shape_table(int32_t kind, int32_t ngauss, double* tab, int32_t* ngauss_out);
 
 /* Host-only (no GPU needed): the CSR pattern pms_elements_create would build for this mesh.
  * Call with indices = NULL to get nnz (indptr[ndof+1] may already be filled). */

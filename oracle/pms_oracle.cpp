@@ -42,21 +42,23 @@
 
 namespace {
 
-enum Kind { TRI3 = 0, TRI6 = 1, QUA4 = 2, QUA8 = 3, QUA9 = 4, TET4 = 5, TET10 = 6, HEX8 = 7, HEX20 = 8 };
+enum Kind { TRI3 = 0, TRI6 = 1, QUA4 = 2, QUA8 = 3, QUA9 = 4, TET4 = 5, TET10 = 6, HEX8 = 7, HEX20 = 8,
+            TRI10 = 9, TRI15 = 10 };
+constexpr int NKIND = 11;
 
 const double SQRT2 = 1.4142135623730951;
 const double SQRT_2_BY_3 = 0.816496580927726;   // sqrt(2/3)
 const double F_TOL = 1e-6;                       // src/material/von_mises.rs:23
 
 int kind_nnode(int k) {
-    static const int n[] = {3, 6, 4, 8, 9, 4, 10, 8, 20};
-    return (k >= 0 && k <= 8) ? n[k] : -1;
+    static const int n[] = {3, 6, 4, 8, 9, 4, 10, 8, 20, 10, 15};
+    return (k >= 0 && k < NKIND) ? n[k] : -1;
 }
-int kind_ndim(int k) { return (k <= QUA9) ? 2 : 3; }
+int kind_ndim(int k) { return (k <= QUA9 || k == TRI10 || k == TRI15) ? 2 : 3; }
 
 int default_ngauss(int k) {
-    static const int n[] = {3, 3, 4, 9, 9, 4, 4, 8, 27};
-    return (k >= 0 && k <= 8) ? n[k] : -1;
+    static const int n[] = {3, 3, 4, 9, 9, 4, 4, 8, 27, 6, 12};
+    return (k >= 0 && k < NKIND) ? n[k] : -1;
 }
 
 // ---------------------------------------------------------------- Gauss rules
@@ -70,7 +72,7 @@ void legendre_1d(int n, double* x, double* w) {
 // Tensor-product rule, x varies fastest, then y, then z.
 int gauss_rule(int kind, int ngauss, double* ksi /*ngauss*3*/, double* w) {
     int nd = kind_ndim(kind);
-    bool simplex = (kind == TRI3 || kind == TRI6 || kind == TET4 || kind == TET10);
+    bool simplex = (kind == TRI3 || kind == TRI6 || kind == TET4 || kind == TET10 || kind == TRI10 || kind == TRI15);
     if (!simplex) {
         int n1 = 0;
         if (nd == 2) { if (ngauss == 1) n1 = 1; else if (ngauss == 4) n1 = 2; else if (ngauss == 9) n1 = 3; }
@@ -99,7 +101,54 @@ int gauss_rule(int kind, int ngauss, double* ksi /*ngauss*3*/, double* w) {
             for (int p = 0; p < 3; p++) { ksi[3*p] = pts[p][0]; ksi[3*p+1] = pts[p][1]; ksi[3*p+2] = 0; w[p] = 1.0 / 6.0; }
             return 3;
         }
-        return -1;
+        // symmetric triangle rules of Dunavant (1985): orbits of barycentric points (a, a, 1-2a), the
+        // centroid, and (a, b, 1-a-b) with its six permutations; weights for unit area, times 1/2 here
+        struct Orbit { int kind; double w, a, b; };  // kind 1: centroid, 3: (a,a,1-2a), 6: (a,b,c)
+        Orbit orb[3];
+        int norb = 0;
+        if (ngauss == 6) {  // degree 4
+            orb[0] = {3, 0.223381589678011, 0.445948490915965, 0};
+            orb[1] = {3, 0.109951743655322, 0.091576213509771, 0};
+            norb = 2;
+        } else if (ngauss == 7) {  // degree 5 (closed form)
+            const double r15 = std::sqrt(15.0);
+            orb[0] = {1, 0.225, 1.0 / 3.0, 0};
+            orb[1] = {3, (155.0 + r15) / 1200.0, (6.0 + r15) / 21.0, 0};
+            orb[2] = {3, (155.0 - r15) / 1200.0, (6.0 - r15) / 21.0, 0};
+            norb = 3;
+        } else if (ngauss == 12) {  // degree 6
+            orb[0] = {3, 0.116786275726379, 0.249286745170910, 0};
+            orb[1] = {3, 0.050844906370207, 0.063089014491502, 0};
+            orb[2] = {6, 0.082851075618374, 0.053145049844817, 0.310352451033784};
+            norb = 3;
+        } else {
+            return -1;
+        }
+        int p = 0;
+        for (int io = 0; io < norb; io++) {
+            const Orbit& o = orb[io];
+            double pts[6][2];
+            int n = 0;
+            if (o.kind == 1) { pts[0][0] = o.a; pts[0][1] = o.a; n = 1; }
+            else if (o.kind == 3) {
+                const double c = 1.0 - 2.0 * o.a;
+                double q[3][2] = {{o.a, o.a}, {c, o.a}, {o.a, c}};
+                for (int i = 0; i < 3; i++) { pts[i][0] = q[i][0]; pts[i][1] = q[i][1]; }
+                n = 3;
+            } else {
+                const double c = 1.0 - o.a - o.b;
+                double q[6][2] = {{o.a, o.b}, {o.b, o.a}, {o.b, c}, {c, o.b}, {c, o.a}, {o.a, c}};
+                for (int i = 0; i < 6; i++) { pts[i][0] = q[i][0]; pts[i][1] = q[i][1]; }
+                n = 6;
+            }
+            for (int i = 0; i < n; i++, p++) {
+                ksi[3 * p] = pts[i][0];
+                ksi[3 * p + 1] = pts[i][1];
+                ksi[3 * p + 2] = 0.0;
+                w[p] = 0.5 * o.w;
+            }
+        }
+        return p;
     }
     if (ngauss == 1) { ksi[0] = ksi[1] = ksi[2] = 0.25; w[0] = 1.0 / 6.0; return 1; }
     if (ngauss == 4) {
@@ -112,10 +161,49 @@ int gauss_rule(int kind, int ngauss, double* ksi /*ngauss*3*/, double* w) {
 }
 
 // ---------------------------------------------------------------- shape functions
+// Complete Lagrange triangle of order n in area coordinates L0 = 1 - r - s, L1 = r, L2 = s: the node
+// at barycentric position (i, j, k)/n has N = P_i(L0) P_j(L1) P_k(L2), P_a(L) = prod_{q<a} (nL - q)/(q+1)
+// (Silvester's formula; Zienkiewicz & Taylor Vol. 1, sec. 6.6).  Node order: corners; for n = 4 the
+// mid-edge nodes of edges 0-1, 1-2, 2-0; then per edge the node nearer its first corner and the one
+// nearer its second; then the interior nodes.
+const int TRI10_IJK[10][3] = {{3, 0, 0}, {0, 3, 0}, {0, 0, 3}, {2, 1, 0}, {1, 2, 0},
+                              {0, 2, 1}, {0, 1, 2}, {1, 0, 2}, {2, 0, 1}, {1, 1, 1}};
+const int TRI15_IJK[15][3] = {{4, 0, 0}, {0, 4, 0}, {0, 0, 4}, {2, 2, 0}, {0, 2, 2}, {2, 0, 2}, {3, 1, 0}, {1, 3, 0},
+                              {0, 3, 1}, {0, 1, 3}, {1, 0, 3}, {3, 0, 1}, {2, 1, 1}, {1, 2, 1}, {1, 1, 2}};
+
+void silvester(int n, int a, double L, double& P, double& dP) {
+    P = 1.0;
+    dP = 0.0;
+    for (int q = 0; q < a; q++) {
+        const double f = (n * L - q) / (q + 1);
+        dP = dP * f + P * n / (q + 1);
+        P *= f;
+    }
+}
+
+void lagrange_triangle(int n, int nn, const int (*ijk)[3], double r, double s, double* N, double* dN) {
+    const double L0 = 1.0 - r - s;
+    for (int m = 0; m < nn; m++) {
+        double P0, d0, P1, d1, P2, d2;
+        silvester(n, ijk[m][0], L0, P0, d0);
+        silvester(n, ijk[m][1], r, P1, d1);
+        silvester(n, ijk[m][2], s, P2, d2);
+        N[m] = P0 * P1 * P2;
+        dN[2 * m] = -d0 * P1 * P2 + P0 * d1 * P2;
+        dN[2 * m + 1] = -d0 * P1 * P2 + P0 * P1 * d2;
+    }
+}
+
 // N[m], dN[m*nd + j] = dN_m/dksi_j
 void shape(int kind, const double* k, double* N, double* dN) {
     const double r = k[0], s = k[1], t = k[2];
     switch (kind) {
+    case TRI10:
+        lagrange_triangle(3, 10, TRI10_IJK, r, s, N, dN);
+        break;
+    case TRI15:
+        lagrange_triangle(4, 15, TRI15_IJK, r, s, N, dN);
+        break;
     case TRI3:
         N[0] = 1 - r - s; N[1] = r; N[2] = s;
         dN[0] = -1; dN[1] = -1; dN[2] = 1; dN[3] = 0; dN[4] = 0; dN[5] = 1;

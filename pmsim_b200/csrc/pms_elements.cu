@@ -224,8 +224,8 @@ template <int NN> __host__ __device__ constexpr int tile_count() {
     return k;
 }
 template <int NN> struct TileShape {
-    static constexpr int RT = NN >= 16 ? 2 : 1;
-    static constexpr int CT = warps_per_cell(NN) == 2 ? 2 : (NN >= 16 ? 4 : (NN >= 7 ? 2 : 1));
+    static constexpr int RT = NN >= 13 ? 2 : 1;
+    static constexpr int CT = warps_per_cell(NN) == 2 ? 2 : (NN >= 13 ? 4 : (NN >= 7 ? 2 : 1));
     static constexpr int NRG = (NN + RT - 1) / RT;
     static constexpr int NCG = (NN + CT - 1) / CT;
 };
@@ -247,7 +247,8 @@ __host__ __device__ constexpr int smem_bytes_for(int nn, int nd, int ng, int wpb
 }
 
 template <int ND, int NN, int UPD, bool DOF, bool DOK, bool CSR>
-__global__ void __launch_bounds__(WPB * 32, warps_per_cell(NN) == 2 ? 3 : (ND == 2 ? 4 : 1)) element_kernel(ElemArgs A) {
+__global__ void __launch_bounds__(WPB * 32, warps_per_cell(NN) == 2 ? 3 : (ND == 2 ? (NN >= 13 ? 2 : 4) : 1))
+element_kernel(ElemArgs A) {
     static_assert(!CSR || warps_per_cell(NN) == 1, "the ordered assembly takes one warp per cell");
     constexpr int NC = 2 * ND;
     constexpr int NE = NN * ND;
@@ -807,6 +808,9 @@ template <int NN> __host__ __device__ constexpr int lanes_packed() {
     return Tile2<NN>::NT > NN ? Tile2<NN>::NT : NN;
 }
 template <int NN> __host__ __device__ constexpr bool packed_layout() { return 32 / lanes_packed<NN>() >= 3; }
+// Whether a 2D kind fits the several-cells-per-warp layout (at most 16 lanes per cell); larger
+// cells (Tri15: 36 node-pair tiles) run in element_kernel with one warp per cell.
+template <int NN> __host__ __device__ constexpr bool fits_2d() { return Tile2<NN>::NT <= 16 && NN <= 16; }
 
 template <int NN, int LPC, int UPD, bool DOF, bool DOK, bool CSR>
 __global__ void __launch_bounds__(WPB2 * 32, 4) element2d_kernel(ElemArgs A) {
@@ -1594,7 +1598,7 @@ void launch_elem2d_t(const ElemArgs& a, cudaStream_t st, bool persistent) {
 
 template <int ND, int NN, int UPD, bool DOF, bool DOK, bool CSR>
 void launch_elem_t(pms_elements* h, const ElemArgs& a) {
-    if constexpr (ND == 2) {
+    if constexpr (ND == 2 && fits_2d<NN>()) {
         if (a.ngauss <= NG2_MAX) {
             launch_elem2d_t<NN, UPD, DOF, DOK, CSR>(a, h->stream, true);
             return;
@@ -1652,6 +1656,8 @@ void launch_elem(pms_elements* h, const ElemArgs& a, int upd, bool dof, bool dok
         case PMS_TET10: launch_elem_t<3, 10, UPD_MODE, true, true, true>(h, a); break;
         case PMS_HEX8: launch_elem_t<3, 8, UPD_MODE, true, true, true>(h, a); break;
         case PMS_HEX20: launch_elem_t<3, 20, UPD_MODE, true, true, true>(h, a); break;
+        case PMS_TRI10: launch_elem_t<2, 10, UPD_MODE, true, true, true>(h, a); break;
+        case PMS_TRI15: launch_elem_t<2, 15, UPD_MODE, true, true, true>(h, a); break;
         }
         h->launches++;
         return;
@@ -1666,6 +1672,8 @@ void launch_elem(pms_elements* h, const ElemArgs& a, int upd, bool dof, bool dok
     case PMS_TET10: launch_elem_nn<3, 10>(h, a, upd, dof, dok, csr); break;
     case PMS_HEX8: launch_elem_nn<3, 8>(h, a, upd, dof, dok, csr); break;
     case PMS_HEX20: launch_elem_nn<3, 20>(h, a, upd, dof, dok, csr); break;
+    case PMS_TRI10: launch_elem_nn<2, 10>(h, a, upd, dof, dok, csr); break;
+    case PMS_TRI15: launch_elem_nn<2, 15>(h, a, upd, dof, dok, csr); break;
     }
     h->launches++;
 }
@@ -1731,6 +1739,8 @@ void launch_kk_gather(pms_elements* h, double* csr, const int32_t* node_prob = n
     case PMS_TET10: launch_kk_gather_t<3, 10>(h, csr, node_prob, pmode, q, node0, nrows); break;
     case PMS_HEX8: launch_kk_gather_t<3, 8>(h, csr, node_prob, pmode, q, node0, nrows); break;
     case PMS_HEX20: launch_kk_gather_t<3, 20>(h, csr, node_prob, pmode, q, node0, nrows); break;
+    case PMS_TRI10: launch_kk_gather_t<2, 10>(h, csr, node_prob, pmode, q, node0, nrows); break;
+    case PMS_TRI15: launch_kk_gather_t<2, 15>(h, csr, node_prob, pmode, q, node0, nrows); break;
     }
     h->launches++;
 }
@@ -1778,7 +1788,7 @@ int pms_elements_create(const pms_mesh* mesh, const pms_material* materials, int
     if (!mesh || !materials || nmaterial < 1 || !config || !mesh->coords || !mesh->cells)
         return refuse(PMS_ERR_INVALID, "mesh, materials and config are required");
     int kind = mesh->kind;
-    if (kind < 0 || kind > 8 || kind_ndim(kind) != mesh->ndim)
+    if (kind_nnode(kind) < 0 || kind_ndim(kind) != mesh->ndim)
         return refuse(PMS_ERR_INVALID, "unknown element kind or kind of another dimension");
     if (config->axisymmetric && mesh->ndim != 2)
         return refuse(PMS_ERR_UNSUPPORTED, "the axisymmetric idealization needs a 2D mesh");
@@ -1824,6 +1834,12 @@ int pms_elements_create(const pms_mesh* mesh, const pms_material* materials, int
     for (int i = 0; i < nmaterial; i++) {
         const pms_material& m = materials[i];
         h->mats.push_back(make_matconst(m.model, m.young, m.poisson, m.hh, m.z_ini, config->plane_stress != 0));
+    }
+    // shape tables: dN[ngauss][nnode][ndim], then w[ngauss], then N[ngauss][nnode]
+    h->tab.assign((size_t)h->ng * h->nn * h->nd + h->ng + (size_t)h->ng * h->nn, 0.0);
+    if (pms_shape_table(kind, config->ngauss, h->tab.data(), nullptr) != PMS_OK) {
+        delete h;
+        return refuse(PMS_ERR_INVALID, "requested number of integration points is not available");
     }
     const char* msg = nullptr;
     if (!build_pattern(h->nd, h->nn, h->npoint, h->ncell, mesh->cells, h->pat, &msg)) {
@@ -2243,8 +2259,27 @@ int pms_elements_kernel_times(pms_elements* h, double* ms, int64_t* counts) {
     return cuda_check(h);
 }
 
+int pms_shape_table(int32_t kind, int32_t ngauss, double* tab, int32_t* ngauss_out) {
+    const int nn = kind_nnode(kind), nd = kind_ndim(kind);
+    if (nn < 0) return PMS_ERR_INVALID;
+    double ksi[3 * 27], w[27];
+    const int ng = integration_rule_into(kind, ngauss, ksi, w);
+    if (ng <= 0) return PMS_ERR_INVALID;
+    if (ngauss_out) *ngauss_out = ng;
+    if (!tab) return PMS_OK;
+    double N[20], dN[60];
+    for (int p = 0; p < ng; p++) {
+        shape_eval(kind, &ksi[3 * p], N, dN);
+        for (int m = 0; m < nn; m++)
+            for (int j = 0; j < nd; j++) tab[(p * nn + m) * nd + j] = dN[m * nd + j];
+        tab[(size_t)ng * nn * nd + p] = w[p];
+        for (int m = 0; m < nn; m++) tab[(size_t)ng * nn * nd + ng + p * nn + m] = N[m];
+    }
+    return PMS_OK;
+}
+
 int pms_mesh_csr_pattern(const pms_mesh* mesh, int64_t* indptr, int32_t* indices, int64_t* nnz) {
-    if (!mesh || !mesh->cells || mesh->kind < 0 || mesh->kind > 8 || kind_ndim(mesh->kind) != mesh->ndim)
+    if (!mesh || !mesh->cells || kind_nnode(mesh->kind) < 0 || kind_ndim(mesh->kind) != mesh->ndim)
         return PMS_ERR_INVALID;
     Pattern p;
     const char* msg = nullptr;
@@ -2386,7 +2421,7 @@ NoallocLayout noalloc_layout(int nn, int nd, int ng, int64_t ncell, bool want_f,
 
 template <int ND, int NN, bool DOF, bool DOK>
 void noalloc_launch_t(const ElemArgs& a, int smem, cudaStream_t st) {
-    if constexpr (ND == 2) {
+    if constexpr (ND == 2 && fits_2d<NN>()) {
         if (a.ngauss <= NG2_MAX) {
             launch_elem2d_t<NN, UPD_NONE, DOF, DOK, false>(a, st, false);
             return;
@@ -2410,7 +2445,7 @@ extern "C" int pms_element_calc_noalloc(int32_t kind, int32_t ngauss, double thi
                                         int64_t ncell, const double* X, const double* sig, const double* ivs,
                                         const uint8_t* elastic, double* f, double* kk, int64_t* max_cells,
                                         void* stream) {
-    if (kind < 0 || kind > 8 || !mat || ncell < 0 || (!f && !kk)) return PMS_ERR_INVALID;
+    if (kind_nnode(kind) < 0 || !mat || ncell < 0 || (!f && !kk)) return PMS_ERR_INVALID;
     if (mat->model != PMS_LINEAR_ELASTIC && mat->model != PMS_VON_MISES) return PMS_ERR_INVALID;
     if (mat->model == PMS_VON_MISES && !(mat->z_ini > F_TOL)) return PMS_ERR_INVALID;
     const int nn = kind_nnode(kind), nd = kind_ndim(kind), nc = 2 * nd;
@@ -2508,6 +2543,8 @@ extern "C" int pms_element_calc_noalloc(int32_t kind, int32_t ngauss, double thi
     case PMS_TET10: noalloc_launch<3, 10>(a, dof, dok, smem, st); break;
     case PMS_HEX8: noalloc_launch<3, 8>(a, dof, dok, smem, st); break;
     case PMS_HEX20: noalloc_launch<3, 20>(a, dof, dok, smem, st); break;
+    case PMS_TRI10: noalloc_launch<2, 10>(a, dof, dok, smem, st); break;
+    case PMS_TRI15: noalloc_launch<2, 15>(a, dof, dok, smem, st); break;
     }
     if (cudaGetLastError() != cudaSuccess) return PMS_ERR_CUDA;
     const int ne = nn * nd;

@@ -6,9 +6,90 @@
 namespace pms {
 
 namespace {
-const int NNODE[9] = {3, 6, 4, 8, 9, 4, 10, 8, 20};
-const int NDIM[9] = {2, 2, 2, 2, 2, 3, 3, 3, 3};
-const int NGAUSS_DEFAULT[9] = {3, 3, 4, 9, 9, 4, 4, 8, 27};
+constexpr int NKIND = 11;
+const int NNODE[NKIND] = {3, 6, 4, 8, 9, 4, 10, 8, 20, 10, 15};
+const int NDIM[NKIND] = {2, 2, 2, 2, 2, 3, 3, 3, 3, 2, 2};
+// Tri10 / Tri15: the lowest symmetric rule that integrates the stiffness of a straight-sided cell
+// exactly (degree 4 and 6)
+const int NGAUSS_DEFAULT[NKIND] = {3, 3, 4, 9, 9, 4, 4, 8, 27, 6, 12};
+bool simplex_kind(int kind) { return kind == 0 || kind == 1 || kind == 5 || kind == 6 || kind == 9 || kind == 10; }
+
+// Barycentric positions (i, j, k)/n of the nodes of the cubic (n = 3) and quartic (n = 4) triangles:
+// corners; for n = 4 the mid-edge nodes of edges 0-1, 1-2, 2-0; then per edge the node nearer its
+// first corner and the one nearer its second; then the interior nodes (the Tri15 order of the
+// reference's meshes, src/base/sample_meshes.rs:305-362).
+const int TRI10_POS[10][3] = {{3, 0, 0}, {0, 3, 0}, {0, 0, 3}, {2, 1, 0}, {1, 2, 0},
+                              {0, 2, 1}, {0, 1, 2}, {1, 0, 2}, {2, 0, 1}, {1, 1, 1}};
+const int TRI15_POS[15][3] = {{4, 0, 0}, {0, 4, 0}, {0, 0, 4}, {2, 2, 0}, {0, 2, 2}, {2, 0, 2}, {3, 1, 0}, {1, 3, 0},
+                              {0, 3, 1}, {0, 1, 3}, {1, 0, 3}, {3, 0, 1}, {2, 1, 1}, {1, 2, 1}, {1, 1, 2}};
+
+// Silvester's factor of a complete Lagrange triangle of order n: P_a(L) = prod_{q<a} (n L - q)/(q + 1)
+// and its derivative in L (Zienkiewicz & Taylor, Vol. 1, sec. 6.6).
+void silvester_factor(int n, int a, double L, double& P, double& dP) {
+    P = 1.0;
+    dP = 0.0;
+    for (int q = 0; q < a; q++) {
+        const double f = (n * L - q) / (q + 1);
+        dP = dP * f + P * n / (q + 1);
+        P *= f;
+    }
+}
+
+// Symmetric triangle rules of Dunavant (1985, Int. J. Numer. Meth. Eng. 21:1129-1148) on the
+// reference triangle (area 1/2): orbit type 1 = centroid, 3 = (a, a, 1 - 2a) and its rotations,
+// 6 = (a, b, 1 - a - b) and its permutations; weights given for unit area.
+int triangle_rule(int ngauss, double* ksi, double* w) {
+    struct Orbit { int type; double w, a, b; };
+    Orbit orb[3];
+    int norb = 0;
+    const double r15 = std::sqrt(15.0);
+    switch (ngauss) {
+    case 6:  // degree 4
+        orb[0] = {3, 0.223381589678011, 0.445948490915965, 0.0};
+        orb[1] = {3, 0.109951743655322, 0.091576213509771, 0.0};
+        norb = 2;
+        break;
+    case 7:  // degree 5 (closed form)
+        orb[0] = {1, 0.225, 1.0 / 3.0, 0.0};
+        orb[1] = {3, (155.0 + r15) / 1200.0, (6.0 + r15) / 21.0, 0.0};
+        orb[2] = {3, (155.0 - r15) / 1200.0, (6.0 - r15) / 21.0, 0.0};
+        norb = 3;
+        break;
+    case 12:  // degree 6
+        orb[0] = {3, 0.116786275726379, 0.249286745170910, 0.0};
+        orb[1] = {3, 0.050844906370207, 0.063089014491502, 0.0};
+        orb[2] = {6, 0.082851075618374, 0.053145049844817, 0.310352451033784};
+        norb = 3;
+        break;
+    default:
+        return -1;
+    }
+    int p = 0;
+    for (int o = 0; o < norb; o++) {
+        const double a = orb[o].a, b = orb[o].b;
+        double pts[6][2];
+        int n = 1;
+        pts[0][0] = pts[0][1] = a;
+        if (orb[o].type == 3) {
+            const double c = 1.0 - 2.0 * a;
+            pts[1][0] = c; pts[1][1] = a;
+            pts[2][0] = a; pts[2][1] = c;
+            n = 3;
+        } else if (orb[o].type == 6) {
+            const double c = 1.0 - a - b;
+            const double q[6][2] = {{a, b}, {b, a}, {b, c}, {c, b}, {c, a}, {a, c}};
+            for (int i = 0; i < 6; i++) { pts[i][0] = q[i][0]; pts[i][1] = q[i][1]; }
+            n = 6;
+        }
+        for (int i = 0; i < n; i++, p++) {
+            ksi[3 * p] = pts[i][0];
+            ksi[3 * p + 1] = pts[i][1];
+            ksi[3 * p + 2] = 0.0;
+            w[p] = 0.5 * orb[o].w;
+        }
+    }
+    return p;
+}
 
 // natural coordinates of the nodes of the hypercube kinds (corners first)
 const double QUA_NODES[9][2] = {{-1, -1}, {1, -1}, {1, 1}, {-1, 1}, {0, -1}, {1, 0}, {0, 1}, {-1, 0}, {0, 0}};
@@ -39,74 +120,26 @@ void gauss_legendre(int n, double* x, double* w) {
 }
 }  // namespace
 
-int kind_nnode(int kind) { return (kind >= 0 && kind < 9) ? NNODE[kind] : -1; }
-int kind_ndim(int kind) { return (kind >= 0 && kind < 9) ? NDIM[kind] : -1; }
-int kind_default_ngauss(int kind) { return (kind >= 0 && kind < 9) ? NGAUSS_DEFAULT[kind] : -1; }
+int kind_nnode(int kind) { return (kind >= 0 && kind < NKIND) ? NNODE[kind] : -1; }
+int kind_ndim(int kind) { return (kind >= 0 && kind < NKIND) ? NDIM[kind] : -1; }
+int kind_default_ngauss(int kind) { return (kind >= 0 && kind < NKIND) ? NGAUSS_DEFAULT[kind] : -1; }
 
 int integration_rule(int kind, int ngauss, std::vector<double>& ksi, std::vector<double>& w) {
-    if (kind < 0 || kind > 8) return -1;
-    if (ngauss <= 0) ngauss = NGAUSS_DEFAULT[kind];
-    int nd = NDIM[kind];
-    ksi.assign(3 * ngauss, 0.0);
-    w.assign(ngauss, 0.0);
-    const bool simplex = (kind == 0 || kind == 1 || kind == 5 || kind == 6);
-    if (!simplex) {
-        int n1 = (int)std::lround(std::pow((double)ngauss, 1.0 / nd));
-        int tot = 1;
-        for (int d = 0; d < nd; d++) tot *= n1;
-        if (n1 < 1 || n1 > 3 || tot != ngauss) return -1;
-        double x[3], ww[3];
-        gauss_legendre(n1, x, ww);
-        for (int p = 0; p < ngauss; p++) {
-            int i = p % n1, j = (p / n1) % n1, k = p / (n1 * n1);
-            ksi[3 * p] = x[i];
-            ksi[3 * p + 1] = x[j];
-            ksi[3 * p + 2] = nd == 3 ? x[k] : 0.0;
-            w[p] = ww[i] * ww[j] * (nd == 3 ? ww[k] : 1.0);
-        }
-        return ngauss;
-    }
-    if (nd == 2) {
-        if (ngauss == 1) {
-            ksi[0] = ksi[1] = 1.0 / 3.0;
-            w[0] = 0.5;
-            return 1;
-        }
-        if (ngauss == 3) {
-            const double lo = 1.0 / 6.0, hi = 2.0 / 3.0;
-            const double pts[3][2] = {{lo, lo}, {hi, lo}, {lo, hi}};
-            for (int p = 0; p < 3; p++) {
-                ksi[3 * p] = pts[p][0];
-                ksi[3 * p + 1] = pts[p][1];
-                w[p] = 1.0 / 6.0;
-            }
-            return 3;
-        }
-        return -1;
-    }
-    if (ngauss == 1) {
-        ksi[0] = ksi[1] = ksi[2] = 0.25;
-        w[0] = 1.0 / 6.0;
-        return 1;
-    }
-    if (ngauss == 4) {
-        const double hi = (5.0 + 3.0 * std::sqrt(5.0)) / 20.0, lo = (5.0 - std::sqrt(5.0)) / 20.0;
-        for (int p = 0; p < 4; p++) {
-            for (int d = 0; d < 3; d++) ksi[3 * p + d] = (p > 0 && d == p - 1) ? hi : lo;
-            w[p] = 1.0 / 24.0;
-        }
-        return 4;
-    }
-    return -1;
+    double k[3 * 27], ww[27];
+    const int n = integration_rule_into(kind, ngauss, k, ww);
+    if (n <= 0) return -1;
+    ksi.assign(k, k + 3 * n);
+    w.assign(ww, ww + n);
+    return n;
 }
 
 int integration_rule_into(int kind, int ngauss, double* ksi, double* w) {
-    if (kind < 0 || kind > 8) return -1;
+    if (kind < 0 || kind >= NKIND) return -1;
     if (ngauss <= 0) ngauss = NGAUSS_DEFAULT[kind];
     if (ngauss > 27) return -1;
     const int nd = NDIM[kind];
     for (int i = 0; i < 3 * ngauss; i++) ksi[i] = 0.0;
-    const bool simplex = (kind == 0 || kind == 1 || kind == 5 || kind == 6);
+    const bool simplex = simplex_kind(kind);
     if (!simplex) {
         int n1 = 0;
         for (int c = 1; c <= 3; c++)
@@ -147,12 +180,29 @@ int integration_rule_into(int kind, int ngauss, double* ksi, double* w) {
         }
         return 4;
     }
+    if (nd == 2) return triangle_rule(ngauss, ksi, w);
     return -1;
 }
 
 void shape_eval(int kind, const double* k, double* N, double* dN) {
     const double r = k[0], s = k[1], t = k[2];
     switch (kind) {
+    case 9:    // Tri10: complete cubic triangle
+    case 10: {  // Tri15: complete quartic triangle
+        const int n = kind == 9 ? 3 : 4, nn = kind == 9 ? 10 : 15;
+        const int(*pos)[3] = kind == 9 ? TRI10_POS : TRI15_POS;
+        const double L0 = 1.0 - r - s;  // area coordinates (L0, L1, L2) = (1 - r - s, r, s)
+        for (int m = 0; m < nn; m++) {
+            double P0, d0, P1, d1, P2, d2;
+            silvester_factor(n, pos[m][0], L0, P0, d0);
+            silvester_factor(n, pos[m][1], r, P1, d1);
+            silvester_factor(n, pos[m][2], s, P2, d2);
+            N[m] = P0 * P1 * P2;
+            dN[2 * m] = P0 * d1 * P2 - d0 * P1 * P2;
+            dN[2 * m + 1] = P0 * P1 * d2 - d0 * P1 * P2;
+        }
+        break;
+    }
     case 2:  // Qua4: bilinear
         for (int m = 0; m < 4; m++) {
             double a = QUA_NODES[m][0], b = QUA_NODES[m][1];

@@ -20,11 +20,21 @@ from dataclasses import dataclass
 import numpy as np
 
 # Element kinds; the integers are part of the C ABI (include/pms.h, enum pms_kind).
-TRI3, TRI6, QUA4, QUA8, QUA9, TET4, TET10, HEX8, HEX20 = range(9)
-KIND_NAMES = ["tri3", "tri6", "qua4", "qua8", "qua9", "tet4", "tet10", "hex8", "hex20"]
-KIND_NNODE = [3, 6, 4, 8, 9, 4, 10, 8, 20]
-KIND_NDIM = [2, 2, 2, 2, 2, 3, 3, 3, 3]
-DEFAULT_NGAUSS = [3, 3, 4, 9, 9, 4, 4, 8, 27]
+TRI3, TRI6, QUA4, QUA8, QUA9, TET4, TET10, HEX8, HEX20, TRI10, TRI15 = range(11)
+KIND_NAMES = ["tri3", "tri6", "qua4", "qua8", "qua9", "tet4", "tet10", "hex8", "hex20", "tri10", "tri15"]
+KIND_NNODE = [3, 6, 4, 8, 9, 4, 10, 8, 20, 10, 15]
+KIND_NDIM = [2, 2, 2, 2, 2, 3, 3, 3, 3, 2, 2]
+DEFAULT_NGAUSS = [3, 3, 4, 9, 9, 4, 4, 8, 27, 6, 12]
+
+# Barycentric positions (multiples of 1/order, order = 3 or 4) of the nodes of the cubic and quartic
+# triangles, in the node order of the reference's meshes: corners, then (Tri15) the mid-edge nodes of
+# edges 0-1, 1-2, 2-0, then the edge nodes nearer the first and then the second corner of each edge,
+# then the interior nodes.  The Tri15 order is pinned by src/base/sample_meshes.rs:305-362
+# (smith_example_5d7_tri15); the Tri10 order follows the same pattern (not pinned by reference data).
+TRI10_NODES = [(3, 0, 0), (0, 3, 0), (0, 0, 3), (2, 1, 0), (1, 2, 0), (0, 2, 1), (0, 1, 2), (1, 0, 2), (2, 0, 1),
+               (1, 1, 1)]
+TRI15_NODES = [(4, 0, 0), (0, 4, 0), (0, 0, 4), (2, 2, 0), (0, 2, 2), (2, 0, 2), (3, 1, 0), (1, 3, 0), (0, 3, 1),
+               (0, 1, 3), (1, 0, 3), (3, 0, 1), (2, 1, 1), (1, 2, 1), (1, 1, 2)]
 
 
 def kind_from_name(name: str) -> int:
@@ -78,9 +88,28 @@ def _grid_ids(keep: np.ndarray) -> np.ndarray:
     return ids
 
 
+def _higher_triangles(kind, nx, ny, lx, ly, x0, y0) -> Mesh:
+    """Tri10/Tri15 rectangle: each grid square split into two triangles (a, b, c), (a, c, d) as for
+    Tri3; the nodes of every triangle placed at their barycentric positions and merged by position."""
+    order, table = (3, TRI10_NODES) if kind == TRI10 else (4, TRI15_NODES)
+    base = structured_2d(TRI3, nx, ny, lx, ly, x0, y0)
+    lam = np.array(table, dtype=np.float64) / order  # (nn, 3)
+    pts = np.einsum("nk,ckd->cnd", lam, base.coords[base.cells])  # (ncell, nn, 2)
+    # integer lattice coordinates (order*nx, order*ny steps) identify shared nodes exactly
+    gx = np.rint((pts[..., 0] - x0) / lx * order * nx).astype(np.int64)
+    gy = np.rint((pts[..., 1] - y0) / ly * order * ny).astype(np.int64)
+    key = gy * (order * nx + 1) + gx
+    uniq, inv = np.unique(key.ravel(), return_inverse=True)
+    coords = np.stack([x0 + lx * (uniq % (order * nx + 1)) / (order * nx),
+                       y0 + ly * (uniq // (order * nx + 1)) / (order * ny)], axis=1)
+    return Mesh(2, coords, inv.reshape(base.ncell, len(table)), kind)
+
+
 def structured_2d(kind: int, nx: int, ny: int, lx: float = 1.0, ly: float = 1.0,
                   x0: float = 0.0, y0: float = 0.0) -> Mesh:
-    """Structured rectangle [x0, x0+lx] x [y0, y0+ly] of Qua4/Qua8/Qua9/Tri3/Tri6 cells."""
+    """Structured rectangle [x0, x0+lx] x [y0, y0+ly] of Qua4/Qua8/Qua9/Tri3/Tri6/Tri10/Tri15 cells."""
+    if kind in (TRI10, TRI15):
+        return _higher_triangles(kind, nx, ny, lx, ly, x0, y0)
     quad = kind in (QUA8, QUA9, TRI6)
     s = 2 if quad else 1
     ni, nj = s * nx + 1, s * ny + 1

@@ -15,6 +15,7 @@ Sources (paths inside the pmsim project):
   * data/results/artificial/*.json, *.msh  (pmsim's own FemState output, uniform fields; the
     raw files are kept as femstate_*.json for the byte-level checkpoint test)
   * data/sgm/sgm_5d17_ref.json and tests/test_solid_smith_5d17_qua4_axisym.rs (axisymmetric Qua4)
+  * tests/test_solid_smith_5d7_tri15_plane_strain.rs and smith_example_5d7_tri15 (Tri15, 12 IP)
   * tests/test_solid_bhatti_1d6_plane_stress.rs and the bhatti_example_1d6_bracket mesh (plane stress)
   * tests/test_solid_smith_5d11_qua4_plane_strain_uy.rs (inline expected displacements) and
     src/base/sample_meshes.rs (smith_example_5d11_qua4, smith_example_5d24_hex20 meshes)
@@ -114,6 +115,8 @@ def main(ref):
     print("wrote smith_5d24_hex20_mesh.npz", coords.shape, conn.shape)
     # linear-elastic SGM runs with natural boundary conditions: mesh, cell attributes, expected U
     for fn, test, out in [("smith_example_5d2_tri3", "test_solid_smith_5d2_tri3_plane_strain.rs", "smith_5d2_tri3"),
+                          ("smith_example_5d7_tri15", "test_solid_smith_5d7_tri15_plane_strain.rs",
+                           "smith_5d7_tri15"),
                           ("smith_example_5d15_qua8", "test_solid_smith_5d15_qua8_plane_strain.rs",
                            "smith_5d15_qua8"),
                           ("smith_example_5d30_tet4", "test_solid_smith_5d30_tet4_3d.rs", "smith_5d30_tet4"),

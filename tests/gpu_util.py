@@ -23,6 +23,8 @@ def perturbed_mesh(kind, seed=0, n=(3, 2, 2), amp=0.08):
     else:
         m = M.structured_3d(kind, n[0], n[1], n[2], float(n[0]), float(n[1]), float(n[2]))
     rng = np.random.default_rng(seed)
+    if kind in (M.TRI10, M.TRI15):  # nodes 1/3 or 1/4 of a cell apart: move them less
+        amp *= 0.4
     c = m.coords.copy()
     lo, hi = c.min(0), c.max(0)
     interior = np.all((c > lo + 1e-9) & (c < hi - 1e-9), axis=1)

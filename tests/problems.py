@@ -111,7 +111,7 @@ def _sgm(name):
 
 def sgm_natural(case):
     """Linear-elastic Smith-Griffiths runs with natural boundary conditions (reduced-system method,
-    one step), from tests/test_solid_smith_5d{2,15,27,30,24}_*.rs."""
+    one step), from tests/test_solid_smith_5d{2,7,15,27,30,24}_*.rs."""
     from pmsim_b200.natural import Natural, find_sides
     if case == "5d2_tri3":
         g, m = _sgm("smith_5d2_tri3")
@@ -125,6 +125,12 @@ def sgm_natural(case):
         nat = Natural(m).sides(find_sides(m, lambda p: abs(p[1]) < TOL, lambda p: p[0] <= 3.0 + TOL), -1.0)
         return dict(mesh=m, mats=[(1e6, 0.3)], cmat=None, ngauss=4 if case == "5d15_qua8" else 0, essential=ess,
                     natural=nat, golden=g, tol=1e-12 if case == "5d15_qua8" else 3e-13)
+    if case == "5d7_tri15":  # tests/test_solid_smith_5d7_tri15_plane_strain.rs (12 IP, point loads)
+        g, m = _sgm("smith_5d7_tri15")
+        ess = (_ess(m.points_where(lambda x, y: abs(x) < TOL), 0, 2) + _ess(m.points_where(lambda x, y: abs(x - 6) < TOL), 0, 2)
+               + _ess(m.points_where(lambda x, y: abs(y + 2) < TOL), 0, 2) + _ess(m.points_where(lambda x, y: abs(y + 2) < TOL), 1, 2))
+        nat = (Natural(m).points([0, 20], 1, -0.0778).points([5, 15], 1, -0.3556).points([10], 1, -0.1333))
+        return dict(mesh=m, mats=[(1e5, 0.2)], cmat=None, ngauss=12, essential=ess, natural=nat, golden=g, tol=1e-11)
     if case == "5d30_tet4":
         g, m = _sgm("smith_5d30_tet4")
         ess = (_ess(m.points_where(lambda x, y, z: abs(x) < TOL), 0, 3) + _ess(m.points_where(lambda x, y, z: abs(y) < TOL), 1, 3)
@@ -143,7 +149,7 @@ def sgm_natural(case):
     raise KeyError(case)
 
 
-SGM_NATURAL = ["5d2_tri3", "5d15_qua8", "5d27_qua9", "5d30_tet4", "5d24_hex20"]
+SGM_NATURAL = ["5d2_tri3", "5d7_tri15", "5d15_qua8", "5d27_qua9", "5d30_tet4", "5d24_hex20"]
 
 P_751 = [0.0, 0.1, 0.14, 0.18, 0.19, 0.192]
 

@@ -112,3 +112,37 @@ def test_general_elastoplastic_rejects_other_models_without_gpu():
     bad = _lib.EpSettings_(0.0, 1e-10, 1.0, 1000, 0)
     assert L.pms_ep_update_stress_batch(ctypes.byref(vm), 2, 1, None, None, None, None, ctypes.byref(bad),
                                         None, None, None, None) == 1
+
+
+def test_shape_tables_match_the_oracle_for_every_kind():
+    """pms_shape_table (the tables pms_elements_create uploads) against the oracle's Gauss rules and
+    shape functions, every kind and its default rule plus the alternative rules (host only)."""
+    import ctypes
+
+    import numpy as np
+
+    import oracle
+    from pmsim_b200 import mesh as M
+    L = _lib.load()
+    rules = {k: [0] for k in range(len(M.KIND_NAMES))}
+    rules[M.QUA8] += [4, 9]
+    rules[M.TRI6] += [6, 7, 12]
+    rules[M.TRI15] += [6, 7]
+    rules[M.HEX8] += [27]
+    for kind, ngs in rules.items():
+        nn, nd = M.KIND_NNODE[kind], M.KIND_NDIM[kind]
+        for ngauss in ngs:
+            ng = ctypes.c_int32(0)
+            assert L.pms_shape_table(kind, ngauss, None, ctypes.byref(ng)) == 0, (kind, ngauss)
+            n = ng.value
+            tab = np.zeros(n * nn * nd + n + n * nn)
+            assert L.pms_shape_table(kind, ngauss, _lib.ptr(tab), None) == 0
+            ksi, w = oracle.gauss(kind, ngauss)
+            assert len(w) == n, (kind, ngauss)
+            np.testing.assert_allclose(tab[n * nn * nd:n * nn * nd + n], w, rtol=0, atol=1e-15)
+            for p in range(n):
+                N, dN = oracle.shape(kind, ksi[p][:nd])
+                np.testing.assert_allclose(tab[p * nn * nd:(p + 1) * nn * nd], dN[:nn * nd], rtol=0, atol=1e-13)
+                off = n * nn * nd + n + p * nn
+                np.testing.assert_allclose(tab[off:off + nn], N[:nn], rtol=0, atol=1e-14)
+    assert L.pms_shape_table(99, 0, None, None) != 0

@@ -14,7 +14,7 @@ from pmsim_b200 import mesh as M
 pytestmark = pytest.mark.gpu
 
 E, NU, H, Z0 = 2e5, 0.3, 1e3, 250.0
-KINDS = [M.TRI3, M.TRI6, M.QUA4, M.QUA8, M.QUA9, M.TET4, M.HEX8, M.HEX20]
+KINDS = [M.TRI3, M.TRI6, M.QUA4, M.QUA8, M.QUA9, M.TET4, M.HEX8, M.HEX20, M.TRI10, M.TRI15]
 GRID = {2: (4, 3, 1), 3: (2, 2, 2)}
 
 

@@ -561,3 +561,31 @@ def test_oracle_reports_the_first_failing_cell_like_the_reference():
             with pytest.raises(oracle.OracleError) as e:
                 o.assemble_kk_coo()
             assert (e.value.code, e.value.cell) == (3, first)
+
+
+@pytest.mark.parametrize("kind", ["tri10", "tri15"])
+def test_oracle_cubic_and_quartic_triangles_pass_the_patch_test(kind):
+    """Tri10 / Tri15 (complete Lagrange triangles, default 6 / 12 IP rules): a linear displacement field
+    on a distorted mesh with straight edges gives the same strain at every IP, hence the elastic stress
+    D : eps everywhere, and the assembled F_int vanishes at the interior nodes (equilibrium of a uniform
+    stress field)."""
+    from pmsim_b200 import mesh as M
+    k = kind_from_name(kind)
+    rect = M.structured_2d(k, 4, 3, 4.0, 3.0)
+    c = rect.coords
+    inner = np.flatnonzero((c[:, 0] > 1e-9) & (c[:, 0] < 4 - 1e-9) & (c[:, 1] > 1e-9) & (c[:, 1] < 3 - 1e-9))
+    A = np.array([[1.1, 0.2], [-0.15, 0.9]])  # an affine map keeps the edges straight
+    m = M.Mesh(2, c @ A.T + np.array([0.3, -0.2]), rect.cells, k)
+    E, NU = 1e4, 0.25
+    el = oracle.OracleElements(m, 0, oracle.Params(E, NU))
+    el.initialize()
+    G = np.array([[2e-3, -1e-3], [5e-4, 1.5e-3]])  # u = G x
+    el.update_secondary_values((m.coords @ G.T).reshape(-1))
+    exx, eyy, exy = G[0, 0], G[1, 1], 0.5 * (G[0, 1] + G[1, 0])
+    lam, mu = E * NU / ((1 + NU) * (1 - 2 * NU)), E / (2 * (1 + NU))
+    tr = exx + eyy
+    expect = np.array([lam * tr + 2 * mu * exx, lam * tr + 2 * mu * eyy, lam * tr, 2 * mu * exy * np.sqrt(2.0)])
+    assert np.max(np.abs(el.sig - expect)) <= 1e-12 * np.max(np.abs(expect))
+    ff = el.assemble_f_int()
+    assert inner.size > 0
+    assert np.max(np.abs(ff.reshape(-1, 2)[inner])) <= 1e-12 * np.max(np.abs(ff))
