@@ -240,6 +240,19 @@ int pms_batch_solve_step(pms_batch* b, const double* c_values, const uint8_t* ac
  * iteration is completed by this tick). */
 int pms_batch_tick(pms_batch* b, const uint8_t* cmd, const double* c_values, int32_t* result, int32_t* iteration,
                    double* norm_rr, int32_t* pcg_iterations);
+/* The same lock-step load step as pms_batch_solve_step (same arguments, same results bit for bit),
+ * with the Newton loop resident on the device: one CUDA graph launch per load step, in which a
+ * conditional WHILE node runs every active problem's Newton iterations -- element pass, residual
+ * test, PCG start, a nested WHILE over PCG iterations, completion and update -- with the
+ * per-problem sequencing of SolverImplicit::iterate (src/fem/solver_implicit.rs:187-272) done by
+ * controller kernels; the host waits once per load step.  Every problem's PCG runs on the
+ * batch-wide engine (the engines give the same bits).  The graph is built on the first call and
+ * kept by the batch.  Not while a tick-driven linear solve is under way (PMS_ERR_INVALID). */
+int pms_batch_solve_step_graph(pms_batch* b, const double* c_values, const uint8_t* active, int32_t* iterations,
+                               double* norm_rr, int32_t* status, int32_t* pcg_iterations);
+/* Host waits for the device made by pms_batch_tick / pms_batch_solve_step / _graph so far. */
+int64_t pms_batch_host_syncs(const pms_batch* b);
+
 /* Launch shapes of the PCG (they change speed only: every engine computes bit-identical iterates).
  * A problem with at most team_max_ndof DOFs runs its whole PCG on a thread-block cluster ("team")
  * of C = 1, 2, 4, 8 or 16 CTAs of team_threads threads (256, 512 or 1024), its vectors resident in

@@ -137,6 +137,8 @@ SIGNATURES = {
     "pms_batch_reset": (_I, [_V]),
     "pms_batch_solve_step": (_I, [_V, _V, _V, _V, _V, _V, _V]),
     "pms_batch_tick": (_I, [_V, _V, _V, _V, _V, _V, _V]),
+    "pms_batch_solve_step_graph": (_I, [_V, _V, _V, _V, _V, _V, _V]),
+    "pms_batch_host_syncs": (_I64, [_V]),
     "pms_batch_set_tuning": (_I, [_V, ctypes.POINTER(BatchTuning_)]),
     "pms_batch_get_tuning": (_I, [_V, ctypes.POINTER(BatchTuning_)]),
     "pms_batch_autotune": (_I, [_V, ctypes.POINTER(BatchTuning_)]),

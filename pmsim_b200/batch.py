@@ -121,8 +121,11 @@ class BatchSolver:
                 out[k] = self.pres_const[k] * fn(t[self.pres_prob[k]])
         return out
 
-    def solve_step(self, active=None):
-        """Advance every active problem by one unit load step (t += 1) and solve it."""
+    def solve_step(self, active=None, device_loop=False):
+        """Advance every active problem by one unit load step (t += 1) and solve it.
+
+        device_loop: the whole Newton loop of the step runs on the device in one CUDA graph launch
+        (pms_batch_solve_step_graph): the same results bit for bit, one host wait per load step."""
         act = np.ones(self.np, np.uint8) if active is None else np.ascontiguousarray(active, np.uint8)
         t_new = self.t + act
         c = self.c_values(t_new)
@@ -130,8 +133,9 @@ class BatchSolver:
         norm = np.zeros(self.np)
         status = np.zeros(self.np, np.int32)
         pcg = np.zeros(self.np, np.int32)
-        self._check(self.L.pms_batch_solve_step(self.h, _lib.ptr(c), _lib.ptr(act), _lib.ptr(iters), _lib.ptr(norm),
-                                                _lib.ptr(status), _lib.ptr(pcg)))
+        fn = self.L.pms_batch_solve_step_graph if device_loop else self.L.pms_batch_solve_step
+        self._check(fn(self.h, _lib.ptr(c), _lib.ptr(act), _lib.ptr(iters), _lib.ptr(norm), _lib.ptr(status),
+                       _lib.ptr(pcg)))
         self.t = t_new
         self.step += act
         for p in np.nonzero(act)[0]:
@@ -144,11 +148,12 @@ class BatchSolver:
                 5: "von Mises stiffness cannot be computed with zero deviatoric norm (norm_s < 1e-10)",
                 6: "the determinant of the Jacobian must be positive"}
 
-    def solve(self, on_step=None, on_fail="raise"):
+    def solve(self, on_step=None, on_fail="raise", device_loop=False):
         """Runs every problem through its load steps (problems with fewer steps drop out).
 
         on_fail="raise" stops at the first failing problem with the reference's message;
-        on_fail="drop" removes failing problems and records them in ``self.failed``."""
+        on_fail="drop" removes failing problems and records them in ``self.failed``;
+        device_loop: each load step's Newton loop runs on the device (one graph launch per step)."""
         self.reset()
         self.failed = {}
         nmax = max(p.nsteps for p in self.problems)
@@ -157,7 +162,7 @@ class BatchSolver:
                             for i, p in enumerate(self.problems)], np.uint8)
             if not act.any():
                 break
-            iters, norm, status, pcg = self.solve_step(act)
+            iters, norm, status, pcg = self.solve_step(act, device_loop=device_loop)
             for i in np.nonzero(status * act)[0]:
                 msg = self.MESSAGES.get(int(status[i]), "error")
                 if on_fail == "raise":
@@ -165,6 +170,10 @@ class BatchSolver:
                 self.failed[int(i)] = (s, msg)
             if on_step is not None:
                 on_step(s, self)
+
+    def host_syncs(self):
+        """Host waits for the device inside the Newton loops so far (pms_batch_host_syncs)."""
+        return int(self.L.pms_batch_host_syncs(self.h))
 
     def tuning(self):
         t = _lib.BatchTuning_()

@@ -2363,6 +2363,102 @@ int elements_run_modes(pms_elements* h, const int32_t* cell_prob, const int32_t*
 
 int elements_status(pms_elements* h) { return finish_host(h); }
 
+namespace graph_pass {
+// Launch shape of the per-problem-mode element kernel (as launch_elem_t<..., UPD_MODE, F, K, CSR>).
+struct ElemLaunchShape {
+    const void* func = nullptr;
+    unsigned grid = 1, block = 128;
+    int smem = 0;
+};
+
+template <int NN, int LPC>
+ElemLaunchShape mode_shape_2d(const ElemArgs& a) {
+    constexpr int CPW = 32 / LPC;
+    auto kern = element2d_kernel<NN, LPC, UPD_MODE, true, true, true>;
+    const int smem = smem2_bytes(NN, a.ngauss, CPW);
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem2_bytes(NN, LPC, CPW));
+    cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
+    int64_t blocks = ((a.ncell + CPW - 1) / CPW + WPB2 - 1) / WPB2;
+    blocks = std::min<int64_t>(blocks, resident_blocks((const void*)kern, smem, WPB2 * 32));
+    ElemLaunchShape r;
+    r.func = (const void*)kern;
+    r.grid = (unsigned)std::max<int64_t>(blocks, 1);
+    r.block = WPB2 * 32;
+    r.smem = smem;
+    return r;
+}
+
+template <int ND, int NN>
+ElemLaunchShape mode_shape(pms_elements* h, const ElemArgs& a) {
+    if constexpr (ND == 2 && fits_2d<NN>()) {
+        if (a.ngauss <= NG2_MAX) {
+            if constexpr (packed_layout<NN>())
+                if (a.ngauss <= lanes_packed<NN>()) return mode_shape_2d<NN, lanes_packed<NN>()>(a);
+            return mode_shape_2d<NN, 16>(a);
+        }
+    }
+    auto kern = element_kernel<ND, NN, UPD_MODE, true, true, true>;
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
+    int64_t blocks = (a.ncell + cells_per_block(NN) - 1) / cells_per_block(NN);
+    blocks = std::min<int64_t>(blocks, resident_blocks((const void*)kern, h->smem_bytes));
+    ElemLaunchShape r;
+    r.func = (const void*)kern;
+    r.grid = (unsigned)std::max<int64_t>(blocks, 1);
+    r.block = WPB * 32;
+    r.smem = h->smem_bytes;
+    return r;
+}
+}  // namespace graph_pass
+
+int elements_graph_pass(pms_elements* h, cudaGraph_t g, cudaGraphNode_t dep, cudaGraphNode_t* last,
+                        const int32_t* cell_prob, const uint8_t* pmode, const double* ddu, double* ff, double* csr,
+                        unsigned long long* prob_err) {
+    ElemArgs a = make_args(h, ddu);
+    a.cell_prob = cell_prob;
+    a.pmode = pmode;
+    a.prob_err = prob_err;
+    a.csr = csr;
+    a.ff = ff;
+    using namespace graph_pass;
+    ElemLaunchShape sh;
+    switch (h->kind) {
+    case PMS_TRI3: sh = mode_shape<2, 3>(h, a); break;
+    case PMS_TRI6: sh = mode_shape<2, 6>(h, a); break;
+    case PMS_QUA4: sh = mode_shape<2, 4>(h, a); break;
+    case PMS_QUA8: sh = mode_shape<2, 8>(h, a); break;
+    case PMS_QUA9: sh = mode_shape<2, 9>(h, a); break;
+    case PMS_TET4: sh = mode_shape<3, 4>(h, a); break;
+    case PMS_TET10: sh = mode_shape<3, 10>(h, a); break;
+    case PMS_HEX8: sh = mode_shape<3, 8>(h, a); break;
+    case PMS_HEX20: sh = mode_shape<3, 20>(h, a); break;
+    case PMS_TRI10: sh = mode_shape<2, 10>(h, a); break;
+    case PMS_TRI15: sh = mode_shape<2, 15>(h, a); break;
+    default: return fail(h, PMS_ERR_INVALID, "unknown element kind");
+    }
+    cudaMemsetParams mp = {};
+    mp.dst = (void*)h->d_next;
+    mp.value = 0;
+    mp.elementSize = 4;
+    mp.width = 2;  // the 8-byte counter
+    mp.height = 1;
+    mp.pitch = 0;
+    cudaGraphNode_t nm, nk;
+    if (cudaGraphAddMemsetNode(&nm, g, dep ? &dep : nullptr, dep ? 1 : 0, &mp) != cudaSuccess)
+        return fail(h, PMS_ERR_CUDA, "graph memset node failed");
+    void* args[] = {&a};
+    cudaKernelNodeParams kp = {};
+    kp.func = (void*)sh.func;
+    kp.gridDim = dim3(sh.grid);
+    kp.blockDim = dim3(sh.block);
+    kp.sharedMemBytes = (unsigned)sh.smem;
+    kp.kernelParams = args;
+    if (cudaGraphAddKernelNode(&nk, g, &nm, 1, &kp) != cudaSuccess)
+        return fail(h, PMS_ERR_CUDA, "graph element node failed");
+    h->launches++;
+    *last = nk;
+    return PMS_OK;
+}
+
 }  // namespace pms
 
 // ------------------------------------------------------------------------------------------

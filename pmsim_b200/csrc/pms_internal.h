@@ -49,6 +49,14 @@ int elements_run_modes(pms_elements* h, const int32_t* cell_prob, const int32_t*
                        const double* ddu, double* ff, double* csr, const WorkQueue* queue = nullptr,
                        unsigned long long* prob_err = nullptr);
 
+// Adds to graph g (after dep, if not null) a memset node that zeroes the element pass's in-order work
+// counter and the node of the per-problem-mode element kernel over every cell (direct assembly into
+// csr and ff; cells of problems whose mode is 0 are skipped; per-problem error keys in prob_err);
+// *last receives the kernel node.  The same kernel and arithmetic as elements_run_modes.
+int elements_graph_pass(pms_elements* h, cudaGraph_t g, cudaGraphNode_t dep, cudaGraphNode_t* last,
+                        const int32_t* cell_prob, const uint8_t* pmode, const double* ddu, double* ff, double* csr,
+                        unsigned long long* prob_err);
+
 // Element error key -> element error code (internal E_* value), cell and IP.
 int decode_error(unsigned long long key, int64_t* cell, int32_t* ip);
 

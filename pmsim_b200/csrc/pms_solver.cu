@@ -802,6 +802,117 @@ __global__ void fill_masked_kernel(SolverArgs S, const uint8_t* flag, double* v,
     if (flag[S.node_prob[i / S.nd]]) v[i] = value;
 }
 
+// ---- device-resident load step (pms_batch_solve_step_graph) --------------------------------
+// One CUDA graph per load step: a conditional WHILE over Newton iterations, each one the element pass,
+// the residual test, the PCG start, a nested WHILE over PCG iterations (batch-wide engine), the
+// completion and the update.  The per-problem sequencing of pms_batch_tick (and of
+// SolverImplicit::iterate, src/fem/solver_implicit.rs:187-272) runs in these controller kernels
+// instead of on the host; each problem's arithmetic is the same kernels' and gives the same bits.
+enum : uint8_t { PH_IDLE = 0, PH_START = 1, PH_CONT = 2, PH_SOLVE = 3 };
+
+__global__ void step_init_kernel(int np, const uint8_t* sel, uint8_t* phase, int32_t* st, int32_t* cnt,
+                                 int32_t* pcgsum, double* lastnorm) {
+    for (int p = threadIdx.x; p < np; p += blockDim.x) {
+        phase[p] = sel[p] ? PH_START : PH_IDLE;
+        st[p] = 0;
+        cnt[p] = 0;
+        pcgsum[p] = 0;
+        lastnorm[p] = 0.0;
+    }
+}
+
+// element modes of this iteration (1: new step, 2: continue), dU = 0 mask of the new steps
+__global__ void step_pre_elem_kernel(int np, const uint8_t* phase, uint8_t* pmode, uint8_t* start, uint8_t* active,
+                                     int32_t* it, unsigned long long* perr) {
+    for (int p = threadIdx.x; p < np; p += blockDim.x) {
+        const uint8_t ph = phase[p];
+        const uint8_t m = ph == PH_START ? 1 : (ph == PH_CONT ? 2 : 0);
+        pmode[p] = m;
+        start[p] = ph == PH_START;
+        active[p] = m != 0;
+        if (ph == PH_START) it[p] = 0;
+        perr[p] = 0;
+    }
+}
+
+// after the residual: element errors, NaN/Inf, convergence on max|R|, or on to the linear solve
+__global__ void step_post_resid_kernel(int np, cudaGraphConditionalHandle pcg_loop, double tol_rr,
+                                       const unsigned long long* perr, const double* norm, uint8_t* phase,
+                                       uint8_t* active, uint8_t* first, const int32_t* it, int32_t* st, int32_t* cnt,
+                                       double* lastnorm) {
+    __shared__ int any;
+    if (threadIdx.x == 0) any = 0;
+    __syncthreads();
+    for (int p = threadIdx.x; p < np; p += blockDim.x) {
+        if (!active[p]) continue;
+        cnt[p] += 1;  // a residual evaluation, as the reference counts iterations
+        const int code = (int)(perr[p] & 0xff);
+        uint8_t solve = 0;
+        if (perr[p] != 0 && (code == 3 || code == 4 || code == 5)) {
+            st[p] = 101 + code;  // 104 zero sigma_d, 105 zero norm_s, 106 Jacobian
+            phase[p] = PH_IDLE;
+        } else {
+            lastnorm[p] = norm[p];
+            if (!isfinite(norm[p])) {
+                st[p] = 101;  // "Found NaN or Inf"
+                phase[p] = PH_IDLE;
+            } else if (norm[p] < tol_rr) {
+                st[p] = 1;
+                phase[p] = PH_IDLE;
+            } else {
+                solve = 1;
+                phase[p] = PH_SOLVE;
+                first[p] = it[p] == 0;
+                any = 1;
+            }
+        }
+        active[p] = solve;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) cudaGraphSetConditional(pcg_loop, any ? 1u : 0u);
+}
+
+__global__ void step_cond_pcg_kernel(cudaGraphConditionalHandle pcg_loop, const int32_t* nactive) {
+    cudaGraphSetConditional(pcg_loop, *nactive > 0 ? 1u : 0u);
+}
+
+// after the linear solve: NaN/Inf in mdu, convergence on rel(mdu) (not applied), or the update
+__global__ void step_post_complete_kernel(int np, int max_it, double tol_mdu, const double* rel, const uint8_t* active,
+                                          const int32_t* pcg_iters, uint8_t* phase, uint8_t* upd, int32_t* it,
+                                          int32_t* st, int32_t* pcgsum) {
+    for (int p = threadIdx.x; p < np; p += blockDim.x) {
+        upd[p] = 0;
+        if (!active[p]) continue;
+        pcgsum[p] += pcg_iters[p];  // parity buffer 0: the PCG loop runs an even number of iterations
+        if (!isfinite(rel[p])) {
+            st[p] = 102;  // "Found NaN or Inf in mdu"
+            phase[p] = PH_IDLE;
+        } else if (it[p] > 0 && rel[p] < tol_mdu) {
+            st[p] = 1;
+            phase[p] = PH_IDLE;
+        } else {
+            upd[p] = 1;
+            it[p] += 1;
+            if (it[p] >= max_it) {
+                st[p] = 103;  // "Newton-Raphson did not converge" (the update is applied, as in the tick)
+                phase[p] = PH_IDLE;
+            } else {
+                phase[p] = PH_CONT;
+            }
+        }
+    }
+}
+
+__global__ void step_cond_newton_kernel(int np, cudaGraphConditionalHandle newton_loop, const uint8_t* phase) {
+    __shared__ int any;
+    if (threadIdx.x == 0) any = 0;
+    __syncthreads();
+    for (int p = threadIdx.x; p < np; p += blockDim.x)
+        if (phase[p] == PH_START || phase[p] == PH_CONT) any = 1;
+    __syncthreads();
+    if (threadIdx.x == 0) cudaGraphSetConditional(newton_loop, any ? 1u : 0u);
+}
+
 }  // namespace
 
 // ------------------------------------------------------------------------------------ handle
@@ -829,6 +940,11 @@ struct pms_batch {
     int32_t *d_iters = nullptr, *d_nactive = nullptr;
     int64_t* d_queue = nullptr;    // work queue of the element pass: 4 arrays of np + 1
     unsigned long long* d_perr = nullptr;  // per problem: key of its element error in the last pass
+    // device-resident load step
+    cudaGraphExec_t step_graph = nullptr;
+    uint8_t *d_phase = nullptr, *d_sel = nullptr, *d_zero_engine = nullptr;
+    int32_t *d_st = nullptr, *d_cnt = nullptr, *d_pcgsum = nullptr, *d_it = nullptr;
+    double* d_lastnorm = nullptr;
     std::vector<int64_t> h_queue;
     const int64_t* d_indptr = nullptr;
     const int32_t* d_indices = nullptr;
@@ -842,6 +958,7 @@ struct pms_batch {
     std::string last_error;
     int64_t launches = 0;
     int64_t pcg_total = 0;
+    int64_t host_syncs = 0;  // host waits for the device inside the Newton loop (instrumentation)
     std::vector<int32_t> it;       // Newton iteration of each problem within its current load step
     std::vector<uint8_t> solving;  // per problem: linear solve under way
     std::vector<uint8_t> engine;   // per problem: 1 = block engine, 0 = batch-wide engine
@@ -869,6 +986,7 @@ struct pms_batch {
             if (c) cudaStreamSynchronize(c);
         std::lock_guard<std::mutex> lock(device_mutex());
         if (graph) cudaGraphExecDestroy(graph);
+        if (step_graph) cudaGraphExecDestroy(step_graph);
         if (ev_fork) cudaEventDestroy(ev_fork);
         for (auto e : ev_cls)
             if (e) cudaEventDestroy(e);
@@ -1105,6 +1223,7 @@ int pcg_phase(pms_batch* b, int nteam, int nwide, int budget, bool exact) {
             done += b->graph_iters_captured;
             if (exact) continue;
             cudaMemcpyAsync(&nact, b->d_nactive, sizeof(int32_t), cudaMemcpyDeviceToHost, st);
+            b->host_syncs++;
             if (cudaStreamSynchronize(st) != cudaSuccess)
                 return bfail(b, PMS_ERR_CUDA, cudaGetErrorString(cudaGetLastError()));
             if (!teams_busy() && (nact <= stop_at || done >= budget)) break;
@@ -1244,7 +1363,10 @@ int pms_batch_create(pms_elements* el, int32_t nproblem, const int64_t* point_pt
               b->alloc(&b->d_norm, nproblem) && b->alloc(&b->d_rel, nproblem) &&
               b->alloc(&b->d_iters, 2 * (size_t)nproblem) &&
               b->alloc(&b->d_nactive, 1) && b->alloc(&b->d_queue, 4 * ((size_t)nproblem + 1)) &&
-              b->alloc(&b->d_perr, (size_t)nproblem);
+              b->alloc(&b->d_perr, (size_t)nproblem) && b->alloc(&b->d_phase, nproblem) &&
+              b->alloc(&b->d_sel, nproblem) && b->alloc(&b->d_zero_engine, nproblem) &&
+              b->alloc(&b->d_st, nproblem) && b->alloc(&b->d_cnt, nproblem) && b->alloc(&b->d_pcgsum, nproblem) &&
+              b->alloc(&b->d_it, nproblem) && b->alloc(&b->d_lastnorm, nproblem);
     if (ok && ff_ext) ok = b->upload(&b->d_fext, ff_ext, n);
     if (!ok) {
         delete b;
@@ -1270,6 +1392,7 @@ int pms_batch_create(pms_elements* el, int32_t nproblem, const int64_t* point_pt
     cudaMemset(b->d_p, 0, n * 8);
     cudaMemset(b->d_pcg_active, 0, 2 * (size_t)nproblem);
     cudaMemset(b->d_cta_active, 0, nproblem);
+    cudaMemset(b->d_zero_engine, 0, nproblem);
     b->S.nd = nd;
     b->S.np = nproblem;
     b->S.engine = b->d_engine;
@@ -1371,6 +1494,7 @@ int pms_batch_tick(pms_batch* b, const uint8_t* cmd, const double* c_values, int
         cudaMemcpyAsync(hnorm.data(), b->d_norm, np * 8, cudaMemcpyDeviceToHost, st);
         std::vector<unsigned long long> perr(np, 0);
         cudaMemcpyAsync(perr.data(), b->d_perr, (size_t)np * 8, cudaMemcpyDeviceToHost, st);
+        b->host_syncs++;
         if (cudaStreamSynchronize(st) != cudaSuccess) return bfail(b, PMS_ERR_CUDA, "residual failed");
         b->launches += 4;
         // a material or geometry error stops its own problem only; every failing problem of this
@@ -1417,6 +1541,7 @@ int pms_batch_tick(pms_batch* b, const uint8_t* cmd, const double* c_values, int
         cudaMemcpyAsync(wa.data(), b->d_pcg_active, np, cudaMemcpyDeviceToHost, st);
         cudaMemcpyAsync(ca.data(), b->d_cta_active, np, cudaMemcpyDeviceToHost, st);
         cudaMemcpyAsync(pcg_step.data(), b->d_iters, np * 4, cudaMemcpyDeviceToHost, st);
+        b->host_syncs++;
         if (cudaStreamSynchronize(st) != cudaSuccess) return bfail(b, PMS_ERR_CUDA, "PCG failed");
         // ---- stage 4: problems whose PCG finished complete their Newton iteration
         bool any_fin = false;
@@ -1444,6 +1569,7 @@ int pms_batch_tick(pms_batch* b, const uint8_t* cmd, const double* c_values, int
             rel_multipliers_kernel<<<grid_of(np, 128), 128, 0, st>>>(np, b->d_active, b->d_first, b->d_ppres,
                                                                       b->d_mdl, b->d_mdl0, b->d_rel);
             cudaMemcpyAsync(hrel.data(), b->d_rel, np * 8, cudaMemcpyDeviceToHost, st);
+            b->host_syncs++;
             if (cudaStreamSynchronize(st) != cudaSuccess) return bfail(b, PMS_ERR_CUDA, "solve failed");
             for (int p = 0; p < np; p++) {
                 if (!sel[p]) continue;
@@ -1469,6 +1595,7 @@ int pms_batch_tick(pms_batch* b, const uint8_t* cmd, const double* c_values, int
             b->launches += 7;
         }
     }
+    b->host_syncs++;
     if (cudaStreamSynchronize(st) != cudaSuccess) return bfail(b, PMS_ERR_CUDA, "tick failed");
     return PMS_OK;
 }
@@ -1513,6 +1640,195 @@ int pms_batch_solve_step(pms_batch* b, const double* c_values, const uint8_t* ac
     }
     return PMS_OK;
 }
+
+}  // extern "C"
+
+namespace {
+// Kernel nodes appended one after another to a graph.
+struct GraphChain {
+    cudaGraph_t g;
+    cudaGraphNode_t prev = nullptr;
+    bool ok = true;
+    int nodes = 0;
+    void kernel(const void* fn, unsigned grid, unsigned block, void** args) {
+        if (!ok) return;
+        cudaGraphNode_t n;
+        ok = add_kernel_node(g, &n, prev, (void*)fn, grid, block, args) == cudaSuccess;
+        if (ok) {
+            prev = n;
+            nodes++;
+        }
+    }
+    // a conditional WHILE node on handle h (created on this graph); returns its body graph
+    cudaGraph_t while_node(cudaGraphConditionalHandle h) {
+        if (!ok) return nullptr;
+        cudaGraphNodeParams cp = {};
+        cp.type = cudaGraphNodeTypeConditional;
+        cp.conditional.handle = h;
+        cp.conditional.type = cudaGraphCondTypeWhile;
+        cp.conditional.size = 1;
+        cudaGraphNode_t n;
+        ok = cudaGraphAddNode(&n, g, prev ? &prev : nullptr, prev ? 1 : 0, &cp) == cudaSuccess;
+        if (!ok) return nullptr;
+        prev = n;
+        return cp.conditional.phGraph_out[0];
+    }
+};
+
+// The load-step graph (built once per batch; every pointer and constant it uses is fixed).
+int build_step_graph(pms_batch* b) {
+    if (b->step_graph) return PMS_OK;
+    std::lock_guard<std::mutex> lock(device_mutex());
+    cudaGraph_t G;
+    if (cudaGraphCreate(&G, 0) != cudaSuccess) return bfail(b, PMS_ERR_CUDA, "graph creation failed");
+    int np = b->np;
+    int64_t npres = b->npres;
+    SolverArgs S = b->S;
+    S.engine = b->d_zero_engine;  // every PCG on the batch-wide engine (the engines give the same bits)
+    double tol_rr = b->cfg.tol_rr_abs, tol_mdu = b->cfg.tol_mdu_rel, rtol = b->cfg.pcg_rtol;
+    int32_t max_it = b->cfg.n_max_iterations, max_pcg = b->cfg.pcg_max_iterations;
+    int zero = 0;
+    bool no_mask = false;
+    const unsigned nch = (unsigned)b->nchunk;
+    const int tpr = tpr_of(b->v.nd);
+    const void* spmv_dot = tpr == 8 ? (const void*)pcg_spmv_dot_kernel<8> : (const void*)pcg_spmv_dot_kernel<16>;
+    const unsigned qthreads = tpr == 8 ? quarter_threads<8>() : quarter_threads<16>();
+    const void* spmv = tpr == 8 ? (const void*)spmv_kernel<8> : (const void*)spmv_kernel<16>;
+    const int64_t* bptr = b->v.d_bptr;
+    const int32_t* kdiag = b->v.d_kdiag;
+    const double* csr = b->d_csr;
+    const double* fext = b->d_fext;
+    GraphChain top{G};
+    void* a_init[] = {&np, &b->d_sel, &b->d_phase, &b->d_st, &b->d_cnt, &b->d_pcgsum, &b->d_lastnorm};
+    top.kernel((const void*)step_init_kernel, 1, 1024, a_init);
+    cudaGraphConditionalHandle hN = 0, hP = 0;
+    if (top.ok) top.ok = cudaGraphConditionalHandleCreate(&hN, G, 1, cudaGraphCondAssignDefault) == cudaSuccess;
+    cudaGraph_t B1 = top.while_node(hN);
+    GraphChain body{B1};
+    body.ok = top.ok;
+    if (body.ok) body.ok = cudaGraphConditionalHandleCreate(&hP, B1, 0, 0) == cudaSuccess;
+    // element pass of the problems that start a step or continue it
+    void* a_pre[] = {&np, &b->d_phase, &b->d_pmode, &b->d_upd, &b->d_active, &b->d_it, &b->d_perr};
+    body.kernel((const void*)step_pre_elem_kernel, 1, 1024, a_pre);
+    void* a_zero[] = {&S, &b->d_upd, &b->d_ddu};
+    body.kernel((const void*)zero_masked_kernel, grid_of(b->ndof), 256, a_zero);
+    if (body.ok)
+        body.ok = elements_graph_pass(b->el, B1, body.prev, &body.prev, b->d_cell_prob, b->d_pmode, b->d_ddu, b->d_ff,
+                                      b->d_csr, b->d_perr) == PMS_OK;
+    // residual and its tests
+    void* a_res[] = {&S, &b->d_ff, (void*)&fext, &b->d_u, &b->d_lam, &b->d_c, &b->d_rr, &b->d_part_a};
+    body.kernel((const void*)residual_kernel, nch, CHN, a_res);
+    void* a_fin_n[] = {&np, &b->d_pchunk, &b->d_part_a, &b->d_norm, &zero};
+    body.kernel((const void*)finalize_kernel, grid_of(np, 128), 128, a_fin_n);
+    void* a_post[] = {&np, &hP, &tol_rr, &b->d_perr, &b->d_norm, &b->d_phase, &b->d_active, &b->d_first, &b->d_it,
+                      &b->d_st, &b->d_cnt, &b->d_lastnorm};
+    body.kernel((const void*)step_post_resid_kernel, 1, 1024, a_post);
+    // PCG start (block Jacobi, prescribed increments, r = R_f - K_fp mdu_p, scalars)
+    void* a_bj[] = {&S, (void*)&bptr, (void*)&kdiag, (void*)&csr, &b->d_binv};
+    body.kernel((const void*)block_jacobi_kernel, grid_of(b->nnode), 256, a_bj);
+    void* a_pi[] = {&S, &b->d_u, &b->d_c, &b->d_mdu};
+    body.kernel((const void*)pres_increment_kernel, grid_of(b->ndof), 256, a_pi);
+    void* a_kt[] = {&S, &b->d_indptr, &b->d_indices, (void*)&csr, &b->d_mdu, &b->d_kt, &b->d_active, &no_mask};
+    body.kernel(spmv, grid_of(b->ndof * tpr), 256, a_kt);
+    void* a_ps[] = {&S, &b->d_rr, &b->d_kt, &b->d_binv, &b->d_r, &b->d_x, &b->d_z, &b->d_p, &b->d_part_a, &b->d_part_b};
+    body.kernel((const void*)pcg_start_kernel, nch, CHN, a_ps);
+    void* a_is[] = {&np, &b->d_active, &b->d_zero_engine, &b->d_pchunk, &b->d_part_a, &b->d_part_b, &b->d_rho,
+                    &b->d_r0, &b->d_pcg_active, &b->d_cta_active, &b->d_iters};
+    body.kernel((const void*)pcg_init_scalars_kernel, (unsigned)np, CHN, a_is);
+    // PCG iterations, two per pass (the scalars are double-buffered by iteration parity)
+    cudaGraph_t B2 = body.while_node(hP);
+    GraphChain pcg{B2};
+    pcg.ok = body.ok;
+    int par0 = 0, par1 = 1;
+    for (int k = 0; k < 2; k++) {
+        int* par = k ? &par1 : &par0;
+        void* a1[] = {&S, par, &b->d_indptr, &b->d_indices, (void*)&csr, &b->d_p, &b->d_q, &b->d_part_c};
+        pcg.kernel(spmv_dot, 4 * nch, qthreads, a1);
+        void* a2[] = {&S, par, &b->d_part_c, &b->d_rho, &b->d_p, &b->d_q, &b->d_binv, &b->d_x, &b->d_r, &b->d_z,
+                      &b->d_part_a, &b->d_part_b, &b->d_nactive};
+        pcg.kernel((const void*)pcg_update_kernel, nch, CHN, a2);
+        void* a3[] = {&S, par, &b->d_part_a, &b->d_part_b, &b->d_rho, &b->d_r0, &rtol, &max_pcg, &b->d_iters, &b->d_z,
+                      &b->d_p, &b->d_nactive};
+        pcg.kernel((const void*)pcg_beta_direction_kernel, nch, CHN, a3);
+    }
+    void* a_cp[] = {&hP, &b->d_nactive};
+    pcg.kernel((const void*)step_cond_pcg_kernel, 1, 1, a_cp);
+    body.ok = body.ok && pcg.ok;
+    // completion: mdu, multiplier increments, rel(mdu), and the update
+    void* a_am[] = {&S, &b->d_x, &b->d_mdu};
+    body.kernel((const void*)assemble_mdu_kernel, grid_of(b->ndof), 256, a_am);
+    if (npres > 0) {
+        void* a_ml[] = {&npres, &b->d_pres_eq, &b->d_pres_prob, &b->d_active, &b->d_indptr, &b->d_indices,
+                        (void*)&csr, &b->d_mdu, &b->d_rr, &b->d_mdl};
+        body.kernel((const void*)multiplier_kernel, grid_of(npres), 256, a_ml);
+    }
+    void* a_rm[] = {&S, &b->d_first, &b->d_mdu, &b->d_mdu0, &b->d_part_a};
+    body.kernel((const void*)rel_mdu_kernel, nch, CHN, a_rm);
+    void* a_fin_r[] = {&np, &b->d_pchunk, &b->d_part_a, &b->d_rel, &zero};
+    body.kernel((const void*)finalize_kernel, grid_of(np, 128), 128, a_fin_r);
+    void* a_rml[] = {&np, &b->d_active, &b->d_first, &b->d_ppres, &b->d_mdl, &b->d_mdl0, &b->d_rel};
+    body.kernel((const void*)rel_multipliers_kernel, grid_of(np, 128), 128, a_rml);
+    void* a_pc[] = {&np, &max_it, &tol_mdu, &b->d_rel, &b->d_active, &b->d_iters, &b->d_phase, &b->d_upd, &b->d_it,
+                    &b->d_st, &b->d_pcgsum};
+    body.kernel((const void*)step_post_complete_kernel, 1, 1024, a_pc);
+    void* a_up[] = {&S, &b->d_upd, &b->d_mdu, &b->d_u, &b->d_ddu};
+    body.kernel((const void*)update_kernel, grid_of(b->ndof), 256, a_up);
+    if (npres > 0) {
+        void* a_uml[] = {&npres, &b->d_pres_prob, &b->d_upd, &b->d_mdl, &b->d_lam};
+        body.kernel((const void*)update_multipliers_kernel, grid_of(npres), 256, a_uml);
+    }
+    void* a_cn[] = {&np, &hN, &b->d_phase};
+    body.kernel((const void*)step_cond_newton_kernel, 1, 1024, a_cn);
+    const bool ok = top.ok && body.ok;
+    if (!ok || cudaGraphInstantiate(&b->step_graph, G, 0) != cudaSuccess) {
+        b->step_graph = nullptr;
+        cudaGraphDestroy(G);
+        return bfail(b, PMS_ERR_CUDA, "load-step graph construction failed");
+    }
+    cudaGraphDestroy(G);
+    b->launches += top.nodes + body.nodes + pcg.nodes + 1;
+    return PMS_OK;
+}
+}  // namespace
+
+extern "C" {
+
+int pms_batch_solve_step_graph(pms_batch* b, const double* c_values, const uint8_t* active, int32_t* iterations,
+                               double* norm_rr, int32_t* status, int32_t* pcg_iterations) {
+    if (!b || !active) return PMS_ERR_INVALID;
+    if (b->npres > 0 && !c_values) return PMS_ERR_INVALID;
+    const int np = b->np;
+    for (int p = 0; p < np; p++)
+        if (b->solving[p]) return bfail(b, PMS_ERR_INVALID, "a tick-driven linear solve is under way");
+    int rc = build_step_graph(b);
+    if (rc) return rc;
+    cudaStream_t st = b->v.stream;
+    if (b->npres > 0) cudaMemcpyAsync(b->d_c, c_values, b->npres * 8, cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(b->d_sel, active, np, cudaMemcpyHostToDevice, st);
+    if (cudaGraphLaunch(b->step_graph, st) != cudaSuccess) return bfail(b, PMS_ERR_CUDA, "load-step graph launch failed");
+    std::vector<int32_t> cnt(np), stv(np), pcg(np), itv(np);
+    std::vector<double> norm(np);
+    cudaMemcpyAsync(cnt.data(), b->d_cnt, np * 4, cudaMemcpyDeviceToHost, st);
+    cudaMemcpyAsync(stv.data(), b->d_st, np * 4, cudaMemcpyDeviceToHost, st);
+    cudaMemcpyAsync(pcg.data(), b->d_pcgsum, np * 4, cudaMemcpyDeviceToHost, st);
+    cudaMemcpyAsync(itv.data(), b->d_it, np * 4, cudaMemcpyDeviceToHost, st);
+    cudaMemcpyAsync(norm.data(), b->d_lastnorm, np * 8, cudaMemcpyDeviceToHost, st);
+    if (cudaStreamSynchronize(st) != cudaSuccess) return bfail(b, PMS_ERR_CUDA, cudaGetErrorString(cudaGetLastError()));
+    rc = elements_status(b->el);  // element errors are per problem (in stv); anything else is fatal
+    if (rc != PMS_OK && rc != PMS_ERR_ZERO_SIGMA_D && rc != PMS_ERR_ZERO_NORM_S && rc != PMS_ERR_JACOBIAN) return rc;
+    for (int p = 0; p < np; p++) {
+        if (active[p]) b->it[p] = itv[p];
+        b->pcg_total += pcg[p];
+        if (iterations) iterations[p] = cnt[p];
+        if (norm_rr) norm_rr[p] = norm[p];
+        if (status) status[p] = stv[p] >= 100 ? stv[p] - 100 : 0;
+        if (pcg_iterations) pcg_iterations[p] = pcg[p];
+    }
+    b->host_syncs += 1;
+    return PMS_OK;
+}
+
+int64_t pms_batch_host_syncs(const pms_batch* b) { return b ? b->host_syncs : 0; }
 
 int pms_batch_set_tuning(pms_batch* b, const pms_batch_tuning* t) {
     if (!b || !t) return PMS_ERR_INVALID;

@@ -165,3 +165,61 @@ def test_pcg_sixteen_cta_team_matches_batch_wide():
     through distributed shared memory) next to a small one: same bits as the batch-wide engine."""
     probs = [footing(64, 32, 1e4, 9.0, 1.0, nsteps=2), footing(6, 3, 2e4, 12.0, 1.5, nsteps=2)]
     _assert_same([(s, _solve_with(probs, s)) for s in ("wide", "teams4")])
+
+
+def test_device_resident_newton_loop_gives_the_same_bits():
+    """pms_batch_solve_step_graph: the Newton loop of each load step on the device (one CUDA graph
+    launch: conditional WHILE over iterations with a nested WHILE over PCG iterations) against the
+    host-sequenced lock-step solve: identical U, IP state, iteration counts and PCG counts, and one
+    host wait per load step instead of several per iteration."""
+    from pmsim_b200.batch import BatchSolver
+    rng = np.random.default_rng(17)
+    probs = [footing(int(rng.integers(4, 10)), int(rng.integers(2, 6)), float(1e4 * np.exp(rng.normal(0, 0.5))),
+                     float(rng.uniform(5, 20)), float(rng.uniform(0.5, 2.0)), nsteps=int(rng.integers(2, 5)))
+             for _ in range(6)]
+    a = BatchSolver(probs)
+    a.solve()
+    b = BatchSolver(probs)
+    b.solve(device_loop=True)
+    assert np.array_equal(a.u(), b.u())
+    for x, y in zip(a.elements.get_state(), b.elements.get_state()):
+        assert np.array_equal(x, y)
+    assert a.history == b.history
+    assert a.pcg_history == b.pcg_history
+    nsteps = max(p.nsteps for p in probs)
+    newton = sum(sum(h) for h in b.history)
+    assert b.host_syncs() == nsteps  # one wait per load step
+    assert a.host_syncs() > newton   # several per Newton iteration when the host drives the loop
+    # the golden SPO run through the device loop, with the oracle driver's iteration counts
+    pb = problems.SPO_PROBLEMS["2x2_elements_2d"]()
+    c = BatchSolver([as_problem(pb)], n_max_iterations=20)
+    worst = [0.0, 0.0]
+
+    def cb(step, bs):
+        du, ds = problems.compare_step(pb["golden"], step, bs.u_of(0), bs.state_of(0)[0], pb["ngauss"])
+        worst[0], worst[1] = max(worst[0], du), max(worst[1], ds)
+
+    c.solve(cb, device_loop=True)
+    assert worst[0] <= pb["tol_u"] and worst[1] <= pb["tol_s"], worst
+
+
+def test_device_resident_loop_stops_failing_problems_alone():
+    """Failures inside the device loop (a NaN prescribed value, a reflected cell) stop their problems
+    with the same step and message as the host-sequenced solve; the others keep their bits."""
+    from pmsim_b200.batch import BatchSolver
+    from test_gpu_errors import _footing
+    import error_cases as C
+    good = [_footing(6, 3, 1e4, 9.0, 1.0, 3), _footing(5, 4, 1.5e4, 12.0, 1.5, 3)]
+    bad_nan = _footing(6, 3, 1e4, 9.0, 1.0, 3, nan_from=2.0)
+    bad_jac = _footing(6, 3, 1e4, 9.0, 1.0, 3)
+    bad_jac.mesh = C.inverted(bad_jac.mesh, 7)
+    mix = [good[0], bad_nan, good[1], bad_jac]
+    a = BatchSolver(mix)
+    a.solve(on_fail="drop")
+    b = BatchSolver(mix)
+    b.solve(on_fail="drop", device_loop=True)
+    assert a.failed == b.failed and set(b.failed) == {1, 3}
+    ua, ub = a.u(), b.u()
+    for i in (0, 2):
+        assert np.array_equal(a.u_of(i, ua), b.u_of(i, ub))
+        assert a.history[i] == b.history[i]

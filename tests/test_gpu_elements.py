@@ -113,11 +113,12 @@ def test_csr_bit_reproducible():
 
 
 @pytest.mark.parametrize("kind", KINDS, ids=[M.KIND_NAMES[k] for k in KINDS])
-def test_direct_and_gather_assembly_give_the_same_bits(kind):
+def test_direct_and_gather_assembly_agree(kind):
     """The direct assembly (blocks added straight into the CSR values and R, row by row in ascending
-    cell order) and the gather assembly (dense element matrices, then row gathers in the same order)
-    sum every entry in the same order: identical bits, on the device and through host buffers, for
-    the fused call and the separate F_int / K calls."""
+    cell order) gives the same bits on every run, and agrees with the gather assembly (dense element
+    matrices, then row gathers in the same order) to 1e-13: the two are different kernel
+    instantiations, which the compiler may contract into fused multiply-adds differently, so only
+    the last bits may differ (a missing or doubled block would differ at O(1))."""
     m, g, o = make(kind, seed=7)
     ddu = plastic_ddu(m, seed=8)
     g.initialize_internal_values()
@@ -129,8 +130,12 @@ def test_direct_and_gather_assembly_give_the_same_bits(kind):
         g.update_and_assemble(ddu, ff, kv)
         f2 = g.assemble_f_int()
         k2 = g.assemble_kk()
-        got.setdefault(mode, []).append((ff.tobytes(), kv.tobytes(), f2.tobytes(), k2.tobytes()))
-    assert got["direct"][0] == got["direct"][1] == got["gather"][0]
+        got.setdefault(mode, []).append((ff, kv, f2, k2))
+    d0, d1, ga = got["direct"][0], got["direct"][1], got["gather"][0]
+    for a, b in zip(d0, d1):
+        assert a.tobytes() == b.tobytes(), "direct assembly not reproducible"
+    for a, b, what in zip(d0, ga, ("f_int", "K", "f_int (separate)", "K (separate)")):
+        assert_close(a, b, tol=1e-13, what=what)
     assert 0 < 1 - g.get_state()[2].mean() < 1
 
 
