@@ -110,7 +110,9 @@ class SolverImplicit:
             kk = (keep @ kk @ keep + sp.diags(self.flags.astype(float))).tocsc()
         return spla.splu(kk)
 
-    def solve(self, on_step=None):
+    def solve(self, on_step=None, on_iteration=None):
+        """on_step(step, t, u, elements) after each load step; on_iteration(step, iteration) after each
+        Newton iteration (a caller may raise there to stop the run)."""
         el = self.el
         u = np.zeros(self.neq_total)
         ddu = np.zeros(self.neq_total)
@@ -172,6 +174,8 @@ class SolverImplicit:
                 t0 = time.perf_counter()
                 el.update_and_assemble(ddu[: self.ndof], ff, None if self.constant_tangent else kv)
                 self.timing["elements"] += time.perf_counter() - t0
+                if on_iteration is not None:
+                    on_iteration(len(self.history), it)
                 if it == self.n_max_iterations - 1:
                     raise NewtonError("Newton-Raphson did not converge")
             if converged:
