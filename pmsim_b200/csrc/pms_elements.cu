@@ -95,6 +95,7 @@ struct ElemArgs {
     const int64_t* bptr = nullptr;       // block-row pointers [npoint + 1]
     const int16_t* cslot = nullptr;      // [cell][a][b]: column slot of node b in block row conn[a]
     const int32_t* crank = nullptr;      // [cell][a]: rank (bits 0..29), last-cell flag (bit 30)
+    const uint32_t* cfirst = nullptr;    // [cell][a] bit b: first contribution to block (conn[a], conn[b])
     int32_t* ticket = nullptr;           // [npoint]: slabs of this launch already added to the row
     unsigned long long* next = nullptr;  // in-order work counter, zero at launch
     double* csr = nullptr;               // CSR values of K (DOK)
@@ -694,20 +695,19 @@ element_kernel(ElemArgs A) {
             const int a0 = max(ti, 0) * RT, b0 = max(tj, 0) * CT;
             int64_t posR[RT], posC[CT];
             int rsR[RT], rsC[CT];
-            bool fR[RT], fC[CT];
+            uint32_t fR[RT];  // per row node: which of its blocks this cell contributes first
 #pragma unroll
             for (int r = 0; r < RT; r++) {
                 const int src = min(a0 + r, NN - 1);
                 posR[r] = __shfl_sync(FULL, pos_m, src);
                 rsR[r] = __shfl_sync(FULL, rs_m, src);
-                fR[r] = __shfl_sync(FULL, rank_m, src) == 0;
+                fR[r] = __ldg(A.cfirst + cell * NN + src);
             }
 #pragma unroll
             for (int c = 0; c < CT; c++) {
                 const int src = min(b0 + c, NN - 1);
                 posC[c] = __shfl_sync(FULL, pos_m, src);
                 rsC[c] = __shfl_sync(FULL, rs_m, src);
-                fC[c] = __shfl_sync(FULL, rank_m, src) == 0;
             }
             const int16_t* cs_cell = A.cslot + cell * (int64_t)(NN * NN);
             int spins = 0;
@@ -742,11 +742,14 @@ element_kernel(ElemArgs A) {
                         for (int c = 0; c < CT; c++) {
                             const int a = a0 + r, b = b0 + c;
                             if (a < NN && b < NN && a <= b) {
+                                // block (A, B) and its mirror (B, A) get their first contribution from
+                                // the lowest cell holding both nodes (one bit, symmetric in a and b)
+                                const bool first = (fR[r] >> b) & 1u;
                                 if ((rmask >> a) & 1u)
-                                    csr_add_block<ND>(A.csr, posR[r] + ND * (int64_t)cs_cell[a * NN + b], rsR[r], fR[r],
+                                    csr_add_block<ND>(A.csr, posR[r] + ND * (int64_t)cs_cell[a * NN + b], rsR[r], first,
                                                       acc[r][c], false);
                                 if (a != b && ((rmask >> b) & 1u))
-                                    csr_add_block<ND>(A.csr, posC[c] + ND * (int64_t)cs_cell[b * NN + a], rsC[c], fC[c],
+                                    csr_add_block<ND>(A.csr, posC[c] + ND * (int64_t)cs_cell[b * NN + a], rsC[c], first,
                                                       acc[r][c], true);
                             }
                         }
@@ -1209,17 +1212,16 @@ __global__ void __launch_bounds__(WPB2 * 32, 4) element2d_kernel(ElemArgs A) {
                 const int a0 = max(ti, 0) * T, b0 = max(tj, 0) * T;
                 int64_t posR[T], posC[T];
                 int rsR[T], rsC[T];
-                bool fR[T], fC[T];
+                uint32_t fR[T];  // per row node: which of its blocks this cell contributes first
 #pragma unroll
                 for (int r = 0; r < T; r++) {
                     const int src = sb + min(a0 + r, NN - 1);
                     posR[r] = __shfl_sync(FULL, pos_m, src);
                     rsR[r] = __shfl_sync(FULL, rs_m, src);
-                    fR[r] = __shfl_sync(FULL, rank_m, src) == 0;
+                    fR[r] = (active && ti >= 0) ? __ldg(A.cfirst + cell * NN + min(a0 + r, NN - 1)) : 0u;
                     const int srcc = sb + min(b0 + r, NN - 1);
                     posC[r] = __shfl_sync(FULL, pos_m, srcc);
                     rsC[r] = __shfl_sync(FULL, rs_m, srcc);
-                    fC[r] = __shfl_sync(FULL, rank_m, srcc) == 0;
                 }
                 const int16_t* cs_cell = A.cslot + cell * (int64_t)(NN * NN);
                 int spins = 0;
@@ -1255,11 +1257,12 @@ __global__ void __launch_bounds__(WPB2 * 32, 4) element2d_kernel(ElemArgs A) {
                             for (int c = 0; c < T; c++) {
                                 const int a = a0 + r, b = b0 + c;
                                 if (a < NN && b < NN && a <= b) {
+                                    const bool first = (fR[r] >> b) & 1u;  // lowest cell holding both nodes
                                     if ((mine >> a) & 1u)
-                                        csr_add_block<2>(A.csr, posR[r] + 2 * (int64_t)cs_cell[a * NN + b], rsR[r], fR[r],
+                                        csr_add_block<2>(A.csr, posR[r] + 2 * (int64_t)cs_cell[a * NN + b], rsR[r], first,
                                                          acc[r][c], false);
                                     if (a != b && ((mine >> b) & 1u))
-                                        csr_add_block<2>(A.csr, posC[c] + 2 * (int64_t)cs_cell[b * NN + a], rsC[c], fC[c],
+                                        csr_add_block<2>(A.csr, posC[c] + 2 * (int64_t)cs_cell[b * NN + a], rsC[c], first,
                                                          acc[r][c], true);
                                 }
                             }
@@ -1461,6 +1464,7 @@ struct pms_elements {
     double* d_ke1 = nullptr;
     int16_t* d_cslot = nullptr;    // direct assembly: per-cell slot map
     int32_t* d_crank = nullptr;    // direct assembly: per-cell incidence ranks
+    uint32_t* d_cfirst = nullptr;  // direct assembly: per-cell first-contribution bits
     int32_t* d_ticket = nullptr;   // direct assembly: per-node tickets (zero between launches)
     unsigned long long* d_next = nullptr;  // direct assembly: in-order work counter
     int assembly = PMS_ASSEMBLY_DIRECT;
@@ -1635,12 +1639,17 @@ void launch_elem_nn(pms_elements* h, const ElemArgs& a, int upd, bool dof, bool 
             else if (dof) launch_elem_t<ND, NN, UPD_NONE, true, false, false>(h, a);
             else launch_elem_t<ND, NN, UPD_NONE, false, true, false>(h, a);
         }
-    } else if (upd == UPD_CURRENT) {
-        if (csr) launch_elem_t<ND, NN, UPD_CURRENT, true, true, true>(h, a);
-        else launch_elem_t<ND, NN, UPD_CURRENT, true, true, false>(h, a);
     } else {
-        if (csr) launch_elem_t<ND, NN, UPD_BACKUP, true, true, true>(h, a);
-        else launch_elem_t<ND, NN, UPD_BACKUP, true, true, false>(h, a);
+        // update from the backup, then the requested outputs (the direct assembly writes exactly
+        // those; the dense outputs always go to the handle's own buffers).  Updates of the current
+        // state with outputs are not used by any call.
+        if (csr) {
+            if (dof && dok) launch_elem_t<ND, NN, UPD_BACKUP, true, true, true>(h, a);
+            else if (dof) launch_elem_t<ND, NN, UPD_BACKUP, true, false, true>(h, a);
+            else launch_elem_t<ND, NN, UPD_BACKUP, false, true, true>(h, a);
+        } else {
+            launch_elem_t<ND, NN, UPD_BACKUP, true, true, false>(h, a);
+        }
     }
 }
 
@@ -1706,6 +1715,7 @@ ElemArgs make_args(pms_elements* h, const double* ddu) {
     a.bptr = h->d_bptr;
     a.cslot = h->d_cslot;
     a.crank = h->d_crank;
+    a.cfirst = h->d_cfirst;
     a.ticket = h->d_ticket;
     a.next = h->d_next;
     return a;
@@ -1867,6 +1877,7 @@ int pms_elements_create(const pms_mesh* mesh, const pms_material* materials, int
          h->upload(&h->d_kdiag, h->pat.kdiag.data(), h->pat.kdiag.size()) &&
          h->upload(&h->d_cslot, h->pat.cslot.data(), h->pat.cslot.size()) &&
          h->upload(&h->d_crank, h->pat.crank.data(), h->pat.crank.size()) &&
+         h->upload(&h->d_cfirst, h->pat.cfirst.data(), h->pat.cfirst.size()) &&
          h->alloc(&h->d_ticket, (size_t)h->npoint) && h->alloc(&h->d_next, 1) &&
          h->alloc(&h->d_ddu, h->ndof) && h->alloc(&h->d_ff, h->ndof) && h->alloc(&h->d_status, 4);
     if (!ok) {
@@ -2257,6 +2268,19 @@ int pms_elements_kernel_times(pms_elements* h, double* ms, int64_t* counts) {
         h->ev_pending[k].clear();
     }
     return cuda_check(h);
+}
+
+int pms_mesh_assembly_maps(const pms_mesh* mesh, int16_t* cslot, int32_t* crank, uint32_t* cfirst) {
+    if (!mesh || !mesh->cells || kind_nnode(mesh->kind) < 0 || kind_ndim(mesh->kind) != mesh->ndim)
+        return PMS_ERR_INVALID;
+    Pattern p;
+    const char* msg = nullptr;
+    if (!build_pattern(mesh->ndim, kind_nnode(mesh->kind), mesh->npoint, mesh->ncell, mesh->cells, p, &msg))
+        return PMS_ERR_INVALID;
+    if (cslot) std::memcpy(cslot, p.cslot.data(), p.cslot.size() * sizeof(int16_t));
+    if (crank) std::memcpy(crank, p.crank.data(), p.crank.size() * sizeof(int32_t));
+    if (cfirst) std::memcpy(cfirst, p.cfirst.data(), p.cfirst.size() * sizeof(uint32_t));
+    return PMS_OK;
 }
 
 int pms_shape_table(int32_t kind, int32_t ngauss, double* tab, int32_t* ngauss_out) {

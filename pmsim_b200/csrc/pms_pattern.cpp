@@ -101,12 +101,23 @@ bool build_pattern(int nd, int nn, int64_t npoint, int64_t ncell, const int64_t*
     // per-cell maps of the direct assembly
     p.cslot.assign((size_t)ncell * nn * nn, 0);
     p.crank.assign((size_t)ncell * nn, 0);
-#pragma omp parallel for schedule(dynamic, 1024)
-    for (int64_t A = 0; A < npoint; A++) {
-        for (int64_t k = p.inc_ptr[A]; k < p.inc_ptr[A + 1]; k++) {
-            const int64_t ca = p.inc[k];  // cell * nn + a
-            p.crank[ca] = (int32_t)(k - p.inc_ptr[A]) | (k + 1 == p.inc_ptr[A + 1] ? CRANK_LAST : 0);
-            std::memcpy(&p.cslot[(size_t)ca * nn], &p.slot[(size_t)k * nn], sizeof(int16_t) * nn);
+    p.cfirst.assign((size_t)ncell * nn, 0);
+#pragma omp parallel
+    {
+        std::vector<char> seen;  // block columns of row A already touched by earlier cells of A
+#pragma omp for schedule(dynamic, 1024)
+        for (int64_t A = 0; A < npoint; A++) {
+            seen.assign((size_t)(p.bptr[A + 1] - p.bptr[A]), 0);
+            for (int64_t k = p.inc_ptr[A]; k < p.inc_ptr[A + 1]; k++) {
+                const int64_t ca = p.inc[k];  // cell * nn + a
+                p.crank[ca] = (int32_t)(k - p.inc_ptr[A]) | (k + 1 == p.inc_ptr[A + 1] ? CRANK_LAST : 0);
+                std::memcpy(&p.cslot[(size_t)ca * nn], &p.slot[(size_t)k * nn], sizeof(int16_t) * nn);
+                uint32_t first = 0;
+                for (int b = 0; b < nn; b++)
+                    if (!seen[p.slot[(size_t)k * nn + b]]) first |= 1u << b;
+                for (int b = 0; b < nn; b++) seen[p.slot[(size_t)k * nn + b]] = 1;
+                p.cfirst[ca] = first;
+            }
         }
     }
     return true;

@@ -9,7 +9,8 @@
 // in ascending order):
 //  * direct: the element kernel adds cell c's slab a into row A once the cells before c in A's
 //    incidence list have added theirs (rank[c*nn + a] = c's position in that list; a ticket per
-//    row counts the slabs added), at the columns cslot[(c*nn + a)*nn + b];
+//    row counts the slabs added), at the columns cslot[(c*nn + a)*nn + b]; a block's first
+//    contribution (cfirst) is stored, the later ones are added;
 //  * gather: a kernel owns one block row and adds the slabs of the cells' dense element matrices in
 //    that order (slot[k*nn + b]: where local node b of incidence k of A lands in the row).
 #pragma once
@@ -35,6 +36,9 @@ struct Pattern {
     // bit 30 set when c is the last of them
     std::vector<int16_t> cslot;
     std::vector<int32_t> crank;
+    // cfirst[c*nn + a] bit b: c is the lowest cell that holds both conn[c][a] and conn[c][b], so it adds
+    // the first contribution of block (conn[a], conn[b]) (and of its mirror); later cells add to it
+    std::vector<uint32_t> cfirst;
     int nbmax = 0;  // largest block row
     int64_t nblock() const { return (int64_t)bcol.size(); }
     int64_t nupper() const;  // blocks with A <= B
