@@ -97,13 +97,15 @@ def synthetic_ddu(m, size, seed=20241203):
     return u.reshape(-1).copy()
 
 
-def flops_per_ip_hex20():
-    """Algorithmic FP64 FLOPs of the fused element kernel per Hex20 IP (FMA = 2).
-    J (20 nodes x 9 FMA) + J^-T dN (20 x 9) + strain (20 x 9) + B^T sigma (20 x 9) +
-    h = S g (20 x 9) + three scaled copies (20 x 9 MUL, counted 1) + 210 node pairs x 33 FMA."""
-    fma = 20 * 9 * 5 + 210 * 33
-    mul = 20 * 9
-    return 2 * fma + mul
+def flops_per_ip_hex20(plastic):
+    """Algorithmic FP64 FLOPs of the fused element kernel per Hex20 IP (FMA = 2) when a fraction
+    `plastic` of the IPs is plastic.  Every IP: J, J^-T dN, strain and B^T sigma (20 nodes x 9 FMA
+    each), alpha g (20 x 3 MUL) and X_ab += alpha g_a g_b^T (210 node pairs x 9 FMA); once per cell,
+    K_ab = X_ab^T + c X_ab + tr(X_ab) 1 (210 x 9 FMA + 5 ADD), spread over the 27 IPs; every plastic
+    IP also h = S g (20 x 9 FMA), kappa g and beta h (20 x 6 MUL) and 210 x 18 FMA."""
+    fma = 20 * 9 * 4 + 210 * 9 + 210 * 9 / 27 + plastic * (20 * 9 + 210 * 18)
+    other = 20 * 3 + 210 * 5 / 27 + plastic * 20 * 6
+    return 2 * fma + other
 
 
 # DRAM bytes (read + write) per cell of one launch of the direct-assembly element kernel
@@ -917,7 +919,7 @@ def main():
         torch.cuda.empty_cache()
         served = run_served(args.served, args.rate, min(args.alone_sample, 16), detail_file=args.served_detail)
     ms_elem = kt[0] / max(kc[0], 1)  # the element kernel is the whole step (direct assembly)
-    fl_ip = flops_per_ip_hex20()
+    fl_ip = flops_per_ip_hex20(plastic)
     achieved_tf = nip * fl_ip / (ms_elem * 1e-3) / 1e12
     alg_bytes = algorithmic_bytes_step(m, ng, nnz)
     step_gbs = alg_bytes / (ms * 1e-3) / 1e9

@@ -128,21 +128,33 @@ __device__ __forceinline__ int64_t dequeue(unsigned long long* next) {
     return (int64_t)__shfl_sync(0xffffffffu, v, 0);
 }
 
-// One ND x ND block added into the CSR values: rows pos + i*rs, columns at the block's slot;
-// the first cell of the row stores 0 + v, later ones add to what is there (ascending cell order).
+// Atomic add at the L2 (relaxed, GPU scope; FP64 adds round to nearest even): no load, so the
+// issuing lane does not wait.  The row tickets order the adds of successive cells (each cell's
+// adds come after the release store that the next cell acquires), so every entry is still summed
+// in ascending cell order.
+__device__ __forceinline__ void red_add(double* p, double v) {
+    asm volatile("red.relaxed.gpu.global.add.f64 [%0], %1;" ::"l"(p), "d"(v) : "memory");
+}
+
+// One ND x ND block added into the CSR values: rows pos + i*rs, columns at the block's slot; the
+// lowest cell holding both nodes stores 0 + v, the later ones add to what is there.
 template <int ND>
 __device__ __forceinline__ void csr_add_block(double* __restrict__ csr, int64_t pos, int rs, bool first,
                                               const double (&v)[ND][ND], bool transpose) {
-    double old[ND][ND];
 #pragma unroll
     for (int i = 0; i < ND; i++)
 #pragma unroll
-        for (int j = 0; j < ND; j++) old[i][j] = first ? 0.0 : __ldcg(csr + pos + (int64_t)i * rs + j);
-#pragma unroll
-    for (int i = 0; i < ND; i++)
-#pragma unroll
-        for (int j = 0; j < ND; j++) csr[pos + (int64_t)i * rs + j] = old[i][j] + (transpose ? v[j][i] : v[i][j]);
+        for (int j = 0; j < ND; j++) {
+            double* q = csr + pos + (int64_t)i * rs + j;
+            const double x = transpose ? v[j][i] : v[i][j];
+            if (first) *q = 0.0 + x;
+            else red_add(q, x);
+        }
 }
+
+// Poll back-off of the row-ticket waits (ns): short first, since a legitimate wait is about the
+// time one earlier cell takes to write its slab.
+__device__ __forceinline__ unsigned order_backoff(int spins) { return spins < 8 ? 32 : (spins < 64 ? 256 : 1024); }
 
 // Item i of a range queue: off[k] <= i < off[k+1] maps to first[k] + (i - off[k]).
 __device__ __forceinline__ int64_t queue_item(int64_t i, int n, const int64_t* __restrict__ off,
@@ -233,15 +245,17 @@ template <int NN> struct TileShape {
 
 // Shared memory (doubles): block-wide dN table [m][j][32] + w[32] (+ N table [m][32] in 2D), then per cell
 // X[NN*ND], dU[NN*ND], G[ng][NN*ND+1] (gradients), TC[ng][10] (alpha, gamma, beta, S), CS[ng][6],
-// V[WPC][NN][VS] (per node at the current IP: alpha g, gamma g^, beta h, g, h, and in 2D g^,
-// 2 (a/2)|J|w r q and q, with h = S g (+ q s_zz e_x), g^ = g (+ q e_x) and q = N/r in the axisymmetric
-// idealization; double-buffered when two warps share the cell).
+// V: per node at the current IP.  3D: V[2][NN][9] = kappa g, beta h, h (plastic points of pass B,
+// double-buffered).  2D: V[WPC][NN][VS] = alpha g, gamma g^, beta h, g, h, g^, 2 (a/2)|J|w r q and
+// q, with h = S g (+ q s_zz e_x), g^ = g (+ q e_x) and q = N/r in the axisymmetric idealization
+// (double-buffered when two warps share the cell).
 __host__ __device__ constexpr int node_vec_doubles(int nd) { return 5 * nd + (nd == 2 ? 4 : 0); }
 __host__ __device__ constexpr int smem_table_doubles(int nn, int nd) {
     return nn * nd * 32 + 32 + (nd == 2 ? nn * 32 : 0);
 }
 __host__ __device__ constexpr int smem_cell_doubles(int nn, int nd, int ng) {
-    return 2 * nn * nd + ng * (nn * nd + 1) + ng * 10 + ng * 6 + warps_per_cell(nn) * nn * node_vec_doubles(nd);
+    return 2 * nn * nd + ng * (nn * nd + 1) + ng * 10 + ng * 6 +
+           (nd == 3 ? 2 * nn * 9 : warps_per_cell(nn) * nn * node_vec_doubles(nd));
 }
 __host__ __device__ constexpr int smem_bytes_for(int nn, int nd, int ng, int wpb) {
     return (smem_table_doubles(nn, nd) + (wpb / warps_per_cell(nn)) * smem_cell_doubles(nn, nd, ng)) * 8;
@@ -518,6 +532,123 @@ element_kernel(ElemArgs A) {
                 for (int i = 0; i < ND; i++)
 #pragma unroll
                     for (int j = 0; j < ND; j++) acc[r][c][i][j] = 0.0;
+        if constexpr (ND == 3) {
+        // Two passes, each entry with a fixed operation order.  With X_ab = sum_p alpha_p g_a g_b^T
+        // (alpha = w|J| a/2) the blocks are
+        //   K_ab = X_ab^T + tr(X_ab) 1 + c X_ab + sum over plastic p of (kappa_p g_a g_b^T + beta_p h_a h_b^T)
+        // with c = lambda/G and kappa_p = gamma_p - c alpha_p (gamma = w|J|(K - a/3)): an elastic
+        // point has a = 2G, so gamma = c alpha there and it adds to X only (9 FMA per node pair,
+        // against 27 at a plastic point).  Pass A needs no staging: alpha comes from TC and g from
+        // the gradients of phase 1.
+        static_assert(WPC == 1, "the 3D node-pair phase takes one warp per cell");
+        const double cvol = (mc.kk - 2.0 * mc.gg / 3.0) / mc.gg;
+        if (ti >= 0) {
+            for (int p = 0; p < ng; p++) {
+                const double al = TC[p * 10];
+                const double* g = G + p * GS;
+                double ar[RT][3];
+#pragma unroll
+                for (int r = 0; r < RT; r++)
+#pragma unroll
+                    for (int i = 0; i < 3; i++) ar[r][i] = al * g[min(a0 + r, NN - 1) * 3 + i];
+#pragma unroll
+                for (int c = 0; c < CT; c++) {
+                    double gb[3];
+#pragma unroll
+                    for (int j = 0; j < 3; j++) gb[j] = g[min(b0 + c, NN - 1) * 3 + j];
+#pragma unroll
+                    for (int r = 0; r < RT; r++)
+#pragma unroll
+                        for (int i = 0; i < 3; i++)
+#pragma unroll
+                            for (int j = 0; j < 3; j++) acc[r][c][i][j] = fma(ar[r][i], gb[j], acc[r][c][i][j]);
+                }
+            }
+#pragma unroll
+            for (int r = 0; r < RT; r++)
+#pragma unroll
+                for (int c = 0; c < CT; c++) {
+                    double x[3][3];
+#pragma unroll
+                    for (int i = 0; i < 3; i++)
+#pragma unroll
+                        for (int j = 0; j < 3; j++) x[i][j] = acc[r][c][i][j];
+                    const double tr = x[0][0] + x[1][1] + x[2][2];
+#pragma unroll
+                    for (int i = 0; i < 3; i++)
+#pragma unroll
+                        for (int j = 0; j < 3; j++) {
+                            const double v = fma(cvol, x[i][j], x[j][i]);
+                            acc[r][c][i][j] = (i == j) ? v + tr : v;
+                        }
+                }
+        }
+        // pass B, plastic points only: the node lanes stage kappa g, beta h and h = S g of their
+        // node (two buffers, one warp barrier per point)
+        int npl = 0;
+        for (int p = 0; p < ng; p++) {
+            const double* t = TC + p * 10;
+            const double be = t[2];
+            if (be == 0.0) continue;  // elastic point: same value on every lane, uniform branch
+            double* V = V0 + (npl & 1) * NN * 9;
+            npl++;
+            const double* g = G + p * GS;
+            if (lane < NN) {
+                const double kap = t[1] - cvol * t[0];
+                double S[3][3];
+                S[0][0] = t[3];
+                S[1][1] = t[4];
+                S[2][2] = t[6];
+                S[0][1] = S[1][0] = t[5];
+                S[1][2] = S[2][1] = t[7];
+                S[0][2] = S[2][0] = t[8];
+                double gv[3];
+#pragma unroll
+                for (int i = 0; i < 3; i++) gv[i] = g[lane * 3 + i];
+                double* v = V + lane * 9;
+#pragma unroll
+                for (int i = 0; i < 3; i++) {
+                    double h = 0.0;
+#pragma unroll
+                    for (int j = 0; j < 3; j++) h = fma(S[i][j], gv[j], h);
+                    v[i] = kap * gv[i];
+                    v[3 + i] = be * h;
+                    v[6 + i] = h;
+                }
+            }
+            __syncwarp();
+            if (ti < 0) continue;
+            double kr[RT][3], hr[RT][3];
+#pragma unroll
+            for (int r = 0; r < RT; r++) {
+                const double* v = V + min(a0 + r, NN - 1) * 9;
+#pragma unroll
+                for (int i = 0; i < 3; i++) {
+                    kr[r][i] = v[i];
+                    hr[r][i] = v[3 + i];
+                }
+            }
+#pragma unroll
+            for (int c = 0; c < CT; c++) {
+                const int b = min(b0 + c, NN - 1);
+                double gb[3], hb[3];
+#pragma unroll
+                for (int j = 0; j < 3; j++) {
+                    gb[j] = g[b * 3 + j];
+                    hb[j] = V[b * 9 + 6 + j];
+                }
+#pragma unroll
+                for (int r = 0; r < RT; r++)
+#pragma unroll
+                    for (int i = 0; i < 3; i++)
+#pragma unroll
+                        for (int j = 0; j < 3; j++) {
+                            acc[r][c][i][j] = fma(kr[r][i], gb[j], acc[r][c][i][j]);
+                            acc[r][c][i][j] = fma(hr[r][i], hb[j], acc[r][c][i][j]);
+                        }
+            }
+        }
+        } else {
         constexpr int VS = node_vec_doubles(ND);
         for (int p = 0; p < ng; p++) {
             const double* t = TC + p * 10;
@@ -631,6 +762,7 @@ element_kernel(ElemArgs A) {
                     for (int r = 0; r < RT; r++) acc[r][c][0][0] = fma(Qr[r], qb, acc[r][c][0][0]);
             }
         }
+        }  // ND
         // dense output: write K_e (row-major NE x NE) through the warp's shared memory, RS node rows at a time:
         // each lane drops its blocks (a, b) and mirrors (b, a) into the staged rows, then the warp
         // copies the rows out with contiguous stores
@@ -720,19 +852,20 @@ element_kernel(ElemArgs A) {
                     ++spins;
                     const bool give_up = __shfl_sync(FULL, spins >= ORDER_WAIT_LIMIT || ((spins & 63) == 0 && order_aborted(A.errkey)), 0);
                     if (!give_up) {
-                        __nanosleep(spins < 16 ? 32 : 1024);
+                        __nanosleep(order_backoff(spins));
                         continue;
                     }
                     if (lane == 0) report(A, RANK_ORDER, E_ORDER, cell, 0);
                     ready = todo;
                     rmask = todo_mask;
                 }
-                __threadfence();  // the rows' earlier slabs are visible to every lane
+                __syncwarp();  // the node lanes' acquires order every lane's writes after the earlier cells'
                 if (DOF && ready) {
 #pragma unroll
                     for (int i = 0; i < ND; i++) {
                         double* q = A.ff + rowA * ND + i;
-                        *q = (rank_m == 0 ? 0.0 : __ldcg(q)) + Us[lane * ND + i];
+                        if (rank_m == 0) *q = 0.0 + Us[lane * ND + i];
+                        else red_add(q, Us[lane * ND + i]);
                     }
                 }
                 if (DOK && ti >= 0) {
@@ -754,8 +887,7 @@ element_kernel(ElemArgs A) {
                             }
                         }
                 }
-                __threadfence();  // this round's slabs are visible before their tickets move
-                __syncwarp();
+                __syncwarp();  // every lane's writes precede the node lanes' (cumulative) release stores
                 if (ready) ticket_store(A.ticket + rowA, last_m ? 0 : rank_m + 1);
                 todo = todo && !ready;
             }
@@ -1088,7 +1220,80 @@ __global__ void __launch_bounds__(WPB2 * 32, 4) element2d_kernel(ElemArgs A) {
                     for (int i = 0; i < 2; i++)
 #pragma unroll
                         for (int j = 0; j < 2; j++) acc[r][c][i][j] = 0.0;
-            if (ti >= 0) {
+            if (ti >= 0 && !A.axisym) {
+                // two passes, as in element_kernel: X_ab = sum_p alpha_p g_a g_b^T over every point,
+                // K_ab = X_ab^T + tr(X_ab) 1 + c X_ab, then kappa_p g_a g_b^T + beta_p h_a h_b^T at
+                // the plastic points (c = gamma/alpha of the elastic tangent, kappa = gamma - c alpha)
+                const double cvol = (mc.plane_stress ? mc.ps12 : mc.kk - 2.0 * mc.gg / 3.0) / mc.gg;
+                for (int p = 0; p < ng; p++) {
+                    const double al = TC[p * 4];
+                    const double2* Gp = reinterpret_cast<const double2*>(G + p * GS);
+                    double ar[T][2];
+#pragma unroll
+                    for (int r = 0; r < T; r++) {
+                        const double2 ga2 = Gp[min(a0 + r, NN - 1)];
+                        ar[r][0] = al * ga2.x;
+                        ar[r][1] = al * ga2.y;
+                    }
+#pragma unroll
+                    for (int c = 0; c < T; c++) {
+                        const double2 gb2 = Gp[min(b0 + c, NN - 1)];
+                        const double gb[2] = {gb2.x, gb2.y};
+#pragma unroll
+                        for (int r = 0; r < T; r++)
+#pragma unroll
+                            for (int i = 0; i < 2; i++)
+#pragma unroll
+                                for (int j = 0; j < 2; j++) acc[r][c][i][j] = fma(ar[r][i], gb[j], acc[r][c][i][j]);
+                    }
+                }
+#pragma unroll
+                for (int r = 0; r < T; r++)
+#pragma unroll
+                    for (int c = 0; c < T; c++) {
+                        const double x00 = acc[r][c][0][0], x01 = acc[r][c][0][1];
+                        const double x10 = acc[r][c][1][0], x11 = acc[r][c][1][1];
+                        const double tr = x00 + x11;
+                        acc[r][c][0][0] = fma(cvol, x00, x00) + tr;
+                        acc[r][c][0][1] = fma(cvol, x01, x10);
+                        acc[r][c][1][0] = fma(cvol, x10, x01);
+                        acc[r][c][1][1] = fma(cvol, x11, x11) + tr;
+                    }
+                for (int p = 0; p < ng; p++) {
+                    const double2 t01 = reinterpret_cast<const double2*>(TC)[2 * p];
+                    const double be = TC[p * 4 + 2];
+                    if (be == 0.0) continue;  // elastic point
+                    const double kap = t01.y - cvol * t01.x;
+                    const double2* Gp = reinterpret_cast<const double2*>(G + p * GS);
+                    const double2* Hp = reinterpret_cast<const double2*>(H + p * GS);
+                    double kr[T][2], hr[T][2];
+#pragma unroll
+                    for (int r = 0; r < T; r++) {
+                        const int a = min(a0 + r, NN - 1);
+                        const double2 ga2 = Gp[a], ha2 = Hp[a];
+                        kr[r][0] = kap * ga2.x;
+                        kr[r][1] = kap * ga2.y;
+                        hr[r][0] = be * ha2.x;
+                        hr[r][1] = be * ha2.y;
+                    }
+#pragma unroll
+                    for (int c = 0; c < T; c++) {
+                        const int b = min(b0 + c, NN - 1);
+                        const double2 gb2 = Gp[b], hb2 = Hp[b];
+                        const double gb[2] = {gb2.x, gb2.y};
+                        const double hb[2] = {hb2.x, hb2.y};
+#pragma unroll
+                        for (int r = 0; r < T; r++)
+#pragma unroll
+                            for (int i = 0; i < 2; i++)
+#pragma unroll
+                                for (int j = 0; j < 2; j++) {
+                                    acc[r][c][i][j] = fma(kr[r][i], gb[j], acc[r][c][i][j]);
+                                    acc[r][c][i][j] = fma(hr[r][i], hb[j], acc[r][c][i][j]);
+                                }
+                    }
+                }
+            } else if (ti >= 0) {  // axisymmetric: the hoop terms take the one-pass form
                 for (int p = 0; p < ng; p++) {
                     const double2 t01 = reinterpret_cast<const double2*>(TC)[2 * p];
                     const double al = t01.x, ga = t01.y, be = TC[p * 4 + 2];
@@ -1234,19 +1439,20 @@ __global__ void __launch_bounds__(WPB2 * 32, 4) element2d_kernel(ElemArgs A) {
                         ++spins;
                         const bool give_up = __shfl_sync(FULL, spins >= ORDER_WAIT_LIMIT || ((spins & 63) == 0 && order_aborted(A.errkey)), 0);
                         if (!give_up) {
-                            __nanosleep(spins < 16 ? 32 : 1024);
+                            __nanosleep(order_backoff(spins));
                             continue;
                         }
                         if (lane == 0) report(A, RANK_ORDER, E_ORDER, cell, 0);
                         ready = todo;
                         rmask = todo_mask;
                     }
-                    __threadfence();  // the rows' earlier slabs are visible to every lane
+                    __syncwarp();  // the node lanes' acquires order every lane's writes after the earlier cells'
                     if (DOF && ready) {
 #pragma unroll
                         for (int i = 0; i < 2; i++) {
                             double* q = A.ff + rowA * 2 + i;
-                            *q = (rank_m == 0 ? 0.0 : __ldcg(q)) + Us[hl * 2 + i];
+                            if (rank_m == 0) *q = 0.0 + Us[hl * 2 + i];
+                        else red_add(q, Us[hl * 2 + i]);
                         }
                     }
                     if (DOK && active && ti >= 0) {
@@ -1267,8 +1473,7 @@ __global__ void __launch_bounds__(WPB2 * 32, 4) element2d_kernel(ElemArgs A) {
                                 }
                             }
                     }
-                    __threadfence();  // this round's slabs are visible before their tickets move
-                    __syncwarp();
+                    __syncwarp();  // every lane's writes precede the node lanes' (cumulative) release stores
                     if (ready) ticket_store(A.ticket + rowA, last_m ? 0 : rank_m + 1);
                     todo = todo && !ready;
                 }
