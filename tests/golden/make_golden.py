@@ -19,6 +19,7 @@ Sources (paths inside the pmsim project):
   * tests/test_solid_bhatti_1d6_plane_stress.rs and the bhatti_example_1d6_bracket mesh (plane stress)
   * tests/test_solid_smith_5d11_qua4_plane_strain_uy.rs (inline expected displacements) and
     src/base/sample_meshes.rs (smith_example_5d11_qua4, smith_example_5d24_hex20 meshes)
+  * data/meshes/test_solid_felippa_thick_cylinder_axisym.msh, test_durand_farias_example4_qua4.msh
 """
 import json
 import os
@@ -156,6 +157,12 @@ def main(ref):
     spo(ref, "spo_751_pres_cylin_ref.json", "spo_751_pres_cylin.npz", mesh="data/spo/spo_751_pres_cylin_qua4.msh")
     spo(ref, "spo_753_circ_plate_ref.json", "spo_753_circ_plate.npz", mesh="data/spo/spo_753_circ_plate.msh")
     spo(ref, "spo_752_pres_sphere_collapse_ref.json", "spo_752_pres_sphere_collapse.npz")
+    # meshes of the linear-elastic benchmark tests that read them from data/meshes
+    for stem, out in [("test_solid_felippa_thick_cylinder_axisym", "felippa_thick_cylinder_axisym"),
+                      ("test_durand_farias_example4_qua4", "durand_farias_example4_qua4")]:
+        ndim, coords, cells, kind = read_msh(os.path.join(ref, "data/meshes", stem + ".msh"))
+        np.savez_compressed(os.path.join(HERE, out + ".npz"), coords=coords, cells=cells, kind=np.array(kind))
+        print("wrote", out, coords.shape, cells.shape, kind)
 
 
 if __name__ == "__main__":

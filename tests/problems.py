@@ -283,3 +283,125 @@ def bhatti_1d6_plane_stress():
     top = find_sides(m, lambda p: abs(p[1] - (2.0 - p[0] / 4.0)) < TOL)
     nat = Natural(m, thickness=0.25).sides(top, -20.0)
     return dict(mesh=m, young=1e4, poisson=0.2, thickness=0.25, essential=ess, natural=nat, golden=g, nsides=len(top))
+
+
+def felippa_thick_cylinder():
+    """tests/test_solid_felippa_thick_cylinder_axisym.rs (Felippa, A-FEM benchmark 14.1): two
+    axisymmetric Qua8 (r from 4 to 10, height 2), 4 IP, linear elastic E=1000, nu=0; u_z = 0 on the
+    bottom and top edges, Qn = -10 (internal pressure) on the inner edge r = 4; one step.  The test
+    checks u_r at the points of y = 0 against the thick-cylinder solution (Felippa's eq. 14.2) to
+    1e-15."""
+    from pmsim_b200.natural import Natural, find_sides
+    g = load("felippa_thick_cylinder_axisym.npz")
+    m = Mesh(2, g["coords"], g["cells"], kind_from_name(str(g["kind"])))
+    rin, rout, pres, young, nu = 4.0, 10.0, 10.0, 1000.0, 0.0
+    ess = _ess(m.points_where(lambda x, y: (np.abs(y) < TOL) | (np.abs(y - 2.0) < TOL)), 1, 2)
+    nat = Natural(m, axisymmetric=True).sides(find_sides(m, lambda p: abs(p[0] - rin) < TOL), -pres)
+
+    def ur(r):
+        return pres * (rin * rin * (1.0 + nu) * (rout * rout + r * r * (1.0 - 2.0 * nu))) / (
+            young * (rout * rout - rin * rin) * r)
+
+    return dict(mesh=m, young=young, poisson=nu, ngauss=4, essential=ess, natural=nat,
+                check_points=m.points_where(lambda x, y: np.abs(y) < TOL), ur=ur, tol=1e-15)
+
+
+def strip_load_stress(x, y, bb, hh, qn, nu):
+    """Flexible strip footing of half-width bb on an elastic half-plane (Davis and Selvadurai,
+    Elasticity and Geomechanics, 1996, p. 138), as src/analytical/elast_plane_strain_flexible_foot.rs:52-80
+    states it: the surface is y = hh, z = hh - y the depth; returns (s_xx, s_yy, s_xy)."""
+    z = hh - y
+    d1, d2 = x - bb, bb + x
+    s = np.sign(d1)
+    if z == 0.0:
+        th1, th2 = s * np.pi / 2.0, np.pi / 2.0
+    else:
+        th1, th2 = s * np.arctan(abs(d1) / z), np.arctan(d2 / z)
+    s1, s2 = np.sin(2.0 * th1), np.sin(2.0 * th2)
+    m = -qn / np.pi
+    syy = m * ((th2 + 0.5 * s2) - (th1 + 0.5 * s1))
+    sxx = m * ((th2 - 0.5 * s2) - (th1 - 0.5 * s1))
+    sxy = m * (s2 * s2 - s1 * s1)
+    return sxx, syy, sxy
+
+
+def durand_farias_example4():
+    """tests/test_durand_farias_example4.rs: flexible strip footing (half-width B = 2.5) on a
+    15B x 15B plane-strain Qua4 domain (49 cells), 4 IP, linear elastic E=1000, nu=0; u_x = 0 on the
+    left and right edges, u_y = 0 on the bottom, Qn = -200 on the top edges with x <= B; one step.
+    The test extrapolates the IP stresses of the cells on the left edge to their nodes (averaged at
+    shared nodes), keeps the nodes with x below half the first cell's width and checks each against
+    the strip-load solution: |s - s_ana| / Qn within 0.25 (xx), 0.23 (yy) and 0.09 (xy)."""
+    from pmsim_b200.natural import Natural, find_sides
+    g = load("durand_farias_example4_qua4.npz")
+    m = Mesh(2, g["coords"], g["cells"], kind_from_name(str(g["kind"])))
+    bb, qn = 2.5, 200.0
+    ww = hh = 15.0 * bb
+    ess = (_ess(m.points_where(lambda x, y: (np.abs(x) < TOL) | (np.abs(x - ww) < TOL)), 0, 2)
+           + _ess(m.points_where(lambda x, y: np.abs(y) < TOL), 1, 2))
+    footing = find_sides(m, lambda p: abs(p[1] - hh) < TOL, lambda p: p[0] <= bb)
+    nat = Natural(m).sides(footing, -qn)
+    left_cells = sorted({c for c, _ in find_sides(m, lambda p: abs(p[0]) < TOL)})
+    return dict(mesh=m, young=1000.0, poisson=0.0, ngauss=4, essential=ess, natural=nat, bb=bb, hh=hh, qn=qn,
+                left_cells=left_cells, tols=(0.25, 0.23, 0.09))
+
+
+def nodal_stresses(mesh, cells, sig, ngauss, keep):
+    """IP stresses (Mandel rows, cell-major) extrapolated to the nodes of `cells` and averaged at
+    shared nodes, for the nodes whose coordinates satisfy keep(x, y), sorted by x then y
+    (src/fem/post_processing.rs:617-670).  The extrapolation matrix is the least-squares inverse of
+    the shape functions at the IPs; with as many IPs as nodes (Qua4, 4 IP) it is N^-1.
+    Returns [(x, y, s_xx, s_yy, s_xy)]."""
+    import oracle
+    nn = mesh.nnode
+    ksi, _ = oracle.gauss(mesh.kind, ngauss)
+    nmat = np.array([oracle.shape(mesh.kind, ksi[p][:mesh.ndim])[0][:nn] for p in range(len(ksi))])
+    ext = np.linalg.pinv(nmat)
+    acc, cnt = {}, {}
+    for c in cells:
+        vals = ext @ sig[c * ngauss:(c + 1) * ngauss]
+        for a, pt in enumerate(mesh.cells[c]):
+            acc[int(pt)] = acc.get(int(pt), 0.0) + vals[a]
+            cnt[int(pt)] = cnt.get(int(pt), 0) + 1
+    out = []
+    for pt in acc:
+        x, y = mesh.coords[pt]
+        if keep(x, y):
+            v = acc[pt] / cnt[pt]
+            out.append((x, y, v[0], v[1], v[3] / np.sqrt(2.0)))
+    return sorted(out, key=lambda r: (r[0], r[1]))
+
+
+def one_qua4_mesh():
+    """gemlab's Samples::one_qua4: the unit square, nodes counter-clockwise from the origin."""
+    return Mesh(2, np.array([[0.0, 0.0], [1.0, 0.0], [1.0, 1.0], [0.0, 1.0]]), np.array([[0, 1, 2, 3]]), QUA4)
+
+
+def prescribe_displacements_2d():
+    """tests/test_prescribe_displacements_2d.rs: one plane-strain Qua4 (default rule, 4 IP), linear
+    elastic E=1500, nu=0.25; u_x = 0 on the left edge, u_y = 0 on the bottom, u_y = -0.1 on the top;
+    Lagrange multipliers, one step.  Expected U: u_x = eps_x = -dy nu / (nu - 1) at the right nodes,
+    u_y = -dy at the top, to 1e-15."""
+    m = one_qua4_mesh()
+    dy, nu = 0.1, 0.25
+    ess = (_ess(m.points_where(lambda x, y: np.abs(x) < TOL), 0, 2)
+           + _ess(m.points_where(lambda x, y: np.abs(y) < TOL), 1, 2)
+           + _ess(m.points_where(lambda x, y: np.abs(y - 1.0) < TOL), 1, 2, -dy))
+    eps_x = -dy * nu / (nu - 1.0)
+    return dict(mesh=m, young=1500.0, poisson=nu, essential=ess,
+                expected=np.array([0.0, 0.0, eps_x, 0.0, eps_x, -dy, 0.0, -dy]), tol=1e-15)
+
+
+def solid_prescribed_displacement():
+    """tests/test_solid_prescribed_displacement.rs: one plane-strain Qua4 (4 IP), linear elastic E=1,
+    nu=0.25; u_x = 0 at point 0, u_y = 0 at points 0 and 1, u_y = STRAIN_Y at points 2 and 3, the
+    uniaxial strain of a vertical stress q = -2.  Both of the test's approaches (partitioned system;
+    residual with unit diagonal rows) must give sigma = (0, q, q nu, 0) at every IP to 1e-15; the
+    residual approach also pins -R on the unknown equations (0.375, 0.375, -0.375 to six
+    decimals) and dU = (0, 0, 0.625, 0, 0.625, -1.875, 0, -1.875) to 1e-15."""
+    young, nu, q = 1.0, 0.25, -2.0
+    strain_y = -q * (nu - 1.0) * (nu + 1.0) / young
+    presc = {0: 0.0, 1: 0.0, 3: 0.0, 5: strain_y, 7: strain_y}
+    return dict(mesh=one_qua4_mesh(), young=young, poisson=nu, prescribed=presc, unknown=[2, 4, 6],
+                stress=np.array([0.0, q, q * nu, 0.0]), e1=np.array([0.375, 0.375, -0.375]),
+                ddu=np.array([0.0, 0.0, 0.625, 0.0, 0.625, -1.875, 0.0, -1.875]), tol=1e-15)

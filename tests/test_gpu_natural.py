@@ -69,3 +69,26 @@ def test_spo_753_axisymmetric_circular_plate_on_device():
     assert worst[0] <= 2.5e-9, worst
     assert worst[1] <= 2.5e-6, worst
     el.close()
+
+
+def test_spo_752_axisymmetric_pressurised_sphere_on_device():
+    """The SPO pressurised sphere (tests/test_spo_752_pres_sphere.rs, collapse run): the SPO 7.5.1
+    mesh as an axisymmetric section of a thick sphere, von Mises, internal pressure to 0.33269 in 4
+    steps with Lagrange multipliers, through the device element path at the reference test's
+    tolerances (the oracle replay is in test_oracle.py)."""
+    from pmsim_b200.elements import Elements, Material
+    from pmsim_b200.solver import SolverImplicit
+    pb = problems.pres_sphere_752()
+    el = Elements(pb["mesh"], Material.von_mises(*pb["params"]), ngauss=pb["ngauss"], axisymmetric=True)
+    solver = SolverImplicit(el, pb["essential"], t_fin=float(pb["nsteps"]), natural=pb["natural"])
+    worst = [0.0, 0.0]
+
+    def cb(step, t, u, e):
+        du, ds = problems.compare_step(pb["golden"], step, u, e.get_state()[0], pb["ngauss"])
+        worst[0] = max(worst[0], du)
+        worst[1] = max(worst[1], ds)
+
+    assert solver.solve(cb) == pb["nsteps"]
+    assert worst[0] <= pb["tol_u"], worst
+    assert worst[1] <= pb["tol_s"], worst
+    el.close()
