@@ -347,6 +347,43 @@ int pms_ep_update_stress_host(const pms_material* mat, int32_t ndim, int64_t n, 
  * (16*iters FLOP per thread); out[blocks*256] receives the chain sums.  Used as the FP64 peak. */
 int pms_probe_fp64_fma(int64_t iters, int32_t blocks, double* out, void* stream);
 
+/* ---- Distributed block-Jacobi PCG (one rank's part of a sharded linear solve) ----
+ * No counterpart in the reference, which solves one problem in one process with a direct solver
+ * (src/fem/solver_implicit.rs:187-272, LinSolver in src/fem/linear_system.rs).  The rank holds the
+ * owned rows of its local K: indptr[n_owned+1] and indices (host arrays) give their pattern in
+ * local DOF numbering (owned DOFs first, then ghosts, n_local in all); fixed_local[n_local] flags the
+ * prescribed DOFs, whose rows and columns are replaced by the identity.  send_idx: the owned DOFs
+ * the neighbours need, recv_idx: the ghost DOFs, each concatenated in ascending neighbour order.
+ * Vectors are device memory bound once (pms_dpcg_bind): x, r, z, q hold n_owned entries, p
+ * n_local, the send and receive buffers nsend and nrecv, scal 6 doubles (slot 0: r.z, slot 1: p.q,
+ * the two slots the caller all-reduces across ranks; 2: r.z of the current iteration, 3: r0.z0,
+ * 4: 1 once converged, 5: iterations).  One iteration, all on the handle's stream:
+ *   pack; post the exchange of the send/receive buffers; spmv(0) (interior rows, overlapping the
+ *   exchange); wait; unpack; spmv(1) (boundary rows); dot_pq; all-reduce slot 1; update;
+ *   all-reduce slot 0; direction(rtol).
+ * A solve starts with set_values (the local CSR values, device; every Newton iteration), start(b)
+ * (b: owned right-hand side, device), the all-reduce of slot 0 and init.  Once slot 4 is set every
+ * call leaves the iterates unchanged, so the host may read it every few iterations. */
+typedef struct pms_dpcg pms_dpcg;
+int pms_dpcg_create(int32_t ndim, int64_t n_owned, int64_t n_local, const int64_t* indptr, const int32_t* indices,
+                    const uint8_t* fixed_local, int64_t nsend, const int64_t* send_idx, int64_t nrecv,
+                    const int64_t* recv_idx, pms_dpcg** out);
+void pms_dpcg_destroy(pms_dpcg* h);
+const char* pms_dpcg_last_error(const pms_dpcg* h); /* NULL: the last refused pms_dpcg_create */
+int pms_dpcg_set_stream(pms_dpcg* h, void* stream);
+int pms_dpcg_bind(pms_dpcg* h, double* x, double* r, double* z, double* p, double* q, double* sendbuf,
+                  double* recvbuf, double* scal);
+int pms_dpcg_set_values(pms_dpcg* h, const double* values);
+int pms_dpcg_start(pms_dpcg* h, const double* b);
+int pms_dpcg_init(pms_dpcg* h);
+int pms_dpcg_pack(pms_dpcg* h);
+int pms_dpcg_unpack(pms_dpcg* h);
+int pms_dpcg_spmv(pms_dpcg* h, int32_t boundary);
+int pms_dpcg_dot_pq(pms_dpcg* h);
+int pms_dpcg_update(pms_dpcg* h);
+int pms_dpcg_direction(pms_dpcg* h, double rtol);
+int pms_dpcg_info(const pms_dpcg* h, int64_t* counts); /* nnz, interior rows, boundary rows, reduction blocks */
+
 /* Element vectors and matrices for a batch of cells WITHOUT ANY DEVICE ALLOCATION.
  * No counterpart in the reference: it exists for callers that cannot call cudaMalloc -- a program
  * running inside another framework that owns the whole device-memory budget, a real-time loop

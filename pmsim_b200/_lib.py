@@ -148,6 +148,21 @@ SIGNATURES = {
     "pms_batch_get_multipliers": (_I, [_V, _V]),
     "pms_batch_counters": (_I64, [_V, ctypes.POINTER(_I64)]),
     "pms_batch_last_error": (ctypes.c_char_p, [_V]),
+    "pms_dpcg_create": (_I, [_I, _I64, _I64, _V, _V, _V, _I64, _V, _I64, _V, ctypes.POINTER(_V)]),
+    "pms_dpcg_destroy": (None, [_V]),
+    "pms_dpcg_last_error": (ctypes.c_char_p, [_V]),
+    "pms_dpcg_set_stream": (_I, [_V, _V]),
+    "pms_dpcg_bind": (_I, [_V, _V, _V, _V, _V, _V, _V, _V, _V]),
+    "pms_dpcg_set_values": (_I, [_V, _V]),
+    "pms_dpcg_start": (_I, [_V, _V]),
+    "pms_dpcg_init": (_I, [_V]),
+    "pms_dpcg_pack": (_I, [_V]),
+    "pms_dpcg_unpack": (_I, [_V]),
+    "pms_dpcg_spmv": (_I, [_V, _I]),
+    "pms_dpcg_dot_pq": (_I, [_V]),
+    "pms_dpcg_update": (_I, [_V]),
+    "pms_dpcg_direction": (_I, [_V, _D]),
+    "pms_dpcg_info": (_I, [_V, _V]),
     "pms_version": (ctypes.c_char_p, []),
     "pms_material_launch_count": (_I64, []),
 }

@@ -15,7 +15,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libpms_b200.so")
-SOURCES = ["pms_material.cu", "pms_plasticity.cu", "pms_elements.cu", "pms_solver.cu", "pms_shapes.cpp", "pms_pattern.cpp"]
+SOURCES = ["pms_material.cu", "pms_plasticity.cu", "pms_elements.cu", "pms_solver.cu", "pms_dpcg.cu", "pms_shapes.cpp", "pms_pattern.cpp"]
 HEADERS = ["pms_device.cuh", "pms_shapes.h", "pms_pattern.h"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

@@ -137,6 +137,25 @@ __device__ __forceinline__ int tangent_coefs(const MatConst& m, double hh, const
     return OK;
 }
 
+// Block-Jacobi inverse of the nf x nf free part of a node's diagonal block, held in a[i][0..nf) with
+// a[i][nf..2nf) = the identity: Gauss-Jordan without pivoting (the free part of a diagonal block of
+// an SPD matrix is SPD), the inverse ends in a[i][nf..2nf).  Returns false at a pivot that is not
+// positive (the caller then falls back to the inverse of the diagonal).
+__device__ __forceinline__ bool spd_block_inverse(double (&a)[3][6], int nf) {
+    for (int k = 0; k < nf; k++) {
+        const double piv = a[k][k];
+        if (!(piv > 0.0)) return false;
+        const double ip = 1.0 / piv;
+        for (int j = 0; j < 2 * nf; j++) a[k][j] *= ip;
+        for (int i = 0; i < nf; i++)
+            if (i != k) {
+                const double f = a[i][k];
+                for (int j = 0; j < 2 * nf; j++) a[i][j] -= f * a[k][j];
+            }
+    }
+    return true;
+}
+
 // Symmetric-deviatoric projector entry in Mandel form
 __device__ __forceinline__ double psd(int i, int j) {
     if (i < 3 && j < 3) return (i == j) ? (2.0 / 3.0) : (-1.0 / 3.0);

@@ -37,6 +37,7 @@
 #include <vector>
 
 #include "../../include/pms.h"
+#include "pms_device.cuh"
 #include "pms_internal.h"
 
 using namespace pms;
@@ -332,19 +333,7 @@ __global__ void block_jacobi_kernel(SolverArgs S, const int64_t* bptr, const int
             a[i][j] = csr[base + (int64_t)fr[i] * nd * nb + fr[j]];
             a[i][nf + j] = (i == j) ? 1.0 : 0.0;
         }
-    // Gauss-Jordan without pivoting: the diagonal block of an SPD matrix is SPD
-    bool ok = true;
-    for (int k = 0; k < nf; k++) {
-        const double piv = a[k][k];
-        if (!(piv > 0.0)) { ok = false; break; }
-        const double ip = 1.0 / piv;
-        for (int j = 0; j < 2 * nf; j++) a[k][j] *= ip;
-        for (int i = 0; i < nf; i++)
-            if (i != k) {
-                const double f = a[i][k];
-                for (int j = 0; j < 2 * nf; j++) a[i][j] -= f * a[k][j];
-            }
-    }
+    const bool ok = spd_block_inverse(a, nf);
     double* out = binv + node * nd * nd;
     for (int i = 0; i < nd * nd; i++) out[i] = 0.0;
     for (int i = 0; i < nf; i++)

@@ -11,7 +11,10 @@ a disjoint set of CSR block rows of K and R:
   then the ghost nodes owned by other ranks;
 * per Newton iteration the ranks exchange the ghost values of the displacement increment (and,
   inside the linear solve, of the search direction) with their neighbours only;
-* the conjugate-gradient solve over the owned rows needs two all-reduces per iteration.
+* the linear solve is this library's distributed block-Jacobi PCG (``DevicePcg`` over the
+  ``pms_dpcg_*`` kernels): the exchange of the search direction's ghost values runs while the
+  interior rows are multiplied, and each iteration needs two all-reduces of one scalar, read by
+  the kernels from device memory (no host synchronisation inside an iteration).
 
 The element work of a rank is the ordinary element path (``Elements`` / ``pms_elements_*``) on its
 sub-mesh: its first ``n_owned`` block rows of K and entries of R are the owned ones.
@@ -127,6 +130,44 @@ class Halo:
             x[idx] = bufs[q]
         return x
 
+    @property
+    def send_dofs(self) -> np.ndarray:
+        """Owned local DOFs sent to the neighbours, concatenated in ascending neighbour order."""
+        return np.concatenate([v for _, v in sorted(self.send.items())] + [np.zeros(0, np.int64)])
+
+    @property
+    def recv_dofs(self) -> np.ndarray:
+        """Ghost local DOFs received from the neighbours, concatenated in ascending neighbour order."""
+        return np.concatenate([v for _, v in sorted(self.recv.items())] + [np.zeros(0, np.int64)])
+
+    def segments(self):
+        """(neighbour, send offset, send count, receive offset, receive count) in ascending order."""
+        out, so, ro = [], 0, 0
+        for q in sorted(set(self.send) | set(self.recv)):
+            ns, nr = len(self.send.get(q, ())), len(self.recv.get(q, ()))
+            out.append((q, so, ns, ro, nr))
+            so += ns
+            ro += nr
+        return out
+
+    def post(self, sendbuf, recvbuf):
+        """Posts the exchange of packed buffers (send_dofs / recv_dofs order) as one group and
+        returns its requests; on NCCL they run on the communicator's stream while the caller's
+        stream goes on (finish makes it wait)."""
+        import torch.distributed as dist
+        ops = []
+        for q, so, ns, ro, nr in self.segments():
+            if ns:
+                ops.append(dist.P2POp(dist.isend, sendbuf[so:so + ns], q))
+            if nr:
+                ops.append(dist.P2POp(dist.irecv, recvbuf[ro:ro + nr], q))
+        return dist.batch_isend_irecv(ops) if ops else []
+
+    @staticmethod
+    def finish(requests):
+        for r in requests:
+            r.wait()
+
 
 def owned_rows(indptr: np.ndarray, indices: np.ndarray, values: np.ndarray, n_owned_dof: int):
     """The owned rows of a local CSR matrix (the first n_owned_dof rows of the sub-mesh's K)."""
@@ -134,81 +175,163 @@ def owned_rows(indptr: np.ndarray, indices: np.ndarray, values: np.ndarray, n_ow
     return indptr[:n_owned_dof + 1].copy(), indices[:end].copy(), values[:end].copy()
 
 
-def _ell(rows, cols, vals, n):
-    """Row-padded (ELL) form of a row-sorted coordinate matrix: cols/vals of shape (n, width),
-    padding entries point at column 0 with value 0."""
-    counts = np.bincount(rows, minlength=n)
-    width = int(counts.max()) if n else 0
-    start = np.concatenate([[0], np.cumsum(counts)[:-1]])
-    slot = np.arange(len(rows)) - start[rows]
-    ec = np.zeros((n, width), dtype=np.int64)
-    ev = np.zeros((n, width))
-    ec[rows, slot] = cols
-    ev[rows, slot] = vals
-    return ec, ev
+# Slots of the PCG scalars (pms_dpcg_bind): the caller all-reduces RZN and PQ across ranks.
+RZN, PQ, RZ, RZ0, DONE, ITERS = range(6)
 
 
-def _spmv(ell_cols, ell_vals, x):
-    """y = A x with A in row-padded form: a fixed-order sum over each row (no atomics), so the
-    product, and the CG iterates built on it, are the same bits on every run."""
-    return (ell_vals * x[ell_cols]).sum(dim=1)
+class DevicePcg:
+    """One rank's distributed block-Jacobi PCG on this library's kernels (``pms_dpcg_*``): the owned
+    rows of K with the prescribed DOFs eliminated, split into interior and boundary rows so that the
+    ghost exchange overlaps the interior SpMV; block-Jacobi preconditioner over the owned nodes;
+    fixed-shape reductions.  CUDA tensors only: there is no host path.
+
+    indptr/indices: pattern of the owned rows of the local K (local DOF numbering); fixed_local:
+    prescribed flags of every local DOF; the values come with set_values every Newton iteration."""
+
+    def __init__(self, indptr, indices, n_owned: int, n_local: int, fixed_local, halo: "Halo", ndim: int, device):
+        import ctypes
+
+        import torch
+
+        from . import _lib
+        dev = torch.device(device)
+        if dev.type != "cuda":
+            raise RuntimeError("DevicePcg runs on the library's CUDA kernels: give it a CUDA device")
+        self.L = _lib.load()
+        self.device = dev
+        ip = np.ascontiguousarray(indptr[:n_owned + 1], dtype=np.int64)
+        ix = np.ascontiguousarray(indices[:int(ip[-1])], dtype=np.int32)
+        fx = np.ascontiguousarray(np.asarray(fixed_local, dtype=bool).astype(np.uint8))
+        sd = np.ascontiguousarray(halo.send_dofs, dtype=np.int64)
+        rd = np.ascontiguousarray(halo.recv_dofs, dtype=np.int64)
+        h = ctypes.c_void_p()
+        with torch.cuda.device(dev):
+            rc = self.L.pms_dpcg_create(ndim, n_owned, n_local, _lib.ptr(ip), _lib.ptr(ix), _lib.ptr(fx), len(sd),
+                                        _lib.ptr(sd), len(rd), _lib.ptr(rd), ctypes.byref(h))
+        if rc != 0:
+            raise _lib.PmsError(rc, (self.L.pms_dpcg_last_error(None) or b"").decode())
+        self.h = h
+        f64 = dict(dtype=torch.float64, device=dev)
+        self.x = torch.zeros(n_owned, **f64)
+        self.r = torch.zeros(n_owned, **f64)
+        self.z = torch.zeros(n_owned, **f64)
+        self.q = torch.zeros(n_owned, **f64)
+        self.p = torch.zeros(n_local, **f64)
+        self.sendbuf = torch.zeros(len(sd), **f64)
+        self.recvbuf = torch.zeros(len(rd), **f64)
+        self.scal = torch.zeros(6, **f64)
+        self._values = None
+        self._check(self.L.pms_dpcg_bind(self.h, *[_lib.ptr(t) if t.numel() else None for t in
+                                                   (self.x, self.r, self.z, self.p, self.q, self.sendbuf,
+                                                    self.recvbuf, self.scal)]))
+        self._check(self.L.pms_dpcg_set_stream(self.h, torch.cuda.current_stream(dev).cuda_stream))
+
+    def _check(self, rc):
+        if rc != 0:
+            from . import _lib
+            raise _lib.PmsError(rc, (self.L.pms_dpcg_last_error(self.h) or b"").decode())
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.pms_dpcg_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def set_values(self, values):
+        """Values of the local K (host array or device tensor); the owned rows are taken."""
+        import torch
+
+        from . import _lib
+        self._values = torch.as_tensor(values, dtype=torch.float64, device=self.device).contiguous()
+        self._check(self.L.pms_dpcg_set_values(self.h, _lib.ptr(self._values)))
+
+    def start(self, b):
+        import torch
+
+        from . import _lib
+        self._b = torch.as_tensor(b, dtype=torch.float64, device=self.device).contiguous()
+        self._check(self.L.pms_dpcg_start(self.h, _lib.ptr(self._b)))
+
+    def init(self):
+        self._check(self.L.pms_dpcg_init(self.h))
+
+    def pack(self):
+        self._check(self.L.pms_dpcg_pack(self.h))
+
+    def unpack(self):
+        self._check(self.L.pms_dpcg_unpack(self.h))
+
+    def spmv(self, boundary: int):
+        self._check(self.L.pms_dpcg_spmv(self.h, int(boundary)))
+
+    def dot_pq(self):
+        self._check(self.L.pms_dpcg_dot_pq(self.h))
+
+    def update(self):
+        self._check(self.L.pms_dpcg_update(self.h))
+
+    def direction(self, rtol: float):
+        self._check(self.L.pms_dpcg_direction(self.h, float(rtol)))
+
+    def info(self):
+        import ctypes
+        c = (ctypes.c_int64 * 4)()
+        self._check(self.L.pms_dpcg_info(self.h, c))
+        return dict(nnz=c[0], interior_rows=c[1], boundary_rows=c[2], reduction_blocks=c[3])
 
 
-def dist_cg(indptr, indices, values, b_owned, halo: Halo, n_local_dof: int, fixed_local: np.ndarray,
-            rtol=1e-12, max_iterations=10000):
-    """Jacobi-preconditioned CG on the owned rows of K with the prescribed DOFs eliminated (their
-    rows and columns replaced by the identity, right-hand side zero there).  indptr/indices/values:
-    the owned rows, columns in local DOF numbering; b_owned: owned right-hand side; fixed_local:
-    prescribed flags of every local DOF (owned and ghost).  Two all-reduces per iteration (r.z and
-    p.q); stops when r.z <= rtol^2 of its initial value.  Returns (x_owned, iterations)."""
-    import torch
-    import torch.distributed as dist
-    n = len(b_owned)
-    dev = b_owned.device
-    fixed_local = np.asarray(fixed_local, dtype=bool)
-    rows = np.repeat(np.arange(n), np.diff(indptr))
-    keep = ~(fixed_local[rows] | fixed_local[indices])
-    fr = np.flatnonzero(fixed_local[:n])
-    r_all = np.concatenate([rows[keep], fr])
-    c_all = np.concatenate([indices[keep], fr])
-    v_all = np.concatenate([values[keep], np.ones(len(fr))])
-    order = np.lexsort((c_all, r_all))
-    r_all, c_all, v_all = r_all[order], c_all[order], v_all[order]
-    diag = np.zeros(n)
-    d = r_all == c_all
-    np.add.at(diag, r_all[d], v_all[d])
-    dinv = torch.as_tensor(1.0 / diag, device=dev)
-    ec, ev = _ell(r_all, c_all.astype(np.int64), v_all, n)  # the device pattern is int32
-    t_cols = torch.as_tensor(ec, device=dev)
-    t_vals = torch.as_tensor(ev, device=dev)
-    b = b_owned.clone()
-    b[torch.as_tensor(fr, device=dev)] = 0.0
+class TorchComm:
+    """The collectives of dist_cg over torch.distributed (NCCL on GPUs, gloo on CPU): in-place sums of
+    the scalar slots and the halo's grouped point-to-point exchange."""
 
-    def allsum(t):
+    def __init__(self, halo: "Halo"):
+        self.halo = halo
+
+    def allsum(self, t):
+        import torch.distributed as dist
         dist.all_reduce(t, op=dist.ReduceOp.SUM)
-        return t
 
-    x = torch.zeros(n, dtype=b.dtype, device=dev)
-    r = b.clone()
-    z = dinv * r
-    p_local = torch.zeros(n_local_dof, dtype=b.dtype, device=dev)
-    p_local[:n] = z
-    rz = allsum((r * z).sum().reshape(1))[0]
-    rz0 = float(rz)
+    def post(self, sendbuf, recvbuf):
+        return self.halo.post(sendbuf, recvbuf)
+
+    def finish(self, requests):
+        self.halo.finish(requests)
+
+
+def dist_cg(pcg, comm, b_owned, rtol=1e-12, max_iterations=10000, check_every=8):
+    """Block-Jacobi PCG over the ranks (the kernels of ``pcg``; the collectives of ``comm``, a
+    TorchComm by default).  One iteration: pack the search direction's sent values, post the ghost
+    exchange, multiply the interior rows while it is in flight, finish it, unpack the ghosts, multiply
+    the boundary rows, then p.q (all-reduced), the update of x, r, z with r.z (all-reduced) and the
+    new direction.  Convergence (r.z <= rtol^2 r0.z0) is decided on the device from the reduced
+    value, the same on every rank, and freezes the iterates; the host reads the flag every
+    ``check_every`` iterations, so the result does not depend on how often it looks.
+    Returns (x_owned, iterations)."""
+    if isinstance(comm, Halo):
+        comm = TorchComm(comm)
+    pcg.start(b_owned)
+    comm.allsum(pcg.scal[RZN:RZN + 1])
+    pcg.init()
     it = 0
-    while it < max_iterations and float(rz) > rtol * rtol * rz0:
-        halo.exchange(p_local)
-        q = _spmv(t_cols, t_vals, p_local)
-        pq = allsum((p_local[:n] * q).sum().reshape(1))[0]
-        alpha = rz / pq
-        x += alpha * p_local[:n]
-        r -= alpha * q
-        z = dinv * r
-        rz_new = allsum((r * z).sum().reshape(1))[0]
-        p_local[:n] = z + (rz_new / rz) * p_local[:n]
-        rz = rz_new
-        it += 1
-    return x, it
+    while it < max_iterations:
+        for _ in range(min(check_every, max_iterations - it)):
+            pcg.pack()
+            req = comm.post(pcg.sendbuf, pcg.recvbuf)
+            pcg.spmv(0)
+            comm.finish(req)
+            pcg.unpack()
+            pcg.spmv(1)
+            pcg.dot_pq()
+            comm.allsum(pcg.scal[PQ:PQ + 1])
+            pcg.update()
+            comm.allsum(pcg.scal[RZN:RZN + 1])
+            pcg.direction(rtol)
+            it += 1
+        if float(pcg.scal[DONE]) != 0.0:
+            break
+    return pcg.x, int(float(pcg.scal[ITERS]))
 
 
 def _call(el, *names):
@@ -228,7 +351,7 @@ def _local_kk(el):
 
 def dist_newton(shard: Shard, ndim: int, elements, fixed_local, ff_ext_owned, nsteps, n_max_iterations=10,
                 tol_rr_abs=1e-10, tol_mdu_rel=1e-8, cg_rtol=1e-13, on_step=None, device="cpu",
-                prescribed_local=None):
+                prescribed_local=None, pcg_factory=None, comm=None):
     """The reference's implicit Newton loop (src/fem/solver_implicit.rs:187-272) over the ranks of a
     sharded problem.  ``elements`` runs the element calls on this rank's sub-mesh (the device
     ``Elements`` or any object with the same calls); ``ff_ext_owned(t)`` gives F_ext on the owned
@@ -244,8 +367,11 @@ def dist_newton(shard: Shard, ndim: int, elements, fixed_local, ff_ext_owned, ns
     Per iteration: R on the owned rows, max|R| over all ranks, K's owned rows, the correction by
     ``dist_cg``, rel(mdu) over all ranks, the owned dU update and the ghost exchange of dU before
     the stress update.  ``device`` holds the vectors that cross ranks ("cpu" for gloo, the rank's
-    CUDA device for NCCL).  Returns the per-step histories [(iteration, max|R|, rel(mdu))...] and
-    the owned displacements."""
+    CUDA device for NCCL).  The linear solves run on ``pcg_factory(indptr, indices, n_owned, n_local,
+    fixed_local, halo, ndim, device)``, built once from the pattern of the owned rows: DevicePcg
+    (this library's kernels) unless another object with the same calls is given; ``comm`` (default
+    TorchComm) carries its collectives.  Returns the per-step histories [(iteration, max|R|,
+    rel(mdu))...] and the owned displacements."""
     import torch
     import torch.distributed as dist
     nl = shard.n_local * ndim
@@ -255,6 +381,8 @@ def dist_newton(shard: Shard, ndim: int, elements, fixed_local, ff_ext_owned, ns
     pres = np.flatnonzero(fixed_own)  # owned prescribed DOFs (one multiplier each in LMM form)
     lmm = prescribed_local is not None
     halo = Halo(shard, ndim)
+    comm = comm if comm is not None else TorchComm(halo)
+    pcg = None
 
     def allmax(x):
         t = torch.tensor([float(x)], dtype=torch.float64, device=device)
@@ -298,20 +426,23 @@ def dist_newton(shard: Shard, ndim: int, elements, fixed_local, ff_ext_owned, ns
                 hist.append((it, norm_rr, None))
                 break
             rows = owned_rows(*_local_kk(elements), n)
+            if pcg is None:
+                pcg = (pcg_factory or DevicePcg)(rows[0], rows[1], n, nl, fixed_local, halo, ndim, device)
+            pcg.set_values(rows[2])
             if lmm:
                 vp = np.zeros(nl)
                 vp[pres] = rr_p  # mdu on the prescribed DOFs
                 b = rr - kmul(rows, vp)
-                mdu_f, _ = dist_cg(*rows, torch.as_tensor(b, device=device), halo, nl, fixed_local, rtol=cg_rtol)
-                mdu = mdu_f.cpu().numpy()
+                mdu_f, _ = dist_cg(pcg, comm, b, rtol=cg_rtol)
+                mdu = mdu_f.cpu().numpy().copy()
                 mdu[pres] = rr_p
                 full = np.zeros(nl)
                 full[:n] = mdu
                 mdl = rr[pres] - kmul(rows, full)[pres]
                 mvec = np.concatenate([mdu, mdl])
             else:
-                mdu_t, _ = dist_cg(*rows, torch.as_tensor(rr, device=device), halo, nl, fixed_local, rtol=cg_rtol)
-                mdu = mdu_t.cpu().numpy()
+                mdu_t, _ = dist_cg(pcg, comm, rr, rtol=cg_rtol)
+                mdu = mdu_t.cpu().numpy().copy()
                 mvec = mdu
             if it == 0:
                 mdu0, rel = mvec.copy(), 1.0

@@ -146,3 +146,27 @@ def test_shape_tables_match_the_oracle_for_every_kind():
                 off = n * nn * nd + n + p * nn
                 np.testing.assert_allclose(tab[off:off + nn], N[:nn], rtol=0, atol=1e-14)
     assert L.pms_shape_table(99, 0, None, None) != 0
+
+
+def test_dpcg_create_refuses_bad_input_before_any_device_call():
+    """pms_dpcg_create checks its host arrays before touching the device (host only)."""
+    import ctypes
+
+    import numpy as np
+    L = _lib.load()
+    ip = np.array([0, 1, 2], dtype=np.int64)
+    ix = np.array([0, 5], dtype=np.int32)  # column 5 is outside the 4 local DOFs
+    fx = np.zeros(4, dtype=np.uint8)
+    h = ctypes.c_void_p()
+    assert L.pms_dpcg_create(4, 2, 4, _lib.ptr(ip), _lib.ptr(ix), _lib.ptr(fx), 0, None, 0, None,
+                             ctypes.byref(h)) == _lib.PMS_ERR_INVALID
+    assert b"ndim" in L.pms_dpcg_last_error(None)
+    assert L.pms_dpcg_create(2, 2, 4, _lib.ptr(ip), _lib.ptr(ix), _lib.ptr(fx), 0, None, 0, None,
+                             ctypes.byref(h)) == _lib.PMS_ERR_INVALID
+    assert b"column" in L.pms_dpcg_last_error(None)
+    ix[1] = 1
+    bad_recv = np.array([0], dtype=np.int64)  # an owned DOF is not a ghost
+    assert L.pms_dpcg_create(2, 2, 4, _lib.ptr(ip), _lib.ptr(ix), _lib.ptr(fx), 0, None, 1, _lib.ptr(bad_recv),
+                             ctypes.byref(h)) == _lib.PMS_ERR_INVALID
+    assert b"ghost" in L.pms_dpcg_last_error(None)
+    assert h.value is None

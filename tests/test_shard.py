@@ -10,6 +10,7 @@ import pytest
 import torch.multiprocessing as mp
 
 import oracle
+from pcg_host import HostPcg
 from pmsim_b200 import shard as S
 from pmsim_b200.mesh import HEX8, QUA4, QUA8, structured_2d, structured_3d
 
@@ -119,7 +120,14 @@ def _cg_rank(rank, ws, port, q):
         xl[:n_own] = torch.as_tensor(xg[dof[:n_own]])
         halo.exchange(xl)
         halo_ok = bool(np.array_equal(xl.numpy(), xg[dof]))
-        x, it = S.dist_cg(op, oi, ov, torch.as_tensor(f[dof[:n_own]]), halo, len(dof), fixed[dof], rtol=1e-13)
+        # packed exchange (the order DevicePcg's pack/unpack use) gives the same ghost values
+        sb = torch.as_tensor(xl.numpy()[halo.send_dofs])
+        rb = torch.zeros(len(halo.recv_dofs), dtype=torch.float64)
+        halo.finish(halo.post(sb, rb))
+        halo_ok = halo_ok and bool(np.array_equal(rb.numpy(), xg[dof][halo.recv_dofs]))
+        pcg = HostPcg(op, oi, n_own, len(dof), fixed[dof], halo, 2)
+        pcg.set_values(ov)
+        x, it = S.dist_cg(pcg, S.TorchComm(halo), f[dof[:n_own]], rtol=1e-13)
         q.put((rank, halo_ok, it, dof[:n_own], x.numpy()))
     finally:
         dist.finalize()
@@ -221,7 +229,7 @@ def _newton_rank(rank, ws, port, q):
             el = _DeviceStyle(el)
         steps = []
         hist, u = S.dist_newton(s, 2, el, fixed[dof], lambda t: pb["natural"].ff_ext(t)[dof[:n_own]], pb["nsteps"],
-                                tol_mdu_rel=1e-10,
+                                tol_mdu_rel=1e-10, pcg_factory=HostPcg,
                                 on_step=lambda k, t, u, e: steps.append((u.copy(), e.sig.copy())))
         q.put((rank, [len(h) for h in hist], dof[:n_own], s.cells, steps))
     finally:
@@ -287,7 +295,7 @@ def _footing_rank(rank, ws, port, q):
                                    ngauss=9, sym_tol=-1.0)
         steps = []
         hist, _ = S.dist_newton(s, 2, el, fixed[dof], lambda t: np.zeros(n_own), 10, n_max_iterations=20,
-                                prescribed_local=lambda t: values(t)[dof],
+                                prescribed_local=lambda t: values(t)[dof], pcg_factory=HostPcg,
                                 on_step=lambda k, t, u, e: steps.append(u.copy()))
         q.put((rank, [len(h) for h in hist], dof[:n_own], steps))
     finally:
