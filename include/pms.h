@@ -174,12 +174,17 @@ int pms_elements_kernel_times(pms_elements* h, double* ms, int64_t* counts);
 int pms_shape_table(int32_t kind, int32_t ngauss, double* tab, int32_t* ngauss_out);
 
 /* Host-only (no GPU needed): the maps of the direct assembly pms_elements_create builds (no
- * counterpart in the reference, which sums COO triplets in the solver, src/base/assembly.rs:70-139):
- * for cell c and local nodes a, b -- cslot[(c*nnode + a)*nnode + b] the column slot of node b in
- * block row conn[a]; crank[c*nnode + a] c's position among the cells of conn[a] (bits 0..29; bit 30
- * set for the last one); cfirst[c*nnode + a] bit b set when c is the lowest cell holding both
- * conn[a] and conn[b] (it stores the first contribution of that block).  Any output may be NULL. */
-int pms_mesh_assembly_maps(const pms_mesh* mesh, int16_t* cslot, int32_t* crank, uint32_t* cfirst);
+ * counterpart in the reference, which sums COO triplets in the solver, src/base/assembly.rs:70-139).
+ * The kernel takes the cells in a processing order: order[k] is the k-th cell, colour classes of a
+ * greedy colouring (cells that share a node get different colours) within each segment of cells that
+ * shares no node with the rest.  Every entry of K and R is summed over its cells in that order.
+ * For cell c and local nodes a, b -- cslot[(c*nnode + a)*nnode + b] the column slot of node b in
+ * block row conn[a]; crank[c*nnode + a] c's position, in the processing order, among the cells of
+ * conn[a] (bits 0..29; bit 30 set for the last one); cfirst[c*nnode + a] bit b set when c is the
+ * first of the cells holding both conn[a] and conn[b] (it stores the first contribution of that
+ * block).  Any output may be NULL. */
+int pms_mesh_assembly_maps(const pms_mesh* mesh, int16_t* cslot, int32_t* crank, uint32_t* cfirst,
+                           int32_t* order);
 
 /* Host-only (no GPU needed): the CSR pattern pms_elements_create would build for this mesh.
  * Call with indices = NULL to get nnz (indptr[ndof+1] may already be filled). */

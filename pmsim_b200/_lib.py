@@ -127,7 +127,7 @@ SIGNATURES = {
     "pms_elements_set_assembly": (_I, [_V, _I]),
     "pms_set_device": (_I, [_I]),
     "pms_shape_table": (_I, [_I, _I, _V, _V]),
-    "pms_mesh_assembly_maps": (_I, [ctypes.POINTER(Mesh_), _V, _V, _V]),
+    "pms_mesh_assembly_maps": (_I, [ctypes.POINTER(Mesh_), _V, _V, _V, _V]),
     "pms_device_count": (_I, [_V]),
     "pms_elements_kernel_times": (_I, [_V, _V, _V]),
     "pms_probe_fp64_fma": (_I, [_I64, _I, _V, _V]),

@@ -96,6 +96,7 @@ struct ElemArgs {
     const int16_t* cslot = nullptr;      // [cell][a][b]: column slot of node b in block row conn[a]
     const int32_t* crank = nullptr;      // [cell][a]: rank (bits 0..29), last-cell flag (bit 30)
     const uint32_t* cfirst = nullptr;    // [cell][a] bit b: first contribution to block (conn[a], conn[b])
+    const int32_t* order = nullptr;      // direct assembly: the k-th dequeued position takes cell order[k]
     int32_t* ticket = nullptr;           // [npoint]: slabs of this launch already added to the row
     unsigned long long* next = nullptr;  // in-order work counter, zero at launch
     double* csr = nullptr;               // CSR values of K (DOK)
@@ -311,7 +312,8 @@ element_kernel(ElemArgs A) {
     for (int64_t cl = CSR ? dequeue(A.next) : (int64_t)blockIdx.x * CPB + cs; cl < A.ncell;
          cl = CSR ? dequeue(A.next) : cl + cstride) {
     cell_sync();  // the previous cell's write-out is done with the cell's shared memory
-    const int64_t cell = A.nq ? queue_item(cl, A.nq, A.q_off, A.q_first) : A.cell0 + cl;
+    int64_t cell = A.nq ? queue_item(cl, A.nq, A.q_off, A.q_first) : A.cell0 + cl;
+    if (CSR) cell = __ldg(A.order + cell);  // processing order (a permutation within each problem)
     int mode = (UPD == UPD_NONE) ? 0 : 2;
     if (UPD == UPD_MODE) {
         mode = A.pmode[A.cell_prob[cell]];
@@ -1015,6 +1017,7 @@ __global__ void __launch_bounds__(WPB2 * 32, 4) element2d_kernel(ElemArgs A) {
             int64_t ck = 0;
             int mk = (UPD == UPD_NONE) ? 0 : 2;
             if (on) ck = A.nq ? queue_item(cl, A.nq, A.q_off, A.q_first) : A.cell0 + cl;
+            if (CSR && on) ck = __ldg(A.order + ck);  // processing order
             if (UPD == UPD_MODE && on) {  // cells of inactive problems are left out
                 mk = A.pmode[A.cell_prob[ck]];
                 on = mk != 0;
@@ -1670,6 +1673,7 @@ struct pms_elements {
     int16_t* d_cslot = nullptr;    // direct assembly: per-cell slot map
     int32_t* d_crank = nullptr;    // direct assembly: per-cell incidence ranks
     uint32_t* d_cfirst = nullptr;  // direct assembly: per-cell first-contribution bits
+    int32_t* d_order = nullptr;    // direct assembly: processing order of the cells
     int32_t* d_ticket = nullptr;   // direct assembly: per-node tickets (zero between launches)
     unsigned long long* d_next = nullptr;  // direct assembly: in-order work counter
     int assembly = PMS_ASSEMBLY_DIRECT;
@@ -1921,6 +1925,7 @@ ElemArgs make_args(pms_elements* h, const double* ddu) {
     a.cslot = h->d_cslot;
     a.crank = h->d_crank;
     a.cfirst = h->d_cfirst;
+    a.order = h->d_order;
     a.ticket = h->d_ticket;
     a.next = h->d_next;
     return a;
@@ -2083,6 +2088,7 @@ int pms_elements_create(const pms_mesh* mesh, const pms_material* materials, int
          h->upload(&h->d_cslot, h->pat.cslot.data(), h->pat.cslot.size()) &&
          h->upload(&h->d_crank, h->pat.crank.data(), h->pat.crank.size()) &&
          h->upload(&h->d_cfirst, h->pat.cfirst.data(), h->pat.cfirst.size()) &&
+         h->upload(&h->d_order, h->pat.order.data(), h->pat.order.size()) &&
          h->alloc(&h->d_ticket, (size_t)h->npoint) && h->alloc(&h->d_next, 1) &&
          h->alloc(&h->d_ddu, h->ndof) && h->alloc(&h->d_ff, h->ndof) && h->alloc(&h->d_status, 4);
     if (!ok) {
@@ -2475,7 +2481,7 @@ int pms_elements_kernel_times(pms_elements* h, double* ms, int64_t* counts) {
     return cuda_check(h);
 }
 
-int pms_mesh_assembly_maps(const pms_mesh* mesh, int16_t* cslot, int32_t* crank, uint32_t* cfirst) {
+int pms_mesh_assembly_maps(const pms_mesh* mesh, int16_t* cslot, int32_t* crank, uint32_t* cfirst, int32_t* order) {
     if (!mesh || !mesh->cells || kind_nnode(mesh->kind) < 0 || kind_ndim(mesh->kind) != mesh->ndim)
         return PMS_ERR_INVALID;
     Pattern p;
@@ -2485,6 +2491,7 @@ int pms_mesh_assembly_maps(const pms_mesh* mesh, int16_t* cslot, int32_t* crank,
     if (cslot) std::memcpy(cslot, p.cslot.data(), p.cslot.size() * sizeof(int16_t));
     if (crank) std::memcpy(crank, p.crank.data(), p.crank.size() * sizeof(int32_t));
     if (cfirst) std::memcpy(cfirst, p.cfirst.data(), p.cfirst.size() * sizeof(uint32_t));
+    if (order) std::memcpy(order, p.order.data(), p.order.size() * sizeof(int32_t));
     return PMS_OK;
 }
 

@@ -3,16 +3,16 @@
 // The reference assembles K as COO triplets with duplicates in cell order and lets the
 // sparse solver sum them (src/base/assembly.rs:70-139, src/fem/linear_system.rs:132-164).
 // Here the pattern is built once per mesh.  Block row A of K (node A, ND x ND blocks) is the sum,
-// over the cells incident to A in ascending cell order, of the node-row slab (a, all b) of each
-// cell's element matrix, where a is A's local index in the cell.  Two assemblies use it, both
-// without atomics and with the same bits on every run (every node-pair block summed over its cells
-// in ascending order):
-//  * direct: the element kernel adds cell c's slab a into row A once the cells before c in A's
-//    incidence list have added theirs (rank[c*nn + a] = c's position in that list; a ticket per
-//    row counts the slabs added), at the columns cslot[(c*nn + a)*nn + b]; a block's first
-//    contribution (cfirst) is stored, the later ones are added;
+// over the cells incident to A, of the node-row slab (a, all b) of each cell's element matrix, where
+// a is A's local index in the cell.  Two assemblies use it, both with the same bits on every run
+// (every node-pair block summed over its cells in a fixed order):
+//  * direct: the element kernel takes the cells in a processing order (order: colour classes, so
+//    that cells taken one after another share no node) and adds cell c's slab a into row A once
+//    the cells before c, in that order, among A's cells have added theirs (rank[c*nn + a] = c's
+//    position; a ticket per row counts the slabs added), at the columns cslot[(c*nn + a)*nn + b];
+//    a block's first contribution (cfirst) is stored, the later ones are added;
 //  * gather: a kernel owns one block row and adds the slabs of the cells' dense element matrices in
-//    that order (slot[k*nn + b]: where local node b of incidence k of A lands in the row).
+//    ascending cell order (slot[k*nn + b]: where local node b of incidence k of A lands in the row).
 #pragma once
 #include <cstdint>
 #include <vector>
@@ -36,9 +36,14 @@ struct Pattern {
     // bit 30 set when c is the last of them
     std::vector<int16_t> cslot;
     std::vector<int32_t> crank;
-    // cfirst[c*nn + a] bit b: c is the lowest cell that holds both conn[c][a] and conn[c][b], so it adds
-    // the first contribution of block (conn[a], conn[b]) (and of its mirror); later cells add to it
+    // cfirst[c*nn + a] bit b: c is the first cell (in the processing order) that holds both conn[c][a]
+    // and conn[c][b], so it stores the first contribution of block (conn[a], conn[b]) (and of its
+    // mirror); later cells add to it
     std::vector<uint32_t> cfirst;
+    // processing order of the direct assembly (order[k] = k-th cell): within each segment of cells
+    // that shares no node with the rest, by greedy colour then index; crank and cfirst follow it
+    std::vector<int32_t> order;
+    int ncolor = 0;
     int nbmax = 0;  // largest block row
     int64_t nblock() const { return (int64_t)bcol.size(); }
     int64_t nupper() const;  // blocks with A <= B
