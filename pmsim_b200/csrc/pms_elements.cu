@@ -133,6 +133,16 @@ __device__ __forceinline__ int64_t dequeue(unsigned long long* next) {
 // issuing lane does not wait.  The row tickets order the adds of successive cells (each cell's
 // adds come after the release store that the next cell acquires), so every entry is still summed
 // in ascending cell order.
+// Asynchronous global -> shared copies (no register passes through; cp.async.wait_all, then a warp
+// barrier, before the data is read).  Sizes 4, 8 and 16 bytes, both addresses aligned to the size.
+template <int B>
+__device__ __forceinline__ void cp_async(void* smem_dst, const void* gsrc) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(smem_dst);
+    if constexpr (B == 16) asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(gsrc) : "memory");
+    else asm volatile("cp.async.ca.shared.global [%0], [%1], %2;" ::"r"(d), "l"(gsrc), "n"(B) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
 __device__ __forceinline__ void red_add(double* p, double v) {
     asm volatile("red.relaxed.gpu.global.add.f64 [%0], %1;" ::"l"(p), "d"(v) : "memory");
 }
@@ -254,9 +264,13 @@ __host__ __device__ constexpr int node_vec_doubles(int nd) { return 5 * nd + (nd
 __host__ __device__ constexpr int smem_table_doubles(int nn, int nd) {
     return nn * nd * 32 + 32 + (nd == 2 ? nn * 32 : 0);
 }
+// Direct-assembly metadata at the start of each cell area (doubles, kept even for 16-byte copies):
+// per node [bptr[A], bptr[A+1], crank | cfirst << 32, A] (NM), the pending ticket releases of the
+// warp's previous cell [row or -1, value] (PEND), and the cell's column-slot map (CSL, int16).
+__host__ __device__ constexpr int meta_doubles(int nn) { return 4 * nn + 2 * nn + 2 * ((nn * nn + 7) / 8); }
 __host__ __device__ constexpr int smem_cell_doubles(int nn, int nd, int ng) {
-    return 2 * nn * nd + ng * (nn * nd + 1) + ng * 10 + ng * 6 +
-           (nd == 3 ? 2 * nn * 9 : warps_per_cell(nn) * nn * node_vec_doubles(nd));
+    return meta_doubles(nn) + 2 * nn * nd + ng * (nn * nd + 1) + ng * 10 + ng * 6 +
+           (nd == 3 ? 2 * nn * 9 : warps_per_cell(nn) * nn * node_vec_doubles(nd)) + (ng & 1);
 }
 __host__ __device__ constexpr int smem_bytes_for(int nn, int nd, int ng, int wpb) {
     return (smem_table_doubles(nn, nd) + (wpb / warps_per_cell(nn)) * smem_cell_doubles(nn, nd, ng)) * 8;
@@ -273,7 +287,7 @@ element_kernel(ElemArgs A) {
     constexpr int RT = TS::RT, CT = TS::CT;
     constexpr int WPC = warps_per_cell(NN), CPB = WPB / WPC;
     static_assert(tile_count<NN>() <= 32 * WPC, "every node-pair tile needs a lane");
-    extern __shared__ double smem[];
+    extern __shared__ __align__(16) double smem[];
     const int ng = A.ngauss;
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const int cs = wid / WPC, half = wid % WPC;  // cell slot in the block, warp within the cell
@@ -281,7 +295,10 @@ element_kernel(ElemArgs A) {
     double* ws = smem + NE * 32;               // [32]
     double* Ns = ws + 32;                      // [m][32] (2D)
     double* wbase = smem + smem_table_doubles(NN, ND) + cs * smem_cell_doubles(NN, ND, ng);
-    double* Xs = wbase;                        // [m][d]
+    int64_t* NM = reinterpret_cast<int64_t*>(wbase);  // [m][4] (direct assembly)
+    int64_t* PEND = NM + 4 * NN;                      // [m][2] (direct assembly)
+    int16_t* CSL = reinterpret_cast<int16_t*>(PEND + 2 * NN);  // [NN*NN] (direct assembly)
+    double* Xs = wbase + meta_doubles(NN);     // [m][d]
     double* Us = Xs + NE;                      // [m][d]
     double* G = Us + NE;                       // [p][GS]
     double* TC = G + ng * GS;                  // [p][10]
@@ -309,6 +326,10 @@ element_kernel(ElemArgs A) {
     // persistent: the block's cell slots walk the queue with a stride of the whole grid, or (direct
     // assembly) take the next cell from the in-order counter
     const int64_t cstride = (int64_t)gridDim.x * CPB;
+    if constexpr (CSR) {
+        if (lane < NN) PEND[2 * lane] = -1;  // no release pending
+        __syncwarp();
+    }
     for (int64_t cl = CSR ? dequeue(A.next) : (int64_t)blockIdx.x * CPB + cs; cl < A.ncell;
          cl = CSR ? dequeue(A.next) : cl + cstride) {
     cell_sync();  // the previous cell's write-out is done with the cell's shared memory
@@ -507,6 +528,29 @@ element_kernel(ElemArgs A) {
 
     }  // warp 0
     cell_sync();  // G and TC are visible to every warp of the cell
+    if constexpr (CSR) {
+        if (DOF || DOK) {  // the scatter's row data and slot map, copied while the node pairs are computed
+            if (lane < NN) {
+                const int64_t pt = A.conn[cell * NN + lane];
+                int64_t* nm = NM + 4 * lane;
+                cp_async<8>(nm, A.bptr + pt);
+                cp_async<8>(nm + 1, A.bptr + pt + 1);
+                cp_async<4>(nm + 2, A.crank + cell * NN + lane);
+                cp_async<4>(reinterpret_cast<int32_t*>(nm + 2) + 1, A.cfirst + cell * NN + lane);
+                nm[3] = pt;
+            }
+            constexpr int CB = NN * NN * 2;  // bytes of the cell's slot map
+            const char* src = reinterpret_cast<const char*>(A.cslot + cell * (int64_t)(NN * NN));
+            char* dst = reinterpret_cast<char*>(CSL);
+            if constexpr (CB % 16 == 0) {
+                for (int k = lane; k < CB / 16; k += 32) cp_async<16>(dst + 16 * k, src + 16 * k);
+            } else if constexpr (CB % 8 == 0) {
+                for (int k = lane; k < CB / 8; k += 32) cp_async<8>(dst + 8 * k, src + 8 * k);
+            } else {  // a map whose cell offset is not 4-byte aligned (Tri15): plain loads
+                for (int k = lane; k < NN * NN; k += 32) CSL[k] = A.cslot[cell * (int64_t)(NN * NN) + k];
+            }
+        }
+    }
 
     // ---------------- phase 2: lane owns a tile of node-pair blocks ----------------
     int ti = -1, tj = -1;
@@ -813,15 +857,24 @@ element_kernel(ElemArgs A) {
     // waits for a row it could already write: no wait chains along the cell order.
     if constexpr (CSR) {
         if (DOF || DOK) {
+            cp_async_wait_all();
+            __syncwarp();  // every lane's copies are visible
+            // release the rows the warp's previous cell left pending before anything can wait here:
+            // a warp never waits while it holds a release
+            if (lane < NN && PEND[2 * lane] >= 0) {
+                ticket_store(A.ticket + PEND[2 * lane], (int)PEND[2 * lane + 1]);
+                PEND[2 * lane] = -1;
+            }
             int64_t rowA = 0, pos_m = 0;
             int rs_m = 0, rank_m = 0;
             bool last_m = false, todo = false;
             if (lane < NN) {
-                rowA = A.conn[cell * NN + lane];
-                const int64_t r0 = __ldg(A.bptr + rowA), r1 = __ldg(A.bptr + rowA + 1);
+                const int64_t* nm = NM + 4 * lane;
+                rowA = nm[3];
+                const int64_t r0 = nm[0], r1 = nm[1];
                 pos_m = (int64_t)ND * ND * r0;
                 rs_m = ND * (int)(r1 - r0);
-                const int32_t cr = __ldg(A.crank + cell * NN + lane);
+                const int32_t cr = reinterpret_cast<const int32_t*>(nm + 2)[0];
                 rank_m = cr & CRANK_MASK;
                 last_m = (cr & CRANK_LAST) != 0;
                 todo = true;
@@ -835,7 +888,7 @@ element_kernel(ElemArgs A) {
                 const int src = min(a0 + r, NN - 1);
                 posR[r] = __shfl_sync(FULL, pos_m, src);
                 rsR[r] = __shfl_sync(FULL, rs_m, src);
-                fR[r] = __ldg(A.cfirst + cell * NN + src);
+                fR[r] = reinterpret_cast<const uint32_t*>(NM + 4 * src + 2)[1];
             }
 #pragma unroll
             for (int c = 0; c < CT; c++) {
@@ -843,7 +896,7 @@ element_kernel(ElemArgs A) {
                 posC[c] = __shfl_sync(FULL, pos_m, src);
                 rsC[c] = __shfl_sync(FULL, rs_m, src);
             }
-            const int16_t* cs_cell = A.cslot + cell * (int64_t)(NN * NN);
+            const int16_t* cs_cell = CSL;
             int spins = 0;
             while (true) {
                 const unsigned todo_mask = __ballot_sync(FULL, todo);
@@ -878,7 +931,7 @@ element_kernel(ElemArgs A) {
                             const int a = a0 + r, b = b0 + c;
                             if (a < NN && b < NN && a <= b) {
                                 // block (A, B) and its mirror (B, A) get their first contribution from
-                                // the lowest cell holding both nodes (one bit, symmetric in a and b)
+                                // the first cell holding both nodes (one bit, symmetric in a and b)
                                 const bool first = (fR[r] >> b) & 1u;
                                 if ((rmask >> a) & 1u)
                                     csr_add_block<ND>(A.csr, posR[r] + ND * (int64_t)cs_cell[a * NN + b], rsR[r], first,
@@ -890,12 +943,25 @@ element_kernel(ElemArgs A) {
                         }
                 }
                 __syncwarp();  // every lane's writes precede the node lanes' (cumulative) release stores
-                if (ready) ticket_store(A.ticket + rowA, last_m ? 0 : rank_m + 1);
+                // the rows of the last round are released at the warp's next scatter (or its exit),
+                // when these writes are long done, so the release does not wait for them here
+                const bool final = rmask == todo_mask;
+                if (ready) {
+                    if (final) {
+                        PEND[2 * lane] = rowA;
+                        PEND[2 * lane + 1] = last_m ? 0 : rank_m + 1;
+                    } else {
+                        ticket_store(A.ticket + rowA, last_m ? 0 : rank_m + 1);
+                    }
+                }
                 todo = todo && !ready;
             }
         }
     }
     }  // cells
+    if constexpr (CSR) {  // the last cell's pending releases
+        if (lane < NN && PEND[2 * lane] >= 0) ticket_store(A.ticket + PEND[2 * lane], (int)PEND[2 * lane + 1]);
+    }
 }
 
 // ------------------------------------------------------------------------------------------------
@@ -934,7 +1000,7 @@ __host__ __device__ constexpr int cell2_doubles(int nn, int ng) {
                  : 4 * nn * nn) + 1) & ~1;
 }
 __host__ __device__ constexpr int smem2_bytes(int nn, int ng, int cpw) {
-    return (table2_doubles(nn) + cpw * WPB2 * cell2_doubles(nn, ng)) * 8;
+    return (table2_doubles(nn) + cpw * WPB2 * (cell2_doubles(nn, ng) + meta_doubles(nn))) * 8;
 }
 
 // Lanes per cell of the packed layout: enough for every node, every node-pair tile and (checked at
@@ -967,6 +1033,11 @@ __global__ void __launch_bounds__(WPB2 * 32, 4) element2d_kernel(ElemArgs A) {
     double* ws = dNs + NE * 16;   // [16]
     double* Ns = ws + 16;         // [m][16]
     double* Xs = smem2 + table2_doubles(NN) + (CPW * wid + hh) * cd;
+    // direct assembly: the slot's row data, pending releases and slot map (as in element_kernel)
+    int64_t* NM = reinterpret_cast<int64_t*>(smem2 + table2_doubles(NN) + CPW * WPB2 * cd +
+                                             (CPW * wid + hh) * meta_doubles(NN));
+    int64_t* PEND = NM + 4 * NN;
+    int16_t* CSL = reinterpret_cast<int16_t*>(PEND + 2 * NN);
     double* Us = Xs + NE;
     double* G = Us + NE;       // [p][GS]
     double* H = G + ng * GS;   // [p][GS]
@@ -1000,6 +1071,10 @@ __global__ void __launch_bounds__(WPB2 * 32, 4) element2d_kernel(ElemArgs A) {
             }
     }
 
+    if constexpr (CSR) {
+        if (hl < NN) PEND[2 * hl] = -1;  // no release pending
+        __syncwarp();
+    }
     const int64_t ngroup = (A.ncell + CPW - 1) / CPW;
     // groups of CPW consecutive cells: grid-strided, or (direct assembly) from the in-order counter
     for (int64_t pr = CSR ? dequeue(A.next) : (int64_t)blockIdx.x * WPB2 + wid; pr < ngroup;
@@ -1211,6 +1286,31 @@ __global__ void __launch_bounds__(WPB2 * 32, 4) element2d_kernel(ElemArgs A) {
             }
         }
 
+        if constexpr (CSR) {
+            if ((DOF || DOK) && active) {  // the scatter's row data and slot map, copied during phase 2
+                if (hl < NN) {
+                    const int64_t pt = A.conn[cell * NN + hl];
+                    int64_t* nm = NM + 4 * hl;
+                    cp_async<8>(nm, A.bptr + pt);
+                    cp_async<8>(nm + 1, A.bptr + pt + 1);
+                    cp_async<4>(nm + 2, A.crank + cell * NN + hl);
+                    cp_async<4>(reinterpret_cast<int32_t*>(nm + 2) + 1, A.cfirst + cell * NN + hl);
+                    nm[3] = pt;
+                }
+                constexpr int CB = NN * NN * 2;
+                const char* src = reinterpret_cast<const char*>(A.cslot + cell * (int64_t)(NN * NN));
+                char* dst = reinterpret_cast<char*>(CSL);
+                if (hl < LPC) {
+                    if constexpr (CB % 16 == 0) {
+                        for (int k = hl; k < CB / 16; k += LPC) cp_async<16>(dst + 16 * k, src + 16 * k);
+                    } else if constexpr (CB % 8 == 0) {
+                        for (int k = hl; k < CB / 8; k += LPC) cp_async<8>(dst + 8 * k, src + 8 * k);
+                    } else {  // a map whose cell offset is not 4-byte aligned (Tri3, Qua9): plain loads
+                        for (int k = hl; k < NN * NN; k += LPC) CSL[k] = A.cslot[cell * (int64_t)(NN * NN) + k];
+                    }
+                }
+            }
+        }
         // ---------------- phase 2: lane owns a tile of node-pair blocks ----------------
         double acc[T][T][2][2];
         if (DOK) {
@@ -1403,16 +1503,24 @@ __global__ void __launch_bounds__(WPB2 * 32, 4) element2d_kernel(ElemArgs A) {
         // added by the lower one first (its rank is lower).  Slots without a cell add nothing.
         if constexpr (CSR) {
             if (DOF || DOK) {
+                cp_async_wait_all();
+                __syncwarp();  // every lane's copies are visible
+                // release the rows the slot's previous cell left pending before anything can wait here
+                if (hl < NN && PEND[2 * hl] >= 0) {
+                    ticket_store(A.ticket + PEND[2 * hl], (int)PEND[2 * hl + 1]);
+                    PEND[2 * hl] = -1;
+                }
                 const int sb = LPC * hh;  // first lane of this slot
                 int64_t rowA = 0, pos_m = 0;
                 int rs_m = 0, rank_m = 0;
                 bool last_m = false, todo = false;
                 if (active && hl < NN) {
-                    rowA = A.conn[cell * NN + hl];
-                    const int64_t r0 = __ldg(A.bptr + rowA), r1 = __ldg(A.bptr + rowA + 1);
+                    const int64_t* nm = NM + 4 * hl;
+                    rowA = nm[3];
+                    const int64_t r0 = nm[0], r1 = nm[1];
                     pos_m = 4 * r0;
                     rs_m = 2 * (int)(r1 - r0);
-                    const int32_t cr = __ldg(A.crank + cell * NN + hl);
+                    const int32_t cr = reinterpret_cast<const int32_t*>(nm + 2)[0];
                     rank_m = cr & CRANK_MASK;
                     last_m = (cr & CRANK_LAST) != 0;
                     todo = true;
@@ -1426,12 +1534,13 @@ __global__ void __launch_bounds__(WPB2 * 32, 4) element2d_kernel(ElemArgs A) {
                     const int src = sb + min(a0 + r, NN - 1);
                     posR[r] = __shfl_sync(FULL, pos_m, src);
                     rsR[r] = __shfl_sync(FULL, rs_m, src);
-                    fR[r] = (active && ti >= 0) ? __ldg(A.cfirst + cell * NN + min(a0 + r, NN - 1)) : 0u;
+                    fR[r] = (active && ti >= 0) ? reinterpret_cast<const uint32_t*>(NM + 4 * min(a0 + r, NN - 1) + 2)[1]
+                                                : 0u;
                     const int srcc = sb + min(b0 + r, NN - 1);
                     posC[r] = __shfl_sync(FULL, pos_m, srcc);
                     rsC[r] = __shfl_sync(FULL, rs_m, srcc);
                 }
-                const int16_t* cs_cell = A.cslot + cell * (int64_t)(NN * NN);
+                const int16_t* cs_cell = CSL;
                 int spins = 0;
                 while (true) {
                     const unsigned todo_mask = __ballot_sync(FULL, todo);
@@ -1477,12 +1586,24 @@ __global__ void __launch_bounds__(WPB2 * 32, 4) element2d_kernel(ElemArgs A) {
                             }
                     }
                     __syncwarp();  // every lane's writes precede the node lanes' (cumulative) release stores
-                    if (ready) ticket_store(A.ticket + rowA, last_m ? 0 : rank_m + 1);
+                    // the last round's rows are released at the slot's next scatter (or the exit)
+                    const bool final = rmask == todo_mask;
+                    if (ready) {
+                        if (final) {
+                            PEND[2 * hl] = rowA;
+                            PEND[2 * hl + 1] = last_m ? 0 : rank_m + 1;
+                        } else {
+                            ticket_store(A.ticket + rowA, last_m ? 0 : rank_m + 1);
+                        }
+                    }
                     todo = todo && !ready;
                 }
             }
         }
     }  // pairs
+    if constexpr (CSR) {  // the last cells' pending releases
+        if (hl < NN && PEND[2 * hl] >= 0) ticket_store(A.ticket + PEND[2 * hl], (int)PEND[2 * hl + 1]);
+    }
 }
 
 // One warp per G = 32/NN consecutive block rows of K (a work-queue range may cut the run); group g
