@@ -1891,6 +1891,15 @@ int grid_1d(int64_t n) {
     return (int)std::max<int64_t>(b, 1);
 }
 
+// Lets a kernel take up to the device's opt-in shared memory per block (each launch still asks for
+// its own size, from which the residency is computed).
+void allow_dynamic_smem(const void* kern) {
+    int dev = 0, optin = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
+}
+
 // Blocks of a kernel that the GPU holds at once (one wave of the persistent element kernel).
 int64_t resident_blocks(const void* kern, int smem, int threads = WPB * 32) {
     int dev = 0, sms = 0, per_sm = 0;
@@ -1939,11 +1948,7 @@ void launch_elem_t(pms_elements* h, const ElemArgs& a) {
         }
     }
     auto kern = element_kernel<ND, NN, UPD, DOF, DOK, CSR>;
-    static thread_local bool configured = false;
-    if (!configured) {
-        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
-        configured = true;
-    }
+    allow_dynamic_smem((const void*)kern);
     int64_t blocks = (a.ncell + cells_per_block(NN) - 1) / cells_per_block(NN);
     blocks = std::min<int64_t>(blocks, resident_blocks((const void*)kern, h->smem_bytes));
     if (CSR) cudaMemsetAsync(a.next, 0, sizeof(unsigned long long), h->stream);
@@ -2755,7 +2760,7 @@ ElemLaunchShape mode_shape(pms_elements* h, const ElemArgs& a) {
         }
     }
     auto kern = element_kernel<ND, NN, UPD_MODE, true, true, true>;
-    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
+    allow_dynamic_smem((const void*)kern);
     int64_t blocks = (a.ncell + cells_per_block(NN) - 1) / cells_per_block(NN);
     blocks = std::min<int64_t>(blocks, resident_blocks((const void*)kern, h->smem_bytes));
     ElemLaunchShape r;
@@ -2881,7 +2886,7 @@ void noalloc_launch_t(const ElemArgs& a, int smem, cudaStream_t st) {
         }
     }
     auto kern = element_kernel<ND, NN, UPD_NONE, DOF, DOK, false>;
-    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
+    allow_dynamic_smem((const void*)kern);
     kern<<<(unsigned)((a.ncell + cells_per_block(NN) - 1) / cells_per_block(NN)), WPB * 32, smem, st>>>(a);
 }
 
