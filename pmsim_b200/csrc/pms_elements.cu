@@ -256,10 +256,9 @@ template <int NN> struct TileShape {
 
 // Shared memory (doubles): block-wide dN table [m][j][32] + w[32] (+ N table [m][32] in 2D), then per cell
 // X[NN*ND], dU[NN*ND], G[ng][NN*ND+1] (gradients), TC[ng][10] (alpha, gamma, beta, S), CS[ng][6],
-// V: per node at the current IP.  3D: V[2][NN][9] = kappa g, beta h, h (plastic points of pass B,
-// double-buffered).  2D: V[WPC][NN][VS] = alpha g, gamma g^, beta h, g, h, g^, 2 (a/2)|J|w r q and
-// q, with h = S g (+ q s_zz e_x), g^ = g (+ q e_x) and q = N/r in the axisymmetric idealization
-// (double-buffered when two warps share the cell).
+// V (2D cells of this kernel only): per node at the current IP, V[WPC][NN][VS] = alpha g, gamma g^,
+// beta h, g, h, g^, 2 (a/2)|J|w r q and q, with h = S g (+ q s_zz e_x), g^ = g (+ q e_x) and q = N/r in
+// the axisymmetric idealization (double-buffered when two warps share the cell).
 __host__ __device__ constexpr int node_vec_doubles(int nd) { return 5 * nd + (nd == 2 ? 4 : 0); }
 __host__ __device__ constexpr int smem_table_doubles(int nn, int nd) {
     return nn * nd * 32 + 32 + (nd == 2 ? nn * 32 : 0);
@@ -270,7 +269,7 @@ __host__ __device__ constexpr int smem_table_doubles(int nn, int nd) {
 __host__ __device__ constexpr int meta_doubles(int nn) { return 4 * nn + 2 * nn + 2 * ((nn * nn + 7) / 8); }
 __host__ __device__ constexpr int smem_cell_doubles(int nn, int nd, int ng) {
     return meta_doubles(nn) + 2 * nn * nd + ng * (nn * nd + 1) + ng * 10 + ng * 6 +
-           (nd == 3 ? 2 * nn * 9 : warps_per_cell(nn) * nn * node_vec_doubles(nd)) + (ng & 1);
+           (nd == 3 ? 0 : warps_per_cell(nn) * nn * node_vec_doubles(nd)) + (ng & 1);
 }
 __host__ __device__ constexpr int smem_bytes_for(int nn, int nd, int ng, int wpb) {
     return (smem_table_doubles(nn, nd) + (wpb / warps_per_cell(nn)) * smem_cell_doubles(nn, nd, ng)) * 8;
@@ -345,19 +344,8 @@ element_kernel(ElemArgs A) {
     const MatConst mc = A.mats[A.cmat ? A.cmat[cell] : 0];
 
     if (half == 0) {  // warp 0 of the cell: node data, integration points, F_int
-    if (lane < NN) {
-        const int pt = A.conn[cell * NN + lane];
-#pragma unroll
-        for (int i = 0; i < ND; i++) {
-            Xs[lane * ND + i] = A.coords[(int64_t)pt * ND + i];
-            Us[lane * ND + i] = do_update ? A.ddu[(int64_t)pt * ND + i] : 0.0;
-        }
-    }
-    __syncwarp();
-
-    // ---------------- phase 1: lane p owns integration point p ----------------
+    // the IP state is loaded first, so that its latency overlaps the node staging below
     const int64_t ip0 = cell * ng;
-    int err = OK, err_t = OK;  // stress-update (and geometry) error, tangent error
     const bool has_ip = lane < ng;
     double sig[NC], z = 0.0, lam = 0.0;
     int el = 1;
@@ -373,6 +361,20 @@ element_kernel(ElemArgs A) {
         z = zsrc[ip0 + lane];
         lam = lsrc[ip0 + lane];
         el = esrc[ip0 + lane];
+    }
+    if (lane < NN) {
+        const int pt = A.conn[cell * NN + lane];
+#pragma unroll
+        for (int i = 0; i < ND; i++) {
+            Xs[lane * ND + i] = A.coords[(int64_t)pt * ND + i];
+            Us[lane * ND + i] = do_update ? A.ddu[(int64_t)pt * ND + i] : 0.0;
+        }
+    }
+    __syncwarp();
+
+    // ---------------- phase 1: lane p owns integration point p ----------------
+    int err = OK, err_t = OK;  // stress-update (and geometry) error, tangent error
+    if (has_ip) {
         if (UPD == UPD_MODE && mode == 1) {
             // reset_algorithmic_variables + backup_secondary_values of a new load step
             lam = 0.0;
@@ -629,17 +631,14 @@ element_kernel(ElemArgs A) {
                         }
                 }
         }
-        // pass B, plastic points only: the node lanes stage kappa g, beta h and h = S g of their
-        // node (two buffers, one warp barrier per point)
-        int npl = 0;
-        for (int p = 0; p < ng; p++) {
-            const double* t = TC + p * 10;
-            const double be = t[2];
-            if (be == 0.0) continue;  // elastic point: same value on every lane, uniform branch
-            double* V = V0 + (npl & 1) * NN * 9;
-            npl++;
-            const double* g = G + p * GS;
-            if (lane < NN) {
+        // pass B, plastic points only: every lane forms kappa g, beta h and h = S g of its own row and
+        // column nodes (the same operations the node would stage), so the points need no staging and
+        // no barrier and follow each other without a wait
+        if (ti >= 0) {
+            for (int p = 0; p < ng; p++) {
+                const double* t = TC + p * 10;
+                const double be = t[2];
+                if (be == 0.0) continue;  // elastic point: same value on every lane, uniform branch
                 const double kap = t[1] - cvol * t[0];
                 double S[3][3];
                 S[0][0] = t[3];
@@ -648,50 +647,43 @@ element_kernel(ElemArgs A) {
                 S[0][1] = S[1][0] = t[5];
                 S[1][2] = S[2][1] = t[7];
                 S[0][2] = S[2][0] = t[8];
-                double gv[3];
+                const double* g = G + p * GS;
+                double kr[RT][3], hr[RT][3];
 #pragma unroll
-                for (int i = 0; i < 3; i++) gv[i] = g[lane * 3 + i];
-                double* v = V + lane * 9;
+                for (int r = 0; r < RT; r++) {
+                    const double* ga = g + min(a0 + r, NN - 1) * 3;
+                    const double gv[3] = {ga[0], ga[1], ga[2]};
 #pragma unroll
-                for (int i = 0; i < 3; i++) {
-                    double h = 0.0;
+                    for (int i = 0; i < 3; i++) {
+                        double h = 0.0;
 #pragma unroll
-                    for (int j = 0; j < 3; j++) h = fma(S[i][j], gv[j], h);
-                    v[i] = kap * gv[i];
-                    v[3 + i] = be * h;
-                    v[6 + i] = h;
-                }
-            }
-            __syncwarp();
-            if (ti < 0) continue;
-            double kr[RT][3], hr[RT][3];
-#pragma unroll
-            for (int r = 0; r < RT; r++) {
-                const double* v = V + min(a0 + r, NN - 1) * 9;
-#pragma unroll
-                for (int i = 0; i < 3; i++) {
-                    kr[r][i] = v[i];
-                    hr[r][i] = v[3 + i];
-                }
-            }
-#pragma unroll
-            for (int c = 0; c < CT; c++) {
-                const int b = min(b0 + c, NN - 1);
-                double gb[3], hb[3];
-#pragma unroll
-                for (int j = 0; j < 3; j++) {
-                    gb[j] = g[b * 3 + j];
-                    hb[j] = V[b * 9 + 6 + j];
+                        for (int j = 0; j < 3; j++) h = fma(S[i][j], gv[j], h);
+                        kr[r][i] = kap * gv[i];
+                        hr[r][i] = be * h;
+                    }
                 }
 #pragma unroll
-                for (int r = 0; r < RT; r++)
+                for (int c = 0; c < CT; c++) {
+                    const double* gbp = g + min(b0 + c, NN - 1) * 3;
+                    const double gb[3] = {gbp[0], gbp[1], gbp[2]};
+                    double hb[3];
 #pragma unroll
-                    for (int i = 0; i < 3; i++)
+                    for (int i = 0; i < 3; i++) {
+                        double h = 0.0;
 #pragma unroll
-                        for (int j = 0; j < 3; j++) {
-                            acc[r][c][i][j] = fma(kr[r][i], gb[j], acc[r][c][i][j]);
-                            acc[r][c][i][j] = fma(hr[r][i], hb[j], acc[r][c][i][j]);
-                        }
+                        for (int j = 0; j < 3; j++) h = fma(S[i][j], gb[j], h);
+                        hb[i] = h;
+                    }
+#pragma unroll
+                    for (int r = 0; r < RT; r++)
+#pragma unroll
+                        for (int i = 0; i < 3; i++)
+#pragma unroll
+                            for (int j = 0; j < 3; j++) {
+                                acc[r][c][i][j] = fma(kr[r][i], gb[j], acc[r][c][i][j]);
+                                acc[r][c][i][j] = fma(hr[r][i], hb[j], acc[r][c][i][j]);
+                            }
+                }
             }
         }
         } else {
@@ -1117,19 +1109,8 @@ __global__ void __launch_bounds__(WPB2 * 32, 4) element2d_kernel(ElemArgs A) {
         const bool from_backup = (UPD == UPD_BACKUP) || (UPD == UPD_MODE && mode == 2);
         const MatConst mc = A.mats[A.cmat ? A.cmat[cell] : 0];
 
-        if (hl < NN) {
-            const int pt = A.conn[cell * NN + hl];
-#pragma unroll
-            for (int i = 0; i < 2; i++) {
-                Xs[hl * 2 + i] = A.coords[(int64_t)pt * 2 + i];
-                Us[hl * 2 + i] = do_update ? A.ddu[(int64_t)pt * 2 + i] : 0.0;
-            }
-        }
-        __syncwarp();
-
-        // ---------------- phase 1: lane p of the half owns integration point p ----------------
+        // the IP state first, so that its latency overlaps the node staging
         const int64_t ip0 = cell * ng;
-        int err = OK, err_t = OK;  // stress-update (and geometry) error, tangent error
         const bool has_ip = hl < ng;
         double sig[4], z = 0.0, lam = 0.0;
         int el = 1;
@@ -1145,6 +1126,20 @@ __global__ void __launch_bounds__(WPB2 * 32, 4) element2d_kernel(ElemArgs A) {
             z = zsrc[ip0 + hl];
             lam = lsrc[ip0 + hl];
             el = esrc[ip0 + hl];
+        }
+        if (hl < NN) {
+            const int pt = A.conn[cell * NN + hl];
+#pragma unroll
+            for (int i = 0; i < 2; i++) {
+                Xs[hl * 2 + i] = A.coords[(int64_t)pt * 2 + i];
+                Us[hl * 2 + i] = do_update ? A.ddu[(int64_t)pt * 2 + i] : 0.0;
+            }
+        }
+        __syncwarp();
+
+        // ---------------- phase 1: lane p of the half owns integration point p ----------------
+        int err = OK, err_t = OK;  // stress-update (and geometry) error, tangent error
+        if (has_ip) {
             if (UPD == UPD_MODE && mode == 1) {
                 // reset_algorithmic_variables + backup_secondary_values of a new load step
                 lam = 0.0;

@@ -178,3 +178,23 @@ def test_failing_problems_stop_alone_and_leave_the_others_bits():
             assert a.history[i] == b.history[j]
         a.close()
         b.close()
+
+
+def test_population_sample_fails_where_the_oracle_driver_fails():
+    """A seeded sample of 32 footings from the batched configuration's population (512, seed 2024),
+    solved together by the batched device solver as the benchmark runs it (independent progress,
+    failing problems dropped): each problem it stops is stopped by the oracle driver (direct solve)
+    at the same load step with the same message, and each problem it converges the oracle
+    converges too."""
+    from pmsim_b200.batch import BatchSolver
+    from pmsim_b200.footing import population
+    probs = population(512, seed=2024)
+    rng = np.random.default_rng(11)
+    sample = sorted(rng.choice(512, size=32, replace=False).tolist())
+    bs = BatchSolver([probs[i] for i in sample], n_max_iterations=20, pcg_max_iterations=5000)
+    bs.solve_independent(on_fail="drop")
+    for k, i in enumerate(sample):
+        ref = _oracle_failure(probs[i])
+        assert bs.failed.get(k) == ref, (i, probs[i].name, bs.failed.get(k), ref)
+    assert bs.failed, "the sample holds failing problems"
+    bs.close()
