@@ -108,9 +108,10 @@ def flops_per_ip_hex20(plastic):
     return 2 * fma + other
 
 
-# DRAM bytes (read + write) per cell of one launch of the direct-assembly element kernel
-# element_kernel<3,20,...,CSR> from an ncu capture of a smaller block (traffic grows with the cell
-# count, so a launch over n cells moves n times this); None until that capture exists.
+# DRAM bytes (read + write) per cell of one launch of the element kernel element_kernel<3,20,...>
+# (gather assembly: upper element-matrix blocks out) from an ncu capture of a smaller block (traffic
+# grows with the cell count, so a launch over n cells moves n times this); None until that capture
+# exists for the current kernel.
 ELEMENT_DRAM_BYTES_PER_CELL = None
 
 
@@ -320,8 +321,8 @@ def run_qua8_step(torch, stream, steps, warmup, hbm_peak, n=1024):
     """The fused Newton iteration on a large 2D mesh, where it is memory-bound: n x n Qua8 cells
     (9 IP) of the footing material (E=1e4, nu=0.3, z0=9, H=0) under a seeded smooth increment that
     leaves a mix of elastic and plastic IPs.  Reports the step's algorithmic bytes per second
-    against the measured HBM peak (one kernel: the blocks go straight into the CSR values), and the
-    same step with the gather assembly for comparison."""
+    against the measured HBM peak, with the default (gather) assembly, and the same step with the
+    direct assembly for comparison."""
     from pmsim_b200 import _lib
     from pmsim_b200 import mesh as M
     from pmsim_b200.elements import Elements, Material
@@ -346,6 +347,14 @@ def run_qua8_step(torch, stream, steps, warmup, hbm_peak, n=1024):
     el.sync()
     plastic = float(1.0 - el.get_state()[2].mean())
     ms = time_steps(torch, el, stream, steps, d_ddu, d_ff, d_csr)
+    L.pms_elements_set_timing(el.h, 1)
+    L.pms_elements_kernel_times(el.h, None, None)
+    for _ in range(steps):
+        el.update_and_assemble(d_ddu, d_ff, d_csr)
+    kt = np.zeros(3)
+    kc = np.zeros(3, np.int64)
+    L.pms_elements_kernel_times(el.h, _lib.ptr(kt), _lib.ptr(kc))
+    L.pms_elements_set_timing(el.h, 0)
     ab = assembly_ab(torch, L, el, stream, steps, warmup, d_ddu, d_ff, d_csr)
     ng, nip = 9, m.ncell * 9
     # the fused step's algorithmic bytes in 2D: coordinates, connectivity, dU, IP state read (sigma 4 +
@@ -357,7 +366,9 @@ def run_qua8_step(torch, stream, steps, warmup, hbm_peak, n=1024):
     gbs_step = step_bytes / (ms * 1e-3) / 1e9
     return {"workload": f"qua8 {n}x{n} footing material, 9 IP, one fused Newton iteration", "ncell": m.ncell,
             "nip": nip, "nnz": int(el.nnz), "plastic_fraction": plastic, "ms_per_step": ms,
-            "kernel": "element2d_kernel<8,10,UPD_BACKUP,F,K,CSR> (update + F_int + K added straight into CSR and R)",
+            "kernels": "element2d_kernel<8,10,UPD_BACKUP,F,K> (update + F_int + upper K_e blocks), f_gather, "
+                       "kk_gather<2,8> (rows summed in ascending cell order)",
+            "kernels_ms_per_step": kernel_ms(kt, kc),
             "assembly_ab": ab,
             "step_roofline": {"bound": "hbm", "achieved": gbs_step, "peak": hbm_peak, "unit": "GB/s",
                               "frac": gbs_step / hbm_peak, "algorithmic_bytes_per_step": step_bytes}}
@@ -374,15 +385,16 @@ def time_steps(torch, el, stream, steps, d_ddu, d_ff, d_csr):
     return e0.elapsed_time(e1) / steps
 
 
-def assembly_ab(torch, L, el, stream, steps, warmup, d_ddu, d_ff, d_csr):
-    """The same step with the gather assembly (dense element matrices, then row gathers; the same
-    bits), timed per kernel, beside the direct assembly's step: the gain of adding the blocks
-    straight into the CSR values."""
+def assembly_ab(torch, L, el, stream, steps, warmup, d_ddu, d_ff, d_csr, other="direct", default="gather"):
+    """The same step with the other assembly, timed per kernel, beside the default's step.  Gather:
+    the element kernel writes each cell's upper element-matrix blocks, row gathers sum them in
+    ascending cell order.  Direct: the element kernel adds the blocks straight into the CSR values
+    (ordered, no element matrices).  Both sum every entry in a fixed order."""
     from pmsim_b200 import _lib
-    el.set_assembly("gather")
+    el.set_assembly(other)
     for _ in range(max(2, warmup)):
         el.update_and_assemble(d_ddu, d_ff, d_csr)
-    ms_g = time_steps(torch, el, stream, steps, d_ddu, d_ff, d_csr)
+    ms_o = time_steps(torch, el, stream, steps, d_ddu, d_ff, d_csr)
     L.pms_elements_set_timing(el.h, 1)
     L.pms_elements_kernel_times(el.h, None, None)
     for _ in range(steps):
@@ -391,13 +403,21 @@ def assembly_ab(torch, L, el, stream, steps, warmup, d_ddu, d_ff, d_csr):
     kc = np.zeros(3, np.int64)
     L.pms_elements_kernel_times(el.h, _lib.ptr(kt), _lib.ptr(kc))
     L.pms_elements_set_timing(el.h, 0)
-    el.set_assembly("direct")
+    el.set_assembly(default)
     el.update_and_assemble(d_ddu, d_ff, d_csr)
     el.sync()
-    return {"gather_ms_per_step": ms_g,
-            "gather_kernels_ms_per_step": {"element_dense": kt[0] / max(kc[0], 1), "f_gather": kt[1] / max(kc[1], 1),
-                                           "kk_gather": kt[2] / max(kc[2], 1)},
-            "note": "gather assembly: element kernel writes dense K_e/F_e, row gathers sum them (same bits)"}
+    return {"default": default, "other": other, "other_ms_per_step": ms_o,
+            "other_kernels_ms_per_step": kernel_ms(kt, kc)}
+
+
+def kernel_ms(kt, kc):
+    """Per-step times of the element kernel and the two gathers (absent under the direct assembly)."""
+    out = {"element": kt[0] / max(kc[0], 1)}
+    if kc[1]:
+        out["f_gather"] = kt[1] / kc[1]
+    if kc[2]:
+        out["kk_gather"] = kt[2] / kc[2]
+    return out
 
 
 def run_batched(nprob, nalone, seed=2024):
@@ -860,7 +880,7 @@ def main():
         gpu_csr = d_csr.cpu().numpy()
         el_pattern = el.csr_pattern()
 
-    # the same step with the gather assembly (same bits), for the A/B of the direct assembly
+    # the same step with the direct assembly, for the A/B of the two assemblies
     ab = assembly_ab(torch, L, el, stream, min(args.steps, 10), args.warmup, d_ddu, d_ff, d_csr)
 
     # e2e through the C ABI with host buffers (pinned): dU in, R and CSR values out, every step
@@ -918,7 +938,7 @@ def main():
     if args.served > 0 and args.size == "full":
         torch.cuda.empty_cache()
         served = run_served(args.served, args.rate, min(args.alone_sample, 16), detail_file=args.served_detail)
-    ms_elem = kt[0] / max(kc[0], 1)  # the element kernel is the whole step (direct assembly)
+    ms_elem = kt[0] / max(kc[0], 1)  # the element kernel (the gathers are memory-bound, separate kernels)
     fl_ip = flops_per_ip_hex20(plastic)
     achieved_tf = nip * fl_ip / (ms_elem * 1e-3) / 1e12
     alg_bytes = algorithmic_bytes_step(m, ng, nnz)
@@ -957,13 +977,13 @@ def main():
                      "traffic": ELEMENT_DRAM_BYTES_PER_CELL * m.ncell if ELEMENT_DRAM_BYTES_PER_CELL else None,
                      "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch on a "
                                        "smaller block, scaled by cells to this launch",
-                     "kernel": "element_kernel<3,20,UPD_BACKUP,F,K,CSR> (fused update + B^T sigma + B^T D B, "
-                               "blocks added straight into the CSR values and R)",
+                     "kernel": "element_kernel<3,20,UPD_BACKUP,F,K> (fused update + B^T sigma + B^T D B, "
+                               "upper element-matrix blocks out)",
                      "flop_per_ip": fl_ip, "peak_source": "FP64 FMA probe measured in this run"},
         "roofline_hbm": {"bound": "hbm", "achieved": step_gbs, "peak": peaks["hbm_gbs"], "unit": "GB/s",
                          "frac": step_gbs / peaks["hbm_gbs"], "algorithmic_bytes_per_step": alg_bytes,
                          "peak_source": peaks_kind},
-        "kernels_ms_per_step": {"element": ms_elem},
+        "kernels_ms_per_step": kernel_ms(kt, kc),
         "assembly_ab": ab,
         "gpu_launches": int(launches),
         "e2e": e2e, "cpu_baseline": cpu, "parity": parity, "k1_microbench": k1, "ep_microbench": ep, "qua8_step": qua8, "batched": batched, "served": served, "c0_footing": c0, "fp64_peak_tflops": fp64, "fp64_peak_clocks": fp64_clocks,

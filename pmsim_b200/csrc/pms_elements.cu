@@ -89,6 +89,9 @@ struct ElemArgs {
     const int64_t* q_first = nullptr;
     // dense outputs (no CSR): the fe / ke rows of cell c are c - ke_cell0
     int64_t ke_cell0 = 0;
+    // ke layout: 0 = full row-major NE x NE (per-cell calls); 1 = the upper node-pair blocks (a <= b),
+    // block-major, NN(NN+1)/2 blocks of ND x ND row-major (the gather assembly)
+    int ke_upper = 0;
     // direct assembly (CSR kernels): cell c adds its node-row slab a into block row A = conn[c][a]
     // and its F_int share into R once ticket[A] equals c's rank among A's cells (crank), then
     // advances the ticket; cells are taken in ascending order from the counter `next`
@@ -133,6 +136,9 @@ __device__ __forceinline__ int64_t dequeue(unsigned long long* next) {
 // issuing lane does not wait.  The row tickets order the adds of successive cells (each cell's
 // adds come after the release store that the next cell acquires), so every entry is still summed
 // in ascending cell order.
+// Position of node-pair block (a, b), a <= b, in the upper block-major layout of an element matrix.
+__host__ __device__ constexpr int upper_block(int nn, int a, int b) { return a * nn - a * (a - 1) / 2 + (b - a); }
+
 // Asynchronous global -> shared copies (no register passes through; cp.async.wait_all, then a warp
 // barrier, before the data is read).  Sizes 4, 8 and 16 bytes, both addresses aligned to the size.
 template <int B>
@@ -805,6 +811,37 @@ element_kernel(ElemArgs A) {
         // each lane drops its blocks (a, b) and mirrors (b, a) into the staged rows, then the warp
         // copies the rows out with contiguous stores
         if constexpr (!CSR) {
+        if (A.ke_upper) {
+            // upper blocks only, block-major: node rows [r0, r0 + RS) hold blocks [u(r0, r0), u(r0 + RS, .))
+            constexpr int NU = NN * (NN + 1) / 2, BB = ND * ND;
+            const int RS = max(1, min(NN, smem_cell_doubles(NN, ND, ng) / (NN * BB)));
+            double* stage = wbase;
+            double* kc = A.ke + (cell - A.ke_cell0) * (int64_t)(NU * BB);
+            for (int r0 = 0; r0 < NN; r0 += RS) {
+                const int r1 = min(NN, r0 + RS);
+                const int u0 = upper_block(NN, r0, r0), u1 = (r1 < NN) ? upper_block(NN, r1, r1) : NU;
+                cell_sync();
+                if (ti >= 0) {
+#pragma unroll
+                    for (int r = 0; r < RT; r++)
+#pragma unroll
+                        for (int c = 0; c < CT; c++) {
+                            const int a = a0 + r, b = b0 + c;
+                            if (a < NN && b < NN && a <= b && a >= r0 && a < r1) {
+                                double* st = stage + (upper_block(NN, a, b) - u0) * BB;
+#pragma unroll
+                                for (int i = 0; i < ND; i++)
+#pragma unroll
+                                    for (int j = 0; j < ND; j++) st[i * ND + j] = acc[r][c][i][j];
+                            }
+                        }
+                }
+                cell_sync();
+                const int n = (u1 - u0) * BB;
+                double* dst = kc + (int64_t)u0 * BB;
+                for (int t = lane + 32 * half; t < n; t += 32 * WPC) dst[t] = stage[t];
+            }
+        } else {
         const int RS = min(NN, smem_cell_doubles(NN, ND, ng) / (ND * NE));
         double* stage = wbase;
         double* kc = A.ke + (cell - A.ke_cell0) * (int64_t)(NE * NE);
@@ -839,6 +876,7 @@ element_kernel(ElemArgs A) {
             double* dst = kc + (int64_t)r0 * ND * NE;
             for (int t = lane + 32 * half; t < n; t += 32 * WPC) dst[t] = stage[t];
         }
+        }  // full layout
         }  // dense output
     }
     // ---------------- direct assembly: ordered scatter into the CSR values and R ----------------
@@ -1466,6 +1504,8 @@ __global__ void __launch_bounds__(WPB2 * 32, 4) element2d_kernel(ElemArgs A) {
             // stage K_e row-major in the cell area (blocks (a, b) and their mirrors (b, a)), then
             // copy it out with 16-byte stores, LPC*16 contiguous bytes per cell and store
             double* stage = Xs;
+            constexpr int NU = NN * (NN + 1) / 2;  // upper layout: blocks (a <= b), block-major, 2x2 each
+            const bool up = A.ke_upper != 0;
             if (ti >= 0) {
 #pragma unroll
                 for (int r = 0; r < T; r++)
@@ -1473,21 +1513,30 @@ __global__ void __launch_bounds__(WPB2 * 32, 4) element2d_kernel(ElemArgs A) {
                     for (int c = 0; c < T; c++) {
                         const int a = a0 + r, b = b0 + c;
                         if (a < NN && b < NN && a <= b) {
+                            if (up) {
+                                double* st = stage + 4 * upper_block(NN, a, b);
 #pragma unroll
-                            for (int i = 0; i < 2; i++)
+                                for (int i = 0; i < 2; i++)
 #pragma unroll
-                                for (int j = 0; j < 2; j++) {
-                                    stage[(a * 2 + i) * NE + b * 2 + j] = acc[r][c][i][j];
-                                    if (a != b) stage[(b * 2 + j) * NE + a * 2 + i] = acc[r][c][i][j];
-                                }
+                                    for (int j = 0; j < 2; j++) st[i * 2 + j] = acc[r][c][i][j];
+                            } else {
+#pragma unroll
+                                for (int i = 0; i < 2; i++)
+#pragma unroll
+                                    for (int j = 0; j < 2; j++) {
+                                        stage[(a * 2 + i) * NE + b * 2 + j] = acc[r][c][i][j];
+                                        if (a != b) stage[(b * 2 + j) * NE + a * 2 + i] = acc[r][c][i][j];
+                                    }
+                            }
                         }
                     }
             }
             __syncwarp();
             if (active && hl < LPC) {
-                double2* dst = reinterpret_cast<double2*>(A.ke + (cell - A.ke_cell0) * (int64_t)(NE * NE));
+                const int nd2 = up ? 2 * NU : NE * NE / 2;  // double2 per cell
+                double2* dst = reinterpret_cast<double2*>(A.ke + (cell - A.ke_cell0) * (int64_t)(2 * nd2));
                 const double2* s2 = reinterpret_cast<const double2*>(stage);
-                for (int t = hl; t < NE * NE / 2; t += LPC) dst[t] = s2[t];
+                for (int t = hl; t < nd2; t += LPC) dst[t] = s2[t];
             }
             }  // dense output
         }
@@ -1603,8 +1652,10 @@ __global__ void __launch_bounds__(WPB2 * 32, 4) element2d_kernel(ElemArgs A) {
 
 // One warp per G = 32/NN consecutive block rows of K (a work-queue range may cut the run); group g
 // of NN lanes owns row A_g.  Lane b of the group loads, for each incidence k of A_g (cell c, local
-// index a), the ND x ND block (a, b) of c's dense element matrix -- the NN lanes read one contiguous
-// node-row slab -- and adds it at column slot[k*NN + b] of the row's buffer in shared memory.  Up
+// index a), the ND x ND block (a, b) of c's element matrix -- kept as its upper blocks, block-major,
+// so lane b reads block (a, b) when a <= b (the lanes b >= a read one contiguous run) and the
+// transpose of block (b, a) otherwise -- and adds it at column slot[k*NN + b] of the row's buffer
+// in shared memory.  Up
 // to NB incidences are loaded before they are added; the adds go in ascending incidence (= cell)
 // order with a group barrier between incidences, so every entry of K is the fixed-order sum over
 // its cells: bit-identical on every run.  The G buffers lie back to back in CSR order, so when the
@@ -1625,7 +1676,7 @@ __global__ void __launch_bounds__(256, ND == 2 ? 4 : 1) kk_gather_kernel(int64_t
                                                         const uint8_t* __restrict__ pmode, int nq,
                                                         const int64_t* __restrict__ q_off,
                                                         const int64_t* __restrict__ q_first, int64_t node0) {
-    constexpr int NE = NN * ND, BB = ND * ND;
+    constexpr int BB = ND * ND, NU = NN * (NN + 1) / 2;
     constexpr int G = GatherShape<ND, NN>::G, NB = GatherShape<ND, NN>::NB;
     extern __shared__ double rowbuf[];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, wpb = blockDim.x >> 5;
@@ -1679,11 +1730,13 @@ __global__ void __launch_bounds__(256, ND == 2 ? 4 : 1) kk_gather_kernel(int64_t
                         const int64_t cell = code / NN;
                         const int a = code - (int)cell * NN;
                         pos[r] = __ldg(slot + k * NN + b);
-                        const double* src = ke + (cell * NE + a * ND) * NE + b * ND;
+                        // block (a, b) of the upper layout: stored as (a, b) when a <= b, else as (b, a)
+                        const bool upper = a <= b;
+                        const double* src = ke + (cell * NU + upper_block(NN, upper ? a : b, upper ? b : a)) * BB;
 #pragma unroll
                         for (int i = 0; i < ND; i++)
 #pragma unroll
-                            for (int j = 0; j < ND; j++) v[r][i * ND + j] = __ldg(src + i * NE + j);
+                            for (int j = 0; j < ND; j++) v[r][i * ND + j] = __ldg(src + (upper ? i * ND + j : j * ND + i));
                     } else {
 #pragma unroll
                         for (int i = 0; i < BB; i++) v[r][i] = 0.0;
@@ -1792,7 +1845,7 @@ struct pms_elements {
     int32_t* d_order = nullptr;    // direct assembly: processing order of the cells
     int32_t* d_ticket = nullptr;   // direct assembly: per-node tickets (zero between launches)
     unsigned long long* d_next = nullptr;  // direct assembly: in-order work counter
-    int assembly = PMS_ASSEMBLY_DIRECT;
+    int assembly = PMS_ASSEMBLY_GATHER;  // measured faster on B200 for every kind benchmarked
     int64_t* d_inc_ptr = nullptr;
     int32_t* d_inc = nullptr;
     int64_t* d_bptr = nullptr;
@@ -2041,6 +2094,7 @@ ElemArgs make_args(pms_elements* h, const double* ddu) {
     a.el = h->d_el;
     a.fe = h->d_fe;
     a.ke = h->d_ke;
+    a.ke_upper = 1;  // the gather assembly reads the upper blocks
     a.errkey = (unsigned long long*)h->d_status;
     a.bptr = h->d_bptr;
     a.cslot = h->d_cslot;
@@ -2378,7 +2432,8 @@ int pms_elements_sync(pms_elements* h) { return h ? finish_host(h) : PMS_ERR_INV
 static int ensure_gather(pms_elements* h) {
     if (h->d_ke) return PMS_OK;
     const size_t ne = (size_t)h->nn * h->nd;
-    if (!h->alloc(&h->d_fe, (size_t)h->ncell * ne) || !h->alloc(&h->d_ke, (size_t)h->ncell * ne * ne) ||
+    const size_t nupper = (size_t)h->nn * (h->nn + 1) / 2 * h->nd * h->nd;  // upper blocks per cell
+    if (!h->alloc(&h->d_fe, (size_t)h->ncell * ne) || !h->alloc(&h->d_ke, (size_t)h->ncell * nupper) ||
         !h->upload(&h->d_inc, h->pat.inc.data(), h->pat.inc.size()) ||
         !h->upload(&h->d_slot, h->pat.slot.data(), h->pat.slot.size()))
         return fail(h, PMS_ERR_NOMEM, "out of device memory for the gather assembly");
@@ -2496,6 +2551,7 @@ static int one_cell(pms_elements* h, int64_t cell, bool dof, bool dok) {
     a.cell0 = cell;
     a.fe = h->d_fe1;  // dense outputs of this one cell
     a.ke = h->d_ke1;
+    a.ke_upper = 0;  // full matrix for the caller
     a.ke_cell0 = cell;
     launch_elem(h, a, UPD_NONE, dof, dok, false);
     int rc = cuda_check(h);

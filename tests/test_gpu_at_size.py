@@ -49,6 +49,15 @@ def fused_vs_oracle(m, mat_args, ngauss, ddu):
     kv2 = np.zeros(g.nnz)
     g.update_and_assemble(ddu, None, kv2)
     assert np.array_equal(kv, kv2), "CSR values differ between two runs"
+    # the other assembly (direct: blocks added straight into the CSR values) at the same size
+    g.set_assembly("direct")
+    ff3, kv3 = np.zeros(g.ndof), np.zeros(g.nnz)
+    g.update_and_assemble(ddu, ff3, kv3)
+    assert_close(ff3, o.assemble_f_int(), what="f_int (direct)")
+    assert_close(kv3, data, what="K (direct)")
+    kv4 = np.zeros(g.nnz)
+    g.update_and_assemble(ddu, None, kv4)
+    assert np.array_equal(kv3, kv4), "direct CSR values differ between two runs"
     g.close()
 
 

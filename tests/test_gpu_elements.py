@@ -114,11 +114,12 @@ def test_csr_bit_reproducible():
 
 @pytest.mark.parametrize("kind", KINDS, ids=[M.KIND_NAMES[k] for k in KINDS])
 def test_direct_and_gather_assembly_agree(kind):
-    """The direct assembly (blocks added straight into the CSR values and R, row by row in ascending
-    cell order) gives the same bits on every run, and agrees with the gather assembly (dense element
-    matrices, then row gathers in the same order) to 1e-13: the two are different kernel
-    instantiations, which the compiler may contract into fused multiply-adds differently, so only
-    the last bits may differ (a missing or doubled block would differ at O(1))."""
+    """The direct assembly (blocks added straight into the CSR values and R, every entry summed over
+    its cells in the colour-major processing order) gives the same bits on every run, and agrees with
+    the gather assembly (upper element-matrix blocks, then row gathers in ascending cell order) to
+    1e-13: the summation orders differ and the two are different kernel instantiations, which the
+    compiler may contract into fused multiply-adds differently, so only the last bits may differ (a
+    missing or doubled block would differ at O(1))."""
     m, g, o = make(kind, seed=7)
     ddu = plastic_ddu(m, seed=8)
     g.initialize_internal_values()
