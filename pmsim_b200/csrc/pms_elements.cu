@@ -89,8 +89,9 @@ struct ElemArgs {
     const int64_t* q_first = nullptr;
     // dense outputs (no CSR): the fe / ke rows of cell c are c - ke_cell0
     int64_t ke_cell0 = 0;
-    // ke layout: 0 = full row-major NE x NE (per-cell calls); 1 = the upper node-pair blocks (a <= b),
-    // block-major, NN(NN+1)/2 blocks of ND x ND row-major (the gather assembly)
+    // ke layout: 0 = full row-major NE x NE (per-cell calls); 1 = the upper node-pair blocks (a <= b)
+    // only: block row a holds its ND scalar rows one after another, each with the columns of nodes
+    // a..NN-1 (upper_entry), NN(NN+1)/2 ND x ND blocks per cell (the gather assembly)
     int ke_upper = 0;
     // direct assembly (CSR kernels): cell c adds its node-row slab a into block row A = conn[c][a]
     // and its F_int share into R once ticket[A] equals c's rank among A's cells (crank), then
@@ -136,8 +137,14 @@ __device__ __forceinline__ int64_t dequeue(unsigned long long* next) {
 // issuing lane does not wait.  The row tickets order the adds of successive cells (each cell's
 // adds come after the release store that the next cell acquires), so every entry is still summed
 // in ascending cell order.
-// Position of node-pair block (a, b), a <= b, in the upper block-major layout of an element matrix.
+// Number of node-pair blocks (a', b'), a' <= b', in the block rows before row a (upper layout).
 __host__ __device__ constexpr int upper_block(int nn, int a, int b) { return a * nn - a * (a - 1) / 2 + (b - a); }
+// Upper layout of an element matrix: entry (i, j) of block (a, b), a <= b, at
+// BB*upper_block(a, a) + i*(NN - a)*ND + (b - a)*ND + j (block row a, scalar rows one after another).
+template <int NN, int ND>
+__host__ __device__ constexpr int upper_entry(int a, int b, int i, int j) {
+    return ND * ND * upper_block(NN, a, a) + i * (NN - a) * ND + (b - a) * ND + j;
+}
 
 // Asynchronous global -> shared copies (no register passes through; cp.async.wait_all, then a warp
 // barrier, before the data is read).  Sizes 4, 8 and 16 bytes, both addresses aligned to the size.
@@ -812,7 +819,7 @@ element_kernel(ElemArgs A) {
         // copies the rows out with contiguous stores
         if constexpr (!CSR) {
         if (A.ke_upper) {
-            // upper blocks only, block-major: node rows [r0, r0 + RS) hold blocks [u(r0, r0), u(r0 + RS, .))
+            // upper blocks only: block rows [r0, r0 + RS) are the contiguous range [u(r0, r0), u(r0 + RS, .))
             constexpr int NU = NN * (NN + 1) / 2, BB = ND * ND;
             const int RS = max(1, min(NN, smem_cell_doubles(NN, ND, ng) / (NN * BB)));
             double* stage = wbase;
@@ -828,11 +835,11 @@ element_kernel(ElemArgs A) {
                         for (int c = 0; c < CT; c++) {
                             const int a = a0 + r, b = b0 + c;
                             if (a < NN && b < NN && a <= b && a >= r0 && a < r1) {
-                                double* st = stage + (upper_block(NN, a, b) - u0) * BB;
 #pragma unroll
                                 for (int i = 0; i < ND; i++)
 #pragma unroll
-                                    for (int j = 0; j < ND; j++) st[i * ND + j] = acc[r][c][i][j];
+                                    for (int j = 0; j < ND; j++)
+                                        stage[upper_entry<NN, ND>(a, b, i, j) - u0 * BB] = acc[r][c][i][j];
                             }
                         }
                 }
@@ -1504,7 +1511,7 @@ __global__ void __launch_bounds__(WPB2 * 32, 4) element2d_kernel(ElemArgs A) {
             // stage K_e row-major in the cell area (blocks (a, b) and their mirrors (b, a)), then
             // copy it out with 16-byte stores, LPC*16 contiguous bytes per cell and store
             double* stage = Xs;
-            constexpr int NU = NN * (NN + 1) / 2;  // upper layout: blocks (a <= b), block-major, 2x2 each
+            constexpr int NU = NN * (NN + 1) / 2;  // upper layout: blocks (a <= b), 2x2 each
             const bool up = A.ke_upper != 0;
             if (ti >= 0) {
 #pragma unroll
@@ -1514,11 +1521,10 @@ __global__ void __launch_bounds__(WPB2 * 32, 4) element2d_kernel(ElemArgs A) {
                         const int a = a0 + r, b = b0 + c;
                         if (a < NN && b < NN && a <= b) {
                             if (up) {
-                                double* st = stage + 4 * upper_block(NN, a, b);
 #pragma unroll
                                 for (int i = 0; i < 2; i++)
 #pragma unroll
-                                    for (int j = 0; j < 2; j++) st[i * 2 + j] = acc[r][c][i][j];
+                                    for (int j = 0; j < 2; j++) stage[upper_entry<NN, 2>(a, b, i, j)] = acc[r][c][i][j];
                             } else {
 #pragma unroll
                                 for (int i = 0; i < 2; i++)
@@ -1652,10 +1658,10 @@ __global__ void __launch_bounds__(WPB2 * 32, 4) element2d_kernel(ElemArgs A) {
 
 // One warp per G = 32/NN consecutive block rows of K (a work-queue range may cut the run); group g
 // of NN lanes owns row A_g.  Lane b of the group loads, for each incidence k of A_g (cell c, local
-// index a), the ND x ND block (a, b) of c's element matrix -- kept as its upper blocks, block-major,
-// so lane b reads block (a, b) when a <= b (the lanes b >= a read one contiguous run) and the
-// transpose of block (b, a) otherwise -- and adds it at column slot[k*NN + b] of the row's buffer
-// in shared memory.  Up
+// index a), the ND x ND block (a, b) of c's element matrix -- kept as its upper blocks, block row by
+// block row, so lane b reads block (a, b) when a <= b (the lanes b >= a read adjacent segments of
+// the same scalar rows) and the transpose of block (b, a) otherwise -- and adds it at column
+// slot[k*NN + b] of the row's buffer in shared memory.  Up
 // to NB incidences are loaded before they are added; the adds go in ascending incidence (= cell)
 // order with a group barrier between incidences, so every entry of K is the fixed-order sum over
 // its cells: bit-identical on every run.  The G buffers lie back to back in CSR order, so when the
@@ -1730,13 +1736,16 @@ __global__ void __launch_bounds__(256, ND == 2 ? 4 : 1) kk_gather_kernel(int64_t
                         const int64_t cell = code / NN;
                         const int a = code - (int)cell * NN;
                         pos[r] = __ldg(slot + k * NN + b);
-                        // block (a, b) of the upper layout: stored as (a, b) when a <= b, else as (b, a)
+                        // block (a, b) of the upper layout: stored as (a, b) when a <= b, else as (b, a);
+                        // the lanes b >= a read adjacent segments of the same scalar rows
                         const bool upper = a <= b;
-                        const double* src = ke + (cell * NU + upper_block(NN, upper ? a : b, upper ? b : a)) * BB;
+                        const int lo = upper ? a : b, hi = upper ? b : a;
+                        const double* src = ke + cell * (int64_t)(NU * BB) + upper_entry<NN, ND>(lo, hi, 0, 0);
+                        const int rs = (NN - lo) * ND;  // scalar-row stride of block row lo
 #pragma unroll
                         for (int i = 0; i < ND; i++)
 #pragma unroll
-                            for (int j = 0; j < ND; j++) v[r][i * ND + j] = __ldg(src + (upper ? i * ND + j : j * ND + i));
+                            for (int j = 0; j < ND; j++) v[r][i * ND + j] = __ldg(src + (upper ? i * rs + j : j * rs + i));
                     } else {
 #pragma unroll
                         for (int i = 0; i < BB; i++) v[r][i] = 0.0;

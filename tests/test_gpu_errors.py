@@ -180,12 +180,37 @@ def test_failing_problems_stop_alone_and_leave_the_others_bits():
         b.close()
 
 
+DIVERGENCE = {"Newton-Raphson did not converge",
+              "von Mises plastic update must not lead to zero sigma_d (sigma_d < 1e-10)"}
+
+
+def _dropin_failure(p):
+    """(load step index, message) at which the drop-in path (device elements, host direct solve, the
+    reference's Newton loop) stops on problem p, or None."""
+    from pmsim_b200.elements import Elements
+    from pmsim_b200.solver import SolverImplicit
+    el = Elements(p.mesh, p.material, ngauss=9)
+    done = []
+    try:
+        SolverImplicit(el, p.essential, n_max_iterations=20, t_fin=float(p.nsteps)).solve(
+            lambda step, t, u, e: done.append(step))
+    except Exception as e:  # the reference's error text
+        return len(done), str(e)
+    finally:
+        el.close()
+    return None
+
+
 def test_population_sample_fails_where_the_oracle_driver_fails():
-    """A seeded sample of 32 footings from the batched configuration's population (512, seed 2024),
-    solved together by the batched device solver as the benchmark runs it (independent progress,
-    failing problems dropped): each problem it stops is stopped by the oracle driver (direct solve)
-    at the same load step with the same message, and each problem it converges the oracle
-    converges too."""
+    """A seeded sample of 32 footings from the batched configuration's population (512, seed 2024).
+    * The batched device solver, as the benchmark runs it (independent progress, failing problems
+      dropped), stops exactly the problems the oracle driver (direct solve) stops, at the same load
+      step.  Its linear solves are PCG to 1e-12 relative, so inside a diverging step its iterates
+      are not the direct solve's: a diverging Newton loop on this perfectly plastic material either
+      drives some sigma_d to zero or runs out of iterations, and which shows first may differ.  The
+      message must match, or both must be one of those two.
+    * The drop-in path (device elements with the same direct solve as the oracle) stops every
+      problem that fails on either side at the oracle's step with the oracle's message."""
     from pmsim_b200.batch import BatchSolver
     from pmsim_b200.footing import population
     probs = population(512, seed=2024)
@@ -193,8 +218,19 @@ def test_population_sample_fails_where_the_oracle_driver_fails():
     sample = sorted(rng.choice(512, size=32, replace=False).tolist())
     bs = BatchSolver([probs[i] for i in sample], n_max_iterations=20, pcg_max_iterations=5000)
     bs.solve_independent(on_fail="drop")
+    bad = []
+    nfail = 0
     for k, i in enumerate(sample):
         ref = _oracle_failure(probs[i])
-        assert bs.failed.get(k) == ref, (i, probs[i].name, bs.failed.get(k), ref)
-    assert bs.failed, "the sample holds failing problems"
+        got = bs.failed.get(k)
+        if ref is None and got is None:
+            continue
+        nfail += 1
+        same_step = (ref is None) == (got is None) and (ref is None or ref[0] == got[0])
+        same_msg = ref is not None and got is not None and (ref[1] == got[1] or {ref[1], got[1]} <= DIVERGENCE)
+        drop = _dropin_failure(probs[i])
+        if not (same_step and same_msg and drop == ref):
+            bad.append((i, probs[i].name, "oracle", ref, "batched", got, "drop-in", drop))
     bs.close()
+    assert not bad, bad
+    assert nfail > 0, "the sample holds failing problems"
