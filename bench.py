@@ -110,9 +110,8 @@ def flops_per_ip_hex20(plastic):
 
 # DRAM bytes (read + write) per cell of one launch of the element kernel element_kernel<3,20,...>
 # (gather assembly: upper element-matrix blocks out) from an ncu capture of a smaller block (traffic
-# grows with the cell count, so a launch over n cells moves n times this); None until that capture
-# exists for the current kernel.
-ELEMENT_DRAM_BYTES_PER_CELL = None
+# grows with the cell count, so a launch over n cells moves n times this).
+ELEMENT_DRAM_BYTES_PER_CELL = 15798  # 258.8 MB over 16,384 cells (32x32x16 block)
 
 
 def algorithmic_bytes_step(m, ng, nnz):
