@@ -278,11 +278,22 @@ __host__ __device__ constexpr int smem_table_doubles(int nn, int nd) {
 }
 // Direct-assembly metadata at the start of each cell area (doubles, kept even for 16-byte copies):
 // per node [bptr[A], bptr[A+1], crank | cfirst << 32, A] (NM), the pending ticket releases of the
-// warp's previous cell [row or -1, value] (PEND), and the cell's column-slot map (CSL, int16).
-__host__ __device__ constexpr int meta_doubles(int nn) { return 4 * nn + 2 * nn + 2 * ((nn * nn + 7) / 8); }
+// warp's previous cell [row or -1, value] (PEND), the cell's column-slot map (CSL, int16) and its
+// local nodes in ascending node id (CSORT, uint8).
+__host__ __device__ constexpr int meta_doubles(int nn) {
+    return 4 * nn + 2 * nn + 2 * ((nn * nn + 7) / 8) + 2 * ((nn + 15) / 16);
+}
+__host__ __device__ constexpr int cell_work_doubles(int nn, int nd, int ng) {
+    return ng * (nn * nd + 1) + ng * 10 + ng * 6 + (nd == 3 ? 0 : warps_per_cell(nn) * nn * node_vec_doubles(nd)) +
+           (ng & 1);
+}
+// Per cell: metadata, X and dU, then the phase work arrays; the direct assembly stages the cell's
+// upper node-pair blocks over the work arrays (after dU, which then holds F_int), so the work area
+// is at least that large.
 __host__ __device__ constexpr int smem_cell_doubles(int nn, int nd, int ng) {
-    return meta_doubles(nn) + 2 * nn * nd + ng * (nn * nd + 1) + ng * 10 + ng * 6 +
-           (nd == 3 ? 0 : warps_per_cell(nn) * nn * node_vec_doubles(nd)) + (ng & 1);
+    return meta_doubles(nn) + 2 * nn * nd +
+           (cell_work_doubles(nn, nd, ng) > nn * (nn + 1) / 2 * nd * nd ? cell_work_doubles(nn, nd, ng)
+                                                                          : ((nn * (nn + 1) / 2 * nd * nd + 1) & ~1));
 }
 __host__ __device__ constexpr int smem_bytes_for(int nn, int nd, int ng, int wpb) {
     return (smem_table_doubles(nn, nd) + (wpb / warps_per_cell(nn)) * smem_cell_doubles(nn, nd, ng)) * 8;
@@ -310,6 +321,7 @@ element_kernel(ElemArgs A) {
     int64_t* NM = reinterpret_cast<int64_t*>(wbase);  // [m][4] (direct assembly)
     int64_t* PEND = NM + 4 * NN;                      // [m][2] (direct assembly)
     int16_t* CSL = reinterpret_cast<int16_t*>(PEND + 2 * NN);  // [NN*NN] (direct assembly)
+    uint8_t* CSORT = reinterpret_cast<uint8_t*>(CSL) + 16 * ((NN * NN + 7) / 8);  // [NN] (direct assembly)
     double* Xs = wbase + meta_doubles(NN);     // [m][d]
     double* Us = Xs + NE;                      // [m][d]
     double* G = Us + NE;                       // [p][GS]
@@ -887,22 +899,41 @@ element_kernel(ElemArgs A) {
         }  // dense output
     }
     // ---------------- direct assembly: ordered scatter into the CSR values and R ----------------
-    // Node lane m adds slab m (block row A = conn[m]) once ticket[A] equals this cell's rank among
-    // A's cells; every lane adds the blocks of its tile that lie in the ready rows -- (a, b) into row
-    // a and the mirror (b, a) into row b -- and node lane m then advances ticket[A] (the last cell of
-    // A puts it back to 0 for the next launch).  Rows become ready in rounds, so this cell never
-    // waits for a row it could already write: no wait chains along the cell order.
+    // The lanes stage the cell's upper node-pair blocks in shared memory (over the phase work
+    // arrays, after dU, which holds F_int).  Node lane m then takes row A = conn[m] once ticket[A]
+    // equals this cell's rank among A's cells; for every ready row the whole warp writes the row's
+    // values -- block (m, b) for every local node b, read transposed from block (b, m) when b < m --
+    // with the nodes taken in ascending node id, which is ascending column slot in every row, so
+    // consecutive lanes write consecutive CSR positions.  Node lane m then advances ticket[A] (the
+    // last cell of A puts it back to 0 for the next launch).  Rows become ready in rounds, so this
+    // cell never waits for a row it could already write.
     if constexpr (CSR) {
         if (DOF || DOK) {
+            double* KS = Us + NE;  // upper blocks, upper_entry layout
+            const int a0 = max(ti, 0) * RT, b0 = max(tj, 0) * CT;
+            if (DOK && ti >= 0) {
+#pragma unroll
+                for (int r = 0; r < RT; r++)
+#pragma unroll
+                    for (int c = 0; c < CT; c++) {
+                        const int a = a0 + r, b = b0 + c;
+                        if (a < NN && b < NN && a <= b) {
+#pragma unroll
+                            for (int i = 0; i < ND; i++)
+#pragma unroll
+                                for (int j = 0; j < ND; j++) KS[upper_entry<NN, ND>(a, b, i, j)] = acc[r][c][i][j];
+                        }
+                    }
+            }
             cp_async_wait_all();
-            __syncwarp();  // every lane's copies are visible
+            __syncwarp();  // the staged blocks and every lane's copies are visible
             // release the rows the warp's previous cell left pending before anything can wait here:
             // a warp never waits while it holds a release
             if (lane < NN && PEND[2 * lane] >= 0) {
                 ticket_store(A.ticket + PEND[2 * lane], (int)PEND[2 * lane + 1]);
                 PEND[2 * lane] = -1;
             }
-            int64_t rowA = 0, pos_m = 0;
+            int64_t rowA = INT64_MAX, pos_m = 0;
             int rs_m = 0, rank_m = 0;
             bool last_m = false, todo = false;
             if (lane < NN) {
@@ -916,24 +947,13 @@ element_kernel(ElemArgs A) {
                 last_m = (cr & CRANK_LAST) != 0;
                 todo = true;
             }
-            const int a0 = max(ti, 0) * RT, b0 = max(tj, 0) * CT;
-            int64_t posR[RT], posC[CT];
-            int rsR[RT], rsC[CT];
-            uint32_t fR[RT];  // per row node: which of its blocks this cell contributes first
+            {  // the cell's local nodes in ascending node id
+                int rk = 0;
 #pragma unroll
-            for (int r = 0; r < RT; r++) {
-                const int src = min(a0 + r, NN - 1);
-                posR[r] = __shfl_sync(FULL, pos_m, src);
-                rsR[r] = __shfl_sync(FULL, rs_m, src);
-                fR[r] = reinterpret_cast<const uint32_t*>(NM + 4 * src + 2)[1];
+                for (int q = 0; q < NN; q++) rk += __shfl_sync(FULL, rowA, q) < rowA;
+                if (lane < NN) CSORT[rk] = (uint8_t)lane;
             }
-#pragma unroll
-            for (int c = 0; c < CT; c++) {
-                const int src = min(b0 + c, NN - 1);
-                posC[c] = __shfl_sync(FULL, pos_m, src);
-                rsC[c] = __shfl_sync(FULL, rs_m, src);
-            }
-            const int16_t* cs_cell = CSL;
+            __syncwarp();
             int spins = 0;
             while (true) {
                 const unsigned todo_mask = __ballot_sync(FULL, todo);
@@ -960,24 +980,23 @@ element_kernel(ElemArgs A) {
                         else red_add(q, Us[lane * ND + i]);
                     }
                 }
-                if (DOK && ti >= 0) {
-#pragma unroll
-                    for (int r = 0; r < RT; r++)
-#pragma unroll
-                        for (int c = 0; c < CT; c++) {
-                            const int a = a0 + r, b = b0 + c;
-                            if (a < NN && b < NN && a <= b) {
-                                // block (A, B) and its mirror (B, A) get their first contribution from
-                                // the first cell holding both nodes (one bit, symmetric in a and b)
-                                const bool first = (fR[r] >> b) & 1u;
-                                if ((rmask >> a) & 1u)
-                                    csr_add_block<ND>(A.csr, posR[r] + ND * (int64_t)cs_cell[a * NN + b], rsR[r], first,
-                                                      acc[r][c], false);
-                                if (a != b && ((rmask >> b) & 1u))
-                                    csr_add_block<ND>(A.csr, posC[c] + ND * (int64_t)cs_cell[b * NN + a], rsC[c], first,
-                                                      acc[r][c], true);
-                            }
+                if (DOK) {
+                    for (unsigned rows = rmask; rows; rows &= rows - 1) {  // the ready rows, one by one
+                        const int a = __ffs(rows) - 1;
+                        const int64_t pa = __shfl_sync(FULL, pos_m, a);
+                        const int rsa = __shfl_sync(FULL, rs_m, a);
+                        // block (A, B) and its mirror get their first contribution from the first cell
+                        // holding both nodes (cfirst bit b of row a)
+                        const uint32_t fa = reinterpret_cast<const uint32_t*>(NM + 4 * a + 2)[1];
+                        for (int e = lane; e < ND * NN * ND; e += 32) {
+                            const int i = e / (NN * ND), k = (e - i * NN * ND) / ND, j = e - i * NN * ND - k * ND;
+                            const int b = CSORT[k];
+                            const double v = (a <= b) ? KS[upper_entry<NN, ND>(a, b, i, j)] : KS[upper_entry<NN, ND>(b, a, j, i)];
+                            double* q = A.csr + pa + (int64_t)i * rsa + ND * (int64_t)CSL[a * NN + b] + j;
+                            if ((fa >> b) & 1u) *q = 0.0 + v;
+                            else red_add(q, v);
                         }
+                    }
                 }
                 __syncwarp();  // every lane's writes precede the node lanes' (cumulative) release stores
                 // the rows of the last round are released at the warp's next scatter (or its exit),
@@ -1075,6 +1094,7 @@ __global__ void __launch_bounds__(WPB2 * 32, 4) element2d_kernel(ElemArgs A) {
                                              (CPW * wid + hh) * meta_doubles(NN));
     int64_t* PEND = NM + 4 * NN;
     int16_t* CSL = reinterpret_cast<int16_t*>(PEND + 2 * NN);
+    uint8_t* CSORT = reinterpret_cast<uint8_t*>(CSL) + 16 * ((NN * NN + 7) / 8);
     double* Us = Xs + NE;
     double* G = Us + NE;       // [p][GS]
     double* H = G + ng * GS;   // [p][GS]
@@ -1547,21 +1567,41 @@ __global__ void __launch_bounds__(WPB2 * 32, 4) element2d_kernel(ElemArgs A) {
             }  // dense output
         }
         // ---------------- direct assembly: ordered scatter into the CSR values and R ----------------
-        // As in element_kernel, with the CPW cells of the warp in one round structure: node lane
-        // (slot h, node m) adds slab m of cell h once ticket[conn[m]] equals that cell's rank, the
-        // tile lanes add their blocks of the ready rows, and a row shared by two cells of the warp is
-        // added by the lower one first (its rank is lower).  Slots without a cell add nothing.
+        // As in element_kernel, with the CPW cells of the warp in one round structure: each slot stages
+        // its cell's upper blocks after its dU slot (which holds F_int), node lane (slot h, node m)
+        // takes row conn[m] of cell h once the row's ticket equals that cell's rank, and for every
+        // ready row the whole warp writes the row's values (nodes in ascending id, so consecutive
+        // lanes write consecutive CSR positions).  A row shared by two cells of the warp is added by
+        // the one earlier in the processing order first (its rank is lower).  Slots without a cell
+        // add nothing.
         if constexpr (CSR) {
             if (DOF || DOK) {
+                double* KS = Us + NE;  // this slot's upper blocks (2x2 each, upper_entry layout)
+                {
+                    const int a0 = max(ti, 0) * T, b0 = max(tj, 0) * T;
+                    if (DOK && active && ti >= 0) {
+#pragma unroll
+                        for (int r = 0; r < T; r++)
+#pragma unroll
+                            for (int c = 0; c < T; c++) {
+                                const int a = a0 + r, b = b0 + c;
+                                if (a < NN && b < NN && a <= b) {
+#pragma unroll
+                                    for (int i = 0; i < 2; i++)
+#pragma unroll
+                                        for (int j = 0; j < 2; j++) KS[upper_entry<NN, 2>(a, b, i, j)] = acc[r][c][i][j];
+                                }
+                            }
+                    }
+                }
                 cp_async_wait_all();
-                __syncwarp();  // every lane's copies are visible
+                __syncwarp();  // the staged blocks and every lane's copies are visible
                 // release the rows the slot's previous cell left pending before anything can wait here
                 if (hl < NN && PEND[2 * hl] >= 0) {
                     ticket_store(A.ticket + PEND[2 * hl], (int)PEND[2 * hl + 1]);
                     PEND[2 * hl] = -1;
                 }
-                const int sb = LPC * hh;  // first lane of this slot
-                int64_t rowA = 0, pos_m = 0;
+                int64_t rowA = INT64_MAX, pos_m = 0;
                 int rs_m = 0, rank_m = 0;
                 bool last_m = false, todo = false;
                 if (active && hl < NN) {
@@ -1575,22 +1615,17 @@ __global__ void __launch_bounds__(WPB2 * 32, 4) element2d_kernel(ElemArgs A) {
                     last_m = (cr & CRANK_LAST) != 0;
                     todo = true;
                 }
-                const int a0 = max(ti, 0) * T, b0 = max(tj, 0) * T;
-                int64_t posR[T], posC[T];
-                int rsR[T], rsC[T];
-                uint32_t fR[T];  // per row node: which of its blocks this cell contributes first
+                {  // each slot's local nodes in ascending node id
+                    const int sb = LPC * hh;
+                    int rk = 0;
 #pragma unroll
-                for (int r = 0; r < T; r++) {
-                    const int src = sb + min(a0 + r, NN - 1);
-                    posR[r] = __shfl_sync(FULL, pos_m, src);
-                    rsR[r] = __shfl_sync(FULL, rs_m, src);
-                    fR[r] = (active && ti >= 0) ? reinterpret_cast<const uint32_t*>(NM + 4 * min(a0 + r, NN - 1) + 2)[1]
-                                                : 0u;
-                    const int srcc = sb + min(b0 + r, NN - 1);
-                    posC[r] = __shfl_sync(FULL, pos_m, srcc);
-                    rsC[r] = __shfl_sync(FULL, rs_m, srcc);
+                    for (int q = 0; q < NN; q++) rk += __shfl_sync(FULL, rowA, sb + q) < rowA;
+                    if (active && hl < NN) CSORT[rk] = (uint8_t)hl;
                 }
-                const int16_t* cs_cell = CSL;
+                __syncwarp();
+                const double* ks_base = smem2 + table2_doubles(NN) + (int64_t)(CPW * wid) * cd + 2 * NE;
+                const int64_t* nm_base = reinterpret_cast<const int64_t*>(smem2 + table2_doubles(NN) + CPW * WPB2 * cd +
+                                                                         (CPW * wid) * meta_doubles(NN));
                 int spins = 0;
                 while (true) {
                     const unsigned todo_mask = __ballot_sync(FULL, todo);
@@ -1614,26 +1649,29 @@ __global__ void __launch_bounds__(WPB2 * 32, 4) element2d_kernel(ElemArgs A) {
                         for (int i = 0; i < 2; i++) {
                             double* q = A.ff + rowA * 2 + i;
                             if (rank_m == 0) *q = 0.0 + Us[hl * 2 + i];
-                        else red_add(q, Us[hl * 2 + i]);
+                            else red_add(q, Us[hl * 2 + i]);
                         }
                     }
-                    if (DOK && active && ti >= 0) {
-                        const unsigned mine = rmask >> sb;
-#pragma unroll
-                        for (int r = 0; r < T; r++)
-#pragma unroll
-                            for (int c = 0; c < T; c++) {
-                                const int a = a0 + r, b = b0 + c;
-                                if (a < NN && b < NN && a <= b) {
-                                    const bool first = (fR[r] >> b) & 1u;  // lowest cell holding both nodes
-                                    if ((mine >> a) & 1u)
-                                        csr_add_block<2>(A.csr, posR[r] + 2 * (int64_t)cs_cell[a * NN + b], rsR[r], first,
-                                                         acc[r][c], false);
-                                    if (a != b && ((mine >> b) & 1u))
-                                        csr_add_block<2>(A.csr, posC[c] + 2 * (int64_t)cs_cell[b * NN + a], rsC[c], first,
-                                                         acc[r][c], true);
-                                }
+                    if (DOK) {
+                        for (unsigned rows = rmask; rows; rows &= rows - 1) {  // the ready rows, one by one
+                            const int bit = __ffs(rows) - 1;
+                            const int h = bit / LPC, a = bit - h * LPC;  // slot and local node of the row
+                            const int64_t pa = __shfl_sync(FULL, pos_m, bit);
+                            const int rsa = __shfl_sync(FULL, rs_m, bit);
+                            const double* ks = ks_base + (int64_t)h * cd;
+                            const int64_t* nm = nm_base + (int64_t)h * (meta_doubles(NN));
+                            const int16_t* csl = reinterpret_cast<const int16_t*>(nm + 6 * NN);
+                            const uint8_t* cso = reinterpret_cast<const uint8_t*>(csl) + 16 * ((NN * NN + 7) / 8);
+                            const uint32_t fa = reinterpret_cast<const uint32_t*>(nm + 4 * a + 2)[1];
+                            for (int e = lane; e < 2 * NN * 2; e += 32) {
+                                const int i = e / (NN * 2), k = (e - i * NN * 2) / 2, j = e - i * NN * 2 - k * 2;
+                                const int b = cso[k];
+                                const double v = (a <= b) ? ks[upper_entry<NN, 2>(a, b, i, j)] : ks[upper_entry<NN, 2>(b, a, j, i)];
+                                double* q = A.csr + pa + (int64_t)i * rsa + 2 * (int64_t)csl[a * NN + b] + j;
+                                if ((fa >> b) & 1u) *q = 0.0 + v;
+                                else red_add(q, v);
                             }
+                        }
                     }
                     __syncwarp();  // every lane's writes precede the node lanes' (cumulative) release stores
                     // the last round's rows are released at the slot's next scatter (or the exit)
