@@ -221,6 +221,9 @@ typedef struct pms_batch_config {
     int32_t n_max_iterations;   /* Newton iterations per step (reference default 10) */
     double pcg_rtol;            /* PCG stops at |r|_2 <= pcg_rtol |r0|_2 (default 1e-12) */
     int32_t pcg_max_iterations; /* PCG iteration cap per solve (default 20000) */
+    int32_t constant_tangent;   /* Config::constant_tangent (src/fem/solver_implicit.rs:216): K assembled (and
+                                   the preconditioner formed) only at the first Newton iteration of each
+                                   load step; later iterations update the IP state and R only */
 } pms_batch_config;
 
 typedef struct pms_batch pms_batch;

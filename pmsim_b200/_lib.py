@@ -68,7 +68,7 @@ class Config_(ctypes.Structure):
 class BatchConfig_(ctypes.Structure):
     _fields_ = [("tol_rr_abs", ctypes.c_double), ("tol_mdu_rel", ctypes.c_double),
                 ("n_max_iterations", ctypes.c_int32), ("pcg_rtol", ctypes.c_double),
-                ("pcg_max_iterations", ctypes.c_int32)]
+                ("pcg_max_iterations", ctypes.c_int32), ("constant_tangent", ctypes.c_int32)]
 
 
 class BatchTuning_(ctypes.Structure):

@@ -34,7 +34,7 @@ class Problem:
 
 class BatchSolver:
     def __init__(self, problems, tol_rr_abs=1e-10, tol_mdu_rel=1e-8, n_max_iterations=20, pcg_rtol=1e-12,
-                 pcg_max_iterations=20000):
+                 pcg_max_iterations=20000, constant_tangent=False):
         if not problems:
             raise ValueError("no problems")
         kinds = {p.mesh.kind for p in problems}
@@ -78,7 +78,10 @@ class BatchSolver:
             for i, p in enumerate(problems):
                 if p.ff_ext is not None:
                     ff_ext[self.dof_ptr[i]:self.dof_ptr[i + 1]] = p.ff_ext
-        cfg = _lib.BatchConfig_(tol_rr_abs, tol_mdu_rel, n_max_iterations, pcg_rtol, pcg_max_iterations)
+        # constant_tangent: Config::constant_tangent (src/fem/solver_implicit.rs:216), K assembled only at the
+        # first Newton iteration of each load step
+        cfg = _lib.BatchConfig_(tol_rr_abs, tol_mdu_rel, n_max_iterations, pcg_rtol, pcg_max_iterations,
+                                1 if constant_tangent else 0)
         h = ctypes.c_void_p()
         rc = self.L.pms_batch_create(self.elements.h, len(problems), _lib.ptr(self.point_ptr),
                                      _lib.ptr(self.cell_ptr), len(self.pres_eq), _lib.ptr(self.pres_eq),

@@ -364,8 +364,10 @@ element_kernel(ElemArgs A) {
         mode = A.pmode[A.cell_prob[cell]];
         if (mode == 0) continue;  // inactive problem: the cell's warps skip it together
     }
-    const bool do_update = (UPD == UPD_MODE) ? (mode == 2) : (UPD != UPD_NONE);
-    const bool from_backup = (UPD == UPD_BACKUP) || (UPD == UPD_MODE && mode == 2);
+    const bool do_update = (UPD == UPD_MODE) ? (mode >= 2) : (UPD != UPD_NONE);
+    const bool from_backup = (UPD == UPD_BACKUP) || (UPD == UPD_MODE && mode >= 2);
+    // mode 3 (batched solver, constant tangent): update and F_int, K left as it is
+    const bool dok_c = DOK && !(UPD == UPD_MODE && mode == 3);
     const MatConst mc = A.mats[A.cmat ? A.cmat[cell] : 0];
 
     if (half == 0) {  // warp 0 of the cell: node data, integration points, F_int
@@ -482,7 +484,7 @@ element_kernel(ElemArgs A) {
                 c6[5] = coef * sig[5 % NC] * INV_SQRT2;
             }
         }
-        if (DOK) {
+        if (dok_c) {
             double a, b, s[NC];
             err_t = tangent_coefs<NC>(mc, mc.hh, sig, lam, el, a, b, s);
             double* t = TC + p * 10;
@@ -582,7 +584,7 @@ element_kernel(ElemArgs A) {
     // ---------------- phase 2: lane owns a tile of node-pair blocks ----------------
     int ti = -1, tj = -1;
     double acc[RT][CT][ND][ND];
-    if (DOK) {
+    if (dok_c) {
         // tile number lane + 32*half: (i, j) with i*RT <= min(j*CT + CT - 1, NN - 1), row-major
         {
             const int me = lane + 32 * half;
@@ -826,6 +828,23 @@ element_kernel(ElemArgs A) {
             }
         }
         }  // ND
+        if constexpr (CSR) {  // direct assembly: stage the upper blocks after dU for the scatter
+            double* KS = Us + NE;
+            if (ti >= 0) {
+#pragma unroll
+                for (int r = 0; r < RT; r++)
+#pragma unroll
+                    for (int c = 0; c < CT; c++) {
+                        const int a = a0 + r, b = b0 + c;
+                        if (a < NN && b < NN && a <= b) {
+#pragma unroll
+                            for (int i = 0; i < ND; i++)
+#pragma unroll
+                                for (int j = 0; j < ND; j++) KS[upper_entry<NN, ND>(a, b, i, j)] = acc[r][c][i][j];
+                        }
+                    }
+            }
+        }
         // dense output: write K_e (row-major NE x NE) through the warp's shared memory, RS node rows at a time:
         // each lane drops its blocks (a, b) and mirrors (b, a) into the staged rows, then the warp
         // copies the rows out with contiguous stores
@@ -909,22 +928,7 @@ element_kernel(ElemArgs A) {
     // cell never waits for a row it could already write.
     if constexpr (CSR) {
         if (DOF || DOK) {
-            double* KS = Us + NE;  // upper blocks, upper_entry layout
-            const int a0 = max(ti, 0) * RT, b0 = max(tj, 0) * CT;
-            if (DOK && ti >= 0) {
-#pragma unroll
-                for (int r = 0; r < RT; r++)
-#pragma unroll
-                    for (int c = 0; c < CT; c++) {
-                        const int a = a0 + r, b = b0 + c;
-                        if (a < NN && b < NN && a <= b) {
-#pragma unroll
-                            for (int i = 0; i < ND; i++)
-#pragma unroll
-                                for (int j = 0; j < ND; j++) KS[upper_entry<NN, ND>(a, b, i, j)] = acc[r][c][i][j];
-                        }
-                    }
-            }
+            const double* KS = Us + NE;  // the cell's upper blocks, staged at the end of phase 2
             cp_async_wait_all();
             __syncwarp();  // the staged blocks and every lane's copies are visible
             // release the rows the warp's previous cell left pending before anything can wait here:
@@ -980,7 +984,7 @@ element_kernel(ElemArgs A) {
                         else red_add(q, Us[lane * ND + i]);
                     }
                 }
-                if (DOK) {
+                if (dok_c) {
                     for (unsigned rows = rmask; rows; rows &= rows - 1) {  // the ready rows, one by one
                         const int a = __ffs(rows) - 1;
                         const int64_t pa = __shfl_sync(FULL, pos_m, a);
@@ -1170,8 +1174,10 @@ __global__ void __launch_bounds__(WPB2 * 32, 4) element2d_kernel(ElemArgs A) {
             cell = cell_first;
             mode = mode_first;
         }
-        const bool do_update = (UPD == UPD_MODE) ? (mode == 2) : (UPD != UPD_NONE);
-        const bool from_backup = (UPD == UPD_BACKUP) || (UPD == UPD_MODE && mode == 2);
+        const bool do_update = (UPD == UPD_MODE) ? (mode >= 2) : (UPD != UPD_NONE);
+        const bool from_backup = (UPD == UPD_BACKUP) || (UPD == UPD_MODE && mode >= 2);
+        // mode 3 (batched solver, constant tangent): update and F_int, K left as it is
+        const bool dok_c = DOK && active && !(UPD == UPD_MODE && mode == 3);
         const MatConst mc = A.mats[A.cmat ? A.cmat[cell] : 0];
 
         // the IP state first, so that its latency overlaps the node staging
@@ -1270,7 +1276,7 @@ __global__ void __launch_bounds__(WPB2 * 32, 4) element2d_kernel(ElemArgs A) {
                 c6[3] = coef * sig[2];
                 c6[4] = rad;
             }
-            if (DOK) {
+            if (dok_c) {
                 double a, b, s[4];
                 err_t = tangent_coefs<4>(mc, mc.hh, sig, lam, el, a, b, s);
                 double* t = TC + p * 4;
@@ -1383,7 +1389,7 @@ __global__ void __launch_bounds__(WPB2 * 32, 4) element2d_kernel(ElemArgs A) {
                     for (int i = 0; i < 2; i++)
 #pragma unroll
                         for (int j = 0; j < 2; j++) acc[r][c][i][j] = 0.0;
-            if (ti >= 0 && !A.axisym) {
+            if (dok_c && ti >= 0 && !A.axisym) {
                 // two passes, as in element_kernel: X_ab = sum_p alpha_p g_a g_b^T over every point,
                 // K_ab = X_ab^T + tr(X_ab) 1 + c X_ab, then kappa_p g_a g_b^T + beta_p h_a h_b^T at
                 // the plastic points (c = gamma/alpha of the elastic tangent, kappa = gamma - c alpha)
@@ -1456,7 +1462,7 @@ __global__ void __launch_bounds__(WPB2 * 32, 4) element2d_kernel(ElemArgs A) {
                                 }
                     }
                 }
-            } else if (ti >= 0) {  // axisymmetric: the hoop terms take the one-pass form
+            } else if (dok_c && ti >= 0) {  // axisymmetric: the hoop terms take the one-pass form
                 for (int p = 0; p < ng; p++) {
                     const double2 t01 = reinterpret_cast<const double2*>(TC)[2 * p];
                     const double al = t01.x, ga = t01.y, be = TC[p * 4 + 2];
@@ -1579,7 +1585,7 @@ __global__ void __launch_bounds__(WPB2 * 32, 4) element2d_kernel(ElemArgs A) {
                 double* KS = Us + NE;  // this slot's upper blocks (2x2 each, upper_entry layout)
                 {
                     const int a0 = max(ti, 0) * T, b0 = max(tj, 0) * T;
-                    if (DOK && active && ti >= 0) {
+                    if (dok_c && ti >= 0) {
 #pragma unroll
                         for (int r = 0; r < T; r++)
 #pragma unroll
@@ -1624,6 +1630,7 @@ __global__ void __launch_bounds__(WPB2 * 32, 4) element2d_kernel(ElemArgs A) {
                 }
                 __syncwarp();
                 const double* ks_base = smem2 + table2_doubles(NN) + (int64_t)(CPW * wid) * cd + 2 * NE;
+                const unsigned dokmask = __ballot_sync(FULL, dok_c);  // the slots whose K rows are written
                 const int64_t* nm_base = reinterpret_cast<const int64_t*>(smem2 + table2_doubles(NN) + CPW * WPB2 * cd +
                                                                          (CPW * wid) * meta_doubles(NN));
                 int spins = 0;
@@ -1653,7 +1660,7 @@ __global__ void __launch_bounds__(WPB2 * 32, 4) element2d_kernel(ElemArgs A) {
                         }
                     }
                     if (DOK) {
-                        for (unsigned rows = rmask; rows; rows &= rows - 1) {  // the ready rows, one by one
+                        for (unsigned rows = rmask & dokmask; rows; rows &= rows - 1) {  // the ready rows
                             const int bit = __ffs(rows) - 1;
                             const int h = bit / LPC, a = bit - h * LPC;  // slot and local node of the row
                             const int64_t pa = __shfl_sync(FULL, pos_m, bit);

@@ -812,10 +812,10 @@ __global__ void step_init_kernel(int np, const uint8_t* sel, uint8_t* phase, int
 
 // element modes of this iteration (1: new step, 2: continue), dU = 0 mask of the new steps
 __global__ void step_pre_elem_kernel(int np, const uint8_t* phase, uint8_t* pmode, uint8_t* start, uint8_t* active,
-                                     int32_t* it, unsigned long long* perr) {
+                                     int32_t* it, unsigned long long* perr, int constant_tangent) {
     for (int p = threadIdx.x; p < np; p += blockDim.x) {
         const uint8_t ph = phase[p];
-        const uint8_t m = ph == PH_START ? 1 : (ph == PH_CONT ? 2 : 0);
+        const uint8_t m = ph == PH_START ? 1 : (ph == PH_CONT ? (constant_tangent ? 3 : 2) : 0);
         pmode[p] = m;
         start[p] = ph == PH_START;
         active[p] = m != 0;
@@ -1443,7 +1443,8 @@ int pms_batch_tick(pms_batch* b, const uint8_t* cmd, const double* c_values, int
             start[p] = 1;
         }
         elem[p] = 1;
-        mode[p] = cmd[p] == 1 ? 1 : 2;
+        // mode 1: step start (K assembled); 2: update, F_int and K; 3: constant tangent, K kept
+        mode[p] = cmd[p] == 1 ? 1 : (b->cfg.constant_tangent ? 3 : 2);
         any_elem = true;
     }
     if (b->npres > 0) cudaMemcpyAsync(b->d_c, c_values, b->npres * 8, cudaMemcpyHostToDevice, st);
@@ -1697,7 +1698,8 @@ int build_step_graph(pms_batch* b) {
     body.ok = top.ok;
     if (body.ok) body.ok = cudaGraphConditionalHandleCreate(&hP, B1, 0, 0) == cudaSuccess;
     // element pass of the problems that start a step or continue it
-    void* a_pre[] = {&np, &b->d_phase, &b->d_pmode, &b->d_upd, &b->d_active, &b->d_it, &b->d_perr};
+    int ct = b->cfg.constant_tangent ? 1 : 0;
+    void* a_pre[] = {&np, &b->d_phase, &b->d_pmode, &b->d_upd, &b->d_active, &b->d_it, &b->d_perr, &ct};
     body.kernel((const void*)step_pre_elem_kernel, 1, 1024, a_pre);
     void* a_zero[] = {&S, &b->d_upd, &b->d_ddu};
     body.kernel((const void*)zero_masked_kernel, grid_of(b->ndof), 256, a_zero);

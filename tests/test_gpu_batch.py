@@ -223,3 +223,33 @@ def test_device_resident_loop_stops_failing_problems_alone():
     for i in (0, 2):
         assert np.array_equal(a.u_of(i, ua), b.u_of(i, ub))
         assert a.history[i] == b.history[i]
+
+
+@pytest.mark.parametrize("name", ["single_element_2d", "2x2_elements_2d"])
+def test_batch_constant_tangent_matches_oracle(name):
+    """Config::constant_tangent (src/fem/solver_implicit.rs:216) in the batched solver: K assembled
+    (and the block-Jacobi preconditioner formed) at the first Newton iteration of each load step only,
+    the later iterations updating the IP state and R (element-pass mode 3).  Host-sequenced and
+    with the Newton loop on the device: the oracle driver's iteration counts (more than full
+    Newton's) and displacements at every step, and the same bits on both paths."""
+    from pmsim_b200.batch import BatchSolver
+    pb = problems.SPO_PROBLEMS[name]()
+    m = pb["mesh"]
+    oel = oracle.OracleElements(m, 1, oracle.Params(*pb["params"]), ngauss=pb["ngauss"], sym_tol=-1.0)
+    ref = []
+    osol = OracleSolver(oel, m.ndof, pb["essential"], n_max_iterations=60, t_fin=float(pb["nsteps"]),
+                        constant_tangent=True)
+    osol.solve(lambda s, t, u, e: ref.append(u[:m.ndof].copy()))
+    runs = {}
+    for device_loop in (False, True):
+        bs = BatchSolver([as_problem(pb)], n_max_iterations=60, constant_tangent=True)
+        got = []
+        bs.solve(lambda step, b: got.append(b.u_of(0).copy()), device_loop=device_loop)
+        assert bs.history[0] == [len(h) for h in osol.history], (device_loop, bs.history[0])
+        for ug, uo in zip(got, ref):
+            assert np.max(np.abs(ug - uo)) <= 1e-9 * max(np.max(np.abs(uo)), 1e-300)
+        runs[device_loop] = got
+        bs.close()
+    for a, b in zip(runs[False], runs[True]):
+        assert np.array_equal(a, b)
+    assert sum(len(h) for h in osol.history) > pb["nsteps"] * 2  # modified Newton takes extra iterations
