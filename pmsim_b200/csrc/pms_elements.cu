@@ -1059,8 +1059,9 @@ __host__ __device__ constexpr int cell2_doubles(int nn, int ng) {
                  ? 4 * nn + 2 * ng * (2 * nn + 2) + ((ng * nn + 1) & ~1) + 10 * ng
                  : 4 * nn * nn) + 1) & ~1;
 }
-__host__ __device__ constexpr int smem2_bytes(int nn, int ng, int cpw) {
-    return (table2_doubles(nn) + cpw * WPB2 * (cell2_doubles(nn, ng) + meta_doubles(nn))) * 8;
+// The direct-assembly metadata (after all cell areas) only for the kernels that assemble directly.
+__host__ __device__ constexpr int smem2_bytes(int nn, int ng, int cpw, bool csr) {
+    return (table2_doubles(nn) + cpw * WPB2 * (cell2_doubles(nn, ng) + (csr ? meta_doubles(nn) : 0))) * 8;
 }
 
 // Lanes per cell of the packed layout: enough for every node, every node-pair tile and (checked at
@@ -1094,8 +1095,9 @@ __global__ void __launch_bounds__(WPB2 * 32, 4) element2d_kernel(ElemArgs A) {
     double* Ns = ws + 16;         // [m][16]
     double* Xs = smem2 + table2_doubles(NN) + (CPW * wid + hh) * cd;
     // direct assembly: the slot's row data, pending releases and slot map (as in element_kernel)
-    int64_t* NM = reinterpret_cast<int64_t*>(smem2 + table2_doubles(NN) + CPW * WPB2 * cd +
-                                             (CPW * wid + hh) * meta_doubles(NN));
+    int64_t* NM = CSR ? reinterpret_cast<int64_t*>(smem2 + table2_doubles(NN) + CPW * WPB2 * cd +
+                                                   (CPW * wid + hh) * meta_doubles(NN))
+                      : reinterpret_cast<int64_t*>(smem2);  // not used without the direct assembly
     int64_t* PEND = NM + 4 * NN;
     int16_t* CSL = reinterpret_cast<int16_t*>(PEND + 2 * NN);
     uint8_t* CSORT = reinterpret_cast<uint8_t*>(CSL) + 16 * ((NN * NN + 7) / 8);
@@ -2017,13 +2019,9 @@ template <int NN, int LPC, int UPD, bool DOF, bool DOK, bool CSR>
 void launch_elem2d_lpc(const ElemArgs& a, cudaStream_t st, bool persistent) {
     constexpr int CPW = 32 / LPC;
     auto kern = element2d_kernel<NN, LPC, UPD, DOF, DOK, CSR>;
-    const int smem = smem2_bytes(NN, a.ngauss, CPW);
-    static thread_local bool configured = false;
-    if (!configured) {
-        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem2_bytes(NN, LPC, CPW));
-        cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
-        configured = true;
-    }
+    const int smem = smem2_bytes(NN, a.ngauss, CPW, CSR);
+    allow_dynamic_smem((const void*)kern);
+    cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
     int64_t blocks = ((a.ncell + CPW - 1) / CPW + WPB2 - 1) / WPB2;
     if (persistent || CSR) blocks = std::min<int64_t>(blocks, resident_blocks((const void*)kern, smem, WPB2 * 32));
     if (CSR) cudaMemsetAsync(a.next, 0, sizeof(unsigned long long), st);
@@ -2842,8 +2840,8 @@ template <int NN, int LPC>
 ElemLaunchShape mode_shape_2d(const ElemArgs& a) {
     constexpr int CPW = 32 / LPC;
     auto kern = element2d_kernel<NN, LPC, UPD_MODE, true, true, true>;
-    const int smem = smem2_bytes(NN, a.ngauss, CPW);
-    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem2_bytes(NN, LPC, CPW));
+    const int smem = smem2_bytes(NN, a.ngauss, CPW, true);
+    allow_dynamic_smem((const void*)kern);
     cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
     int64_t blocks = ((a.ncell + CPW - 1) / CPW + WPB2 - 1) / WPB2;
     blocks = std::min<int64_t>(blocks, resident_blocks((const void*)kern, smem, WPB2 * 32));
