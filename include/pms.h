@@ -131,7 +131,7 @@ int pms_elements_update_secondary(pms_elements* h, const double* ddu, int32_t me
 int pms_elements_assemble_f_int(pms_elements* h, double* ff_int, int32_t mem);
 /* Elements::assemble_kke (elements.rs:156-163; element_solid.rs:168-185; assembly.rs:70-139):
  * csr_values[nnz] = sum_e sum_p B^T D_ep B |J| w t in the pattern of pms_elements_csr_pattern.
- * Bit-reproducible: every entry sums its element contributions in ascending cell order. */
+ * Bit-reproducible: every entry sums its element contributions in a fixed order (pms_assembly). */
 int pms_elements_assemble_kk(pms_elements* h, double* csr_values, int32_t mem);
 /* Fused Newton-iteration call = restore + update_secondary(ddu) + assemble_f_int + assemble_kk
  * on the updated state, in one pass over the cells (ff_int/csr_values nullable).  Every IP starts
@@ -150,13 +150,14 @@ int pms_elements_get_state(pms_elements* h, double* sig, double* ivs, uint8_t* e
 int pms_elements_set_state(pms_elements* h, const double* sig, const double* ivs, const uint8_t* elastic);
 
 /* How K and R are assembled (no counterpart in the reference, whose COO triplets are summed by the
- * sparse solver, src/base/assembly.rs:70-139).  Both give the same bits: every entry is the sum of
- * its cells' contributions in ascending cell order.
- *   PMS_ASSEMBLY_DIRECT (default): the element kernel adds each cell's blocks straight into the
- *     CSR values and R, row by row in ascending cell order (per-row tickets); no element matrices
- *     are stored.
- *   PMS_ASSEMBLY_GATHER: the element kernel writes every cell's dense K_e and F_e, then gather
- *     kernels sum them row by row (needs 8*ncell*(nnode*ndim)^2 bytes more device memory). */
+ * sparse solver, src/base/assembly.rs:70-139).  Both are bit-reproducible run to run; they agree to
+ * the last bits (their summation orders differ).
+ *   PMS_ASSEMBLY_GATHER (default): the element kernel writes each cell's upper node-pair blocks of
+ *     K_e (a <= b) and F_e, then gather kernels sum them row by row, every entry over its cells in
+ *     ascending cell order (8*ncell*nnode*(nnode+1)/2*ndim^2 bytes more device memory).
+ *   PMS_ASSEMBLY_DIRECT: the element kernel adds each cell's blocks straight into the CSR values
+ *     and R (per-row tickets), every entry over its cells in the processing order of
+ *     pms_mesh_assembly_maps; no element matrices are stored. */
 enum pms_assembly { PMS_ASSEMBLY_DIRECT = 0, PMS_ASSEMBLY_GATHER = 1 };
 int pms_elements_set_assembly(pms_elements* h, int32_t mode);
 

@@ -91,8 +91,9 @@ class Elements:
         return self._pattern
 
     def set_assembly(self, mode):
-        """"direct" (default: blocks added straight into the CSR values and R in ascending cell
-        order) or "gather" (dense element matrices, then row gathers); the same bits either way."""
+        """"gather" (default: upper element-matrix blocks, then row gathers summing every entry in
+        ascending cell order) or "direct" (blocks added straight into the CSR values and R in the
+        colour-major processing order); each reproducible, the two equal to the last bits."""
         code = {"direct": _lib.PMS_ASSEMBLY_DIRECT, "gather": _lib.PMS_ASSEMBLY_GATHER}[mode]
         self._check(self.L.pms_elements_set_assembly(self.h, code))
 
