@@ -409,6 +409,29 @@ def assembly_ab(torch, L, el, stream, steps, warmup, d_ddu, d_ff, d_csr, other="
             "other_kernels_ms_per_step": kernel_ms(kt, kc)}
 
 
+def lower_triangle_step(torch, L, el, stream, steps, warmup, d_ddu, d_ff):
+    """The same device-resident step with K stored as its lower triangle (Sym::YesLower): the row
+    gather skips the blocks above the diagonal and writes about half the CSR values."""
+    from pmsim_b200 import _lib
+    el.set_symmetry("lower")
+    d_low = torch.empty(el.nnz, device=d_ddu.device, dtype=torch.float64)
+    for _ in range(max(2, warmup)):
+        el.update_and_assemble(d_ddu, d_ff, d_low)
+    ms = time_steps(torch, el, stream, steps, d_ddu, d_ff, d_low)
+    L.pms_elements_set_timing(el.h, 1)
+    L.pms_elements_kernel_times(el.h, None, None)
+    for _ in range(steps):
+        el.update_and_assemble(d_ddu, d_ff, d_low)
+    kt = np.zeros(3)
+    kc = np.zeros(3, np.int64)
+    L.pms_elements_kernel_times(el.h, _lib.ptr(kt), _lib.ptr(kc))
+    L.pms_elements_set_timing(el.h, 0)
+    nnz = el.nnz
+    el.set_symmetry("full")
+    del d_low
+    return {"nnz": nnz, "ms_per_step": ms, "kernels_ms_per_step": kernel_ms(kt, kc)}
+
+
 def kernel_ms(kt, kc):
     """Per-step times of the element kernel and the two gathers (absent under the direct assembly)."""
     out = {"element": kt[0] / max(kc[0], 1)}
@@ -881,6 +904,7 @@ def main():
 
     # the same step with the direct assembly, for the A/B of the two assemblies
     ab = assembly_ab(torch, L, el, stream, min(args.steps, 10), args.warmup, d_ddu, d_ff, d_csr)
+    ab["lower_triangle"] = lower_triangle_step(torch, L, el, stream, min(args.steps, 10), args.warmup, d_ddu, d_ff)
 
     # e2e through the C ABI with host buffers (pinned): dU in, R and CSR values out, every step
     e2e = None
@@ -896,6 +920,21 @@ def main():
         t_e2e = dist.max_over_ranks((time.perf_counter() - t0) / args.steps, dev)
         e2e = {"value": world * nip / t_e2e, "unit": "IP/s", "h2d_bytes_per_step": ndof * 8,
                "d2h_bytes_per_step": (ndof + nnz) * 8, "ms_per_step": t_e2e * 1e3}
+        del h_csr
+        # the same call with K stored as its lower triangle (Sym::YesLower, pmsim's storage when the
+        # linear solver is MUMPS); the headline above keeps both triangles (pmsim's default, UMFPACK)
+        el.set_symmetry("lower")
+        nnz_lower = el.nnz
+        h_csr = torch.empty(nnz_lower, dtype=torch.float64).pin_memory().numpy()
+        el.update_and_assemble(h_ddu, h_ff, h_csr)
+        barrier()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            el.update_and_assemble(h_ddu, h_ff, h_csr)
+        t_low = dist.max_over_ranks((time.perf_counter() - t0) / args.steps, dev)
+        el.set_symmetry("full")
+        e2e["lower_triangle"] = {"value": world * nip / t_low, "unit": "IP/s", "h2d_bytes_per_step": ndof * 8,
+                                 "d2h_bytes_per_step": (ndof + nnz_lower) * 8, "ms_per_step": t_low * 1e3}
         del h_csr
 
     if world > 1:

@@ -161,6 +161,20 @@ int pms_elements_set_state(pms_elements* h, const double* sig, const double* ivs
 enum pms_assembly { PMS_ASSEMBLY_DIRECT = 0, PMS_ASSEMBLY_GATHER = 1 };
 int pms_elements_set_assembly(pms_elements* h, int32_t mode);
 
+/* Storage of K in the CSR values, as russell_sparse's Sym that LinearSystem::new picks from the
+ * linear solver when every element Jacobian is symmetric (src/fem/linear_system.rs:96-119), with the
+ * entries kept as assemble_matrix keeps them (src/base/assembly.rs:92-136):
+ *   PMS_SYM_FULL (default): both triangles (Sym::YesFull, Sym::No);
+ *   PMS_SYM_LOWER: the entries with column <= row (Sym::YesLower, the choice for MUMPS);
+ *   PMS_SYM_UPPER: the entries with column >= row (Sym::YesUpper).
+ * It sets what pms_elements_get_info's nnz, pms_elements_csr_pattern and the CSR values of
+ * pms_elements_assemble_kk / pms_elements_update_and_assemble hold; a kept entry has the bits of
+ * the same entry of the full matrix.  The triangles need the gather assembly: PMS_ERR_UNSUPPORTED
+ * when PMS_ASSEMBLY_DIRECT is set (either call refuses the other's combination).  The per-cell calls
+ * always return full element matrices. */
+enum pms_sym { PMS_SYM_FULL = 0, PMS_SYM_LOWER = 1, PMS_SYM_UPPER = 2 };
+int pms_elements_set_symmetry(pms_elements* h, int32_t sym);
+
 /* Instrumentation: when on, every batched call records CUDA events around its kernels on the
  * handle's stream; pms_elements_kernel_times waits for the stream and returns the summed device
  * time (ms) and launch count of [0] element kernel, [1] F_int gather, [2] CSR gather since the

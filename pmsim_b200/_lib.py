@@ -20,9 +20,11 @@ PMS_ERR_INVALID = 1
 PMS_ERR_ZERO_SIGMA_D = 3
 PMS_ERR_ZERO_NORM_S = 4
 PMS_ERR_JACOBIAN = 5
+PMS_ERR_UNSUPPORTED = 7
 PMS_ERR_ORDER = 13
 PMS_ASSEMBLY_DIRECT = 0
 PMS_ASSEMBLY_GATHER = 1
+PMS_SYM_FULL, PMS_SYM_LOWER, PMS_SYM_UPPER = 0, 1, 2
 LINEAR_ELASTIC = 0
 VON_MISES = 1
 
@@ -125,6 +127,7 @@ SIGNATURES = {
     "pms_mesh_csr_pattern": (_I, [ctypes.POINTER(Mesh_), _V, _V, ctypes.POINTER(_I64)]),
     "pms_elements_set_timing": (_I, [_V, _I]),
     "pms_elements_set_assembly": (_I, [_V, _I]),
+    "pms_elements_set_symmetry": (_I, [_V, _I]),
     "pms_set_device": (_I, [_I]),
     "pms_shape_table": (_I, [_I, _I, _V, _V]),
     "pms_mesh_assembly_maps": (_I, [ctypes.POINTER(Mesh_), _V, _V, _V, _V]),

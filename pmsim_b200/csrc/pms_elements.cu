@@ -1719,7 +1719,11 @@ template <int ND, int NN> struct GatherShape {
     static constexpr int NB = 4;                      // incidences loaded before they are added
 };
 
-template <int ND, int NN>
+// TRI: the CSR values hold one triangle of K (sym = PMS_SYM_LOWER: columns <= row, PMS_SYM_UPPER:
+// columns >= row; src/base/assembly.rs:92-122): the lanes skip the blocks that fall outside it, and
+// row (A, i) starts at tbase[A] plus the lengths of rows (A, 0..i-1); kdiag[A] = A's own position
+// in its block row.
+template <int ND, int NN, bool TRI>
 __global__ void __launch_bounds__(256, ND == 2 ? 4 : 1) kk_gather_kernel(int64_t npoint, int nbmax, const int64_t* __restrict__ bptr,
                                                         const int64_t* __restrict__ inc_ptr,
                                                         const int32_t* __restrict__ inc,
@@ -1728,7 +1732,9 @@ __global__ void __launch_bounds__(256, ND == 2 ? 4 : 1) kk_gather_kernel(int64_t
                                                         const int32_t* __restrict__ node_prob,
                                                         const uint8_t* __restrict__ pmode, int nq,
                                                         const int64_t* __restrict__ q_off,
-                                                        const int64_t* __restrict__ q_first, int64_t node0) {
+                                                        const int64_t* __restrict__ q_first, int64_t node0,
+                                                        int sym, const int32_t* __restrict__ kdiag,
+                                                        const int64_t* __restrict__ tbase) {
     constexpr int BB = ND * ND, NU = NN * (NN + 1) / 2;
     constexpr int G = GatherShape<ND, NN>::G, NB = GatherShape<ND, NN>::NB;
     extern __shared__ double rowbuf[];
@@ -1748,10 +1754,11 @@ __global__ void __launch_bounds__(256, ND == 2 ? 4 : 1) kk_gather_kernel(int64_t
             if (pmode && pmode[node_prob[A]] == 0) on = false;
         }
         int64_t ba = 0;
-        int nba = 0;
+        int nba = 0, dp = 0;
         if (on) {
             ba = bptr[A];
             nba = (int)(bptr[A + 1] - ba);
+            if constexpr (TRI) dp = kdiag[A];
         }
         // buffer offsets of the group rows (exclusive scan over the groups) and the run test
         int off = 0, total = 0;
@@ -1764,7 +1771,7 @@ __global__ void __launch_bounds__(256, ND == 2 ? 4 : 1) kk_gather_kernel(int64_t
         const int64_t A0 = __shfl_sync(FULL, A, 0);
         const bool on0 = __shfl_sync(FULL, on, 0);
         const bool fits = !lane_on || Ai >= npoint || (on && A == A0 + g);
-        const bool run = __all_sync(FULL, fits) && on0;
+        const bool run = !TRI && __all_sync(FULL, fits) && on0;
         for (int t = lane; t < total * BB; t += 32) buf[t] = 0.0;
         __syncwarp();
         if (on) {
@@ -1783,6 +1790,14 @@ __global__ void __launch_bounds__(256, ND == 2 ? 4 : 1) kk_gather_kernel(int64_t
                         const int64_t cell = code / NN;
                         const int a = code - (int)cell * NN;
                         pos[r] = __ldg(slot + k * NN + b);
+                        if constexpr (TRI) {
+                            if (sym == PMS_SYM_LOWER ? pos[r] > dp : pos[r] < dp) {
+                                pos[r] = -1;  // outside the stored triangle: neither loaded nor added
+#pragma unroll
+                                for (int i = 0; i < BB; i++) v[r][i] = 0.0;
+                                continue;
+                            }
+                        }
                         // block (a, b) of the upper layout: stored as (a, b) when a <= b, else as (b, a);
                         // the lanes b >= a read adjacent segments of the same scalar rows
                         const bool upper = a <= b;
@@ -1814,6 +1829,33 @@ __global__ void __launch_bounds__(256, ND == 2 ? 4 : 1) kk_gather_kernel(int64_t
         if (run) {
             double* dst = csr + (int64_t)BB * __shfl_sync(FULL, ba, 0);
             for (int t = lane; t < total * BB; t += 32) dst[t] = buf[t];
+        } else if constexpr (TRI) {
+            // buffer entry (i, c = p*ND + j) of a row group is K(A*ND + i, B_p*ND + j).  The group's
+            // stored entries are contiguous from tbase[A]: row i holds, lower, c = 0 .. ND*dq + i
+            // (from i*ND*dq + i(i+1)/2 on), upper, c = dq*ND + i .. ND*nq - 1 (from
+            // i*ND*(nq - dq) - i(i-1)/2 on); each lane takes destinations and finds their row
+            const bool lower = sym == PMS_SYM_LOWER;
+            const int64_t tb = on ? tbase[A] : 0;
+            int oq = 0;
+#pragma unroll 1
+            for (int q = 0; q < G; q++) {
+                const int nq_ = __shfl_sync(FULL, nba, q * NN);
+                const int dq = __shfl_sync(FULL, dp, q * NN);
+                double* dst = csr + __shfl_sync(FULL, tb, q * NN);
+                const double* src = buf + (int64_t)oq * BB;
+                const int nrow = ND * nq_, w = lower ? ND * dq : ND * (nq_ - dq);
+                const int cnt = nq_ ? (lower ? BB * dq : BB * (nq_ - dq - 1)) + ND * (ND + 1) / 2 : 0;
+                for (int u = lane; u < cnt; u += 32) {
+                    int i = 0, s0 = 0;
+#pragma unroll
+                    for (int ii = 1; ii < ND; ii++) {
+                        const int s = lower ? ii * w + ii * (ii + 1) / 2 : ii * w - ii * (ii - 1) / 2;
+                        if (u >= s) i = ii, s0 = s;
+                    }
+                    dst[u] = src[i * nrow + (u - s0) + (lower ? 0 : dq * ND + i)];
+                }
+                oq += nq_;
+            }
         } else {
             int oq = 0;
 #pragma unroll 1
@@ -1902,6 +1944,9 @@ struct pms_elements {
     int32_t* d_ticket = nullptr;   // direct assembly: per-node tickets (zero between launches)
     unsigned long long* d_next = nullptr;  // direct assembly: in-order work counter
     int assembly = PMS_ASSEMBLY_GATHER;  // measured faster on B200 for every kind benchmarked
+    int sym = PMS_SYM_FULL;              // storage of the public CSR values (pms_elements_set_symmetry)
+    std::vector<int64_t> tbase;          // triangle layouts: first value of each node's rows [npoint + 1]
+    int64_t* d_tbase = nullptr;
     int64_t* d_inc_ptr = nullptr;
     int32_t* d_inc = nullptr;
     int64_t* d_bptr = nullptr;
@@ -2158,10 +2203,17 @@ ElemArgs make_args(pms_elements* h, const double* ddu) {
     return a;
 }
 
+// Number of public CSR values, and where the values of node A's rows start among them.
+static int64_t public_nnz(const pms_elements* h) { return h->sym == PMS_SYM_FULL ? h->nnz : h->tbase[h->npoint]; }
+static int64_t value_offset(const pms_elements* h, int64_t A) {
+    return h->sym == PMS_SYM_FULL ? (int64_t)h->nd * h->nd * h->pat.bptr[A] : h->tbase[A];
+}
+
 template <int ND, int NN>
 void launch_kk_gather_t(pms_elements* h, double* csr, const int32_t* node_prob, const uint8_t* pmode,
-                        const pms::WorkQueue* q, int64_t node0, int64_t nrows) {
-    auto kern = kk_gather_kernel<ND, NN>;
+                        const pms::WorkQueue* q, int64_t node0, int64_t nrows, bool pub) {
+    const bool tri = pub && h->sym != PMS_SYM_FULL;
+    auto kern = tri ? kk_gather_kernel<ND, NN, true> : kk_gather_kernel<ND, NN, false>;
     if (h->gather_smem > 48 * 1024)
         cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, h->gather_smem);
     const int64_t np = q ? q->nnode : (nrows >= 0 ? nrows : h->npoint), wpb = h->gather_wpb;
@@ -2169,25 +2221,27 @@ void launch_kk_gather_t(pms_elements* h, double* csr, const int32_t* node_prob, 
     const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>((nw + wpb - 1) / wpb, 148 * 32));
     kern<<<blocks, (unsigned)(32 * wpb), h->gather_smem, h->stream>>>(
         np, h->pat.nbmax, h->d_bptr, h->d_inc_ptr, h->d_inc, h->d_slot, h->d_ke, csr, node_prob, pmode,
-        q ? q->nq : 0, q ? q->node_off : nullptr, q ? q->node_first : nullptr, node0);
+        q ? q->nq : 0, q ? q->node_off : nullptr, q ? q->node_first : nullptr, node0, tri ? h->sym : PMS_SYM_FULL,
+        h->d_kdiag, h->d_tbase);
 }
 
-// CSR gather of the block rows [node0, node0 + nrows) (nrows < 0: all), or of a work queue
+// CSR gather of the block rows [node0, node0 + nrows) (nrows < 0: all), or of a work queue; pub: into
+// the public layout of the values (pms_elements_set_symmetry), else the full one
 void launch_kk_gather(pms_elements* h, double* csr, const int32_t* node_prob = nullptr,
                       const uint8_t* pmode = nullptr, const pms::WorkQueue* q = nullptr, int64_t node0 = 0,
-                      int64_t nrows = -1) {
+                      int64_t nrows = -1, bool pub = false) {
     switch (h->kind) {
-    case PMS_TRI3: launch_kk_gather_t<2, 3>(h, csr, node_prob, pmode, q, node0, nrows); break;
-    case PMS_TRI6: launch_kk_gather_t<2, 6>(h, csr, node_prob, pmode, q, node0, nrows); break;
-    case PMS_QUA4: launch_kk_gather_t<2, 4>(h, csr, node_prob, pmode, q, node0, nrows); break;
-    case PMS_QUA8: launch_kk_gather_t<2, 8>(h, csr, node_prob, pmode, q, node0, nrows); break;
-    case PMS_QUA9: launch_kk_gather_t<2, 9>(h, csr, node_prob, pmode, q, node0, nrows); break;
-    case PMS_TET4: launch_kk_gather_t<3, 4>(h, csr, node_prob, pmode, q, node0, nrows); break;
-    case PMS_TET10: launch_kk_gather_t<3, 10>(h, csr, node_prob, pmode, q, node0, nrows); break;
-    case PMS_HEX8: launch_kk_gather_t<3, 8>(h, csr, node_prob, pmode, q, node0, nrows); break;
-    case PMS_HEX20: launch_kk_gather_t<3, 20>(h, csr, node_prob, pmode, q, node0, nrows); break;
-    case PMS_TRI10: launch_kk_gather_t<2, 10>(h, csr, node_prob, pmode, q, node0, nrows); break;
-    case PMS_TRI15: launch_kk_gather_t<2, 15>(h, csr, node_prob, pmode, q, node0, nrows); break;
+    case PMS_TRI3: launch_kk_gather_t<2, 3>(h, csr, node_prob, pmode, q, node0, nrows, pub); break;
+    case PMS_TRI6: launch_kk_gather_t<2, 6>(h, csr, node_prob, pmode, q, node0, nrows, pub); break;
+    case PMS_QUA4: launch_kk_gather_t<2, 4>(h, csr, node_prob, pmode, q, node0, nrows, pub); break;
+    case PMS_QUA8: launch_kk_gather_t<2, 8>(h, csr, node_prob, pmode, q, node0, nrows, pub); break;
+    case PMS_QUA9: launch_kk_gather_t<2, 9>(h, csr, node_prob, pmode, q, node0, nrows, pub); break;
+    case PMS_TET4: launch_kk_gather_t<3, 4>(h, csr, node_prob, pmode, q, node0, nrows, pub); break;
+    case PMS_TET10: launch_kk_gather_t<3, 10>(h, csr, node_prob, pmode, q, node0, nrows, pub); break;
+    case PMS_HEX8: launch_kk_gather_t<3, 8>(h, csr, node_prob, pmode, q, node0, nrows, pub); break;
+    case PMS_HEX20: launch_kk_gather_t<3, 20>(h, csr, node_prob, pmode, q, node0, nrows, pub); break;
+    case PMS_TRI10: launch_kk_gather_t<2, 10>(h, csr, node_prob, pmode, q, node0, nrows, pub); break;
+    case PMS_TRI15: launch_kk_gather_t<2, 15>(h, csr, node_prob, pmode, q, node0, nrows, pub); break;
     }
     h->launches++;
 }
@@ -2366,7 +2420,7 @@ int pms_elements_get_info(const pms_elements* h, pms_elements_info* o) {
     o->ncell = h->ncell;
     o->ndof = h->ndof;
     o->nip = h->nip;
-    o->nnz = h->nnz;
+    o->nnz = public_nnz(h);
     o->nblock_upper = h->pat.nupper();
     o->ncontrib = h->ncell * h->nn * h->nn;
     o->device_bytes = h->device_bytes;
@@ -2379,32 +2433,37 @@ int pms_elements_set_stream(pms_elements* h, void* stream) {
     return PMS_OK;
 }
 
-int pms_elements_csr_pattern(pms_elements* h, int64_t* indptr, int32_t* indices, int32_t mem) {
-    if (!h) return PMS_ERR_INVALID;
+// The CSR pattern of K in the layout sym (the device-side users inside the library take the full one).
+static int csr_pattern(pms_elements* h, int64_t* indptr, int32_t* indices, int32_t mem, int sym) {
     const int nd = h->nd;
+    const int64_t nnz = sym == PMS_SYM_FULL ? h->nnz : h->tbase[h->npoint];
     std::vector<int64_t> ip;
     std::vector<int32_t> ix;
     int64_t* ipo = indptr;
     int32_t* ixo = indices;
     if (mem == PMS_MEM_DEVICE) {
         ip.resize(h->ndof + 1);
-        ix.resize(indices ? h->nnz : 0);
+        ix.resize(indices ? nnz : 0);
         ipo = ip.data();
         ixo = indices ? ix.data() : nullptr;
     }
     const Pattern& p = h->pat;
     for (int64_t A = 0; A < h->npoint; A++) {
-        int64_t b0 = p.bptr[A], nb = p.bptr[A + 1] - b0;
+        const int64_t b0 = p.bptr[A], nb = p.bptr[A + 1] - b0;
+        int64_t start = sym == PMS_SYM_FULL ? (int64_t)nd * nd * b0 : h->tbase[A];
         for (int i = 0; i < nd; i++) {
-            int64_t r = A * nd + i;
-            int64_t start = (int64_t)nd * nd * b0 + (int64_t)i * nd * nb;
+            const int64_t r = A * nd + i;
             if (ipo) ipo[r] = start;
-            if (ixo)
-                for (int64_t k = 0; k < nb; k++)
-                    for (int j = 0; j < nd; j++) ixo[start + k * nd + j] = p.bcol[b0 + k] * nd + j;
+            for (int64_t k = 0; k < nb; k++)
+                for (int j = 0; j < nd; j++) {
+                    const int64_t c = (int64_t)p.bcol[b0 + k] * nd + j;
+                    if ((sym == PMS_SYM_LOWER && c > r) || (sym == PMS_SYM_UPPER && c < r)) continue;
+                    if (ixo) ixo[start] = (int32_t)c;
+                    start++;
+                }
         }
     }
-    if (ipo) ipo[h->ndof] = h->nnz;
+    if (ipo) ipo[h->ndof] = nnz;
     if (mem == PMS_MEM_DEVICE) {
         if (indptr && cudaMemcpy(indptr, ip.data(), ip.size() * 8, cudaMemcpyHostToDevice) != cudaSuccess)
             return fail(h, PMS_ERR_CUDA, "copy of indptr failed");
@@ -2412,6 +2471,11 @@ int pms_elements_csr_pattern(pms_elements* h, int64_t* indptr, int32_t* indices,
             return fail(h, PMS_ERR_CUDA, "copy of indices failed");
     }
     return PMS_OK;
+}
+
+int pms_elements_csr_pattern(pms_elements* h, int64_t* indptr, int32_t* indices, int32_t mem) {
+    if (!h) return PMS_ERR_INVALID;
+    return csr_pattern(h, indptr, indices, mem, h->sym);
 }
 
 int pms_elements_initialize(pms_elements* h) {
@@ -2536,13 +2600,13 @@ static int run(pms_elements* h, const double* ddu, double* ff, double* csr, int 
     if (upd != UPD_NONE || dof || dok) timed(0, [&] { launch_elem(h, a, upd, dof, dok, direct); });
     if (dof && !direct) timed(1, [&] { launch_f_gather(h, d_ff); });
     if (mem == PMS_MEM_DEVICE || !dok || direct) {
-        if (dok && !direct) timed(2, [&] { launch_kk_gather(h, d_csr); });
+        if (dok && !direct) timed(2, [&] { launch_kk_gather(h, d_csr, nullptr, nullptr, nullptr, 0, -1, true); });
         int rc = cuda_check(h);
         if (rc) return rc;
         if (mem == PMS_MEM_HOST) {
             if (dof) cudaMemcpyAsync(ff, d_ff, (size_t)h->ndof * 8, cudaMemcpyDeviceToHost, h->stream);
             if (dok && direct)
-                cudaMemcpyAsync(csr, d_csr, (size_t)h->nnz * 8, cudaMemcpyDeviceToHost, h->stream);
+                cudaMemcpyAsync(csr, d_csr, (size_t)public_nnz(h) * 8, cudaMemcpyDeviceToHost, h->stream);
             return finish_host(h);
         }
         return PMS_OK;
@@ -2557,14 +2621,13 @@ static int run(pms_elements* h, const double* ddu, double* ff, double* csr, int 
                 return fail(h, PMS_ERR_CUDA, "event creation failed");
     }
     constexpr int NS = pms_elements::NSLAB;
-    const int64_t BB = (int64_t)h->nd * h->nd;
     timed(2, [&] {
         for (int k = 0; k < NS; k++) {
             const int64_t A0 = h->npoint * k / NS, A1 = h->npoint * (k + 1) / NS;
-            if (A1 > A0) launch_kk_gather(h, d_csr, nullptr, nullptr, nullptr, A0, A1 - A0);
+            if (A1 > A0) launch_kk_gather(h, d_csr, nullptr, nullptr, nullptr, A0, A1 - A0, true);
             cudaEventRecord(h->slab_ev[k], h->stream);
             cudaStreamWaitEvent(h->copy_stream, h->slab_ev[k], 0);
-            const int64_t v0 = BB * h->pat.bptr[A0], v1 = BB * h->pat.bptr[A1];
+            const int64_t v0 = value_offset(h, A0), v1 = value_offset(h, A1);
             if (v1 > v0)
                 cudaMemcpyAsync(csr + v0, d_csr + v0, (size_t)(v1 - v0) * 8, cudaMemcpyDeviceToHost, h->copy_stream);
         }
@@ -2682,7 +2745,33 @@ int64_t pms_elements_launch_count(const pms_elements* h) { return h ? h->launche
 
 int pms_elements_set_assembly(pms_elements* h, int32_t mode) {
     if (!h || (mode != PMS_ASSEMBLY_DIRECT && mode != PMS_ASSEMBLY_GATHER)) return PMS_ERR_INVALID;
+    if (mode == PMS_ASSEMBLY_DIRECT && h->sym != PMS_SYM_FULL)
+        return fail(h, PMS_ERR_UNSUPPORTED, "the direct assembly writes both triangles of K");
     h->assembly = mode;
+    return PMS_OK;
+}
+
+int pms_elements_set_symmetry(pms_elements* h, int32_t sym) {
+    if (!h || (sym != PMS_SYM_FULL && sym != PMS_SYM_LOWER && sym != PMS_SYM_UPPER)) return PMS_ERR_INVALID;
+    if (sym != PMS_SYM_FULL && h->assembly == PMS_ASSEMBLY_DIRECT)
+        return fail(h, PMS_ERR_UNSUPPORTED, "the direct assembly writes both triangles of K");
+    if (sym != PMS_SYM_FULL) {
+        // node A's rows hold its blocks on the stored side of the diagonal block, and the diagonal
+        // block's own triangle (nd(nd+1)/2 entries)
+        const Pattern& p = h->pat;
+        const int64_t nd = h->nd, bb = nd * nd;
+        std::vector<int64_t> tb(h->npoint + 1, 0);
+        for (int64_t A = 0; A < h->npoint; A++) {
+            const int64_t nb = p.bptr[A + 1] - p.bptr[A], dp = p.kdiag[A];
+            tb[A + 1] = tb[A] + bb * (sym == PMS_SYM_LOWER ? dp : nb - dp - 1) + nd * (nd + 1) / 2;
+        }
+        if (!h->d_tbase && !h->alloc(&h->d_tbase, (size_t)h->npoint + 1))
+            return fail(h, PMS_ERR_NOMEM, "out of device memory");
+        if (cudaMemcpy(h->d_tbase, tb.data(), tb.size() * 8, cudaMemcpyHostToDevice) != cudaSuccess)
+            return fail(h, PMS_ERR_CUDA, "copy of the triangle offsets failed");
+        h->tbase.swap(tb);
+    }
+    h->sym = sym;
     return PMS_OK;
 }
 
@@ -2797,7 +2886,7 @@ int elements_device_pattern(pms_elements* h, const int64_t** indptr, const int32
     if (!h->d_indptr) {
         if (!h->alloc(&h->d_indptr, (size_t)h->ndof + 1) || !h->alloc(&h->d_indices, (size_t)h->nnz))
             return fail(h, PMS_ERR_NOMEM, "out of device memory for the CSR pattern");
-        int rc = pms_elements_csr_pattern(h, h->d_indptr, h->d_indices, PMS_MEM_DEVICE);
+        int rc = csr_pattern(h, h->d_indptr, h->d_indices, PMS_MEM_DEVICE, PMS_SYM_FULL);
         if (rc) return rc;
     }
     *indptr = h->d_indptr;

@@ -97,6 +97,19 @@ class Elements:
         code = {"direct": _lib.PMS_ASSEMBLY_DIRECT, "gather": _lib.PMS_ASSEMBLY_GATHER}[mode]
         self._check(self.L.pms_elements_set_assembly(self.h, code))
 
+    def set_symmetry(self, sym):
+        """Storage of K in the CSR values, as russell_sparse's Sym (src/fem/linear_system.rs:119,
+        src/base/assembly.rs:92-136): "full" (default, both triangles), "lower" (column <= row,
+        Sym::YesLower) or "upper" (column >= row, Sym::YesUpper).  Changes ``nnz``,
+        ``csr_pattern()`` and the values of ``assemble_kk`` / ``update_and_assemble``; the triangles
+        need the gather assembly."""
+        code = {"full": _lib.PMS_SYM_FULL, "lower": _lib.PMS_SYM_LOWER, "upper": _lib.PMS_SYM_UPPER}[sym]
+        self._check(self.L.pms_elements_set_symmetry(self.h, code))
+        info = _lib.Info_()
+        self._check(self.L.pms_elements_get_info(self.h, ctypes.byref(info)))
+        self.info, self.nnz = info, info.nnz
+        self._pattern = None
+
     def set_stream(self, stream):
         """stream: torch.cuda.Stream, a raw cudaStream_t, or None for the handle's own stream."""
         raw = getattr(stream, "cuda_stream", stream)
