@@ -2872,6 +2872,7 @@ ElementsView elements_view(pms_elements* h) {
     v.ndof = h->ndof;
     v.nnz = h->nnz;
     v.d_bptr = h->d_bptr;
+    v.d_bcol = h->d_bcol;
     v.d_kdiag = h->d_kdiag;
     v.stream = h->stream;
     return v;

@@ -19,6 +19,7 @@ struct ElementsView {
     int nd, nn, ng;
     int64_t npoint, ncell, ndof, nnz;
     const int64_t* d_bptr;   // block-row pointers (npoint + 1)
+    const int32_t* d_bcol;   // block columns (node ids, sorted in each block row)
     const int32_t* d_kdiag;  // position of the diagonal block in each block row
     cudaStream_t stream;
 };

@@ -153,80 +153,50 @@ __device__ __forceinline__ double row_dot(int64_t row, int sub, bool on, const i
     return s;
 }
 
-// Rows with entries [k0[j], k1[j]) by TPR lanes (row j: the same FMA chain and shuffle tree as
-// row_dot), M entries per lane loaded ahead of each round of FMAs, so that the loads of R rows x M
-// entries are in flight together; gather(col) supplies x[col].
-template <int TPR, int R, int M, class Gather>
-__device__ __forceinline__ void rows_dot_pf(const int64_t (&k0)[R], const int64_t (&k1)[R], int sub,
-                                            const double* __restrict__ val, const int32_t* __restrict__ indices,
-                                            const Gather& gather, double (&s)[R]) {
-    int64_t k[R];
-    bool more = false;
+// The ND rows of node A of K in the node-block layout of the element handle: block row A holds nba
+// ND x ND blocks from bb = bptr[A], row i of the node at val[ND*ND*bb + i*ND*nba + pos*ND + j], block
+// columns bcol[bb + pos].  TPR lanes: lane sub takes the blocks pos = sub, sub + TPR, ... two per round
+// (both loaded before either is added), each block's FMAs in (i, j) order, then a shuffle tree per row.
+// Every lane of the warp calls it (nba = 0 for a lane group without a node); gather(B, x) supplies
+// x[B*ND + 0 .. ND-1].  The PCG engines all use it, so their iterates agree bit for bit.
+template <int ND, int TPR, class GatherN>
+__device__ __forceinline__ void node_rows_dot(int64_t bb, int nba, int sub, const double* __restrict__ val,
+                                              const int32_t* __restrict__ bcol, const GatherN& gather,
+                                              double (&s)[ND]) {
 #pragma unroll
-    for (int j = 0; j < R; j++) {
-        s[j] = 0.0;
-        k[j] = k0[j] + sub;
-        more = more || k[j] < k1[j];
-    }
-    while (more) {
-        double v[R][M], x[R][M];
-        int32_t c[R][M];
+    for (int i = 0; i < ND; i++) s[i] = 0.0;
+    const double* v = val + (int64_t)ND * ND * bb;
+    const int rs = ND * nba;
+    for (int pos = sub; pos < nba; pos += 2 * TPR) {
+        const int p1 = pos + TPR;
+        const bool two = p1 < nba;
+        const int32_t c0 = bcol[bb + pos];
+        const int32_t c1 = two ? bcol[bb + p1] : c0;
+        double a0[ND][ND], a1[ND][ND], x0[ND], x1[ND];
 #pragma unroll
-        for (int j = 0; j < R; j++)
+        for (int i = 0; i < ND; i++)
 #pragma unroll
-            for (int m = 0; m < M; m++) {
-                const int64_t kk = k[j] + (int64_t)m * TPR;
-                const bool ok = kk < k1[j];
-                v[j][m] = ok ? val[kk] : 0.0;
-                c[j][m] = ok ? indices[kk] : -1;
+            for (int j = 0; j < ND; j++) {
+                a0[i][j] = v[i * rs + pos * ND + j];
+                a1[i][j] = two ? v[i * rs + p1 * ND + j] : 0.0;
             }
+        gather(c0, x0);
+        gather(c1, x1);
 #pragma unroll
-        for (int j = 0; j < R; j++)
+        for (int i = 0; i < ND; i++)
 #pragma unroll
-            for (int m = 0; m < M; m++) x[j][m] = (c[j][m] >= 0) ? gather(c[j][m]) : 0.0;
-        more = false;
+            for (int j = 0; j < ND; j++) s[i] = fma(a0[i][j], x0[j], s[i]);
+        if (two) {
 #pragma unroll
-        for (int j = 0; j < R; j++) {
+            for (int i = 0; i < ND; i++)
 #pragma unroll
-            for (int m = 0; m < M; m++)
-                if (c[j][m] >= 0) s[j] = fma(v[j][m], x[j][m], s[j]);
-            k[j] += (int64_t)M * TPR;
-            more = more || k[j] < k1[j];
+                for (int j = 0; j < ND; j++) s[i] = fma(a1[i][j], x1[j], s[i]);
         }
     }
 #pragma unroll
-    for (int j = 0; j < R; j++)
+    for (int i = 0; i < ND; i++)
 #pragma unroll
-        for (int o = TPR / 2; o > 0; o >>= 1) s[j] += __shfl_down_sync(FULL, s[j], o, TPR);
-}
-
-// q = K p on rows [row0, row1) by BD threads, R rows per lane group per pass; store(row, v)
-// receives q_row (0 on prescribed rows).
-template <int BD, int TPR, int R, class Gather, class Store>
-__device__ __forceinline__ void spmv_rows(const int32_t* pres_idx, int64_t row0, int64_t row1,
-                                          const int64_t* __restrict__ indptr, const int32_t* __restrict__ indices,
-                                          const double* __restrict__ val, const Gather& gather, const Store& store) {
-    constexpr int GR = BD / TPR;  // lane groups
-    const int sub = threadIdx.x % TPR, grp = threadIdx.x / TPR;
-    for (int64_t base = row0; base < row1; base += (int64_t)R * GR) {
-        int64_t row[R];
-        bool on[R];
-        double sv[R];
-        int64_t k0[R], k1[R];
-#pragma unroll
-        for (int j = 0; j < R; j++) {
-            row[j] = base + j * GR + grp;
-            on[j] = row[j] < row1;
-            k0[j] = on[j] ? indptr[row[j]] : 0;
-            k1[j] = on[j] ? indptr[row[j] + 1] : 0;
-        }
-        rows_dot_pf<TPR, R, 4>(k0, k1, sub, val, indices, gather, sv);
-        if (sub == 0) {
-#pragma unroll
-            for (int j = 0; j < R; j++)
-                if (on[j]) store(row[j], (pres_idx[row[j]] >= 0) ? 0.0 : sv[j]);
-        }
-    }
+        for (int o = TPR / 2; o > 0; o >>= 1) s[i] += __shfl_down_sync(FULL, s[i], o, TPR);
 }
 
 // a.b over the free DOFs of a node; pres, a, b point at the node's first DOF
@@ -422,26 +392,38 @@ pcg_init_scalars_kernel(int np, const uint8_t* active, const uint8_t* engine, co
 
 // ---- batch-wide PCG engine (one CUDA graph node per kernel) --------------------------------
 
-// q = K p on the rows of one chunk quarter (32 nodes; one pass of TPR lanes x 4 rows per lane group),
+// q = K p on the nodes of one chunk quarter (32 nodes, one group of TPR lanes each, node_rows_dot),
 // then the quarter's partial of p.q by the warp tree.  Block b covers quarter b % 4 of chunk b / 4.
 template <int TPR>
-__host__ __device__ constexpr int quarter_threads() { return 32 * (TPR == 8 ? 2 : 3) * TPR / 4; }
+__host__ __device__ constexpr int quarter_threads() { return 32 * TPR; }
 
 template <int TPR>
 __global__ void __launch_bounds__(quarter_threads<TPR>())
-pcg_spmv_dot_kernel(SolverArgs S, int par, const int64_t* __restrict__ indptr, const int32_t* __restrict__ indices,
+pcg_spmv_dot_kernel(SolverArgs S, int par, const int64_t* __restrict__ bptr, const int32_t* __restrict__ bcol,
                     const double* __restrict__ val, const double* p, double* q, double* part4) {
-    constexpr int QB = quarter_threads<TPR>();
+    constexpr int ND = TPR == 8 ? 2 : 3;  // the lanes per node follow the dimension
     const int64_t ch = blockIdx.x >> 2;
     const int k = blockIdx.x & 3;
     const int pr = S.chunk_prob[ch];
     if (!S.pcg_active[par * S.np + pr]) return;  // whole block
     const int nn = max(0, min(32, S.chunk_nnode[ch] - 32 * k));
     const int64_t node0 = S.chunk_node0[ch] + 32 * k;
-    if (nn > 0)
-        spmv_rows<QB, TPR, 4>(
-            S.pres_idx, node0 * S.nd, (node0 + nn) * S.nd, indptr, indices, val, [&](int32_t c) { return p[c]; },
-            [&](int64_t row, double v) { q[row] = v; });
+    const int grp = threadIdx.x / TPR, sub = threadIdx.x % TPR;
+    const bool on = grp < nn;
+    const int64_t A = node0 + grp;
+    const int64_t bb = on ? bptr[A] : 0;
+    const int nba = on ? (int)(bptr[A + 1] - bb) : 0;
+    double sv[ND];
+    node_rows_dot<ND, TPR>(bb, nba, sub, val, bcol,
+                           [&](int32_t c, double (&x)[ND]) {
+#pragma unroll
+                               for (int j = 0; j < ND; j++) x[j] = p[(int64_t)c * ND + j];
+                           },
+                           sv);
+    if (on && sub == 0) {
+#pragma unroll
+        for (int i = 0; i < ND; i++) q[A * ND + i] = (S.pres_idx[A * ND + i] >= 0) ? 0.0 : sv[i];
+    }
     __syncthreads();
     if (threadIdx.x < 32) {
         const int64_t i0 = (node0 + threadIdx.x) * S.nd;
@@ -535,9 +517,9 @@ constexpr int TEAM_MAX_CHUNKS = 256;  // chunks of a team problem
 constexpr size_t TEAM_SMEM_LIMIT = 200 * 1024;
 
 // Shared memory of a team CTA: doubles p, q, r, z, x (npc*nd each), the inverse diagonal blocks
-// (npc*nd*nd), three chunk-partial arrays and the reduction scratch (2*bd); then int32 row
-// pointers of its rows (npc*nd + 1) and the CTAs' node offsets (TEAM_MAX + 1); then one byte per
-// DOF (-1 free, 0 prescribed).
+// (npc*nd*nd), three chunk-partial arrays and the reduction scratch (2*bd); then int32 block
+// pointers of its nodes (npc*nd + 1 room) and the CTAs' node offsets (TEAM_MAX + 1); then one byte
+// per DOF (-1 free, 0 prescribed).
 __host__ __device__ inline size_t team_fixed_bytes(int bd) {
     return (size_t)8 * (3 * TEAM_MAX_CHUNKS + 2 * bd) + 4 * (TEAM_MAX + 2) + 16;
 }
@@ -553,14 +535,13 @@ __host__ __device__ inline size_t team_smem_bytes(int nd, int bd) {
 
 template <int BD, int TPR>
 __global__ void __launch_bounds__(BD, 1)
-pcg_team_kernel(SolverArgs S, const int32_t* list, const int64_t* __restrict__ indptr,
-                const int32_t* __restrict__ indices, const double* __restrict__ val, const double* binv_g,
+pcg_team_kernel(SolverArgs S, const int32_t* list, const int64_t* __restrict__ bptr,
+                const int32_t* __restrict__ bcol, const double* __restrict__ val, const double* binv_g,
                 double* x_g, double* r_g, double* z_g, double* p_g, double* rho_g, const double* r0_g,
                 int32_t* iters_g, uint8_t* cta_active, double rtol, int32_t max_iter, int32_t budget) {
     namespace cg = cooperative_groups;
     constexpr int G = BD / CHN;
-    constexpr int RT = BD >= 1024 ? 2 : 4;  // rows per lane group per SpMV pass
-    constexpr int nd = TPR == 8 ? 2 : 3;    // DOFs per node (the lanes per row follow the dimension)
+    constexpr int nd = TPR == 8 ? 2 : 3;    // DOFs per node (the lanes per node follow the dimension)
     cg::cluster_group cl = cg::this_cluster();
     const int C = (int)cl.num_blocks();
     const int me = (int)cl.block_rank();
@@ -583,7 +564,7 @@ pcg_team_kernel(SolverArgs S, const int32_t* list, const int64_t* __restrict__ i
     double* part_rz = part_pq + TEAM_MAX_CHUNKS;
     double* part_rr = part_rz + TEAM_MAX_CHUNKS;
     double* red = part_rr + TEAM_MAX_CHUNKS;     // 2 * BD
-    int32_t* rp = (int32_t*)(red + 2 * BD);      // npc * nd + 1 row pointers (relative)
+    int32_t* rp = (int32_t*)(red + 2 * BD);      // block pointers of my nodes (relative; npc * nd + 1 room)
     int32_t* kb = rp + npc * nd + 1;             // TEAM_MAX + 1 node offsets of the CTAs' runs
     int8_t* fr = (int8_t*)(kb + TEAM_MAX + 1);   // npc * nd: -1 free DOF, 0 prescribed
     const int64_t c0 = S.pchunk[pr];
@@ -598,17 +579,16 @@ pcg_team_kernel(SolverArgs S, const int32_t* list, const int64_t* __restrict__ i
     const int cb = (int)((int64_t)me * nch / C), ce = (int)((int64_t)(me + 1) * nch / C);  // my chunks
     const int nb = kb[me], ne = kb[me + 1];                                               // my nodes
     const int64_t gd0 = (n0 + nb) * nd;  // my first DOF (= first row)
-    const int ndl = (ne - nb) * nd;
-    const int64_t kbase = indptr[gd0];
+    const int nloc = ne - nb, ndl = nloc * nd;
+    const int64_t bbase = bptr[n0 + nb];
     for (int i = threadIdx.x; i < ndl; i += BD) {
         ps[i] = p_g[gd0 + i];
         rs[i] = r_g[gd0 + i];
         zs[i] = z_g[gd0 + i];
         xs[i] = x_g[gd0 + i];
         fr[i] = S.pres_idx[gd0 + i] < 0 ? -1 : 0;
-        rp[i] = (int32_t)(indptr[gd0 + i] - kbase);
     }
-    if (threadIdx.x == 0) rp[ndl] = (int32_t)(indptr[gd0 + ndl] - kbase);
+    for (int i = threadIdx.x; i <= nloc; i += BD) rp[i] = (int32_t)(bptr[n0 + nb + i] - bbase);
     for (int i = threadIdx.x; i < ndl * nd; i += BD) bs[i] = binv_g[gd0 * nd + i];
     double rho = rho_g[pr];
     const double r0 = r0_g[pr];
@@ -616,36 +596,33 @@ pcg_team_kernel(SolverArgs S, const int32_t* list, const int64_t* __restrict__ i
     bool active = true;
     const int g = threadIdx.x / CHN, tg = threadIdx.x % CHN;
     const int sub = threadIdx.x % TPR, grp = threadIdx.x / TPR;
-    // x[col] of the problem: from my shared memory or from the owning CTA's
-    auto gather = [&](int32_t col) -> double {
-        const int64_t l = col - gd0;
-        if (l >= 0 && l < ndl) return ps[l];
-        const int node = col / nd - (int)n0;
-        // owner of chunk c: the largest k with floor(k*nch/C) <= c
-        const int k = (int)(((int64_t)(node / CHN + 1) * C - 1) / nch);
-        const double* rpk = cl.map_shared_rank(ps, k);
-        return rpk[(node - kb[k]) * nd + col % nd];
+    // p of node B of the problem: from my shared memory or from the owning CTA's
+    auto gather = [&](int32_t B, double (&xv)[nd]) {
+        const int node = B - (int)n0;
+        const double* src;
+        if (node >= nb && node < ne) {
+            src = ps + (node - nb) * nd;
+        } else {
+            // owner of chunk c: the largest k with floor(k*nch/C) <= c
+            const int k = (int)(((int64_t)(node / CHN + 1) * C - 1) / nch);
+            src = cl.map_shared_rank(ps, k) + (node - kb[k]) * nd;
+        }
+#pragma unroll
+        for (int j = 0; j < nd; j++) xv[j] = src[j];
     };
     team_sync();  // every CTA holds its p before the first remote read
     for (int step = 0; step < budget && active; step++) {
-        // q = K p on my rows
-        for (int base = 0; base < ndl; base += RT * (BD / TPR)) {
-            int row[RT];
-            bool on[RT];
-            int64_t k0[RT], k1[RT];
-            double sv[RT];
+        // q = K p on my nodes (one group of TPR lanes per node)
+        for (int base = 0; base < nloc; base += BD / TPR) {
+            const int ln = base + grp;
+            const bool on = ln < nloc;
+            const int64_t bb = on ? bbase + rp[ln] : 0;
+            const int nba = on ? rp[ln + 1] - rp[ln] : 0;
+            double sv[nd];
+            node_rows_dot<nd, TPR>(bb, nba, sub, val, bcol, gather, sv);
+            if (on && sub == 0) {
 #pragma unroll
-            for (int j = 0; j < RT; j++) {
-                row[j] = base + j * (BD / TPR) + grp;
-                on[j] = row[j] < ndl;
-                k0[j] = on[j] ? kbase + rp[row[j]] : 0;
-                k1[j] = on[j] ? kbase + rp[row[j] + 1] : 0;
-            }
-            rows_dot_pf<TPR, RT, 4>(k0, k1, sub, val, indices, gather, sv);
-            if (sub == 0) {
-#pragma unroll
-                for (int j = 0; j < RT; j++)
-                    if (on[j]) qs[row[j]] = (fr[row[j]] >= 0) ? 0.0 : sv[j];
+                for (int i = 0; i < nd; i++) qs[ln * nd + i] = (fr[ln * nd + i] >= 0) ? 0.0 : sv[i];
             }
         }
         __syncthreads();
@@ -1043,7 +1020,9 @@ int ensure_graph(pms_batch* b) {
         const double* val = b->d_csr;
         double rtol = b->cfg.pcg_rtol;
         int32_t max_iter = b->cfg.pcg_max_iterations;
-        void* a1[] = {&b->S, &par, (void*)&b->d_indptr, (void*)&b->d_indices, (void*)&val, &b->d_p, &b->d_q,
+        const int64_t* bptr = b->v.d_bptr;
+        const int32_t* bcol = b->v.d_bcol;
+        void* a1[] = {&b->S, &par, (void*)&bptr, (void*)&bcol, (void*)&val, &b->d_p, &b->d_q,
                       &b->d_part_c};
         void* a2[] = {&b->S, &par, &b->d_part_c, &b->d_rho, &b->d_p, &b->d_q, &b->d_binv, &b->d_x, &b->d_r,
                       &b->d_z, &b->d_part_a, &b->d_part_b, &b->d_nactive};
@@ -1082,7 +1061,7 @@ cudaError_t launch_team_t(pms_batch* b, const int32_t* list, int n, int C, int b
     at[0].val.clusterDim.z = 1;
     cfg.attrs = at;
     cfg.numAttrs = 1;
-    return cudaLaunchKernelEx(&cfg, pcg_team_kernel<BD, TPR>, b->S, list, b->d_indptr, b->d_indices,
+    return cudaLaunchKernelEx(&cfg, pcg_team_kernel<BD, TPR>, b->S, list, b->v.d_bptr, b->v.d_bcol,
                               (const double*)b->d_csr, (const double*)b->d_binv, b->d_x, b->d_r, b->d_z, b->d_p,
                               b->d_rho, (const double*)b->d_r0, b->d_iters, b->d_cta_active, b->cfg.pcg_rtol,
                               b->cfg.pcg_max_iterations, budget);
@@ -1686,6 +1665,7 @@ int build_step_graph(pms_batch* b) {
     const void* spmv = tpr == 8 ? (const void*)spmv_kernel<8> : (const void*)spmv_kernel<16>;
     const int64_t* bptr = b->v.d_bptr;
     const int32_t* kdiag = b->v.d_kdiag;
+    const int32_t* bcol = b->v.d_bcol;
     const double* csr = b->d_csr;
     const double* fext = b->d_fext;
     GraphChain top{G};
@@ -1733,7 +1713,7 @@ int build_step_graph(pms_batch* b) {
     int par0 = 0, par1 = 1;
     for (int k = 0; k < 2; k++) {
         int* par = k ? &par1 : &par0;
-        void* a1[] = {&S, par, &b->d_indptr, &b->d_indices, (void*)&csr, &b->d_p, &b->d_q, &b->d_part_c};
+        void* a1[] = {&S, par, (void*)&bptr, (void*)&bcol, (void*)&csr, &b->d_p, &b->d_q, &b->d_part_c};
         pcg.kernel(spmv_dot, 4 * nch, qthreads, a1);
         void* a2[] = {&S, par, &b->d_part_c, &b->d_rho, &b->d_p, &b->d_q, &b->d_binv, &b->d_x, &b->d_r, &b->d_z,
                       &b->d_part_a, &b->d_part_b, &b->d_nactive};
