@@ -92,7 +92,8 @@ typedef struct pms_config {
 typedef struct pms_elements_info {
     int32_t ndim, kind, nnode, ngauss, ncomp;  /* ncomp = Mandel components (4 in 2D, 6 in 3D) */
     int64_t npoint, ncell, ndof, nip;          /* nip = ncell*ngauss */
-    int64_t nnz;                               /* CSR nonzeros of K (full, both triangles) */
+    int64_t nnz;                               /* CSR nonzeros of K in the storage set by
+                                                  pms_elements_set_symmetry (default: both triangles) */
     int64_t nblock_upper;                      /* node-pair blocks with A <= B */
     int64_t ncontrib;                          /* element blocks summed into them */
     int64_t device_bytes;                      /* device memory held by the handle so far */
@@ -107,6 +108,12 @@ int pms_elements_create(const pms_mesh* mesh, const pms_material* materials, int
                         const pms_config* config, pms_elements** out);
 void pms_elements_destroy(pms_elements* h);
 int pms_elements_get_info(const pms_elements* h, pms_elements_info* out);
+/* ElementTrait::symmetric_jacobian (src/fem/element_solid.rs:100-102): 1 when the Jacobian of every
+ * cell is symmetric, i.e. every material's symmetric_stiffness() is true -- always, for the linear
+ * elastic (src/material/linear_elastic.rs:26-28) and von Mises (src/material/von_mises.rs:92-94)
+ * models.  A caller picks the storage of K from it as LinearSystem::new does
+ * (src/fem/linear_system.rs:96-119; pms_elements_set_symmetry). */
+int pms_elements_symmetric_jacobian(const pms_elements* h, int32_t* out);
 /* stream: a cudaStream_t (or NULL for the handle's own stream) */
 int pms_elements_set_stream(pms_elements* h, void* stream);
 /* CSR pattern of K (sorted columns): indptr[ndof+1], indices[nnz] (host or device) */

@@ -128,6 +128,7 @@ SIGNATURES = {
     "pms_elements_set_timing": (_I, [_V, _I]),
     "pms_elements_set_assembly": (_I, [_V, _I]),
     "pms_elements_set_symmetry": (_I, [_V, _I]),
+    "pms_elements_symmetric_jacobian": (_I, [_V, _V]),
     "pms_set_device": (_I, [_I]),
     "pms_shape_table": (_I, [_I, _I, _V, _V]),
     "pms_mesh_assembly_maps": (_I, [ctypes.POINTER(Mesh_), _V, _V, _V, _V]),

@@ -2409,6 +2409,14 @@ int pms_elements_create(const pms_mesh* mesh, const pms_material* materials, int
 
 void pms_elements_destroy(pms_elements* h) { delete h; }
 
+int pms_elements_symmetric_jacobian(const pms_elements* h, int32_t* out) {
+    if (!h || !out) return PMS_ERR_INVALID;
+    bool sym = true;
+    for (const MatConst& m : h->mats) sym = sym && (m.model == PMS_LINEAR_ELASTIC || m.model == PMS_VON_MISES);
+    *out = sym ? 1 : 0;
+    return PMS_OK;
+}
+
 int pms_elements_get_info(const pms_elements* h, pms_elements_info* o) {
     if (!h || !o) return PMS_ERR_INVALID;
     o->ndim = h->nd;

@@ -97,6 +97,13 @@ class Elements:
         code = {"direct": _lib.PMS_ASSEMBLY_DIRECT, "gather": _lib.PMS_ASSEMBLY_GATHER}[mode]
         self._check(self.L.pms_elements_set_assembly(self.h, code))
 
+    def symmetric_jacobian(self):
+        """ElementTrait::symmetric_jacobian (src/fem/element_solid.rs:100-102): True for the linear
+        elastic and von Mises models."""
+        out = ctypes.c_int32()
+        self._check(self.L.pms_elements_symmetric_jacobian(self.h, ctypes.byref(out)))
+        return bool(out.value)
+
     def set_symmetry(self, sym):
         """Storage of K in the CSR values, as russell_sparse's Sym (src/fem/linear_system.rs:119,
         src/base/assembly.rs:92-136): "full" (default, both triangles), "lower" (column <= row,

@@ -54,6 +54,7 @@ def test_triangles_hold_the_full_matrix_bits(kind):
     assert np.array_equal(oip, ip) and np.array_equal(oix, ix)
     assert_close(full, ov, what="K full")
     nnz_full = g.nnz
+    assert g.symmetric_jacobian()  # von Mises: symmetric_stiffness() is true (von_mises.rs:92-94)
     for sym in ("lower", "upper"):
         tp, tx, tv = _triangle(ip, ix, full, sym)
         g.set_symmetry(sym)
