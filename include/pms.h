@@ -211,6 +211,9 @@ int pms_mesh_assembly_maps(const pms_mesh* mesh, int16_t* cslot, int32_t* crank,
 /* Host-only (no GPU needed): the CSR pattern pms_elements_create would build for this mesh.
  * Call with indices = NULL to get nnz (indptr[ndof+1] may already be filled). */
 int pms_mesh_csr_pattern(const pms_mesh* mesh, int64_t* indptr, int32_t* indices, int64_t* nnz);
+/* Host-only (no GPU needed): the same in the storage sym of pms_elements_set_symmetry (enum pms_sym;
+ * the full pattern's entries with column <= row, or >= row, in the same order). */
+int pms_mesh_csr_pattern_sym(const pms_mesh* mesh, int32_t sym, int64_t* indptr, int32_t* indices, int64_t* nnz);
 
 /* Waits for the handle's stream and returns the first device-side error (PMS_OK if none). */
 int pms_elements_sync(pms_elements* h);

@@ -125,6 +125,7 @@ SIGNATURES = {
                                        ctypes.POINTER(EpSettings_), _V, _V]),
     "pms_vm_update_and_stiffness_host": (_I, [ctypes.POINTER(Material_), _I, _I64, _V, _V, _V, _V, _V, _V, _V]),
     "pms_mesh_csr_pattern": (_I, [ctypes.POINTER(Mesh_), _V, _V, ctypes.POINTER(_I64)]),
+    "pms_mesh_csr_pattern_sym": (_I, [ctypes.POINTER(Mesh_), _I, _V, _V, ctypes.POINTER(_I64)]),
     "pms_elements_set_timing": (_I, [_V, _I]),
     "pms_elements_set_assembly": (_I, [_V, _I]),
     "pms_elements_set_symmetry": (_I, [_V, _I]),

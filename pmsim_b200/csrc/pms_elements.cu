@@ -2441,6 +2441,42 @@ int pms_elements_set_stream(pms_elements* h, void* stream) {
     return PMS_OK;
 }
 
+// Triangle storages: the first value of each node's rows (npoint + 1).  Node A's rows hold its blocks
+// on the stored side of the diagonal block and that block's own triangle (nd(nd+1)/2 entries).
+static std::vector<int64_t> triangle_base(const Pattern& p, int nd, int64_t npoint, int sym) {
+    const int64_t bb = (int64_t)nd * nd;
+    std::vector<int64_t> tb(npoint + 1, 0);
+    for (int64_t A = 0; A < npoint; A++) {
+        const int64_t nb = p.bptr[A + 1] - p.bptr[A], dp = p.kdiag[A];
+        tb[A + 1] = tb[A] + bb * (sym == PMS_SYM_LOWER ? dp : nb - dp - 1) + (int64_t)nd * (nd + 1) / 2;
+    }
+    return tb;
+}
+
+// indptr[npoint*nd + 1] / indices (either may be null) of K in the storage sym; tbase: the
+// triangle_base of sym (unused for PMS_SYM_FULL).  Returns the number of values.
+static int64_t fill_pattern(const Pattern& p, int nd, int64_t npoint, int sym, const std::vector<int64_t>& tbase,
+                            int64_t* ipo, int32_t* ixo) {
+    const int64_t nnz = sym == PMS_SYM_FULL ? p.nblock() * nd * nd : tbase[npoint];
+    for (int64_t A = 0; A < npoint; A++) {
+        const int64_t b0 = p.bptr[A], nb = p.bptr[A + 1] - b0;
+        int64_t start = sym == PMS_SYM_FULL ? (int64_t)nd * nd * b0 : tbase[A];
+        for (int i = 0; i < nd; i++) {
+            const int64_t r = A * nd + i;
+            if (ipo) ipo[r] = start;
+            for (int64_t k = 0; k < nb; k++)
+                for (int j = 0; j < nd; j++) {
+                    const int64_t c = (int64_t)p.bcol[b0 + k] * nd + j;
+                    if ((sym == PMS_SYM_LOWER && c > r) || (sym == PMS_SYM_UPPER && c < r)) continue;
+                    if (ixo) ixo[start] = (int32_t)c;
+                    start++;
+                }
+        }
+    }
+    if (ipo) ipo[npoint * nd] = nnz;
+    return nnz;
+}
+
 // The CSR pattern of K in the layout sym (the device-side users inside the library take the full one).
 static int csr_pattern(pms_elements* h, int64_t* indptr, int32_t* indices, int32_t mem, int sym) {
     const int nd = h->nd;
@@ -2455,23 +2491,7 @@ static int csr_pattern(pms_elements* h, int64_t* indptr, int32_t* indices, int32
         ipo = ip.data();
         ixo = indices ? ix.data() : nullptr;
     }
-    const Pattern& p = h->pat;
-    for (int64_t A = 0; A < h->npoint; A++) {
-        const int64_t b0 = p.bptr[A], nb = p.bptr[A + 1] - b0;
-        int64_t start = sym == PMS_SYM_FULL ? (int64_t)nd * nd * b0 : h->tbase[A];
-        for (int i = 0; i < nd; i++) {
-            const int64_t r = A * nd + i;
-            if (ipo) ipo[r] = start;
-            for (int64_t k = 0; k < nb; k++)
-                for (int j = 0; j < nd; j++) {
-                    const int64_t c = (int64_t)p.bcol[b0 + k] * nd + j;
-                    if ((sym == PMS_SYM_LOWER && c > r) || (sym == PMS_SYM_UPPER && c < r)) continue;
-                    if (ixo) ixo[start] = (int32_t)c;
-                    start++;
-                }
-        }
-    }
-    if (ipo) ipo[h->ndof] = nnz;
+    fill_pattern(h->pat, nd, h->npoint, sym, h->tbase, ipo, ixo);
     if (mem == PMS_MEM_DEVICE) {
         if (indptr && cudaMemcpy(indptr, ip.data(), ip.size() * 8, cudaMemcpyHostToDevice) != cudaSuccess)
             return fail(h, PMS_ERR_CUDA, "copy of indptr failed");
@@ -2764,15 +2784,7 @@ int pms_elements_set_symmetry(pms_elements* h, int32_t sym) {
     if (sym != PMS_SYM_FULL && h->assembly == PMS_ASSEMBLY_DIRECT)
         return fail(h, PMS_ERR_UNSUPPORTED, "the direct assembly writes both triangles of K");
     if (sym != PMS_SYM_FULL) {
-        // node A's rows hold its blocks on the stored side of the diagonal block, and the diagonal
-        // block's own triangle (nd(nd+1)/2 entries)
-        const Pattern& p = h->pat;
-        const int64_t nd = h->nd, bb = nd * nd;
-        std::vector<int64_t> tb(h->npoint + 1, 0);
-        for (int64_t A = 0; A < h->npoint; A++) {
-            const int64_t nb = p.bptr[A + 1] - p.bptr[A], dp = p.kdiag[A];
-            tb[A + 1] = tb[A] + bb * (sym == PMS_SYM_LOWER ? dp : nb - dp - 1) + nd * (nd + 1) / 2;
-        }
+        std::vector<int64_t> tb = triangle_base(h->pat, h->nd, h->npoint, sym);
         if (!h->d_tbase && !h->alloc(&h->d_tbase, (size_t)h->npoint + 1))
             return fail(h, PMS_ERR_NOMEM, "out of device memory");
         if (cudaMemcpy(h->d_tbase, tb.data(), tb.size() * 8, cudaMemcpyHostToDevice) != cudaSuccess)
@@ -2840,28 +2852,24 @@ int pms_shape_table(int32_t kind, int32_t ngauss, double* tab, int32_t* ngauss_o
     return PMS_OK;
 }
 
-int pms_mesh_csr_pattern(const pms_mesh* mesh, int64_t* indptr, int32_t* indices, int64_t* nnz) {
-    if (!mesh || !mesh->cells || kind_nnode(mesh->kind) < 0 || kind_ndim(mesh->kind) != mesh->ndim)
+int pms_mesh_csr_pattern_sym(const pms_mesh* mesh, int32_t sym, int64_t* indptr, int32_t* indices, int64_t* nnz) {
+    if (!mesh || !mesh->cells || kind_nnode(mesh->kind) < 0 || kind_ndim(mesh->kind) != mesh->ndim ||
+        (sym != PMS_SYM_FULL && sym != PMS_SYM_LOWER && sym != PMS_SYM_UPPER))
         return PMS_ERR_INVALID;
     Pattern p;
     const char* msg = nullptr;
     const int nd = mesh->ndim;
     if (!build_pattern(nd, kind_nnode(mesh->kind), mesh->npoint, mesh->ncell, mesh->cells, p, &msg))
         return PMS_ERR_INVALID;
-    const int64_t total = p.nblock() * nd * nd;
+    const std::vector<int64_t> tb =
+        sym == PMS_SYM_FULL ? std::vector<int64_t>() : triangle_base(p, nd, mesh->npoint, sym);
+    const int64_t total = fill_pattern(p, nd, mesh->npoint, sym, tb, indptr, indices);
     if (nnz) *nnz = total;
-    for (int64_t A = 0; A < mesh->npoint; A++) {
-        int64_t b0 = p.bptr[A], nb = p.bptr[A + 1] - b0;
-        for (int i = 0; i < nd; i++) {
-            int64_t start = (int64_t)nd * nd * b0 + (int64_t)i * nd * nb;
-            if (indptr) indptr[A * nd + i] = start;
-            if (indices)
-                for (int64_t k = 0; k < nb; k++)
-                    for (int j = 0; j < nd; j++) indices[start + k * nd + j] = p.bcol[b0 + k] * nd + j;
-        }
-    }
-    if (indptr) indptr[mesh->npoint * nd] = total;
     return PMS_OK;
+}
+
+int pms_mesh_csr_pattern(const pms_mesh* mesh, int64_t* indptr, int32_t* indices, int64_t* nnz) {
+    return pms_mesh_csr_pattern_sym(mesh, PMS_SYM_FULL, indptr, indices, nnz);
 }
 
 }  // extern "C"

@@ -56,6 +56,33 @@ def test_host_csr_pattern_matches_oracle(kind):
     assert np.array_equal(ip, indptr) and np.array_equal(ix, indices)
 
 
+@pytest.mark.parametrize("kind", [M.TRI3, M.QUA8, M.TET4, M.HEX8, M.HEX20])
+def test_host_triangle_patterns(kind):
+    """Sym::YesLower / YesUpper storage (src/base/assembly.rs:92-122): the full pattern's entries with
+    column <= row (lower) or >= row (upper), in order; a symmetric pattern keeps its diagonal and
+    half of the rest."""
+    if M.KIND_NDIM[kind] == 2:
+        m = M.structured_2d(kind, 4, 3, 4.0, 3.0)
+    else:
+        m = M.structured_3d(kind, 2, 2, 2)
+    L = _lib.load()
+    cm = _lib.Mesh_(m.ndim, m.kind, m.npoint, m.ncell, _lib.ptr(m.coords), _lib.ptr(m.cells), None)
+    o = oracle.OracleElements(m, 0, oracle.Params(1.0, 0.3))
+    o.initialize()
+    ip, ix, _ = o.assemble_kk_csr()
+    rows = np.repeat(np.arange(m.ndof), np.diff(ip))
+    for sym, keep in ((_lib.PMS_SYM_LOWER, ix <= rows), (_lib.PMS_SYM_UPPER, ix >= rows)):
+        nnz = ctypes.c_int64()
+        assert L.pms_mesh_csr_pattern_sym(ctypes.byref(cm), sym, None, None, ctypes.byref(nnz)) == 0
+        assert nnz.value == int(keep.sum()) and 2 * nnz.value - m.ndof == len(ix)
+        indptr = np.zeros(m.ndof + 1, np.int64)
+        indices = np.zeros(nnz.value, np.int32)
+        assert L.pms_mesh_csr_pattern_sym(ctypes.byref(cm), sym, _lib.ptr(indptr), _lib.ptr(indices), None) == 0
+        assert np.array_equal(indices, ix[keep])
+        assert np.array_equal(np.diff(indptr), np.bincount(rows[keep], minlength=m.ndof))
+    assert L.pms_mesh_csr_pattern_sym(ctypes.byref(cm), 3, None, None, None) == _lib.PMS_ERR_INVALID
+
+
 def test_hex20_block_sizes_of_the_large_problem():
     """64x64x32 Hex20: 549,185 points, 1,647,555 DOF, nnz 279,514,377 (host pattern, no GPU)."""
     m = M.structured_3d(M.HEX20, 64, 64, 32, 64.0, 64.0, 32.0)
@@ -65,6 +92,8 @@ def test_hex20_block_sizes_of_the_large_problem():
     nnz = ctypes.c_int64()
     assert L.pms_mesh_csr_pattern(ctypes.byref(cm), None, None, ctypes.byref(nnz)) == 0
     assert nnz.value == 279514377
+    assert L.pms_mesh_csr_pattern_sym(ctypes.byref(cm), _lib.PMS_SYM_LOWER, None, None, ctypes.byref(nnz)) == 0
+    assert nnz.value == (279514377 + 1647555) // 2  # 140,580,966 values of MUMPS's lower triangle
 
 
 def test_invalid_arguments_are_rejected_without_gpu():
