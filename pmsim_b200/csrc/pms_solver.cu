@@ -83,20 +83,22 @@ __device__ __forceinline__ double quarters(double q0, double q1, double q2, doub
     return MAX ? fmax(fmax(q0, q1), fmax(q2, q3)) : (q0 + q1) + (q2 + q3);
 }
 
-// All threads of the block must call it; sh holds at least 4 doubles per group.
+// All threads of the block must call it; sh holds at least 4 doubles per group.  trailing = false
+// leaves out the barrier that protects sh from the block's next write to it: for a caller whose next
+// write to sh follows another block (or cluster) barrier anyway, or goes to another region.
 template <bool MAX>
-__device__ __forceinline__ double group_reduce(double v, double* sh) {
+__device__ __forceinline__ double group_reduce(double v, double* sh, bool trailing = true) {
     const double w = warp_tree<MAX>(v);
     double* s = sh + 4 * (threadIdx.x / CHN);
     if ((threadIdx.x & 31) == 0) s[(threadIdx.x & (CHN - 1)) >> 5] = w;
     __syncthreads();
     const double r = quarters<MAX>(s[0], s[1], s[2], s[3]);
-    __syncthreads();
+    if (trailing) __syncthreads();
     return r;
 }
 
 // Two sums at once (same trees as two group_reduce<false> calls); sh holds 8 doubles per group.
-__device__ __forceinline__ void group_reduce2(double& a, double& b, double* sh) {
+__device__ __forceinline__ void group_reduce2(double& a, double& b, double* sh, bool trailing = true) {
     const double wa = warp_tree<false>(a), wb = warp_tree<false>(b);
     double* s = sh + 8 * (threadIdx.x / CHN);
     if ((threadIdx.x & 31) == 0) {
@@ -107,16 +109,17 @@ __device__ __forceinline__ void group_reduce2(double& a, double& b, double* sh) 
     __syncthreads();
     a = quarters<false>(s[0], s[1], s[2], s[3]);
     b = quarters<false>(s[4], s[5], s[6], s[7]);
-    __syncthreads();
+    if (trailing) __syncthreads();
 }
 
 // Total of a problem's chunk partials (the per-problem half of every PCG reduction), computed by a
 // group of 128 threads: thread t adds the partials t, t+128, ... in order, then the group tree.
 // Every PCG engine computes its totals this way, so they agree to the bit.
-__device__ __forceinline__ double problem_total(const double* part, int64_t c0, int64_t c1, double* sh) {
+__device__ __forceinline__ double problem_total(const double* part, int64_t c0, int64_t c1, double* sh,
+                                                bool trailing = true) {
     double s = 0.0;
     for (int64_t c = c0 + (threadIdx.x & (CHN - 1)); c < c1; c += CHN) s += part[c];
-    return group_reduce<false>(s, sh);
+    return group_reduce<false>(s, sh, trailing);
 }
 
 // The same total from quarter partials (four per chunk, in chunk order).
@@ -128,14 +131,14 @@ __device__ __forceinline__ double problem_total_quarters(const double* part4, in
 }
 
 __device__ __forceinline__ void problem_total2(const double* pa, const double* pb, int64_t c0, int64_t c1,
-                                               double& a, double& b, double* sh) {
+                                               double& a, double& b, double* sh, bool trailing = true) {
     a = 0.0;
     b = 0.0;
     for (int64_t c = c0 + (threadIdx.x & (CHN - 1)); c < c1; c += CHN) {
         a += pa[c];
         b += pb[c];
     }
-    group_reduce2(a, b, sh);
+    group_reduce2(a, b, sh, trailing);
 }
 
 // ---- per-row / per-node PCG arithmetic shared by both engines -----------------------------
@@ -634,12 +637,12 @@ pcg_team_kernel(SolverArgs S, const int32_t* list, const int64_t* __restrict__ b
                 const int l = (CHN * j - nb + tg) * nd;
                 v = node_dot(fr + l, nd, ps + l, qs + l);
             }
-            v = group_reduce<false>(v, red);
+            v = group_reduce<false>(v, red, j0 + G < ce);  // (region A; the cluster barrier follows)
             if (tg == 0 && j < ce)
                 for (int k = 0; k < C; k++) cl.map_shared_rank(part_pq, k)[j] = v;
         }
         team_sync();
-        const double pq = problem_total(part_pq, 0, nch, red);
+        const double pq = problem_total(part_pq, 0, nch, red + 8 * G, false);  // region B: nothing else writes it
         const double alpha = (pq != 0.0) ? rho / pq : 0.0;
         for (int j0 = cb; j0 < ce; j0 += G) {
             const int j = j0 + g;
@@ -648,7 +651,7 @@ pcg_team_kernel(SolverArgs S, const int32_t* list, const int64_t* __restrict__ b
                 const int ln = CHN * j - nb + tg, l = ln * nd;
                 node_update(fr + l, nd, alpha, ps + l, qs + l, bs + ln * nd * nd, xs + l, rs + l, zs + l, rz, r2);
             }
-            group_reduce2(rz, r2, red);
+            group_reduce2(rz, r2, red + 16 * G, j0 + G < ce);  // region C; the cluster barrier follows
             if (tg == 0 && j < ce)
                 for (int k = 0; k < C; k++) {
                     cl.map_shared_rank(part_rz, k)[j] = rz;
@@ -657,7 +660,7 @@ pcg_team_kernel(SolverArgs S, const int32_t* list, const int64_t* __restrict__ b
         }
         team_sync();
         double rzt, rrt, beta;
-        problem_total2(part_rz, part_rr, 0, nch, rzt, rrt, red);
+        problem_total2(part_rz, part_rr, 0, nch, rzt, rrt, red, false);  // region A, last written before two barriers
         const bool done = pcg_scalar_step(rzt, rrt, rho, r0, it, rtol, max_iter, beta);
         for (int i = threadIdx.x; i < ndl; i += BD) dof_direction(fr[i], beta, zs + i, ps + i);
         active = !done;
